@@ -1,0 +1,278 @@
+"""Python binding of the C ABI in include/crava_gpu.h (ctypes; no torch types cross it).
+
+The classes mirror the reference's objects on the hot path:
+
+* ``Context``   -- one device (the process-wide FFTGrid/FFTW state of the reference)
+* ``Job``       -- one AVOInversion on one block (src/avoinversion.cpp:53-111): upload the
+                   inputs, ``run()`` = constructor transforms + computePostMeanResidAndFFTCov +
+                   simulate + invFFTCovGrids, then download the outputs
+* ``fft_r2c`` / ``fft_c2r`` -- FFTGrid::fftInPlace / invFFTInPlace on a device grid
+
+The library is required: importing works without it, but every call raises
+``CravaError`` when ``libcrava_gpu.so`` is missing, so no path silently falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcrava_gpu.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEDOUT, ENUMERIC, ENOTSUP, ESTATE = range(8)
+ROLE_DATA, ROLE_MEAN, ROLE_PRIOR_COV, ROLE_ERR_CORR, ROLE_POST_COV, ROLE_SIM, ROLE_NOISE, \
+    ROLE_RESIDUAL, ROLE_POST_MEAN = range(9)
+PRIOR_SEPARABLE, PRIOR_GRIDS = 0, 1
+FLAG_HOST_NOISE, FLAG_KEEP_RESIDUAL = 1, 2
+
+# exported symbols the header declares (checked by the CPU tests)
+EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_status_string",
+           "crava_job_create", "crava_job_destroy", "crava_job_footprint", "crava_job_upload",
+           "crava_job_download", "crava_job_device_ptr", "crava_job_run", "crava_job_counters",
+           "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches"]
+
+
+class CravaError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"crava status {status}: {msg}")
+        self.status = status
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class JobDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("nxp", ctypes.c_int), ("nyp", ctypes.c_int), ("nzp", ctypes.c_int),
+                ("ntheta", ctypes.c_int), ("lz", ctypes.c_double), ("min_rel_thick", ctypes.c_double),
+                ("low_cut", ctypes.c_float), ("high_cut", ctypes.c_float), ("wnc", ctypes.c_float),
+                ("A", _dp), ("err_theta_cov", _dp), ("wavelet", _fp), ("wavelet_norm", _fp),
+                ("prior_var0", _dp), ("prior_mode", ctypes.c_int), ("corr_xy", _fp),
+                ("circ_corr_t", _fp), ("nsim", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("flags", ctypes.c_int)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [("inverted_bins", ctypes.c_longlong), ("chol_fallbacks", ctypes.c_longlong),
+                ("sim_chol_zero", ctypes.c_longlong), ("post_var0", ctypes.c_float * 9)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library; raises CravaError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CravaError(ENOTSUP, f"{LIB_PATH} is missing: build it with `python -m crava_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.crava_ctx_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t]
+    L.crava_ctx_destroy.argtypes = [vp]
+    L.crava_last_error.restype = ctypes.c_char_p
+    L.crava_status_string.restype = ctypes.c_char_p
+    L.crava_status_string.argtypes = [ctypes.c_int]
+    L.crava_job_create.argtypes = [vp, ctypes.POINTER(JobDesc), ctypes.POINTER(vp)]
+    L.crava_job_destroy.argtypes = [vp]
+    L.crava_job_footprint.argtypes = [ctypes.POINTER(JobDesc), ctypes.POINTER(ctypes.c_size_t)]
+    L.crava_job_upload.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    L.crava_job_download.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    L.crava_job_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.crava_job_run.argtypes = [vp, vp]
+    L.crava_job_counters.argtypes = [vp, ctypes.POINTER(Counters)]
+    L.crava_fft_r2c.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    L.crava_fft_c2r.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    L.crava_ctx_kernel_launches.argtypes = [vp]
+    L.crava_ctx_kernel_launches.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+def _check(status: int):
+    if status != OK:
+        L = lib()
+        raise CravaError(status, (L.crava_last_error() or b"").decode())
+
+
+class Context:
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(lib().crava_ctx_create(ctypes.byref(self._h), device, hbm_budget))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def kernel_launches(self) -> int:
+        return int(lib().crava_ctx_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            lib().crava_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_desc(blk, prior_mode: int = PRIOR_SEPARABLE, flags: int = 0, seed: Optional[int] = None,
+              nsim: Optional[int] = None):
+    """Job description of a synth.Block; returns (desc, keepalive arrays)."""
+    keep = {
+        "A": np.ascontiguousarray(blk.A, dtype=np.float64),
+        "etc": np.ascontiguousarray(blk.err_theta_cov, dtype=np.float64),
+        "wav": np.ascontiguousarray(blk.wavelet, dtype=np.float32),
+        "wn": np.ascontiguousarray(blk.wavelet_norm, dtype=np.float32),
+        "pv": np.ascontiguousarray(blk.prior_var0, dtype=np.float64),
+        "cxy": np.ascontiguousarray(blk.corr_xy, dtype=np.float32),
+        "cct": np.ascontiguousarray(blk.circ_corr_t, dtype=np.float32),
+    }
+    d = JobDesc()
+    d.nx, d.ny, d.nz = blk.nx, blk.ny, blk.nz
+    d.nxp, d.nyp, d.nzp = blk.nxp, blk.nyp, blk.nzp
+    d.ntheta = blk.ntheta
+    d.lz = float(blk.lz)
+    d.min_rel_thick = float(blk.min_rel_thick)
+    d.low_cut, d.high_cut, d.wnc = float(blk.low_cut), float(blk.high_cut), float(blk.wnc)
+    d.A = keep["A"].ctypes.data_as(_dp)
+    d.err_theta_cov = keep["etc"].ctypes.data_as(_dp)
+    d.wavelet = keep["wav"].ctypes.data_as(_fp)
+    d.wavelet_norm = keep["wn"].ctypes.data_as(_fp)
+    d.prior_var0 = keep["pv"].ctypes.data_as(_dp)
+    d.prior_mode = prior_mode
+    d.corr_xy = keep["cxy"].ctypes.data_as(_fp)
+    d.circ_corr_t = keep["cct"].ctypes.data_as(_fp)
+    d.nsim = blk.nsim if nsim is None else nsim
+    d.seed = int(blk.seed if seed is None else seed) & ((1 << 64) - 1)
+    d.flags = flags
+    return d, keep
+
+
+def footprint(blk, prior_mode=PRIOR_SEPARABLE, flags=0, nsim=None) -> int:
+    d, _keep = make_desc(blk, prior_mode, flags, nsim=nsim)
+    out = ctypes.c_size_t()
+    _check(lib().crava_job_footprint(ctypes.byref(d), ctypes.byref(out)))
+    return int(out.value)
+
+
+class Job:
+    """One inversion block on the device."""
+
+    def __init__(self, ctx: Context, blk, prior_mode: int = PRIOR_SEPARABLE, flags: int = 0,
+                 seed: Optional[int] = None, nsim: Optional[int] = None):
+        self.ctx = ctx
+        self.blk = blk
+        self.flags = flags
+        self.prior_mode = prior_mode
+        self.nsim = blk.nsim if nsim is None else nsim
+        desc, self._keep = make_desc(blk, prior_mode, flags, seed, nsim)
+        self._h = ctypes.c_void_p()
+        _check(lib().crava_job_create(ctx.handle, ctypes.byref(desc), ctypes.byref(self._h)))
+        self.shape = (blk.nzp, blk.nyp, 2 * (blk.nxp // 2 + 1))
+
+    def upload(self, role: int, index: int, host: np.ndarray, stream=None):
+        a = np.ascontiguousarray(host)
+        if a.dtype == np.complex64:
+            a = a.view(np.float32)
+        assert a.dtype == np.float32 and a.size == int(np.prod(self.shape)), (a.dtype, a.shape)
+        _check(lib().crava_job_upload(self._h, role, index, a.ctypes.data, stream))
+        return a  # caller keeps it alive until the copy is done
+
+    def download(self, role: int, index: int, out: Optional[np.ndarray] = None, stream=None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float32)
+        _check(lib().crava_job_download(self._h, role, index, out.ctypes.data, stream))
+        return out
+
+    def device_ptr(self, role: int, index: int) -> int:
+        p = ctypes.c_void_p()
+        _check(lib().crava_job_device_ptr(self._h, role, index, ctypes.byref(p)))
+        return int(p.value)
+
+    def run(self, stream=None):
+        _check(lib().crava_job_run(self._h, stream))
+
+    def counters(self) -> dict:
+        c = Counters()
+        _check(lib().crava_job_counters(self._h, ctypes.byref(c)))
+        return {"inverted_bins": c.inverted_bins, "chol_fallbacks": c.chol_fallbacks,
+                "sim_chol_zero": c.sim_chol_zero,
+                "post_var0": np.array(list(c.post_var0), dtype=np.float32).reshape(3, 3)}
+
+    def upload_block(self, cov_grids=None, err_corr=None, noise=None):
+        """Upload data and prior mean (and the GRIDS-mode prior, host noise)."""
+        keep = []
+        blk = self.blk
+        for l in range(blk.ntheta):
+            keep.append(self.upload(ROLE_DATA, l, blk.data[l]))
+        for a in range(3):
+            keep.append(self.upload(ROLE_MEAN, a, blk.mean[a]))
+        if self.prior_mode == PRIOR_GRIDS:
+            rnxp = self.shape[2]
+            for q in range(6):
+                g = np.zeros(self.shape, dtype=np.float32)
+                g[..., :blk.nxp] = cov_grids[q]
+                keep.append(self.upload(ROLE_PRIOR_COV, q, g))
+            g = np.zeros(self.shape, dtype=np.float32)
+            g[..., :blk.nxp] = err_corr
+            keep.append(self.upload(ROLE_ERR_CORR, 0, g))
+        if self.flags & FLAG_HOST_NOISE:
+            for s in range(self.nsim):
+                for a in range(3):
+                    keep.append(self.upload(ROLE_NOISE, 3 * s + a, noise[s, a]))
+        return keep
+
+    def download_outputs(self) -> dict:
+        blk = self.blk
+        out = {"mean": np.stack([self.download(ROLE_POST_MEAN, a) for a in range(3)]),
+               "cov": np.stack([self.download(ROLE_POST_COV, q) for q in range(6)])}
+        if self.nsim:
+            out["sims"] = np.stack([self.download(ROLE_SIM, q) for q in range(3 * self.nsim)]).reshape(
+                (self.nsim, 3) + self.shape)
+        if self.flags & FLAG_KEEP_RESIDUAL:
+            out["resid_spec"] = np.stack([self.download(ROLE_RESIDUAL, l).view(np.complex64)
+                                          for l in range(blk.ntheta)])
+        return out
+
+    def close(self):
+        if self._h:
+            lib().crava_job_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def invert_block(ctx: Context, blk, prior_mode=PRIOR_SEPARABLE, noise=None, keep_residual=False,
+                 cov_grids=None, err_corr=None, seed=None) -> dict:
+    """Host-to-host inversion of one block (the e2e path): upload, run, download."""
+    flags = (FLAG_HOST_NOISE if noise is not None else 0) | (FLAG_KEEP_RESIDUAL if keep_residual else 0)
+    job = Job(ctx, blk, prior_mode, flags, seed=seed)
+    try:
+        _keep = job.upload_block(cov_grids, err_corr, noise)
+        job.run()
+        out = job.download_outputs()
+        out["counters"] = job.counters()
+        return out
+    finally:
+        job.close()
+
+
+def fft_r2c(ctx: Context, dptr: int, nxp: int, nyp: int, nzp: int, covariance: bool, stream=None):
+    _check(lib().crava_fft_r2c(ctx.handle, ctypes.c_void_p(dptr), nxp, nyp, nzp, int(covariance), stream))
+
+
+def fft_c2r(ctx: Context, dptr: int, nxp: int, nyp: int, nzp: int, covariance: bool, stream=None):
+    _check(lib().crava_fft_c2r(ctx.handle, ctypes.c_void_p(dptr), nxp, nyp, nzp, int(covariance), stream))

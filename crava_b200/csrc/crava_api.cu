@@ -1,0 +1,672 @@
+// C ABI of the B200 AVO-inversion path (declared in include/crava_gpu.h).
+//
+// Host side of one inversion block: device grid allocation, per-kz operator tables
+// (AVOInversion's fillkW / fillkWNorm / diff operators, src/avoinversion.cpp:845-975 and
+// :1275-1300), transform plans with double-precision twiddles, and the launch sequence
+// that replaces the reference's call chain
+//   AVOInversion::AVOInversion -> computePostMeanResidAndFFTCov -> simulate ->
+//   invFFTCovGrids (src/avoinversion.cpp:229-282).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/crava_gpu.h"
+#include "kernels.cuh"
+
+using namespace crava;
+typedef std::complex<double> cd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+crava_status fail(crava_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+crava_status cuda_fail(cudaError_t e, const char* where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  return CRAVA_ECUDA;
+}
+
+#define CUDA_TRY(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+bool smooth(int n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+// Stage radices for a length-n transform: radix 8 while possible, then 4 or 2, then
+// the odd primes.
+bool make_plan(int n, LinePlan& pl) {
+  if (!smooth(n)) return false;
+  pl.n = n;
+  pl.nst = 0;
+  int m = n;
+  while (m % 8 == 0) { pl.radix[pl.nst++] = 8; m /= 8; }
+  if (m % 4 == 0) { pl.radix[pl.nst++] = 4; m /= 4; }
+  if (m % 2 == 0) { pl.radix[pl.nst++] = 2; m /= 2; }
+  for (int p : {3, 5, 7})
+    while (m % p == 0) {
+      if (pl.nst >= kMaxStages) return false;
+      pl.radix[pl.nst++] = (int8_t)p;
+      m /= p;
+    }
+  if (n == 1) { pl.radix[pl.nst++] = 2; }  // never used: n >= 2 enforced by callers
+  return m == 1;
+}
+
+struct Plan {
+  LinePlan lp;
+  float2* tw = nullptr;  // device, e^{-2 pi i t/n}
+};
+
+}  // namespace
+
+struct crava_ctx {
+  int device = 0;
+  size_t budget = 0;
+  size_t allocated = 0;
+  long long launches = 0;
+  std::mutex mu;
+  std::map<int, Plan> plans;
+};
+
+struct crava_job {
+  crava_ctx* ctx = nullptr;
+  crava_job_desc d{};
+  int cnxp = 0, rnxp = 0;
+  size_t rsize = 0;          // floats per grid
+  size_t N = 0;              // nxp*nyp*nzp
+  char* pool = nullptr;      // one allocation for everything below
+  size_t pool_bytes = 0;
+  float* in_data[kMaxTheta] = {};  // caller inputs (preserved)
+  float* in_mean[3] = {};
+  float* in_cov[6] = {};
+  float* in_err = nullptr;
+  float* data[kMaxTheta] = {};     // work: data spectra, then residual spectra
+  float* mean[3] = {};             // work: mean spectra, then posterior mean
+  float* cov[6] = {};              // work: prior spectra (GRIDS), then posterior covariance
+  float* err = nullptr;            // work: error correlation spectrum (GRIDS)
+  float* sim[3 * kMaxSim] = {};
+  float* noise[3 * kMaxSim] = {};
+  float2* kw = nullptr;
+  float2* e1 = nullptr;
+  float2* e2 = nullptr;
+  uint8_t* inv = nullptr;
+  float2* cxy = nullptr;     // SEPARABLE
+  float2* ct = nullptr;
+  float* cxy_grid = nullptr; // staging for the corr_xy transform
+  unsigned long long* counters = nullptr;
+  // host copies of the small inputs
+  std::vector<double> A, etc, pv;
+  std::vector<float> wav, wnorm, corr_xy, circ;
+  bool ran = false;
+};
+
+namespace {
+
+crava_status get_plan(crava_ctx* ctx, int n, Plan** out) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->plans.find(n);
+  if (it != ctx->plans.end()) { *out = &it->second; return CRAVA_OK; }
+  Plan p;
+  if (!make_plan(n, p.lp)) return fail(CRAVA_ENOTSUP, "transform length " + std::to_string(n) + " is not 2,3,5,7-smooth");
+  std::vector<float2> tw(n);
+  for (int t = 0; t < n; t++) {
+    double ang = 2.0 * M_PI * (double)t / (double)n;
+    tw[t] = make_float2((float)std::cos(ang), (float)(-std::sin(ang)));
+  }
+  CUDA_TRY(cudaMalloc(&p.tw, sizeof(float2) * n));
+  CUDA_TRY(cudaMemcpy(p.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  auto res = ctx->plans.emplace(n, p);
+  *out = &res.first->second;
+  return CRAVA_OK;
+}
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+struct Layout {
+  size_t grid_bytes, total;
+  size_t off_tables;
+};
+
+crava_status validate(const crava_job_desc* d) {
+  if (!d) return fail(CRAVA_EINVAL, "null job description");
+  if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->nxp < d->nx || d->nyp < d->ny || d->nzp < d->nz)
+    return fail(CRAVA_EINVAL, "inconsistent grid dimensions");
+  if (d->nxp < 2 || d->nyp < 2 || d->nzp < 2) return fail(CRAVA_ENOTSUP, "padded dimensions must be >= 2");
+  if (!smooth(d->nxp) || !smooth(d->nyp) || !smooth(d->nzp))
+    return fail(CRAVA_ENOTSUP, "padded dimensions must be 2,3,5,7-smooth");
+  if (d->nxp > 4096 || d->nyp > 4096 || d->nzp > 4096) return fail(CRAVA_ENOTSUP, "transform length above 4096");
+  if (d->nzp * 4 > 16 * 256) return fail(CRAVA_ENOTSUP, "nzp above 1024 is not supported by the pencil pass");
+  if (d->ntheta < 1 || d->ntheta > kMaxTheta) return fail(CRAVA_ENOTSUP, "ntheta must be 1..8");
+  if (d->nsim < 0 || d->nsim > kMaxSim) return fail(CRAVA_ENOTSUP, "nsim must be 0..16");
+  if (!d->A || !d->err_theta_cov || !d->wavelet || !d->wavelet_norm || !d->prior_var0)
+    return fail(CRAVA_EINVAL, "null pointer in job description");
+  if (d->prior_mode == CRAVA_PRIOR_SEPARABLE) {
+    if (!d->corr_xy || !d->circ_corr_t) return fail(CRAVA_EINVAL, "separable prior needs corr_xy and circ_corr_t");
+  } else if (d->prior_mode != CRAVA_PRIOR_GRIDS) {
+    return fail(CRAVA_EINVAL, "unknown prior mode");
+  }
+  if (!(d->lz > 0)) return fail(CRAVA_EINVAL, "lz must be positive");
+  for (int l = 0; l < d->ntheta; l++)
+    if (!(d->wavelet_norm[l] > 0)) return fail(CRAVA_EINVAL, "wavelet norm must be positive");
+  return CRAVA_OK;
+}
+
+size_t footprint(const crava_job_desc* d) {
+  size_t cnxp = d->nxp / 2 + 1;
+  size_t gb = align256(sizeof(float) * 2 * cnxp * d->nyp * d->nzp);
+  size_t ngrids = 2 * ((size_t)d->ntheta + 3) + 6 + 3 * (size_t)d->nsim;
+  if (d->prior_mode == CRAVA_PRIOR_GRIDS) ngrids += 6 + 2;
+  if (d->flags & CRAVA_FLAG_HOST_NOISE) ngrids += 3 * (size_t)d->nsim;
+  size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) + align256(d->nzp) +
+                  align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float2) * d->nzp) +
+                  align256(sizeof(float) * 2 * cnxp * d->nyp) + 256;
+  return ngrids * gb + tables;
+}
+
+// DFT of a real vector in double precision, e^{-2 pi i k t / n}.
+std::vector<cd> dft(const std::vector<double>& x) {
+  size_t n = x.size();
+  std::vector<double> c(n), s(n);
+  for (size_t q = 0; q < n; q++) {
+    double ang = 2.0 * M_PI * (double)q / (double)n;
+    c[q] = std::cos(ang);
+    s[q] = std::sin(ang);
+  }
+  std::vector<cd> X(n);
+  for (size_t k = 0; k < n; k++) {
+    double re = 0, im = 0;
+    size_t q = 0;
+    for (size_t t = 0; t < n; t++) {
+      re += x[t] * c[q];
+      im -= x[t] * s[q];
+      q += k;
+      if (q >= n) q -= n;
+    }
+    X[k] = cd(re, im);
+  }
+  return X;
+}
+
+// Per-kz operator tables, constant-thickness branch of computePostMeanResidAndFFTCov.
+void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vector<float2>& e1,
+                     std::vector<float2>& e2, std::vector<uint8_t>& inv) {
+  int n = d.nzp, nth = d.ntheta;
+  kw.assign((size_t)n * nth, make_float2(0, 0));
+  e1 = kw;
+  e2 = kw;
+  inv.assign(n, 0);
+  // diff1Operator: FIRSTORDERFORWARDDIFF, -1 at 0 and +1 at nzp-1 (src/wavelet1D.cpp:407-411)
+  std::vector<double> d1(n, 0.0);
+  d1[0] = -1.0;
+  d1[n - 1] = 1.0;
+  std::vector<cd> kD = dft(d1);
+  for (int l = 0; l < nth; l++) {
+    std::vector<float> wf(d.wavelet + (size_t)l * n, d.wavelet + (size_t)(l + 1) * n);
+    std::vector<double> w(wf.begin(), wf.end());
+    std::vector<cd> W = dft(w);
+    // errorSmooth3 = central(backward(forward(w))) in float (src/wavelet1D.cpp:438-500)
+    std::vector<float> f1(n), f2(n), f3(n);
+    for (int i = 0; i < n; i++) f1[i] = (i == n - 1) ? wf[0] - wf[i] : wf[i + 1] - wf[i];
+    for (int i = 0; i < n; i++) f2[i] = (i == 0) ? f1[0] - f1[n - 1] : f1[i] - f1[i - 1];
+    for (int i = 0; i < n; i++) {
+      if (i == 0) f3[i] = (float)(0.5 * (f2[i + 1] - f2[n - 1]));
+      else if (i == n - 1) f3[i] = (float)(0.5 * (f2[0] - f2[i - 1]));
+      else f3[i] = (float)(0.5 * (f2[i + 1] - f2[i - 1]));
+    }
+    double n3 = 0;
+    for (int i = 0; i < n; i++) n3 += (double)(f3[i] * f3[i]);
+    float norm3 = (float)std::sqrt(n3);
+    std::vector<double> e3(f3.begin(), f3.end());
+    std::vector<cd> E3 = dft(e3);
+    double wn = d.wavelet_norm[l];
+    for (int k = 0; k < n; k++) {
+      cd kwv = std::conj(W[k]) * kD[k];
+      cd a = std::conj(W[k]) / wn;
+      cd b = norm3 > 0 ? std::conj(E3[k]) / (double)norm3 : cd(0, 0);
+      kw[(size_t)k * nth + l] = make_float2((float)kwv.real(), (float)kwv.imag());
+      e1[(size_t)k * nth + l] = make_float2((float)a.real(), (float)a.imag());
+      e2[(size_t)k * nth + l] = make_float2((float)b.real(), (float)b.imag());
+    }
+  }
+  // realFrequency and the inversion band (src/avoinversion.cpp:946, :1029)
+  for (int k = 0; k < n; k++) {
+    int kk = std::min(k, n - k);
+    float rf = static_cast<float>((d.nz * 1000.0f) / (d.lz * n) * kk);
+    inv[k] = (rf > d.low_cut * d.min_rel_thick && rf < d.high_cut) ? 1 : 0;
+  }
+}
+
+float* grid_ptr(crava_job* j, crava_role role, int index, crava_status* st) {
+  *st = CRAVA_OK;
+  const crava_job_desc& d = j->d;
+  switch ((int)role) {
+    case CRAVA_ROLE_DATA:
+      if (index >= 0 && index < d.ntheta) return j->in_data[index];
+      break;
+    case CRAVA_ROLE_RESIDUAL:
+      if ((d.flags & CRAVA_FLAG_KEEP_RESIDUAL) && index >= 0 && index < d.ntheta) return j->data[index];
+      break;
+    case CRAVA_ROLE_MEAN:
+      if (index >= 0 && index < 3) return j->in_mean[index];
+      break;
+    case CRAVA_ROLE_POST_MEAN:
+      if (index >= 0 && index < 3) return j->mean[index];
+      break;
+    case CRAVA_ROLE_PRIOR_COV:
+      if (d.prior_mode == CRAVA_PRIOR_GRIDS && index >= 0 && index < 6) return j->in_cov[index];
+      break;
+    case CRAVA_ROLE_POST_COV:
+      if (index >= 0 && index < 6) return j->cov[index];
+      break;
+    case CRAVA_ROLE_ERR_CORR:
+      if (d.prior_mode == CRAVA_PRIOR_GRIDS && index == 0) return j->in_err;
+      break;
+    case CRAVA_ROLE_SIM:
+      if (index >= 0 && index < 3 * d.nsim) return j->sim[index];
+      break;
+    case CRAVA_ROLE_NOISE:
+      if ((d.flags & CRAVA_FLAG_HOST_NOISE) && index >= 0 && index < 3 * d.nsim) return j->noise[index];
+      break;
+  }
+  *st = fail(CRAVA_EINVAL, "role/index not valid for this job");
+  return nullptr;
+}
+
+float fwd_scale(size_t N) { return 1.0f / std::sqrt(static_cast<float>(N)); }
+float inv_scale(size_t N, bool cov) {
+  if (cov) return float(1.0 / (double)N);
+  return float(1.0 / std::sqrt(float(N)));
+}
+
+// 3D transforms of a list of grids (x, y[, z]) -- the FFTGrid::fftInPlace work split over
+// batched launches.
+crava_status fwd_xy(crava_ctx* ctx, const std::vector<const float*>& src, const std::vector<float*>& g,
+                    const std::vector<float>& sc, int nxp, int nyp, int nzp, bool with_z, cudaStream_t st) {
+  if (g.empty()) return CRAVA_OK;
+  Plan *px, *py, *pz;
+  crava_status s;
+  if ((s = get_plan(ctx, nxp, &px)) || (s = get_plan(ctx, nyp, &py)) || (s = get_plan(ctx, nzp, &pz))) return s;
+  int cnxp = nxp / 2 + 1;
+  int nl = 0;
+  for (size_t b = 0; b < g.size(); b += kMaxGrids) {
+    GridSet gs;
+    gs.n = (int)std::min(g.size() - b, (size_t)kMaxGrids);
+    for (int q = 0; q < gs.n; q++) { gs.p[q] = g[b + q]; gs.src[q] = src[b + q]; gs.scale[q] = sc[b + q]; }
+    CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+    CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, -1.f, st, &nl));
+    if (with_z)
+      CUDA_TRY(launch_line_fft(gs, cnxp, nzp, (size_t)cnxp * nyp, nyp, (size_t)cnxp, pz->lp, pz->tw, -1.f, st, &nl));
+  }
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+crava_status inv_xy(crava_ctx* ctx, const std::vector<float*>& g, const std::vector<float>& sc, int nxp, int nyp,
+                    int nzp, bool with_z, cudaStream_t st) {
+  if (g.empty()) return CRAVA_OK;
+  Plan *px, *py, *pz;
+  crava_status s;
+  if ((s = get_plan(ctx, nxp, &px)) || (s = get_plan(ctx, nyp, &py)) || (s = get_plan(ctx, nzp, &pz))) return s;
+  int cnxp = nxp / 2 + 1;
+  int nl = 0;
+  for (size_t b = 0; b < g.size(); b += kMaxGrids) {
+    GridSet gs;
+    gs.n = (int)std::min(g.size() - b, (size_t)kMaxGrids);
+    for (int q = 0; q < gs.n; q++) { gs.p[q] = g[b + q]; gs.src[q] = g[b + q]; gs.scale[q] = sc[b + q]; }
+    if (with_z)
+      CUDA_TRY(launch_line_fft(gs, cnxp, nzp, (size_t)cnxp * nyp, nyp, (size_t)cnxp, pz->lp, pz->tw, 1.f, st, &nl));
+    CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, 1.f, st, &nl));
+    CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+  }
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* crava_last_error(void) { return g_last_error.c_str(); }
+
+const char* crava_status_string(crava_status s) {
+  switch (s) {
+    case CRAVA_OK: return "ok";
+    case CRAVA_EINVAL: return "invalid argument";
+    case CRAVA_ENOMEM: return "out of device memory or over budget";
+    case CRAVA_ECUDA: return "CUDA error";
+    case CRAVA_ETIMEDOUT: return "timed out";
+    case CRAVA_ENUMERIC: return "numeric error";
+    case CRAVA_ENOTSUP: return "not supported";
+    case CRAVA_ESTATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+crava_status crava_ctx_create(crava_ctx** ctx, int device, size_t hbm_budget) {
+  if (!ctx) return fail(CRAVA_EINVAL, "null ctx");
+  int n = 0;
+  CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(CRAVA_EINVAL, "no such device");
+  CUDA_TRY(cudaSetDevice(device));
+  crava_ctx* c = new crava_ctx();
+  c->device = device;
+  c->budget = hbm_budget;
+  *ctx = c;
+  return CRAVA_OK;
+}
+
+crava_status crava_ctx_destroy(crava_ctx* ctx) {
+  if (!ctx) return CRAVA_OK;
+  cudaSetDevice(ctx->device);
+  for (auto& kv : ctx->plans) cudaFree(kv.second.tw);
+  delete ctx;
+  return CRAVA_OK;
+}
+
+long long crava_ctx_kernel_launches(crava_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+crava_status crava_job_footprint(const crava_job_desc* desc, size_t* bytes) {
+  crava_status s = validate(desc);
+  if (s) return s;
+  if (!bytes) return fail(CRAVA_EINVAL, "null output");
+  *bytes = footprint(desc);
+  return CRAVA_OK;
+}
+
+crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_job** job) {
+  if (!ctx || !job) return fail(CRAVA_EINVAL, "null argument");
+  crava_status s = validate(desc);
+  if (s) return s;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  size_t need = footprint(desc);
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->budget && ctx->allocated + need > ctx->budget)
+      return fail(CRAVA_ENOMEM, "job needs " + std::to_string(need) + " bytes; budget left " +
+                                    std::to_string(ctx->budget - ctx->allocated));
+  }
+  crava_job* j = new crava_job();
+  j->ctx = ctx;
+  j->d = *desc;
+  const crava_job_desc& d = j->d;
+  j->cnxp = d.nxp / 2 + 1;
+  j->rnxp = 2 * j->cnxp;
+  j->rsize = (size_t)j->rnxp * d.nyp * d.nzp;
+  j->N = (size_t)d.nxp * d.nyp * d.nzp;
+  j->A.assign(d.A, d.A + 3 * d.ntheta);
+  j->etc.assign(d.err_theta_cov, d.err_theta_cov + d.ntheta * d.ntheta);
+  j->pv.assign(d.prior_var0, d.prior_var0 + 9);
+  j->wav.assign(d.wavelet, d.wavelet + (size_t)d.ntheta * d.nzp);
+  j->wnorm.assign(d.wavelet_norm, d.wavelet_norm + d.ntheta);
+  if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) {
+    j->corr_xy.assign(d.corr_xy, d.corr_xy + (size_t)d.nxp * d.nyp);
+    j->circ.assign(d.circ_corr_t, d.circ_corr_t + d.nzp);
+  }
+  j->d.A = j->A.data();
+  j->d.err_theta_cov = j->etc.data();
+  j->d.prior_var0 = j->pv.data();
+  j->d.wavelet = j->wav.data();
+  j->d.wavelet_norm = j->wnorm.data();
+  j->d.corr_xy = j->corr_xy.empty() ? nullptr : j->corr_xy.data();
+  j->d.circ_corr_t = j->circ.empty() ? nullptr : j->circ.data();
+
+  cudaError_t e = cudaMalloc(&j->pool, need);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete j;
+    return fail(CRAVA_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  j->pool_bytes = need;
+  size_t gb = align256(sizeof(float) * j->rsize);
+  char* p = j->pool;
+  auto take = [&](size_t bytes) { char* q = p; p += align256(bytes); return q; };
+  for (int l = 0; l < d.ntheta; l++) j->in_data[l] = (float*)take(gb);
+  for (int a = 0; a < 3; a++) j->in_mean[a] = (float*)take(gb);
+  for (int l = 0; l < d.ntheta; l++) j->data[l] = (float*)take(gb);
+  for (int a = 0; a < 3; a++) j->mean[a] = (float*)take(gb);
+  for (int q = 0; q < 6; q++) j->cov[q] = (float*)take(gb);
+  if (d.prior_mode == CRAVA_PRIOR_GRIDS) {
+    for (int q = 0; q < 6; q++) j->in_cov[q] = (float*)take(gb);
+    j->in_err = (float*)take(gb);
+    j->err = (float*)take(gb);
+  }
+  for (int q = 0; q < 3 * d.nsim; q++) j->sim[q] = (float*)take(gb);
+  if (d.flags & CRAVA_FLAG_HOST_NOISE)
+    for (int q = 0; q < 3 * d.nsim; q++) j->noise[q] = (float*)take(gb);
+  j->kw = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
+  j->e1 = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
+  j->e2 = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
+  j->inv = (uint8_t*)take(d.nzp);
+  j->cxy = (float2*)take(sizeof(float2) * j->cnxp * d.nyp);
+  j->ct = (float2*)take(sizeof(float2) * d.nzp);
+  j->cxy_grid = (float*)take(sizeof(float) * j->rnxp * d.nyp);
+  j->counters = (unsigned long long*)take(256);
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->allocated += need;
+  }
+
+  // per-kz tables
+  std::vector<float2> kw, e1, e2;
+  std::vector<uint8_t> inv;
+  build_kz_tables(j->d, kw, e1, e2, inv);
+  CUDA_TRY(cudaMemcpy(j->kw, kw.data(), sizeof(float2) * kw.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(j->e1, e1.data(), sizeof(float2) * e1.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(j->e2, e2.data(), sizeof(float2) * e2.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(j->inv, inv.data(), inv.size(), cudaMemcpyHostToDevice));
+  if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) {
+    // temporal factor: DFT of circCorrT (1D, double)
+    std::vector<double> c(j->circ.begin(), j->circ.end());
+    std::vector<cd> C = dft(c);
+    std::vector<float2> ct(d.nzp);
+    for (int k = 0; k < d.nzp; k++) ct[k] = make_float2((float)C[k].real(), (float)C[k].imag());
+    CUDA_TRY(cudaMemcpy(j->ct, ct.data(), sizeof(float2) * d.nzp, cudaMemcpyHostToDevice));
+    // lateral factor: 2D transform of corrXY on the device (x then y)
+    std::vector<float> g((size_t)j->rnxp * d.nyp, 0.f);
+    for (int jj = 0; jj < d.nyp; jj++)
+      for (int ii = 0; ii < d.nxp; ii++) g[(size_t)jj * j->rnxp + ii] = j->corr_xy[(size_t)jj * d.nxp + ii];
+    CUDA_TRY(cudaMemcpy(j->cxy_grid, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice));
+    Plan *px, *py;
+    crava_status ps;
+    if ((ps = get_plan(ctx, d.nxp, &px)) || (ps = get_plan(ctx, d.nyp, &py))) return ps;
+    GridSet gs;
+    gs.n = 1;
+    gs.p[0] = j->cxy_grid;
+    gs.src[0] = j->cxy_grid;
+    gs.scale[0] = 1.0f;
+    int nl = 0;
+    CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, 0, &nl));
+    CUDA_TRY(launch_line_fft(gs, j->cnxp, d.nyp, (size_t)j->cnxp, 1, 0, py->lp, py->tw, -1.f, 0, &nl));
+    CUDA_TRY(cudaMemcpy(j->cxy, j->cxy_grid, sizeof(float2) * j->cnxp * d.nyp, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaDeviceSynchronize());
+    ctx->launches += nl;
+  }
+  *job = j;
+  return CRAVA_OK;
+}
+
+crava_status crava_job_destroy(crava_job* job) {
+  if (!job) return CRAVA_OK;
+  cudaSetDevice(job->ctx->device);
+  cudaFree(job->pool);
+  {
+    std::lock_guard<std::mutex> lk(job->ctx->mu);
+    job->ctx->allocated -= job->pool_bytes;
+  }
+  delete job;
+  return CRAVA_OK;
+}
+
+crava_status crava_job_device_ptr(crava_job* job, crava_role role, int index, float** dptr) {
+  if (!job || !dptr) return fail(CRAVA_EINVAL, "null argument");
+  crava_status s;
+  float* p = grid_ptr(job, role, index, &s);
+  if (s) return s;
+  *dptr = p;
+  return CRAVA_OK;
+}
+
+crava_status crava_job_upload(crava_job* job, crava_role role, int index, const float* host, void* stream) {
+  if (!job || !host) return fail(CRAVA_EINVAL, "null argument");
+  crava_status s;
+  float* p = grid_ptr(job, role, index, &s);
+  if (s) return s;
+  CUDA_TRY(cudaMemcpyAsync(p, host, sizeof(float) * job->rsize, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+  return CRAVA_OK;
+}
+
+crava_status crava_job_download(crava_job* job, crava_role role, int index, float* host, void* stream) {
+  if (!job || !host) return fail(CRAVA_EINVAL, "null argument");
+  if (!job->ran && (role == CRAVA_ROLE_POST_MEAN || role == CRAVA_ROLE_POST_COV || role == CRAVA_ROLE_SIM ||
+                    role == CRAVA_ROLE_RESIDUAL))
+    return fail(CRAVA_ESTATE, "outputs are defined only after crava_job_run");
+  crava_status s;
+  float* p = grid_ptr(job, role, index, &s);
+  if (s) return s;
+  CUDA_TRY(cudaMemcpyAsync(host, p, sizeof(float) * job->rsize, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  return CRAVA_OK;
+}
+
+crava_status crava_job_run(crava_job* job, void* stream) {
+  if (!job) return fail(CRAVA_EINVAL, "null job");
+  crava_ctx* ctx = job->ctx;
+  const crava_job_desc& d = job->d;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  CUDA_TRY(cudaMemsetAsync(job->counters, 0, 3 * sizeof(unsigned long long), st));
+  const bool grids = d.prior_mode == CRAVA_PRIOR_GRIDS;
+  const float fs = fwd_scale(job->N);
+  crava_status s;
+  // forward transforms: data + mean (x, y); GRIDS mode also the prior grids (x, y, z)
+  {
+    std::vector<const float*> src;
+    std::vector<float*> g;
+    std::vector<float> sc;
+    for (int l = 0; l < d.ntheta; l++) { src.push_back(job->in_data[l]); g.push_back(job->data[l]); sc.push_back(fs); }
+    for (int a = 0; a < 3; a++) { src.push_back(job->in_mean[a]); g.push_back(job->mean[a]); sc.push_back(fs); }
+    if ((s = fwd_xy(ctx, src, g, sc, d.nxp, d.nyp, d.nzp, false, st))) return s;
+  }
+  if (grids) {
+    std::vector<const float*> src;
+    std::vector<float*> g;
+    std::vector<float> sc;
+    for (int q = 0; q < 6; q++) { src.push_back(job->in_cov[q]); g.push_back(job->cov[q]); sc.push_back(1.0f); }
+    src.push_back(job->in_err);
+    g.push_back(job->err);
+    sc.push_back(1.0f);
+    if ((s = fwd_xy(ctx, src, g, sc, d.nxp, d.nyp, d.nzp, true, st))) return s;
+  }
+  // the fused pencil pass
+  Plan* pz;
+  if ((s = get_plan(ctx, d.nzp, &pz))) return s;
+  ZParams zp;
+  std::memset(&zp, 0, sizeof(zp));
+  zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = job->cnxp;
+  zp.nxp_even = (d.nxp % 2) == 0;
+  int W = 8;
+  while (W > 1 && (W * d.nzp > 16 * 256 || zpass_smem_bytes(W, d.nzp, d.ntheta) > 113 * 1024)) W /= 2;
+  if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
+  zp.W = W;
+  zp.nIT = (job->cnxp + W - 1) / W;
+  zp.nth = d.ntheta;
+  zp.nsim = d.nsim;
+  zp.separable = grids ? 0 : 1;
+  zp.host_noise = (d.flags & CRAVA_FLAG_HOST_NOISE) ? 1 : 0;
+  zp.keep_resid = (d.flags & CRAVA_FLAG_KEEP_RESIDUAL) ? 1 : 0;
+  for (int l = 0; l < d.ntheta; l++) zp.data[l] = (float2*)job->data[l];
+  for (int a = 0; a < 3; a++) zp.mean[a] = (float2*)job->mean[a];
+  for (int q = 0; q < 6; q++) zp.cov[q] = (float2*)job->cov[q];
+  zp.errspec = (const float2*)job->err;
+  for (int q = 0; q < 3 * d.nsim; q++) {
+    zp.sim[q] = (float2*)job->sim[q];
+    zp.noise[q] = (const float2*)job->noise[q];
+  }
+  zp.cxy = job->cxy;
+  zp.ct = job->ct;
+  const int qa[6] = {0, 1, 2, 0, 0, 1}, qb[6] = {0, 1, 2, 1, 2, 2};
+  for (int q = 0; q < 6; q++) zp.pv[q] = static_cast<float>(job->pv[qa[q] * 3 + qb[q]]);
+  for (int l = 0; l < d.ntheta; l++) {
+    for (int c = 0; c < 3; c++) zp.A[l][c] = static_cast<float>(job->A[l * 3 + c]);
+    for (int m = 0; m < d.ntheta; m++) zp.ec[l][m] = float(0.5 * (1.0 - d.wnc) * job->etc[l * d.ntheta + m]);
+    zp.ed[l] = float(d.wnc * job->etc[l * d.ntheta + l]);
+  }
+  zp.kz.kw = job->kw; zp.kz.e1 = job->e1; zp.kz.e2 = job->e2; zp.kz.inv = job->inv;
+  zp.zp = pz->lp;
+  zp.twz = pz->tw;
+  zp.seed = d.seed;
+  zp.counters = job->counters;
+  int nl = 0;
+  CUDA_TRY(launch_zpass(zp, st, &nl));
+  ctx->launches += nl;
+  // inverse transforms (y, x) of the outputs with FFTGrid::invFFTInPlace scales
+  {
+    std::vector<float*> g;
+    std::vector<float> sc;
+    float ps = inv_scale(job->N, false), cs = inv_scale(job->N, true);
+    for (int a = 0; a < 3; a++) { g.push_back(job->mean[a]); sc.push_back(ps); }
+    for (int q = 0; q < 6; q++) { g.push_back(job->cov[q]); sc.push_back(cs); }
+    for (int q = 0; q < 3 * d.nsim; q++) { g.push_back(job->sim[q]); sc.push_back(ps); }
+    if ((s = inv_xy(ctx, g, sc, d.nxp, d.nyp, d.nzp, false, st))) return s;
+  }
+  job->ran = true;
+  return CRAVA_OK;
+}
+
+crava_status crava_job_counters(crava_job* job, crava_counters* out) {
+  if (!job || !out) return fail(CRAVA_EINVAL, "null argument");
+  if (!job->ran) return fail(CRAVA_ESTATE, "counters are defined only after crava_job_run");
+  CUDA_TRY(cudaSetDevice(job->ctx->device));
+  unsigned long long c[3];
+  CUDA_TRY(cudaMemcpy(c, job->counters, sizeof(c), cudaMemcpyDeviceToHost));
+  out->inverted_bins = (long long)c[0];
+  out->chol_fallbacks = (long long)c[1];
+  out->sim_chol_zero = (long long)c[2];
+  float v[6];
+  for (int q = 0; q < 6; q++) CUDA_TRY(cudaMemcpy(&v[q], job->cov[q], sizeof(float), cudaMemcpyDeviceToHost));
+  float P[9] = {v[0], v[3], v[4], v[3], v[1], v[5], v[4], v[5], v[2]};
+  std::memcpy(out->post_var0, P, sizeof(P));
+  return CRAVA_OK;
+}
+
+crava_status crava_fft_r2c(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream) {
+  if (!ctx || !dgrid) return fail(CRAVA_EINVAL, "null argument");
+  if (!smooth(nxp) || !smooth(nyp) || !smooth(nzp) || nxp < 2 || nyp < 2 || nzp < 2)
+    return fail(CRAVA_ENOTSUP, "dimensions must be 2,3,5,7-smooth and >= 2");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  size_t N = (size_t)nxp * nyp * nzp;
+  std::vector<const float*> src{dgrid};
+  std::vector<float*> g{dgrid};
+  std::vector<float> sc{covariance ? 1.0f : fwd_scale(N)};
+  return fwd_xy(ctx, src, g, sc, nxp, nyp, nzp, true, (cudaStream_t)stream);
+}
+
+crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream) {
+  if (!ctx || !dgrid) return fail(CRAVA_EINVAL, "null argument");
+  if (!smooth(nxp) || !smooth(nyp) || !smooth(nzp) || nxp < 2 || nyp < 2 || nzp < 2)
+    return fail(CRAVA_ENOTSUP, "dimensions must be 2,3,5,7-smooth and >= 2");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  size_t N = (size_t)nxp * nyp * nzp;
+  std::vector<float*> g{dgrid};
+  std::vector<float> sc{inv_scale(N, covariance != 0)};
+  return inv_xy(ctx, g, sc, nxp, nyp, nzp, true, (cudaStream_t)stream);
+}
+
+}  // extern "C"

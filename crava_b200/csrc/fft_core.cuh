@@ -1,0 +1,251 @@
+// Shared-memory mixed-radix Stockham FFT on a set of lines held by one CTA.
+//
+// Replaces the FFTW 2.1.2 codelets the reference calls through rfftw3d
+// (libs/fft/fftw/fn_*.c, ftw_*.c, generic.c): lengths are the 2,3,5,7-smooth sizes that
+// FFTGrid::findClosestFactorableNumber produces (src/fftgrid.cpp:2630-2658).
+//
+// A transform of length n = r_0 r_1 ... r_{s-1} runs s autosorting (Stockham) stages.
+// Stage t with radix R and Ns = r_0...r_{t-1} maps butterfly j (0 <= j < n/R) as
+//   v_r   = x[j + r n/R] * w^(r (j mod Ns) n/(Ns R)),   w = e^{sign 2 pi i / n}
+//   y     = DFT_R(v)
+//   x'[(j - j mod Ns) R + j mod Ns + r Ns] = y_r
+// after which x' is in natural order.  Stages alternate between the lines' buffer and a
+// scratch buffer of the same layout in shared memory.  Twiddles come from a table of e^{-2 pi i t / n} evaluated in double precision
+// on the host and rounded to float (conjugated for inverse transforms).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace crava {
+
+constexpr int kMaxStages = 16;
+
+struct LinePlan {
+  int n;
+  int nst;
+  int8_t radix[kMaxStages];
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// i*s*a for s = +-1
+__device__ __forceinline__ float2 cmul_isign(float2 a, float s) { return make_float2(-s * a.y, s * a.x); }
+
+// cos/sin of 2 pi k / R for the odd radices (values of the constants themselves)
+#define C3_S 0.86602540378443864676f
+#define C5_C1 0.30901699437494742410f
+#define C5_S1 0.95105651629515357212f
+#define C5_C2 (-0.80901699437494742410f)
+#define C5_S2 0.58778525229247312917f
+#define C7_C1 0.62348980185873353053f
+#define C7_S1 0.78183148246802980871f
+#define C7_C2 (-0.22252093395631440429f)
+#define C7_S2 0.97492791218182360702f
+#define C7_C3 (-0.90096886790241912624f)
+#define C7_S3 0.43388373911755812048f
+#define SQRT1_2 0.70710678118654752440f
+
+// In-register DFT of length R, y_m = sum_r v_r e^{sign 2 pi i r m / R}.
+template <int R>
+struct Dft;
+
+template <>
+struct Dft<2> {
+  static __device__ __forceinline__ void run(float2* v, float) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <>
+struct Dft<3> {
+  static __device__ __forceinline__ void run(float2* v, float s) {
+    float2 t1 = cadd(v[1], v[2]);
+    float2 t2 = csub(v[1], v[2]);
+    float2 m = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+    float2 r = cmul_isign(cscale(t2, C3_S), s);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+  }
+};
+
+template <>
+struct Dft<4> {
+  static __device__ __forceinline__ void run(float2* v, float s) {
+    float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    float2 c = cadd(v[1], v[3]), d = cmul_isign(csub(v[1], v[3]), s);
+    v[0] = cadd(a, c);
+    v[2] = csub(a, c);
+    v[1] = cadd(b, d);
+    v[3] = csub(b, d);
+  }
+};
+
+template <>
+struct Dft<5> {
+  static __device__ __forceinline__ void run(float2* v, float s) {
+    float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    float2 x0 = v[0];
+    float2 c1 = make_float2(x0.x + C5_C1 * a1.x + C5_C2 * a2.x, x0.y + C5_C1 * a1.y + C5_C2 * a2.y);
+    float2 c2 = make_float2(x0.x + C5_C2 * a1.x + C5_C1 * a2.x, x0.y + C5_C2 * a1.y + C5_C1 * a2.y);
+    float2 s1 = cmul_isign(make_float2(C5_S1 * b1.x + C5_S2 * b2.x, C5_S1 * b1.y + C5_S2 * b2.y), s);
+    float2 s2 = cmul_isign(make_float2(C5_S2 * b1.x - C5_S1 * b2.x, C5_S2 * b1.y - C5_S1 * b2.y), s);
+    v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+    v[1] = cadd(c1, s1);
+    v[4] = csub(c1, s1);
+    v[2] = cadd(c2, s2);
+    v[3] = csub(c2, s2);
+  }
+};
+
+template <>
+struct Dft<7> {
+  static __device__ __forceinline__ void run(float2* v, float s) {
+    float2 a1 = cadd(v[1], v[6]), b1 = csub(v[1], v[6]);
+    float2 a2 = cadd(v[2], v[5]), b2 = csub(v[2], v[5]);
+    float2 a3 = cadd(v[3], v[4]), b3 = csub(v[3], v[4]);
+    float2 x0 = v[0];
+    // m = 1, 2, 3: cos terms sum a_r cos(2 pi r m/7), sin terms b_r sin(2 pi r m/7)
+    float2 c1 = make_float2(x0.x + C7_C1 * a1.x + C7_C2 * a2.x + C7_C3 * a3.x,
+                            x0.y + C7_C1 * a1.y + C7_C2 * a2.y + C7_C3 * a3.y);
+    float2 c2 = make_float2(x0.x + C7_C2 * a1.x + C7_C3 * a2.x + C7_C1 * a3.x,
+                            x0.y + C7_C2 * a1.y + C7_C3 * a2.y + C7_C1 * a3.y);
+    float2 c3 = make_float2(x0.x + C7_C3 * a1.x + C7_C1 * a2.x + C7_C2 * a3.x,
+                            x0.y + C7_C3 * a1.y + C7_C1 * a2.y + C7_C2 * a3.y);
+    // sin(2 pi r m / 7): m=1: S1 S2 S3; m=2: S2 -S3 -S1; m=3: S3 -S1 S2
+    float2 s1 = cmul_isign(make_float2(C7_S1 * b1.x + C7_S2 * b2.x + C7_S3 * b3.x,
+                                       C7_S1 * b1.y + C7_S2 * b2.y + C7_S3 * b3.y), s);
+    float2 s2 = cmul_isign(make_float2(C7_S2 * b1.x - C7_S3 * b2.x - C7_S1 * b3.x,
+                                       C7_S2 * b1.y - C7_S3 * b2.y - C7_S1 * b3.y), s);
+    float2 s3 = cmul_isign(make_float2(C7_S3 * b1.x - C7_S1 * b2.x + C7_S2 * b3.x,
+                                       C7_S3 * b1.y - C7_S1 * b2.y + C7_S2 * b3.y), s);
+    v[0] = make_float2(x0.x + a1.x + a2.x + a3.x, x0.y + a1.y + a2.y + a3.y);
+    v[1] = cadd(c1, s1);
+    v[6] = csub(c1, s1);
+    v[2] = cadd(c2, s2);
+    v[5] = csub(c2, s2);
+    v[3] = cadd(c3, s3);
+    v[4] = csub(c3, s3);
+  }
+};
+
+template <>
+struct Dft<8> {
+  static __device__ __forceinline__ void run(float2* v, float s) {
+    // radix-2 split: DFT4 of even and odd, odd twiddled by e^{sign 2 pi i m/8}
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4>::run(e, s);
+    Dft<4>::run(o, s);
+    // w1 = (1 + s i)/sqrt2, w2 = s i, w3 = (-1 + s i)/sqrt2
+    float2 o1 = make_float2(SQRT1_2 * (o[1].x - s * o[1].y), SQRT1_2 * (o[1].y + s * o[1].x));
+    float2 o2 = cmul_isign(o[2], s);
+    float2 o3 = make_float2(SQRT1_2 * (-o[3].x - s * o[3].y), SQRT1_2 * (-o[3].y + s * o[3].x));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+  }
+};
+
+// Butterfly j of line `line` for the ordering used by a layout: when points are
+// contiguous (PFAST) consecutive threads take consecutive j of one line, otherwise
+// consecutive lines at the same j (lines contiguous in memory).
+template <bool PFAST>
+__device__ __forceinline__ void bfly_index(int idx, int nb, int nlines, int& line, int& j) {
+  if (PFAST) {
+    line = idx / nb;
+    j = idx - line * nb;
+  } else {
+    j = idx / nlines;
+    line = idx - j * nlines;
+  }
+}
+
+// One Stockham stage over nlines lines from `in` to `out` (both shared memory, same
+// layout: element p of line l at l*ls + p*ps).  Each thread loops over whole butterflies,
+// so a thread holds only R points at a time.
+template <int R, bool PFAST>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out, int nlines,
+                                          int ls, int ps, int n, int Ns, const float2* __restrict__ tw,
+                                          float sign) {
+  const int nb = n / R;
+  const int total = nlines * nb;
+  const int twstride = n / (Ns * R);
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    int line, j;
+    bfly_index<PFAST>(idx, nb, nlines, line, j);
+    const float2* src = in + line * ls + j * ps;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = src[r * nb * ps];
+    int k = j % Ns;
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        float2 w = tw[r * k * twstride];
+        w.y *= -sign;  // table holds e^{-2 pi i t/n}; sign=+1 conjugates
+        v[r] = cmul(v[r], w);
+      }
+    }
+    Dft<R>::run(v, sign);
+    float2* dst = out + line * ls + ((j - k) * R + k) * ps;
+#pragma unroll
+    for (int r = 0; r < R; r++) dst[r * Ns * ps] = v[r];
+  }
+  __syncthreads();
+}
+
+// Full transform of nlines lines of length pl.n held in `buf`, using `scratch` (same
+// size and layout) for the ping-pong stages; the result is left in `buf`.  sign = -1
+// forward, +1 inverse (unnormalised both ways, like FFTW).  tw: the length-n table,
+// usually in shared memory.  The caller synchronises before the call (buf complete);
+// the function returns after a barrier.  The stages run grouped by radix in the plan's
+// fixed order 8..8, 4, 2, 3..3, 5..5, 7..7.
+template <bool PFAST>
+__device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlines, int ls, int ps,
+                                          const LinePlan pl, const float2* __restrict__ tw, float sign) {
+  int Ns = 1;
+  const int n = pl.n;
+  int c8 = 0, c4 = 0, c2 = 0, c3 = 0, c5 = 0, c7 = 0;
+  for (int s = 0; s < pl.nst; s++) {
+    int R = pl.radix[s];
+    c8 += R == 8; c4 += R == 4; c2 += R == 2; c3 += R == 3; c5 += R == 5; c7 += R == 7;
+  }
+  float2* a = buf;
+  float2* b = scratch;
+#define CRAVA_STAGE(RR)                                                    \
+  {                                                                        \
+    fft_stage<RR, PFAST>(a, b, nlines, ls, ps, n, Ns, tw, sign);           \
+    Ns *= RR;                                                              \
+    float2* t_ = a; a = b; b = t_;                                         \
+  }
+#pragma unroll 1
+  for (int q = 0; q < c8; q++) CRAVA_STAGE(8)
+  if (c4) CRAVA_STAGE(4)
+  if (c2) CRAVA_STAGE(2)
+#pragma unroll 1
+  for (int q = 0; q < c3; q++) CRAVA_STAGE(3)
+#pragma unroll 1
+  for (int q = 0; q < c5; q++) CRAVA_STAGE(5)
+#pragma unroll 1
+  for (int q = 0; q < c7; q++) CRAVA_STAGE(7)
+#undef CRAVA_STAGE
+  if (a != buf) {  // odd number of stages: copy back (the layouts used are dense)
+    for (int e = threadIdx.x; e < nlines * n; e += blockDim.x) buf[e] = a[e];
+    __syncthreads();
+  }
+}
+
+}  // namespace crava

@@ -1,0 +1,71 @@
+// Kernel parameter blocks and launch helpers shared by the host API and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_core.cuh"
+
+namespace crava {
+
+constexpr int kMaxGrids = 64;   // grids per batched transform launch
+constexpr int kMaxTheta = 8;    // angle stacks per block
+constexpr int kMaxSim = 16;     // realisations per job launch
+
+// Grids of one batched transform launch.  p[] are the grids transformed in place;
+// for the forward x pass src[] are the real inputs it reads (src[q] == p[q] is in place).
+struct GridSet {
+  float* p[kMaxGrids];
+  const float* src[kMaxGrids];
+  float scale[kMaxGrids];
+  int n;
+};
+
+// Per-kz operator tables of one block (device pointers), see the host-side builder.
+struct KzTables {
+  const float2* kw;     // nzp x nth : conj(W_l(k)) kD(k)
+  const float2* e1;     // nzp x nth : conj(W_l(k)) / |w_l|
+  const float2* e2;     // nzp x nth : conj(E3_l(k)) / |e3_l|
+  const uint8_t* inv;   // nzp       : invert_frequency
+};
+
+struct ZParams {
+  int nxp, nyp, nzp, cnxp;
+  int W, nIT;                  // tile width in x-bins, tiles per x-row
+  int nth, nsim;
+  int separable;               // 1: prior from cxy/ct factors, 0: from spectral grids
+  int host_noise;              // 1: noise from `noise` grids
+  int keep_resid;              // 1: write residual spectra into data grids
+  int nxp_even;
+  float2* data[kMaxTheta];
+  float2* mean[3];
+  float2* cov[6];              // out; in GRIDS mode also the prior spectra (in)
+  const float2* errspec;       // GRIDS mode: error correlation spectrum
+  float2* sim[3 * kMaxSim];
+  const float2* noise[3 * kMaxSim];
+  const float2* cxy;           // SEPARABLE: nyp x cnxp spectrum of corrXY
+  const float2* ct;            // SEPARABLE: nzp spectrum of circCorrT
+  float pv[6];                 // priorVar0: 00 11 22 01 02 12
+  float A[kMaxTheta][3];
+  float ec[kMaxTheta][kMaxTheta];  // 0.5 (1 - wnc) errThetaCov
+  float ed[kMaxTheta];             // wnc errThetaCov_ll |e3_l|^2
+  KzTables kz;
+  LinePlan zp;
+  const float2* twz;
+  uint64_t seed;
+  unsigned long long* counters;    // [0] inverted bins [1] chol fallbacks [2] zero sim bins
+};
+
+// launchers (kernels.cu)
+cudaError_t launch_x_r2c(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
+                         cudaStream_t st, int* nlaunch);
+cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
+                         cudaStream_t st, int* nlaunch);
+// Complex transform along a strided axis, in place, for all grids of gs:
+//   element (i, p, o) at ((size_t)o * ostride + (size_t)p * pstride + i) complex,
+//   0 <= i < ni (contiguous), 0 <= p < n (the transform axis), 0 <= o < no.
+cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
+                            const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch);
+cudaError_t launch_zpass(const ZParams& zp, cudaStream_t st, int* nlaunch);
+size_t zpass_smem_bytes(int W, int nzp, int nth);
+
+}  // namespace crava

@@ -1,0 +1,154 @@
+/* crava_gpu.h -- C ABI of the B200 implementation of CRAVA's FFT-domain AVO inversion.
+ *
+ * The reference has no FFI for this path: its boundary is in-process C++ classes.  Each
+ * entry point below replaces one of those calls, so a C++ shim (a DeviceFFTGrid subclass
+ * of FFTGrid and an AVOInversion that calls crava_job_run) can route the reference's own
+ * call sites here.  Plain C types only; `stream` arguments are cudaStream_t passed as
+ * void* (NULL = the legacy default stream).
+ *
+ * Conventions shared with the reference:
+ *   - grids are FFTGrid-padded float arrays of rnxp*nyp*nzp values, x fastest,
+ *     rnxp = 2*(nxp/2+1), index i + rnxp*j + rnxp*nyp*k          (src/fftgrid.cpp:34-47)
+ *   - spectra occupy the same buffer as cnxp*nyp*nzp interleaved complex values,
+ *     cnxp = nxp/2+1, index i + cnxp*j + cnxp*nyp*k               (src/fftgrid.h:256-259)
+ *   - forward transforms are unnormalised e^{-2 pi i}; PARAMETER/DATA grids are scaled
+ *     by 1/sqrt(N) before the forward and after the inverse transform, COVARIANCE grids
+ *     by nothing before and 1/N after                             (src/fftgrid.cpp:1587-1643)
+ *
+ * Every call returns a crava_status; nothing aborts the process.
+ */
+#ifndef CRAVA_GPU_H
+#define CRAVA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CRAVA_OK = 0,
+  CRAVA_EINVAL = 1,     /* bad argument: size, role, index, null pointer          */
+  CRAVA_ENOMEM = 2,     /* device allocation failed or the HBM budget is exceeded */
+  CRAVA_ECUDA = 3,      /* a CUDA runtime call failed (message in crava_last_error) */
+  CRAVA_ETIMEDOUT = 4,  /* a bounded wait gave up                                  */
+  CRAVA_ENUMERIC = 5,   /* non-finite input detected                               */
+  CRAVA_ENOTSUP = 6,    /* size or configuration outside what the kernels handle   */
+  CRAVA_ESTATE = 7      /* call out of order (e.g. download before run)            */
+} crava_status;
+
+typedef struct crava_ctx crava_ctx;
+typedef struct crava_job crava_job;
+
+/* Grid roles of one inversion block.  Inputs are never modified by crava_job_run, so a
+ * job can be run again on the same resident inputs; the reference's in-place aliasing
+ * (posterior mean over prior mean, residual over data, posterior covariance over the
+ * holder's covariance grids) is a matter of where the caller downloads the outputs. */
+typedef enum {
+  CRAVA_ROLE_DATA = 0,       /* seismic angle stack l (in, real)                          */
+  CRAVA_ROLE_MEAN = 1,       /* prior mean a=0..2, order Vp, Vs, Rho (in, real)           */
+  CRAVA_ROLE_PRIOR_COV = 2,  /* prior covariance grid q=0..5 (in, real, COVARIANCE) in the
+                                order Vp, Vs, Rho, VpVs, VpRho, VsRho; CRAVA_PRIOR_GRIDS only */
+  CRAVA_ROLE_ERR_CORR = 3,   /* error correlation grid (in, real, COVARIANCE);
+                                CRAVA_PRIOR_GRIDS only                                     */
+  CRAVA_ROLE_POST_COV = 4,   /* posterior covariance q=0..5 (out, real, after
+                                invFFTCovGrids, src/seismicparametersholder.cpp:432-456)  */
+  CRAVA_ROLE_SIM = 5,        /* realisation s, parameter a: index 3*s+a (out, real)       */
+  CRAVA_ROLE_NOISE = 6,      /* complex noise of realisation s, parameter a, index 3*s+a
+                                (in, complex cnxp*nyp*nzp); CRAVA_FLAG_HOST_NOISE only    */
+  CRAVA_ROLE_RESIDUAL = 7,   /* residual spectrum l (out, complex), the reference's
+                                seisData_ after the loop (src/avoinversion.cpp:1080-1081);
+                                CRAVA_FLAG_KEEP_RESIDUAL only                              */
+  CRAVA_ROLE_POST_MEAN = 8   /* posterior mean a (out, real), postVp_/postVs_/postRho_
+                                after invFFTInPlace (src/avoinversion.cpp:1112-1114)      */
+} crava_role;
+
+enum {
+  CRAVA_PRIOR_SEPARABLE = 0, /* prior and error correlation given as the separable
+                                factors corr_xy (nxp*nyp) and circ_corr_t (nzp) with zero
+                                correlation gradients: the covariance grids of
+                                InitializeCorrelations are never materialised             */
+  CRAVA_PRIOR_GRIDS = 1      /* six prior covariance grids and the error correlation grid
+                                uploaded as real grids (any gradients)                     */
+};
+
+enum {
+  CRAVA_FLAG_HOST_NOISE = 1,   /* realisation noise uploaded by the caller (parity with a
+                                  sequential generator such as the reference RandomGen)   */
+  CRAVA_FLAG_KEEP_RESIDUAL = 2 /* keep the residual spectra for CRAVA_ROLE_RESIDUAL          */
+};
+
+/* One inversion block: the scalars and small arrays AVOInversion reads from ModelSettings,
+ * ModelAVODynamic, Simbox and SeismicParametersHolder (src/avoinversion.cpp:72-111). */
+typedef struct {
+  int nx, ny, nz;              /* simbox dims                                  */
+  int nxp, nyp, nzp;           /* padded dims (2,3,5,7-smooth)                 */
+  int ntheta;                  /* angle stacks, 1..8                           */
+  double lz;                   /* Simbox::getlz (ms)                           */
+  double min_rel_thick;        /* Simbox::getMinRelThick                       */
+  float low_cut, high_cut;     /* ModelSettings::getLowCut/getHighCut (Hz)     */
+  float wnc;                   /* white-noise component                        */
+  const double* A;             /* ntheta x 3 reflection matrix, row-major      */
+  const double* err_theta_cov; /* ntheta x ntheta                              */
+  const float* wavelet;        /* ntheta x nzp, resampled wavelets, FFT order  */
+  const float* wavelet_norm;   /* ntheta, Wavelet::getNorm                     */
+  const double* prior_var0;    /* 3 x 3, SeismicParametersHolder::priorVar0_  */
+  int prior_mode;              /* CRAVA_PRIOR_SEPARABLE or CRAVA_PRIOR_GRIDS   */
+  const float* corr_xy;        /* nxp*nyp lateral correlation, index i+nxp*j   */
+  const float* circ_corr_t;    /* nzp circular temporal correlation            */
+  int nsim;                    /* realisations                                 */
+  uint64_t seed;               /* device noise seed (ignored with HOST_NOISE)  */
+  int flags;                   /* CRAVA_FLAG_*                                 */
+} crava_job_desc;
+
+typedef struct {
+  long long inverted_bins;     /* bins inside (lowCut*minRelThick, highCut)    */
+  long long chol_fallbacks;    /* inverted bins whose Cholesky failed: prior kept */
+  long long sim_chol_zero;     /* realisation bins left at zero (simulate fallback) */
+  float post_var0[9];          /* SeismicParametersHolder::updatePriorVar after the run */
+} crava_counters;
+
+/* Context on one device; hbm_budget = 0 means no limit beyond the device's memory. */
+crava_status crava_ctx_create(crava_ctx** ctx, int device, size_t hbm_budget);
+crava_status crava_ctx_destroy(crava_ctx* ctx);
+const char* crava_last_error(void);
+const char* crava_status_string(crava_status s);
+
+/* Job = one AVOInversion on one block.  Allocates the device grids for the block.
+ * Replaces the AVOInversion constructor's set-up (src/avoinversion.cpp:53-111). */
+crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_job** job);
+crava_status crava_job_destroy(crava_job* job);
+/* Bytes of device memory crava_job_create would allocate for desc. */
+crava_status crava_job_footprint(const crava_job_desc* desc, size_t* bytes);
+
+/* Host <-> device copies of one grid (rnxp*nyp*nzp floats; NOISE/RESIDUAL are
+ * cnxp*nyp*nzp complex = the same number of floats).  Asynchronous on `stream`. */
+crava_status crava_job_upload(crava_job* job, crava_role role, int index, const float* host, void* stream);
+crava_status crava_job_download(crava_job* job, crava_role role, int index, float* host, void* stream);
+/* Device pointer of one grid (for callers that keep data resident). */
+crava_status crava_job_device_ptr(crava_job* job, crava_role role, int index, float** dptr);
+
+/* The whole hot path of one block on `stream`:
+ *   forward transforms of data and prior mean     (src/avoinversion.cpp:229-244)
+ *   FFTCovGrids + errCorr transform, GRIDS mode   (:908, :917)
+ *   computePostMeanResidAndFFTCov per-bin loop    (:944-1091)
+ *   simulate, nsim realisations                   (:1354-1511)
+ *   inverse transforms of mean, covariance, realisations (:1112-1114, :1476-1483,
+ *   src/seismicparametersholder.cpp:432-456)
+ * Counters are available after the stream reaches the end of the call. */
+crava_status crava_job_run(crava_job* job, void* stream);
+crava_status crava_job_counters(crava_job* job, crava_counters* out);
+
+/* FFTGrid drop-ins on a device grid (src/fftgrid.cpp:1587-1612 / 1615-1643).
+ * covariance != 0 selects the COVARIANCE scaling. */
+crava_status crava_fft_r2c(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream);
+crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream);
+
+/* Kernels launched by this library since the context was created (all entry points). */
+long long crava_ctx_kernel_launches(crava_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRAVA_GPU_H */

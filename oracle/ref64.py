@@ -1,0 +1,379 @@
+"""FP64 oracle: a numpy restatement of the reference's FFT-domain AVO inversion.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product path imports this module; it is the
+checker the CUDA path is compared against (tests, the smoke check and the CPU leg of the
+benchmark).
+
+Restated from the reference, in float64 with numpy's pocketfft transforms:
+
+* FFTGrid::fftInPlace / invFFTInPlace            src/fftgrid.cpp:1587-1643
+    forward = rfftw3d r2c (unnormalised, e^{-2 pi i}), grid pre-scaled by 1/sqrt(N) unless
+    the grid is a COVARIANCE grid; inverse = c2r then x 1/N (COVARIANCE) or 1/sqrt(N).
+* FFTGrid::fillInParamCorr / fillInErrCorr       src/fftgrid.cpp:777-828, 878-928
+* SeismicParametersHolder::InitializeCorrelations src/seismicparametersholder.cpp:325-351
+* SeismicParametersHolder::getNextParameterCovariance  :485-557  (|Re|, Im dropped)
+* Wavelet1D diff operators                        src/wavelet1D.cpp:389-500
+* Wavelet::getCAmp / findNorm                     src/wavelet.cpp:318-334, 882-900
+* AVOInversion::computePostMeanResidAndFFTCov     src/avoinversion.cpp:794-1091
+    K = diag(conj(W) kD) A (:948-975), getNextErrorVariance (:1236-1272), per-bin posterior
+    (:1016-1082) with lib_matrCholCpx (libs/lib/lib_matr.c:78-168) and
+    lib_matrAXeqBMatCpx (:330-378)
+* AVOInversion::simulate                          src/avoinversion.cpp:1354-1526
+    lib_matrCholCpx(3) + lib_matrProdCholVec (libs/lib/lib_matr.c:453-471)
+* SeismicParametersHolder::updatePriorVar / createPostCov00   :1031-1067
+
+Layout: real grids are (nzp, nyp, rnxp) float arrays (FFTGrid index i + rnxp*j +
+rnxp*nyp*k); spectra are (nzp, nyp, cnxp) complex arrays (index i + cnxp*j + cnxp*nyp*k).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+TOL = 1e-20  # libs/lib/lib_matr.c:20
+
+
+# ---------------------------------------------------------------- transforms
+
+def fft_in_place(real_padded: np.ndarray, nxp: int, covariance: bool) -> np.ndarray:
+    """FFTGrid::fftInPlace (src/fftgrid.cpp:1587-1612) in float64."""
+    x = real_padded[..., :nxp].astype(np.float64)
+    N = x.size
+    if not covariance:
+        x = x / math.sqrt(N)
+    return np.fft.rfftn(x, axes=(0, 1, 2))
+
+
+def inv_fft_in_place(spec: np.ndarray, nxp: int, covariance: bool) -> np.ndarray:
+    """FFTGrid::invFFTInPlace (src/fftgrid.cpp:1615-1643): c2r (unnormalised), then the
+    1/N (COVARIANCE) or 1/sqrt(N) scale.  Returns the padded real layout."""
+    nzp, nyp, cnxp = spec.shape
+    out = np.fft.irfftn(spec, s=(nzp, nyp, nxp), axes=(0, 1, 2))  # = c2r / N
+    N = nzp * nyp * nxp
+    if not covariance:
+        out = out * math.sqrt(N)
+    res = np.zeros((nzp, nyp, 2 * cnxp))
+    res[..., :nxp] = out
+    return res
+
+
+# ---------------------------------------------------------------- prior grids
+
+def fill_param_corr(corr_xy, circ_corr_t, nxp, nyp, nzp, grad_i=0.0, grad_j=0.0):
+    """FFTGrid::fillInParamCorr (src/fftgrid.cpp:878-928), float arithmetic as the
+    reference; returns (nzp, nyp, nxp) float32."""
+    f32 = np.float32
+    i = np.arange(nxp)
+    j = np.arange(nyp)
+    ci = np.where(i < -(i - nxp), i, i - nxp)
+    cj = np.where(j < -(j - nyp), j, j - nyp)
+    out = np.empty((nzp, nyp, nxp), dtype=np.float32)
+    cxy = corr_xy.astype(np.float32)
+    ct = circ_corr_t.astype(np.float32)
+    for k in range(nzp):
+        subk = (f32(k) + (ci[None, :] * f32(grad_i)).astype(np.float32)
+                + (cj[:, None] * f32(grad_j)).astype(np.float32)).astype(np.float32)
+        basek = np.floor(subk).astype(np.int64)
+        subk = (subk - basek).astype(np.float32)
+        basek = np.mod(basek, nzp)
+        nxt = np.where(basek != nzp - 1, basek + 1, 0)
+        v = ((f32(1) - subk) * ct[basek] + subk * ct[nxt]).astype(np.float32)
+        out[k] = (v * cxy).astype(np.float32)
+    return out
+
+
+def fill_err_corr(corr_xy, nxp, nyp, nzp, grad_i=0.0, grad_j=0.0):
+    """FFTGrid::fillInErrCorr (src/fftgrid.cpp:777-828): corrXY at the (rotated) k=0 lag."""
+    out = np.zeros((nzp, nyp, nxp), dtype=np.float32)
+    cxy = corr_xy.astype(np.float32)
+    for j in range(nyp):
+        cj = j if j < -(j - nyp) else j - nyp
+        for i in range(nxp):
+            ci = i if i < -(i - nxp) else i - nxp
+            for k in range(nzp):
+                subk = np.float32(k + ci * grad_i + cj * grad_j)
+                if abs(subk) < 1.0 or abs(subk - nzp) < 1.0:
+                    basek = int(subk)
+                    subk = np.float32(subk - basek)
+                    while basek < -1:
+                        basek += nzp
+                    while basek >= 1:
+                        basek -= nzp
+                    if basek < 0:
+                        subk = np.float32(1 - subk)
+                    out[k, j, i] = np.float32((1 - subk) * cxy[j, i])
+    return out
+
+
+def fill_err_corr_zero_grad(corr_xy, nxp, nyp, nzp):
+    """fillInErrCorr with zero correlation gradients: corrXY on the k = 0 plane only."""
+    out = np.zeros((nzp, nyp, nxp), dtype=np.float32)
+    out[0] = corr_xy.astype(np.float32)
+    return out
+
+
+def prior_cov_grids(blk, full_grid=True):
+    """The six prior covariance grids (COVARIANCE type) of InitializeCorrelations
+    (src/seismicparametersholder.cpp:334-348): fillInParamCorr x priorVar0(a,b), in the
+    order Vp, Vs, Rho, VpVs, VpRho, VsRho."""
+    base = fill_param_corr(blk.corr_xy, blk.circ_corr_t, blk.nxp, blk.nyp, blk.nzp,
+                           blk.corr_grad_i, blk.corr_grad_j)
+    pv = blk.prior_var0
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    return [(base * np.float32(pv[a, b])).astype(np.float32) for a, b in pairs], pairs
+
+
+# ---------------------------------------------------------------- wavelets / per-kz
+
+def wavelet_spectrum_full(w: np.ndarray) -> np.ndarray:
+    """Wavelet::fft1DInPlace + getCAmp(k) with the Hermitian mirror for k >= cnzp
+    (src/wavelet.cpp:255-270, 318-334): the full DFT (e^{-2 pi i}) at every k."""
+    return np.fft.fft(w.astype(np.float64))
+
+
+def diff_forward(w):
+    """Wavelet1D(w, FIRSTORDERFORWARDDIFF) (src/wavelet1D.cpp:447-452)."""
+    return np.roll(w, -1) - w
+
+
+def diff_backward(w):
+    return w - np.roll(w, 1)
+
+
+def diff_central(w):
+    return 0.5 * (np.roll(w, -1) - np.roll(w, 1))
+
+
+def real_norm(w):
+    """Wavelet::findNorm for a real vector (src/wavelet.cpp:882-889)."""
+    return math.sqrt(float(np.sum(np.asarray(w, dtype=np.float64) ** 2)))
+
+
+def per_kz_operators(blk):
+    """Per-kz quantities of computePostMeanResidAndFFTCov's constant-thickness branch
+    (src/avoinversion.cpp:845-975):
+      K[k]   = diag(conj(W_l(k)) * kD(k)) A          (fillkW, ProdScalVec, ProdDiagCpxR)
+      e1[k]  = conj(W_l(k)) / |w_l|                   (fillkWNorm on seisWaveletForNorm)
+      e2[k]  = conj(E3_l(k)) / |e3_l|                 (fillkWNorm on errorSmooth3)
+      e3[k]  = 1                                      (lib_matrFillOnesVecCpx)
+      inv[k] = lowCut*minRelThick < f(k) < highCut    (:946, :1029)
+    """
+    nzp, nth = blk.nzp, blk.ntheta
+    d1 = np.zeros(nzp)
+    d1[0] = -1.0
+    d1[nzp - 1] = 1.0
+    kD = np.fft.fft(d1)
+    K = np.zeros((nzp, nth, 3), dtype=np.complex128)
+    e1 = np.zeros((nzp, nth), dtype=np.complex128)
+    e2 = np.zeros((nzp, nth), dtype=np.complex128)
+    for l in range(nth):
+        w = blk.wavelet[l].astype(np.float64)
+        W = wavelet_spectrum_full(w)
+        kW = np.conj(W) * kD
+        K[:, l, :] = kW[:, None] * blk.A[l][None, :]
+        e1[:, l] = np.conj(W) / float(blk.wavelet_norm[l])
+        es3 = diff_central(diff_backward(diff_forward(w)))
+        e2[:, l] = np.conj(np.fft.fft(es3)) / real_norm(es3)
+    e3 = np.ones((nzp, nth))
+    inv = invert_mask(blk)
+    return K, e1, e2, e3, inv
+
+
+def real_frequency(blk) -> np.ndarray:
+    """realFrequency (src/avoinversion.cpp:946), evaluated exactly as the reference:
+    (float(nz)*1000.0f) / (lz * nzp) * min(k, nzp-k) in double, stored as float."""
+    k = np.arange(blk.nzp)
+    kk = np.minimum(k, blk.nzp - k).astype(np.float64)
+    nz1000 = float(np.float32(blk.nz) * np.float32(1000.0))
+    return (nz1000 / (float(blk.lz) * blk.nzp) * kk).astype(np.float32)
+
+
+def invert_mask(blk) -> np.ndarray:
+    f = real_frequency(blk).astype(np.float64)
+    lo = float(np.float32(blk.low_cut)) * float(blk.min_rel_thick)
+    hi = float(np.float32(blk.high_cut))
+    return (f > lo) & (f < hi)
+
+
+# ---------------------------------------------------------------- per-bin algebra
+
+def chol_cpx(M: np.ndarray):
+    """lib_matrCholCpx (libs/lib/lib_matr.c:78-168) vectorised over leading axes.
+    Scales by M[0,0].re, rejects a non-positive scale, a scaled diagonal <= TOL before the
+    update and an updated pivot <= TOL.  Returns (L, ok)."""
+    n = M.shape[-1]
+    fac = M[..., 0, 0].real
+    ok = fac > 0
+    safe = np.where(ok, fac, 1.0)
+    X = M / safe[..., None, None]
+    L = np.zeros_like(X)
+    for i in range(n):
+        ok &= X[..., i, i].real > TOL
+        for j in range(i):
+            s = np.zeros(X.shape[:-2], dtype=X.dtype)
+            for k in range(j):
+                s = s + L[..., i, k] * np.conj(L[..., j, k])
+            L[..., i, j] = (X[..., i, j] - s) / L[..., j, j]
+        r = X[..., i, i].real - sum(np.abs(L[..., i, k]) ** 2 for k in range(i)) if i else X[..., i, i].real
+        ok &= r > TOL
+        L[..., i, i] = np.sqrt(np.where(r > TOL, r, 1.0))
+    L = L * np.sqrt(safe)[..., None, None]
+    return L, ok
+
+
+def chol_solve(L, B):
+    """lib_matrAXeqBMatCpx (libs/lib/lib_matr.c:330-378): X = (L L^H)^{-1} B."""
+    n = L.shape[-1]
+    Y = np.array(B, copy=True)
+    for i in range(n):
+        acc = Y[..., i, :]
+        for j in range(i):
+            acc = acc - L[..., i, j, None] * Y[..., j, :]
+        Y[..., i, :] = acc / L[..., i, i, None]
+    for i in range(n - 1, -1, -1):
+        acc = Y[..., i, :]
+        for j in range(i + 1, n):
+            acc = acc - np.conj(L[..., j, i, None]) * Y[..., j, :]
+        Y[..., i, :] = acc / np.conj(L[..., i, i, None])
+    return Y
+
+
+def param_cov_from_spectra(spec6, pv):
+    """getNextParameterCovariance (src/seismicparametersholder.cpp:485-557):
+    S_ab = |Re(spec_ab) / pv_ab| * pv_ab (division skipped when pv_ab == 0), Im = 0."""
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    shp = spec6[0].shape
+    S = np.zeros(shp + (3, 3), dtype=np.complex128)
+    for s, (a, b) in zip(spec6, pairs):
+        p = float(pv[a, b])
+        v = np.abs(s.real / p) * p if p != 0 else np.abs(s.real)
+        S[..., a, b] = v
+        S[..., b, a] = v
+    return S
+
+
+# ---------------------------------------------------------------- the inversion
+
+class Posterior:
+    """Outputs of computePostMeanResidAndFFTCov + invFFTCovGrids, float64."""
+
+    def __init__(self):
+        self.mean_spec = None     # (3, nzp, nyp, cnxp)
+        self.cov_spec = None      # (6, ...) Vp, Vs, Rho, VpVs, VpRho, VsRho
+        self.resid_spec = None    # (ntheta, ...)
+        self.mean = None          # (3, nzp, nyp, rnxp) real, 1/sqrt(N)
+        self.cov = None           # (6, nzp, nyp, rnxp) real, 1/N
+        self.n_inverted = 0
+        self.n_chol_fail = 0
+
+
+def posterior(blk, slab: int = 16) -> Posterior:
+    """AVOInversion constructor FFTs + computePostMeanResidAndFFTCov + invFFTCovGrids."""
+    nxp, nyp, nzp, nth = blk.nxp, blk.nyp, blk.nzp, blk.ntheta
+    covs, pairs = prior_cov_grids(blk)
+    cov_spec = [fft_in_place(c, nxp, True) for c in covs]
+    if abs(blk.corr_grad_i) > 0 or abs(blk.corr_grad_j) > 0:
+        ec = fill_err_corr(blk.corr_xy, nxp, nyp, nzp, blk.corr_grad_i, blk.corr_grad_j)
+    else:
+        ec = fill_err_corr_zero_grad(blk.corr_xy, nxp, nyp, nzp)
+    err_spec = fft_in_place(ec, nxp, True)
+    data_spec = np.stack([fft_in_place(blk.data[l], nxp, False) for l in range(nth)])
+    mean_spec = np.stack([fft_in_place(blk.mean[a], nxp, False) for a in range(3)])
+    K, e1, e2, e3, inv = per_kz_operators(blk)
+    Sth = blk.err_theta_cov
+    wnc = float(np.float32(blk.wnc))
+    out = Posterior()
+    out.mean_spec = mean_spec.copy()
+    out.resid_spec = data_spec.copy()
+    cs = np.zeros((6,) + mean_spec.shape[1:], dtype=np.complex128)
+    for k0 in range(0, nzp, slab):
+        k1 = min(nzp, k0 + slab)
+        S = param_cov_from_spectra([c[k0:k1] for c in cov_spec], blk.prior_var0)  # (z,y,x,3,3)
+        lam = np.abs(err_spec[k0:k1].real)
+        Kk = K[k0:k1][:, None, None]                      # (z,1,1,nth,3)
+        e1k = e1[k0:k1][:, None, None]
+        e2k = e2[k0:k1][:, None, None]
+        e3k = e3[k0:k1][:, None, None]
+        E = 0.5 * (1.0 - wnc) * Sth * lam[..., None, None] * (
+            e1k[..., :, None] * np.conj(e1k[..., None, :]) + e2k[..., :, None] * np.conj(e2k[..., None, :]))
+        E = E + np.eye(nth) * (wnc * np.diag(Sth) * np.abs(e3k) ** 2)[..., None, :]
+        KS = Kk @ S
+        Sd = KS @ np.conj(np.swapaxes(Kk, -1, -2)) + E
+        L, ok = chol_cpx(Sd)
+        invk = np.broadcast_to(inv[k0:k1][:, None, None], ok.shape)
+        ok_eff = ok & invk
+        M = chol_solve(L, KS)                               # Sd^{-1} K S
+        red = np.conj(np.swapaxes(KS, -1, -2)) @ M
+        Spost = np.where(ok_eff[..., None, None], S - red, S)
+        mu = np.moveaxis(mean_spec[:, k0:k1], 0, -1)       # (z,y,x,3)
+        d = np.moveaxis(data_spec[:, k0:k1], 0, -1)        # (z,y,x,nth)
+        dm = d - (Kk @ mu[..., None])[..., 0]
+        mu_post = mu + (np.conj(np.swapaxes(M, -1, -2)) @ dm[..., None])[..., 0]
+        res = d - (Kk @ mu_post[..., None])[..., 0]
+        mu_post = np.where(ok_eff[..., None], mu_post, mu)
+        res = np.where(ok_eff[..., None], res, d)
+        out.mean_spec[:, k0:k1] = np.moveaxis(mu_post, -1, 0)
+        out.resid_spec[:, k0:k1] = np.moveaxis(res, -1, 0)
+        for g, (a, b) in enumerate(pairs):
+            cs[g, k0:k1] = Spost[..., a, b]
+        out.n_inverted += int(invk.sum())
+        out.n_chol_fail += int((invk & ~ok).sum())
+    out.cov_spec = cs
+    out.mean = np.stack([inv_fft_in_place(out.mean_spec[a], nxp, False) for a in range(3)])
+    out.cov = np.stack([inv_fft_in_place(cs[g], nxp, True) for g in range(6)])
+    return out
+
+
+def simulate(blk, post: Posterior, noise: np.ndarray) -> np.ndarray:
+    """AVOInversion::simulate (src/avoinversion.cpp:1401-1511) for one realisation given
+    its three complex noise grids noise (3, nzp, nyp, cnxp).  Returns (3, nzp, nyp, rnxp)."""
+    cs = post.cov_spec
+    C = np.zeros(cs.shape[1:] + (3, 3), dtype=np.complex128)
+    C[..., 0, 0] = cs[0]
+    C[..., 1, 1] = cs[1]
+    C[..., 2, 2] = cs[2]
+    C[..., 0, 1] = cs[3]
+    C[..., 0, 2] = cs[4]
+    C[..., 1, 2] = cs[5]
+    C[..., 1, 0] = np.conj(cs[3])
+    C[..., 2, 0] = np.conj(cs[4])
+    C[..., 2, 1] = np.conj(cs[5])
+    L, ok = chol_cpx(C)
+    z = np.moveaxis(noise.astype(np.complex128), 0, -1)
+    s = (np.tril(L) @ z[..., None])[..., 0]
+    s = np.where(ok[..., None], s, 0.0)
+    s = np.moveaxis(s, -1, 0)
+    real = np.stack([inv_fft_in_place(s[a], blk.nxp, False) for a in range(3)])
+    return real + post.mean
+
+
+def post_var0(post: Posterior) -> np.ndarray:
+    """updatePriorVar (src/seismicparametersholder.cpp:1031-1043): cov grids at (0,0,0)."""
+    v = post.cov[:, 0, 0, 0]
+    P = np.zeros((3, 3))
+    P[0, 0], P[1, 1], P[2, 2] = v[0], v[1], v[2]
+    P[0, 1] = P[1, 0] = v[3]
+    P[0, 2] = P[2, 0] = v[4]
+    P[1, 2] = P[2, 1] = v[5]
+    return P
+
+
+def post_cov00(post: Posterior, nz: int) -> np.ndarray:
+    """createPostCov00 (src/seismicparametersholder.cpp:1056-1067) for Vp, Vs, Rho."""
+    return post.cov[:3, :nz, 0, 0].copy()
+
+
+def rel_err(x, ref) -> float:
+    """Norm-wise relative error ||x - ref|| / ||ref||."""
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    den = np.linalg.norm(ref)
+    return float(np.linalg.norm(x - ref) / (den if den > 0 else 1.0))
+
+
+def max_rel_err(x, ref) -> float:
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    den = np.max(np.abs(ref))
+    return float(np.max(np.abs(x - ref)) / (den if den > 0 else 1.0))
