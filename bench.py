@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FFT-domain AVO inversion (posterior mean + covariance + realisations).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one whole inversion block of the 540x540x256 production workload (5 angle
+stacks 5..45 deg, 4 conditional realisations, separable prior): forward transforms of the
+data and prior mean, the fused per-bin posterior and simulation pencil pass, inverse
+transforms of mean, covariance and realisations.  Under torchrun every rank inverts its own
+block (weak scaling, no collective on the data path).
+
+`value` is voxels/s with inputs resident in HBM; `e2e` is the same metric through the
+C-ABI job calls with pinned host buffers (uploads, run, downloads of every output inside
+the timed region).  `--impl reference` times the reference's own CPU numerics (FFTW 2.1.2
+float + lib_matr, built into oracle/_ref) on bounded samples of the same workload on the
+host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "posterior voxels/s batched+served vs plain GPU at ≤1e-4 rel err; p99 latency"
+UNIT = "voxels/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def workload_spec(rank: int = 0, dims=None):
+    from crava_b200 import synth
+    spec = synth.config1(seed=21 + rank)
+    if dims:
+        spec.nx, spec.ny, spec.nz = dims
+    return spec
+
+
+def sample_spec(seed: int = 101):
+    """Bounded CPU sample of the same workload: the 540x540x256 block's parameters on a
+    135x135x256 lateral window (1/16 of the voxels, same z length and angle count)."""
+    from crava_b200 import synth
+    spec = synth.config1(seed=seed)
+    spec.nx = spec.ny = 135
+    return spec
+
+
+# ------------------------------------------------------------------ clocks
+
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def start_clock_sampler(path):
+    try:
+        f = open(path, "w")
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={CLOCK_FIELDS}", "--format=csv", "-lms", "200"],
+                             stdout=f, stderr=subprocess.DEVNULL)
+        return p, f
+    except Exception:
+        return None, None
+
+
+def stop_clock_sampler(p, f):
+    if p is None:
+        return
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except Exception:
+        p.kill()
+    f.close()
+
+
+def summarize_clocks(path, gpu_index):
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    sm, mx, reasons = [], None, set()
+    try:
+        with open(path) as f:
+            lines = [l.strip() for l in f if l.strip()]
+    except Exception:
+        return None
+    for l in lines[1:]:
+        parts = [p.strip() for p in l.split(",")]
+        if len(parts) < 9 or not parts[0].isdigit() or int(parts[0]) != gpu_index:
+            continue
+        try:
+            sm.append(float(parts[1].split()[0]))
+            mx = float(parts[2].split()[0])
+        except ValueError:
+            continue
+        for nm, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ------------------------------------------------------------------ CPU reference (oracle/_ref)
+
+_worker_block = None
+
+
+def _ref_worker_init(seed):
+    global _worker_block
+    from crava_b200 import synth
+    _worker_block = synth.make_block(sample_spec(seed))
+
+
+def _ref_worker_run(_):
+    """One sample inversion with the reference numerics; returns (voxels, seconds)."""
+    from oracle import bindings as ob
+    from oracle import ref64
+    blk = _worker_block
+    covs, _ = ref64.prior_cov_grids(blk)
+    ec = ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)
+    t = time.perf_counter()
+    ob.ref32_invert(blk, covs, ec, nsim=blk.nsim, seed=blk.seed)
+    return blk.n_voxels, time.perf_counter() - t
+
+
+def cpu_reference_available():
+    from oracle import bindings as ob
+    return ob.ref32_available()
+
+
+def run_cpu_sample(nproc=1, steps=1, warmup=0):
+    """Runs the sample on nproc spawned processes; returns per-step (voxels/s) list."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    vals = []
+    with ctx.Pool(nproc, initializer=_ref_worker_init, initargs=(101,)) as pool:
+        for s in range(warmup + steps):
+            t0 = time.perf_counter()
+            res = pool.map(_ref_worker_run, range(nproc), chunksize=1)
+            dt = time.perf_counter() - t0
+            if s >= warmup:
+                vals.append(sum(r[0] for r in res) / dt)
+    return vals
+
+
+def reference_main(args, rank, world):
+    spec = workload_spec(0)
+    cfg = {"workload": f"{spec.nx}x{spec.ny}x{spec.nz}, {len(spec.theta_deg)} angles, {spec.nsim} realisations",
+           "prior": "separable (reference: six covariance grids + errCorr grid, as InitializeCorrelations builds)"}
+    if rank != 0:
+        return
+    if not cpu_reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref32.so was not built (reference tree absent at build time)"}))
+        return
+    ncores = os.cpu_count() or 1
+    nproc = max(1, min(16, ncores // 2))
+    vals = run_cpu_sample(nproc=nproc, steps=args.steps, warmup=args.warmup)
+    v = statistics.median(vals)
+    smp = sample_spec()
+    vox = smp.nx * smp.ny * smp.nz
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * nproc * vox / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nproc, "kind": "reference",
+                             "sample": f"{nproc} processes, each one full inversion (5 angles, 4 realisations) of a "
+                                       f"{smp.nx}x{smp.ny}x{smp.nz} window of the workload per step; FFTW 2.1.2 float "
+                                       f"and lib_matr.c from the reference, single-threaded as in the reference; "
+                                       f"host has {ncores} logical cores"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def alg_bytes(blk, nsim, cls, ngrids):
+    """Algorithmic HBM bytes of one launch of a kernel class over ngrids grids."""
+    N = blk.nxp * blk.nyp * blk.nzp
+    Nc = (blk.nxp // 2 + 1) * blk.nyp * blk.nzp
+    if cls == "x_r2c":
+        return ngrids * (4 * N + 8 * Nc)
+    if cls == "x_c2r":
+        return ngrids * (8 * Nc + 4 * N)
+    if cls in ("line_fwd", "line_inv"):
+        return ngrids * 16 * Nc
+    if cls == "zpass":
+        return 8 * Nc * ((blk.ntheta + 3) + (9 + 3 * nsim))
+    raise ValueError(cls)
+
+
+def read_traffic(kernel_class):
+    """dram bytes per launch from the committed ncu summary (line 'traffic_bytes_per_launch')."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_class}_540x540x256.md")
+    try:
+        with open(path) as f:
+            for l in f:
+                if l.startswith("traffic_bytes_per_launch:"):
+                    return float(l.split(":", 1)[1].strip())
+    except Exception:
+        pass
+    return None
+
+
+def parity_check(ctx):
+    """GPU vs the FP64 oracle on the 64x64x128 block (parity mode noise)."""
+    import numpy as np
+    from crava_b200 import api, synth
+    from oracle import bindings as ob
+    from oracle import ref64
+    blk = synth.make_block(synth.config0())
+    post = ref64.posterior(blk)
+    noise = ob.sim_noise(blk.seed, blk.nsim, blk.nxp, blk.nyp, blk.nzp)
+    out = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=noise)
+    nx = blk.nxp
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    em = max(rel(out["mean"][a][..., :nx], post.mean[a][..., :nx]) for a in range(3))
+    ec = max(rel(out["cov"][q][..., :nx], post.cov[q][..., :nx]) for q in range(6))
+    sim = ref64.simulate(blk, post, noise[0])
+    es = max(rel(out["sims"][0, a][..., :nx], sim[a][..., :nx]) for a in range(3))
+    return {"block": "64x64x128, 3 angles", "oracle": "fp64", "mean_rel_err": em, "cov_rel_err": ec,
+            "sim_rel_err": es}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--dims", default=None, help="nx,ny,nz of a smaller block (profiling runs only)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_main(args, rank, world)
+
+    # CPU baseline first, in a spawned process, before this process touches the GPU
+    cpu = None
+    if rank == 0 and not args.no_cpu and cpu_reference_available():
+        try:
+            vals = run_cpu_sample(nproc=1, steps=1, warmup=0)
+            smp = sample_spec()
+            cpu = {"value": vals[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"one full inversion (5 angles, 4 realisations) of a {smp.nx}x{smp.ny}x{smp.nz} "
+                             f"window of the workload, reference FFTW 2.1.2 float + lib_matr.c, 1 thread"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    import numpy as np
+    import torch
+    from crava_b200 import api, synth
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else None
+    spec = workload_spec(rank, dims)
+    blk = synth.make_block(spec)
+    ctx = api.Context(local_rank)
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=1000 + rank)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    keep = job.upload_block()
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        job.run(sh)
+    torch.cuda.synchronize()
+
+    ctx.set_profiling(True)
+    ctx.kernel_times(reset=True)
+    clk_path = os.path.join(tempfile.gettempdir(), f"crava_clocks_{rank}.csv")
+    sampler = start_clock_sampler(clk_path)
+    time.sleep(0.3)
+    launches0 = ctx.kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        job.run(sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    stop_clock_sampler(*sampler)
+    launches = ctx.kernel_launches() - launches0
+    ms = e0.elapsed_time(e1) / args.steps
+    kt = ctx.kernel_times(reset=True)
+    ctx.set_profiling(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * blk.n_voxels / (ms / 1000.0)
+
+    # e2e through the job API with pinned host buffers
+    shape = job.shape
+    nin = blk.ntheta + 3
+    nout = 9 + 3 * job.nsim
+    pin_in = [torch.empty(shape, dtype=torch.float32).pin_memory() for _ in range(nin)]
+    for l in range(blk.ntheta):
+        pin_in[l].numpy()[...] = blk.data[l]
+    for a in range(3):
+        pin_in[blk.ntheta + a].numpy()[...] = blk.mean[a]
+    pin_out = [torch.empty(shape, dtype=torch.float32).pin_memory() for _ in range(nout)]
+    roles_out = [(api.ROLE_POST_MEAN, a) for a in range(3)] + [(api.ROLE_POST_COV, q) for q in range(6)] + \
+                [(api.ROLE_SIM, q) for q in range(3 * job.nsim)]
+    roles_in = [(api.ROLE_DATA, l) for l in range(blk.ntheta)] + [(api.ROLE_MEAN, a) for a in range(3)]
+
+    def e2e_step():
+        for (r, i), h in zip(roles_in, pin_in):
+            api._check(api.lib().crava_job_upload(job._h, r, i, h.data_ptr(), sh))
+        job.run(sh)
+        for (r, i), h in zip(roles_out, pin_out):
+            api._check(api.lib().crava_job_download(job._h, r, i, h.data_ptr(), sh))
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / e2e_steps
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    bytes_grid = 4 * int(np.prod(shape))
+
+    # roofline of the dominant kernel class
+    peak, peak_kind = peaks()
+    ngrids = {"x_r2c": nin, "line_fwd": nin, "zpass": 1, "line_inv": nout, "x_c2r": nout}
+    dom = max(kt, key=lambda c: kt[c][0])
+    tot_ms, nl = kt[dom]
+    per_launch_ms = tot_ms / max(nl, 1)
+    ab = alg_bytes(blk, job.nsim, dom, ngrids[dom])
+    achieved = ab / (per_launch_ms / 1000.0) / 1e9
+    share = {c: round(kt[c][0] / max(sum(v[0] for v in kt.values()), 1e-9), 4) for c in kt}
+    B_alg = 12 * blk.n_voxels * (nin + nout)
+
+    parity = parity_check(ctx) if rank == 0 else None
+    clocks = summarize_clocks(clk_path, physical_gpu_index(local_rank))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"single block {blk.nx}x{blk.ny}x{blk.nz}, {blk.ntheta} angles 5..45 deg, "
+                                   f"{job.nsim} realisations, separable prior (one block per GPU)",
+                       "nx": blk.nx, "ny": blk.ny, "nz": blk.nz, "ntheta": blk.ntheta, "nsim": job.nsim,
+                       "parallelism": f"replicas x{world}",
+                       "l2": f"no flush: every step reads {nin} input grids and writes {nout} output grids of "
+                             f"{bytes_grid / 1e6:.0f} MB each (> 126 MB L2)"},
+            "e2e": {"value": world * blk.n_voxels / (ms_e2e / 1000.0), "unit": UNIT,
+                    "h2d_bytes_per_step": nin * bytes_grid, "d2h_bytes_per_step": nout * bytes_grid},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": read_traffic(dom),
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                         "alg_bytes_per_launch": ab, "ms_per_launch": per_launch_ms},
+            "job_roofline": {"alg_bytes": B_alg, "achieved_gbs": B_alg / (ms / 1000.0) / 1e9,
+                             "frac": B_alg / (ms / 1000.0) / 1e9 / peak,
+                             "model": "12*N*(G_in+G_out): every real grid crosses HBM once plus one write+read of its half-transformed intermediate"},
+            "kernel_ms_per_step": {c: kt[c][0] / args.steps for c in kt},
+            "kernel_share": share,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "parity": parity,
+        }
+        print(json.dumps(line))
+    job.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -32,7 +32,9 @@ FLAG_HOST_NOISE, FLAG_KEEP_RESIDUAL = 1, 2
 EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_status_string",
            "crava_job_create", "crava_job_destroy", "crava_job_footprint", "crava_job_upload",
            "crava_job_download", "crava_job_device_ptr", "crava_job_run", "crava_job_counters",
-           "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches"]
+           "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches", "crava_ctx_set_profiling",
+           "crava_ctx_kernel_times"]
+KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r"]
 
 
 class CravaError(RuntimeError):
@@ -90,6 +92,9 @@ def lib() -> ctypes.CDLL:
     L.crava_fft_c2r.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
     L.crava_ctx_kernel_launches.argtypes = [vp]
     L.crava_ctx_kernel_launches.restype = ctypes.c_longlong
+    L.crava_ctx_set_profiling.argtypes = [vp, ctypes.c_int]
+    L.crava_ctx_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.c_int, ctypes.c_int]
     _lib = L
     return L
 
@@ -111,6 +116,17 @@ class Context:
 
     def kernel_launches(self) -> int:
         return int(lib().crava_ctx_kernel_launches(self._h))
+
+    def set_profiling(self, on: bool):
+        _check(lib().crava_ctx_set_profiling(self._h, int(on)))
+
+    def kernel_times(self, reset: bool = True) -> dict:
+        """{class: (total ms, launches)} for launches since the last reset."""
+        n = len(KERNEL_CLASSES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        _check(lib().crava_ctx_kernel_times(self._h, ms, cnt, n, int(reset)))
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(KERNEL_CLASSES)}
 
     def close(self):
         if self._h:

@@ -77,6 +77,14 @@ struct Plan {
 
 }  // namespace
 
+// Per-kernel-class CUDA-event timing (off unless crava_ctx_set_profiling enables it).
+enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_COUNT = 5 };
+
+struct ProfRec {
+  int cat;
+  cudaEvent_t a, b;
+};
+
 struct crava_ctx {
   int device = 0;
   size_t budget = 0;
@@ -84,7 +92,32 @@ struct crava_ctx {
   long long launches = 0;
   std::mutex mu;
   std::map<int, Plan> plans;
+  bool profiling = false;
+  std::vector<ProfRec> prof;
+  double kt_ms[KT_COUNT] = {0, 0, 0, 0, 0};
+  long long kt_n[KT_COUNT] = {0, 0, 0, 0, 0};
 };
+
+namespace {
+// Brackets one launch with events on its stream when profiling is on.
+struct ProfScope {
+  crava_ctx* ctx;
+  int cat;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  ProfScope(crava_ctx* c, int k, cudaStream_t s) : ctx(c), cat(k), st(s) {
+    if (ctx->profiling && cudaEventCreate(&a) == cudaSuccess) cudaEventRecord(a, st);
+  }
+  ~ProfScope() {
+    if (!a) return;
+    cudaEvent_t b;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
+    cudaEventRecord(b, st);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->prof.push_back({cat, a, b});
+  }
+};
+}  // namespace
 
 struct crava_job {
   crava_ctx* ctx = nullptr;
@@ -310,10 +343,18 @@ crava_status fwd_xy(crava_ctx* ctx, const std::vector<const float*>& src, const 
     GridSet gs;
     gs.n = (int)std::min(g.size() - b, (size_t)kMaxGrids);
     for (int q = 0; q < gs.n; q++) { gs.p[q] = g[b + q]; gs.src[q] = src[b + q]; gs.scale[q] = sc[b + q]; }
-    CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
-    CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, -1.f, st, &nl));
-    if (with_z)
+    {
+      ProfScope ps(ctx, KT_X_R2C, st);
+      CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+    }
+    {
+      ProfScope ps(ctx, KT_LINE_FWD, st);
+      CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, -1.f, st, &nl));
+    }
+    if (with_z) {
+      ProfScope ps(ctx, KT_LINE_FWD, st);
       CUDA_TRY(launch_line_fft(gs, cnxp, nzp, (size_t)cnxp * nyp, nyp, (size_t)cnxp, pz->lp, pz->tw, -1.f, st, &nl));
+    }
   }
   ctx->launches += nl;
   return CRAVA_OK;
@@ -331,10 +372,18 @@ crava_status inv_xy(crava_ctx* ctx, const std::vector<float*>& g, const std::vec
     GridSet gs;
     gs.n = (int)std::min(g.size() - b, (size_t)kMaxGrids);
     for (int q = 0; q < gs.n; q++) { gs.p[q] = g[b + q]; gs.src[q] = g[b + q]; gs.scale[q] = sc[b + q]; }
-    if (with_z)
+    if (with_z) {
+      ProfScope ps(ctx, KT_LINE_INV, st);
       CUDA_TRY(launch_line_fft(gs, cnxp, nzp, (size_t)cnxp * nyp, nyp, (size_t)cnxp, pz->lp, pz->tw, 1.f, st, &nl));
-    CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, 1.f, st, &nl));
-    CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+    }
+    {
+      ProfScope ps(ctx, KT_LINE_INV, st);
+      CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, 1.f, st, &nl));
+    }
+    {
+      ProfScope ps(ctx, KT_X_C2R, st);
+      CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+    }
   }
   ctx->launches += nl;
   return CRAVA_OK;
@@ -382,6 +431,39 @@ crava_status crava_ctx_destroy(crava_ctx* ctx) {
 }
 
 long long crava_ctx_kernel_launches(crava_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable) {
+  if (!ctx) return fail(CRAVA_EINVAL, "null ctx");
+  ctx->profiling = enable != 0;
+  return CRAVA_OK;
+}
+
+crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset) {
+  if (!ctx || !ms || !launches) return fail(CRAVA_EINVAL, "null argument");
+  std::vector<ProfRec> recs;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    recs.swap(ctx->prof);
+  }
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  for (auto& r : recs) {
+    float t = 0.f;
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.a, r.b);
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel timing");
+    ctx->kt_ms[r.cat] += t;
+    ctx->kt_n[r.cat] += 1;
+  }
+  for (int c = 0; c < n && c < KT_COUNT; c++) {
+    ms[c] = ctx->kt_ms[c];
+    launches[c] = ctx->kt_n[c];
+  }
+  if (reset)
+    for (int c = 0; c < KT_COUNT; c++) { ctx->kt_ms[c] = 0; ctx->kt_n[c] = 0; }
+  return CRAVA_OK;
+}
 
 crava_status crava_job_footprint(const crava_job_desc* desc, size_t* bytes) {
   crava_status s = validate(desc);
@@ -614,7 +696,10 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.seed = d.seed;
   zp.counters = job->counters;
   int nl = 0;
-  CUDA_TRY(launch_zpass(zp, st, &nl));
+  {
+    ProfScope ps(ctx, KT_ZPASS, st);
+    CUDA_TRY(launch_zpass(zp, st, &nl));
+  }
   ctx->launches += nl;
   // inverse transforms (y, x) of the outputs with FFTGrid::invFFTInPlace scales
   {

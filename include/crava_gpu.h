@@ -148,6 +148,16 @@ crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int n
 /* Kernels launched by this library since the context was created (all entry points). */
 long long crava_ctx_kernel_launches(crava_ctx* ctx);
 
+/* Per-kernel-class device time (no reference counterpart: the reference's TimeKit records
+ * wall/CPU time per phase, libs/lib/timekit.cpp:9-27, src/avoinversion.cpp:1229).
+ * With profiling on, every launch is bracketed by CUDA events on its stream.
+ * crava_ctx_kernel_times waits for the recorded launches and returns, per class
+ *   0 forward x transform, 1 forward line transforms, 2 fused pencil pass,
+ *   3 inverse line transforms, 4 inverse x transform,
+ * the summed milliseconds and launch counts (n entries), then clears them if reset. */
+crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable);
+crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset);
+
 #ifdef __cplusplus
 }
 #endif
