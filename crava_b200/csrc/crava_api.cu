@@ -11,7 +11,9 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>
@@ -66,8 +68,7 @@ bool make_plan(int n, LinePlan& pl) {
       pl.radix[pl.nst++] = (int8_t)p;
       m /= p;
     }
-  if (n == 1) { pl.radix[pl.nst++] = 2; }  // never used: n >= 2 enforced by callers
-  return m == 1;
+  return m == 1;  // n == 1: no stages (identity)
 }
 
 struct Plan {
@@ -152,6 +153,16 @@ struct crava_job {
 };
 
 namespace {
+
+crava_status get_plan(crava_ctx* ctx, int n, Plan** out);
+
+// Plans of the x transform: the transform length (nxp/2 for even nxp, nxp for odd) and
+// the length-nxp table used to split the half-length transform.
+crava_status get_xplans(crava_ctx* ctx, int nxp, Plan** px, Plan** pn) {
+  crava_status s = get_plan(ctx, (nxp % 2 == 0) ? nxp / 2 : nxp, px);
+  if (s) return s;
+  return get_plan(ctx, nxp, pn);
+}
 
 crava_status get_plan(crava_ctx* ctx, int n, Plan** out) {
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -334,9 +345,9 @@ float inv_scale(size_t N, bool cov) {
 crava_status fwd_xy(crava_ctx* ctx, const std::vector<const float*>& src, const std::vector<float*>& g,
                     const std::vector<float>& sc, int nxp, int nyp, int nzp, bool with_z, cudaStream_t st) {
   if (g.empty()) return CRAVA_OK;
-  Plan *px, *py, *pz;
+  Plan *px, *pn, *py, *pz;
   crava_status s;
-  if ((s = get_plan(ctx, nxp, &px)) || (s = get_plan(ctx, nyp, &py)) || (s = get_plan(ctx, nzp, &pz))) return s;
+  if ((s = get_xplans(ctx, nxp, &px, &pn)) || (s = get_plan(ctx, nyp, &py)) || (s = get_plan(ctx, nzp, &pz))) return s;
   int cnxp = nxp / 2 + 1;
   int nl = 0;
   for (size_t b = 0; b < g.size(); b += kMaxGrids) {
@@ -345,7 +356,7 @@ crava_status fwd_xy(crava_ctx* ctx, const std::vector<const float*>& src, const 
     for (int q = 0; q < gs.n; q++) { gs.p[q] = g[b + q]; gs.src[q] = src[b + q]; gs.scale[q] = sc[b + q]; }
     {
       ProfScope ps(ctx, KT_X_R2C, st);
-      CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+      CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, pn->tw, st, &nl));
     }
     {
       ProfScope ps(ctx, KT_LINE_FWD, st);
@@ -363,9 +374,9 @@ crava_status fwd_xy(crava_ctx* ctx, const std::vector<const float*>& src, const 
 crava_status inv_xy(crava_ctx* ctx, const std::vector<float*>& g, const std::vector<float>& sc, int nxp, int nyp,
                     int nzp, bool with_z, cudaStream_t st) {
   if (g.empty()) return CRAVA_OK;
-  Plan *px, *py, *pz;
+  Plan *px, *pn, *py, *pz;
   crava_status s;
-  if ((s = get_plan(ctx, nxp, &px)) || (s = get_plan(ctx, nyp, &py)) || (s = get_plan(ctx, nzp, &pz))) return s;
+  if ((s = get_xplans(ctx, nxp, &px, &pn)) || (s = get_plan(ctx, nyp, &py)) || (s = get_plan(ctx, nzp, &pz))) return s;
   int cnxp = nxp / 2 + 1;
   int nl = 0;
   for (size_t b = 0; b < g.size(); b += kMaxGrids) {
@@ -382,7 +393,7 @@ crava_status inv_xy(crava_ctx* ctx, const std::vector<float*>& g, const std::vec
     }
     {
       ProfScope ps(ctx, KT_X_C2R, st);
-      CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, st, &nl));
+      CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, pn->tw, st, &nl));
     }
   }
   ctx->launches += nl;
@@ -566,16 +577,16 @@ crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_
     for (int jj = 0; jj < d.nyp; jj++)
       for (int ii = 0; ii < d.nxp; ii++) g[(size_t)jj * j->rnxp + ii] = j->corr_xy[(size_t)jj * d.nxp + ii];
     CUDA_TRY(cudaMemcpy(j->cxy_grid, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice));
-    Plan *px, *py;
+    Plan *px, *pn, *py;
     crava_status ps;
-    if ((ps = get_plan(ctx, d.nxp, &px)) || (ps = get_plan(ctx, d.nyp, &py))) return ps;
+    if ((ps = get_xplans(ctx, d.nxp, &px, &pn)) || (ps = get_plan(ctx, d.nyp, &py))) return ps;
     GridSet gs;
     gs.n = 1;
     gs.p[0] = j->cxy_grid;
     gs.src[0] = j->cxy_grid;
     gs.scale[0] = 1.0f;
     int nl = 0;
-    CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, 0, &nl));
+    CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, pn->tw, 0, &nl));
     CUDA_TRY(launch_line_fft(gs, j->cnxp, d.nyp, (size_t)j->cnxp, 1, 0, py->lp, py->tw, -1.f, 0, &nl));
     CUDA_TRY(cudaMemcpy(j->cxy, j->cxy_grid, sizeof(float2) * j->cnxp * d.nyp, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaDeviceSynchronize());
@@ -663,10 +674,17 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   std::memset(&zp, 0, sizeof(zp));
   zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = job->cnxp;
   zp.nxp_even = (d.nxp % 2) == 0;
-  int W = 8;
-  while (W > 1 && (W * d.nzp > 16 * 256 || zpass_smem_bytes(W, d.nzp, d.ntheta) > 113 * 1024)) W /= 2;
+  // pencil tile: W x-bins (power of two); prefer two resident CTAs of 256 threads per
+  // SM, else one CTA of 512 threads (CRAVA_ZPASS_W / CRAVA_ZPASS_T override)
+  int W = 4, T = 256;
+  if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 113 * 1024) T = 512;
+  while (W > 1 && zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) W /= 2;
+  if (const char* ev = getenv("CRAVA_ZPASS_W")) W = std::max(1, atoi(ev));
+  if (const char* ev = getenv("CRAVA_ZPASS_T")) T = std::max(64, atoi(ev));
   if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
   zp.W = W;
+  zp.logW = 0;
+  while ((1 << zp.logW) < W) zp.logW++;
   zp.nIT = (job->cnxp + W - 1) / W;
   zp.nth = d.ntheta;
   zp.nsim = d.nsim;
@@ -698,7 +716,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   int nl = 0;
   {
     ProfScope ps(ctx, KT_ZPASS, st);
-    CUDA_TRY(launch_zpass(zp, st, &nl));
+    CUDA_TRY(launch_zpass(zp, T, st, &nl));
   }
   ctx->launches += nl;
   // inverse transforms (y, x) of the outputs with FFTGrid::invFFTInPlace scales

@@ -159,63 +159,103 @@ struct Dft<8> {
   }
 };
 
-// Butterfly j of line `line` for the ordering used by a layout: when points are
-// contiguous (PFAST) consecutive threads take consecutive j of one line, otherwise
-// consecutive lines at the same j (lines contiguous in memory).
-template <bool PFAST>
-__device__ __forceinline__ void bfly_index(int idx, int nb, int nlines, int& line, int& j) {
-  if (PFAST) {
-    line = idx / nb;
-    j = idx - line * nb;
-  } else {
-    j = idx / nlines;
-    line = idx - j * nlines;
-  }
+// q = x / d, r = x % d for 0 <= x < 2^22 and d >= 1, with rcp = 1/d rounded to float:
+// the float quotient is within one of the exact one and a single correction fixes it.
+__device__ __forceinline__ int fdivmod(int x, int d, float rcp, int& r) {
+  int q = __float2int_rz(__int2float_rn(x) * rcp);
+  r = x - q * d;
+  if (r < 0) { q -= 1; r += d; }
+  else if (r >= d) { q += 1; r -= d; }
+  return q;
 }
 
-// One Stockham stage over nlines lines from `in` to `out` (both shared memory, same
-// layout: element p of line l at l*ls + p*ps).  Each thread loops over whole butterflies,
-// so a thread holds only R points at a time.
-template <int R, bool PFAST>
+// Thread-to-line mapping shared by every stage of one fft_lines call in LC mode:
+// thread t starts at line t % nlines, butterfly row t / nlines, and advances by T.
+struct LcMap {
+  int f0, s0, df, ds;
+};
+
+// One Stockham stage over nlines lines from `in` to `out` (shared memory).  Element p of
+// line l sits at l*ls + p*psi in `in` and l*ls + p*pso in `out`.  LC (lines contiguous):
+// consecutive threads take consecutive lines of one butterfly index j; otherwise
+// consecutive j of one line.  The (line, j, j mod Ns, j / Ns) of a thread's butterflies
+// are advanced incrementally after a few reciprocal-based divisions per stage.
+template <int R, bool LC>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out, int nlines,
-                                          int ls, int ps, int n, int Ns, const float2* __restrict__ tw,
-                                          float sign) {
+                                          int ls, int psi, int pso, int n, int Ns, const LcMap& mp,
+                                          const float2* __restrict__ tw, float sign) {
   const int nb = n / R;
   const int total = nlines * nb;
-  const int twstride = n / (Ns * R);
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    int line, j;
-    bfly_index<PFAST>(idx, nb, nlines, line, j);
-    const float2* src = in + line * ls + j * ps;
+  const int T = blockDim.x;
+  const float rNs = __frcp_rn((float)Ns);
+  int tmp;
+  const int nbh = fdivmod(nb, Ns, rNs, tmp);  // nb / Ns (exact)
+  const int twstride = nbh;                   // n / (Ns R)
+  int idx = threadIdx.x;
+  int line, j, df, ds;
+  if (LC) {
+    line = mp.f0; j = mp.s0; df = mp.df; ds = mp.ds;
+  } else {
+    const float rnb = __frcp_rn((float)nb);
+    int f;
+    line = fdivmod(idx, nb, rnb, f);
+    j = f;
+    ds = fdivmod(T, nb, rnb, df);
+  }
+  int k;
+  int jh = fdivmod(j, Ns, rNs, k);
+  // j advances by dj per iteration, plus a carry from the fast index when LC; when not
+  // LC, j wraps at nb (a multiple of Ns) into the next line
+  const int dj = LC ? ds : df;
+  int dk;
+  const int djh = fdivmod(dj, Ns, rNs, dk);
+  for (; idx < total; idx += T) {
+    const float2* src = in + line * ls + j * psi;
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = src[r * nb * ps];
-    int k = j % Ns;
+    for (int r = 0; r < R; r++) v[r] = src[r * nb * psi];
     if (Ns > 1) {
+      const int tk = k * twstride;
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        float2 w = tw[r * k * twstride];
+        float2 w = tw[r * tk];
         w.y *= -sign;  // table holds e^{-2 pi i t/n}; sign=+1 conjugates
         v[r] = cmul(v[r], w);
       }
     }
     Dft<R>::run(v, sign);
-    float2* dst = out + line * ls + ((j - k) * R + k) * ps;
+    float2* dst = out + line * ls + (jh * Ns * R + k) * pso;
 #pragma unroll
-    for (int r = 0; r < R; r++) dst[r * Ns * ps] = v[r];
+    for (int r = 0; r < R; r++) dst[r * Ns * pso] = v[r];
+    if (LC) {
+      line += df;
+      int carry = line >= nlines;
+      if (carry) line -= nlines;
+      j += dj + carry;
+      k += dk + carry;
+      jh += djh;
+      if (k >= Ns) { k -= Ns; jh += 1; }
+    } else {
+      j += dj;
+      k += dk;
+      jh += djh;
+      if (k >= Ns) { k -= Ns; jh += 1; }
+      line += ds;
+      if (j >= nb) { j -= nb; jh -= nbh; line += 1; }
+    }
   }
   __syncthreads();
 }
 
-// Full transform of nlines lines of length pl.n held in `buf`, using `scratch` (same
-// size and layout) for the ping-pong stages; the result is left in `buf`.  sign = -1
-// forward, +1 inverse (unnormalised both ways, like FFTW).  tw: the length-n table,
-// usually in shared memory.  The caller synchronises before the call (buf complete);
-// the function returns after a barrier.  The stages run grouped by radix in the plan's
-// fixed order 8..8, 4, 2, 3..3, 5..5, 7..7.
-template <bool PFAST>
+// Full transform of nlines lines of length pl.n.  The lines start in `buf` (point stride
+// ps) and end there; `scratch` (dense, point stride nlines when LC, line stride n
+// otherwise) holds the odd stages.  sign = -1 forward, +1 inverse, unnormalised both
+// ways like FFTW.  tw: the length-n table, usually in shared memory.  The caller
+// synchronises before the call; the function returns after a barrier.  Stages run
+// grouped by radix in the plan's fixed order 8..8, 4, 2, 3..3, 5..5, 7..7.
+template <bool LC>
 __device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlines, int ls, int ps,
-                                          const LinePlan pl, const float2* __restrict__ tw, float sign) {
+                                          const LinePlan& pl, const float2* __restrict__ tw, float sign) {
   int Ns = 1;
   const int n = pl.n;
   int c8 = 0, c4 = 0, c2 = 0, c3 = 0, c5 = 0, c7 = 0;
@@ -223,13 +263,26 @@ __device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlin
     int R = pl.radix[s];
     c8 += R == 8; c4 += R == 4; c2 += R == 2; c3 += R == 3; c5 += R == 5; c7 += R == 7;
   }
-  float2* a = buf;
-  float2* b = scratch;
-#define CRAVA_STAGE(RR)                                                    \
-  {                                                                        \
-    fft_stage<RR, PFAST>(a, b, nlines, ls, ps, n, Ns, tw, sign);           \
-    Ns *= RR;                                                              \
-    float2* t_ = a; a = b; b = t_;                                         \
+  LcMap mp{0, 0, 0, 0};
+  if (LC) {
+    const float rl = __frcp_rn((float)nlines);
+    mp.s0 = fdivmod(threadIdx.x, nlines, rl, mp.f0);
+    mp.ds = fdivmod(blockDim.x, nlines, rl, mp.df);
+  }
+  // scratch layout: LC -> element (l, p) at l + p*nlines; else at l*n + p
+  const int sps = LC ? nlines : 1;
+  bool in_buf = true;
+#define CRAVA_STAGE(RR)                                                                             \
+  {                                                                                                 \
+    if (in_buf) {                                                                                   \
+      if (LC) fft_stage<RR, LC>(buf, scratch, nlines, 1, ps, sps, n, Ns, mp, tw, sign);             \
+      else fft_stage<RR, LC>(buf, scratch, nlines, ls, ps, sps, n, Ns, mp, tw, sign);               \
+    } else {                                                                                        \
+      if (LC) fft_stage<RR, LC>(scratch, buf, nlines, 1, sps, ps, n, Ns, mp, tw, sign);             \
+      else fft_stage<RR, LC>(scratch, buf, nlines, ls, sps, ps, n, Ns, mp, tw, sign);               \
+    }                                                                                               \
+    Ns *= RR;                                                                                       \
+    in_buf = !in_buf;                                                                               \
   }
 #pragma unroll 1
   for (int q = 0; q < c8; q++) CRAVA_STAGE(8)
@@ -242,8 +295,22 @@ __device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlin
 #pragma unroll 1
   for (int q = 0; q < c7; q++) CRAVA_STAGE(7)
 #undef CRAVA_STAGE
-  if (a != buf) {  // odd number of stages: copy back (the layouts used are dense)
-    for (int e = threadIdx.x; e < nlines * n; e += blockDim.x) buf[e] = a[e];
+  if (!in_buf) {  // odd number of stages: copy back
+    if (LC) {
+      const float rl = __frcp_rn((float)nlines);
+      for (int e = threadIdx.x; e < nlines * n; e += blockDim.x) {
+        int l;
+        int p = fdivmod(e, nlines, rl, l);
+        buf[l + p * ps] = scratch[e];
+      }
+    } else {
+      const float rn = __frcp_rn((float)n);
+      for (int e = threadIdx.x; e < nlines * n; e += blockDim.x) {
+        int p;
+        int l = fdivmod(e, n, rn, p);
+        buf[l * ls + p * ps] = scratch[e];
+      }
+    }
     __syncthreads();
   }
 }

@@ -19,75 +19,178 @@ namespace crava {
 constexpr int kThreads = 256;
 
 // ------------------------------------------------------------------ x transforms
+//
+// Even nxp (h = nxp/2): a row x is read as h complex values z[m] = x[2m] + i x[2m+1]
+// (the same bytes), transformed with a length-h complex FFT, and split into the half
+// spectrum with w = e^{-2 pi i/nxp}:
+//   E = (Z[k] + conj Z[h-k]) / 2,  O = (Z[k] - conj Z[h-k]) / 2i,
+//   X[k] = E + w^k O,  X[h-k] = conj(E - w^k O),  X[0] = Re+Im Z[0], X[h] = Re-Im Z[0].
+// The inverse runs the same steps backwards:
+//   P = X[k] + conj X[h-k], Q = (X[k] - conj X[h-k]) conj(w^k),
+//   Z'[k] = P + iQ, Z'[h-k] = conj P + i conj Q, Z'[0] from Re X[0], Re X[h] only
+// (a real-output inverse has no slot for Im X[0], Im X[h]), then a length-h inverse
+// FFT gives nxp * (x[2m] + i x[2m+1]).  Odd nxp uses a full-length complex transform.
 
-__global__ void __launch_bounds__(512) k_x_r2c(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc, LinePlan pl,
-                                                const float2* __restrict__ twg) {
+__global__ void __launch_bounds__(512) k_x_r2c(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
+                                                const __grid_constant__ LinePlan pl, const float2* __restrict__ twg,
+                                                const float2* __restrict__ twn) {
   extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* buf = sm + nxp;
-  float2* scr = buf + rpc * nxp;
   const int T = blockDim.x, tid = threadIdx.x;
+  const bool even = (nxp & 1) == 0;
+  const int n = even ? nxp / 2 : nxp;       // transform length
+  const int cnxp = nxp / 2 + 1;
+  const float rn = __frcp_rn((float)n);
+  float2* tw = sm;                          // n
+  float2* twh = tw + n;                     // nxp/2 (even only): e^{-2 pi i k / nxp}
+  float2* buf = twh + (even ? nxp / 2 : 0);
+  float2* scr = buf + rpc * n;
   float* g = gs.p[blockIdx.y];
   const float scale = gs.scale[blockIdx.y];
   const int row0 = blockIdx.x * rpc;
   const int nr = min(rpc, rows - row0);
-  const int rnxp = 2 * (nxp / 2 + 1), cnxp = nxp / 2 + 1;
-  for (int t = tid; t < nxp; t += T) tw[t] = twg[t];
-  const float* src = gs.src[blockIdx.y] + (size_t)row0 * rnxp;
-  for (int e = tid; e < nr * nxp; e += T) {
-    int r = e / nxp, p = e - r * nxp;
-    buf[e] = make_float2(src[(size_t)r * rnxp + p] * scale, 0.f);
+  for (int t = tid; t < n; t += T) tw[t] = twg[t];
+  if (even)
+    for (int t = tid; t < nxp / 2; t += T) twh[t] = twn[t];
+  if (even) {
+    const float2* src = reinterpret_cast<const float2*>(gs.src[blockIdx.y]) + (size_t)row0 * cnxp;
+    for (int e = tid; e < nr * n; e += T) {
+      int m;
+      int r = fdivmod(e, n, rn, m);
+      float2 v = src[(size_t)r * cnxp + m];
+      buf[e] = make_float2(v.x * scale, v.y * scale);
+    }
+  } else {
+    const float* src = gs.src[blockIdx.y] + (size_t)row0 * 2 * cnxp;
+    for (int e = tid; e < nr * n; e += T) {
+      int p;
+      int r = fdivmod(e, n, rn, p);
+      buf[e] = make_float2(src[(size_t)r * 2 * cnxp + p] * scale, 0.f);
+    }
   }
   __syncthreads();
-  fft_lines<true>(buf, scr, nr, nxp, 1, pl, tw, -1.f);
+  fft_lines<false>(buf, scr, nr, n, 1, pl, tw, -1.f);
   float2* dst = reinterpret_cast<float2*>(g) + (size_t)row0 * cnxp;
-  for (int e = tid; e < nr * cnxp; e += T) {
-    int r = e / cnxp, p = e - r * cnxp;
-    dst[e] = buf[r * nxp + p];
+  if (even) {
+    const int h = n, np = h / 2 + 1;  // pairs (k, h-k), k = 0..h/2
+    const float rnp = __frcp_rn((float)np);
+    for (int e = tid; e < nr * np; e += T) {
+      int k;
+      int r = fdivmod(e, np, rnp, k);
+      const float2* Z = buf + r * h;
+      float2* X = dst + (size_t)r * cnxp;
+      if (k == 0) {
+        float2 z0 = Z[0];
+        X[0] = make_float2(z0.x + z0.y, 0.f);
+        X[h] = make_float2(z0.x - z0.y, 0.f);
+        continue;
+      }
+      float2 A = Z[k], Bc = Z[h - k];  // B = conj(Bc)
+      float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y - Bc.y));
+      // O = (A - B) / 2i = -i (A - B) / 2
+      float2 D = make_float2(A.x - Bc.x, A.y + Bc.y);
+      float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+      float2 t = cmul(twh[k], O);
+      X[k] = cadd(E, t);
+      if (2 * k != h) {
+        float2 m = csub(E, t);
+        X[h - k] = make_float2(m.x, -m.y);
+      }
+    }
+  } else {
+    const float rc = __frcp_rn((float)cnxp);
+    for (int e = tid; e < nr * cnxp; e += T) {
+      int p;
+      int r = fdivmod(e, cnxp, rc, p);
+      dst[e] = buf[r * n + p];
+    }
   }
 }
 
-__global__ void __launch_bounds__(512) k_x_c2r(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc, LinePlan pl,
-                                                const float2* __restrict__ twg) {
+__global__ void __launch_bounds__(512) k_x_c2r(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
+                                                const __grid_constant__ LinePlan pl, const float2* __restrict__ twg,
+                                                const float2* __restrict__ twn) {
   extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* buf = sm + nxp;
-  float2* scr = buf + rpc * nxp;
   const int T = blockDim.x, tid = threadIdx.x;
+  const bool even = (nxp & 1) == 0;
+  const int n = even ? nxp / 2 : nxp;
+  const int cnxp = nxp / 2 + 1;
+  const float rn = __frcp_rn((float)n);
+  float2* tw = sm;
+  float2* twh = tw + n;
+  float2* buf = twh + (even ? nxp / 2 : 0);
+  float2* scr = buf + rpc * n;
   float* g = gs.p[blockIdx.y];
   const float scale = gs.scale[blockIdx.y];
   const int row0 = blockIdx.x * rpc;
   const int nr = min(rpc, rows - row0);
-  const int rnxp = 2 * (nxp / 2 + 1), cnxp = nxp / 2 + 1;
-  for (int t = tid; t < nxp; t += T) tw[t] = twg[t];
+  for (int t = tid; t < n; t += T) tw[t] = twg[t];
+  if (even)
+    for (int t = tid; t < nxp / 2; t += T) twh[t] = twn[t];
+  __syncthreads();
   const float2* src = reinterpret_cast<const float2*>(g) + (size_t)row0 * cnxp;
-  // Hermitian extension of each row; the imaginary parts of the DC and Nyquist terms do
-  // not enter a real-output inverse (halfcomplex input has no slot for them)
-  for (int e = tid; e < nr * nxp; e += T) {
-    int r = e / nxp, p = e - r * nxp;
-    float2 v;
-    if (p < cnxp) {
-      v = src[(size_t)r * cnxp + p];
-      if (p == 0 || 2 * p == nxp) v.y = 0.f;
-    } else {
-      v = src[(size_t)r * cnxp + (nxp - p)];
-      v.y = -v.y;
+  if (even) {
+    const int h = n, np = h / 2 + 1;
+    const float rnp = __frcp_rn((float)np);
+    for (int e = tid; e < nr * np; e += T) {
+      int k;
+      int r = fdivmod(e, np, rnp, k);
+      const float2* X = src + (size_t)r * cnxp;
+      float2* Z = buf + r * h;
+      if (k == 0) {
+        float a = X[0].x, b = X[h].x;
+        Z[0] = make_float2(a + b, a - b);
+        continue;
+      }
+      float2 xk = X[k], xm = X[h - k];
+      float2 P = make_float2(xk.x + xm.x, xk.y - xm.y);       // X[k] + conj X[h-k]
+      float2 M = make_float2(xk.x - xm.x, xk.y + xm.y);       // X[k] - conj X[h-k]
+      float2 w = twh[k];
+      float2 Q = make_float2(M.x * w.x + M.y * w.y, M.y * w.x - M.x * w.y);  // M conj(w)
+      Z[k] = make_float2(P.x - Q.y, P.y + Q.x);               // P + iQ
+      if (2 * k != h) Z[h - k] = make_float2(P.x + Q.y, -P.y + Q.x);  // conj P + i conj Q
     }
-    buf[e] = v;
+  } else {
+    // Hermitian extension; Im X[0] (and Im X[nxp/2]) do not enter a real-output inverse
+    for (int e = tid; e < nr * n; e += T) {
+      int p;
+      int r = fdivmod(e, n, rn, p);
+      float2 v;
+      if (p < cnxp) {
+        v = src[(size_t)r * cnxp + p];
+        if (p == 0) v.y = 0.f;
+      } else {
+        v = src[(size_t)r * cnxp + (n - p)];
+        v.y = -v.y;
+      }
+      buf[e] = v;
+    }
   }
   __syncthreads();
-  fft_lines<true>(buf, scr, nr, nxp, 1, pl, tw, 1.f);
-  float* dst = g + (size_t)row0 * rnxp;
-  for (int e = tid; e < nr * rnxp; e += T) {
-    int r = e / rnxp, p = e - r * rnxp;
-    dst[e] = (p < nxp) ? buf[r * nxp + p].x * scale : 0.f;
+  fft_lines<false>(buf, scr, nr, n, 1, pl, tw, 1.f);
+  if (even) {
+    float2* dst = reinterpret_cast<float2*>(g) + (size_t)row0 * cnxp;
+    const float rc = __frcp_rn((float)cnxp);
+    for (int e = tid; e < nr * cnxp; e += T) {
+      int m;
+      int r = fdivmod(e, cnxp, rc, m);
+      float2 v = (m < n) ? buf[r * n + m] : make_float2(0.f, 0.f);
+      dst[e] = make_float2(v.x * scale, v.y * scale);
+    }
+  } else {
+    float* dst = g + (size_t)row0 * 2 * cnxp;
+    const float r2c = __frcp_rn((float)(2 * cnxp));
+    for (int e = tid; e < nr * 2 * cnxp; e += T) {
+      int p;
+      int r = fdivmod(e, 2 * cnxp, r2c, p);
+      dst[e] = (p < n) ? buf[r * n + p].x * scale : 0.f;
+    }
   }
 }
 
 // ------------------------------------------------------------------ strided line transform
 
 __global__ void __launch_bounds__(512) k_line_fft(const __grid_constant__ GridSet gs, int ni, int n, size_t pstride, int no,
-                                                   size_t ostride, int W, int nIT, LinePlan pl,
+                                                   size_t ostride, int W, int nIT, const __grid_constant__ LinePlan pl,
                                                    const float2* __restrict__ twg, float sign) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -100,14 +203,15 @@ __global__ void __launch_bounds__(512) k_line_fft(const __grid_constant__ GridSe
   const int nw = min(W, ni - i0);
   float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)o * ostride + i0;
   for (int t = tid; t < n; t += T) tw[t] = twg[t];
+  const int lw = 31 - __clz(W);  // W is a power of two
   for (int e = tid; e < n * W; e += T) {
-    int p = e / W, w = e - p * W;
+    int p = e >> lw, w = e & (W - 1);
     buf[e] = (w < nw) ? g[(size_t)p * pstride + w] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_lines<false>(buf, scr, W, 1, W, pl, tw, sign);
+  fft_lines<true>(buf, scr, W, 1, W, pl, tw, sign);
   for (int e = tid; e < n * W; e += T) {
-    int p = e / W, w = e - p * W;
+    int p = e >> lw, w = e & (W - 1);
     if (w < nw) g[(size_t)p * pstride + w] = buf[e];
   }
 }
@@ -119,41 +223,40 @@ static int round_threads(int t) {
   return t < 64 ? 64 : t;
 }
 
-cudaError_t launch_x_r2c(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
-                         cudaStream_t st, int* nlaunch) {
-  int rpc = std::max(1, std::min(64, 4096 / nxp));
-  int T = std::min(512, round_threads(rpc * nxp / 8));
-  size_t smem = sizeof(float2) * (size_t)(nxp + 2 * rpc * nxp);
+static cudaError_t launch_x(bool fwd, const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
+                            const float2* twn, cudaStream_t st, int* nlaunch) {
+  const bool even = (nxp & 1) == 0;
+  const int n = even ? nxp / 2 : nxp;
+  int rpc = std::max(1, std::min(64, 2048 / n));
+  int T = std::min(512, round_threads(rpc * n / 8));
+  size_t smem = sizeof(float2) * (size_t)(n + (even ? nxp / 2 : 0) + 2 * rpc * n);
   dim3 grid((rows + rpc - 1) / rpc, gs.n);
+  const void* fn = fwd ? (const void*)k_x_r2c : (const void*)k_x_c2r;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_x_r2c<<<grid, T, smem, st>>>(gs, nxp, rows, rpc, pl, tw);
+  if (fwd) k_x_r2c<<<grid, T, smem, st>>>(gs, nxp, rows, rpc, pl, tw, twn);
+  else k_x_c2r<<<grid, T, smem, st>>>(gs, nxp, rows, rpc, pl, tw, twn);
   if (nlaunch) (*nlaunch)++;
   return cudaGetLastError();
 }
 
+cudaError_t launch_x_r2c(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
+                         const float2* twn, cudaStream_t st, int* nlaunch) {
+  return launch_x(true, gs, nxp, rows, pl, tw, twn, st, nlaunch);
+}
+
 cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
-                         cudaStream_t st, int* nlaunch) {
-  int rpc = std::max(1, std::min(64, 4096 / nxp));
-  int T = std::min(512, round_threads(rpc * nxp / 8));
-  size_t smem = sizeof(float2) * (size_t)(nxp + 2 * rpc * nxp);
-  dim3 grid((rows + rpc - 1) / rpc, gs.n);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  k_x_c2r<<<grid, T, smem, st>>>(gs, nxp, rows, rpc, pl, tw);
-  if (nlaunch) (*nlaunch)++;
-  return cudaGetLastError();
+                         const float2* twn, cudaStream_t st, int* nlaunch) {
+  return launch_x(false, gs, nxp, rows, pl, tw, twn, st, nlaunch);
 }
 
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch) {
   int W = 16;
   while (W > 1 && W * n > 8192) W /= 2;
-  if (W > ni) W = ni < 1 ? 1 : ni;
+  while (W > 1 && W / 2 >= ni) W /= 2;  // power of two, not wider than needed
   int T = std::min(512, round_threads(W * n / 8));
   int nIT = (ni + W - 1) / W;
   size_t smem = sizeof(float2) * (size_t)(n + 2 * W * n);

@@ -30,7 +30,7 @@ struct KzTables {
 
 struct ZParams {
   int nxp, nyp, nzp, cnxp;
-  int W, nIT;                  // tile width in x-bins, tiles per x-row
+  int W, logW, nIT;            // tile width in x-bins (power of two), log2 W, tiles per x-row
   int nth, nsim;
   int separable;               // 1: prior from cxy/ct factors, 0: from spectral grids
   int host_noise;              // 1: noise from `noise` grids
@@ -56,16 +56,18 @@ struct ZParams {
 };
 
 // launchers (kernels.cu)
+// x transforms: pl/tw are the plan and table of length nxp/2 (even nxp) or nxp (odd);
+// twn is the length-nxp table (its first nxp/2 entries are read; unused for odd nxp).
 cudaError_t launch_x_r2c(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
-                         cudaStream_t st, int* nlaunch);
+                         const float2* twn, cudaStream_t st, int* nlaunch);
 cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
-                         cudaStream_t st, int* nlaunch);
+                         const float2* twn, cudaStream_t st, int* nlaunch);
 // Complex transform along a strided axis, in place, for all grids of gs:
 //   element (i, p, o) at ((size_t)o * ostride + (size_t)p * pstride + i) complex,
 //   0 <= i < ni (contiguous), 0 <= p < n (the transform axis), 0 <= o < no.
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch);
-cudaError_t launch_zpass(const ZParams& zp, cudaStream_t st, int* nlaunch);
+cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch);
 size_t zpass_smem_bytes(int W, int nzp, int nth);
 
 }  // namespace crava

@@ -14,7 +14,6 @@
 
 namespace crava {
 
-constexpr int kThreads = 256;
 
 // ------------------------------------------------------------------ noise (product mode)
 
@@ -31,13 +30,24 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
   return c;
 }
 
-// Standard complex normal for bin (i,j,k) of noise grid g, Hermitian-consistent on the
-// planes whose x-bin is its own mirror (i = 0, and i = nxp/2 for even nxp): the pair
-// (j,k) / (-j,-k) share one draw (conjugated), self-mirrored bins are real with unit
-// variance, all others have variance 1/2 per component (FFTGrid::fillInComplexNoise,
-// src/fftgrid.cpp:997-1055, with the mirror plane test done on the x index).
-__device__ __forceinline__ float2 device_noise(uint64_t seed, int g, int i, int j, int k, int nyp, int nzp,
-                                               int cnxp, bool nxp_even) {
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, float& n1) {
+  float u1 = ((float)a + 0.5f) * 2.3283064365386963e-10f;
+  float u2 = (float)b * 2.3283064365386963e-10f;
+  float rad = sqrtf(-2.0f * logf(u1));
+  float sn, cs;
+  sincospif(2.0f * u2, &sn, &cs);
+  n0 = rad * cs;
+  n1 = rad * sn;
+}
+
+// Three standard complex normals (one per parameter) for bin (i,j,k) of realisation s,
+// Hermitian-consistent on the planes whose x-bin is its own mirror (i = 0, and
+// i = nxp/2 for even nxp): the pair (j,k) / (-j,-k) share one draw (conjugated),
+// self-mirrored bins are real with unit variance, all others have variance 1/2 per
+// component (the properties FFTGrid::fillInComplexNoise gives its noise,
+// src/fftgrid.cpp:997-1055, with the mirror-plane test done on the x index).
+__device__ __forceinline__ void device_noise3(uint64_t seed, int s, int i, int j, int k, int nyp, int nzp,
+                                              int cnxp, bool nxp_even, float2 (&z)[3]) {
   bool mirror_plane = (i == 0) || (nxp_even && i == cnxp - 1);
   int jj = j, kk = k;
   bool conj = false, self = false;
@@ -49,18 +59,19 @@ __device__ __forceinline__ float2 device_noise(uint64_t seed, int g, int i, int 
     else if (b < a) { jj = jc; kk = kc; conj = true; }
   }
   uint64_t bin = ((uint64_t)kk * nyp + jj) * cnxp + i;
-  uint4 r = philox4x32_10(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)g, 0x43524156u),
-                          make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
-  float u1 = ((float)r.x + 0.5f) * 2.3283064365386963e-10f;
-  float u2 = (float)r.y * 2.3283064365386963e-10f;
-  float rad = sqrtf(-2.0f * logf(u1));
-  float sn, cs;
-  sincospif(2.0f * u2, &sn, &cs);
-  if (self) return make_float2(rad * cs, 0.f);
-  const float h = 0.70710678118654752f;
-  float2 z = make_float2(h * rad * cs, h * rad * sn);
-  if (conj) z.y = -z.y;
-  return z;
+  uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  uint4 r0 = philox4x32_10(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 0u), key);
+  uint4 r1 = philox4x32_10(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 1u), key);
+  float n[6];
+  box_muller(r0.x, r0.y, n[0], n[1]);
+  box_muller(r0.z, r0.w, n[2], n[3]);
+  box_muller(r1.x, r1.y, n[4], n[5]);
+  const float h = self ? 1.0f : 0.70710678118654752f;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    z[c] = make_float2(h * n[2 * c], self ? 0.f : h * n[2 * c + 1]);
+    if (conj) z[c].y = -z[c].y;
+  }
 }
 
 // ------------------------------------------------------------------ per-bin algebra
@@ -212,17 +223,27 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
 
 // ------------------------------------------------------------------ the fused z pass
 
+// Shared-memory layout of one pencil tile (W consecutive x-bins at one y, all nzp kz):
+//   tw  [nzp]             z twiddles
+//   R   [nzp][G][W]       G = max(nth + 3, 9) slots per bin: inputs data 0..nth-1 and
+//                         mean nth..nth+2; after the per-bin step outputs S_post 0..5 and
+//                         mu_post 6..8 (each bin's slots are owned by the thread of that bin)
+//   S3  [nzp][3][W]       one realisation's three output spectra
+//   SC  [3 * W * nzp]     transform scratch for groups of up to three slots
+// Element (slot g, kz k, x-offset w) of R is R[(k * G + g) * W + w].
+__device__ __forceinline__ int zslots(int nth) { return nth + 3 > 9 ? nth + 3 : 9; }
+
 template <int NTH>
-__global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ ZParams P) {
+__global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P) {
   extern __shared__ float2 sm[];
-  const int nzp = P.nzp, W = P.W;
-  const int TS = W * nzp;                      // points per tile
-  constexpr int NR1 = NTH > 6 ? NTH : 6;
-  float2* tw = sm;                             // nzp
-  float2* R1 = tw + nzp;                       // NR1 tiles: data, then S_post
-  float2* R2 = R1 + NR1 * TS;                  // 3 tiles: mean, then mu_post
-  float2* R3 = R2 + 3 * TS;                    // 1 tile: realisation output
-  float2* SC = R3 + TS;                        // 1 tile: transform scratch
+  const int nzp = P.nzp, W = P.W, lw = P.logW;
+  const int TS = W * nzp;
+  constexpr int G = NTH + 3 > 9 ? NTH + 3 : 9;
+  constexpr int GIN = NTH + 3;
+  float2* tw = sm;
+  float2* R = tw + nzp;
+  float2* S3 = R + G * TS;
+  float2* SC = S3 + 3 * TS;
   __shared__ unsigned long long cnt[3];
   const int T = blockDim.x, tid = threadIdx.x;
   const int it = blockIdx.x % P.nIT;
@@ -234,36 +255,32 @@ __global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ ZPar
 
   if (tid < 3) cnt[tid] = 0;
   for (int t = tid; t < nzp; t += T) tw[t] = P.twz[t];
-  auto load_tile = [&](float2* dst, const float2* g) {
-    for (int e = tid; e < TS; e += T) {
-      int k = e / W, w = e - k * W;
-      dst[e] = (w < nw) ? g[base + (size_t)k * kstride + w] : make_float2(0.f, 0.f);
-    }
-  };
-  auto store_tile = [&](float2* g, const float2* src) {
-    for (int e = tid; e < TS; e += T) {
-      int k = e / W, w = e - k * W;
-      if (w < nw) g[base + (size_t)k * kstride + w] = src[e];
-    }
-  };
-#pragma unroll 1
-  for (int l = 0; l < NTH; l++) load_tile(R1 + l * TS, P.data[l]);
-#pragma unroll 1
-  for (int a = 0; a < 3; a++) load_tile(R2 + a * TS, P.mean[a]);
+  // ---- load inputs: slot g <- data[g] (g < NTH) or mean[g - NTH]
+  const float rz = __frcp_rn((float)nzp);
+  for (int e = tid; e < GIN * TS; e += T) {
+    int w = e & (W - 1);
+    int r = e >> lw;            // (g, k) with k fastest
+    int k;
+    int g = fdivmod(r, nzp, rz, k);
+    const float2* src = g < NTH ? P.data[g] : P.mean[g - NTH];
+    R[(k * G + g) * W + w] = (w < nw) ? src[base + (size_t)k * kstride + w] : make_float2(0.f, 0.f);
+  }
   __syncthreads();
-  // forward z transform of the inputs (completes FFTGrid::fftInPlace)
+  // forward z transforms, three slots per call
 #pragma unroll 1
-  for (int l = 0; l < NTH; l++) fft_lines<false>(R1 + l * TS, SC, W, 1, W, P.zp, tw, -1.f);
-#pragma unroll 1
-  for (int a = 0; a < 3; a++) fft_lines<false>(R2 + a * TS, SC, W, 1, W, P.zp, tw, -1.f);
+  for (int g0 = 0; g0 < GIN; g0 += 3) {
+    int ng = min(3, GIN - g0);
+    fft_lines<true>(R + g0 * W, SC, ng * W, 1, G * W, P.zp, tw, -1.f);
+  }
 
   // ---- per-bin posterior (src/avoinversion.cpp:1016-1082)
   unsigned long long n_inv = 0, n_fail = 0;
   for (int b = tid; b < TS; b += T) {
-    int k = b / W, w = b - k * W;
+    int k = b >> lw, w = b & (W - 1);
     if (w >= nw) continue;
     int i = i0 + w;
     size_t gidx = base + (size_t)k * kstride + w;
+    float2* slot = R + k * G * W + w;   // slot g at slot[g * W]
     float S[6], lam;
     if (P.separable) {
       float2 cx = __ldg(P.cxy + (size_t)j * P.cnxp + i);
@@ -285,9 +302,9 @@ __global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ ZPar
     }
     float2 mu[3], d[NTH];
 #pragma unroll
-    for (int a = 0; a < 3; a++) mu[a] = R2[a * TS + b];
+    for (int a = 0; a < 3; a++) mu[a] = slot[(NTH + a) * W];
 #pragma unroll
-    for (int l = 0; l < NTH; l++) d[l] = R1[l * TS + b];
+    for (int l = 0; l < NTH; l++) d[l] = slot[l * W];
     BinOut o;
     bool inv = P.kz.inv[k] != 0;
     bool ok = false;
@@ -301,77 +318,83 @@ __global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ ZPar
       for (int a = 0; a < 3; a++) o.mu[a] = mu[a];
 #pragma unroll
       for (int q = 0; q < 6; q++) o.sp[q] = make_float2(S[q], 0.f);
-#pragma unroll
-      for (int l = 0; l < NTH; l++) d[l] = R1[l * TS + b];
     }
     if (P.keep_resid) {
 #pragma unroll
       for (int l = 0; l < NTH; l++) P.data[l][gidx] = d[l];
     }
 #pragma unroll
-    for (int a = 0; a < 3; a++) R2[a * TS + b] = o.mu[a];
+    for (int q = 0; q < 6; q++) slot[q * W] = o.sp[q];
 #pragma unroll
-    for (int q = 0; q < 6; q++) R1[q * TS + b] = o.sp[q];
+    for (int a = 0; a < 3; a++) slot[(6 + a) * W] = o.mu[a];
   }
   __syncthreads();
 
-  // ---- realisations (src/avoinversion.cpp:1401-1511), spectral sum with the mean
+  // ---- realisations (src/avoinversion.cpp:1401-1511), mean added in the spectral domain
   unsigned long long n_zero = 0;
 #pragma unroll 1
   for (int s = 0; s < P.nsim; s++) {
-#pragma unroll 1
-    for (int a = 0; a < 3; a++) {
-      for (int b = tid; b < TS; b += T) {
-        int k = b / W, w = b - k * W;
-        float2 out = make_float2(0.f, 0.f);
-        if (w < nw) {
-          int i = i0 + w;
-          size_t gidx = base + (size_t)k * kstride + w;
-          float2 C[3][3];
-          C[0][0] = R1[0 * TS + b];
-          C[1][1] = R1[1 * TS + b];
-          C[2][2] = R1[2 * TS + b];
-          float2 c01 = R1[3 * TS + b], c02 = R1[4 * TS + b], c12 = R1[5 * TS + b];
-          C[1][0] = make_float2(c01.x, -c01.y);
-          C[2][0] = make_float2(c02.x, -c02.y);
-          C[2][1] = make_float2(c12.x, -c12.y);
-          C[0][1] = c01; C[0][2] = c02; C[1][2] = c12;
-          float2 z[3];
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            if (c > a) { z[c] = make_float2(0.f, 0.f); continue; }
-            z[c] = P.host_noise ? P.noise[3 * s + c][gidx]
-                                : device_noise(P.seed, 3 * s + c, i, j, k, P.nyp, nzp, P.cnxp, P.nxp_even);
-          }
-          float2 seed = make_float2(0.f, 0.f);
-          if (chol_ref<3>(C)) {
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-              if (c <= a) seed = cadd(seed, cmul(C[a][c], z[c]));
-          } else if (a == 0) {
-            n_zero++;
-          }
-          out = cadd(R2[a * TS + b], seed);
-        }
-        R3[b] = out;
+    for (int b = tid; b < TS; b += T) {
+      int k = b >> lw, w = b & (W - 1);
+      float2* o3 = S3 + k * 3 * W + w;
+      if (w >= nw) {
+        o3[0] = o3[W] = o3[2 * W] = make_float2(0.f, 0.f);
+        continue;
       }
-      __syncthreads();
-      fft_lines<false>(R3, SC, W, 1, W, P.zp, tw, 1.f);
-      store_tile(P.sim[3 * s + a], R3);
-      __syncthreads();
+      int i = i0 + w;
+      size_t gidx = base + (size_t)k * kstride + w;
+      const float2* slot = R + k * G * W + w;
+      float2 C[3][3];
+      C[0][0] = slot[0];
+      C[1][1] = slot[W];
+      C[2][2] = slot[2 * W];
+      float2 c01 = slot[3 * W], c02 = slot[4 * W], c12 = slot[5 * W];
+      C[1][0] = make_float2(c01.x, -c01.y);
+      C[2][0] = make_float2(c02.x, -c02.y);
+      C[2][1] = make_float2(c12.x, -c12.y);
+      C[0][1] = c01; C[0][2] = c02; C[1][2] = c12;
+      float2 z[3];
+      if (P.host_noise) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
+      } else {
+        device_noise3(P.seed, s, i, j, k, P.nyp, nzp, P.cnxp, P.nxp_even, z);
+      }
+      float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      if (chol_ref<3>(C)) {
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int c = 0; c <= a; c++) sd[a] = cadd(sd[a], cmul(C[a][c], z[c]));
+      } else {
+        n_zero++;
+      }
+#pragma unroll
+      for (int a = 0; a < 3; a++) o3[a * W] = cadd(slot[(6 + a) * W], sd[a]);
     }
+    __syncthreads();
+    fft_lines<true>(S3, SC, 3 * W, 1, 3 * W, P.zp, tw, 1.f);
+    for (int e = tid; e < 3 * TS; e += T) {
+      int w = e & (W - 1);
+      int r = e >> lw;
+      int k;
+      int a = fdivmod(r, nzp, rz, k);
+      if (w < nw) P.sim[3 * s + a][base + (size_t)k * kstride + w] = S3[(k * 3 + a) * W + w];
+    }
+    __syncthreads();
   }
 
-  // ---- inverse z transform of posterior covariance and mean
+  // ---- inverse z transform of posterior covariance (slots 0..5) and mean (6..8)
 #pragma unroll 1
-  for (int q = 0; q < 6; q++) {
-    fft_lines<false>(R1 + q * TS, SC, W, 1, W, P.zp, tw, 1.f);
-    store_tile(P.cov[q], R1 + q * TS);
-  }
-#pragma unroll 1
-  for (int a = 0; a < 3; a++) {
-    fft_lines<false>(R2 + a * TS, SC, W, 1, W, P.zp, tw, 1.f);
-    store_tile(P.mean[a], R2 + a * TS);
+  for (int g0 = 0; g0 < 9; g0 += 3)
+    fft_lines<true>(R + g0 * W, SC, 3 * W, 1, G * W, P.zp, tw, 1.f);
+  for (int e = tid; e < 9 * TS; e += T) {
+    int w = e & (W - 1);
+    int r = e >> lw;
+    int k;
+    int g = fdivmod(r, nzp, rz, k);
+    float2* dst = g < 6 ? P.cov[g] : P.mean[g - 6];
+    if (w < nw) dst[base + (size_t)k * kstride + w] = R[(k * G + g) * W + w];
   }
 
   // counters
@@ -396,31 +419,32 @@ __global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ ZPar
 // ------------------------------------------------------------------ launchers
 
 size_t zpass_smem_bytes(int W, int nzp, int nth) {
-  int nr1 = nth > 6 ? nth : 6;
-  return sizeof(float2) * ((size_t)nzp + (size_t)(nr1 + 3 + 2) * W * nzp);
+  int G = nth + 3 > 9 ? nth + 3 : 9;
+  return sizeof(float2) * ((size_t)nzp + (size_t)(G + 6) * W * nzp);
 }
 
 template <int NTH>
-static cudaError_t launch_zpass_t(const ZParams& zp, cudaStream_t st) {
+static cudaError_t launch_zpass_t(const ZParams& zp, int threads, cudaStream_t st) {
   size_t smem = zpass_smem_bytes(zp.W, zp.nzp, zp.nth);
   cudaError_t e = cudaFuncSetAttribute(k_zpass<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(zp.nIT * zp.nyp));
-  k_zpass<NTH><<<grid, kThreads, smem, st>>>(zp);
+  k_zpass<NTH><<<grid, threads, smem, st>>>(zp);
   return cudaGetLastError();
 }
 
-cudaError_t launch_zpass(const ZParams& zp, cudaStream_t st, int* nlaunch) {
+cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch) {
+  if ((zp.W & (zp.W - 1)) || (1 << zp.logW) != zp.W) return cudaErrorInvalidValue;
   if (nlaunch) (*nlaunch)++;
   switch (zp.nth) {
-    case 1: return launch_zpass_t<1>(zp, st);
-    case 2: return launch_zpass_t<2>(zp, st);
-    case 3: return launch_zpass_t<3>(zp, st);
-    case 4: return launch_zpass_t<4>(zp, st);
-    case 5: return launch_zpass_t<5>(zp, st);
-    case 6: return launch_zpass_t<6>(zp, st);
-    case 7: return launch_zpass_t<7>(zp, st);
-    case 8: return launch_zpass_t<8>(zp, st);
+    case 1: return launch_zpass_t<1>(zp, threads, st);
+    case 2: return launch_zpass_t<2>(zp, threads, st);
+    case 3: return launch_zpass_t<3>(zp, threads, st);
+    case 4: return launch_zpass_t<4>(zp, threads, st);
+    case 5: return launch_zpass_t<5>(zp, threads, st);
+    case 6: return launch_zpass_t<6>(zp, threads, st);
+    case 7: return launch_zpass_t<7>(zp, threads, st);
+    case 8: return launch_zpass_t<8>(zp, threads, st);
     default: return cudaErrorInvalidValue;
   }
 }
