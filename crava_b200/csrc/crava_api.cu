@@ -52,23 +52,33 @@ bool smooth(int n) {
   return n == 1;
 }
 
-// Stage radices for a length-n transform: radix 8 while possible, then 4 or 2, then
-// the odd primes.
-bool make_plan(int n, LinePlan& pl) {
+// Stage radices for a length-n transform, fewest stages first: radix 16 while four
+// factors of two remain, then 8, 4 or 2 (a lone 2 pairs with a 3 into radix 6); pairs of
+// threes become radix 9; then 3, 5, 7.
+bool make_plan(int n, LinePlan& pl, bool allow16) {
   if (!smooth(n)) return false;
   pl.n = n;
   pl.nst = 0;
-  int m = n;
-  while (m % 8 == 0) { pl.radix[pl.nst++] = 8; m /= 8; }
-  if (m % 4 == 0) { pl.radix[pl.nst++] = 4; m /= 4; }
-  if (m % 2 == 0) { pl.radix[pl.nst++] = 2; m /= 2; }
-  for (int p : {3, 5, 7})
-    while (m % p == 0) {
-      if (pl.nst >= kMaxStages) return false;
-      pl.radix[pl.nst++] = (int8_t)p;
-      m /= p;
-    }
-  return m == 1;  // n == 1: no stages (identity)
+  int a = 0, b = 0, c = 0, e = 0, m = n;
+  while (m % 2 == 0) { a++; m /= 2; }
+  while (m % 3 == 0) { b++; m /= 3; }
+  while (m % 5 == 0) { c++; m /= 5; }
+  while (m % 7 == 0) { e++; m /= 7; }
+  auto push = [&](int r) { if (pl.nst < kMaxStages) pl.radix[pl.nst++] = (int8_t)r; };
+  while (allow16 && a >= 4) { push(16); a -= 4; }
+  while (a >= 3) { push(8); a -= 3; }
+  if (a == 3) { push(8); a = 0; }
+  if (a == 2) { push(4); a = 0; }
+  if (a == 1) {
+    if (b > 0 && b % 2 == 1) { push(6); b--; }
+    else push(2);
+    a = 0;
+  }
+  while (b >= 2) { push(9); b -= 2; }
+  if (b == 1) push(3);
+  while (c-- > 0) push(5);
+  while (e-- > 0) push(7);
+  return pl.nst < kMaxStages;  // n == 1: no stages (identity)
 }
 
 struct Plan {
@@ -154,7 +164,7 @@ struct crava_job {
 
 namespace {
 
-crava_status get_plan(crava_ctx* ctx, int n, Plan** out);
+crava_status get_plan(crava_ctx* ctx, int n, Plan** out, bool allow16 = false);
 
 // Plans of the x transform: the transform length (nxp/2 for even nxp, nxp for odd) and
 // the length-nxp table used to split the half-length transform.
@@ -164,12 +174,15 @@ crava_status get_xplans(crava_ctx* ctx, int nxp, Plan** px, Plan** pn) {
   return get_plan(ctx, nxp, pn);
 }
 
-crava_status get_plan(crava_ctx* ctx, int n, Plan** out) {
+// Plans are cached per (length, radix-16 allowed): the pencil pass has the register room
+// for radix-16 butterflies, the row and column passes run capped at 64 registers.
+crava_status get_plan(crava_ctx* ctx, int n, Plan** out, bool allow16) {
   std::lock_guard<std::mutex> lk(ctx->mu);
-  auto it = ctx->plans.find(n);
+  const int key = 2 * n + (allow16 ? 1 : 0);
+  auto it = ctx->plans.find(key);
   if (it != ctx->plans.end()) { *out = &it->second; return CRAVA_OK; }
   Plan p;
-  if (!make_plan(n, p.lp)) return fail(CRAVA_ENOTSUP, "transform length " + std::to_string(n) + " is not 2,3,5,7-smooth");
+  if (!make_plan(n, p.lp, allow16)) return fail(CRAVA_ENOTSUP, "transform length " + std::to_string(n) + " is not 2,3,5,7-smooth");
   std::vector<float2> tw(n);
   for (int t = 0; t < n; t++) {
     double ang = 2.0 * M_PI * (double)t / (double)n;
@@ -177,7 +190,7 @@ crava_status get_plan(crava_ctx* ctx, int n, Plan** out) {
   }
   CUDA_TRY(cudaMalloc(&p.tw, sizeof(float2) * n));
   CUDA_TRY(cudaMemcpy(p.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
-  auto res = ctx->plans.emplace(n, p);
+  auto res = ctx->plans.emplace(key, p);
   *out = &res.first->second;
   return CRAVA_OK;
 }
@@ -669,13 +682,14 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   }
   // the fused pencil pass
   Plan* pz;
-  if ((s = get_plan(ctx, d.nzp, &pz))) return s;
+  const char* r16 = getenv("CRAVA_ZPASS_R16");
+  if ((s = get_plan(ctx, d.nzp, &pz, !(r16 && r16[0] == '0')))) return s;
   ZParams zp;
   std::memset(&zp, 0, sizeof(zp));
   zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = job->cnxp;
   zp.nxp_even = (d.nxp % 2) == 0;
-  // pencil tile: W x-bins (power of two); prefer two resident CTAs of 256 threads per
-  // SM, else one CTA of 512 threads (CRAVA_ZPASS_W / CRAVA_ZPASS_T override)
+  // pencil tile: W x-bins (power of two) and T threads; one resident CTA of 512 threads
+  // per SM unless two of 256 fit (CRAVA_ZPASS_W / CRAVA_ZPASS_T override)
   int W = 4, T = 256;
   if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 113 * 1024) T = 512;
   while (W > 1 && zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) W /= 2;

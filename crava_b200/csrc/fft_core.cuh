@@ -159,6 +159,88 @@ struct Dft<8> {
   }
 };
 
+// Composite radix R = A*B in registers (Cooley-Tukey): B-point DFTs over the A
+// decimated subsequences v[r1 + A r2], twiddles e^{sign 2 pi i r1 k2 / R}, A-point DFTs,
+// output X[k2 + B k1].  TW::c(m), TW::s(m): cos and sin of 2 pi m / R.
+template <int A, int B, int R, class TW>
+__device__ __forceinline__ void dft_composite(float2* v, float s) {
+  float2 u[A][B];
+#pragma unroll
+  for (int r1 = 0; r1 < A; r1++) {
+#pragma unroll
+    for (int r2 = 0; r2 < B; r2++) u[r1][r2] = v[r1 + A * r2];
+    Dft<B>::run(u[r1], s);
+#pragma unroll
+    for (int k2 = 1; k2 < B; k2++) {
+      const int m = (r1 * k2) % R;
+      if (r1 > 0) u[r1][k2] = cmul(u[r1][k2], make_float2(TW::c(m), s * TW::s(m)));
+    }
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < B; k2++) {
+    float2 t[A];
+#pragma unroll
+    for (int r1 = 0; r1 < A; r1++) t[r1] = u[r1][k2];
+    Dft<A>::run(t, s);
+#pragma unroll
+    for (int k1 = 0; k1 < A; k1++) v[k2 + B * k1] = t[k1];
+  }
+}
+
+struct Tw6 {
+  static __device__ __forceinline__ float c(int m) {
+    constexpr float t[6] = {1.f, 0.5f, -0.5f, -1.f, -0.5f, 0.5f};
+    return t[m];
+  }
+  static __device__ __forceinline__ float s(int m) {
+    constexpr float t[6] = {0.f, 0.86602540378443865f, 0.86602540378443865f, 0.f, -0.86602540378443865f,
+                            -0.86602540378443865f};
+    return t[m];
+  }
+};
+struct Tw9 {
+  static __device__ __forceinline__ float c(int m) {
+    constexpr float t[9] = {1.f, 0.76604444311897804f, 0.17364817766693035f, -0.5f, -0.93969262078590838f,
+                            -0.93969262078590838f, -0.5f, 0.17364817766693035f, 0.76604444311897804f};
+    return t[m];
+  }
+  static __device__ __forceinline__ float s(int m) {
+    constexpr float t[9] = {0.f, 0.64278760968653933f, 0.98480775301220806f, 0.86602540378443865f,
+                            0.34202014332566873f, -0.34202014332566873f, -0.86602540378443865f,
+                            -0.98480775301220806f, -0.64278760968653933f};
+    return t[m];
+  }
+};
+struct Tw16 {
+  static __device__ __forceinline__ float c(int m) {
+    constexpr float t[16] = {1.f, 0.92387953251128676f, 0.70710678118654752f, 0.38268343236508977f, 0.f,
+                             -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128676f, -1.f,
+                             -0.92387953251128676f, -0.70710678118654752f, -0.38268343236508977f, 0.f,
+                             0.38268343236508977f, 0.70710678118654752f, 0.92387953251128676f};
+    return t[m];
+  }
+  static __device__ __forceinline__ float s(int m) {
+    constexpr float t[16] = {0.f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128676f, 1.f,
+                             0.92387953251128676f, 0.70710678118654752f, 0.38268343236508977f, 0.f,
+                             -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128676f, -1.f,
+                             -0.92387953251128676f, -0.70710678118654752f, -0.38268343236508977f};
+    return t[m];
+  }
+};
+
+template <>
+struct Dft<6> {
+  static __device__ __forceinline__ void run(float2* v, float s) { dft_composite<2, 3, 6, Tw6>(v, s); }
+};
+template <>
+struct Dft<9> {
+  static __device__ __forceinline__ void run(float2* v, float s) { dft_composite<3, 3, 9, Tw9>(v, s); }
+};
+template <>
+struct Dft<16> {
+  static __device__ __forceinline__ void run(float2* v, float s) { dft_composite<4, 4, 16, Tw16>(v, s); }
+};
+
 // q = x / d, r = x % d for 0 <= x < 2^22 and d >= 1, with rcp = 1/d rounded to float:
 // the float quotient is within one of the exact one and a single correction fixes it.
 __device__ __forceinline__ int fdivmod(int x, int d, float rcp, int& r) {
@@ -169,28 +251,45 @@ __device__ __forceinline__ int fdivmod(int x, int d, float rcp, int& r) {
   return q;
 }
 
+// 32-bit shared-memory addressing: stages address their buffers by shared-window byte
+// addresses so that index arithmetic stays 32-bit.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ float2 lds2(uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts2(uint32_t a, float2 v) {
+  asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+
 // Thread-to-line mapping shared by every stage of one fft_lines call in LC mode:
 // thread t starts at line t % nlines, butterfly row t / nlines, and advances by T.
 struct LcMap {
   int f0, s0, df, ds;
 };
 
-// One Stockham stage over nlines lines from `in` to `out` (shared memory).  Element p of
-// line l sits at l*ls + p*psi in `in` and l*ls + p*pso in `out`.  LC (lines contiguous):
-// consecutive threads take consecutive lines of one butterfly index j; otherwise
-// consecutive j of one line.  The (line, j, j mod Ns, j / Ns) of a thread's butterflies
-// are advanced incrementally after a few reciprocal-based divisions per stage.
-template <int R, bool LC>
-__device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out, int nlines,
-                                          int ls, int psi, int pso, int n, int Ns, const LcMap& mp,
-                                          const float2* __restrict__ tw, float sign) {
+// One Stockham stage over nlines lines from `in` to `out` (shared-window byte addresses).
+// Element p of line l sits at in + 8 (l*ls + p*psi) and out + 8 (l*ls + p*pso).  LC
+// (lines contiguous): consecutive threads take consecutive lines of one butterfly index
+// j; otherwise consecutive j of one line.  The (line, j, j mod Ns, j / Ns) of a thread's
+// butterflies advance incrementally after a few reciprocal-based divisions per stage.
+// DIR = -1 forward, +1 inverse.
+template <int R, bool LC, int DIR>
+__device__ __forceinline__ void fft_stage(uint32_t in, uint32_t out, int nlines, int ls, int psi, int pso, int n,
+                                          int Ns, const LcMap& mp, uint32_t tw) {
+  constexpr float sign = (float)DIR;
   const int nb = n / R;
   const int total = nlines * nb;
   const int T = blockDim.x;
   const float rNs = __frcp_rn((float)Ns);
   int tmp;
-  const int nbh = fdivmod(nb, Ns, rNs, tmp);  // nb / Ns (exact)
-  const int twstride = nbh;                   // n / (Ns R)
+  const int nbh = fdivmod(nb, Ns, rNs, tmp);  // nb / Ns (exact) = n / (Ns R), the twiddle stride
+  const uint32_t istep = 8u * (uint32_t)(nb * psi);   // bytes between the R inputs
+  const uint32_t ostep = 8u * (uint32_t)(Ns * pso);   // bytes between the R outputs
+  const uint32_t tstep = 8u * (uint32_t)nbh;          // twiddle bytes per unit of r*k
   int idx = threadIdx.x;
   int line, j, df, ds;
   if (LC) {
@@ -204,29 +303,28 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
   }
   int k;
   int jh = fdivmod(j, Ns, rNs, k);
-  // j advances by dj per iteration, plus a carry from the fast index when LC; when not
-  // LC, j wraps at nb (a multiple of Ns) into the next line
   const int dj = LC ? ds : df;
   int dk;
   const int djh = fdivmod(dj, Ns, rNs, dk);
+  const int RNs = R * Ns;
   for (; idx < total; idx += T) {
-    const float2* src = in + line * ls + j * psi;
+    uint32_t a = in + 8u * (uint32_t)(line * ls + j * psi);
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = src[r * nb * psi];
+    for (int r = 0; r < R; r++) v[r] = lds2(a + r * istep);
     if (Ns > 1) {
-      const int tk = k * twstride;
+      const uint32_t kt = (uint32_t)k * tstep;  // byte offset of e^{-2 pi i k/(Ns R)}
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        float2 w = tw[r * tk];
-        w.y *= -sign;  // table holds e^{-2 pi i t/n}; sign=+1 conjugates
+        float2 w = lds2(tw + r * kt);
+        if (DIR > 0) w.y = -w.y;  // table holds e^{-2 pi i t/n}
         v[r] = cmul(v[r], w);
       }
     }
     Dft<R>::run(v, sign);
-    float2* dst = out + line * ls + (jh * Ns * R + k) * pso;
+    uint32_t o = out + 8u * (uint32_t)(line * ls + (jh * RNs + k) * pso);
 #pragma unroll
-    for (int r = 0; r < R; r++) dst[r * Ns * pso] = v[r];
+    for (int r = 0; r < R; r++) sts2(o + r * ostep, v[r]);
     if (LC) {
       line += df;
       int carry = line >= nlines;
@@ -249,19 +347,22 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
 
 // Full transform of nlines lines of length pl.n.  The lines start in `buf` (point stride
 // ps) and end there; `scratch` (dense, point stride nlines when LC, line stride n
-// otherwise) holds the odd stages.  sign = -1 forward, +1 inverse, unnormalised both
-// ways like FFTW.  tw: the length-n table, usually in shared memory.  The caller
+// otherwise) holds the odd stages.  DIR = -1 forward, +1 inverse, unnormalised both ways
+// like FFTW.  tw: the length-n table of e^{-2 pi i t/n} in shared memory.  The caller
 // synchronises before the call; the function returns after a barrier.  Stages run
-// grouped by radix in the plan's fixed order 8..8, 4, 2, 3..3, 5..5, 7..7.
-template <bool LC>
+// grouped by radix in the fixed order 16.., 8.., 4, 2, 9.., 3.., 6.., 5.., 7.. (any order
+// of the radices gives the same transform).  R16 = false compiles without the radix-16
+// stage (for kernels capped at 64 registers; their plans never contain it).
+template <bool LC, int DIR, bool R16 = true>
 __device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlines, int ls, int ps,
-                                          const LinePlan& pl, const float2* __restrict__ tw, float sign) {
+                                          const LinePlan& pl, const float2* tw) {
   int Ns = 1;
   const int n = pl.n;
-  int c8 = 0, c4 = 0, c2 = 0, c3 = 0, c5 = 0, c7 = 0;
+  int c16 = 0, c8 = 0, c4 = 0, c2 = 0, c9 = 0, c3 = 0, c6 = 0, c5 = 0, c7 = 0;
   for (int s = 0; s < pl.nst; s++) {
     int R = pl.radix[s];
-    c8 += R == 8; c4 += R == 4; c2 += R == 2; c3 += R == 3; c5 += R == 5; c7 += R == 7;
+    c16 += R == 16; c8 += R == 8; c4 += R == 4; c2 += R == 2; c9 += R == 9; c3 += R == 3;
+    c6 += R == 6; c5 += R == 5; c7 += R == 7;
   }
   LcMap mp{0, 0, 0, 0};
   if (LC) {
@@ -269,27 +370,32 @@ __device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlin
     mp.s0 = fdivmod(threadIdx.x, nlines, rl, mp.f0);
     mp.ds = fdivmod(blockDim.x, nlines, rl, mp.df);
   }
+  const uint32_t b = smem_addr(buf), sc = smem_addr(scratch), t = smem_addr(tw);
   // scratch layout: LC -> element (l, p) at l + p*nlines; else at l*n + p
   const int sps = LC ? nlines : 1;
+  const int lsx = LC ? 1 : ls;
   bool in_buf = true;
-#define CRAVA_STAGE(RR)                                                                             \
-  {                                                                                                 \
-    if (in_buf) {                                                                                   \
-      if (LC) fft_stage<RR, LC>(buf, scratch, nlines, 1, ps, sps, n, Ns, mp, tw, sign);             \
-      else fft_stage<RR, LC>(buf, scratch, nlines, ls, ps, sps, n, Ns, mp, tw, sign);               \
-    } else {                                                                                        \
-      if (LC) fft_stage<RR, LC>(scratch, buf, nlines, 1, sps, ps, n, Ns, mp, tw, sign);             \
-      else fft_stage<RR, LC>(scratch, buf, nlines, ls, sps, ps, n, Ns, mp, tw, sign);               \
-    }                                                                                               \
-    Ns *= RR;                                                                                       \
-    in_buf = !in_buf;                                                                               \
+#define CRAVA_STAGE(RR)                                                                       \
+  {                                                                                           \
+    if (in_buf) fft_stage<RR, LC, DIR>(b, sc, nlines, lsx, ps, sps, n, Ns, mp, t);            \
+    else fft_stage<RR, LC, DIR>(sc, b, nlines, lsx, sps, ps, n, Ns, mp, t);                   \
+    Ns *= RR;                                                                                 \
+    in_buf = !in_buf;                                                                         \
+  }
+  if (R16) {  // plans built without radix 16 leave c16 == 0
+#pragma unroll 1
+    for (int q = 0; q < c16; q++) CRAVA_STAGE(16)
   }
 #pragma unroll 1
   for (int q = 0; q < c8; q++) CRAVA_STAGE(8)
   if (c4) CRAVA_STAGE(4)
   if (c2) CRAVA_STAGE(2)
 #pragma unroll 1
+  for (int q = 0; q < c9; q++) CRAVA_STAGE(9)
+#pragma unroll 1
   for (int q = 0; q < c3; q++) CRAVA_STAGE(3)
+#pragma unroll 1
+  for (int q = 0; q < c6; q++) CRAVA_STAGE(6)
 #pragma unroll 1
   for (int q = 0; q < c5; q++) CRAVA_STAGE(5)
 #pragma unroll 1
@@ -301,14 +407,14 @@ __device__ __forceinline__ void fft_lines(float2* buf, float2* scratch, int nlin
       for (int e = threadIdx.x; e < nlines * n; e += blockDim.x) {
         int l;
         int p = fdivmod(e, nlines, rl, l);
-        buf[l + p * ps] = scratch[e];
+        sts2(b + 8u * (uint32_t)(l + p * ps), lds2(sc + 8u * (uint32_t)e));
       }
     } else {
       const float rn = __frcp_rn((float)n);
       for (int e = threadIdx.x; e < nlines * n; e += blockDim.x) {
         int p;
         int l = fdivmod(e, n, rn, p);
-        buf[l * ls + p * ps] = scratch[e];
+        sts2(b + 8u * (uint32_t)(l * ls + p * ps), lds2(sc + 8u * (uint32_t)e));
       }
     }
     __syncthreads();

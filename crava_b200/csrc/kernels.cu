@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "fft_core.cuh"
 #include "kernels.cuh"
@@ -31,7 +32,7 @@ constexpr int kThreads = 256;
 // (a real-output inverse has no slot for Im X[0], Im X[h]), then a length-h inverse
 // FFT gives nxp * (x[2m] + i x[2m+1]).  Odd nxp uses a full-length complex transform.
 
-__global__ void __launch_bounds__(512) k_x_r2c(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
+__global__ void __launch_bounds__(512, 2) k_x_r2c(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
                                                 const __grid_constant__ LinePlan pl, const float2* __restrict__ twg,
                                                 const float2* __restrict__ twn) {
   extern __shared__ float2 sm[];
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(512) k_x_r2c(const __grid_constant__ GridSet g
     }
   }
   __syncthreads();
-  fft_lines<false>(buf, scr, nr, n, 1, pl, tw, -1.f);
+  fft_lines<false, -1, false>(buf, scr, nr, n, 1, pl, tw);
   float2* dst = reinterpret_cast<float2*>(g) + (size_t)row0 * cnxp;
   if (even) {
     const int h = n, np = h / 2 + 1;  // pairs (k, h-k), k = 0..h/2
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(512) k_x_r2c(const __grid_constant__ GridSet g
   }
 }
 
-__global__ void __launch_bounds__(512) k_x_c2r(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
+__global__ void __launch_bounds__(512, 2) k_x_c2r(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
                                                 const __grid_constant__ LinePlan pl, const float2* __restrict__ twg,
                                                 const float2* __restrict__ twn) {
   extern __shared__ float2 sm[];
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(512) k_x_c2r(const __grid_constant__ GridSet g
     }
   }
   __syncthreads();
-  fft_lines<false>(buf, scr, nr, n, 1, pl, tw, 1.f);
+  fft_lines<false, 1, false>(buf, scr, nr, n, 1, pl, tw);
   if (even) {
     float2* dst = reinterpret_cast<float2*>(g) + (size_t)row0 * cnxp;
     const float rc = __frcp_rn((float)cnxp);
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(512) k_x_c2r(const __grid_constant__ GridSet g
 
 // ------------------------------------------------------------------ strided line transform
 
-__global__ void __launch_bounds__(512) k_line_fft(const __grid_constant__ GridSet gs, int ni, int n, size_t pstride, int no,
+__global__ void __launch_bounds__(512, 2) k_line_fft(const __grid_constant__ GridSet gs, int ni, int n, size_t pstride, int no,
                                                    size_t ostride, int W, int nIT, const __grid_constant__ LinePlan pl,
                                                    const float2* __restrict__ twg, float sign) {
   extern __shared__ float2 sm[];
@@ -209,7 +210,8 @@ __global__ void __launch_bounds__(512) k_line_fft(const __grid_constant__ GridSe
     buf[e] = (w < nw) ? g[(size_t)p * pstride + w] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_lines<true>(buf, scr, W, 1, W, pl, tw, sign);
+  if (sign < 0.f) fft_lines<true, -1, false>(buf, scr, W, 1, W, pl, tw);
+  else fft_lines<true, 1, false>(buf, scr, W, 1, W, pl, tw);
   for (int e = tid; e < n * W; e += T) {
     int p = e >> lw, w = e & (W - 1);
     if (w < nw) g[(size_t)p * pstride + w] = buf[e];
@@ -227,8 +229,11 @@ static cudaError_t launch_x(bool fwd, const GridSet& gs, int nxp, int rows, cons
                             const float2* twn, cudaStream_t st, int* nlaunch) {
   const bool even = (nxp & 1) == 0;
   const int n = even ? nxp / 2 : nxp;
+  // rows per CTA and threads: about 16 points per thread (CRAVA_X_PPT overrides)
+  int ppt = 16;
+  if (const char* ev = getenv("CRAVA_X_PPT")) ppt = std::max(1, atoi(ev));
   int rpc = std::max(1, std::min(64, 2048 / n));
-  int T = std::min(512, round_threads(rpc * n / 8));
+  int T = std::min(512, round_threads((rpc * n + ppt - 1) / ppt));
   size_t smem = sizeof(float2) * (size_t)(n + (even ? nxp / 2 : 0) + 2 * rpc * n);
   dim3 grid((rows + rpc - 1) / rpc, gs.n);
   const void* fn = fwd ? (const void*)k_x_r2c : (const void*)k_x_c2r;
@@ -255,9 +260,12 @@ cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& p
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch) {
   int W = 16;
+  if (const char* ev = getenv("CRAVA_LINE_W")) W = std::max(1, atoi(ev));
   while (W > 1 && W * n > 8192) W /= 2;
   while (W > 1 && W / 2 >= ni) W /= 2;  // power of two, not wider than needed
-  int T = std::min(512, round_threads(W * n / 8));
+  int tdiv = 16;
+  if (const char* ev = getenv("CRAVA_LINE_TDIV")) tdiv = std::max(1, atoi(ev));
+  int T = std::min(512, round_threads((W * n + tdiv - 1) / tdiv));
   int nIT = (ni + W - 1) / W;
   size_t smem = sizeof(float2) * (size_t)(n + 2 * W * n);
   dim3 grid((unsigned)(nIT * no), gs.n);

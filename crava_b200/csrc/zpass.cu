@@ -17,10 +17,11 @@ namespace crava {
 
 // ------------------------------------------------------------------ noise (product mode)
 
-// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+// Philox-4x32 (Salmon, Moraes, Dror, Shaw, SC'11) with 7 rounds, which the authors
+// report passes TestU01 BigCrush.
+__device__ __forceinline__ uint4 philox4x32_7(uint4 c, uint2 k) {
 #pragma unroll
-  for (int r = 0; r < 10; r++) {
+  for (int r = 0; r < 7; r++) {
     uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
     uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
     c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
@@ -60,8 +61,8 @@ __device__ __forceinline__ void device_noise3(uint64_t seed, int s, int i, int j
   }
   uint64_t bin = ((uint64_t)kk * nyp + jj) * cnxp + i;
   uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-  uint4 r0 = philox4x32_10(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 0u), key);
-  uint4 r1 = philox4x32_10(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 1u), key);
+  uint4 r0 = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 0u), key);
+  uint4 r1 = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 1u), key);
   float n[6];
   box_muller(r0.x, r0.y, n[0], n[1]);
   box_muller(r0.z, r0.w, n[2], n[3]);
@@ -231,7 +232,7 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
 //   S3  [nzp][3][W]       one realisation's three output spectra
 //   SC  [3 * W * nzp]     transform scratch for groups of up to three slots
 // Element (slot g, kz k, x-offset w) of R is R[(k * G + g) * W + w].
-__device__ __forceinline__ int zslots(int nth) { return nth + 3 > 9 ? nth + 3 : 9; }
+
 
 template <int NTH>
 __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P) {
@@ -256,25 +257,24 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   if (tid < 3) cnt[tid] = 0;
   for (int t = tid; t < nzp; t += T) tw[t] = P.twz[t];
   // ---- load inputs: slot g <- data[g] (g < NTH) or mean[g - NTH]
-  const float rz = __frcp_rn((float)nzp);
-  for (int e = tid; e < GIN * TS; e += T) {
-    int w = e & (W - 1);
-    int r = e >> lw;            // (g, k) with k fastest
-    int k;
-    int g = fdivmod(r, nzp, rz, k);
-    const float2* src = g < NTH ? P.data[g] : P.mean[g - NTH];
-    R[(k * G + g) * W + w] = (w < nw) ? src[base + (size_t)k * kstride + w] : make_float2(0.f, 0.f);
+#pragma unroll 1
+  for (int g = 0; g < GIN; g++) {
+    const float2* src = (g < NTH ? P.data[g] : P.mean[g - NTH]) + base;
+    for (int e = tid; e < TS; e += T) {
+      int w = e & (W - 1), k = e >> lw;
+      R[(k * G + g) * W + w] = (w < nw) ? src[(size_t)k * kstride + w] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   // forward z transforms, three slots per call
 #pragma unroll 1
   for (int g0 = 0; g0 < GIN; g0 += 3) {
     int ng = min(3, GIN - g0);
-    fft_lines<true>(R + g0 * W, SC, ng * W, 1, G * W, P.zp, tw, -1.f);
+    fft_lines<true, -1>(R + g0 * W, SC, ng * W, 1, G * W, P.zp, tw);
   }
 
   // ---- per-bin posterior (src/avoinversion.cpp:1016-1082)
-  unsigned long long n_inv = 0, n_fail = 0;
+  unsigned long long n_inv = 0, n_fail = 0, n_zero_bins = 0;
   for (int b = tid; b < TS; b += T) {
     int k = b >> lw, w = b & (W - 1);
     if (w >= nw) continue;
@@ -323,15 +323,34 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
 #pragma unroll
       for (int l = 0; l < NTH; l++) P.data[l][gidx] = d[l];
     }
+    // Factor S_post once for all realisations (lib_matrCholCpx(3), simulate :1425-1443).
+    // Slots 0..5 then hold L (diagonal real, slot 0 imaginary part set to -1 as the mark)
+    // or, where the factorisation fails, S_post itself; the covariance output is rebuilt
+    // as L L^H before its inverse transform.
+    float2 C[3][3];
+    C[0][0] = o.sp[0]; C[1][1] = o.sp[1]; C[2][2] = o.sp[2];
+    C[0][1] = o.sp[3]; C[0][2] = o.sp[4]; C[1][2] = o.sp[5];
+    C[1][0] = make_float2(o.sp[3].x, -o.sp[3].y);
+    C[2][0] = make_float2(o.sp[4].x, -o.sp[4].y);
+    C[2][1] = make_float2(o.sp[5].x, -o.sp[5].y);
+    if (P.nsim > 0 && chol_ref<3>(C)) {
+      slot[0] = make_float2(C[0][0].x, -1.f);
+      slot[W] = make_float2(C[1][1].x, 0.f);
+      slot[2 * W] = make_float2(C[2][2].x, 0.f);
+      slot[3 * W] = C[1][0];
+      slot[4 * W] = C[2][0];
+      slot[5 * W] = C[2][1];
+    } else {
+      if (P.nsim > 0) n_zero_bins++;
 #pragma unroll
-    for (int q = 0; q < 6; q++) slot[q * W] = o.sp[q];
+      for (int q = 0; q < 6; q++) slot[q * W] = o.sp[q];
+    }
 #pragma unroll
     for (int a = 0; a < 3; a++) slot[(6 + a) * W] = o.mu[a];
   }
   __syncthreads();
 
   // ---- realisations (src/avoinversion.cpp:1401-1511), mean added in the spectral domain
-  unsigned long long n_zero = 0;
 #pragma unroll 1
   for (int s = 0; s < P.nsim; s++) {
     for (int b = tid; b < TS; b += T) {
@@ -344,42 +363,53 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
       int i = i0 + w;
       size_t gidx = base + (size_t)k * kstride + w;
       const float2* slot = R + k * G * W + w;
-      float2 C[3][3];
-      C[0][0] = slot[0];
-      C[1][1] = slot[W];
-      C[2][2] = slot[2 * W];
-      float2 c01 = slot[3 * W], c02 = slot[4 * W], c12 = slot[5 * W];
-      C[1][0] = make_float2(c01.x, -c01.y);
-      C[2][0] = make_float2(c02.x, -c02.y);
-      C[2][1] = make_float2(c12.x, -c12.y);
-      C[0][1] = c01; C[0][2] = c02; C[1][2] = c12;
-      float2 z[3];
-      if (P.host_noise) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
-      } else {
-        device_noise3(P.seed, s, i, j, k, P.nyp, nzp, P.cnxp, P.nxp_even, z);
-      }
       float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      if (chol_ref<3>(C)) {
+      const float2 l0 = slot[0];
+      if (l0.y == -1.f) {
+        float2 z[3];
+        if (P.host_noise) {
 #pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-          for (int c = 0; c <= a; c++) sd[a] = cadd(sd[a], cmul(C[a][c], z[c]));
-      } else {
-        n_zero++;
+          for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
+        } else {
+          device_noise3(P.seed, s, i, j, k, P.nyp, nzp, P.cnxp, P.nxp_even, z);
+        }
+        const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
+        sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
+        sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
+        sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
       }
 #pragma unroll
       for (int a = 0; a < 3; a++) o3[a * W] = cadd(slot[(6 + a) * W], sd[a]);
     }
     __syncthreads();
-    fft_lines<true>(S3, SC, 3 * W, 1, 3 * W, P.zp, tw, 1.f);
-    for (int e = tid; e < 3 * TS; e += T) {
-      int w = e & (W - 1);
-      int r = e >> lw;
-      int k;
-      int a = fdivmod(r, nzp, rz, k);
-      if (w < nw) P.sim[3 * s + a][base + (size_t)k * kstride + w] = S3[(k * 3 + a) * W + w];
+    fft_lines<true, 1>(S3, SC, 3 * W, 1, 3 * W, P.zp, tw);
+#pragma unroll 1
+    for (int a = 0; a < 3; a++) {
+      float2* dst = P.sim[3 * s + a] + base;
+      for (int e = tid; e < TS; e += T) {
+        int w = e & (W - 1), k = e >> lw;
+        if (w < nw) dst[(size_t)k * kstride + w] = S3[(k * 3 + a) * W + w];
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- rebuild S_post = L L^H where slots 0..5 hold the factor
+  if (P.nsim > 0) {
+    for (int b = tid; b < TS; b += T) {
+      int k = b >> lw, w = b & (W - 1);
+      float2* slot = R + k * G * W + w;
+      const float2 l0 = slot[0];
+      if (l0.y != -1.f) continue;
+      const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
+      // S_ab = sum_c L_ac conj(L_bc)
+      slot[0] = make_float2(l0.x * l0.x, 0.f);
+      slot[W] = make_float2(l10.x * l10.x + l10.y * l10.y + l1.x * l1.x, 0.f);
+      slot[2 * W] = make_float2(l20.x * l20.x + l20.y * l20.y + l21.x * l21.x + l21.y * l21.y + l2.x * l2.x, 0.f);
+      slot[3 * W] = make_float2(l0.x * l10.x, -l0.x * l10.y);
+      slot[4 * W] = make_float2(l0.x * l20.x, -l0.x * l20.y);
+      slot[5 * W] = make_float2(l10.x * l20.x + l10.y * l20.y + l1.x * l21.x,
+                                l10.y * l20.x - l10.x * l20.y - l1.x * l21.y);
     }
     __syncthreads();
   }
@@ -387,17 +417,18 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   // ---- inverse z transform of posterior covariance (slots 0..5) and mean (6..8)
 #pragma unroll 1
   for (int g0 = 0; g0 < 9; g0 += 3)
-    fft_lines<true>(R + g0 * W, SC, 3 * W, 1, G * W, P.zp, tw, 1.f);
-  for (int e = tid; e < 9 * TS; e += T) {
-    int w = e & (W - 1);
-    int r = e >> lw;
-    int k;
-    int g = fdivmod(r, nzp, rz, k);
-    float2* dst = g < 6 ? P.cov[g] : P.mean[g - 6];
-    if (w < nw) dst[base + (size_t)k * kstride + w] = R[(k * G + g) * W + w];
+    fft_lines<true, 1>(R + g0 * W, SC, 3 * W, 1, G * W, P.zp, tw);
+#pragma unroll 1
+  for (int g = 0; g < 9; g++) {
+    float2* dst = (g < 6 ? P.cov[g] : P.mean[g - 6]) + base;
+    for (int e = tid; e < TS; e += T) {
+      int w = e & (W - 1), k = e >> lw;
+      if (w < nw) dst[(size_t)k * kstride + w] = R[(k * G + g) * W + w];
+    }
   }
 
   // counters
+  unsigned long long n_zero = n_zero_bins * (unsigned long long)P.nsim;
   for (int off = 16; off > 0; off >>= 1) {
     n_inv += __shfl_down_sync(0xffffffffu, n_inv, off);
     n_fail += __shfl_down_sync(0xffffffffu, n_fail, off);
