@@ -787,3 +787,210 @@ crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int n
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Inversion without device allocation (crava_invert_noalloc).
+//
+// Some callers cannot call cudaMalloc: code running inside a CUDA stream capture whose
+// allocations are forbidden, plugins hosted by an application that owns the device memory
+// pool and forbids other allocators, or hot loops where an allocation's implicit device
+// synchronisation is not acceptable.  For them this entry point runs one small block with
+// every intermediate in g_noalloc_scratch, a fixed array in the library's own device image:
+// each GPU that loads the library holds its CRAVA_NOALLOC_SCRATCH_BYTES until the process
+// exits, every call reuses it (so calls whose work overlaps on the GPU race), and blocks
+// whose intermediates do not fit are rejected with CRAVA_ENOTSUP.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CRAVA_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array on the current device, looked up once per device:
+// in host code g_noalloc_scratch names a host-side stand-in, not device memory.
+crava_status noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= 64) return fail(CRAVA_ENOTSUP, "device index above 63");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return CRAVA_OK;
+}
+
+// Host copy of one transform plan: stage radices and the twiddle table.
+struct HostPlan {
+  LinePlan lp;
+  std::vector<float2> tw;
+};
+
+bool host_plan(int n, bool allow16, HostPlan& hp) {
+  if (!make_plan(n, hp.lp, allow16)) return false;
+  hp.tw.resize(n);
+  for (int t = 0; t < n; t++) {
+    double ang = 2.0 * M_PI * (double)t / (double)n;
+    hp.tw[t] = make_float2((float)std::cos(ang), (float)(-std::sin(ang)));
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const float* const* d_in,
+                                             float* const* d_out, void* stream) {
+  crava_status s = validate(desc);
+  if (s) return s;
+  if (!d_in || !d_out) return fail(CRAVA_EINVAL, "null grid pointer array");
+  const crava_job_desc& d = *desc;
+  if (d.prior_mode != CRAVA_PRIOR_SEPARABLE)
+    return fail(CRAVA_ENOTSUP, "crava_invert_noalloc takes the separable prior only");
+  if (d.flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL))
+    return fail(CRAVA_ENOTSUP, "crava_invert_noalloc supports neither host noise nor residual output");
+  const int nin = d.ntheta + 3, nout = 9 + 3 * d.nsim;
+  for (int q = 0; q < nin; q++)
+    if (!d_in[q]) return fail(CRAVA_EINVAL, "null input grid");
+  for (int q = 0; q < nout; q++)
+    if (!d_out[q]) return fail(CRAVA_EINVAL, "null output grid");
+  cudaStream_t st = (cudaStream_t)stream;
+  int device = 0;
+  CUDA_TRY(cudaGetDevice(&device));
+
+  const int cnxp = d.nxp / 2 + 1, rnxp = 2 * cnxp;
+  const size_t rsize = (size_t)rnxp * d.nyp * d.nzp;
+  const size_t N = (size_t)d.nxp * d.nyp * d.nzp;
+  const bool even = d.nxp % 2 == 0;
+  HostPlan px, pn, py, pz;
+  if (!host_plan(even ? d.nxp / 2 : d.nxp, false, px) || !host_plan(d.nxp, false, pn) ||
+      !host_plan(d.nyp, false, py) || !host_plan(d.nzp, true, pz))
+    return fail(CRAVA_ENOTSUP, "transform length is not 2,3,5,7-smooth");
+
+  // scratch layout: data work grids, twiddle tables, per-kz tables, lateral and temporal
+  // prior factors, counters
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align256(bytes); return o; };
+  const size_t o_data = take(sizeof(float) * rsize * d.ntheta);
+  const size_t o_twx = take(sizeof(float2) * px.tw.size());
+  const size_t o_twn = take(sizeof(float2) * pn.tw.size());
+  const size_t o_twy = take(sizeof(float2) * py.tw.size());
+  const size_t o_twz = take(sizeof(float2) * pz.tw.size());
+  const size_t o_kw = take(sizeof(float2) * d.nzp * d.ntheta);
+  const size_t o_e1 = take(sizeof(float2) * d.nzp * d.ntheta);
+  const size_t o_e2 = take(sizeof(float2) * d.nzp * d.ntheta);
+  const size_t o_inv = take(d.nzp);
+  const size_t o_cxy = take(sizeof(float) * rnxp * d.nyp);
+  const size_t o_ct = take(sizeof(float2) * d.nzp);
+  const size_t o_cnt = take(3 * sizeof(unsigned long long));
+  if (off > (size_t)CRAVA_NOALLOC_SCRATCH_BYTES)
+    return fail(CRAVA_ENOTSUP, "block needs " + std::to_string(off) + " bytes of scratch; crava_invert_noalloc has " +
+                                   std::to_string((size_t)CRAVA_NOALLOC_SCRATCH_BYTES));
+  unsigned char* base = nullptr;
+  if ((s = noalloc_scratch(device, &base))) return s;
+
+  // host-built tables, copied into the scratch on the stream
+  std::vector<float2> kw, e1, e2;
+  std::vector<uint8_t> inv;
+  build_kz_tables(d, kw, e1, e2, inv);
+  std::vector<double> c(d.circ_corr_t, d.circ_corr_t + d.nzp);
+  std::vector<cd> C = dft(c);
+  std::vector<float2> ct(d.nzp);
+  for (int k = 0; k < d.nzp; k++) ct[k] = make_float2((float)C[k].real(), (float)C[k].imag());
+  std::vector<float> gxy((size_t)rnxp * d.nyp, 0.f);
+  for (int jj = 0; jj < d.nyp; jj++)
+    for (int ii = 0; ii < d.nxp; ii++) gxy[(size_t)jj * rnxp + ii] = d.corr_xy[(size_t)jj * d.nxp + ii];
+  auto put = [&](size_t o, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, st);
+  };
+  CUDA_TRY(put(o_twx, px.tw.data(), sizeof(float2) * px.tw.size()));
+  CUDA_TRY(put(o_twn, pn.tw.data(), sizeof(float2) * pn.tw.size()));
+  CUDA_TRY(put(o_twy, py.tw.data(), sizeof(float2) * py.tw.size()));
+  CUDA_TRY(put(o_twz, pz.tw.data(), sizeof(float2) * pz.tw.size()));
+  CUDA_TRY(put(o_kw, kw.data(), sizeof(float2) * kw.size()));
+  CUDA_TRY(put(o_e1, e1.data(), sizeof(float2) * e1.size()));
+  CUDA_TRY(put(o_e2, e2.data(), sizeof(float2) * e2.size()));
+  CUDA_TRY(put(o_inv, inv.data(), inv.size()));
+  CUDA_TRY(put(o_ct, ct.data(), sizeof(float2) * ct.size()));
+  CUDA_TRY(put(o_cxy, gxy.data(), sizeof(float) * gxy.size()));
+  CUDA_TRY(cudaMemsetAsync(base + o_cnt, 0, 3 * sizeof(unsigned long long), st));
+  const float2* twx = (const float2*)(base + o_twx);
+  const float2* twn = (const float2*)(base + o_twn);
+  const float2* twy = (const float2*)(base + o_twy);
+  const float2* twz = (const float2*)(base + o_twz);
+  float* data = (float*)(base + o_data);
+
+  // lateral prior factor: 2D transform of corrXY in place
+  {
+    GridSet gs;
+    gs.n = 1;
+    gs.p[0] = (float*)(base + o_cxy);
+    gs.src[0] = gs.p[0];
+    gs.scale[0] = 1.0f;
+    CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px.lp, twx, twn, st, nullptr));
+    CUDA_TRY(launch_line_fft(gs, cnxp, d.nyp, (size_t)cnxp, 1, 0, py.lp, twy, -1.f, st, nullptr));
+  }
+  // forward x, y transforms: data into scratch, prior mean into the posterior-mean outputs
+  {
+    GridSet gs;
+    gs.n = nin;
+    const float fs = fwd_scale(N);
+    for (int l = 0; l < d.ntheta; l++) { gs.src[l] = d_in[l]; gs.p[l] = data + rsize * l; gs.scale[l] = fs; }
+    for (int a = 0; a < 3; a++) { gs.src[d.ntheta + a] = d_in[d.ntheta + a]; gs.p[d.ntheta + a] = d_out[a]; gs.scale[d.ntheta + a] = fs; }
+    CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp * d.nzp, px.lp, twx, twn, st, nullptr));
+    CUDA_TRY(launch_line_fft(gs, cnxp, d.nyp, (size_t)cnxp, d.nzp, (size_t)cnxp * d.nyp, py.lp, twy, -1.f, st, nullptr));
+  }
+  // pencil pass
+  ZParams zp;
+  std::memset(&zp, 0, sizeof(zp));
+  zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = cnxp;
+  zp.nxp_even = even;
+  int W = 4, T = 256;
+  if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 113 * 1024) T = 512;
+  while (W > 1 && zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) W /= 2;
+  if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
+  zp.W = W;
+  zp.logW = 0;
+  while ((1 << zp.logW) < W) zp.logW++;
+  zp.nIT = (cnxp + W - 1) / W;
+  zp.nth = d.ntheta;
+  zp.nsim = d.nsim;
+  zp.separable = 1;
+  for (int l = 0; l < d.ntheta; l++) zp.data[l] = (float2*)(data + rsize * l);
+  for (int a = 0; a < 3; a++) zp.mean[a] = (float2*)d_out[a];
+  for (int q = 0; q < 6; q++) zp.cov[q] = (float2*)d_out[3 + q];
+  for (int q = 0; q < 3 * d.nsim; q++) zp.sim[q] = (float2*)d_out[9 + q];
+  zp.cxy = (const float2*)(base + o_cxy);
+  zp.ct = (const float2*)(base + o_ct);
+  const int qa[6] = {0, 1, 2, 0, 0, 1}, qb[6] = {0, 1, 2, 1, 2, 2};
+  for (int q = 0; q < 6; q++) zp.pv[q] = static_cast<float>(d.prior_var0[qa[q] * 3 + qb[q]]);
+  for (int l = 0; l < d.ntheta; l++) {
+    for (int c3 = 0; c3 < 3; c3++) zp.A[l][c3] = static_cast<float>(d.A[l * 3 + c3]);
+    for (int m = 0; m < d.ntheta; m++) zp.ec[l][m] = float(0.5 * (1.0 - d.wnc) * d.err_theta_cov[l * d.ntheta + m]);
+    zp.ed[l] = float(d.wnc * d.err_theta_cov[l * d.ntheta + l]);
+  }
+  zp.kz.kw = (const float2*)(base + o_kw);
+  zp.kz.e1 = (const float2*)(base + o_e1);
+  zp.kz.e2 = (const float2*)(base + o_e2);
+  zp.kz.inv = (const uint8_t*)(base + o_inv);
+  zp.zp = pz.lp;
+  zp.twz = twz;
+  zp.seed = d.seed;
+  zp.counters = (unsigned long long*)(base + o_cnt);
+  CUDA_TRY(launch_zpass(zp, T, st, nullptr));
+  // inverse y, x transforms of the outputs in place
+  {
+    GridSet gs;
+    gs.n = nout;
+    const float ps = inv_scale(N, false), cs = inv_scale(N, true);
+    for (int q = 0; q < nout; q++) {
+      gs.p[q] = d_out[q];
+      gs.src[q] = d_out[q];
+      gs.scale[q] = (q >= 3 && q < 9) ? cs : ps;
+    }
+    CUDA_TRY(launch_line_fft(gs, cnxp, d.nyp, (size_t)cnxp, d.nzp, (size_t)cnxp * d.nyp, py.lp, twy, 1.f, st, nullptr));
+    CUDA_TRY(launch_x_c2r(gs, d.nxp, d.nyp * d.nzp, px.lp, twx, twn, st, nullptr));
+  }
+  return CRAVA_OK;
+}

@@ -158,6 +158,24 @@ long long crava_ctx_kernel_launches(crava_ctx* ctx);
 crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable);
 crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset);
 
+/* One block, end to end, with no device allocation (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory: code inside a CUDA stream capture that
+ * forbids allocation, plugins in applications that own the device memory pool, loops that
+ * cannot afford an allocation's implicit synchronisation.  All intermediates live in a
+ * fixed array of CRAVA_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that
+ * loads the library keeps until the process exits.  The caller passes device grids:
+ *   d_in  : ntheta data grids, then the 3 prior mean grids (real, read only);
+ *   d_out : 3 posterior mean, 6 posterior covariance, 3*nsim realisations (real).
+ * Separable prior only; no host noise, no residual output.  Blocks whose intermediates
+ * exceed the array return CRAVA_ENOTSUP.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that call before any stream
+ * capture.  Every call shares the array: calls whose work overlaps on the GPU (other
+ * streams, other threads) race; serialise them on one stream. */
+#define CRAVA_NOALLOC_SCRATCH_BYTES (64u << 20)
+crava_status crava_invert_noalloc(const crava_job_desc* desc, const float* const* d_in, float* const* d_out,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif
