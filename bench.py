@@ -196,6 +196,16 @@ def reference_main(args, rank, world):
 
 # ------------------------------------------------------------------ GPU arm
 
+def max_over_ranks(x: float, dist, device: str = "cuda") -> float:
+    """Max of a per-rank timing over all ranks (a no-op without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def alg_bytes(blk, nsim, cls, ngrids):
     """Algorithmic HBM bytes of one launch of a kernel class over ngrids grids."""
     N = blk.nxp * blk.nyp * blk.nzp
@@ -317,10 +327,7 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     kt = ctx.kernel_times(reset=True)
     ctx.set_profiling(False)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     value = world * blk.n_voxels / (ms / 1000.0)
 
     # e2e through the job API with pinned host buffers
@@ -355,10 +362,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1) / e2e_steps
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dist)
     bytes_grid = 4 * int(np.prod(shape))
 
     # roofline of the dominant kernel class

@@ -1,0 +1,67 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own FP32 numerics.
+
+    python tests/golden/make_golden.py          (needs oracle/_ref/libref32.so, built by
+                                                 `make -C oracle` from the reference tree)
+
+Each fixture holds one small block's inputs (the synth.Block arrays), the reference-path
+outputs computed by oracle/_ref (FFTW 2.1.2 float + lib_matr.c with the restated loops):
+posterior mean, posterior covariance, residual spectra, realisations drawn with the
+reference RandomGen, the inverted-bin and Cholesky-fallback counts, and the noise grids
+themselves.  The cases cover even, odd and padded sizes, 1..6 angle stacks, and a prior
+with correlation gradients (covariance grids that are not separable).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from crava_b200 import synth  # noqa: E402
+from oracle import bindings as ob  # noqa: E402
+from oracle import ref64  # noqa: E402
+
+CASES = {
+    "g1_even": dict(nx=16, ny=12, nz=20, theta_deg=(8.0, 24.0), peak_hz=(28.0, 32.0), sn=(4.0, 6.0), nsim=1, seed=5),
+    "g2_odd": dict(nx=15, ny=9, nz=21, theta_deg=(10.0, 20.0, 30.0), peak_hz=(30.0,) * 3, sn=(5.0,) * 3, nsim=2,
+                   seed=6),
+    "g3_padded": dict(nx=13, ny=11, nz=19, nxp=14, nyp=12, nzp=20, theta_deg=(5.0, 15.0, 25.0, 35.0, 45.0, 55.0),
+                      peak_hz=(30.0,) * 6, sn=(3.0,) * 6, nsim=1, seed=7),
+    "g4_gradients": dict(nx=12, ny=10, nz=16, theta_deg=(10.0, 30.0), peak_hz=(30.0, 30.0), sn=(5.0, 5.0), nsim=1,
+                         seed=9, corr_grad_i=0.3, corr_grad_j=-0.2),
+    "g5_one_angle_wideband": dict(nx=10, ny=8, nz=24, theta_deg=(20.0,), peak_hz=(40.0,), sn=(8.0,), nsim=1, seed=10,
+                                  low_cut=1.0, high_cut=200.0),
+}
+
+SCALARS = ["nx", "ny", "nz", "nxp", "nyp", "nzp", "lz", "low_int_cut", "low_cut", "high_cut", "wnc",
+           "min_rel_thick", "corr_grad_i", "corr_grad_j", "nsim", "seed"]
+ARRAYS = ["A", "err_theta_cov", "wavelet", "wavelet_norm", "prior_var0", "corr_xy", "prior_corr_t",
+          "circ_corr_t", "mean", "data"]
+
+
+def make(name, kw, noise_seed=1234):
+    blk = synth.make_block(synth.BlockSpec(**kw))
+    covs, _ = ref64.prior_cov_grids(blk)
+    if blk.corr_grad_i or blk.corr_grad_j:
+        ec = ref64.fill_err_corr(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp, blk.corr_grad_i, blk.corr_grad_j)
+    else:
+        ec = ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)
+    noise = ob.sim_noise(noise_seed, blk.nsim, blk.nxp, blk.nyp, blk.nzp, use_ref=True)
+    r = ob.ref32_invert(blk, covs, ec, nsim=blk.nsim, seed=noise_seed)
+    out = {k: np.asarray(getattr(blk, k)) for k in SCALARS}
+    out.update({k: getattr(blk, k) for k in ARRAYS})
+    out.update({"cov_grids": np.stack(covs), "err_corr": ec, "noise": noise, "noise_seed": np.int64(noise_seed),
+                "ref_mean": r.mean, "ref_cov": r.cov, "ref_resid_spec": r.resid_spec, "ref_sims": r.sims,
+                "ref_n_inverted": np.int64(r.n_inverted), "ref_n_chol_fail": np.int64(r.n_chol_fail)})
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return out
+
+
+if __name__ == "__main__":
+    if not ob.ref32_available():
+        sys.exit("oracle/_ref/libref32.so missing: run `make -C oracle` with the reference tree present")
+    for name, kw in CASES.items():
+        make(name, kw)
+        print("wrote", name)

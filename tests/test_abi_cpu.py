@@ -1,0 +1,99 @@
+"""The C ABI without a GPU: the library loads, exports every entry point the header
+declares, sizes jobs and rejects invalid descriptions; the Python binding fails loudly when
+the library is missing."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "crava_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(crava_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_built():
+    assert os.path.exists(api.LIB_PATH), "run python -m crava_b200.build"
+
+
+def test_every_declared_entry_point_is_exported():
+    L = ctypes.CDLL(api.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 18
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    L = api.lib()
+    for s in range(8):
+        assert L.crava_status_string(s)
+
+
+def _desc(blk, **over):
+    d, keep = api.make_desc(blk)
+    for k, v in over.items():
+        setattr(d, k, v)
+    return d, keep
+
+
+@pytest.fixture(scope="module")
+def small():
+    return synth.make_block(synth.BlockSpec(nx=16, ny=12, nz=20, nsim=2))
+
+
+def test_footprint_counts_grids_and_tables(small):
+    blk = small
+    nb = api.footprint(blk)
+    cnxp = blk.nxp // 2 + 1
+    grid = -(-(8 * cnxp * blk.nyp * blk.nzp) // 256) * 256
+    ngrids = 2 * (blk.ntheta + 3) + 6 + 3 * blk.nsim
+    assert nb >= ngrids * grid
+    assert nb < ngrids * grid + 64 * 1024
+    nb_grids = api.footprint(blk, prior_mode=api.PRIOR_GRIDS)
+    assert nb_grids - nb == 8 * grid
+    nb_noise = api.footprint(blk, flags=api.FLAG_HOST_NOISE)
+    assert nb_noise - nb == 3 * blk.nsim * grid
+
+
+@pytest.mark.parametrize("field,value,status", [
+    ("nxp", 11 * 13, api.ENOTSUP),     # not 2,3,5,7-smooth
+    ("ntheta", 9, api.ENOTSUP),
+    ("nsim", 17, api.ENOTSUP),
+    ("nxp", 8, api.EINVAL),            # padded below simbox size
+    ("lz", 0.0, api.EINVAL),
+    ("prior_mode", 7, api.EINVAL),
+])
+def test_invalid_descriptions_rejected(small, field, value, status):
+    d, _k = _desc(small, **{field: value})
+    out = ctypes.c_size_t()
+    st = api.lib().crava_job_footprint(ctypes.byref(d), ctypes.byref(out))
+    assert st == status
+    assert api.lib().crava_last_error()
+
+
+def test_null_description_rejected():
+    out = ctypes.c_size_t()
+    assert api.lib().crava_job_footprint(None, ctypes.byref(out)) == api.EINVAL
+
+
+def test_context_without_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.CravaError):
+        api.Context(0)
+
+
+def test_missing_library_raises(monkeypatch):
+    monkeypatch.setattr(api, "_lib", None)
+    monkeypatch.setattr(api, "LIB_PATH", "/nonexistent/libcrava_gpu.so")
+    with pytest.raises(api.CravaError):
+        api.lib()

@@ -165,3 +165,32 @@ def test_inputs_preserved_and_rerun_bitwise(ctx, block0):
     for k in ("mean", "cov", "sims"):
         assert np.array_equal(a[k], b[k]), k
     job.close()
+
+
+from tests.golden import golden_io  # noqa: E402
+
+
+@pytest.mark.parametrize("name", golden_io.names())
+def test_against_reference_fixtures(ctx, name):
+    """GPU (grids mode, reference RandomGen noise) against the reference's own FP32 path."""
+    blk, z = golden_io.load(name)
+    out = api.invert_block(ctx, blk, api.PRIOR_GRIDS, cov_grids=list(z["cov_grids"]), err_corr=z["err_corr"],
+                           noise=z["noise"], keep_residual=True)
+    nx = blk.nxp
+    assert out["counters"]["inverted_bins"] == int(z["ref_n_inverted"])
+    assert out["counters"]["chol_fallbacks"] == int(z["ref_n_chol_fail"])
+    for a in range(3):
+        assert crel(out["mean"][a][..., :nx], z["ref_mean"][a][..., :nx]) < TOL_MEAN
+    for q in range(6):
+        assert crel(out["cov"][q][..., :nx], z["ref_cov"][q][..., :nx]) < TOL_COV
+    for l in range(blk.ntheta):
+        assert crel(out["resid_spec"][l], z["ref_resid_spec"][l]) < 1e-3
+    for s in range(blk.nsim):
+        for a in range(3):
+            assert crel(out["sims"][s, a][..., :nx], z["ref_sims"][s, a][..., :nx]) < TOL_SIM
+    if not (blk.corr_grad_i or blk.corr_grad_j):
+        sep = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=z["noise"])
+        for a in range(3):
+            assert crel(sep["mean"][a][..., :nx], z["ref_mean"][a][..., :nx]) < TOL_MEAN
+        for q in range(6):
+            assert crel(sep["cov"][q][..., :nx], z["ref_cov"][q][..., :nx]) < TOL_COV
