@@ -35,6 +35,7 @@ EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_s
            "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches", "crava_ctx_set_profiling",
            "crava_ctx_kernel_times"]
 KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r"]
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
 
 
 class CravaError(RuntimeError):
@@ -61,6 +62,11 @@ class JobDesc(ctypes.Structure):
 class Counters(ctypes.Structure):
     _fields_ = [("inverted_bins", ctypes.c_longlong), ("chol_fallbacks", ctypes.c_longlong),
                 ("sim_chol_zero", ctypes.c_longlong), ("post_var0", ctypes.c_float * 9)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("queue_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -95,6 +101,16 @@ def lib() -> ctypes.CDLL:
     L.crava_ctx_set_profiling.argtypes = [vp, ctypes.c_int]
     L.crava_ctx_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.c_int, ctypes.c_int]
+    L.crava_batch_create.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.crava_batch_run.argtypes = [vp, vp]
+    L.crava_batch_destroy.argtypes = [vp]
+    L.crava_serve_start.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+    L.crava_serve_submit.argtypes = [vp, ctypes.POINTER(JobDesc), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                     ctypes.POINTER(ctypes.c_uint64)]
+    L.crava_serve_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(RequestInfo)]
+    L.crava_serve_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
+    L.crava_serve_stop.argtypes = [vp]
+    L.crava_invert_noalloc.argtypes = [ctypes.POINTER(JobDesc), ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
     _lib = L
     return L
 
@@ -292,3 +308,73 @@ def fft_r2c(ctx: Context, dptr: int, nxp: int, nyp: int, nzp: int, covariance: b
 
 def fft_c2r(ctx: Context, dptr: int, nxp: int, nyp: int, nzp: int, covariance: bool, stream=None):
     _check(lib().crava_fft_c2r(ctx.handle, ctypes.c_void_p(dptr), nxp, nyp, nzp, int(covariance), stream))
+
+
+class Batch:
+    """Many created jobs replayed as one CUDA graph with concurrent branches."""
+
+    def __init__(self, ctx: Context, jobs, branches: int = 16):
+        self.ctx = ctx
+        self.jobs = list(jobs)
+        arr = (ctypes.c_void_p * len(self.jobs))(*[j._h.value for j in self.jobs])
+        self._h = ctypes.c_void_p()
+        _check(lib().crava_batch_create(ctx.handle, arr, len(self.jobs), branches, ctypes.byref(self._h)))
+
+    def run(self, stream=None):
+        _check(lib().crava_batch_run(self._h, stream))
+
+    def close(self):
+        if self._h:
+            lib().crava_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The native serving loop: submit blocks (host buffers), poll/wait for completion."""
+
+    def __init__(self, ctx: Context, max_inflight: int = 8):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        self._keep = {}
+        _check(lib().crava_serve_start(ctx.handle, max_inflight, ctypes.byref(self._h)))
+
+    def submit(self, blk, host_in, host_out, seed=None) -> int:
+        """host_in / host_out: lists of host buffers (numpy float32 or pinned torch tensors)
+        kept alive until the request finishes."""
+        desc, keep = make_desc(blk, PRIOR_SEPARABLE, 0, seed=seed)
+        ptr = lambda a: a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+        ins = (ctypes.c_void_p * len(host_in))(*[ptr(a) for a in host_in])
+        outs = (ctypes.c_void_p * len(host_out))(*[ptr(a) if a is not None else None for a in host_out])
+        t = ctypes.c_uint64()
+        _check(lib().crava_serve_submit(self._h, ctypes.byref(desc), ins, outs, ctypes.byref(t)))
+        self._keep[t.value] = (desc, keep, host_in, host_out, ins, outs)
+        return t.value
+
+    def poll(self, ticket: int) -> dict:
+        info = RequestInfo()
+        _check(lib().crava_serve_poll(self._h, ticket, ctypes.byref(info)))
+        return {"state": info.state, "status": info.status, "queue_ms": info.queue_ms, "latency_ms": info.latency_ms}
+
+    def wait(self, ticket: int, timeout_ms: float = 600000.0) -> dict:
+        info = RequestInfo()
+        _check(lib().crava_serve_wait(self._h, ticket, timeout_ms, ctypes.byref(info)))
+        self._keep.pop(ticket, None)
+        return {"state": info.state, "status": info.status, "queue_ms": info.queue_ms, "latency_ms": info.latency_ms}
+
+    def stop(self):
+        if self._h:
+            lib().crava_serve_stop(self._h)
+            self._h = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass

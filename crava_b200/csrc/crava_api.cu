@@ -160,6 +160,8 @@ struct crava_job {
   std::vector<double> A, etc, pv;
   std::vector<float> wav, wnorm, corr_xy, circ;
   bool ran = false;
+  bool async = false;             // pool from cudaMallocAsync on alloc_stream
+  cudaStream_t alloc_stream = nullptr;
 };
 
 namespace {
@@ -497,18 +499,31 @@ crava_status crava_job_footprint(const crava_job_desc* desc, size_t* bytes) {
   return CRAVA_OK;
 }
 
-crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_job** job) {
+}  // extern "C"
+
+namespace {
+
+void job_release(crava_job* j) {
+  if (!j) return;
+  if (j->pool) {
+    if (j->async) cudaFreeAsync(j->pool, j->alloc_stream);
+    else cudaFree(j->pool);
+    std::lock_guard<std::mutex> lk(j->ctx->mu);
+    j->ctx->allocated -= j->pool_bytes;
+  }
+  delete j;
+}
+
+// Job set-up on stream st.  async: the pool comes from the stream-ordered allocator and
+// nothing waits for the GPU (the serving loop); otherwise the call returns with the job
+// ready (the public crava_job_create).
+crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStream_t st, bool async,
+                             crava_job** job) {
   if (!ctx || !job) return fail(CRAVA_EINVAL, "null argument");
   crava_status s = validate(desc);
   if (s) return s;
   CUDA_TRY(cudaSetDevice(ctx->device));
   size_t need = footprint(desc);
-  {
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    if (ctx->budget && ctx->allocated + need > ctx->budget)
-      return fail(CRAVA_ENOMEM, "job needs " + std::to_string(need) + " bytes; budget left " +
-                                    std::to_string(ctx->budget - ctx->allocated));
-  }
   crava_job* j = new crava_job();
   j->ctx = ctx;
   j->d = *desc;
@@ -534,13 +549,29 @@ crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_
   j->d.corr_xy = j->corr_xy.empty() ? nullptr : j->corr_xy.data();
   j->d.circ_corr_t = j->circ.empty() ? nullptr : j->circ.data();
 
-  cudaError_t e = cudaMalloc(&j->pool, need);
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->budget && ctx->allocated + need > ctx->budget) {
+      size_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
+      delete j;
+      return fail(CRAVA_ENOMEM, "job needs " + std::to_string(need) + " bytes; budget left " + std::to_string(left));
+    }
+    ctx->allocated += need;
+  }
+  j->async = async;
+  j->alloc_stream = st;
+  j->pool_bytes = need;
+  cudaError_t e = async ? cudaMallocAsync((void**)&j->pool, need, st) : cudaMalloc(&j->pool, need);
   if (e != cudaSuccess) {
     cudaGetLastError();
+    j->pool = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      ctx->allocated -= need;
+    }
     delete j;
-    return fail(CRAVA_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return fail(CRAVA_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
   }
-  j->pool_bytes = need;
   size_t gb = align256(sizeof(float) * j->rsize);
   char* p = j->pool;
   auto take = [&](size_t bytes) { char* q = p; p += align256(bytes); return q; };
@@ -565,59 +596,74 @@ crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_
   j->ct = (float2*)take(sizeof(float2) * d.nzp);
   j->cxy_grid = (float*)take(sizeof(float) * j->rnxp * d.nyp);
   j->counters = (unsigned long long*)take(256);
-  {
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->allocated += need;
-  }
+#define JOB_TRY(call)                                          \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) {                                   \
+      crava_status st_ = cuda_fail(e_, #call);                 \
+      job_release(j);                                          \
+      return st_;                                              \
+    }                                                          \
+  } while (0)
 
   // per-kz tables
   std::vector<float2> kw, e1, e2;
   std::vector<uint8_t> inv;
   build_kz_tables(j->d, kw, e1, e2, inv);
-  CUDA_TRY(cudaMemcpy(j->kw, kw.data(), sizeof(float2) * kw.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(j->e1, e1.data(), sizeof(float2) * e1.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(j->e2, e2.data(), sizeof(float2) * e2.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(j->inv, inv.data(), inv.size(), cudaMemcpyHostToDevice));
+  JOB_TRY(cudaMemcpyAsync(j->kw, kw.data(), sizeof(float2) * kw.size(), cudaMemcpyHostToDevice, st));
+  JOB_TRY(cudaMemcpyAsync(j->e1, e1.data(), sizeof(float2) * e1.size(), cudaMemcpyHostToDevice, st));
+  JOB_TRY(cudaMemcpyAsync(j->e2, e2.data(), sizeof(float2) * e2.size(), cudaMemcpyHostToDevice, st));
+  JOB_TRY(cudaMemcpyAsync(j->inv, inv.data(), inv.size(), cudaMemcpyHostToDevice, st));
   if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) {
     // temporal factor: DFT of circCorrT (1D, double)
     std::vector<double> c(j->circ.begin(), j->circ.end());
     std::vector<cd> C = dft(c);
     std::vector<float2> ct(d.nzp);
     for (int k = 0; k < d.nzp; k++) ct[k] = make_float2((float)C[k].real(), (float)C[k].imag());
-    CUDA_TRY(cudaMemcpy(j->ct, ct.data(), sizeof(float2) * d.nzp, cudaMemcpyHostToDevice));
+    JOB_TRY(cudaMemcpyAsync(j->ct, ct.data(), sizeof(float2) * d.nzp, cudaMemcpyHostToDevice, st));
     // lateral factor: 2D transform of corrXY on the device (x then y)
     std::vector<float> g((size_t)j->rnxp * d.nyp, 0.f);
     for (int jj = 0; jj < d.nyp; jj++)
       for (int ii = 0; ii < d.nxp; ii++) g[(size_t)jj * j->rnxp + ii] = j->corr_xy[(size_t)jj * d.nxp + ii];
-    CUDA_TRY(cudaMemcpy(j->cxy_grid, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice));
+    JOB_TRY(cudaMemcpyAsync(j->cxy_grid, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st));
     Plan *px, *pn, *py;
     crava_status ps;
-    if ((ps = get_xplans(ctx, d.nxp, &px, &pn)) || (ps = get_plan(ctx, d.nyp, &py))) return ps;
+    if ((ps = get_xplans(ctx, d.nxp, &px, &pn)) || (ps = get_plan(ctx, d.nyp, &py))) {
+      job_release(j);
+      return ps;
+    }
     GridSet gs;
     gs.n = 1;
     gs.p[0] = j->cxy_grid;
     gs.src[0] = j->cxy_grid;
     gs.scale[0] = 1.0f;
     int nl = 0;
-    CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, pn->tw, 0, &nl));
-    CUDA_TRY(launch_line_fft(gs, j->cnxp, d.nyp, (size_t)j->cnxp, 1, 0, py->lp, py->tw, -1.f, 0, &nl));
-    CUDA_TRY(cudaMemcpy(j->cxy, j->cxy_grid, sizeof(float2) * j->cnxp * d.nyp, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaDeviceSynchronize());
-    ctx->launches += nl;
+    JOB_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, pn->tw, st, &nl));
+    JOB_TRY(launch_line_fft(gs, j->cnxp, d.nyp, (size_t)j->cnxp, 1, 0, py->lp, py->tw, -1.f, st, &nl));
+    JOB_TRY(cudaMemcpyAsync(j->cxy, j->cxy_grid, sizeof(float2) * j->cnxp * d.nyp, cudaMemcpyDeviceToDevice, st));
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      ctx->launches += nl;
+    }
   }
+  if (!async) JOB_TRY(cudaStreamSynchronize(st));
+#undef JOB_TRY
   *job = j;
   return CRAVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_job** job) {
+  return job_create_impl(ctx, desc, 0, false, job);
 }
 
 crava_status crava_job_destroy(crava_job* job) {
   if (!job) return CRAVA_OK;
   cudaSetDevice(job->ctx->device);
-  cudaFree(job->pool);
-  {
-    std::lock_guard<std::mutex> lk(job->ctx->mu);
-    job->ctx->allocated -= job->pool_bytes;
-  }
-  delete job;
+  job_release(job);
   return CRAVA_OK;
 }
 
@@ -994,3 +1040,388 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   }
   return CRAVA_OK;
 }
+
+// ---------------------------------------------------------------------------------------
+// Batches: many blocks of uneven size and angle count captured into one CUDA graph whose
+// branches run concurrently (no reference counterpart: the reference inverts one interval
+// at a time, main.cpp:217-353).
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+
+struct crava_batch {
+  crava_ctx* ctx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;  // kernel launches per replay
+};
+
+namespace {
+
+// Plans a job's run needs, created before a capture (plan creation allocates).
+crava_status prewarm_plans(crava_ctx* ctx, const crava_job_desc& d) {
+  Plan *a, *b;
+  crava_status s;
+  if ((s = get_xplans(ctx, d.nxp, &a, &b))) return s;
+  if ((s = get_plan(ctx, d.nyp, &a))) return s;
+  if ((s = get_plan(ctx, d.nzp, &a))) return s;
+  const char* r16 = getenv("CRAVA_ZPASS_R16");
+  return get_plan(ctx, d.nzp, &a, !(r16 && r16[0] == '0'));
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_batch_create(crava_ctx* ctx, crava_job* const* jobs, int n, int branches, crava_batch** out) {
+  if (!ctx || !jobs || !out || n < 1) return fail(CRAVA_EINVAL, "bad batch arguments");
+  if (branches < 1) branches = 1;
+  if (branches > n) branches = n;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  for (int i = 0; i < n; i++) {
+    if (!jobs[i] || jobs[i]->ctx != ctx) return fail(CRAVA_EINVAL, "job of another context");
+    crava_status s = prewarm_plans(ctx, jobs[i]->d);
+    if (s) return s;
+  }
+  const bool prof = ctx->profiling;
+  ctx->profiling = false;
+  std::vector<cudaStream_t> br(branches);
+  cudaStream_t cap;
+  CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  for (auto& b : br) CUDA_TRY(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+  cudaEvent_t fork;
+  std::vector<cudaEvent_t> join(branches);
+  CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  for (auto& e : join) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  long long l0 = ctx->launches;
+  crava_status st = CRAVA_OK;
+  cudaGraph_t graph = nullptr;
+  cudaError_t ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed);
+  if (ce == cudaSuccess) {
+    cudaEventRecord(fork, cap);
+    for (int b = 0; b < branches; b++) cudaStreamWaitEvent(br[b], fork, 0);
+    for (int i = 0; i < n && !st; i++) st = crava_job_run(jobs[i], br[i % branches]);
+    for (int b = 0; b < branches; b++) {
+      cudaEventRecord(join[b], br[b]);
+      cudaStreamWaitEvent(cap, join[b], 0);
+    }
+    ce = cudaStreamEndCapture(cap, &graph);
+  }
+  ctx->profiling = prof;
+  crava_batch* bt = nullptr;
+  if (!st && ce == cudaSuccess) {
+    bt = new crava_batch();
+    bt->ctx = ctx;
+    bt->graph = graph;
+    bt->kernels = ctx->launches - l0;
+    ce = cudaGraphInstantiate(&bt->exec, graph, 0);
+  }
+  ctx->launches = l0;  // the capture launched nothing
+  cudaEventDestroy(fork);
+  for (auto& e : join) cudaEventDestroy(e);
+  for (auto& b : br) cudaStreamDestroy(b);
+  cudaStreamDestroy(cap);
+  if (st) {
+    if (graph) cudaGraphDestroy(graph);
+    delete bt;
+    return st;
+  }
+  if (ce != cudaSuccess) {
+    if (bt) {
+      if (bt->graph) cudaGraphDestroy(bt->graph);
+      delete bt;
+    }
+    return cuda_fail(ce, "batch graph capture");
+  }
+  *out = bt;
+  return CRAVA_OK;
+}
+
+crava_status crava_batch_run(crava_batch* b, void* stream) {
+  if (!b) return fail(CRAVA_EINVAL, "null batch");
+  CUDA_TRY(cudaSetDevice(b->ctx->device));
+  CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  b->ctx->launches += b->kernels;
+  return CRAVA_OK;
+}
+
+crava_status crava_batch_destroy(crava_batch* b) {
+  if (!b) return CRAVA_OK;
+  cudaSetDevice(b->ctx->device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  delete b;
+  return CRAVA_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Serving: a native request loop that admits jobs by their HBM footprint against the
+// context's budget and an in-flight limit, runs each admitted job on its own stream
+// (host->device inputs, the whole inversion, device->host outputs) so that jobs that
+// arrive while others run overlap on the device, and releases each job's memory
+// (stream-ordered) when its completion event fires.
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct ServeReq {
+  uint64_t id = 0;
+  crava_job_desc d{};
+  std::vector<double> A, etc, pv;
+  std::vector<float> wav, wn, cxy, circ;
+  std::vector<const float*> in;
+  std::vector<float*> out;
+  double t_submit = 0, t_start = 0, t_done = 0;
+  int state = CRAVA_REQ_QUEUED;
+  crava_status status = CRAVA_OK;
+  std::string err;
+  crava_job* job = nullptr;
+  int slot = -1;
+  cudaEvent_t done = nullptr;
+};
+
+}  // namespace
+
+struct crava_server {
+  crava_ctx* ctx = nullptr;
+  int max_inflight = 1;
+  std::vector<cudaStream_t> streams;
+  std::vector<char> busy;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool stopping = false;
+  uint64_t next_id = 1;
+  std::deque<ServeReq*> pending;
+  std::vector<ServeReq*> inflight;
+  std::map<uint64_t, ServeReq*> reqs;
+  long long completed = 0;
+};
+
+namespace {
+
+// Starts one request on a free stream; returns false when it does not fit yet.
+bool serve_admit(crava_server* sv, ServeReq* r, int slot) {
+  cudaStream_t st = sv->streams[slot];
+  crava_job* job = nullptr;
+  crava_status s = job_create_impl(sv->ctx, &r->d, st, true, &job);
+  if (s == CRAVA_ENOMEM) return false;
+  r->t_start = now_ms();
+  if (s) {
+    r->status = s;
+    r->err = crava_last_error();
+    r->state = CRAVA_REQ_FAILED;
+    return true;
+  }
+  r->job = job;
+  r->slot = slot;
+  const int nth = r->d.ntheta;
+  for (int l = 0; l < nth && !s; l++) s = crava_job_upload(job, CRAVA_ROLE_DATA, l, r->in[l], st);
+  for (int a = 0; a < 3 && !s; a++) s = crava_job_upload(job, CRAVA_ROLE_MEAN, a, r->in[nth + a], st);
+  if (!s) s = crava_job_run(job, st);
+  for (size_t q = 0; q < r->out.size() && !s; q++) {
+    if (!r->out[q]) continue;
+    if (q < 3) s = crava_job_download(job, CRAVA_ROLE_POST_MEAN, (int)q, r->out[q], st);
+    else if (q < 9) s = crava_job_download(job, CRAVA_ROLE_POST_COV, (int)q - 3, r->out[q], st);
+    else s = crava_job_download(job, CRAVA_ROLE_SIM, (int)q - 9, r->out[q], st);
+  }
+  if (!s && cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) s = CRAVA_ECUDA;
+  if (!s && cudaEventRecord(r->done, st) != cudaSuccess) s = CRAVA_ECUDA;
+  if (s) {
+    r->status = s;
+    r->err = crava_last_error();
+    r->state = CRAVA_REQ_FAILED;
+    cudaStreamSynchronize(st);
+    job_release(job);
+    r->job = nullptr;
+    return true;
+  }
+  r->state = CRAVA_REQ_RUNNING;
+  sv->busy[slot] = 1;
+  sv->inflight.push_back(r);
+  return true;
+}
+
+void serve_loop(crava_server* sv) {
+  cudaSetDevice(sv->ctx->device);
+  std::unique_lock<std::mutex> lk(sv->mu);
+  for (;;) {
+    bool progressed = false;
+    // completions
+    for (size_t i = 0; i < sv->inflight.size();) {
+      ServeReq* r = sv->inflight[i];
+      cudaError_t q = cudaEventQuery(r->done);
+      if (q == cudaErrorNotReady) { i++; continue; }
+      r->t_done = now_ms();
+      if (q != cudaSuccess) {
+        r->status = CRAVA_ECUDA;
+        r->err = cudaGetErrorString(q);
+        r->state = CRAVA_REQ_FAILED;
+      } else {
+        r->state = CRAVA_REQ_DONE;
+      }
+      cudaEventDestroy(r->done);
+      r->done = nullptr;
+      job_release(r->job);
+      r->job = nullptr;
+      sv->busy[r->slot] = 0;
+      sv->inflight.erase(sv->inflight.begin() + i);
+      sv->completed++;
+      progressed = true;
+    }
+    // admissions, first come first served
+    while (!sv->pending.empty() && (int)sv->inflight.size() < sv->max_inflight && !sv->stopping) {
+      int slot = -1;
+      for (int k = 0; k < (int)sv->busy.size(); k++)
+        if (!sv->busy[k]) { slot = k; break; }
+      if (slot < 0) break;
+      ServeReq* r = sv->pending.front();
+      if (!serve_admit(sv, r, slot)) break;  // waits for memory to be released
+      sv->pending.pop_front();
+      if (r->state == CRAVA_REQ_FAILED) r->t_done = now_ms();
+      progressed = true;
+    }
+    if (sv->stopping) {
+      for (ServeReq* r : sv->pending) {
+        r->state = CRAVA_REQ_FAILED;
+        r->status = CRAVA_ESTATE;
+        r->err = "server stopped before the request started";
+      }
+      sv->pending.clear();
+      if (sv->inflight.empty()) break;
+    }
+    if (progressed) sv->cv.notify_all();
+    sv->cv.wait_for(lk, std::chrono::microseconds(progressed ? 0 : 100));
+  }
+  sv->cv.notify_all();
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_serve_start(crava_ctx* ctx, int max_inflight, crava_server** out) {
+  if (!ctx || !out) return fail(CRAVA_EINVAL, "null argument");
+  if (max_inflight < 1 || max_inflight > 256) return fail(CRAVA_EINVAL, "max_inflight must be 1..256");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  // keep freed job memory in the stream-ordered pool instead of returning it to the driver
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  crava_server* sv = new crava_server();
+  sv->ctx = ctx;
+  sv->max_inflight = max_inflight;
+  sv->streams.resize(max_inflight);
+  sv->busy.assign(max_inflight, 0);
+  for (auto& s : sv->streams) {
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  }
+  sv->th = std::thread(serve_loop, sv);
+  *out = sv;
+  return CRAVA_OK;
+}
+
+crava_status crava_serve_submit(crava_server* sv, const crava_job_desc* desc, const float* const* host_in,
+                                float* const* host_out, uint64_t* ticket) {
+  if (!sv || !desc || !host_in || !ticket) return fail(CRAVA_EINVAL, "null argument");
+  crava_status s = validate(desc);
+  if (s) return s;
+  if (desc->prior_mode != CRAVA_PRIOR_SEPARABLE || (desc->flags & CRAVA_FLAG_HOST_NOISE))
+    return fail(CRAVA_ENOTSUP, "served jobs take the separable prior and device noise");
+  ServeReq* r = new ServeReq();
+  r->d = *desc;
+  const int nth = desc->ntheta;
+  r->A.assign(desc->A, desc->A + 3 * nth);
+  r->etc.assign(desc->err_theta_cov, desc->err_theta_cov + nth * nth);
+  r->pv.assign(desc->prior_var0, desc->prior_var0 + 9);
+  r->wav.assign(desc->wavelet, desc->wavelet + (size_t)nth * desc->nzp);
+  r->wn.assign(desc->wavelet_norm, desc->wavelet_norm + nth);
+  r->cxy.assign(desc->corr_xy, desc->corr_xy + (size_t)desc->nxp * desc->nyp);
+  r->circ.assign(desc->circ_corr_t, desc->circ_corr_t + desc->nzp);
+  r->d.A = r->A.data();
+  r->d.err_theta_cov = r->etc.data();
+  r->d.prior_var0 = r->pv.data();
+  r->d.wavelet = r->wav.data();
+  r->d.wavelet_norm = r->wn.data();
+  r->d.corr_xy = r->cxy.data();
+  r->d.circ_corr_t = r->circ.data();
+  r->d.flags &= ~CRAVA_FLAG_KEEP_RESIDUAL;
+  r->in.assign(host_in, host_in + nth + 3);
+  const int nout = 9 + 3 * desc->nsim;
+  if (host_out) r->out.assign(host_out, host_out + nout);
+  else r->out.assign(nout, nullptr);
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (sv->stopping) {
+    delete r;
+    return fail(CRAVA_ESTATE, "server is stopping");
+  }
+  r->id = sv->next_id++;
+  r->t_submit = now_ms();
+  sv->reqs[r->id] = r;
+  sv->pending.push_back(r);
+  *ticket = r->id;
+  sv->cv.notify_all();
+  return CRAVA_OK;
+}
+
+crava_status crava_serve_poll(crava_server* sv, uint64_t ticket, crava_request_info* info) {
+  if (!sv || !info) return fail(CRAVA_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket");
+  const ServeReq* r = it->second;
+  info->state = r->state;
+  info->status = r->status;
+  info->queue_ms = (r->t_start > 0 ? r->t_start : now_ms()) - r->t_submit;
+  info->latency_ms = r->t_done > 0 ? r->t_done - r->t_submit : -1.0;
+  return CRAVA_OK;
+}
+
+crava_status crava_serve_wait(crava_server* sv, uint64_t ticket, double timeout_ms, crava_request_info* info) {
+  if (!sv) return fail(CRAVA_EINVAL, "null server");
+  const double t_end = now_ms() + timeout_ms;
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket");
+  ServeReq* r = it->second;
+  while (r->state == CRAVA_REQ_QUEUED || r->state == CRAVA_REQ_RUNNING) {
+    double left = t_end - now_ms();
+    if (left <= 0) return fail(CRAVA_ETIMEDOUT, "request not finished within the timeout");
+    sv->cv.wait_for(lk, std::chrono::microseconds((long long)std::min(left * 1000.0, 10000.0)));
+  }
+  lk.unlock();
+  if (info) crava_serve_poll(sv, ticket, info);
+  if (r->state == CRAVA_REQ_FAILED) return fail(r->status ? r->status : CRAVA_ECUDA, r->err);
+  return CRAVA_OK;
+}
+
+crava_status crava_serve_stop(crava_server* sv) {
+  if (!sv) return CRAVA_OK;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stopping = true;
+    sv->cv.notify_all();
+  }
+  if (sv->th.joinable()) sv->th.join();
+  cudaSetDevice(sv->ctx->device);
+  for (auto& s : sv->streams) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (auto& kv : sv->reqs) delete kv.second;
+  delete sv;
+  return CRAVA_OK;
+}
+
+}  // extern "C"

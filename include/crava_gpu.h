@@ -158,6 +158,41 @@ long long crava_ctx_kernel_launches(crava_ctx* ctx);
 crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable);
 crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset);
 
+/* Batches (no counterpart in the reference, which inverts one interval at a time,
+ * main.cpp:217-353): the runs of n created jobs, of any sizes and angle counts, captured
+ * once into a CUDA graph with `branches` concurrent branches; every crava_batch_run
+ * replays the whole batch on `stream`.  Inputs are uploaded to the jobs beforehand. */
+typedef struct crava_batch crava_batch;
+crava_status crava_batch_create(crava_ctx* ctx, crava_job* const* jobs, int n, int branches, crava_batch** out);
+crava_status crava_batch_run(crava_batch* b, void* stream);
+crava_status crava_batch_destroy(crava_batch* b);
+
+/* Serving (no counterpart in the reference): a request loop on a native thread.  Jobs
+ * are admitted first come first served while the in-flight count is below max_inflight
+ * and their footprint fits the context's HBM budget; each runs on its own stream (inputs
+ * host->device, the inversion, outputs device->host) and overlaps with the others; its
+ * device memory is released, stream-ordered, when it completes.  host_in: ntheta data
+ * grids then 3 prior mean grids; host_out: 3 posterior mean, 6 covariance, 3*nsim
+ * realisation grids (NULL entries are not downloaded).  Host buffers stay owned by the
+ * caller and must stay valid until the request is done (pinned buffers keep the copies
+ * asynchronous).  Served jobs take the separable prior and device noise. */
+typedef struct crava_server crava_server;
+enum { CRAVA_REQ_QUEUED = 0, CRAVA_REQ_RUNNING = 1, CRAVA_REQ_DONE = 2, CRAVA_REQ_FAILED = 3 };
+typedef struct {
+  int state;           /* CRAVA_REQ_*                                     */
+  crava_status status; /* failure reason                                  */
+  double queue_ms;     /* submit -> admission                             */
+  double latency_ms;   /* submit -> completion seen by the loop (-1 if not done) */
+} crava_request_info;
+crava_status crava_serve_start(crava_ctx* ctx, int max_inflight, crava_server** out);
+crava_status crava_serve_submit(crava_server* sv, const crava_job_desc* desc, const float* const* host_in,
+                                float* const* host_out, uint64_t* ticket);
+crava_status crava_serve_poll(crava_server* sv, uint64_t ticket, crava_request_info* info);
+/* Waits at most timeout_ms; CRAVA_ETIMEDOUT when the request is still queued or running. */
+crava_status crava_serve_wait(crava_server* sv, uint64_t ticket, double timeout_ms, crava_request_info* info);
+/* Finishes the running requests, fails the queued ones, joins the loop thread. */
+crava_status crava_serve_stop(crava_server* sv);
+
 /* One block, end to end, with no device allocation (no counterpart in the reference).
  *
  * For callers that cannot allocate device memory: code inside a CUDA stream capture that

@@ -1,0 +1,126 @@
+"""Batches and the serving loop: every block's result is the same alone, in a batch and in
+a served mix (bitwise: the kernels are deterministic and the per-block work does not depend
+on what else runs)."""
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+SPECS = [
+    dict(nx=64, ny=48, nz=64, theta_deg=(10.0, 30.0), peak_hz=(30.0, 30.0), sn=(5.0, 5.0), nsim=2, seed=1),
+    dict(nx=75, ny=90, nz=81, theta_deg=(5.0, 20.0, 35.0, 50.0), peak_hz=(28.0,) * 4, sn=(4.0,) * 4, nsim=1, seed=2),
+    dict(nx=96, ny=80, nz=100, theta_deg=tuple(np.linspace(5, 45, 6)), peak_hz=(32.0,) * 6, sn=(6.0,) * 6, nsim=3,
+         seed=3),
+    dict(nx=45, ny=64, nz=128, theta_deg=(15.0, 25.0, 35.0), peak_hz=(30.0,) * 3, sn=(5.0,) * 3, nsim=1, seed=4),
+]
+
+
+@pytest.fixture(scope="module")
+def blocks():
+    return [synth.make_block(synth.BlockSpec(**s)) for s in SPECS]
+
+
+@pytest.fixture(scope="module")
+def alone(ctx, blocks):
+    outs = []
+    for i, b in enumerate(blocks):
+        j = api.Job(ctx, b, api.PRIOR_SEPARABLE, 0, seed=100 + i)
+        _k = j.upload_block()
+        j.run()
+        outs.append(j.download_outputs())
+        j.close()
+    return outs
+
+
+def test_batch_matches_alone(ctx, blocks, alone):
+    jobs = []
+    for i, b in enumerate(blocks):
+        j = api.Job(ctx, b, api.PRIOR_SEPARABLE, 0, seed=100 + i)
+        j._k = j.upload_block()
+        jobs.append(j)
+    bt = api.Batch(ctx, jobs, branches=3)
+    l0 = ctx.kernel_launches()
+    for _ in range(2):
+        bt.run()
+    import torch
+    torch.cuda.synchronize()
+    assert ctx.kernel_launches() - l0 == 2 * 5 * len(jobs)
+    for j, ref in zip(jobs, alone):
+        got = j.download_outputs()
+        for k in ("mean", "cov", "sims"):
+            assert np.array_equal(got[k], ref[k]), k
+    bt.close()
+    for j in jobs:
+        j.close()
+
+
+def _host_buffers(b, nsim):
+    import torch
+    shape = (b.nzp, b.nyp, 2 * (b.nxp // 2 + 1))
+    ins = [torch.from_numpy(np.ascontiguousarray(b.data[l])).pin_memory() for l in range(b.ntheta)] + \
+          [torch.from_numpy(np.ascontiguousarray(b.mean[a])).pin_memory() for a in range(3)]
+    outs = [torch.empty(shape, dtype=torch.float32).pin_memory() for _ in range(9 + 3 * nsim)]
+    return ins, outs
+
+
+def test_served_mix_matches_alone(ctx, blocks, alone):
+    sv = api.Server(ctx, max_inflight=3)
+    tickets, bufs = [], []
+    for rep in range(2):
+        for i, b in enumerate(blocks):
+            ins, outs = _host_buffers(b, b.nsim)
+            tickets.append((i, sv.submit(b, ins, outs, seed=100 + i)))
+            bufs.append(outs)
+    for (i, t), outs in zip(tickets, bufs):
+        info = sv.wait(t, timeout_ms=120000)
+        assert info["state"] == api.REQ_DONE
+        assert info["latency_ms"] > 0
+        ref = alone[i]
+        got_mean = np.stack([o.numpy() for o in outs[:3]])
+        got_cov = np.stack([o.numpy() for o in outs[3:9]])
+        assert np.array_equal(got_mean, ref["mean"])
+        assert np.array_equal(got_cov, ref["cov"])
+        got_sims = np.stack([o.numpy() for o in outs[9:]]).reshape(ref["sims"].shape)
+        assert np.array_equal(got_sims, ref["sims"])
+    sv.stop()
+
+
+def test_served_admission_by_budget(blocks):
+    """A budget that holds one job at a time: requests queue and still all complete."""
+    fp = max(api.footprint(b) for b in blocks)
+    c = api.Context(0, hbm_budget=int(fp * 1.2))
+    sv = api.Server(c, max_inflight=4)
+    ts = []
+    keep = []
+    for i, b in enumerate(blocks):
+        ins, outs = _host_buffers(b, b.nsim)
+        keep.append((ins, outs))
+        ts.append(sv.submit(b, ins, outs, seed=7))
+    infos = [sv.wait(t, timeout_ms=120000) for t in ts]
+    assert all(x["state"] == api.REQ_DONE for x in infos)
+    # later requests waited in the queue for memory
+    assert max(x["queue_ms"] for x in infos) > 0
+    sv.stop()
+    c.close()
+
+
+def test_wait_times_out_and_stop_fails_queued(ctx, blocks):
+    sv = api.Server(ctx, max_inflight=1)
+    b = blocks[2]
+    bufs = [_host_buffers(b, b.nsim) for _ in range(3)]
+    ts = [sv.submit(b, ins, outs, seed=1) for ins, outs in bufs]
+    with pytest.raises(api.CravaError) as e:
+        sv.wait(ts[-1], timeout_ms=0.01)
+    assert e.value.status == api.ETIMEDOUT
+    sv.wait(ts[0], timeout_ms=120000)
+    sv.stop()
