@@ -234,6 +234,115 @@ def read_traffic(kernel_class):
     return None
 
 
+def batched_leg(ctx, torch, n_blocks=64, nsim=16, reps=3, branches=16):
+    """64 blocks of uneven size and angle count (nx, ny smooth in [64,256], nz smooth in
+    [64,200], 2..6 angles, 16 realisations): one-job-at-a-time (run, wait) against the whole
+    batch replayed as one CUDA graph with concurrent branches; inputs resident."""
+    from crava_b200 import api, synth
+    blocks = [synth.make_block_fast(s) for s in synth.batch_specs(n_blocks, nsim=nsim)]
+    jobs = []
+    for i, b in enumerate(blocks):
+        j = api.Job(ctx, b, api.PRIOR_SEPARABLE, 0, seed=500 + i)
+        j._keep_in = j.upload_block()
+        jobs.append(j)
+    vox = sum(b.n_voxels for b in blocks)
+    st = torch.cuda.current_stream()
+    sh = st.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for j in jobs:
+        j.run(sh)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for j in jobs:
+        j.run(sh)
+        st.synchronize()
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1) / 1000.0
+    bt = api.Batch(ctx, jobs, branches=branches)
+    bt.run(sh)
+    torch.cuda.synchronize()
+    l0 = ctx.kernel_launches()
+    e0.record(st)
+    for _ in range(reps):
+        bt.run(sh)
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_b = e0.elapsed_time(e1) / 1000.0 / reps
+    launches = (ctx.kernel_launches() - l0) // reps
+    bt.close()
+    for j in jobs:
+        j.close()
+    return {"workload": f"{n_blocks} blocks, nx,ny in smooth[64,256], nz in smooth[64,200], 2..6 angles, "
+                        f"{nsim} realisations, separable prior, white-noise seismic of seismic amplitude",
+            "voxels": vox, "voxels_per_s": vox / t_b, "jobs_per_s": n_blocks / t_b, "ms_per_batch": 1000 * t_b,
+            "plain_voxels_per_s": vox / t_plain, "plain_jobs_per_s": n_blocks / t_plain,
+            "speedup_vs_plain": t_plain / t_b, "branches": branches, "gpu_launches_per_batch": launches}
+
+
+def served_leg(torch, n_jobs=48, distinct=8, rate=20.0, nsim=16, max_inflight=8, budget_gb=120):
+    """Served stream: Poisson arrivals at `rate` jobs/s of blocks log-uniform between
+    64x64x64 and 512x512x256, 3..6 angles, 16 realisations; host->device inputs, inversion,
+    device->host of the posterior mean, covariance and first realisation per request.
+    Against the plain one-job-at-a-time path (create, upload, run, download, release)."""
+    import numpy as np
+    from crava_b200 import api, synth
+    specs = synth.served_specs(n_jobs, nsim=nsim)
+    uniq = [synth.make_block_fast(s) for s in specs[:distinct]]
+    reqs = [i % distinct for i in range(n_jobs)]
+    bufs = []
+    for b in uniq:
+        shape = (b.nzp, b.nyp, 2 * (b.nxp // 2 + 1))
+        ins = [torch.from_numpy(np.ascontiguousarray(b.data[l])).pin_memory() for l in range(b.ntheta)] +               [torch.from_numpy(np.ascontiguousarray(b.mean[a])).pin_memory() for a in range(3)]
+        outs = [torch.empty(shape, dtype=torch.float32).pin_memory() for _ in range(12)] +                [None] * (3 * nsim - 3)
+        bufs.append((ins, outs))
+    vox = sum(uniq[i].n_voxels for i in reqs)
+    ctx = api.Context(torch.cuda.current_device(), hbm_budget=int(budget_gb * 1e9))
+    # plain path
+    t0 = time.perf_counter()
+    for i in reqs:
+        b = uniq[i]
+        j = api.Job(ctx, b, api.PRIOR_SEPARABLE, 0, seed=900 + i)
+        ins, outs = bufs[i]
+        for q, h in enumerate(ins):
+            role, idx = (api.ROLE_DATA, q) if q < b.ntheta else (api.ROLE_MEAN, q - b.ntheta)
+            api._check(api.lib().crava_job_upload(j._h, role, idx, h.data_ptr(), None))
+        j.run()
+        for q in range(12):
+            role, idx = (api.ROLE_POST_MEAN, q) if q < 3 else ((api.ROLE_POST_COV, q - 3) if q < 9 else (api.ROLE_SIM, q - 9))
+            api._check(api.lib().crava_job_download(j._h, role, idx, outs[q].data_ptr(), None))
+        torch.cuda.synchronize()
+        j.close()
+    t_plain = time.perf_counter() - t0
+    # served at `rate` (Poisson) and saturated (all at once)
+    rng = np.random.default_rng(77)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_jobs))
+    res = {}
+    for mode in ("poisson", "saturated"):
+        sv = api.Server(ctx, max_inflight=max_inflight)
+        tickets = []
+        t0 = time.perf_counter()
+        for k, i in enumerate(reqs):
+            if mode == "poisson":
+                dt = arrivals[k] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+            ins, outs = bufs[i]
+            tickets.append(sv.submit(uniq[i], ins, outs, seed=900 + i))
+        infos = [sv.wait(t, timeout_ms=600000) for t in tickets]
+        t_all = time.perf_counter() - t0
+        sv.stop()
+        lat = np.array([x["latency_ms"] for x in infos])
+        res[mode] = {"jobs_per_s": n_jobs / t_all, "voxels_per_s": vox / t_all,
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "speedup_vs_plain": t_plain / t_all}
+    ctx.close()
+    return {"workload": f"{n_jobs} requests over {distinct} blocks log-uniform 64^3..512x512x256 voxels, 3..6 angles, "
+                        f"{nsim} realisations; outputs mean+cov+1 realisation to host; {rate:g} jobs/s Poisson",
+            "voxels": vox, "plain_jobs_per_s": n_jobs / t_plain, "plain_voxels_per_s": vox / t_plain,
+            "max_inflight": max_inflight, "budget_gb": budget_gb, **res}
+
+
 def parity_check(ctx):
     """GPU vs the FP64 oracle on the 64x64x128 block (parity mode noise)."""
     import numpy as np
@@ -262,6 +371,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--dims", default=None, help="nx,ny,nz of a smaller block (profiling runs only)")
+    ap.add_argument("--no-legs", action="store_true", help="skip the batched and served legs")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -377,6 +487,11 @@ def main():
     B_alg = 12 * blk.n_voxels * (nin + nout)
 
     parity = parity_check(ctx) if rank == 0 else None
+    job.close()
+    batched = served = None
+    if rank == 0 and not args.no_legs and not args.dims:
+        batched = batched_leg(ctx, torch)
+        served = served_leg(torch)
     clocks = summarize_clocks(clk_path, physical_gpu_index(local_rank))
     if rank == 0:
         line = {
@@ -404,9 +519,10 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "parity": parity,
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(line))
-    job.close()
     ctx.close()
     if dist:
         dist.destroy_process_group()

@@ -361,6 +361,46 @@ def make_block(spec: BlockSpec) -> Block:
                  nsim=spec.nsim, seed=spec.seed)
 
 
+def make_block_fast(spec: BlockSpec) -> Block:
+    """Same shapes, operators and priors as make_block, with the seismic replaced by seeded
+    white noise of seismic amplitude (no prior realisation, no forward model).  The
+    inversion's cost does not depend on the data values, so throughput runs over many
+    blocks use this to keep input synthesis short."""
+    nxp, nyp, nzp = spec.padded()
+    nx, ny, nz = spec.nx, spec.ny, spec.nz
+    rng = np.random.default_rng(spec.seed)
+    nth = spec.ntheta
+    A = reflection_matrix(spec.theta_deg, spec.vsvp)
+    sd = np.asarray(spec.std, dtype=np.float64)
+    C = np.eye(3)
+    C[0, 1] = C[1, 0] = spec.corr[0]
+    C[0, 2] = C[2, 0] = spec.corr[1]
+    C[1, 2] = C[2, 1] = spec.corr[2]
+    P0 = (sd[:, None] * sd[None, :] * C).astype(np.float32).astype(np.float64)
+    cxy = corr_xy_surface(nxp, nyp, spec.dx, spec.dy, spec.lateral_range)
+    pct = prior_corr_t(nzp, spec.dt, spec.temporal_range)
+    low_int_cut = int(math.floor(spec.low_cut * (nzp * 0.001 * spec.dt)))
+    cct = circ_corr_t(pct, low_int_cut, nzp)
+    wav = np.stack([wavelet_fft_order(nzp, spec.dt, f) for f in spec.peak_hz])
+    wnorm = np.array([wavelet_norm(w) for w in wav], dtype=np.float32)
+    rnxp = 2 * (nxp // 2 + 1)
+    data = np.zeros((nth, nzp, nyp, rnxp), dtype=np.float32)
+    amp = np.float32(0.02)
+    for l in range(nth):
+        data[l, :, :, :nxp] = rng.standard_normal((nzp, nyp, nxp), dtype=np.float32) * amp
+    err_var = np.full(nth, float(amp) ** 2) / np.asarray(spec.sn, dtype=np.float64)
+    ang = angular_corr(spec.theta_deg, spec.angular[0], spec.angular[1]).astype(np.float32)
+    etc = (np.sqrt(err_var)[:, None] * np.sqrt(err_var)[None, :] * ang).astype(np.float32).astype(np.float64)
+    mean = np.zeros((3, nzp, nyp, rnxp), dtype=np.float32)
+    for a in range(3):
+        mean[a, :, :, :nxp] = np.float32(spec.mean[a])
+    return Block(spec=spec, nx=nx, ny=ny, nz=nz, nxp=nxp, nyp=nyp, nzp=nzp, lz=nz * spec.dt,
+                 A=A, err_theta_cov=etc, wavelet=wav, wavelet_norm=wnorm, prior_var0=P0,
+                 corr_xy=cxy, prior_corr_t=pct, circ_corr_t=cct, low_int_cut=low_int_cut,
+                 mean=mean, data=data, low_cut=spec.low_cut, high_cut=spec.high_cut,
+                 wnc=spec.wnc, nsim=spec.nsim, seed=spec.seed)
+
+
 # --- the configurations of the benchmark suite -------------------------------------
 
 def config0(seed: int = 11) -> BlockSpec:
@@ -389,6 +429,29 @@ def config3(seed: int = 31) -> BlockSpec:
     return BlockSpec(nx=768, ny=768, nz=320, theta_deg=th, peak_hz=(30.0,) * 6,
                      sn=tuple(np.linspace(2.0, 10.0, 6)), low_cut=2.0, high_cut=120.0,
                      nsim=1, seed=seed)
+
+
+def served_specs(n_jobs: int = 48, seed: int = 51, nsim: int = 16) -> list[BlockSpec]:
+    """Served stream: grids log-uniform between 64x64x64 and 512x512x256 voxels (2,3,5,7-
+    smooth), 3..6 angles, priors as the mixed-size batch."""
+    rng = np.random.default_rng(seed)
+    xy = np.array(smooth_sizes(64, 512))
+    zz = np.array(smooth_sizes(64, 256))
+    lo, hi = math.log(64 * 64 * 64), math.log(512 * 512 * 256)
+    base = config0()
+    out = []
+    for b in range(n_jobs):
+        target = math.exp(rng.uniform(lo, hi))
+        f = (target / (64 * 64 * 64)) ** (1.0 / 3.0)
+        nz = int(zz[np.argmin(np.abs(zz - min(256, 64 * f)))])
+        nxy = math.sqrt(target / nz)
+        nx = int(xy[np.argmin(np.abs(xy - nxy * rng.uniform(0.85, 1.15)))])
+        ny = int(xy[np.argmin(np.abs(xy - nxy * rng.uniform(0.85, 1.15)))])
+        nth = int(rng.integers(3, 7))
+        out.append(BlockSpec(nx=nx, ny=ny, nz=nz, theta_deg=tuple(np.linspace(5.0, 45.0, nth)),
+                             peak_hz=(30.0,) * nth, sn=(5.0,) * nth, std=base.std, corr=base.corr,
+                             nsim=nsim, seed=seed * 1000 + b))
+    return out
 
 
 def batch_specs(n_blocks: int = 64, seed: int = 41, nsim: int = 16,
