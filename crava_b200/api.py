@@ -64,6 +64,11 @@ class Counters(ctypes.Structure):
                 ("sim_chol_zero", ctypes.c_longlong), ("post_var0", ctypes.c_float * 9)]
 
 
+class FaciesDesc(ctypes.Structure):
+    _fields_ = [("nfacies", ctypes.c_int), ("nbins", ctypes.c_int * 3), ("vmin", ctypes.c_double * 3),
+                ("dv", ctypes.c_double * 3), ("prior", _fp), ("p_undefined", ctypes.c_float)]
+
+
 class RequestInfo(ctypes.Structure):
     _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("queue_ms", ctypes.c_double),
                 ("latency_ms", ctypes.c_double)]
@@ -111,6 +116,9 @@ def lib() -> ctypes.CDLL:
     L.crava_serve_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
     L.crava_serve_stop.argtypes = [vp]
     L.crava_invert_noalloc.argtypes = [ctypes.POINTER(JobDesc), ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
+    L.crava_facies_smooth.argtypes = [vp, ctypes.POINTER(FaciesDesc), ctypes.POINTER(ctypes.c_double), vp, vp]
+    L.crava_facies_prob.argtypes = [vp, ctypes.POINTER(FaciesDesc), vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     _lib = L
     return L
 
@@ -378,3 +386,28 @@ class Server:
             self.stop()
         except Exception:
             pass
+
+
+def facies_desc(prior, nbins, vmin, dv, p_undefined):
+    pr = np.ascontiguousarray(prior, dtype=np.float32)
+    fd = FaciesDesc()
+    fd.nfacies = len(pr)
+    for d in range(3):
+        fd.nbins[d], fd.vmin[d], fd.dv[d] = int(nbins[d]), float(vmin[d]), float(dv[d])
+    fd.prior = pr.ctypes.data_as(_fp)
+    fd.p_undefined = float(p_undefined)
+    return fd, pr
+
+
+def facies_smooth(ctx: Context, fd, sigma_inv, d_hist: int, stream=None):
+    """Gaussian smoothing of nfacies device histograms (FFTGrid layout) in place."""
+    S = np.ascontiguousarray(sigma_inv, dtype=np.float64)
+    _check(lib().crava_facies_smooth(ctx.handle, ctypes.byref(fd), S.ctypes.data_as(_dp), d_hist, stream))
+
+
+def facies_prob(ctx: Context, fd, d_density: int, density_row: int, d_post, nx, ny, nz, nxp, nyp, d_prob,
+                d_seis_lh=None, stream=None):
+    post = (ctypes.c_void_p * 3)(*d_post)
+    prob = (ctypes.c_void_p * len(d_prob))(*d_prob)
+    _check(lib().crava_facies_prob(ctx.handle, ctypes.byref(fd), d_density, density_row, post, nx, ny, nz, nxp, nyp,
+                                   prob, d_seis_lh, stream))

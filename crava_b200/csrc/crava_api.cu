@@ -1425,3 +1425,115 @@ crava_status crava_serve_stop(crava_server* sv) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Facies probabilities (FaciesProb::makeFaciesDens smoothing and calculateFaciesProb).
+
+extern "C" {
+
+crava_status crava_facies_smooth(crava_ctx* ctx, const crava_facies_desc* fd, const double* sigma_inv, float* d_hist,
+                                 void* stream) {
+  if (!ctx || !fd || !sigma_inv || !d_hist) return fail(CRAVA_EINVAL, "null argument");
+  const int na = fd->nbins[0], nb = fd->nbins[1], nr = fd->nbins[2];
+  if (fd->nfacies < 1 || fd->nfacies > kMaxFacies) return fail(CRAVA_EINVAL, "nfacies must be 1..16");
+  if (!smooth(na) || !smooth(nb) || !smooth(nr) || na < 2 || nb < 1 || nr < 2)
+    return fail(CRAVA_ENOTSUP, "density bins must be 2,3,5,7-smooth");
+  if (nb < 2) return fail(CRAVA_ENOTSUP, "a single Vs bin is not supported by the smoothing transform");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int rna = 2 * (na / 2 + 1);
+  const size_t gsize = (size_t)rna * nb * nr;
+  // Gaussian smoother with cyclic bin offsets, exp in float, normalised to unit sum
+  // (src/faciesprob.cpp:447-496)
+  std::vector<float> sm((size_t)na * nb * nr);
+  float sum = 0.0f;
+  const double dv0 = fd->dv[0], dv1 = fd->dv[1], dv2 = fd->dv[2];
+  const double* S = sigma_inv;
+  for (int l = 0; l < nr; l++) {
+    int ll = l <= nr / 2 ? l : l - nr;
+    for (int k = 0; k < nb; k++) {
+      int kk = k <= nb / 2 ? k : k - nb;
+      for (int j = 0; j < na; j++) {
+        int jj = j <= na / 2 ? j : j - na;
+        float factor = static_cast<float>(jj * dv0 * jj * dv0 * S[0] + kk * dv1 * kk * dv1 * S[4] +
+                                          ll * dv2 * ll * dv2 * S[8] + 2 * jj * dv0 * kk * dv1 * S[3] +
+                                          2 * jj * dv0 * ll * dv2 * S[6] + 2 * kk * dv1 * ll * dv2 * S[7]);
+        float v = std::exp(-0.5f * factor);
+        sm[j + (size_t)k * na + (size_t)l * na * nb] = v;
+        sum += v;
+      }
+    }
+  }
+  std::vector<float> g(gsize, 0.f);
+  for (int l = 0; l < nr; l++)
+    for (int k = 0; k < nb; k++)
+      for (int j = 0; j < na; j++) g[j + (size_t)rna * (k + (size_t)nb * l)] = sm[j + (size_t)k * na + (size_t)l * na * nb] / sum;
+  float* d_sm = nullptr;
+  CUDA_TRY(cudaMalloc(&d_sm, sizeof(float) * gsize));
+  crava_status s = CRAVA_OK;
+  cudaError_t e = cudaMemcpyAsync(d_sm, g.data(), sizeof(float) * gsize, cudaMemcpyHostToDevice, st);
+  // PARAMETER-scaled transforms: smoothed = IFFT(FFT(h)/sqrt(N) * FFT(s)/sqrt(N))/sqrt(N) * sqrt(N)
+  const size_t N = (size_t)na * nb * nr;
+  const float fs = fwd_scale(N);
+  std::vector<const float*> src;
+  std::vector<float*> gr;
+  std::vector<float> sc;
+  src.push_back(d_sm);
+  gr.push_back(d_sm);
+  sc.push_back(fs);
+  for (int f = 0; f < fd->nfacies; f++) {
+    src.push_back(d_hist + gsize * f);
+    gr.push_back(d_hist + gsize * f);
+    sc.push_back(fs);
+  }
+  if (e == cudaSuccess) s = fwd_xy(ctx, src, gr, sc, na, nb, nr, true, st);
+  else s = cuda_fail(e, "cudaMemcpyAsync");
+  const size_t nbins = (size_t)(na / 2 + 1) * nb * nr;
+  for (int f = 0; f < fd->nfacies && !s; f++) {
+    e = launch_spec_mul((float2*)(d_hist + gsize * f), (const float2*)d_sm, nbins, st);
+    if (e != cudaSuccess) s = cuda_fail(e, "spectrum product");
+  }
+  if (!s) {
+    std::vector<float*> out(gr.begin() + 1, gr.end());
+    const float is = inv_scale(N, false) * std::sqrt(static_cast<float>(N));
+    std::vector<float> osc(out.size(), is);
+    s = inv_xy(ctx, out, osc, na, nb, nr, true, st);
+  }
+  cudaStreamSynchronize(st);
+  cudaFree(d_sm);
+  return s;
+}
+
+crava_status crava_facies_prob(crava_ctx* ctx, const crava_facies_desc* fd, const float* d_density, int density_row,
+                               const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
+                               float* const* d_prob, float* d_seis_lh, void* stream) {
+  if (!ctx || !fd || !d_density || !d_post || !d_prob) return fail(CRAVA_EINVAL, "null argument");
+  if (fd->nfacies < 1 || fd->nfacies > kMaxFacies) return fail(CRAVA_EINVAL, "nfacies must be 1..16");
+  for (int d = 0; d < 3; d++)
+    if (fd->nbins[d] < 1 || !(fd->dv[d] > 0)) return fail(CRAVA_EINVAL, "bad density box");
+  if (nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny) return fail(CRAVA_EINVAL, "bad grid dimensions");
+  if (density_row < fd->nbins[0]) return fail(CRAVA_EINVAL, "density row stride below the vp bin count");
+  for (int f = 0; f <= fd->nfacies; f++)
+    if (!d_prob[f]) return fail(CRAVA_EINVAL, "null probability grid");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  FaciesBoxHost hb;
+  for (int d = 0; d < 3; d++) {
+    hb.nb[d] = fd->nbins[d];
+    hb.vmin[d] = fd->vmin[d];
+    hb.dv[d] = fd->dv[d];
+  }
+  hb.rs = density_row;
+  hb.fstride = (size_t)density_row * fd->nbins[1] * fd->nbins[2];
+  // FaciesProb::calculateFaciesProb: undefSum = p_undefined / (bins of the density volume)
+  const float undef_sum = fd->p_undefined / (float)(fd->nbins[0] * fd->nbins[1] * fd->nbins[2]);
+  const int rnxp_in = 2 * (nxp / 2 + 1), rnxp_out = 2 * (nx / 2 + 1);
+  CUDA_TRY(launch_facies_prob(d_post[0], d_post[1], d_post[2], nx, ny, nz, rnxp_in, nyp, rnxp_out, d_density, hb,
+                              fd->nfacies, fd->prior, undef_sum, d_prob, d_seis_lh, (cudaStream_t)stream));
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->launches += 1;
+  }
+  return CRAVA_OK;
+}
+
+}  // extern "C"

@@ -55,6 +55,17 @@ struct ZParams {
   unsigned long long* counters;    // [0] inverted bins [1] chol fallbacks [2] zero sim bins
 };
 
+constexpr int kMaxFacies = 16;
+struct FaciesPrior { float p[kMaxFacies]; };
+struct FaciesOut { float* p[kMaxFacies + 1]; };
+struct FaciesBoxHost {
+  int nb[3];
+  double vmin[3];
+  double dv[3];
+  int rs;
+  size_t fstride;
+};
+
 // launchers (kernels.cu)
 // x transforms: pl/tw are the plan and table of length nxp/2 (even nxp) or nxp (odd);
 // twn is the length-nxp table (its first nxp/2 entries are read; unused for odd nxp).
@@ -69,5 +80,11 @@ cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, in
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch);
 cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch);
 size_t zpass_smem_bytes(int W, int nzp, int nth);
+// facies.cu: prior[] and out[] are host arrays (copied into the launch parameters)
+cudaError_t launch_facies_prob(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz,
+                               int rnxp_in, int nyp_in, int rnxp_out, const float* dens, const FaciesBoxHost& hb,
+                               int nf, const float* prior, float undef_sum, float* const* out, float* seis_lh,
+                               cudaStream_t st);
+cudaError_t launch_spec_mul(float2* a, const float2* b, size_t n, cudaStream_t st);
 
 }  // namespace crava

@@ -158,6 +158,31 @@ long long crava_ctx_kernel_launches(crava_ctx* ctx);
 crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable);
 crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset);
 
+/* Facies probabilities from the posterior (FaciesProb, src/faciesprob.cpp).  A density
+ * volume per facies over (ln Vp, ln Vs, ln rho) with nbins (100, 100, 50 in the reference),
+ * lower edges vmin and bin widths dv (the Simbox makeFaciesDens builds, :428-441). */
+typedef struct {
+  int nfacies;            /* 1..16                                        */
+  int nbins[3];
+  double vmin[3];
+  double dv[3];
+  const float* prior;     /* nfacies prior probabilities (host)           */
+  float p_undefined;      /* probability mass of the undefined class       */
+} crava_facies_desc;
+/* Gaussian smoothing of the facies histograms in place (makeFaciesDens, :440-522):
+ * d_hist holds nfacies device grids in the FFTGrid layout of the density volume
+ * (2*(nbins[0]/2+1) floats per row); sigma_inv is the 3x3 inverse smoothing covariance. */
+crava_status crava_facies_smooth(crava_ctx* ctx, const crava_facies_desc* fd, const double* sigma_inv, float* d_hist,
+                                 void* stream);
+/* Per voxel, calculateFaciesProb / findDensity (:1909-2075, :1307-1423): trilinear density
+ * lookups at the posterior parameters d_post[3] (real grids, padded nxp x nyp), prior-
+ * weighted and normalised.  Outputs d_prob[nfacies+1] (the last is the undefined class) and
+ * optionally the seismic likelihood, each in the FFTGrid(nx,ny,nz) layout (2*(nx/2+1)
+ * floats per row, RMISSING in the padding).  density_row: floats per density row. */
+crava_status crava_facies_prob(crava_ctx* ctx, const crava_facies_desc* fd, const float* d_density, int density_row,
+                               const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
+                               float* const* d_prob, float* d_seis_lh, void* stream);
+
 /* Batches (no counterpart in the reference, which inverts one interval at a time,
  * main.cpp:217-353): the runs of n created jobs, of any sizes and angle counts, captured
  * once into a CUDA graph with `branches` concurrent branches; every crava_batch_run

@@ -377,3 +377,61 @@ def max_rel_err(x, ref) -> float:
     ref = np.asarray(ref, dtype=np.float64)
     den = np.max(np.abs(ref))
     return float(np.max(np.abs(x - ref)) / (den if den > 0 else 1.0))
+
+
+# ---------------------------------------------------------------- facies probabilities
+
+def facies_smoother(nbins, dv, sigma_inv):
+    """Normalised Gaussian smoother with cyclic bin offsets (FaciesProb::makeFaciesDens,
+    src/faciesprob.cpp:447-496), (nr, nb, na) array."""
+    na, nb, nr = nbins
+    cyc = lambda n: np.where(np.arange(n) <= n // 2, np.arange(n), np.arange(n) - n).astype(np.float64)
+    jj, kk, ll = cyc(na)[None, None, :] * dv[0], cyc(nb)[None, :, None] * dv[1], cyc(nr)[:, None, None] * dv[2]
+    S = np.asarray(sigma_inv, dtype=np.float64)
+    f = (jj * jj * S[0, 0] + kk * kk * S[1, 1] + ll * ll * S[2, 2] + 2 * jj * kk * S[1, 0] + 2 * jj * ll * S[2, 0]
+         + 2 * kk * ll * S[2, 1])
+    sm = np.exp(-0.5 * f)
+    return sm / sm.sum()
+
+
+def facies_smooth(hist, nbins, dv, sigma_inv):
+    """Circular convolution of each (nr, nb, na) histogram with the smoother, the effect
+    of fftInPlace / multiply / invFFTInPlace / x sqrt(N) in makeFaciesDens (:505-515)."""
+    sm = facies_smoother(nbins, dv, sigma_inv)
+    Fs = np.fft.rfftn(sm)
+    return np.stack([np.fft.irfftn(np.fft.rfftn(h) * Fs, s=h.shape, axes=(0, 1, 2)) for h in np.asarray(hist, dtype=np.float64)])
+
+
+def facies_prob(post, dens, nbins, vmin, dv, prior, p_undefined, nx, ny, nz):
+    """FaciesProb::calculateFaciesProb with findDensity (src/faciesprob.cpp:1909-2075,
+    1307-1423), one density volume per facies (no local-noise corners).
+    post: three real (nz, ny, >=nx) arrays of ln Vp, ln Vs, ln rho; dens: (nf, nr, nb, na).
+    Returns (nf+1, nz, ny, nx): facies probabilities and the undefined class."""
+    nf = len(prior)
+    v = [np.asarray(post[d][:nz, :ny, :nx], dtype=np.float64) for d in range(3)]
+    idx, w = [], []
+    for d in range(3):
+        f = (v[d] - vmin[d]) / dv[d] - 0.5
+        i1 = np.floor(f).astype(np.int64)
+        lo = i1 < 0
+        hi = i1 >= nbins[d] - 1
+        ww = np.where(lo | hi, 0.0, f - i1)
+        i1 = np.where(lo, 0, np.where(hi, nbins[d] - 1, i1))
+        i2 = np.where(lo | hi, i1, i1 + 1)
+        idx.append((i1, i2))
+        w.append(ww)
+    undef = p_undefined / float(nbins[0] * nbins[1] * nbins[2])
+    vals = []
+    for f in range(nf):
+        D = np.maximum(np.asarray(dens[f], dtype=np.float64), 0.0)
+        d = 0.0
+        for a in (0, 1):
+            wa = w[0] if a else 1 - w[0]
+            for b in (0, 1):
+                wb = w[1] if b else 1 - w[1]
+                for c in (0, 1):
+                    wc = w[2] if c else 1 - w[2]
+                    d = d + wa * wb * wc * D[idx[2][c], idx[1][b], idx[0][a]]
+        vals.append(prior[f] * np.maximum(d, 0.0))
+    s = undef + sum(vals)
+    return np.stack([x / s for x in vals] + [undef / s])

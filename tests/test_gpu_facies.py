@@ -1,0 +1,80 @@
+"""Facies probabilities on the GPU against the oracle restatement (norm-wise relative
+tolerance 5e-5 for the smoothed densities, an FP32 3D transform of up to 500k bins, and
+1e-5 for the probabilities)."""
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+from oracle import ref64
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("nbins", [(100, 100, 50), (20, 16, 10), (15, 12, 9)])
+def test_smoothing_matches_oracle(ctx, nbins):
+    import torch
+    rng = np.random.default_rng(sum(nbins))
+    nf = 3
+    na, nb, nr = nbins
+    rna = 2 * (na // 2 + 1)
+    hist = np.zeros((nf, nr, nb, na))
+    for f in range(nf):
+        idx = rng.integers(0, [nr, nb, na], size=(200, 3))
+        for l, k, j in idx:
+            hist[f, l, k, j] += 1.0 / 200
+    dv = (0.02, 0.03, 0.01)
+    sig = np.array([[0.003, 0.001, 0.0005], [0.001, 0.004, 0.0002], [0.0005, 0.0002, 0.001]])
+    S = np.linalg.inv(sig)
+    g = np.zeros((nf, nr, nb, rna), dtype=np.float32)
+    g[..., :na] = hist
+    d = torch.from_numpy(g).cuda()
+    fd, _k = api.facies_desc([0.4, 0.4, 0.2], nbins, (7.9, 7.0, 7.7), dv, 0.05)
+    api.facies_smooth(ctx, fd, S, d.data_ptr())
+    torch.cuda.synchronize()
+    got = d.cpu().numpy()[..., :na]
+    ref = ref64.facies_smooth(hist, nbins, dv, S)
+    assert rel(got, ref) < 5e-5
+
+
+def test_facies_prob_on_posterior_mean(ctx):
+    import torch
+    blk = synth.make_block(synth.config0())
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=3)
+    _k = job.upload_block()
+    job.run()
+    mean = [job.download(api.ROLE_POST_MEAN, a) for a in range(3)]
+    nbins = (100, 100, 50)
+    m = [x[..., :blk.nx] for x in mean]
+    vmin = [float(x.min()) - 0.05 for x in m]
+    dv = [(float(x.max()) + 0.05 - vmin[i]) / nbins[i] for i, x in enumerate(m)]
+    rng = np.random.default_rng(5)
+    nf = 4
+    dens = rng.random((nf, nbins[2], nbins[1], nbins[0])).astype(np.float32)
+    prior = [0.1, 0.2, 0.3, 0.4]
+    fd, _k2 = api.facies_desc(prior, nbins, vmin, dv, 0.02)
+    d_dens = torch.from_numpy(dens).cuda()
+    d_mean = [torch.from_numpy(x).cuda() for x in mean]
+    rnx = 2 * (blk.nx // 2 + 1)
+    outs = [torch.zeros((blk.nz, blk.ny, rnx), dtype=torch.float32, device="cuda") for _ in range(nf + 1)]
+    lh = torch.zeros((blk.nz, blk.ny, rnx), dtype=torch.float32, device="cuda")
+    api.facies_prob(ctx, fd, d_dens.data_ptr(), nbins[0], [t.data_ptr() for t in d_mean], blk.nx, blk.ny, blk.nz,
+                    blk.nxp, blk.nyp, [t.data_ptr() for t in outs], lh.data_ptr())
+    torch.cuda.synchronize()
+    got = np.stack([t.cpu().numpy()[..., :blk.nx] for t in outs])
+    ref = ref64.facies_prob(mean, dens, nbins, vmin, dv, prior, 0.02, blk.nx, blk.ny, blk.nz)
+    assert rel(got, ref) < 1e-5
+    assert np.allclose(got.sum(axis=0), 1.0, atol=1e-5)
+    pad = outs[0].cpu().numpy()[..., blk.nx:]
+    assert pad.size == 0 or np.all(pad == -99999.0)
+    job.close()
