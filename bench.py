@@ -343,26 +343,6 @@ def served_leg(torch, n_jobs=48, distinct=8, rate=20.0, nsim=16, max_inflight=8,
             "max_inflight": max_inflight, "budget_gb": budget_gb, **res}
 
 
-def parity_check(ctx):
-    """GPU vs the FP64 oracle on the 64x64x128 block (parity mode noise)."""
-    import numpy as np
-    from crava_b200 import api, synth
-    from oracle import bindings as ob
-    from oracle import ref64
-    blk = synth.make_block(synth.config0())
-    post = ref64.posterior(blk)
-    noise = ob.sim_noise(blk.seed, blk.nsim, blk.nxp, blk.nyp, blk.nzp)
-    out = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=noise)
-    nx = blk.nxp
-    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    em = max(rel(out["mean"][a][..., :nx], post.mean[a][..., :nx]) for a in range(3))
-    ec = max(rel(out["cov"][q][..., :nx], post.cov[q][..., :nx]) for q in range(6))
-    sim = ref64.simulate(blk, post, noise[0])
-    es = max(rel(out["sims"][0, a][..., :nx], sim[a][..., :nx]) for a in range(3))
-    return {"block": "64x64x128, 3 angles", "oracle": "fp64", "mean_rel_err": em, "cov_rel_err": ec,
-            "sim_rel_err": es}
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -486,7 +466,6 @@ def main():
     share = {c: round(kt[c][0] / max(sum(v[0] for v in kt.values()), 1e-9), 4) for c in kt}
     B_alg = 12 * blk.n_voxels * (nin + nout)
 
-    parity = parity_check(ctx) if rank == 0 else None
     job.close()
     batched = served = None
     if rank == 0 and not args.no_legs and not args.dims:
@@ -518,7 +497,6 @@ def main():
             "kernel_share": share,
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "parity": parity,
             "batched": batched,
             "served": served,
         }
