@@ -26,7 +26,7 @@ OK, EINVAL, ENOMEM, ECUDA, ETIMEDOUT, ENUMERIC, ENOTSUP, ESTATE = range(8)
 ROLE_DATA, ROLE_MEAN, ROLE_PRIOR_COV, ROLE_ERR_CORR, ROLE_POST_COV, ROLE_SIM, ROLE_NOISE, \
     ROLE_RESIDUAL, ROLE_POST_MEAN = range(9)
 PRIOR_SEPARABLE, PRIOR_GRIDS = 0, 1
-FLAG_HOST_NOISE, FLAG_KEEP_RESIDUAL = 1, 2
+FLAG_HOST_NOISE, FLAG_KEEP_RESIDUAL, FLAG_SPECTRAL_COV = 1, 2, 4
 
 # exported symbols the header declares (checked by the CPU tests)
 EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_status_string",
@@ -56,12 +56,13 @@ class JobDesc(ctypes.Structure):
                 ("A", _dp), ("err_theta_cov", _dp), ("wavelet", _fp), ("wavelet_norm", _fp),
                 ("prior_var0", _dp), ("prior_mode", ctypes.c_int), ("corr_xy", _fp),
                 ("circ_corr_t", _fp), ("nsim", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("flags", ctypes.c_int)]
+                ("flags", ctypes.c_int), ("fp64_threshold", ctypes.c_float)]
 
 
 class Counters(ctypes.Structure):
     _fields_ = [("inverted_bins", ctypes.c_longlong), ("chol_fallbacks", ctypes.c_longlong),
-                ("sim_chol_zero", ctypes.c_longlong), ("post_var0", ctypes.c_float * 9)]
+                ("sim_chol_zero", ctypes.c_longlong), ("fp64_bins", ctypes.c_longlong),
+                ("post_var0", ctypes.c_float * 9)]
 
 
 class FaciesDesc(ctypes.Structure):
@@ -165,7 +166,7 @@ class Context:
 
 
 def make_desc(blk, prior_mode: int = PRIOR_SEPARABLE, flags: int = 0, seed: Optional[int] = None,
-              nsim: Optional[int] = None):
+              nsim: Optional[int] = None, fp64_threshold: float = 0.0):
     """Job description of a synth.Block; returns (desc, keepalive arrays)."""
     keep = {
         "A": np.ascontiguousarray(blk.A, dtype=np.float64),
@@ -194,6 +195,7 @@ def make_desc(blk, prior_mode: int = PRIOR_SEPARABLE, flags: int = 0, seed: Opti
     d.nsim = blk.nsim if nsim is None else nsim
     d.seed = int(blk.seed if seed is None else seed) & ((1 << 64) - 1)
     d.flags = flags
+    d.fp64_threshold = float(fp64_threshold)
     return d, keep
 
 
@@ -208,13 +210,13 @@ class Job:
     """One inversion block on the device."""
 
     def __init__(self, ctx: Context, blk, prior_mode: int = PRIOR_SEPARABLE, flags: int = 0,
-                 seed: Optional[int] = None, nsim: Optional[int] = None):
+                 seed: Optional[int] = None, nsim: Optional[int] = None, fp64_threshold: float = 0.0):
         self.ctx = ctx
         self.blk = blk
         self.flags = flags
         self.prior_mode = prior_mode
         self.nsim = blk.nsim if nsim is None else nsim
-        desc, self._keep = make_desc(blk, prior_mode, flags, seed, nsim)
+        desc, self._keep = make_desc(blk, prior_mode, flags, seed, nsim, fp64_threshold)
         self._h = ctypes.c_void_p()
         _check(lib().crava_job_create(ctx.handle, ctypes.byref(desc), ctypes.byref(self._h)))
         self.shape = (blk.nzp, blk.nyp, 2 * (blk.nxp // 2 + 1))
@@ -245,7 +247,7 @@ class Job:
         c = Counters()
         _check(lib().crava_job_counters(self._h, ctypes.byref(c)))
         return {"inverted_bins": c.inverted_bins, "chol_fallbacks": c.chol_fallbacks,
-                "sim_chol_zero": c.sim_chol_zero,
+                "sim_chol_zero": c.sim_chol_zero, "fp64_bins": c.fp64_bins,
                 "post_var0": np.array(list(c.post_var0), dtype=np.float32).reshape(3, 3)}
 
     def upload_block(self, cov_grids=None, err_corr=None, noise=None):
@@ -273,8 +275,12 @@ class Job:
 
     def download_outputs(self) -> dict:
         blk = self.blk
-        out = {"mean": np.stack([self.download(ROLE_POST_MEAN, a) for a in range(3)]),
-               "cov": np.stack([self.download(ROLE_POST_COV, q) for q in range(6)])}
+        out = {"mean": np.stack([self.download(ROLE_POST_MEAN, a) for a in range(3)])}
+        cov = np.stack([self.download(ROLE_POST_COV, q) for q in range(6)])
+        if self.flags & FLAG_SPECTRAL_COV:
+            out["cov_spec"] = cov.view(np.complex64)
+        else:
+            out["cov"] = cov
         if self.nsim:
             out["sims"] = np.stack([self.download(ROLE_SIM, q) for q in range(3 * self.nsim)]).reshape(
                 (self.nsim, 3) + self.shape)
@@ -296,10 +302,11 @@ class Job:
 
 
 def invert_block(ctx: Context, blk, prior_mode=PRIOR_SEPARABLE, noise=None, keep_residual=False,
-                 cov_grids=None, err_corr=None, seed=None) -> dict:
+                 cov_grids=None, err_corr=None, seed=None, fp64_threshold=0.0, spectral_cov=False) -> dict:
     """Host-to-host inversion of one block (the e2e path): upload, run, download."""
-    flags = (FLAG_HOST_NOISE if noise is not None else 0) | (FLAG_KEEP_RESIDUAL if keep_residual else 0)
-    job = Job(ctx, blk, prior_mode, flags, seed=seed)
+    flags = (FLAG_HOST_NOISE if noise is not None else 0) | (FLAG_KEEP_RESIDUAL if keep_residual else 0) | \
+        (FLAG_SPECTRAL_COV if spectral_cov else 0)
+    job = Job(ctx, blk, prior_mode, flags, seed=seed, fp64_threshold=fp64_threshold)
     try:
         _keep = job.upload_block(cov_grids, err_corr, noise)
         job.run()

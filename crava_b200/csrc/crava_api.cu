@@ -149,6 +149,9 @@ struct crava_job {
   float* sim[3 * kMaxSim] = {};
   float* noise[3 * kMaxSim] = {};
   float2* kw = nullptr;
+  double2* kwd = nullptr;
+  double2* e1d = nullptr;
+  double2* e2d = nullptr;
   float2* e1 = nullptr;
   float2* e2 = nullptr;
   uint8_t* inv = nullptr;
@@ -223,6 +226,10 @@ crava_status validate(const crava_job_desc* d) {
     return fail(CRAVA_EINVAL, "unknown prior mode");
   }
   if (!(d->lz > 0)) return fail(CRAVA_EINVAL, "lz must be positive");
+  if (d->flags & ~(CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL | CRAVA_FLAG_SPECTRAL_COV))
+    return fail(CRAVA_EINVAL, "unknown flag");
+  if (!(d->fp64_threshold >= 0.f) || !(d->fp64_threshold < INFINITY))
+    return fail(CRAVA_EINVAL, "fp64_threshold must be finite and >= 0");
   for (int l = 0; l < d->ntheta; l++)
     if (!(d->wavelet_norm[l] > 0)) return fail(CRAVA_EINVAL, "wavelet norm must be positive");
   return CRAVA_OK;
@@ -234,7 +241,8 @@ size_t footprint(const crava_job_desc* d) {
   size_t ngrids = 2 * ((size_t)d->ntheta + 3) + 6 + 3 * (size_t)d->nsim;
   if (d->prior_mode == CRAVA_PRIOR_GRIDS) ngrids += 6 + 2;
   if (d->flags & CRAVA_FLAG_HOST_NOISE) ngrids += 3 * (size_t)d->nsim;
-  size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) + align256(d->nzp) +
+  size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) +
+                  3 * align256(sizeof(double2) * d->nzp * d->ntheta) + align256(d->nzp) +
                   align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float2) * d->nzp) +
                   align256(sizeof(float) * 2 * cnxp * d->nyp) + 256;
   return ngrids * gb + tables;
@@ -265,13 +273,20 @@ std::vector<cd> dft(const std::vector<double>& x) {
 }
 
 // Per-kz operator tables, constant-thickness branch of computePostMeanResidAndFFTCov.
+// With kwd/e1d/e2d given, the same three tables are also written in double.
 void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vector<float2>& e1,
-                     std::vector<float2>& e2, std::vector<uint8_t>& inv) {
+                     std::vector<float2>& e2, std::vector<uint8_t>& inv, std::vector<double2>* kwd = nullptr,
+                     std::vector<double2>* e1d = nullptr, std::vector<double2>* e2d = nullptr) {
   int n = d.nzp, nth = d.ntheta;
   kw.assign((size_t)n * nth, make_float2(0, 0));
   e1 = kw;
   e2 = kw;
   inv.assign(n, 0);
+  if (kwd) {
+    kwd->assign((size_t)n * nth, make_double2(0, 0));
+    *e1d = *kwd;
+    *e2d = *kwd;
+  }
   // diff1Operator: FIRSTORDERFORWARDDIFF, -1 at 0 and +1 at nzp-1 (src/wavelet1D.cpp:407-411)
   std::vector<double> d1(n, 0.0);
   d1[0] = -1.0;
@@ -303,6 +318,11 @@ void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vect
       kw[(size_t)k * nth + l] = make_float2((float)kwv.real(), (float)kwv.imag());
       e1[(size_t)k * nth + l] = make_float2((float)a.real(), (float)a.imag());
       e2[(size_t)k * nth + l] = make_float2((float)b.real(), (float)b.imag());
+      if (kwd) {
+        (*kwd)[(size_t)k * nth + l] = make_double2(kwv.real(), kwv.imag());
+        (*e1d)[(size_t)k * nth + l] = make_double2(a.real(), a.imag());
+        (*e2d)[(size_t)k * nth + l] = make_double2(b.real(), b.imag());
+      }
     }
   }
   // realFrequency and the inversion band (src/avoinversion.cpp:946, :1029)
@@ -591,6 +611,9 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->kw = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
   j->e1 = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
   j->e2 = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
+  j->kwd = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
+  j->e1d = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
+  j->e2d = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
   j->inv = (uint8_t*)take(d.nzp);
   j->cxy = (float2*)take(sizeof(float2) * j->cnxp * d.nyp);
   j->ct = (float2*)take(sizeof(float2) * d.nzp);
@@ -608,8 +631,12 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
 
   // per-kz tables
   std::vector<float2> kw, e1, e2;
+  std::vector<double2> kwd, e1d, e2d;
   std::vector<uint8_t> inv;
-  build_kz_tables(j->d, kw, e1, e2, inv);
+  build_kz_tables(j->d, kw, e1, e2, inv, &kwd, &e1d, &e2d);
+  JOB_TRY(cudaMemcpyAsync(j->kwd, kwd.data(), sizeof(double2) * kwd.size(), cudaMemcpyHostToDevice, st));
+  JOB_TRY(cudaMemcpyAsync(j->e1d, e1d.data(), sizeof(double2) * e1d.size(), cudaMemcpyHostToDevice, st));
+  JOB_TRY(cudaMemcpyAsync(j->e2d, e2d.data(), sizeof(double2) * e2d.size(), cudaMemcpyHostToDevice, st));
   JOB_TRY(cudaMemcpyAsync(j->kw, kw.data(), sizeof(float2) * kw.size(), cudaMemcpyHostToDevice, st));
   JOB_TRY(cudaMemcpyAsync(j->e1, e1.data(), sizeof(float2) * e1.size(), cudaMemcpyHostToDevice, st));
   JOB_TRY(cudaMemcpyAsync(j->e2, e2.data(), sizeof(float2) * e2.size(), cudaMemcpyHostToDevice, st));
@@ -703,7 +730,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   const crava_job_desc& d = job->d;
   cudaStream_t st = (cudaStream_t)stream;
   CUDA_TRY(cudaSetDevice(ctx->device));
-  CUDA_TRY(cudaMemsetAsync(job->counters, 0, 3 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(job->counters, 0, 4 * sizeof(unsigned long long), st));
   const bool grids = d.prior_mode == CRAVA_PRIOR_GRIDS;
   const float fs = fwd_scale(job->N);
   crava_status s;
@@ -751,6 +778,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.separable = grids ? 0 : 1;
   zp.host_noise = (d.flags & CRAVA_FLAG_HOST_NOISE) ? 1 : 0;
   zp.keep_resid = (d.flags & CRAVA_FLAG_KEEP_RESIDUAL) ? 1 : 0;
+  zp.cov_spectral = (d.flags & CRAVA_FLAG_SPECTRAL_COV) ? 1 : 0;
   for (int l = 0; l < d.ntheta; l++) zp.data[l] = (float2*)job->data[l];
   for (int a = 0; a < 3; a++) zp.mean[a] = (float2*)job->mean[a];
   for (int q = 0; q < 6; q++) zp.cov[q] = (float2*)job->cov[q];
@@ -769,6 +797,13 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     zp.ed[l] = float(d.wnc * job->etc[l * d.ntheta + l]);
   }
   zp.kz.kw = job->kw; zp.kz.e1 = job->e1; zp.kz.e2 = job->e2; zp.kz.inv = job->inv;
+  zp.kz.kwd = job->kwd; zp.kz.e1d = job->e1d; zp.kz.e2d = job->e2d;
+  zp.fp64_threshold = d.fp64_threshold;
+  for (int l = 0; l < d.ntheta; l++) {
+    for (int c = 0; c < 3; c++) zp.Ad[l][c] = job->A[l * 3 + c];
+    for (int m = 0; m < d.ntheta; m++) zp.ecd[l][m] = 0.5 * (1.0 - d.wnc) * job->etc[l * d.ntheta + m];
+    zp.edd[l] = d.wnc * job->etc[l * d.ntheta + l];
+  }
   zp.zp = pz->lp;
   zp.twz = pz->tw;
   zp.seed = d.seed;
@@ -785,7 +820,8 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     std::vector<float> sc;
     float ps = inv_scale(job->N, false), cs = inv_scale(job->N, true);
     for (int a = 0; a < 3; a++) { g.push_back(job->mean[a]); sc.push_back(ps); }
-    for (int q = 0; q < 6; q++) { g.push_back(job->cov[q]); sc.push_back(cs); }
+    if (!(d.flags & CRAVA_FLAG_SPECTRAL_COV))
+      for (int q = 0; q < 6; q++) { g.push_back(job->cov[q]); sc.push_back(cs); }
     for (int q = 0; q < 3 * d.nsim; q++) { g.push_back(job->sim[q]); sc.push_back(ps); }
     if ((s = inv_xy(ctx, g, sc, d.nxp, d.nyp, d.nzp, false, st))) return s;
   }
@@ -797,11 +833,12 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out) {
   if (!job || !out) return fail(CRAVA_EINVAL, "null argument");
   if (!job->ran) return fail(CRAVA_ESTATE, "counters are defined only after crava_job_run");
   CUDA_TRY(cudaSetDevice(job->ctx->device));
-  unsigned long long c[3];
+  unsigned long long c[4];
   CUDA_TRY(cudaMemcpy(c, job->counters, sizeof(c), cudaMemcpyDeviceToHost));
   out->inverted_bins = (long long)c[0];
   out->chol_fallbacks = (long long)c[1];
   out->sim_chol_zero = (long long)c[2];
+  out->fp64_bins = (long long)c[3];
   float v[6];
   for (int q = 0; q < 6; q++) CUDA_TRY(cudaMemcpy(&v[q], job->cov[q], sizeof(float), cudaMemcpyDeviceToHost));
   float P[9] = {v[0], v[3], v[4], v[3], v[1], v[5], v[4], v[5], v[2]};
@@ -894,7 +931,8 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   const crava_job_desc& d = *desc;
   if (d.prior_mode != CRAVA_PRIOR_SEPARABLE)
     return fail(CRAVA_ENOTSUP, "crava_invert_noalloc takes the separable prior only");
-  if (d.flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL))
+  if (d.fp64_threshold > 0.f) return fail(CRAVA_ENOTSUP, "crava_invert_noalloc runs FP32 only");
+  if (d.flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL | CRAVA_FLAG_SPECTRAL_COV))
     return fail(CRAVA_ENOTSUP, "crava_invert_noalloc supports neither host noise nor residual output");
   const int nin = d.ntheta + 3, nout = 9 + 3 * d.nsim;
   for (int q = 0; q < nin; q++)
@@ -929,7 +967,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   const size_t o_inv = take(d.nzp);
   const size_t o_cxy = take(sizeof(float) * rnxp * d.nyp);
   const size_t o_ct = take(sizeof(float2) * d.nzp);
-  const size_t o_cnt = take(3 * sizeof(unsigned long long));
+  const size_t o_cnt = take(4 * sizeof(unsigned long long));
   if (off > (size_t)CRAVA_NOALLOC_SCRATCH_BYTES)
     return fail(CRAVA_ENOTSUP, "block needs " + std::to_string(off) + " bytes of scratch; crava_invert_noalloc has " +
                                    std::to_string((size_t)CRAVA_NOALLOC_SCRATCH_BYTES));
@@ -960,7 +998,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   CUDA_TRY(put(o_inv, inv.data(), inv.size()));
   CUDA_TRY(put(o_ct, ct.data(), sizeof(float2) * ct.size()));
   CUDA_TRY(put(o_cxy, gxy.data(), sizeof(float) * gxy.size()));
-  CUDA_TRY(cudaMemsetAsync(base + o_cnt, 0, 3 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(base + o_cnt, 0, 4 * sizeof(unsigned long long), st));
   const float2* twx = (const float2*)(base + o_twx);
   const float2* twn = (const float2*)(base + o_twn);
   const float2* twy = (const float2*)(base + o_twy);

@@ -26,6 +26,9 @@ struct KzTables {
   const float2* e1;     // nzp x nth : conj(W_l(k)) / |w_l|
   const float2* e2;     // nzp x nth : conj(E3_l(k)) / |e3_l|
   const uint8_t* inv;   // nzp       : invert_frequency
+  const double2* kwd;   // the same three tables in double, read by the FP64
+  const double2* e1d;   //   re-factorisation of flagged bins
+  const double2* e2d;
 };
 
 struct ZParams {
@@ -35,6 +38,7 @@ struct ZParams {
   int separable;               // 1: prior from cxy/ct factors, 0: from spectral grids
   int host_noise;              // 1: noise from `noise` grids
   int keep_resid;              // 1: write residual spectra into data grids
+  int cov_spectral;            // 1: posterior covariance left as per-bin spectra
   int nxp_even;
   float2* data[kMaxTheta];
   float2* mean[3];
@@ -52,7 +56,12 @@ struct ZParams {
   LinePlan zp;
   const float2* twz;
   uint64_t seed;
+  float fp64_threshold;            // > 0: re-factorise flagged bins in FP64
+  double Ad[kMaxTheta][3];         // A, ec, ed in double for that path
+  double ecd[kMaxTheta][kMaxTheta];
+  double edd[kMaxTheta];
   unsigned long long* counters;    // [0] inverted bins [1] chol fallbacks [2] zero sim bins
+                                   // [3] bins re-factorised in FP64
 };
 
 constexpr int kMaxFacies = 16;

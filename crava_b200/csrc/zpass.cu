@@ -31,12 +31,14 @@ __device__ __forceinline__ uint4 philox4x32_7(uint4 c, uint2 k) {
   return c;
 }
 
+// Box-Muller with the hardware approximations of log, sine and cosine: their absolute
+// errors (about 2^-21 on these ranges) are far below what the normals' statistics can show.
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, float& n1) {
   float u1 = ((float)a + 0.5f) * 2.3283064365386963e-10f;
-  float u2 = (float)b * 2.3283064365386963e-10f;
-  float rad = sqrtf(-2.0f * logf(u1));
+  float u2 = ((float)b + 0.5f) * 2.3283064365386963e-10f - 0.5f;   // (-1/2, 1/2)
+  float rad = sqrtf(-2.0f * __logf(u1));
   float sn, cs;
-  sincospif(2.0f * u2, &sn, &cs);
+  __sincosf(6.283185307179586f * u2, &sn, &cs);   // angle in (-pi, pi)
   n0 = rad * cs;
   n1 = rad * sn;
 }
@@ -78,49 +80,44 @@ __device__ __forceinline__ void device_noise3(uint64_t seed, int s, int i, int j
 // ------------------------------------------------------------------ per-bin algebra
 
 // lib_matrCholCpx (libs/lib/lib_matr.c:78-168) on the lower triangle of a Hermitian
-// n x n matrix stored row-major in a[]: scale by a00, reject a00 <= 0, a scaled diagonal
-// <= 1e-20 or an updated pivot <= 1e-20, factor, rescale by sqrt(a00).
+// n x n matrix a[][]: the reference scales by a00, rejects a00 <= 0, a scaled diagonal
+// <= 1e-20 before its update or an updated pivot <= 1e-20, factors and rescales by
+// sqrt(a00).  Here the factor is computed unscaled with the two pivot tests applied as
+// a_ii > 1e-20 a00 (the same comparisons up to rounding), and each pivot's reciprocal
+// comes from one reciprocal square root.  No division.  The diagonal entry holds
+// (L_ii, 1 / L_ii): its imaginary part, zero for a Hermitian factor, carries the reciprocal.
 template <int N>
 __device__ __forceinline__ bool chol_ref(float2 (&a)[N][N]) {
-  const float TOLF = 1e-20f;
-  float f = a[0][0].x;
+  const float f = a[0][0].x;
   if (!(f > 0.f)) return false;
-#pragma unroll
-  for (int i = 0; i < N; i++)
-#pragma unroll
-    for (int j = 0; j <= i; j++) a[i][j] = make_float2(a[i][j].x / f, a[i][j].y / f);
+  const float tol = 1e-20f * f;
 #pragma unroll
   for (int i = 0; i < N; i++) {
-    if (!(a[i][i].x > TOLF)) return false;
+    if (!(a[i][i].x > tol)) return false;
 #pragma unroll
     for (int j = 0; j < i; j++) {
-      float2 s = make_float2(0.f, 0.f);
+      float2 s = a[i][j];
 #pragma unroll
-      for (int k = 0; k < j; k++) {  // L_ik conj(L_jk)
-        s.x += a[i][k].x * a[j][k].x + a[i][k].y * a[j][k].y;
-        s.y += -(a[i][k].x * a[j][k].y) + a[i][k].y * a[j][k].x;
+      for (int k = 0; k < j; k++) {  // - L_ik conj(L_jk)
+        s.x -= a[i][k].x * a[j][k].x + a[i][k].y * a[j][k].y;
+        s.y -= -(a[i][k].x * a[j][k].y) + a[i][k].y * a[j][k].x;
       }
-      float d = a[j][j].x;  // real pivot
-      a[i][j] = make_float2((a[i][j].x - s.x) / d, (a[i][j].y - s.y) / d);
+      a[i][j] = make_float2(s.x * a[j][j].y, s.y * a[j][j].y);
     }
-    float r = 0.f;
+    float r = a[i][i].x;
 #pragma unroll
-    for (int k = 0; k < i; k++) r += a[i][k].x * a[i][k].x + a[i][k].y * a[i][k].y;
-    r = a[i][i].x - r;
-    if (!(r > TOLF)) return false;
-    a[i][i] = make_float2(sqrtf(r), 0.f);
+    for (int k = 0; k < i; k++) r -= a[i][k].x * a[i][k].x + a[i][k].y * a[i][k].y;
+    if (!(r > tol)) return false;
+    const float rs = rsqrtf(r);
+    a[i][i] = make_float2(r * rs, rs);
   }
-  float sf = sqrtf(f);
-#pragma unroll
-  for (int i = 0; i < N; i++)
-#pragma unroll
-    for (int j = 0; j <= i; j++) a[i][j] = make_float2(a[i][j].x * sf, a[i][j].y * sf);
   return true;
 }
 
 struct BinOut {
   float2 mu[3];
   float2 sp[6];
+  float cond;   // (max / min Cholesky pivot)^2 of Sd, an estimate of its condition number
 };
 
 // Posterior of one bin.  Follows src/avoinversion.cpp:1036-1061 with
@@ -163,6 +160,15 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
     }
   }
   if (!chol_ref<NTH>(Sd)) return false;
+  {
+    float dmax = Sd[0][0].x, rmax = Sd[0][0].y;
+#pragma unroll
+    for (int l = 1; l < NTH; l++) {
+      dmax = fmaxf(dmax, Sd[l][l].x);
+      rmax = fmaxf(rmax, Sd[l][l].y);
+    }
+    o.cond = (dmax * rmax) * (dmax * rmax);
+  }
   // Y = L^{-1} KS, KS[l][j] = kw_l AS[l][j]
   float2 Y[NTH][3];
 #pragma unroll
@@ -172,8 +178,7 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
       float2 acc = make_float2(kw[l].x * AS[l][j], kw[l].y * AS[l][j]);
 #pragma unroll
       for (int m = 0; m < l; m++) acc = csub(acc, cmul(Sd[l][m], Y[m][j]));
-      float inv = 1.f / Sd[l][l].x;
-      Y[l][j] = make_float2(acc.x * inv, acc.y * inv);
+      Y[l][j] = make_float2(acc.x * Sd[l][l].y, acc.y * Sd[l][l].y);
     }
   }
   // S_post = S - Y^H Y
@@ -198,8 +203,7 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
     float2 acc = csub(d[l], cmul(kw[l], am));
 #pragma unroll
     for (int m = 0; m < l; m++) acc = csub(acc, cmul(Sd[l][m], yd[m]));
-    float inv = 1.f / Sd[l][l].x;
-    yd[l] = make_float2(acc.x * inv, acc.y * inv);
+    yd[l] = make_float2(acc.x * Sd[l][l].y, acc.y * Sd[l][l].y);
   }
 #pragma unroll
   for (int a = 0; a < 3; a++) {
@@ -222,6 +226,179 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
   return true;
 }
 
+// ------------------------------------------------------------------ FP64 re-factorisation
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// lib_matrCholCpx semantics (libs/lib/lib_matr.c:78-168) in double.
+template <int N>
+__device__ __forceinline__ bool chol_ref_d(double2 (&a)[N][N]) {
+  const double TOLD = 1e-20;
+  double f = a[0][0].x;
+  if (!(f > 0.0)) return false;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j <= i; j++) a[i][j] = make_double2(a[i][j].x / f, a[i][j].y / f);
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    if (!(a[i][i].x > TOLD)) return false;
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < j; k++) {
+        s.x += a[i][k].x * a[j][k].x + a[i][k].y * a[j][k].y;
+        s.y += -(a[i][k].x * a[j][k].y) + a[i][k].y * a[j][k].x;
+      }
+      double dd = a[j][j].x;
+      a[i][j] = make_double2((a[i][j].x - s.x) / dd, (a[i][j].y - s.y) / dd);
+    }
+    double r = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; k++) r += a[i][k].x * a[i][k].x + a[i][k].y * a[i][k].y;
+    r = a[i][i].x - r;
+    if (!(r > TOLD)) return false;
+    a[i][i] = make_double2(sqrt(r), 0.0);
+  }
+  double sf = sqrt(f);
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j <= i; j++) a[i][j] = make_double2(a[i][j].x * sf, a[i][j].y * sf);
+  return true;
+}
+
+// The per-bin posterior of bin_posterior re-done in double for a bin the FP32 pass flagged
+// as ill-conditioned, with one step of iterative refinement of the data solve
+// x = Sd^{-1} (d - K mu): x0 from the factor, r = (d - K mu) - Sd x0, x = x0 + Sd^{-1} r.
+// Out of line: only flagged bins call it, and only the REFINE instantiation of the pencil
+// kernel carries the call.
+template <int NTH>
+__device__ __noinline__ bool bin_posterior_fp64(const ZParams& P, int k, const float (&Sf)[6], float lamf,
+                                                const float2 (&mu)[3], float2 (&d)[NTH], BinOut& o) {
+  double2 kw[NTH], e1[NTH], e2[NTH];
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+    kw[l] = P.kz.kwd[k * NTH + l];
+    e1[l] = P.kz.e1d[k * NTH + l];
+    e2[l] = P.kz.e2d[k * NTH + l];
+  }
+  double S[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) S[q] = Sf[q];
+  const double lam = lamf;
+  double AS[NTH][3];
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+    AS[l][0] = P.Ad[l][0] * S[0] + P.Ad[l][1] * S[3] + P.Ad[l][2] * S[4];
+    AS[l][1] = P.Ad[l][0] * S[3] + P.Ad[l][1] * S[1] + P.Ad[l][2] * S[5];
+    AS[l][2] = P.Ad[l][0] * S[4] + P.Ad[l][1] * S[5] + P.Ad[l][2] * S[2];
+  }
+  double2 Sd[NTH][NTH], Sfull[NTH][NTH];
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+#pragma unroll
+    for (int m = 0; m <= l; m++) {
+      double g = AS[l][0] * P.Ad[m][0] + AS[l][1] * P.Ad[m][1] + AS[l][2] * P.Ad[m][2];
+      double2 kk = make_double2(kw[l].x * kw[m].x + kw[l].y * kw[m].y, kw[l].y * kw[m].x - kw[l].x * kw[m].y);
+      double c = P.ecd[l][m] * lam;
+      double2 ee = make_double2(e1[l].x * e1[m].x + e1[l].y * e1[m].y + e2[l].x * e2[m].x + e2[l].y * e2[m].y,
+                                e1[l].y * e1[m].x - e1[l].x * e1[m].y + e2[l].y * e2[m].x - e2[l].x * e2[m].y);
+      Sd[l][m] = make_double2(kk.x * g + c * ee.x, kk.y * g + c * ee.y);
+      if (l == m) Sd[l][m] = make_double2(Sd[l][m].x + P.edd[l], 0.0);
+      Sfull[l][m] = Sd[l][m];
+      Sfull[m][l] = make_double2(Sd[l][m].x, -Sd[l][m].y);
+    }
+  }
+  if (!chol_ref_d<NTH>(Sd)) return false;
+  // Y = L^{-1} K S, S_post = S - Y^H Y
+  double2 Y[NTH][3];
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      double2 acc = make_double2(kw[l].x * AS[l][j], kw[l].y * AS[l][j]);
+#pragma unroll
+      for (int m = 0; m < l; m++) acc = zsub(acc, zmul(Sd[l][m], Y[m][j]));
+      Y[l][j] = make_double2(acc.x / Sd[l][l].x, acc.y / Sd[l][l].x);
+    }
+  }
+  const int qa[6] = {0, 1, 2, 0, 0, 1}, qb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    double2 r = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+      r.x += Y[l][qa[q]].x * Y[l][qb[q]].x + Y[l][qa[q]].y * Y[l][qb[q]].y;
+      r.y += Y[l][qa[q]].x * Y[l][qb[q]].y - Y[l][qa[q]].y * Y[l][qb[q]].x;
+    }
+    o.sp[q] = make_float2((float)(S[q] - r.x), (float)(-r.y));
+  }
+  // b = d - K mu; x = Sd^{-1} b with one refinement step
+  double2 b[NTH], x[NTH], t[NTH];
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+    double2 am = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 3; j++) am = make_double2(am.x + P.Ad[l][j] * mu[j].x, am.y + P.Ad[l][j] * mu[j].y);
+    b[l] = zsub(make_double2(d[l].x, d[l].y), zmul(kw[l], am));
+  }
+  auto solve = [&](const double2 (&rhs)[NTH], double2 (&out)[NTH]) {
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+      double2 acc = rhs[l];
+#pragma unroll
+      for (int m = 0; m < l; m++) acc = zsub(acc, zmul(Sd[l][m], t[m]));
+      t[l] = make_double2(acc.x / Sd[l][l].x, acc.y / Sd[l][l].x);
+    }
+#pragma unroll
+    for (int l = NTH - 1; l >= 0; l--) {
+      double2 acc = t[l];
+#pragma unroll
+      for (int m = l + 1; m < NTH; m++) acc = zsub(acc, zmul(make_double2(Sd[m][l].x, -Sd[m][l].y), out[m]));
+      out[l] = make_double2(acc.x / Sd[l][l].x, acc.y / Sd[l][l].x);
+    }
+  };
+  solve(b, x);
+  double2 r[NTH], dx[NTH];
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+    double2 acc = b[l];
+#pragma unroll
+    for (int m = 0; m < NTH; m++) acc = zsub(acc, zmul(Sfull[l][m], x[m]));
+    r[l] = acc;
+  }
+  solve(r, dx);
+#pragma unroll
+  for (int l = 0; l < NTH; l++) x[l] = make_double2(x[l].x + dx[l].x, x[l].y + dx[l].y);
+  // mu_post = mu + (K S)^H x, residual d - K mu_post
+  double2 mp[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    double2 acc = make_double2(mu[a].x, mu[a].y);
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {  // conj(kw_l AS[l][a]) x_l
+      double2 ks = make_double2(kw[l].x * AS[l][a], -kw[l].y * AS[l][a]);
+      acc = make_double2(acc.x + ks.x * x[l].x - ks.y * x[l].y, acc.y + ks.x * x[l].y + ks.y * x[l].x);
+    }
+    mp[a] = acc;
+    o.mu[a] = make_float2((float)acc.x, (float)acc.y);
+  }
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+    double2 am = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 3; j++) am = make_double2(am.x + P.Ad[l][j] * mp[j].x, am.y + P.Ad[l][j] * mp[j].y);
+    double2 rr = zsub(make_double2(d[l].x, d[l].y), zmul(kw[l], am));
+    d[l] = make_float2((float)rr.x, (float)rr.y);
+  }
+  return true;
+}
+
 // ------------------------------------------------------------------ the fused z pass
 
 // Shared-memory layout of one pencil tile (W consecutive x-bins at one y, all nzp kz):
@@ -234,7 +411,9 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
 // Element (slot g, kz k, x-offset w) of R is R[(k * G + g) * W + w].
 
 
-template <int NTH>
+// REFINE instantiates the FP64 re-factorisation of flagged bins; the FP32-only kernel is
+// a separate instantiation so that its register allocation does not carry the call.
+template <int NTH, bool REFINE>
 __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P) {
   extern __shared__ float2 sm[];
   const int nzp = P.nzp, W = P.W, lw = P.logW;
@@ -245,7 +424,7 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   float2* R = tw + nzp;
   float2* S3 = R + G * TS;
   float2* SC = S3 + 3 * TS;
-  __shared__ unsigned long long cnt[3];
+  __shared__ unsigned long long cnt[4];
   const int T = blockDim.x, tid = threadIdx.x;
   const int it = blockIdx.x % P.nIT;
   const int j = blockIdx.x / P.nIT;
@@ -254,7 +433,7 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   const size_t kstride = (size_t)P.nyp * P.cnxp;
   const size_t base = (size_t)j * P.cnxp + i0;
 
-  if (tid < 3) cnt[tid] = 0;
+  if (tid < 4) cnt[tid] = 0;
   for (int t = tid; t < nzp; t += T) tw[t] = P.twz[t];
   // ---- load inputs: slot g <- data[g] (g < NTH) or mean[g - NTH]
 #pragma unroll 1
@@ -274,7 +453,7 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   }
 
   // ---- per-bin posterior (src/avoinversion.cpp:1016-1082)
-  unsigned long long n_inv = 0, n_fail = 0, n_zero_bins = 0;
+  unsigned long long n_inv = 0, n_fail = 0, n_zero_bins = 0, n_fp64 = 0;
   for (int b = tid; b < TS; b += T) {
     int k = b >> lw, w = b & (W - 1);
     if (w >= nw) continue;
@@ -311,6 +490,25 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     if (inv) {
       n_inv++;
       ok = bin_posterior<NTH>(P, k, S, lam, mu, d, o);
+      if constexpr (REFINE) {
+        if (ok) {
+          float ratio = 1.f;
+#pragma unroll
+          for (int a = 0; a < 3; a++)
+            if (S[a] > 0.f) ratio = fminf(ratio, o.sp[a].x / S[a]);
+          if (o.cond > P.fp64_threshold || ratio * P.fp64_threshold < 1.f) {
+            // the data are still in their slots: restart from them
+            float2 d64[NTH];
+#pragma unroll
+            for (int l = 0; l < NTH; l++) d64[l] = slot[l * W];
+            if (bin_posterior_fp64<NTH>(P, k, S, lam, mu, d64, o)) {
+              n_fp64++;
+#pragma unroll
+              for (int l = 0; l < NTH; l++) d[l] = d64[l];
+            }
+          }
+        }
+      }
       if (!ok) n_fail++;
     }
     if (!ok) {
@@ -414,9 +612,10 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     __syncthreads();
   }
 
-  // ---- inverse z transform of posterior covariance (slots 0..5) and mean (6..8)
+  // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
+  //      and mean (6..8)
 #pragma unroll 1
-  for (int g0 = 0; g0 < 9; g0 += 3)
+  for (int g0 = P.cov_spectral ? 6 : 0; g0 < 9; g0 += 3)
     fft_lines<true, 1>(R + g0 * W, SC, 3 * W, 1, G * W, P.zp, tw);
 #pragma unroll 1
   for (int g = 0; g < 9; g++) {
@@ -433,17 +632,20 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     n_inv += __shfl_down_sync(0xffffffffu, n_inv, off);
     n_fail += __shfl_down_sync(0xffffffffu, n_fail, off);
     n_zero += __shfl_down_sync(0xffffffffu, n_zero, off);
+    n_fp64 += __shfl_down_sync(0xffffffffu, n_fp64, off);
   }
   if ((tid & 31) == 0) {
     atomicAdd(&cnt[0], n_inv);
     atomicAdd(&cnt[1], n_fail);
     atomicAdd(&cnt[2], n_zero);
+    atomicAdd(&cnt[3], n_fp64);
   }
   __syncthreads();
   if (tid == 0 && P.counters) {
     atomicAdd(P.counters + 0, cnt[0]);
     atomicAdd(P.counters + 1, cnt[1]);
     atomicAdd(P.counters + 2, cnt[2]);
+    atomicAdd(P.counters + 3, cnt[3]);
   }
 }
 
@@ -454,14 +656,20 @@ size_t zpass_smem_bytes(int W, int nzp, int nth) {
   return sizeof(float2) * ((size_t)nzp + (size_t)(G + 6) * W * nzp);
 }
 
-template <int NTH>
-static cudaError_t launch_zpass_t(const ZParams& zp, int threads, cudaStream_t st) {
+template <int NTH, bool REFINE>
+static cudaError_t launch_zpass_r(const ZParams& zp, int threads, cudaStream_t st) {
   size_t smem = zpass_smem_bytes(zp.W, zp.nzp, zp.nth);
-  cudaError_t e = cudaFuncSetAttribute(k_zpass<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_zpass<NTH, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(zp.nIT * zp.nyp));
-  k_zpass<NTH><<<grid, threads, smem, st>>>(zp);
+  k_zpass<NTH, REFINE><<<grid, threads, smem, st>>>(zp);
   return cudaGetLastError();
+}
+
+template <int NTH>
+static cudaError_t launch_zpass_t(const ZParams& zp, int threads, cudaStream_t st) {
+  return zp.fp64_threshold > 0.f ? launch_zpass_r<NTH, true>(zp, threads, st)
+                                 : launch_zpass_r<NTH, false>(zp, threads, st);
 }
 
 cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch) {

@@ -76,7 +76,12 @@ enum {
 enum {
   CRAVA_FLAG_HOST_NOISE = 1,   /* realisation noise uploaded by the caller (parity with a
                                   sequential generator such as the reference RandomGen)   */
-  CRAVA_FLAG_KEEP_RESIDUAL = 2 /* keep the residual spectra for CRAVA_ROLE_RESIDUAL          */
+  CRAVA_FLAG_KEEP_RESIDUAL = 2, /* keep the residual spectra for CRAVA_ROLE_RESIDUAL         */
+  CRAVA_FLAG_SPECTRAL_COV = 4   /* leave the posterior covariance in the Fourier domain, as
+                                   the reference holds it between computePostMeanResidAndFFTCov
+                                   and invFFTCovGrids (src/avoinversion.cpp:1071-1077,
+                                   src/seismicparametersholder.cpp:432-456): CRAVA_ROLE_POST_COV
+                                   then reads complex cnxp*nyp*nzp per-bin S_post           */
 };
 
 /* One inversion block: the scalars and small arrays AVOInversion reads from ModelSettings,
@@ -100,12 +105,17 @@ typedef struct {
   int nsim;                    /* realisations                                 */
   uint64_t seed;               /* device noise seed (ignored with HOST_NOISE)  */
   int flags;                   /* CRAVA_FLAG_*                                 */
+  float fp64_threshold;        /* 0: FP32 only.  t > 0: a bin whose FP32 factorisation has
+                                  (max/min pivot)^2 of Sd > t, or S_post/S < 1/t on a
+                                  diagonal entry, is re-factorised in FP64 with one
+                                  iterative-refinement step of the data solve         */
 } crava_job_desc;
 
 typedef struct {
   long long inverted_bins;     /* bins inside (lowCut*minRelThick, highCut)    */
   long long chol_fallbacks;    /* inverted bins whose Cholesky failed: prior kept */
   long long sim_chol_zero;     /* realisation bins left at zero (simulate fallback) */
+  long long fp64_bins;         /* bins re-factorised in FP64 (fp64_threshold > 0)   */
   float post_var0[9];          /* SeismicParametersHolder::updatePriorVar after the run */
 } crava_counters;
 
@@ -227,7 +237,8 @@ crava_status crava_serve_stop(crava_server* sv);
  * loads the library keeps until the process exits.  The caller passes device grids:
  *   d_in  : ntheta data grids, then the 3 prior mean grids (real, read only);
  *   d_out : 3 posterior mean, 6 posterior covariance, 3*nsim realisations (real).
- * Separable prior only; no host noise, no residual output.  Blocks whose intermediates
+ * Separable prior only, FP32 only (fp64_threshold 0); no host noise, no residual or
+ * spectral covariance output.  Blocks whose intermediates
  * exceed the array return CRAVA_ENOTSUP.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress), so make that call before any stream
  * capture.  Every call shares the array: calls whose work overlaps on the GPU (other

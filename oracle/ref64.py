@@ -255,6 +255,53 @@ def param_cov_from_spectra(spec6, pv):
 
 # ---------------------------------------------------------------- the inversion
 
+def _data_system(K, e1, e2, e3, Sth, wnc, S, lam, k0, k1):
+    """K S and Sd = K S K^H + Sigma_e for kz in [k0, k1) (src/avoinversion.cpp:1036-1044
+    with getNextErrorVariance :1236-1272).  S (z,y,x,3,3), lam (z,y,x)."""
+    nth = K.shape[-2]
+    Kk = K[k0:k1][:, None, None]                      # (z,1,1,nth,3)
+    e1k = e1[k0:k1][:, None, None]
+    e2k = e2[k0:k1][:, None, None]
+    e3k = e3[k0:k1][:, None, None]
+    E = 0.5 * (1.0 - wnc) * Sth * lam[..., None, None] * (
+        e1k[..., :, None] * np.conj(e1k[..., None, :]) + e2k[..., :, None] * np.conj(e2k[..., None, :]))
+    E = E + np.eye(nth) * (wnc * np.diag(Sth) * np.abs(e3k) ** 2)[..., None, :]
+    KS = Kk @ S
+    Sd = KS @ np.conj(np.swapaxes(Kk, -1, -2)) + E
+    return Kk, KS, Sd
+
+
+def post_cov_given_inputs(blk, S6, lam, slab: int = 16):
+    """Posterior covariance spectra per bin, S_post = S - (KS)^H Sd^-1 KS, in FP64 from a
+    given prior covariance spectrum S6 (6, nzp, nyp, cnxp) real, order Vp, Vs, Rho, VpVs,
+    VpRho, VsRho, and error-correlation spectrum lam (nzp, nyp, cnxp), real >= 0: the
+    per-bin algebra of computePostMeanResidAndFFTCov (src/avoinversion.cpp:1036-1061)
+    without the transforms that make its inputs.  Returns (cov_spec (6, ...), ok) with ok
+    the bins that were inverted and factorised; the others keep S."""
+    K, e1, e2, e3, inv = per_kz_operators(blk)
+    Sth = blk.err_theta_cov
+    wnc = float(np.float32(blk.wnc))
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    nzp = S6.shape[1]
+    cs = np.zeros(S6.shape, dtype=np.complex128)
+    okall = np.zeros(S6.shape[1:], dtype=bool)
+    for k0 in range(0, nzp, slab):
+        k1 = min(nzp, k0 + slab)
+        S = np.zeros(S6[:, k0:k1].shape[1:] + (3, 3), dtype=np.complex128)
+        for g, (a, b) in enumerate(pairs):
+            S[..., a, b] = S6[g, k0:k1]
+            S[..., b, a] = S6[g, k0:k1]
+        _, KS, Sd = _data_system(K, e1, e2, e3, Sth, wnc, S, lam[k0:k1], k0, k1)
+        L, ok = chol_cpx(Sd)
+        ok &= np.broadcast_to(inv[k0:k1][:, None, None], ok.shape)
+        red = np.conj(np.swapaxes(KS, -1, -2)) @ chol_solve(L, KS)
+        Spost = np.where(ok[..., None, None], S - red, S)
+        for g, (a, b) in enumerate(pairs):
+            cs[g, k0:k1] = Spost[..., a, b]
+        okall[k0:k1] = ok
+    return cs, okall
+
+
 class Posterior:
     """Outputs of computePostMeanResidAndFFTCov + invFFTCovGrids, float64."""
 
@@ -291,15 +338,7 @@ def posterior(blk, slab: int = 16) -> Posterior:
         k1 = min(nzp, k0 + slab)
         S = param_cov_from_spectra([c[k0:k1] for c in cov_spec], blk.prior_var0)  # (z,y,x,3,3)
         lam = np.abs(err_spec[k0:k1].real)
-        Kk = K[k0:k1][:, None, None]                      # (z,1,1,nth,3)
-        e1k = e1[k0:k1][:, None, None]
-        e2k = e2[k0:k1][:, None, None]
-        e3k = e3[k0:k1][:, None, None]
-        E = 0.5 * (1.0 - wnc) * Sth * lam[..., None, None] * (
-            e1k[..., :, None] * np.conj(e1k[..., None, :]) + e2k[..., :, None] * np.conj(e2k[..., None, :]))
-        E = E + np.eye(nth) * (wnc * np.diag(Sth) * np.abs(e3k) ** 2)[..., None, :]
-        KS = Kk @ S
-        Sd = KS @ np.conj(np.swapaxes(Kk, -1, -2)) + E
+        Kk, KS, Sd = _data_system(K, e1, e2, e3, Sth, wnc, S, lam, k0, k1)
         L, ok = chol_cpx(Sd)
         invk = np.broadcast_to(inv[k0:k1][:, None, None], ok.shape)
         ok_eff = ok & invk

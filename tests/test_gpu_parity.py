@@ -136,6 +136,37 @@ def test_posterior_grids_with_gradients(ctx):
     _check_posterior(blk, out, post, post.n_inverted)
 
 
+def test_fp64_refine_every_bin_config0(ctx, block0, post0):
+    """fp64_threshold 1 flags (nearly) every inverted bin: the FP64 re-factorisation with
+    its refinement step reproduces the oracle like the FP32 path does."""
+    noise = ob.sim_noise(block0.seed, block0.nsim, block0.nxp, block0.nyp, block0.nzp)
+    out = api.invert_block(ctx, block0, api.PRIOR_SEPARABLE, noise=noise, keep_residual=True, fp64_threshold=1.0)
+    _check_posterior(block0, out, post0, post0.n_inverted)
+    assert out["counters"]["fp64_bins"] > 0.9 * post0.n_inverted
+    for l in range(block0.ntheta):
+        assert crel(out["resid_spec"][l], post0.resid_spec[l]) < 1e-3, ("resid", l)
+    sim = ref64.simulate(block0, post0, noise[0])
+    for a in range(3):
+        assert crel(out["sims"][0, a][..., :block0.nxp], sim[a][..., :block0.nxp]) < TOL_SIM
+
+
+def test_spectral_cov_matches_oracle_spectrum(ctx, block0, post0):
+    """CRAVA_FLAG_SPECTRAL_COV leaves S_post per bin, the oracle's cov_spec."""
+    job = api.Job(ctx, block0, api.PRIOR_SEPARABLE, api.FLAG_SPECTRAL_COV, nsim=0)
+    _keep = job.upload_block()
+    job.run()
+    out = job.download_outputs()
+    job.close()
+    for q in range(6):
+        assert crel(out["cov_spec"][q], post0.cov_spec[q]) < TOL_COV, q
+
+
+def test_descriptor_rejects_unknown_flag_and_bad_threshold(ctx, block0):
+    for kw in (dict(flags=64), dict(fp64_threshold=-1.0), dict(fp64_threshold=float("inf"))):
+        with pytest.raises(api.CravaError):
+            api.Job(ctx, block0, api.PRIOR_SEPARABLE, **kw)
+
+
 def test_device_noise_statistics(ctx, block0, post0):
     """Product-mode noise: each realisation's deviation from the posterior mean has, per
     voxel, the posterior variance (the covariance grids at lag 0)."""
