@@ -107,6 +107,9 @@ struct crava_ctx {
   std::vector<ProfRec> prof;
   double kt_ms[KT_COUNT] = {0, 0, 0, 0, 0};
   long long kt_n[KT_COUNT] = {0, 0, 0, 0, 0};
+  std::mutex stage_mu;         // device staging grid of the host-grid transforms
+  float* stage = nullptr;
+  size_t stage_bytes = 0;
 };
 
 namespace {
@@ -472,6 +475,7 @@ crava_status crava_ctx_destroy(crava_ctx* ctx) {
   if (!ctx) return CRAVA_OK;
   cudaSetDevice(ctx->device);
   for (auto& kv : ctx->plans) cudaFree(kv.second.tw);
+  if (ctx->stage) cudaFree(ctx->stage);
   delete ctx;
   return CRAVA_OK;
 }
@@ -761,14 +765,31 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   std::memset(&zp, 0, sizeof(zp));
   zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = job->cnxp;
   zp.nxp_even = (d.nxp % 2) == 0;
-  // pencil tile: W x-bins (power of two) and T threads; one resident CTA of 512 threads
-  // per SM unless two of 256 fit (CRAVA_ZPASS_W / CRAVA_ZPASS_T override)
-  int W = 4, T = 256;
-  if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 113 * 1024) T = 512;
-  while (W > 1 && zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) W /= 2;
+  // pencil tile: W x-bins (power of two), GT slots per z-transform call, SB realisations
+  // per batch and T threads.  Preferred: every slot of a phase in one call (GT = G,
+  // SB = 2) in two CTAs of 256 threads per SM; else one CTA of 512; else the three-slot
+  // layout.  CRAVA_ZPASS_{W,T,GT,SB} override.
+  const int Gs = std::max(d.ntheta + 3, 9);
+  int W = 2, T = 256, GT = Gs, SB = 2;
+  {
+    const int cand[6][3] = {{2, Gs, 2}, {4, Gs, 2}, {1, Gs, 2}, {4, 3, 1}, {2, 3, 1}, {1, 3, 1}};
+    for (const auto& c : cand) {
+      if (zpass_smem_bytes(c[0], d.nzp, d.ntheta, c[1], c[2]) <= 227 * 1024) {
+        W = c[0]; GT = c[1]; SB = c[2];
+        break;
+      }
+    }
+  }
   if (const char* ev = getenv("CRAVA_ZPASS_W")) W = std::max(1, atoi(ev));
+  if (const char* ev = getenv("CRAVA_ZPASS_GT")) GT = std::max(3, atoi(ev));
+  if (const char* ev = getenv("CRAVA_ZPASS_SB")) SB = std::max(1, atoi(ev));
+  SB = std::min(SB, GT / 3);
+  T = zpass_smem_bytes(W, d.nzp, d.ntheta, GT, SB) > 113 * 1024 ? 512 : 256;
   if (const char* ev = getenv("CRAVA_ZPASS_T")) T = std::max(64, atoi(ev));
-  if (zpass_smem_bytes(W, d.nzp, d.ntheta) > 227 * 1024) return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
+  if (zpass_smem_bytes(W, d.nzp, d.ntheta, GT, SB) > 227 * 1024)
+    return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
+  zp.GT = GT;
+  zp.SB = SB;
   zp.W = W;
   zp.logW = 0;
   while ((1 << zp.logW) < W) zp.logW++;
@@ -856,6 +877,37 @@ crava_status crava_fft_r2c(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int n
   std::vector<float*> g{dgrid};
   std::vector<float> sc{covariance ? 1.0f : fwd_scale(N)};
   return fwd_xy(ctx, src, g, sc, nxp, nyp, nzp, true, (cudaStream_t)stream);
+}
+
+// Host-resident grid: copied to the context's staging grid, transformed, copied back.
+static crava_status fft_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance, bool fwd) {
+  if (!ctx || !hgrid) return fail(CRAVA_EINVAL, "null argument");
+  if (!smooth(nxp) || !smooth(nyp) || !smooth(nzp) || nxp < 2 || nyp < 2 || nzp < 2)
+    return fail(CRAVA_ENOTSUP, "dimensions must be 2,3,5,7-smooth and >= 2");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const size_t bytes = sizeof(float) * 2 * (size_t)(nxp / 2 + 1) * nyp * nzp;
+  std::lock_guard<std::mutex> lk(ctx->stage_mu);
+  if (ctx->stage_bytes < bytes) {
+    if (ctx->stage) CUDA_TRY(cudaFree(ctx->stage));
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    CUDA_TRY(cudaMalloc(&ctx->stage, bytes));
+    ctx->stage_bytes = bytes;
+  }
+  CUDA_TRY(cudaMemcpy(ctx->stage, hgrid, bytes, cudaMemcpyHostToDevice));
+  crava_status s = fwd ? crava_fft_r2c(ctx, ctx->stage, nxp, nyp, nzp, covariance, nullptr)
+                       : crava_fft_c2r(ctx, ctx->stage, nxp, nyp, nzp, covariance, nullptr);
+  if (s) return s;
+  CUDA_TRY(cudaMemcpy(hgrid, ctx->stage, bytes, cudaMemcpyDeviceToHost));
+  return CRAVA_OK;
+}
+
+crava_status crava_fft_r2c_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance) {
+  return fft_host(ctx, hgrid, nxp, nyp, nzp, covariance, true);
+}
+
+crava_status crava_fft_c2r_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance) {
+  return fft_host(ctx, hgrid, nxp, nyp, nzp, covariance, false);
 }
 
 crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream) {

@@ -218,6 +218,228 @@ __global__ void __launch_bounds__(512, 2) k_line_fft(const __grid_constant__ Gri
   }
 }
 
+// ------------------------------------------------------------------ pipelined transforms
+//
+// Persistent forms of the transforms above: each CTA walks work units (row chunks, or
+// column tiles) with a stride of the grid size, and copies the next unit's input into a
+// second shared buffer with cp.async while it transforms the current one, so that loads
+// are in flight during the arithmetic.  Same arithmetic as the one-unit kernels.
+
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+}
+// zero-filling form: src_bytes 0 writes 8 zero bytes and reads nothing
+__device__ __forceinline__ void cp_async8_zfill(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Even nxp only.  Unit u = (grid u / nchunk, rows [c rpc, c rpc + rpc)).
+__global__ void __launch_bounds__(512, 2) k_x_r2c_pipe(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
+                                                     int nchunk, const __grid_constant__ LinePlan pl,
+                                                     const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  extern __shared__ float2 sm[];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int h = nxp / 2, cnxp = h + 1, np = h / 2 + 1;
+  const float rh = __frcp_rn((float)h), rnp = __frcp_rn((float)np), rchunk = __frcp_rn((float)nchunk);
+  float2* tw = sm;
+  float2* twh = tw + h;
+  float2* const tile0 = twh + h;
+  float2* const tile1 = tile0 + rpc * h;
+  float2* scr = tile1 + rpc * h;
+  for (int t = tid; t < h; t += T) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  const int units = gs.n * nchunk;
+  auto issue = [&](int u, float2* dst) {
+    int c;
+    const int gi = fdivmod(u, nchunk, rchunk, c);
+    const int row0 = c * rpc, nr = min(rpc, rows - row0);
+    const float2* src = reinterpret_cast<const float2*>(gs.src[gi]) + (size_t)row0 * cnxp;
+    const uint32_t d = smem_addr(dst);
+    for (int e = tid; e < nr * h; e += T) {
+      int m;
+      const int r = fdivmod(e, h, rh, m);
+      cp_async8(d + 8u * (uint32_t)e, src + (size_t)r * cnxp + m);
+    }
+  };
+  int i = 0;
+  if ((int)blockIdx.x < units) issue(blockIdx.x, tile0);
+  cp_async_commit();
+  for (int u = blockIdx.x; u < units; u += gridDim.x, i ^= 1) {
+    if (u + (int)gridDim.x < units) issue(u + gridDim.x, i ? tile0 : tile1);
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncthreads();
+    int c;
+    const int gi = fdivmod(u, nchunk, rchunk, c);
+    const int row0 = c * rpc, nr = min(rpc, rows - row0);
+    float2* buf = i ? tile1 : tile0;
+    fft_lines<false, -1, false>(buf, scr, nr, h, 1, pl, tw);
+    const float scale = gs.scale[gi];
+    float2* dst = reinterpret_cast<float2*>(gs.p[gi]) + (size_t)row0 * cnxp;
+    for (int e = tid; e < nr * np; e += T) {
+      int k;
+      const int r = fdivmod(e, np, rnp, k);
+      const float2* Z = buf + r * h;
+      float2* X = dst + (size_t)r * cnxp;
+      if (k == 0) {
+        const float2 z0 = Z[0];
+        X[0] = make_float2(scale * (z0.x + z0.y), 0.f);
+        X[h] = make_float2(scale * (z0.x - z0.y), 0.f);
+        continue;
+      }
+      const float2 A = Z[k], Bc = Z[h - k];
+      const float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y - Bc.y));
+      const float2 D = make_float2(A.x - Bc.x, A.y + Bc.y);
+      const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+      const float2 t = cmul(twh[k], O);
+      const float2 xk = cadd(E, t);
+      X[k] = make_float2(scale * xk.x, scale * xk.y);
+      if (2 * k != h) {
+        const float2 m = csub(E, t);
+        X[h - k] = make_float2(scale * m.x, -scale * m.y);
+      }
+    }
+    __syncthreads();  // the buffer is refilled by the prefetch of the next iteration but one
+  }
+  cp_async_wait_0();
+}
+
+// Even nxp only.  The raw half-spectrum rows land in tile0/tile1; the merge step writes the
+// length-h complex input of the inverse into buf.
+__global__ void __launch_bounds__(512, 2) k_x_c2r_pipe(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,
+                                                     int nchunk, const __grid_constant__ LinePlan pl,
+                                                     const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  extern __shared__ float2 sm[];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int h = nxp / 2, cnxp = h + 1, np = h / 2 + 1;
+  const float rc = __frcp_rn((float)cnxp), rnp = __frcp_rn((float)np), rchunk = __frcp_rn((float)nchunk);
+  float2* tw = sm;
+  float2* twh = tw + h;
+  float2* const tile0 = twh + h;
+  float2* const tile1 = tile0 + rpc * cnxp;
+  float2* buf = tile1 + rpc * cnxp;
+  float2* scr = buf + rpc * h;
+  for (int t = tid; t < h; t += T) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  const int units = gs.n * nchunk;
+  auto issue = [&](int u, float2* dst) {
+    int c;
+    const int gi = fdivmod(u, nchunk, rchunk, c);
+    const int row0 = c * rpc, nr = min(rpc, rows - row0);
+    const float2* src = reinterpret_cast<const float2*>(gs.p[gi]) + (size_t)row0 * cnxp;
+    const uint32_t d = smem_addr(dst);
+    for (int e = tid; e < nr * cnxp; e += T) cp_async8(d + 8u * (uint32_t)e, src + e);
+  };
+  int i = 0;
+  if ((int)blockIdx.x < units) issue(blockIdx.x, tile0);
+  cp_async_commit();
+  for (int u = blockIdx.x; u < units; u += gridDim.x, i ^= 1) {
+    if (u + (int)gridDim.x < units) issue(u + gridDim.x, i ? tile0 : tile1);
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncthreads();
+    int c;
+    const int gi = fdivmod(u, nchunk, rchunk, c);
+    const int row0 = c * rpc, nr = min(rpc, rows - row0);
+    const float2* xin = i ? tile1 : tile0;
+    for (int e = tid; e < nr * np; e += T) {
+      int k;
+      const int r = fdivmod(e, np, rnp, k);
+      const float2* X = xin + r * cnxp;
+      float2* Z = buf + r * h;
+      if (k == 0) {
+        const float a = X[0].x, b = X[h].x;
+        Z[0] = make_float2(a + b, a - b);
+        continue;
+      }
+      const float2 xk = X[k], xm = X[h - k];
+      const float2 P = make_float2(xk.x + xm.x, xk.y - xm.y);
+      const float2 M = make_float2(xk.x - xm.x, xk.y + xm.y);
+      const float2 w = twh[k];
+      const float2 Q = make_float2(M.x * w.x + M.y * w.y, M.y * w.x - M.x * w.y);
+      Z[k] = make_float2(P.x - Q.y, P.y + Q.x);
+      if (2 * k != h) Z[h - k] = make_float2(P.x + Q.y, -P.y + Q.x);
+    }
+    __syncthreads();
+    fft_lines<false, 1, false>(buf, scr, nr, h, 1, pl, tw);
+    const float scale = gs.scale[gi];
+    float2* dst = reinterpret_cast<float2*>(gs.p[gi]) + (size_t)row0 * cnxp;
+    for (int e = tid; e < nr * cnxp; e += T) {
+      int m;
+      const int r = fdivmod(e, cnxp, rc, m);
+      const float2 v = (m < h) ? buf[r * h + m] : make_float2(0.f, 0.f);
+      dst[e] = make_float2(v.x * scale, v.y * scale);
+    }
+    __syncthreads();
+  }
+  cp_async_wait_0();
+}
+
+// Unit u = (grid, outer index o, column tile it): W consecutive columns i0.. of the
+// n points at stride pstride; columns beyond ni are zero-filled and not stored.
+template <int DIR>
+__global__ void __launch_bounds__(512, 2) k_line_pipe(const __grid_constant__ GridSet gs, int ni, int n, size_t pstride,
+                                                    int no, size_t ostride, int W, int nIT,
+                                                    const __grid_constant__ LinePlan pl,
+                                                    const float2* __restrict__ twg) {
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* const tile0 = sm + n;
+  float2* const tile1 = tile0 + W * n;
+  float2* scr = tile1 + W * n;
+  const int T = blockDim.x, tid = threadIdx.x;
+  for (int t = tid; t < n; t += T) tw[t] = twg[t];
+  const int lw = 31 - __clz(W);
+  const int per_grid = nIT * no;
+  const float rpg = __frcp_rn((float)per_grid), rit = __frcp_rn((float)nIT);
+  const int units = gs.n * per_grid;
+  auto locate = [&](int u, int& gi, int& i0, int& nw) -> float2* {
+    int rem, it;
+    gi = fdivmod(u, per_grid, rpg, rem);
+    const int o = fdivmod(rem, nIT, rit, it);
+    i0 = it * W;
+    nw = min(W, ni - i0);
+    return reinterpret_cast<float2*>(gs.p[gi]) + (size_t)o * ostride + i0;
+  };
+  auto issue = [&](int u, float2* dst) {
+    int gi, i0, nw;
+    const float2* g = locate(u, gi, i0, nw);
+    const uint32_t d = smem_addr(dst);
+    for (int e = tid; e < n * W; e += T) {
+      const int p = e >> lw, w = e & (W - 1);
+      const bool ok = w < nw;
+      cp_async8_zfill(d + 8u * (uint32_t)e, ok ? g + (size_t)p * pstride + w : g, ok);
+    }
+  };
+  int i = 0;
+  if ((int)blockIdx.x < units) issue(blockIdx.x, tile0);
+  cp_async_commit();
+  for (int u = blockIdx.x; u < units; u += gridDim.x, i ^= 1) {
+    if (u + (int)gridDim.x < units) issue(u + gridDim.x, i ? tile0 : tile1);
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncthreads();
+    float2* buf = i ? tile1 : tile0;
+    fft_lines<true, DIR, false>(buf, scr, W, 1, W, pl, tw);
+    int gi, i0, nw;
+    float2* g = locate(u, gi, i0, nw);
+    for (int e = tid; e < n * W; e += T) {
+      const int p = e >> lw, w = e & (W - 1);
+      if (w < nw) g[(size_t)p * pstride + w] = buf[e];
+    }
+    __syncthreads();
+  }
+  cp_async_wait_0();
+}
+
 // ------------------------------------------------------------------ launchers
 
 static int round_threads(int t) {
@@ -225,10 +447,52 @@ static int round_threads(int t) {
   return t < 64 ? 64 : t;
 }
 
+static bool pipe_enabled() {
+  static const bool on = [] {
+    const char* ev = getenv("CRAVA_PIPE");
+    return !(ev && ev[0] == '0');
+  }();
+  return on;
+}
+
+// Persistent grid: resident CTAs of `fn` at (T, smem) on every SM of the current device,
+// no more than the work units.
+static cudaError_t persistent_grid(const void* fn, int T, size_t smem, int units, int* grid) {
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  *grid = std::max(1, std::min(units, per_sm * nsm));
+  return cudaSuccess;
+}
+
 static cudaError_t launch_x(bool fwd, const GridSet& gs, int nxp, int rows, const LinePlan& pl, const float2* tw,
                             const float2* twn, cudaStream_t st, int* nlaunch) {
   const bool even = (nxp & 1) == 0;
   const int n = even ? nxp / 2 : nxp;
+  if (even && pipe_enabled()) {
+    // rows per unit and threads: about 8 points per thread (CRAVA_X_PPT overrides)
+    int ppt = 8;
+    if (const char* ev = getenv("CRAVA_X_PPT")) ppt = std::max(1, atoi(ev));
+    int rpc = std::max(1, std::min(64, 2048 / n));
+    if (const char* ev = getenv("CRAVA_X_RPC")) rpc = std::max(1, atoi(ev));
+    const int T = std::min(512, round_threads((rpc * n + ppt - 1) / ppt));
+    const int h = n, cnxp = h + 1;
+    const size_t smem = fwd ? sizeof(float2) * (size_t)(2 * h + 3 * rpc * h)
+                            : sizeof(float2) * (size_t)(2 * h + 2 * rpc * cnxp + 2 * rpc * h);
+    const int nchunk = (rows + rpc - 1) / rpc;
+    const void* fn = fwd ? (const void*)k_x_r2c_pipe : (const void*)k_x_c2r_pipe;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int grid = 0;
+    if ((e = persistent_grid(fn, T, smem, gs.n * nchunk, &grid)) != cudaSuccess) return e;
+    if (fwd) k_x_r2c_pipe<<<grid, T, smem, st>>>(gs, nxp, rows, rpc, nchunk, pl, tw, twn);
+    else k_x_c2r_pipe<<<grid, T, smem, st>>>(gs, nxp, rows, rpc, nchunk, pl, tw, twn);
+    if (nlaunch) (*nlaunch)++;
+    return cudaGetLastError();
+  }
   // rows per CTA and threads: about 16 points per thread (CRAVA_X_PPT overrides)
   int ppt = 16;
   if (const char* ev = getenv("CRAVA_X_PPT")) ppt = std::max(1, atoi(ev));
@@ -267,6 +531,18 @@ cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, in
   if (const char* ev = getenv("CRAVA_LINE_TDIV")) tdiv = std::max(1, atoi(ev));
   int T = std::min(512, round_threads((W * n + tdiv - 1) / tdiv));
   int nIT = (ni + W - 1) / W;
+  if (pipe_enabled()) {
+    const size_t smem = sizeof(float2) * (size_t)(n + 3 * W * n);
+    const void* fn = sign < 0.f ? (const void*)k_line_pipe<-1> : (const void*)k_line_pipe<1>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int grid = 0;
+    if ((e = persistent_grid(fn, T, smem, gs.n * nIT * no, &grid)) != cudaSuccess) return e;
+    if (sign < 0.f) k_line_pipe<-1><<<grid, T, smem, st>>>(gs, ni, n, pstride, no, ostride, W, nIT, pl, tw);
+    else k_line_pipe<1><<<grid, T, smem, st>>>(gs, ni, n, pstride, no, ostride, W, nIT, pl, tw);
+    if (nlaunch) (*nlaunch)++;
+    return cudaGetLastError();
+  }
   size_t smem = sizeof(float2) * (size_t)(n + 2 * W * n);
   dim3 grid((unsigned)(nIT * no), gs.n);
   if (smem > 48 * 1024) {

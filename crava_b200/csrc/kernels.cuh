@@ -34,6 +34,7 @@ struct KzTables {
 struct ZParams {
   int nxp, nyp, nzp, cnxp;
   int W, logW, nIT;            // tile width in x-bins (power of two), log2 W, tiles per x-row
+  int GT, SB;                  // slots per z-transform call, realisations per batch (3 SB <= GT)
   int nth, nsim;
   int separable;               // 1: prior from cxy/ct factors, 0: from spectral grids
   int host_noise;              // 1: noise from `noise` grids
@@ -88,7 +89,8 @@ cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& p
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch);
 cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch);
-size_t zpass_smem_bytes(int W, int nzp, int nth);
+size_t zpass_smem_bytes(int W, int nzp, int nth);                  // GT = 3, SB = 1
+size_t zpass_smem_bytes(int W, int nzp, int nth, int GT, int SB);
 // facies.cu: prior[] and out[] are host arrays (copied into the launch parameters)
 cudaError_t launch_facies_prob(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz,
                                int rnxp_in, int nyp_in, int rnxp_out, const float* dens, const FaciesBoxHost& hb,

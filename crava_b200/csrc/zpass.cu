@@ -406,9 +406,9 @@ __device__ __noinline__ bool bin_posterior_fp64(const ZParams& P, int k, const f
 //   R   [nzp][G][W]       G = max(nth + 3, 9) slots per bin: inputs data 0..nth-1 and
 //                         mean nth..nth+2; after the per-bin step outputs S_post 0..5 and
 //                         mu_post 6..8 (each bin's slots are owned by the thread of that bin)
-//   S3  [nzp][3][W]       one realisation's three output spectra
-//   SC  [3 * W * nzp]     transform scratch for groups of up to three slots
-// Element (slot g, kz k, x-offset w) of R is R[(k * G + g) * W + w].
+//   SC  [GT * W * nzp]    transform scratch: the z transforms run GT slots per call
+//   S3  [nzp][3 SB][W]    the output spectra of SB realisations, transformed together
+// Element (slot g, kz k, x-offset w) of R is R[(k * G + g) * W + w].  3 SB <= GT.
 
 
 // REFINE instantiates the FP64 re-factorisation of flagged bins; the FP32-only kernel is
@@ -420,10 +420,11 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   const int TS = W * nzp;
   constexpr int G = NTH + 3 > 9 ? NTH + 3 : 9;
   constexpr int GIN = NTH + 3;
+  const int GT = P.GT, SB = P.SB;
   float2* tw = sm;
   float2* R = tw + nzp;
-  float2* S3 = R + G * TS;
-  float2* SC = S3 + 3 * TS;
+  float2* SC = R + G * TS;
+  float2* S3 = SC + GT * TS;
   __shared__ unsigned long long cnt[4];
   const int T = blockDim.x, tid = threadIdx.x;
   const int it = blockIdx.x % P.nIT;
@@ -445,10 +446,10 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     }
   }
   __syncthreads();
-  // forward z transforms, three slots per call
+  // forward z transforms, GT slots per call
 #pragma unroll 1
-  for (int g0 = 0; g0 < GIN; g0 += 3) {
-    int ng = min(3, GIN - g0);
+  for (int g0 = 0; g0 < GIN; g0 += GT) {
+    int ng = min(GT, GIN - g0);
     fft_lines<true, -1>(R + g0 * W, SC, ng * W, 1, G * W, P.zp, tw);
   }
 
@@ -548,50 +549,58 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   }
   __syncthreads();
 
-  // ---- realisations (src/avoinversion.cpp:1401-1511), mean added in the spectral domain
+  // ---- realisations (src/avoinversion.cpp:1401-1511), mean added in the spectral domain;
+  //      SB realisations per batch share one transform call
 #pragma unroll 1
-  for (int s = 0; s < P.nsim; s++) {
+  for (int s0 = 0; s0 < P.nsim; s0 += SB) {
+    const int nb = min(SB, P.nsim - s0);
+    const int SG = 3 * nb;  // slots of this batch
     for (int b = tid; b < TS; b += T) {
       int k = b >> lw, w = b & (W - 1);
-      float2* o3 = S3 + k * 3 * W + w;
+      float2* o3 = S3 + k * SG * W + w;
       if (w >= nw) {
-        o3[0] = o3[W] = o3[2 * W] = make_float2(0.f, 0.f);
+        for (int q = 0; q < SG; q++) o3[q * W] = make_float2(0.f, 0.f);
         continue;
       }
       int i = i0 + w;
       size_t gidx = base + (size_t)k * kstride + w;
       const float2* slot = R + k * G * W + w;
-      float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
       const float2 l0 = slot[0];
-      if (l0.y == -1.f) {
-        float2 z[3];
-        if (P.host_noise) {
+      const float2 m0 = slot[6 * W], m1 = slot[7 * W], m2 = slot[8 * W];
+#pragma unroll 1
+      for (int sb = 0; sb < nb; sb++) {
+        const int s = s0 + sb;
+        float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if (l0.y == -1.f) {
+          float2 z[3];
+          if (P.host_noise) {
 #pragma unroll
-          for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
-        } else {
-          device_noise3(P.seed, s, i, j, k, P.nyp, nzp, P.cnxp, P.nxp_even, z);
+            for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
+          } else {
+            device_noise3(P.seed, s, i, j, k, P.nyp, nzp, P.cnxp, P.nxp_even, z);
+          }
+          const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
+          sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
+          sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
+          sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
         }
-        const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
-        sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
-        sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
-        sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
+        o3[(3 * sb + 0) * W] = cadd(m0, sd[0]);
+        o3[(3 * sb + 1) * W] = cadd(m1, sd[1]);
+        o3[(3 * sb + 2) * W] = cadd(m2, sd[2]);
       }
-#pragma unroll
-      for (int a = 0; a < 3; a++) o3[a * W] = cadd(slot[(6 + a) * W], sd[a]);
     }
     __syncthreads();
-    fft_lines<true, 1>(S3, SC, 3 * W, 1, 3 * W, P.zp, tw);
+    fft_lines<true, 1>(S3, SC, SG * W, 1, SG * W, P.zp, tw);
 #pragma unroll 1
-    for (int a = 0; a < 3; a++) {
-      float2* dst = P.sim[3 * s + a] + base;
+    for (int q = 0; q < SG; q++) {
+      float2* dst = P.sim[3 * s0 + q] + base;
       for (int e = tid; e < TS; e += T) {
         int w = e & (W - 1), k = e >> lw;
-        if (w < nw) dst[(size_t)k * kstride + w] = S3[(k * 3 + a) * W + w];
+        if (w < nw) dst[(size_t)k * kstride + w] = S3[(k * SG + q) * W + w];
       }
     }
     __syncthreads();
   }
-
   // ---- rebuild S_post = L L^H where slots 0..5 hold the factor
   if (P.nsim > 0) {
     for (int b = tid; b < TS; b += T) {
@@ -615,8 +624,8 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
   //      and mean (6..8)
 #pragma unroll 1
-  for (int g0 = P.cov_spectral ? 6 : 0; g0 < 9; g0 += 3)
-    fft_lines<true, 1>(R + g0 * W, SC, 3 * W, 1, G * W, P.zp, tw);
+  for (int g0 = P.cov_spectral ? 6 : 0; g0 < 9; g0 += GT)
+    fft_lines<true, 1>(R + g0 * W, SC, min(GT, 9 - g0) * W, 1, G * W, P.zp, tw);
 #pragma unroll 1
   for (int g = 0; g < 9; g++) {
     float2* dst = (g < 6 ? P.cov[g] : P.mean[g - 6]) + base;
@@ -651,14 +660,16 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
 
 // ------------------------------------------------------------------ launchers
 
-size_t zpass_smem_bytes(int W, int nzp, int nth) {
+size_t zpass_smem_bytes(int W, int nzp, int nth, int GT, int SB) {
   int G = nth + 3 > 9 ? nth + 3 : 9;
-  return sizeof(float2) * ((size_t)nzp + (size_t)(G + 6) * W * nzp);
+  return sizeof(float2) * ((size_t)nzp + (size_t)(G + GT + 3 * SB) * W * nzp);
 }
+
+size_t zpass_smem_bytes(int W, int nzp, int nth) { return zpass_smem_bytes(W, nzp, nth, 3, 1); }
 
 template <int NTH, bool REFINE>
 static cudaError_t launch_zpass_r(const ZParams& zp, int threads, cudaStream_t st) {
-  size_t smem = zpass_smem_bytes(zp.W, zp.nzp, zp.nth);
+  size_t smem = zpass_smem_bytes(zp.W, zp.nzp, zp.nth, zp.GT, zp.SB);
   cudaError_t e = cudaFuncSetAttribute(k_zpass<NTH, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(zp.nIT * zp.nyp));
@@ -672,8 +683,12 @@ static cudaError_t launch_zpass_t(const ZParams& zp, int threads, cudaStream_t s
                                  : launch_zpass_r<NTH, false>(zp, threads, st);
 }
 
-cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch) {
+cudaError_t launch_zpass(const ZParams& zp_in, int threads, cudaStream_t st, int* nlaunch) {
+  ZParams zp = zp_in;
+  if (zp.GT <= 0) zp.GT = 3;  // unset: the three-slot layout
+  if (zp.SB <= 0) zp.SB = 1;
   if ((zp.W & (zp.W - 1)) || (1 << zp.logW) != zp.W) return cudaErrorInvalidValue;
+  if (3 * zp.SB > zp.GT) return cudaErrorInvalidValue;
   if (nlaunch) (*nlaunch)++;
   switch (zp.nth) {
     case 1: return launch_zpass_t<1>(zp, threads, st);

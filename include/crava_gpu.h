@@ -154,6 +154,11 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out);
  * covariance != 0 selects the COVARIANCE scaling. */
 crava_status crava_fft_r2c(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream);
 crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream);
+/* The same on a host-resident grid (the FFTGrid's own buffer, rnxp*nyp*nzp floats): the
+ * grid is staged through a device grid the context keeps, transformed, and copied back
+ * before the call returns.  Calls on one context serialise on that staging grid. */
+crava_status crava_fft_r2c_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance);
+crava_status crava_fft_c2r_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance);
 
 /* Kernels launched by this library since the context was created (all entry points). */
 long long crava_ctx_kernel_launches(crava_ctx* ctx);
