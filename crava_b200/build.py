@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrava_gpu.so")
-SOURCES = ["crava_api.cu", "kernels.cu", "zpass.cu", "facies.cu"]
-HEADERS = ["fft_core.cuh", "kernels.cuh"]
+SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "facies.cu"]
+HEADERS = ["fft_core.cuh", "fft2.cuh", "kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -56,6 +56,36 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libcrava_host.so")
+HOST_DEMO = os.path.join(HOST, "avo_host_demo")
+CXX = os.environ.get("CXX", "g++")
+
+
+def build_host(force: bool = False, verbose: bool = False) -> str:
+    """The C++ host layer (FFTGrid / AVOInversion over the C ABI) and its demo driver."""
+    inc = ["-I" + os.path.join(ROOT, "include"), "-I" + HOST]
+    steps = [
+        (HOST_LIB, [os.path.join(HOST, "crava_host.cpp"), os.path.join(HOST, "crava_host.h"), LIB],
+         [CXX, "-std=c++17", "-O2", "-fPIC", "-Wall", "-shared"] + inc +
+         [os.path.join(HOST, "crava_host.cpp"), "-L" + HERE, "-lcrava_gpu", "-Wl,-rpath,$ORIGIN", "-o", HOST_LIB]),
+        (HOST_DEMO, [os.path.join(HOST, "avo_host_demo.cpp"), os.path.join(HOST, "crava_host.h"), HOST_LIB],
+         [CXX, "-std=c++17", "-O2", "-Wall"] + inc +
+         [os.path.join(HOST, "avo_host_demo.cpp"), "-L" + HERE, "-lcrava_host", "-lcrava_gpu",
+          "-Wl,-rpath,$ORIGIN/..", "-o", HOST_DEMO]),
+    ]
+    for target, deps, cmd in steps:
+        if not force and not _newer(target, deps):
+            continue
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"host build failed for {target}:\n{r.stdout}\n{r.stderr}")
+    return HOST_LIB
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv)
+    build_host(force="--force" in sys.argv, verbose=True)
     print(LIB)

@@ -1,0 +1,313 @@
+// Four-step transform kernels for the lengths of the size table below (sm_100a): the
+// same transforms as k_x_r2c / k_x_c2r / k_line_fft (kernels.cu), with each line done in
+// two register-codelet passes (fft2.cuh) instead of one shared-memory stage per radix.
+//
+//   k_line4<N1,N2,DIR>  W columns of one strided line set: global -> pass 1 -> shared
+//                       -> pass 2 -> global
+//   k_xr2c4<N1,N2>      rows of even nxp, h = nxp/2 = N1 N2: global -> pass 1 -> shared
+//                       -> pass 2 -> shared (natural order) -> split -> global
+//   k_xc2r4<N1,N2>      global -> merge -> shared -> pass 1 -> pass 2 -> global
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdlib>
+
+#include "fft2.cuh"
+#include "kernels.cuh"
+
+namespace crava {
+
+// ------------------------------------------------------------------ strided lines
+//
+// Shared layout of the W lines: element (w, p = t + N2 m) at p W + w + m SK, with SK
+// chosen so that the pass-2 reads of neighbouring k2 fall on disjoint banks.
+template <int N1, int N2, int DIR>
+__global__ void __launch_bounds__(256) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
+                                               size_t ostride, int W, int lw, int nIT, int SK,
+                                               const float2* __restrict__ twg) {
+  constexpr int N = N1 * N2;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* Y = sm + N;
+  const int T = blockDim.x, tid = threadIdx.x;
+  for (int t = tid; t < N; t += T) tw[t] = twg[t];
+  const int it = blockIdx.x % nIT, o = blockIdx.x / nIT;
+  const int i0 = it * W, nw = min(W, ni - i0);
+  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)o * ostride + i0;
+  const size_t mstride = (size_t)N2 * pstride;
+  const int mpitch = N2 * W + SK;
+  __syncthreads();
+  for (int q = tid; q < W * N2; q += T) {
+    const int w = q & (W - 1), t = q >> lw;
+    const bool ok = w < nw;
+    const float2* src = g + (size_t)t * pstride + w;
+    float2* y = Y + t * W + w;
+    four_step_pass1<N1, N2, DIR>(
+        t, tw, [&](int, int m) { return ok ? src[m * mstride] : make_float2(0.f, 0.f); },
+        [&](int, int k2, float2 v) { y[k2 * mpitch] = v; });
+  }
+  __syncthreads();
+  for (int q = tid; q < W * N1; q += T) {
+    const int w = q & (W - 1), k2 = q >> lw;
+    const float2* y = Y + k2 * mpitch + w;
+    float2 v[N2];
+    four_step_pass2<N1, N2, DIR>(k2, [&](int, int t) { return y[t * W]; }, v);
+    if (w < nw) {
+      float2* dst = g + (size_t)k2 * pstride + w;
+#pragma unroll
+      for (int k1 = 0; k1 < N2; k1++) dst[(size_t)k1 * N1 * pstride] = v[k1];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ rows, even nxp
+//
+// Row r of a unit in shared memory at r * PITCH; pass-1 position t + N2 m at
+// t + m (N2 + SK) with SK = 1 for even N2 (odd stride for the pass-2 reads).
+template <int N1, int N2>
+struct RowLayout {
+  static constexpr int H = N1 * N2;
+  static constexpr int SK = (N2 % 2 == 0) ? 1 : 0;
+  static constexpr int PITCH = H + N1 * SK;
+  static __device__ __forceinline__ int pad(int t, int m) { return t + m * (N2 + SK); }
+};
+
+// Even nxp only; the split step as k_x_r2c (kernels.cu).
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_xr2c4(const __grid_constant__ GridSet gs, int rows, int rpc,
+                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  using L = RowLayout<N1, N2>;
+  constexpr int H = L::H, PITCH = L::PITCH;
+  constexpr int CN = H + 1, NP = H / 2 + 1;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* twh = tw + H;
+  float2* Z = twh + H;
+  const int T = blockDim.x, tid = threadIdx.x;
+  for (int t = tid; t < H; t += T) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
+  const float2* src = reinterpret_cast<const float2*>(gs.src[blockIdx.y]) + (size_t)row0 * CN;
+  float2* dst = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
+  const float scale = gs.scale[blockIdx.y];
+  __syncthreads();
+  for (int q = tid; q < nr * N2; q += T) {
+    const int r = q / N2, t = q - r * N2;
+    const float2* x = src + (size_t)r * CN + t;
+    float2* z = Z + r * PITCH;
+    four_step_pass1<N1, N2, -1>(
+        t, tw, [&](int, int m) { return x[m * N2]; }, [&](int, int k2, float2 v) { z[L::pad(t, k2)] = v; });
+  }
+  __syncthreads();
+  // pass 2: one item per thread (nr N1 <= T), outputs held across the barrier
+  float2 v[N2];
+  const int q = tid;
+  const bool have = q < nr * N1;
+  const int r2 = have ? q / N1 : 0, k2 = have ? q - r2 * N1 : 0;
+  if (have) {
+    const float2* z = Z + r2 * PITCH;
+    four_step_pass2<N1, N2, -1>(k2, [&](int k, int t) { return z[L::pad(t, k)]; }, v);
+  }
+  __syncthreads();
+  if (have) {
+    float2* z = Z + r2 * PITCH;
+#pragma unroll
+    for (int k1 = 0; k1 < N2; k1++) z[k2 + N1 * k1] = v[k1];
+  }
+  __syncthreads();
+  for (int e = tid; e < nr * NP; e += T) {
+    const int r = e / NP, k = e - r * NP;
+    const float2* Zr = Z + r * PITCH;
+    float2* X = dst + (size_t)r * CN;
+    if (k == 0) {
+      const float2 z0 = Zr[0];
+      X[0] = make_float2(scale * (z0.x + z0.y), 0.f);
+      X[H] = make_float2(scale * (z0.x - z0.y), 0.f);
+      continue;
+    }
+    const float2 A = Zr[k], Bc = Zr[H - k];
+    const float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y - Bc.y));
+    const float2 D = make_float2(A.x - Bc.x, A.y + Bc.y);
+    const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+    const float2 tt = cmul(twh[k], O);
+    const float2 xk = cadd(E, tt);
+    X[k] = make_float2(scale * xk.x, scale * xk.y);
+    if (2 * k != H) {
+      const float2 m = csub(E, tt);
+      X[H - k] = make_float2(scale * m.x, -scale * m.y);
+    }
+  }
+}
+
+// Even nxp only; the merge step as k_x_c2r (kernels.cu).
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet gs, int rows, int rpc,
+                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  using L = RowLayout<N1, N2>;
+  constexpr int H = L::H, PITCH = L::PITCH;
+  constexpr int CN = H + 1, NP = H / 2 + 1;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* twh = tw + H;
+  float2* Z = twh + H;
+  const int T = blockDim.x, tid = threadIdx.x;
+  for (int t = tid; t < H; t += T) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
+  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
+  const float scale = gs.scale[blockIdx.y];
+  __syncthreads();
+  for (int e = tid; e < nr * NP; e += T) {
+    const int r = e / NP, k = e - r * NP;
+    const float2* X = g + (size_t)r * CN;
+    float2* z = Z + r * PITCH;
+    if (k == 0) {
+      const float a = X[0].x, b = X[H].x;
+      z[0] = make_float2(a + b, a - b);
+      continue;
+    }
+    const float2 xk = X[k], xm = X[H - k];
+    const float2 P = make_float2(xk.x + xm.x, xk.y - xm.y);
+    const float2 M = make_float2(xk.x - xm.x, xk.y + xm.y);
+    const float2 w = twh[k];
+    const float2 Q = make_float2(M.x * w.x + M.y * w.y, M.y * w.x - M.x * w.y);
+    z[L::pad(k % N2, k / N2)] = make_float2(P.x - Q.y, P.y + Q.x);
+    if (2 * k != H) {
+      const int kk = H - k;
+      z[L::pad(kk % N2, kk / N2)] = make_float2(P.x + Q.y, -P.y + Q.x);
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < nr * N2; q += T) {
+    const int r = q / N2, t = q - r * N2;
+    float2* z = Z + r * PITCH;
+    four_step_pass1<N1, N2, 1>(
+        t, tw, [&](int, int m) { return z[L::pad(t, m)]; }, [&](int, int k2, float2 v) { z[L::pad(t, k2)] = v; });
+  }
+  __syncthreads();
+  for (int q = tid; q < nr * N1; q += T) {
+    const int r = q / N1, k2 = q - r * N1;
+    const float2* z = Z + r * PITCH;
+    float2 v[N2];
+    four_step_pass2<N1, N2, 1>(k2, [&](int k, int t) { return z[L::pad(t, k)]; }, v);
+    float2* X = g + (size_t)r * CN;
+#pragma unroll
+    for (int k1 = 0; k1 < N2; k1++) X[k2 + N1 * k1] = make_float2(v[k1].x * scale, v[k1].y * scale);
+    if (k2 == 0) X[H] = make_float2(0.f, 0.f);
+  }
+}
+
+// ------------------------------------------------------------------ size table and launchers
+
+// Lengths with a four-step split N = N1 N2 (N1 >= N2).
+#define CRAVA_FOUR_STEP_SIZES(X) \
+  X(32, 8, 4)                    \
+  X(64, 8, 8)                    \
+  X(128, 16, 8)                  \
+  X(135, 15, 9)                  \
+  X(160, 16, 10)                 \
+  X(256, 16, 16)                 \
+  X(270, 18, 15)                 \
+  X(320, 20, 16)                 \
+  X(384, 24, 16)                 \
+  X(512, 32, 16)                 \
+  X(540, 27, 20)                 \
+  X(768, 32, 24)                 \
+  X(1024, 32, 32)
+
+static bool four_step_enabled() {
+  static const bool on = [] {
+    const char* ev = getenv("CRAVA_FOUR_STEP");
+    return !(ev && ev[0] == '0');
+  }();
+  return on;
+}
+
+static int round_up32(int t) { return std::max(64, (t + 31) / 32 * 32); }
+
+template <int N1, int N2>
+static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size_t ostride, const float2* tw,
+                         float sign, cudaStream_t st) {
+  constexpr int N = N1 * N2;
+  int W = 8;
+  if (const char* ev = getenv("CRAVA_LINE4_W")) W = std::max(1, atoi(ev));
+  while (W > 1 && W / 2 >= ni) W /= 2;
+  int lw = 0;
+  while ((1 << lw) < W) lw++;
+  W = 1 << lw;
+  const int SK = W < 16 ? (((W - N2 * W) % 16) + 16) % 16 : 0;
+  const int T = std::min(256, round_up32(W * std::max(N1, N2)));
+  const int nIT = (ni + W - 1) / W;
+  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)W * N + (size_t)N1 * SK);
+  const void* fn = sign < 0.f ? (const void*)k_line4<N1, N2, -1> : (const void*)k_line4<N1, N2, 1>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)(nIT * no), gs.n);
+  if (sign < 0.f) k_line4<N1, N2, -1><<<grid, T, smem, st>>>(gs, ni, pstride, ostride, W, lw, nIT, SK, tw);
+  else k_line4<N1, N2, 1><<<grid, T, smem, st>>>(gs, ni, pstride, ostride, W, lw, nIT, SK, tw);
+  return cudaGetLastError();
+}
+
+template <int N1, int N2>
+static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, const float2* twn, cudaStream_t st) {
+  using L = RowLayout<N1, N2>;
+  const int T = 256;
+  int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
+  if (const char* ev = getenv("CRAVA_X4_RPC")) rpc = std::max(1, std::min(rpc, atoi(ev)));
+  const size_t smem = sizeof(float2) * (2 * (size_t)L::H + (size_t)rpc * L::PITCH);
+  const void* fn = fwd ? (const void*)k_xr2c4<N1, N2> : (const void*)k_xc2r4<N1, N2>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((rows + rpc - 1) / rpc), gs.n);
+  if (fwd) k_xr2c4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn);
+  else k_xc2r4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn);
+  return cudaGetLastError();
+}
+
+bool four_step_supported(int n) {
+  if (!four_step_enabled()) return false;
+  switch (n) {
+#define CRAVA_CASE(NN, A, B) case NN:
+    CRAVA_FOUR_STEP_SIZES(CRAVA_CASE)
+#undef CRAVA_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+cudaError_t launch_line4(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride, const float2* tw,
+                         float sign, cudaStream_t st, int* nlaunch) {
+  if (nlaunch) (*nlaunch)++;
+  switch (n) {
+#define CRAVA_CASE(NN, A, B) \
+  case NN:                   \
+    return line4<A, B>(gs, ni, pstride, no, ostride, tw, sign, st);
+    CRAVA_FOUR_STEP_SIZES(CRAVA_CASE)
+#undef CRAVA_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_x4(bool fwd, const GridSet& gs, int nxp, int rows, const float2* tw, const float2* twn,
+                      cudaStream_t st, int* nlaunch) {
+  if (nxp & 1) return cudaErrorInvalidValue;
+  if (nlaunch) (*nlaunch)++;
+  switch (nxp / 2) {
+#define CRAVA_CASE(NN, A, B) \
+  case NN:                   \
+    return x4<A, B>(fwd, gs, rows, tw, twn, st);
+    CRAVA_FOUR_STEP_SIZES(CRAVA_CASE)
+#undef CRAVA_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace crava

@@ -472,6 +472,7 @@ static cudaError_t launch_x(bool fwd, const GridSet& gs, int nxp, int rows, cons
                             const float2* twn, cudaStream_t st, int* nlaunch) {
   const bool even = (nxp & 1) == 0;
   const int n = even ? nxp / 2 : nxp;
+  if (even && four_step_supported(n)) return launch_x4(fwd, gs, nxp, rows, tw, twn, st, nlaunch);
   if (even && pipe_enabled()) {
     // rows per unit and threads: about 8 points per thread (CRAVA_X_PPT overrides)
     int ppt = 8;
@@ -523,6 +524,7 @@ cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& p
 
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch) {
+  if (four_step_supported(n)) return launch_line4(gs, ni, n, pstride, no, ostride, tw, sign, st, nlaunch);
   int W = 16;
   if (const char* ev = getenv("CRAVA_LINE_W")) W = std::max(1, atoi(ev));
   while (W > 1 && W * n > 8192) W /= 2;
@@ -531,7 +533,12 @@ cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, in
   if (const char* ev = getenv("CRAVA_LINE_TDIV")) tdiv = std::max(1, atoi(ev));
   int T = std::min(512, round_threads((W * n + tdiv - 1) / tdiv));
   int nIT = (ni + W - 1) / W;
-  if (pipe_enabled()) {
+  // the pipelined form measured slower for column tiles (fewer resident CTAs): opt-in
+  static const bool line_pipe = [] {
+    const char* ev = getenv("CRAVA_LINE_PIPE");
+    return ev && ev[0] == '1';
+  }();
+  if (line_pipe) {
     const size_t smem = sizeof(float2) * (size_t)(n + 3 * W * n);
     const void* fn = sign < 0.f ? (const void*)k_line_pipe<-1> : (const void*)k_line_pipe<1>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

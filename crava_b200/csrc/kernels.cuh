@@ -76,6 +76,13 @@ struct FaciesBoxHost {
   size_t fstride;
 };
 
+// four-step launchers (fft4.cu): lengths of its size table only
+bool four_step_supported(int n);
+cudaError_t launch_line4(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride, const float2* tw,
+                         float sign, cudaStream_t st, int* nlaunch);
+cudaError_t launch_x4(bool fwd, const GridSet& gs, int nxp, int rows, const float2* tw, const float2* twn,
+                      cudaStream_t st, int* nlaunch);
+
 // launchers (kernels.cu)
 // x transforms: pl/tw are the plan and table of length nxp/2 (even nxp) or nxp (odd);
 // twn is the length-nxp table (its first nxp/2 entries are read; unused for odd nxp).
