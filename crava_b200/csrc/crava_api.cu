@@ -791,6 +791,11 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.GT = GT;
   zp.SB = SB;
   zp.W = W;
+  {
+    const char* ev = getenv("CRAVA_ZPASS_FOUR");
+    const bool four = !(ev && ev[0] == '0') && GT >= Gs;
+    zp.zsplit = !four ? 0 : d.nzp == 256 ? 1 : d.nzp == 320 ? 2 : d.nzp == 128 ? 3 : 0;
+  }
   zp.logW = 0;
   while ((1 << zp.logW) < W) zp.logW++;
   zp.nIT = (job->cnxp + W - 1) / W;

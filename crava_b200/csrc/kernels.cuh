@@ -35,6 +35,7 @@ struct ZParams {
   int nxp, nyp, nzp, cnxp;
   int W, logW, nIT;            // tile width in x-bins (power of two), log2 W, tiles per x-row
   int GT, SB;                  // slots per z-transform call, realisations per batch (3 SB <= GT)
+  int zsplit;                  // four-step z transform: 0 none, 1 16x16, 2 20x16, 3 16x8
   int nth, nsim;
   int separable;               // 1: prior from cxy/ct factors, 0: from spectral grids
   int host_noise;              // 1: noise from `noise` grids

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 
+#include "fft2.cuh"
 #include "fft_core.cuh"
 #include "kernels.cuh"
 
@@ -411,6 +412,48 @@ __device__ __noinline__ bool bin_posterior_fp64(const ZParams& P, int k, const f
 // Element (slot g, kz k, x-offset w) of R is R[(k * G + g) * W + w].  3 SB <= GT.
 
 
+// z transform of nl lines of a pencil tile by the four-step passes (fft2.cuh): line l at
+// in + l, point p at in + l + p * ps; pass 1 in place, pass 2 into out at the same
+// offsets, so the result (natural order) is in out and in is overwritten.
+template <int N1, int N2, int DIR>
+__device__ __forceinline__ void zfft4(float2* in, float2* out, int nl, int ps, const float2* tw) {
+  const int T = blockDim.x;
+  const float rl = __frcp_rn((float)nl);
+  const int mstep = N2 * ps;
+  for (int q = threadIdx.x; q < nl * N2; q += T) {
+    int l;
+    const int t = fdivmod(q, nl, rl, l);
+    float2* x = in + l + t * ps;
+    four_step_pass1<N1, N2, DIR>(
+        t, tw, [&](int, int m) { return x[m * mstep]; }, [&](int, int k2, float2 v) { x[k2 * mstep] = v; });
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nl * N1; q += T) {
+    int l;
+    const int k2 = fdivmod(q, nl, rl, l);
+    const float2* y = in + l + k2 * mstep;
+    float2 v[N2];
+    four_step_pass2<N1, N2, DIR>(k2, [&](int, int t) { return y[t * ps]; }, v);
+    float2* o = out + l + k2 * ps;
+#pragma unroll
+    for (int k1 = 0; k1 < N2; k1++) o[k1 * N1 * ps] = v[k1];
+  }
+  __syncthreads();
+}
+
+// Four-step z transform for the lengths with a split (P.zsplit 1: 16x16, 2: 20x16,
+// 3: 16x8); returns false for the others.
+template <int DIR>
+__device__ __forceinline__ bool z_four_step(const ZParams& P, float2* in, float2* out, int nl, int ps,
+                                            const float2* tw) {
+  switch (P.zsplit) {
+    case 1: zfft4<16, 16, DIR>(in, out, nl, ps, tw); return true;
+    case 2: zfft4<20, 16, DIR>(in, out, nl, ps, tw); return true;
+    case 3: zfft4<16, 8, DIR>(in, out, nl, ps, tw); return true;
+    default: return false;
+  }
+}
+
 // REFINE instantiates the FP64 re-factorisation of flagged bins; the FP32-only kernel is
 // a separate instantiation so that its register allocation does not carry the call.
 template <int NTH, bool REFINE>
@@ -425,6 +468,8 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   float2* R = tw + nzp;
   float2* SC = R + G * TS;
   float2* S3 = SC + GT * TS;
+  // four-step z transforms write into the other G-slot buffer, which then takes over
+  const bool four = P.zsplit != 0 && GT >= G;
   __shared__ unsigned long long cnt[4];
   const int T = blockDim.x, tid = threadIdx.x;
   const int it = blockIdx.x % P.nIT;
@@ -447,10 +492,17 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   }
   __syncthreads();
   // forward z transforms, GT slots per call
+  if (four) {
+    z_four_step<-1>(P, R, SC, GIN * W, G * W, tw);
+    float2* t = R;
+    R = SC;
+    SC = t;
+  } else {
 #pragma unroll 1
-  for (int g0 = 0; g0 < GIN; g0 += GT) {
-    int ng = min(GT, GIN - g0);
-    fft_lines<true, -1>(R + g0 * W, SC, ng * W, 1, G * W, P.zp, tw);
+    for (int g0 = 0; g0 < GIN; g0 += GT) {
+      int ng = min(GT, GIN - g0);
+      fft_lines<true, -1>(R + g0 * W, SC, ng * W, 1, G * W, P.zp, tw);
+    }
   }
 
   // ---- per-bin posterior (src/avoinversion.cpp:1016-1082)
@@ -590,13 +642,19 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
       }
     }
     __syncthreads();
-    fft_lines<true, 1>(S3, SC, SG * W, 1, SG * W, P.zp, tw);
+    const float2* res = S3;
+    if (four) {
+      z_four_step<1>(P, S3, SC, SG * W, SG * W, tw);
+      res = SC;
+    } else {
+      fft_lines<true, 1>(S3, SC, SG * W, 1, SG * W, P.zp, tw);
+    }
 #pragma unroll 1
     for (int q = 0; q < SG; q++) {
       float2* dst = P.sim[3 * s0 + q] + base;
       for (int e = tid; e < TS; e += T) {
         int w = e & (W - 1), k = e >> lw;
-        if (w < nw) dst[(size_t)k * kstride + w] = S3[(k * SG + q) * W + w];
+        if (w < nw) dst[(size_t)k * kstride + w] = res[(k * SG + q) * W + w];
       }
     }
     __syncthreads();
@@ -623,15 +681,21 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
 
   // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
   //      and mean (6..8)
+  const int gs0 = P.cov_spectral ? 6 : 0;
+  if (four) {
+    z_four_step<1>(P, R + gs0 * W, SC + gs0 * W, (9 - gs0) * W, G * W, tw);
+  } else {
 #pragma unroll 1
-  for (int g0 = P.cov_spectral ? 6 : 0; g0 < 9; g0 += GT)
-    fft_lines<true, 1>(R + g0 * W, SC, min(GT, 9 - g0) * W, 1, G * W, P.zp, tw);
+    for (int g0 = gs0; g0 < 9; g0 += GT)
+      fft_lines<true, 1>(R + g0 * W, SC, min(GT, 9 - g0) * W, 1, G * W, P.zp, tw);
+  }
 #pragma unroll 1
   for (int g = 0; g < 9; g++) {
     float2* dst = (g < 6 ? P.cov[g] : P.mean[g - 6]) + base;
+    const float2* src = (four && g >= gs0) ? SC : R;
     for (int e = tid; e < TS; e += T) {
       int w = e & (W - 1), k = e >> lw;
-      if (w < nw) dst[(size_t)k * kstride + w] = R[(k * G + g) * W + w];
+      if (w < nw) dst[(size_t)k * kstride + w] = src[(k * G + g) * W + w];
     }
   }
 

@@ -97,3 +97,16 @@ def test_missing_library_raises(monkeypatch):
     monkeypatch.setattr(api, "LIB_PATH", "/nonexistent/libcrava_gpu.so")
     with pytest.raises(api.CravaError):
         api.lib()
+
+
+def test_host_layer_built_and_exports_the_reference_entry_points():
+    """The C++ host layer keeps the reference's class and method names."""
+    import subprocess
+    lib = os.path.join(os.path.dirname(api.LIB_PATH), "libcrava_host.so")
+    assert os.path.exists(lib), "run python -m crava_b200.build"
+    syms = subprocess.run(["nm", "-DC", lib], capture_output=True, text=True, check=True).stdout
+    for name in ("crava_b200::FFTGrid::fftInPlace()", "crava_b200::FFTGrid::invFFTInPlace()",
+                 "crava_b200::AVOInversion::computePostMeanResidAndFFTCov()",
+                 "crava_b200::AVOInversion::simulate(", "crava_b200::FFTGrid::getNextComplex()",
+                 "crava_b200::FFTGrid::setRealValue("):
+        assert name in syms, name

@@ -1,0 +1,109 @@
+"""The C++ host layer (crava_b200/host: FFTGrid / AVOInversion over the C ABI) against the
+FP64 oracle, through its demo driver: DATA and PARAMETER grids go in as FFTGrid objects,
+computePostMeanResidAndFFTCov and simulate run, and the posterior is read back from the
+same grids, as the reference's AVOInversion leaves it.
+
+Tolerances (norm-wise relative): posterior mean 1e-4, covariance 1e-3, realisations 1e-4,
+residual spectra 2e-3 (a residual is a small difference of FP32 spectra, so its relative
+error is larger than the mean's); Cholesky fallbacks and inverted bins exactly.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from crava_b200 import synth
+from oracle import bindings as ob
+from oracle import ref64
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DEMO = os.path.join(ROOT, "crava_b200", "host", "avo_host_demo")
+
+
+def crel(x, ref):
+    x = np.asarray(x, dtype=np.complex128)
+    ref = np.asarray(ref, dtype=np.complex128)
+    return float(np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300))
+
+
+def write_block(path, blk, grids, noise):
+    rnxp = 2 * (blk.nxp // 2 + 1)
+    shape = (blk.nzp, blk.nyp, rnxp)
+
+    def padded(a):
+        g = np.zeros(shape, dtype=np.float32)
+        g[..., :a.shape[-1]] = a
+        return g
+
+    with open(path, "wb") as f:
+        np.array([blk.nx, blk.ny, blk.nz, blk.nxp, blk.nyp, blk.nzp, blk.ntheta, blk.nsim,
+                  1 if grids else 0, 1 if noise is not None else 0], dtype=np.int32).tofile(f)
+        np.array([blk.seed], dtype=np.uint64).tofile(f)
+        np.array([blk.lz, blk.min_rel_thick, blk.low_cut, blk.high_cut, blk.wnc], dtype=np.float64).tofile(f)
+        np.asarray(blk.A, dtype=np.float64).tofile(f)
+        np.asarray(blk.err_theta_cov, dtype=np.float64).tofile(f)
+        np.asarray(blk.prior_var0, dtype=np.float64).tofile(f)
+        np.asarray(blk.wavelet, dtype=np.float32).tofile(f)
+        np.asarray(blk.wavelet_norm, dtype=np.float32).tofile(f)
+        if grids:
+            covs, _ = ref64.prior_cov_grids(blk)
+            for c in covs:
+                padded(c).tofile(f)
+            padded(ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)).tofile(f)
+        else:
+            np.asarray(blk.corr_xy, dtype=np.float32).tofile(f)
+            np.asarray(blk.circ_corr_t, dtype=np.float32).tofile(f)
+        for l in range(blk.ntheta):
+            np.asarray(blk.data[l], dtype=np.float32).tofile(f)
+        for a in range(3):
+            np.asarray(blk.mean[a], dtype=np.float32).tofile(f)
+        if noise is not None:
+            np.ascontiguousarray(noise, dtype=np.complex64).tofile(f)
+
+
+def read_out(path, blk):
+    rnxp = 2 * (blk.nxp // 2 + 1)
+    rs = blk.nzp * blk.nyp * rnxp
+    shape = (blk.nzp, blk.nyp, rnxp)
+    with open(path, "rb") as f:
+        grids = np.fromfile(f, dtype=np.float32, count=rs * (9 + 3 * blk.nsim + blk.ntheta))
+        cnt = np.fromfile(f, dtype=np.int64, count=4)
+        pv = np.fromfile(f, dtype=np.float32, count=9)
+        rt = np.fromfile(f, dtype=np.float32, count=1)
+    grids = grids.reshape((-1,) + shape)
+    return {"mean": grids[:3], "cov": grids[3:9], "sims": grids[9:9 + 3 * blk.nsim].reshape((blk.nsim, 3) + shape),
+            "resid": grids[9 + 3 * blk.nsim:].view(np.complex64), "counters": cnt, "post_var0": pv,
+            "fft_roundtrip": float(rt[0])}
+
+
+@pytest.mark.parametrize("grids", [False, True])
+def test_host_layer_matches_oracle(tmp_path, grids):
+    assert os.path.exists(DEMO), "crava_b200/host/avo_host_demo is not built (python -m crava_b200.build)"
+    blk = synth.make_block(synth.BlockSpec(nx=30, ny=28, nz=40, theta_deg=(8.0, 20.0, 32.0), peak_hz=(30.0,) * 3,
+                                           sn=(5.0,) * 3, nsim=2, seed=17))
+    noise = ob.sim_noise(23, blk.nsim, blk.nxp, blk.nyp, blk.nzp)
+    fin, fout = tmp_path / "block.bin", tmp_path / "out.bin"
+    write_block(fin, blk, grids, noise)
+    r = subprocess.run([DEMO, str(fin), str(fout)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = read_out(fout, blk)
+    post = ref64.posterior(blk)
+    nx = blk.nxp
+    assert out["counters"][0] == post.n_inverted
+    assert out["counters"][1] == post.n_chol_fail
+    for a in range(3):
+        assert crel(out["mean"][a][..., :nx], post.mean[a][..., :nx]) < 1e-4, ("mean", a)
+    for q in range(6):
+        assert crel(out["cov"][q][..., :nx], post.cov[q][..., :nx]) < 1e-3, ("cov", q)
+    for l in range(blk.ntheta):
+        assert crel(out["resid"][l], post.resid_spec[l]) < 2e-3, ("resid", l)
+    for s in range(blk.nsim):
+        sim = ref64.simulate(blk, post, noise[s])
+        for a in range(3):
+            assert crel(out["sims"][s, a][..., :nx], sim[a][..., :nx]) < 1e-4, ("sim", s, a)
+    assert np.allclose(out["post_var0"].reshape(3, 3), ref64.post_var0(post), rtol=1e-3)
+    scale = float(np.abs(blk.data[0]).max())
+    assert out["fft_roundtrip"] < 1e-5 * scale
