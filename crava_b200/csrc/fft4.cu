@@ -153,18 +153,25 @@ __global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet g
   float2* tw = sm;
   float2* twh = tw + H;
   float2* Z = twh + H;
+  float2* Xs = Z + rpc * PITCH;   // the unit's half-spectrum rows, as stored
   const int T = blockDim.x, tid = threadIdx.x;
+  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
+  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
+  {
+    const uint32_t xb = smem_addr(Xs);
+    for (int e = tid; e < nr * CN; e += T) cp_async8(xb + 8u * (uint32_t)e, g + e);
+    cp_async_commit();
+  }
   for (int t = tid; t < H; t += T) {
     tw[t] = twg[t];
     twh[t] = twn[t];
   }
-  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
-  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
   const float scale = gs.scale[blockIdx.y];
+  cp_async_wait_0();
   __syncthreads();
   for (int e = tid; e < nr * NP; e += T) {
     const int r = e / NP, k = e - r * NP;
-    const float2* X = g + (size_t)r * CN;
+    const float2* X = Xs + r * CN;
     float2* z = Z + r * PITCH;
     if (k == 0) {
       const float a = X[0].x, b = X[H].x;
@@ -259,7 +266,8 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   const int T = 256;
   int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
   if (const char* ev = getenv("CRAVA_X4_RPC")) rpc = std::max(1, std::min(rpc, atoi(ev)));
-  const size_t smem = sizeof(float2) * (2 * (size_t)L::H + (size_t)rpc * L::PITCH);
+  const size_t smem = sizeof(float2) * (2 * (size_t)L::H + (size_t)rpc * L::PITCH +
+                                         (fwd ? 0 : (size_t)rpc * (L::H + 1)));
   const void* fn = fwd ? (const void*)k_xr2c4<N1, N2> : (const void*)k_xc2r4<N1, N2>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -267,6 +267,20 @@ __device__ __forceinline__ void sts2(uint32_t a, float2 v) {
 
 // Thread-to-line mapping shared by every stage of one fft_lines call in LC mode:
 // thread t starts at line t % nlines, butterfly row t / nlines, and advances by T.
+// cp.async (global -> shared without registers), 8 bytes; the zero-filling form with
+// valid = false writes 8 zero bytes and reads nothing.
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+}
+// zero-filling form: src_bytes 0 writes 8 zero bytes and reads nothing
+__device__ __forceinline__ void cp_async8_zfill(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 struct LcMap {
   int f0, s0, df, ds;
 };

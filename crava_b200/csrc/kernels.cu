@@ -225,17 +225,7 @@ __global__ void __launch_bounds__(512, 2) k_line_fft(const __grid_constant__ Gri
 // second shared buffer with cp.async while it transforms the current one, so that loads
 // are in flight during the arithmetic.  Same arithmetic as the one-unit kernels.
 
-__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
-}
-// zero-filling form: src_bytes 0 writes 8 zero bytes and reads nothing
-__device__ __forceinline__ void cp_async8_zfill(uint32_t dst, const void* src, bool valid) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 8 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 
 // Even nxp only.  Unit u = (grid u / nchunk, rows [c rpc, c rpc + rpc)).
 __global__ void __launch_bounds__(512, 2) k_x_r2c_pipe(const __grid_constant__ GridSet gs, int nxp, int rows, int rpc,

@@ -481,14 +481,21 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
 
   if (tid < 4) cnt[tid] = 0;
   for (int t = tid; t < nzp; t += T) tw[t] = P.twz[t];
-  // ---- load inputs: slot g <- data[g] (g < NTH) or mean[g - NTH]
+  // ---- load inputs: slot g <- data[g] (g < NTH) or mean[g - NTH]; every copy is issued
+  //      before the first is waited for (cp.async), x-bins beyond the grid are zero-filled
+  {
+    const uint32_t rb = smem_addr(R);
 #pragma unroll 1
-  for (int g = 0; g < GIN; g++) {
-    const float2* src = (g < NTH ? P.data[g] : P.mean[g - NTH]) + base;
-    for (int e = tid; e < TS; e += T) {
-      int w = e & (W - 1), k = e >> lw;
-      R[(k * G + g) * W + w] = (w < nw) ? src[(size_t)k * kstride + w] : make_float2(0.f, 0.f);
+    for (int g = 0; g < GIN; g++) {
+      const float2* src = (g < NTH ? P.data[g] : P.mean[g - NTH]) + base;
+      for (int e = tid; e < TS; e += T) {
+        const int w = e & (W - 1), k = e >> lw;
+        const bool ok = w < nw;
+        cp_async8_zfill(rb + 8u * (uint32_t)((k * G + g) * W + w), ok ? src + (size_t)k * kstride + w : src, ok);
+      }
     }
+    cp_async_commit();
+    cp_async_wait_0();
   }
   __syncthreads();
   // forward z transforms, GT slots per call
