@@ -210,9 +210,9 @@ def alg_bytes(blk, nsim, cls, ngrids):
     """Algorithmic HBM bytes of one launch of a kernel class over ngrids grids."""
     N = blk.nxp * blk.nyp * blk.nzp
     Nc = (blk.nxp // 2 + 1) * blk.nyp * blk.nzp
-    if cls == "x_r2c":
+    if cls in ("x_r2c", "xy_fwd"):   # the fused xy pass keeps the x->y intermediate in L2
         return ngrids * (4 * N + 8 * Nc)
-    if cls == "x_c2r":
+    if cls in ("x_c2r", "xy_inv"):
         return ngrids * (8 * Nc + 4 * N)
     if cls in ("line_fwd", "line_inv"):
         return ngrids * 16 * Nc
@@ -457,7 +457,8 @@ def main():
 
     # roofline of the dominant kernel class
     peak, peak_kind = peaks()
-    ngrids = {"x_r2c": nin, "line_fwd": nin, "zpass": 1, "line_inv": nout, "x_c2r": nout}
+    ngrids = {"x_r2c": nin, "line_fwd": nin, "zpass": 1, "line_inv": nout, "x_c2r": nout, "xy_fwd": nin,
+              "xy_inv": nout}
     dom = max(kt, key=lambda c: kt[c][0])
     tot_ms, nl = kt[dom]
     per_launch_ms = tot_ms / max(nl, 1)

@@ -34,7 +34,7 @@ EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_s
            "crava_job_download", "crava_job_device_ptr", "crava_job_run", "crava_job_counters",
            "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches", "crava_ctx_set_profiling",
            "crava_ctx_kernel_times"]
-KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r"]
+KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r", "xy_fwd", "xy_inv"]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
 
 

@@ -89,7 +89,8 @@ struct Plan {
 }  // namespace
 
 // Per-kernel-class CUDA-event timing (off unless crava_ctx_set_profiling enables it).
-enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_COUNT = 5 };
+enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_XY_FWD = 5, KT_XY_INV = 6,
+       KT_COUNT = 7 };
 
 struct ProfRec {
   int cat;
@@ -105,8 +106,8 @@ struct crava_ctx {
   std::map<int, Plan> plans;
   bool profiling = false;
   std::vector<ProfRec> prof;
-  double kt_ms[KT_COUNT] = {0, 0, 0, 0, 0};
-  long long kt_n[KT_COUNT] = {0, 0, 0, 0, 0};
+  double kt_ms[KT_COUNT] = {};
+  long long kt_n[KT_COUNT] = {};
   std::mutex stage_mu;         // device staging grid of the host-grid transforms
   float* stage = nullptr;
   size_t stage_bytes = 0;
@@ -392,13 +393,18 @@ crava_status fwd_xy(crava_ctx* ctx, const std::vector<const float*>& src, const 
     GridSet gs;
     gs.n = (int)std::min(g.size() - b, (size_t)kMaxGrids);
     for (int q = 0; q < gs.n; q++) { gs.p[q] = g[b + q]; gs.src[q] = src[b + q]; gs.scale[q] = sc[b + q]; }
-    {
-      ProfScope ps(ctx, KT_X_R2C, st);
-      CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, pn->tw, st, &nl));
-    }
-    {
-      ProfScope ps(ctx, KT_LINE_FWD, st);
-      CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, -1.f, st, &nl));
+    if (xy_fused_supported(nxp, nyp)) {
+      ProfScope ps(ctx, KT_XY_FWD, st);
+      CUDA_TRY(launch_xy4(true, gs, nxp, nyp, nzp, px->tw, pn->tw, py->tw, st, &nl));
+    } else {
+      {
+        ProfScope ps(ctx, KT_X_R2C, st);
+        CUDA_TRY(launch_x_r2c(gs, nxp, nyp * nzp, px->lp, px->tw, pn->tw, st, &nl));
+      }
+      {
+        ProfScope ps(ctx, KT_LINE_FWD, st);
+        CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, -1.f, st, &nl));
+      }
     }
     if (with_z) {
       ProfScope ps(ctx, KT_LINE_FWD, st);
@@ -425,13 +431,18 @@ crava_status inv_xy(crava_ctx* ctx, const std::vector<float*>& g, const std::vec
       ProfScope ps(ctx, KT_LINE_INV, st);
       CUDA_TRY(launch_line_fft(gs, cnxp, nzp, (size_t)cnxp * nyp, nyp, (size_t)cnxp, pz->lp, pz->tw, 1.f, st, &nl));
     }
-    {
-      ProfScope ps(ctx, KT_LINE_INV, st);
-      CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, 1.f, st, &nl));
-    }
-    {
-      ProfScope ps(ctx, KT_X_C2R, st);
-      CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, pn->tw, st, &nl));
+    if (xy_fused_supported(nxp, nyp)) {
+      ProfScope ps(ctx, KT_XY_INV, st);
+      CUDA_TRY(launch_xy4(false, gs, nxp, nyp, nzp, px->tw, pn->tw, py->tw, st, &nl));
+    } else {
+      {
+        ProfScope ps(ctx, KT_LINE_INV, st);
+        CUDA_TRY(launch_line_fft(gs, cnxp, nyp, (size_t)cnxp, nzp, (size_t)cnxp * nyp, py->lp, py->tw, 1.f, st, &nl));
+      }
+      {
+        ProfScope ps(ctx, KT_X_C2R, st);
+        CUDA_TRY(launch_x_c2r(gs, nxp, nyp * nzp, px->lp, px->tw, pn->tw, st, &nl));
+      }
     }
   }
   ctx->launches += nl;
@@ -766,13 +777,14 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = job->cnxp;
   zp.nxp_even = (d.nxp % 2) == 0;
   // pencil tile: W x-bins (power of two), GT slots per z-transform call, SB realisations
-  // per batch and T threads.  Preferred: every slot of a phase in one call (GT = G,
-  // SB = 2) in two CTAs of 256 threads per SM; else one CTA of 512; else the three-slot
-  // layout.  CRAVA_ZPASS_{W,T,GT,SB} override.
+  // per batch and T threads.  Preferred: the widest tile (longest contiguous rows, fewest
+  // tiles) with every slot of a phase in one call (GT = G), the first of the candidates
+  // that fits; 512 threads when one CTA fills the SM's shared memory, 256 when two fit.
+  // CRAVA_ZPASS_{W,T,GT,SB} override.
   const int Gs = std::max(d.ntheta + 3, 9);
   int W = 2, T = 256, GT = Gs, SB = 2;
   {
-    const int cand[6][3] = {{2, Gs, 2}, {4, Gs, 2}, {1, Gs, 2}, {4, 3, 1}, {2, 3, 1}, {1, 3, 1}};
+    const int cand[8][3] = {{4, Gs, 2}, {4, Gs, 1}, {2, Gs, 2}, {2, Gs, 1}, {1, Gs, 2}, {4, 3, 1}, {2, 3, 1}, {1, 3, 1}};
     for (const auto& c : cand) {
       if (zpass_smem_bytes(c[0], d.nzp, d.ntheta, c[1], c[2]) <= 227 * 1024) {
         W = c[0]; GT = c[1]; SB = c[2];

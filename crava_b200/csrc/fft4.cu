@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdlib>
 
@@ -20,24 +22,16 @@ namespace crava {
 
 // ------------------------------------------------------------------ strided lines
 //
-// Shared layout of the W lines: element (w, p = t + N2 m) at p W + w + m SK, with SK
-// chosen so that the pass-2 reads of neighbouring k2 fall on disjoint banks.
+// One tile of W columns (nw of them valid) of the lines through g: point p of column w at
+// g[p pstride + w].  Shared layout of the W lines: element (w, p = t + N2 m) at
+// p W + w + m SK, with SK chosen so that the pass-2 reads of neighbouring k2 fall on
+// disjoint banks.  Needs tw (the length-N table) in shared memory; ends with a barrier.
 template <int N1, int N2, int DIR>
-__global__ void __launch_bounds__(256) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
-                                               size_t ostride, int W, int lw, int nIT, int SK,
-                                               const float2* __restrict__ twg) {
-  constexpr int N = N1 * N2;
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* Y = sm + N;
+__device__ __forceinline__ void line4_tile(float2* g, int nw, size_t pstride, int W, int lw, int SK,
+                                           const float2* tw, float2* Y) {
   const int T = blockDim.x, tid = threadIdx.x;
-  for (int t = tid; t < N; t += T) tw[t] = twg[t];
-  const int it = blockIdx.x % nIT, o = blockIdx.x / nIT;
-  const int i0 = it * W, nw = min(W, ni - i0);
-  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)o * ostride + i0;
   const size_t mstride = (size_t)N2 * pstride;
   const int mpitch = N2 * W + SK;
-  __syncthreads();
   for (int q = tid; q < W * N2; q += T) {
     const int w = q & (W - 1), t = q >> lw;
     const bool ok = w < nw;
@@ -59,6 +53,27 @@ __global__ void __launch_bounds__(256) k_line4(const __grid_constant__ GridSet g
       for (int k1 = 0; k1 < N2; k1++) dst[(size_t)k1 * N1 * pstride] = v[k1];
     }
   }
+  __syncthreads();
+}
+
+template <int N1, int N2>
+constexpr size_t line4_smem(int W, int SK) {
+  return sizeof(float2) * ((size_t)W * N1 * N2 + (size_t)N1 * SK);
+}
+
+template <int N1, int N2, int DIR>
+__global__ void __launch_bounds__(256) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
+                                               size_t ostride, int W, int lw, int nIT, int SK,
+                                               const float2* __restrict__ twg) {
+  constexpr int N = N1 * N2;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twg[t];
+  const int it = blockIdx.x % nIT, o = blockIdx.x / nIT;
+  const int i0 = it * W, nw = min(W, ni - i0);
+  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)o * ostride + i0;
+  __syncthreads();
+  line4_tile<N1, N2, DIR>(g, nw, pstride, W, lw, SK, tw, sm + N);
 }
 
 // ------------------------------------------------------------------ rows, even nxp
@@ -73,27 +88,17 @@ struct RowLayout {
   static __device__ __forceinline__ int pad(int t, int m) { return t + m * (N2 + SK); }
 };
 
-// Even nxp only; the split step as k_x_r2c (kernels.cu).
+// nr (<= blockDim / N1) rows, even nxp: src rows (h complex values x[2m] + i x[2m+1] each,
+// row pitch h + 1) to the scaled half spectra in dst (may equal src).  The split step as
+// k_x_r2c (kernels.cu).  Needs tw (length h) and twh (e^{-2 pi i k / nxp}, k < h) in
+// shared memory; Z: rpc * PITCH.  Ends with a barrier.
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) k_xr2c4(const __grid_constant__ GridSet gs, int rows, int rpc,
-                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+__device__ __forceinline__ void xr2c4_rows(const float2* src, float2* dst, int nr, float scale, const float2* tw,
+                                           const float2* twh, float2* Z) {
   using L = RowLayout<N1, N2>;
   constexpr int H = L::H, PITCH = L::PITCH;
   constexpr int CN = H + 1, NP = H / 2 + 1;
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* twh = tw + H;
-  float2* Z = twh + H;
   const int T = blockDim.x, tid = threadIdx.x;
-  for (int t = tid; t < H; t += T) {
-    tw[t] = twg[t];
-    twh[t] = twn[t];
-  }
-  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
-  const float2* src = reinterpret_cast<const float2*>(gs.src[blockIdx.y]) + (size_t)row0 * CN;
-  float2* dst = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
-  const float scale = gs.scale[blockIdx.y];
-  __syncthreads();
   for (int q = tid; q < nr * N2; q += T) {
     const int r = q / N2, t = q - r * N2;
     const float2* x = src + (size_t)r * CN + t;
@@ -140,34 +145,24 @@ __global__ void __launch_bounds__(256) k_xr2c4(const __grid_constant__ GridSet g
       X[H - k] = make_float2(scale * m.x, -scale * m.y);
     }
   }
+  __syncthreads();
 }
 
-// Even nxp only; the merge step as k_x_c2r (kernels.cu).
+// nr rows of half spectra in g (pitch h + 1) to scaled real rows in place; the merge step
+// as k_x_c2r (kernels.cu).  Z: rpc * PITCH, Xs: rpc * (h + 1).  Ends with a barrier.
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet gs, int rows, int rpc,
-                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+__device__ __forceinline__ void xc2r4_rows(float2* g, int nr, float scale, const float2* tw, const float2* twh,
+                                           float2* Z, float2* Xs) {
   using L = RowLayout<N1, N2>;
   constexpr int H = L::H, PITCH = L::PITCH;
   constexpr int CN = H + 1, NP = H / 2 + 1;
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* twh = tw + H;
-  float2* Z = twh + H;
-  float2* Xs = Z + rpc * PITCH;   // the unit's half-spectrum rows, as stored
   const int T = blockDim.x, tid = threadIdx.x;
-  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
-  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
   {
     const uint32_t xb = smem_addr(Xs);
     for (int e = tid; e < nr * CN; e += T) cp_async8(xb + 8u * (uint32_t)e, g + e);
     cp_async_commit();
+    cp_async_wait_0();
   }
-  for (int t = tid; t < H; t += T) {
-    tw[t] = twg[t];
-    twh[t] = twn[t];
-  }
-  const float scale = gs.scale[blockIdx.y];
-  cp_async_wait_0();
   __syncthreads();
   for (int e = tid; e < nr * NP; e += T) {
     const int r = e / NP, k = e - r * NP;
@@ -206,6 +201,116 @@ __global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet g
 #pragma unroll
     for (int k1 = 0; k1 < N2; k1++) X[k2 + N1 * k1] = make_float2(v[k1].x * scale, v[k1].y * scale);
     if (k2 == 0) X[H] = make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+}
+
+template <int N1, int N2>
+constexpr size_t x4_smem(bool fwd, int rpc) {
+  using L = RowLayout<N1, N2>;
+  return sizeof(float2) * ((size_t)rpc * L::PITCH + (fwd ? 0 : (size_t)rpc * (L::H + 1)));
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_xr2c4(const __grid_constant__ GridSet gs, int rows, int rpc,
+                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  constexpr int H = N1 * N2;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* twh = tw + H;
+  for (int t = threadIdx.x; t < H; t += blockDim.x) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
+  const float2* src = reinterpret_cast<const float2*>(gs.src[blockIdx.y]) + (size_t)row0 * (H + 1);
+  float2* dst = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * (H + 1);
+  __syncthreads();
+  xr2c4_rows<N1, N2>(src, dst, nr, gs.scale[blockIdx.y], tw, twh, twh + H);
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet gs, int rows, int rpc,
+                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  using L = RowLayout<N1, N2>;
+  constexpr int H = N1 * N2;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* twh = tw + H;
+  float2* Z = twh + H;
+  const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
+  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * (H + 1);
+  for (int t = threadIdx.x; t < H; t += blockDim.x) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  __syncthreads();
+  xc2r4_rows<N1, N2>(g, nr, gs.scale[blockIdx.y], tw, twh, Z, Z + rpc * L::PITCH);
+}
+
+// ------------------------------------------------------------------ fused xy passes
+//
+// One z-plane of one grid at a time per cluster of C CTAs: the rows of the plane (x
+// transform, split across the cluster), a cluster barrier, then the columns (y transform,
+// split across the cluster), in place in the destination grid.  The plane (nyp half-
+// spectrum rows, 1-2.4 MB) is written by the first phase and read back by the second while
+// it sits in L2, so each grid crosses HBM once each way per xy pass.  Persistent clusters
+// walk the planes of every grid in the set.  The inverse runs the phases the other way.
+template <int HX1, int HX2, int NY1, int NY2, bool FWD>
+__global__ void __launch_bounds__(256, 2) k_xy4(const __grid_constant__ GridSet gs, int nzp, int rpc, int W, int lw,
+                                             int SK, const float2* __restrict__ twx, const float2* __restrict__ twn,
+                                             const float2* __restrict__ twy) {
+  namespace cg = cooperative_groups;
+  constexpr int H = HX1 * HX2, NY = NY1 * NY2, CN = H + 1;
+  using L = RowLayout<HX1, HX2>;
+  extern __shared__ float2 sm[];
+  float2* tx = sm;
+  float2* th = tx + H;
+  float2* ty = th + H;
+  float2* work = ty + NY;
+  for (int t = threadIdx.x; t < H; t += blockDim.x) {
+    tx[t] = twx[t];
+    th[t] = twn[t];
+  }
+  for (int t = threadIdx.x; t < NY; t += blockDim.x) ty[t] = twy[t];
+  __syncthreads();
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int ncl = gridDim.x / C, cid = blockIdx.x / C;
+  const int planes = gs.n * nzp;
+  const int nchunk = (NY + rpc - 1) / rpc, ntile = (CN + W - 1) / W;
+  const size_t plane = (size_t)NY * CN;
+  for (int p = cid; p < planes; p += ncl) {
+    const int gi = p / nzp, z = p - gi * nzp;
+    float2* dst = reinterpret_cast<float2*>(gs.p[gi]) + (size_t)z * plane;
+    const float scale = gs.scale[gi];
+    if (FWD) {
+      const float2* src = reinterpret_cast<const float2*>(gs.src[gi]) + (size_t)z * plane;
+      for (int c = rank; c < nchunk; c += C) {
+        const int row0 = c * rpc, nr = min(rpc, NY - row0);
+        xr2c4_rows<HX1, HX2>(src + (size_t)row0 * CN, dst + (size_t)row0 * CN, nr, scale, tx, th, work);
+      }
+      __threadfence();
+      cl.sync();
+      __threadfence();  // acquire side: no line of this plane cached before the barrier is reused
+      for (int it = rank; it < ntile; it += C) {
+        const int i0 = it * W;
+        line4_tile<NY1, NY2, -1>(dst + i0, min(W, CN - i0), (size_t)CN, W, lw, SK, ty, work);
+      }
+    } else {
+      for (int it = rank; it < ntile; it += C) {
+        const int i0 = it * W;
+        line4_tile<NY1, NY2, 1>(dst + i0, min(W, CN - i0), (size_t)CN, W, lw, SK, ty, work);
+      }
+      __threadfence();
+      cl.sync();
+      __threadfence();
+      for (int c = rank; c < nchunk; c += C) {
+        const int row0 = c * rpc, nr = min(rpc, NY - row0);
+        xc2r4_rows<HX1, HX2>(dst + (size_t)row0 * CN, nr, scale, tx, th, work, work + rpc * L::PITCH);
+      }
+    }
+    // a plane's two phases touch only that plane: the next plane needs no cluster barrier
   }
 }
 
@@ -250,7 +355,7 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   const int SK = W < 16 ? (((W - N2 * W) % 16) + 16) % 16 : 0;
   const int T = std::min(256, round_up32(W * std::max(N1, N2)));
   const int nIT = (ni + W - 1) / W;
-  const size_t smem = sizeof(float2) * ((size_t)N + (size_t)W * N + (size_t)N1 * SK);
+  const size_t smem = sizeof(float2) * (size_t)N + line4_smem<N1, N2>(W, SK);
   const void* fn = sign < 0.f ? (const void*)k_line4<N1, N2, -1> : (const void*)k_line4<N1, N2, 1>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -266,8 +371,7 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   const int T = 256;
   int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
   if (const char* ev = getenv("CRAVA_X4_RPC")) rpc = std::max(1, std::min(rpc, atoi(ev)));
-  const size_t smem = sizeof(float2) * (2 * (size_t)L::H + (size_t)rpc * L::PITCH +
-                                         (fwd ? 0 : (size_t)rpc * (L::H + 1)));
+  const size_t smem = sizeof(float2) * 2 * (size_t)L::H + x4_smem<N1, N2>(fwd, rpc);
   const void* fn = fwd ? (const void*)k_xr2c4<N1, N2> : (const void*)k_xc2r4<N1, N2>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -275,6 +379,78 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   if (fwd) k_xr2c4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn);
   else k_xc2r4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn);
   return cudaGetLastError();
+}
+
+// Fused xy pass for (h, nyp) pairs; cluster size from CRAVA_XY_CLUSTER (default 8).
+template <int HX1, int HX2, int NY1, int NY2>
+static cudaError_t xy4(bool fwd, const GridSet& gs, int nzp, const float2* twx, const float2* twn, const float2* twy,
+                       cudaStream_t st) {
+  constexpr int H = HX1 * HX2, NY = NY1 * NY2;
+  const int T = 256;
+  const int rpc = std::max(1, T / HX1);
+  int W = 8, lw = 3;
+  const int SK = (((W - NY2 * W) % 16) + 16) % 16;
+  int C = 8;
+  if (const char* ev = getenv("CRAVA_XY_CLUSTER")) C = std::max(1, std::min(16, atoi(ev)));
+  const size_t work = std::max(x4_smem<HX1, HX2>(false, rpc), line4_smem<NY1, NY2>(W, SK));
+  const size_t smem = sizeof(float2) * (2 * (size_t)H + NY) + work;
+  const void* fn = fwd ? (const void*)k_xy4<HX1, HX2, NY1, NY2, true> : (const void*)k_xy4<HX1, HX2, NY1, NY2, false>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (C > 8 && (e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+    return e;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(C);
+  int nclusters = 0;
+  if ((e = cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg)) != cudaSuccess) return e;
+  if (nclusters < 1) return cudaErrorInvalidConfiguration;
+  const int planes = gs.n * nzp;
+  cfg.gridDim = dim3((unsigned)(std::min(nclusters, planes) * C));
+  if (fwd) return cudaLaunchKernelEx(&cfg, k_xy4<HX1, HX2, NY1, NY2, true>, gs, nzp, rpc, W, lw, SK, twx, twn, twy);
+  return cudaLaunchKernelEx(&cfg, k_xy4<HX1, HX2, NY1, NY2, false>, gs, nzp, rpc, W, lw, SK, twx, twn, twy);
+}
+
+// (nxp, nyp) pairs with a fused xy pass
+#define CRAVA_XY_PAIRS(X)   \
+  X(64, 64, 8, 4, 8, 8)     \
+  X(540, 540, 18, 15, 27, 20) \
+  X(768, 768, 24, 16, 32, 24)
+
+static bool xy_enabled() {
+  static const bool on = [] {
+    const char* ev = getenv("CRAVA_XY_FUSED");
+    return !(ev && ev[0] == '0');
+  }();
+  return on;
+}
+
+bool xy_fused_supported(int nxp, int nyp) {
+  if (!xy_enabled() || !four_step_enabled()) return false;
+#define CRAVA_CASE(NX, NY, A, B, C2, D) \
+  if (nxp == NX && nyp == NY) return true;
+  CRAVA_XY_PAIRS(CRAVA_CASE)
+#undef CRAVA_CASE
+  return false;
+}
+
+cudaError_t launch_xy4(bool fwd, const GridSet& gs, int nxp, int nyp, int nzp, const float2* twx, const float2* twn,
+                       const float2* twy, cudaStream_t st, int* nlaunch) {
+  if (nlaunch) (*nlaunch)++;
+#define CRAVA_CASE(NX, NY, A, B, C2, D) \
+  if (nxp == NX && nyp == NY) return xy4<A, B, C2, D>(fwd, gs, nzp, twx, twn, twy, st);
+  CRAVA_XY_PAIRS(CRAVA_CASE)
+#undef CRAVA_CASE
+  return cudaErrorInvalidValue;
 }
 
 bool four_step_supported(int n) {

@@ -83,6 +83,11 @@ cudaError_t launch_line4(const GridSet& gs, int ni, int n, size_t pstride, int n
                          float sign, cudaStream_t st, int* nlaunch);
 cudaError_t launch_x4(bool fwd, const GridSet& gs, int nxp, int rows, const float2* tw, const float2* twn,
                       cudaStream_t st, int* nlaunch);
+// fused xy pass (fft4.cu) for the (nxp, nyp) pairs of its table: x then y forward (src ->
+// p), or y then x inverse (in place in p); twx/twn as launch_x4, twy the length-nyp table
+bool xy_fused_supported(int nxp, int nyp);
+cudaError_t launch_xy4(bool fwd, const GridSet& gs, int nxp, int nyp, int nzp, const float2* twx, const float2* twn,
+                       const float2* twy, cudaStream_t st, int* nlaunch);
 
 // launchers (kernels.cu)
 // x transforms: pl/tw are the plan and table of length nxp/2 (even nxp) or nxp (odd);

@@ -35,7 +35,7 @@ def ctx():
 
 
 @pytest.mark.parametrize("dims", [(64, 64, 128), (15, 12, 20), (27, 25, 14), (7, 5, 9), (540, 8, 6), (6, 768, 10),
-                                  (8, 6, 320), (245, 3, 2), (2, 2, 2)])
+                                  (8, 6, 320), (245, 3, 2), (2, 2, 2), (540, 540, 3), (768, 768, 2)])
 @pytest.mark.parametrize("covariance", [False, True])
 def test_fft_matches_numpy(ctx, dims, covariance):
     import torch
