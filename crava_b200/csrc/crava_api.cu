@@ -154,6 +154,7 @@ struct crava_job {
   float* noise[3 * kMaxSim] = {};
   float2* kw = nullptr;
   double2* kwd = nullptr;
+  float2* septab = nullptr;   // SEPARABLE: per-kz error part of Sd (lower triangle)
   double2* e1d = nullptr;
   double2* e2d = nullptr;
   float2* e1 = nullptr;
@@ -245,7 +246,8 @@ size_t footprint(const crava_job_desc* d) {
   size_t ngrids = 2 * ((size_t)d->ntheta + 3) + 6 + 3 * (size_t)d->nsim;
   if (d->prior_mode == CRAVA_PRIOR_GRIDS) ngrids += 6 + 2;
   if (d->flags & CRAVA_FLAG_HOST_NOISE) ngrids += 3 * (size_t)d->nsim;
-  size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) +
+  const size_t sep_stride = (size_t)d->ntheta * (d->ntheta + 1) / 2;
+  size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) + align256(sizeof(float2) * d->nzp * sep_stride) +
                   3 * align256(sizeof(double2) * d->nzp * d->ntheta) + align256(d->nzp) +
                   align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float2) * d->nzp) +
                   align256(sizeof(float) * 2 * cnxp * d->nyp) + 256;
@@ -629,6 +631,7 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->kwd = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
   j->e1d = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
   j->e2d = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
+  j->septab = (float2*)take(sizeof(float2) * d.nzp * ((size_t)d.ntheta * (d.ntheta + 1) / 2));
   j->inv = (uint8_t*)take(d.nzp);
   j->cxy = (float2*)take(sizeof(float2) * j->cnxp * d.nyp);
   j->ct = (float2*)take(sizeof(float2) * d.nzp);
@@ -657,6 +660,24 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   JOB_TRY(cudaMemcpyAsync(j->e2, e2.data(), sizeof(float2) * e2.size(), cudaMemcpyHostToDevice, st));
   JOB_TRY(cudaMemcpyAsync(j->inv, inv.data(), inv.size(), cudaMemcpyHostToDevice, st));
   if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) {
+    // Separable prior: the error part of Sd per kz, M2 = ec o (e1 e1^H + e2 e2^H) with
+    // ec = (1 - wnc) errThetaCov / 2 (getNextErrorVariance, src/avoinversion.cpp:1236-1272),
+    // lower triangle row by row.
+    const int nth = d.ntheta, tri = nth * (nth + 1) / 2;
+    std::vector<float2> sep((size_t)d.nzp * tri);
+    for (int k = 0; k < d.nzp; k++) {
+      float2* row = sep.data() + (size_t)k * tri;
+      const double2* a1 = e1d.data() + (size_t)k * nth;
+      const double2* a2 = e2d.data() + (size_t)k * nth;
+      for (int l = 0; l < nth; l++)
+        for (int m = 0; m <= l; m++) {
+          const cd ee = cd(a1[l].x, a1[l].y) * std::conj(cd(a1[m].x, a1[m].y)) +
+                        cd(a2[l].x, a2[l].y) * std::conj(cd(a2[m].x, a2[m].y));
+          const cd m2 = ee * (0.5 * (1.0 - d.wnc) * j->etc[l * nth + m]);
+          row[l * (l + 1) / 2 + m] = make_float2((float)m2.real(), (float)m2.imag());
+        }
+    }
+    JOB_TRY(cudaMemcpyAsync(j->septab, sep.data(), sizeof(float2) * sep.size(), cudaMemcpyHostToDevice, st));
     // temporal factor: DFT of circCorrT (1D, double)
     std::vector<double> c(j->circ.begin(), j->circ.end());
     std::vector<cd> C = dft(c);
@@ -827,6 +848,18 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   }
   zp.cxy = job->cxy;
   zp.ct = job->ct;
+  zp.septab = grids ? nullptr : job->septab;
+  for (int l = 0; l < d.ntheta; l++) {
+    double ap[3] = {0, 0, 0};
+    for (int c = 0; c < 3; c++)
+      for (int b = 0; b < 3; b++) ap[c] += job->A[l * 3 + b] * job->pv[b * 3 + c];
+    for (int c = 0; c < 3; c++) zp.AP[l][c] = (float)ap[c];
+    for (int m = 0; m < d.ntheta; m++) {
+      double g = 0;
+      for (int c = 0; c < 3; c++) g += ap[c] * job->A[m * 3 + c];
+      zp.G0[l][m] = (float)g;
+    }
+  }
   const int qa[6] = {0, 1, 2, 0, 0, 1}, qb[6] = {0, 1, 2, 1, 2, 2};
   for (int q = 0; q < 6; q++) zp.pv[q] = static_cast<float>(job->pv[qa[q] * 3 + qb[q]]);
   for (int l = 0; l < d.ntheta; l++) {

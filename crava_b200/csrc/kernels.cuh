@@ -50,10 +50,13 @@ struct ZParams {
   const float2* noise[3 * kMaxSim];
   const float2* cxy;           // SEPARABLE: nyp x cnxp spectrum of corrXY
   const float2* ct;            // SEPARABLE: nzp spectrum of circCorrT
+  const float2* septab;        // SEPARABLE: per-kz lower triangle of M2 (or null)
   float pv[6];                 // priorVar0: 00 11 22 01 02 12
   float A[kMaxTheta][3];
   float ec[kMaxTheta][kMaxTheta];  // 0.5 (1 - wnc) errThetaCov
   float ed[kMaxTheta];             // wnc errThetaCov_ll |e3_l|^2
+  float G0[kMaxTheta][kMaxTheta];  // SEPARABLE: A P0 A^T
+  float AP[kMaxTheta][3];          // SEPARABLE: A P0
   KzTables kz;
   LinePlan zp;
   const float2* twz;

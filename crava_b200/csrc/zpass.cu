@@ -127,37 +127,68 @@ struct BinOut {
 //   S_post = S - Y^H Y, mu_post = mu + Y^H L^{-1} (d - K mu), res = d - K mu_post,
 // which is the reference's  KS <- Sd^{-1} KS; S - KS_old^H KS;  mu + KS^H (d - K mu)
 // regrouped through the Cholesky factor.
-template <int NTH>
-__device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const float (&S)[6], float lam,
+// SEP: separable prior.  Then S = rho P0, so K S K^H = rho (kw kw^H) o G0 and K S = rho
+// diag(kw) AP with G0 = A P0 A^T and AP = A P0 job constants, and the error part of Sd is
+// lam M2 with M2 = ec o (e1 e1^H + e2 e2^H) read per kz from the job's table (lower
+// triangle, row by row), in place of the per-bin products.
+template <int NTH, bool SEP>
+__device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const float (&S)[6], float lam, float rho,
                                               const float2 (&mu)[3], float2 (&d)[NTH], BinOut& o) {
-  float2 kw[NTH], e1[NTH], e2[NTH];
+  constexpr int TRI = NTH * (NTH + 1) / 2;
+  float2 kw[NTH];
 #pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    kw[l] = __ldg(P.kz.kw + k * NTH + l);
-    e1[l] = __ldg(P.kz.e1 + k * NTH + l);
-    e2[l] = __ldg(P.kz.e2 + k * NTH + l);
-  }
-  // AS = A S (NTH x 3), G = A S A^T
-  float AS[NTH][3];
-#pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    AS[l][0] = P.A[l][0] * S[0] + P.A[l][1] * S[3] + P.A[l][2] * S[4];
-    AS[l][1] = P.A[l][0] * S[3] + P.A[l][1] * S[1] + P.A[l][2] * S[5];
-    AS[l][2] = P.A[l][0] * S[4] + P.A[l][1] * S[5] + P.A[l][2] * S[2];
-  }
+  for (int l = 0; l < NTH; l++) kw[l] = __ldg(P.kz.kw + k * NTH + l);
   float2 Sd[NTH][NTH];
+  float2 Y[NTH][3];  // K S, then L^{-1} K S
+  if constexpr (SEP) {
+    const float2* m2 = P.septab + (size_t)k * TRI;
 #pragma unroll
-  for (int l = 0; l < NTH; l++) {
+    for (int l = 0; l < NTH; l++) {
 #pragma unroll
-    for (int m = 0; m <= l; m++) {
-      float g = AS[l][0] * P.A[m][0] + AS[l][1] * P.A[m][1] + AS[l][2] * P.A[m][2];
-      // kw_l conj(kw_m)
-      float2 kk = make_float2(kw[l].x * kw[m].x + kw[l].y * kw[m].y, kw[l].y * kw[m].x - kw[l].x * kw[m].y);
-      float c = P.ec[l][m] * lam;
-      float2 ee = make_float2(e1[l].x * e1[m].x + e1[l].y * e1[m].y + e2[l].x * e2[m].x + e2[l].y * e2[m].y,
-                              e1[l].y * e1[m].x - e1[l].x * e1[m].y + e2[l].y * e2[m].x - e2[l].x * e2[m].y);
-      Sd[l][m] = make_float2(kk.x * g + c * ee.x, kk.y * g + c * ee.y);
-      if (l == m) Sd[l][m] = make_float2(Sd[l][m].x + P.ed[l], 0.f);
+      for (int m = 0; m <= l; m++) {
+        const float2 b = __ldg(m2 + l * (l + 1) / 2 + m);
+        const float g = rho * P.G0[l][m];
+        // rho G0_lm kw_l conj(kw_m) + lam M2_lm
+        Sd[l][m] = make_float2(g * (kw[l].x * kw[m].x + kw[l].y * kw[m].y) + lam * b.x,
+                               g * (kw[l].y * kw[m].x - kw[l].x * kw[m].y) + lam * b.y);
+      }
+      Sd[l][l] = make_float2(Sd[l][l].x + P.ed[l], 0.f);
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const float a = rho * P.AP[l][j];
+        Y[l][j] = make_float2(kw[l].x * a, kw[l].y * a);
+      }
+    }
+  } else {
+    float2 e1[NTH], e2[NTH];
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+      e1[l] = __ldg(P.kz.e1 + k * NTH + l);
+      e2[l] = __ldg(P.kz.e2 + k * NTH + l);
+    }
+    // AS = A S (NTH x 3), G = A S A^T
+    float AS[NTH][3];
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+      AS[l][0] = P.A[l][0] * S[0] + P.A[l][1] * S[3] + P.A[l][2] * S[4];
+      AS[l][1] = P.A[l][0] * S[3] + P.A[l][1] * S[1] + P.A[l][2] * S[5];
+      AS[l][2] = P.A[l][0] * S[4] + P.A[l][1] * S[5] + P.A[l][2] * S[2];
+    }
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+#pragma unroll
+      for (int m = 0; m <= l; m++) {
+        float g = AS[l][0] * P.A[m][0] + AS[l][1] * P.A[m][1] + AS[l][2] * P.A[m][2];
+        // kw_l conj(kw_m)
+        float2 kk = make_float2(kw[l].x * kw[m].x + kw[l].y * kw[m].y, kw[l].y * kw[m].x - kw[l].x * kw[m].y);
+        float c = P.ec[l][m] * lam;
+        float2 ee = make_float2(e1[l].x * e1[m].x + e1[l].y * e1[m].y + e2[l].x * e2[m].x + e2[l].y * e2[m].y,
+                                e1[l].y * e1[m].x - e1[l].x * e1[m].y + e2[l].y * e2[m].x - e2[l].x * e2[m].y);
+        Sd[l][m] = make_float2(kk.x * g + c * ee.x, kk.y * g + c * ee.y);
+        if (l == m) Sd[l][m] = make_float2(Sd[l][m].x + P.ed[l], 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < 3; j++) Y[l][j] = make_float2(kw[l].x * AS[l][j], kw[l].y * AS[l][j]);
     }
   }
   if (!chol_ref<NTH>(Sd)) return false;
@@ -170,13 +201,12 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
     }
     o.cond = (dmax * rmax) * (dmax * rmax);
   }
-  // Y = L^{-1} KS, KS[l][j] = kw_l AS[l][j]
-  float2 Y[NTH][3];
+  // Y = L^{-1} KS (forward substitution in place)
 #pragma unroll
   for (int l = 0; l < NTH; l++) {
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      float2 acc = make_float2(kw[l].x * AS[l][j], kw[l].y * AS[l][j]);
+      float2 acc = Y[l][j];
 #pragma unroll
       for (int m = 0; m < l; m++) acc = csub(acc, cmul(Sd[l][m], Y[m][j]));
       Y[l][j] = make_float2(acc.x * Sd[l][l].y, acc.y * Sd[l][l].y);
@@ -485,14 +515,14 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
   //      before the first is waited for (cp.async), x-bins beyond the grid are zero-filled
   {
     const uint32_t rb = smem_addr(R);
-#pragma unroll 1
-    for (int g = 0; g < GIN; g++) {
-      const float2* src = (g < NTH ? P.data[g] : P.mean[g - NTH]) + base;
-      for (int e = tid; e < TS; e += T) {
-        const int w = e & (W - 1), k = e >> lw;
-        const bool ok = w < nw;
-        cp_async8_zfill(rb + 8u * (uint32_t)((k * G + g) * W + w), ok ? src + (size_t)k * kstride + w : src, ok);
-      }
+    for (int e = tid; e < TS; e += T) {
+      const int w = e & (W - 1), k = e >> lw;
+      const bool ok = w < nw;
+      const size_t go = base + (ok ? (size_t)k * kstride + w : 0);   // nothing is read when !ok
+      const uint32_t sa = rb + 8u * (uint32_t)(k * G * W + w);
+#pragma unroll
+      for (int g = 0; g < GIN; g++)
+        cp_async8_zfill(sa + 8u * (uint32_t)(g * W), (g < NTH ? P.data[g] : P.mean[g - NTH]) + go, ok);
     }
     cp_async_commit();
     cp_async_wait_0();
@@ -520,11 +550,11 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     int i = i0 + w;
     size_t gidx = base + (size_t)k * kstride + w;
     float2* slot = R + k * G * W + w;   // slot g at slot[g * W]
-    float S[6], lam;
+    float S[6], lam, rho = 0.f;
     if (P.separable) {
       float2 cx = __ldg(P.cxy + (size_t)j * P.cnxp + i);
       float2 c_t = __ldg(P.ct + k);
-      float rho = fabsf(cx.x * c_t.x - cx.y * c_t.y);
+      rho = fabsf(cx.x * c_t.x - cx.y * c_t.y);
 #pragma unroll
       for (int q = 0; q < 6; q++) S[q] = P.pv[q] * rho;
       lam = fabsf(cx.x);
@@ -549,7 +579,8 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     bool ok = false;
     if (inv) {
       n_inv++;
-      ok = bin_posterior<NTH>(P, k, S, lam, mu, d, o);
+      ok = P.septab ? bin_posterior<NTH, true>(P, k, S, lam, rho, mu, d, o)
+                    : bin_posterior<NTH, false>(P, k, S, lam, rho, mu, d, o);
       if constexpr (REFINE) {
         if (ok) {
           float ratio = 1.f;
@@ -656,13 +687,14 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     } else {
       fft_lines<true, 1>(S3, SC, SG * W, 1, SG * W, P.zp, tw);
     }
-#pragma unroll 1
-    for (int q = 0; q < SG; q++) {
-      float2* dst = P.sim[3 * s0 + q] + base;
-      for (int e = tid; e < TS; e += T) {
-        int w = e & (W - 1), k = e >> lw;
-        if (w < nw) dst[(size_t)k * kstride + w] = res[(k * SG + q) * W + w];
-      }
+    for (int e = tid; e < TS; e += T) {
+      const int w = e & (W - 1), k = e >> lw;
+      if (w >= nw) continue;
+      const size_t go = base + (size_t)k * kstride + w;
+      const float2* r = res + k * SG * W + w;
+#pragma unroll
+      for (int q = 0; q < 6; q++)
+        if (q < SG) P.sim[3 * s0 + q][go] = r[q * W];
     }
     __syncthreads();
   }
@@ -696,13 +728,15 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     for (int g0 = gs0; g0 < 9; g0 += GT)
       fft_lines<true, 1>(R + g0 * W, SC, min(GT, 9 - g0) * W, 1, G * W, P.zp, tw);
   }
-#pragma unroll 1
-  for (int g = 0; g < 9; g++) {
-    float2* dst = (g < 6 ? P.cov[g] : P.mean[g - 6]) + base;
-    const float2* src = (four && g >= gs0) ? SC : R;
-    for (int e = tid; e < TS; e += T) {
-      int w = e & (W - 1), k = e >> lw;
-      if (w < nw) dst[(size_t)k * kstride + w] = src[(k * G + g) * W + w];
+  for (int e = tid; e < TS; e += T) {
+    const int w = e & (W - 1), k = e >> lw;
+    if (w >= nw) continue;
+    const size_t go = base + (size_t)k * kstride + w;
+    const int so = k * G * W + w;
+#pragma unroll
+    for (int g = 0; g < 9; g++) {
+      const float2* src = (four && g >= gs0) ? SC : R;
+      (g < 6 ? P.cov[g] : P.mean[g - 6])[go] = src[so + g * W];
     }
   }
 
