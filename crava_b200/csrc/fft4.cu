@@ -23,19 +23,20 @@ namespace crava {
 // ------------------------------------------------------------------ strided lines
 //
 // One tile of W columns (nw of them valid) of the lines through g: point p of column w at
-// g[p pstride + w].  Shared layout of the W lines: element (w, p = t + N2 m) at
+// g[p pstride + w], read from src[p spstride + w] (g itself, or a staged copy of the tile in
+// shared memory).  Shared layout of the W lines: element (w, p = t + N2 m) at
 // p W + w + m SK, with SK chosen so that the pass-2 reads of neighbouring k2 fall on
 // disjoint banks.  Needs tw (the length-N table) in shared memory; ends with a barrier.
 template <int N1, int N2, int DIR>
-__device__ __forceinline__ void line4_tile(float2* g, int nw, size_t pstride, int W, int lw, int SK,
-                                           const float2* tw, float2* Y) {
+__device__ __forceinline__ void line4_tile(const float2* srcb, size_t spstride, float2* g, int nw, size_t pstride,
+                                           int W, int lw, int SK, const float2* tw, float2* Y) {
   const int T = blockDim.x, tid = threadIdx.x;
-  const size_t mstride = (size_t)N2 * pstride;
+  const size_t mstride = (size_t)N2 * spstride;
   const int mpitch = N2 * W + SK;
   for (int q = tid; q < W * N2; q += T) {
     const int w = q & (W - 1), t = q >> lw;
     const bool ok = w < nw;
-    const float2* src = g + (size_t)t * pstride + w;
+    const float2* src = srcb + (size_t)t * spstride + w;
     float2* y = Y + t * W + w;
     four_step_pass1<N1, N2, DIR>(
         t, tw, [&](int, int m) { return ok ? src[m * mstride] : make_float2(0.f, 0.f); },
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(256) k_line4(const __grid_constant__ GridSet g
   const int i0 = it * W, nw = min(W, ni - i0);
   float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)o * ostride + i0;
   __syncthreads();
-  line4_tile<N1, N2, DIR>(g, nw, pstride, W, lw, SK, tw, sm + N);
+  line4_tile<N1, N2, DIR>(g, pstride, g, nw, pstride, W, lw, SK, tw, sm + N);
 }
 
 // ------------------------------------------------------------------ rows, even nxp
@@ -150,20 +151,14 @@ __device__ __forceinline__ void xr2c4_rows(const float2* src, float2* dst, int n
 
 // nr rows of half spectra in g (pitch h + 1) to scaled real rows in place; the merge step
 // as k_x_c2r (kernels.cu).  Z: rpc * PITCH, Xs: rpc * (h + 1).  Ends with a barrier.
+// The same from rows already staged in Xs (shared), writing g.
 template <int N1, int N2>
-__device__ __forceinline__ void xc2r4_rows(float2* g, int nr, float scale, const float2* tw, const float2* twh,
-                                           float2* Z, float2* Xs) {
+__device__ __forceinline__ void xc2r4_staged(const float2* Xs, float2* g, int nr, float scale, const float2* tw,
+                                             const float2* twh, float2* Z) {
   using L = RowLayout<N1, N2>;
   constexpr int H = L::H, PITCH = L::PITCH;
   constexpr int CN = H + 1, NP = H / 2 + 1;
   const int T = blockDim.x, tid = threadIdx.x;
-  {
-    const uint32_t xb = smem_addr(Xs);
-    for (int e = tid; e < nr * CN; e += T) cp_async8(xb + 8u * (uint32_t)e, g + e);
-    cp_async_commit();
-    cp_async_wait_0();
-  }
-  __syncthreads();
   for (int e = tid; e < nr * NP; e += T) {
     const int r = e / NP, k = e - r * NP;
     const float2* X = Xs + r * CN;
@@ -203,6 +198,20 @@ __device__ __forceinline__ void xc2r4_rows(float2* g, int nr, float scale, const
     if (k2 == 0) X[H] = make_float2(0.f, 0.f);
   }
   __syncthreads();
+}
+
+template <int N1, int N2>
+__device__ __forceinline__ void xc2r4_rows(float2* g, int nr, float scale, const float2* tw, const float2* twh,
+                                           float2* Z, float2* Xs) {
+  constexpr int CN = N1 * N2 + 1;
+  {
+    const uint32_t xb = smem_addr(Xs);
+    for (int e = threadIdx.x; e < nr * CN; e += blockDim.x) cp_async8(xb + 8u * (uint32_t)e, g + e);
+    cp_async_commit();
+    cp_async_wait_0();
+  }
+  __syncthreads();
+  xc2r4_staged<N1, N2>(Xs, g, nr, scale, tw, twh, Z);
 }
 
 template <int N1, int N2>
@@ -246,6 +255,117 @@ __global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet g
   }
   __syncthreads();
   xc2r4_rows<N1, N2>(g, nr, gs.scale[blockIdx.y], tw, twh, Z, Z + rpc * L::PITCH);
+}
+
+// ------------------------------------------------------------------ persistent, pipelined
+//
+// The same row and column transforms as persistent CTAs that stage the next unit's input
+// in shared memory with cp.async while the current unit is transformed: every CTA keeps one
+// unit of loads in flight during its arithmetic.  Units are disjoint row chunks or column
+// tiles, each read and written by the one CTA that owns it, so in-place grids are safe.
+
+template <int N1, int N2, bool FWD>
+__global__ void __launch_bounds__(256) k_x4p(const __grid_constant__ GridSet gs, int rows, int rpc, int nchunk,
+                                             const float2* __restrict__ twg, const float2* __restrict__ twn) {
+  using L = RowLayout<N1, N2>;
+  constexpr int H = N1 * N2, CN = H + 1;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* twh = tw + H;
+  float2* const X0 = twh + H;
+  float2* const X1 = X0 + rpc * CN;
+  float2* Z = X1 + rpc * CN;
+  for (int t = threadIdx.x; t < H; t += blockDim.x) {
+    tw[t] = twg[t];
+    twh[t] = twn[t];
+  }
+  const int units = gs.n * nchunk;
+  auto issue = [&](int u, float2* buf) {
+    const int gi = u / nchunk, c = u - gi * nchunk;
+    const int row0 = c * rpc, nr = min(rpc, rows - row0);
+    const float2* src = reinterpret_cast<const float2*>(FWD ? gs.src[gi] : gs.p[gi]) + (size_t)row0 * CN;
+    const uint32_t b = smem_addr(buf);
+    for (int e = threadIdx.x; e < nr * CN; e += blockDim.x) cp_async8(b + 8u * (uint32_t)e, src + e);
+  };
+  if ((int)blockIdx.x < units) issue(blockIdx.x, X0);
+  cp_async_commit();
+  int i = 0;
+  for (int u = blockIdx.x; u < units; u += gridDim.x, i ^= 1) {
+    if (u + (int)gridDim.x < units) issue(u + gridDim.x, i ? X0 : X1);
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncthreads();
+    const int gi = u / nchunk, c = u - gi * nchunk;
+    const int row0 = c * rpc, nr = min(rpc, rows - row0);
+    float2* dst = reinterpret_cast<float2*>(gs.p[gi]) + (size_t)row0 * CN;
+    const float2* cur = i ? X1 : X0;
+    if (FWD) xr2c4_rows<N1, N2>(cur, dst, nr, gs.scale[gi], tw, twh, Z);
+    else xc2r4_staged<N1, N2>(cur, dst, nr, gs.scale[gi], tw, twh, Z);
+  }
+  cp_async_wait_0();
+  (void)L::PITCH;
+}
+
+template <int N1, int N2, int DIR>
+__global__ void __launch_bounds__(256) k_line4p(const __grid_constant__ GridSet gs, int ni, size_t pstride, int no,
+                                                size_t ostride, int W, int lw, int nIT, int SK,
+                                                const float2* __restrict__ twg) {
+  constexpr int N = N1 * N2;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* const T0 = sm + N;
+  float2* const T1 = T0 + W * N;
+  float2* Y = T1 + W * N;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twg[t];
+  const int per_grid = nIT * no, units = gs.n * per_grid;
+  auto locate = [&](int u, int& nw) -> float2* {
+    const int gi = u / per_grid, rem = u - gi * per_grid;
+    const int o = rem / nIT, it = rem - o * nIT;
+    nw = min(W, ni - it * W);
+    return reinterpret_cast<float2*>(gs.p[gi]) + (size_t)o * ostride + (size_t)it * W;
+  };
+  auto issue = [&](int u, float2* buf) {
+    int nw;
+    const float2* g = locate(u, nw);
+    const uint32_t b = smem_addr(buf);
+    for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
+      const int p = e >> lw, w = e & (W - 1);
+      const bool ok = w < nw;
+      cp_async8_zfill(b + 8u * (uint32_t)e, ok ? g + (size_t)p * pstride + w : g, ok);
+    }
+  };
+  if ((int)blockIdx.x < units) issue(blockIdx.x, T0);
+  cp_async_commit();
+  int i = 0;
+  for (int u = blockIdx.x; u < units; u += gridDim.x, i ^= 1) {
+    if (u + (int)gridDim.x < units) issue(u + gridDim.x, i ? T0 : T1);
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncthreads();
+    int nw;
+    float2* g = locate(u, nw);
+    line4_tile<N1, N2, DIR>(i ? T1 : T0, (size_t)W, g, nw, pstride, W, lw, SK, tw, Y);
+  }
+  cp_async_wait_0();
+}
+
+static bool pipe4_enabled() {
+  static const bool on = [] {
+    const char* ev = getenv("CRAVA_PIPE4");
+    return !(ev && ev[0] == '0');
+  }();
+  return on;
+}
+
+static cudaError_t resident_grid(const void* fn, int T, size_t smem, int units, int* grid) {
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  *grid = std::max(1, std::min(units, per_sm * nsm));
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ fused xy passes
@@ -295,12 +415,12 @@ __global__ void __launch_bounds__(256, 2) k_xy4(const __grid_constant__ GridSet 
       __threadfence();  // acquire side: no line of this plane cached before the barrier is reused
       for (int it = rank; it < ntile; it += C) {
         const int i0 = it * W;
-        line4_tile<NY1, NY2, -1>(dst + i0, min(W, CN - i0), (size_t)CN, W, lw, SK, ty, work);
+        line4_tile<NY1, NY2, -1>(dst + i0, (size_t)CN, dst + i0, min(W, CN - i0), (size_t)CN, W, lw, SK, ty, work);
       }
     } else {
       for (int it = rank; it < ntile; it += C) {
         const int i0 = it * W;
-        line4_tile<NY1, NY2, 1>(dst + i0, min(W, CN - i0), (size_t)CN, W, lw, SK, ty, work);
+        line4_tile<NY1, NY2, 1>(dst + i0, (size_t)CN, dst + i0, min(W, CN - i0), (size_t)CN, W, lw, SK, ty, work);
       }
       __threadfence();
       cl.sync();
@@ -355,6 +475,27 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   const int SK = W < 16 ? (((W - N2 * W) % 16) + 16) % 16 : 0;
   const int T = std::min(256, round_up32(W * std::max(N1, N2)));
   const int nIT = (ni + W - 1) / W;
+  if (pipe4_enabled()) {
+    // two staged tiles and the work tile: narrower tiles for the longest lines
+    int Wp = W;
+    while (Wp > 1 && sizeof(float2) * (2 * (size_t)Wp * N) + line4_smem<N1, N2>(Wp, SK) > 104 * 1024) Wp /= 2;
+    int lwp = 0;
+    while ((1 << lwp) < Wp) lwp++;
+    const int SKp = Wp < 16 ? (((Wp - N2 * Wp) % 16) + 16) % 16 : 0;
+    const int Tp = std::min(256, round_up32(Wp * std::max(N1, N2)));
+    const int nITp = (ni + Wp - 1) / Wp;
+    const size_t smem = sizeof(float2) * ((size_t)N + 2 * (size_t)Wp * N) + line4_smem<N1, N2>(Wp, SKp);
+    const void* fn = sign < 0.f ? (const void*)k_line4p<N1, N2, -1> : (const void*)k_line4p<N1, N2, 1>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int grid = 0;
+    if ((e = resident_grid(fn, Tp, smem, gs.n * nITp * no, &grid)) != cudaSuccess) return e;
+    if (sign < 0.f)
+      k_line4p<N1, N2, -1><<<grid, Tp, smem, st>>>(gs, ni, pstride, no, ostride, Wp, lwp, nITp, SKp, tw);
+    else
+      k_line4p<N1, N2, 1><<<grid, Tp, smem, st>>>(gs, ni, pstride, no, ostride, Wp, lwp, nITp, SKp, tw);
+    return cudaGetLastError();
+  }
   const size_t smem = sizeof(float2) * (size_t)N + line4_smem<N1, N2>(W, SK);
   const void* fn = sign < 0.f ? (const void*)k_line4<N1, N2, -1> : (const void*)k_line4<N1, N2, 1>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -371,6 +512,18 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   const int T = 256;
   int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
   if (const char* ev = getenv("CRAVA_X4_RPC")) rpc = std::max(1, std::min(rpc, atoi(ev)));
+  if (pipe4_enabled()) {
+    const int nchunk = (rows + rpc - 1) / rpc;
+    const size_t smem = sizeof(float2) * (2 * (size_t)L::H + 2 * (size_t)rpc * (L::H + 1) + (size_t)rpc * L::PITCH);
+    const void* fn = fwd ? (const void*)k_x4p<N1, N2, true> : (const void*)k_x4p<N1, N2, false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int grid = 0;
+    if ((e = resident_grid(fn, T, smem, gs.n * nchunk, &grid)) != cudaSuccess) return e;
+    if (fwd) k_x4p<N1, N2, true><<<grid, T, smem, st>>>(gs, rows, rpc, nchunk, tw, twn);
+    else k_x4p<N1, N2, false><<<grid, T, smem, st>>>(gs, rows, rpc, nchunk, tw, twn);
+    return cudaGetLastError();
+  }
   const size_t smem = sizeof(float2) * 2 * (size_t)L::H + x4_smem<N1, N2>(fwd, rpc);
   const void* fn = fwd ? (const void*)k_xr2c4<N1, N2> : (const void*)k_xc2r4<N1, N2>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
