@@ -349,10 +349,12 @@ __global__ void __launch_bounds__(256) k_line4p(const __grid_constant__ GridSet 
   cp_async_wait_0();
 }
 
+// Opt-in (CRAVA_PIPE4=1): measured slower than the one-unit kernels for the column
+// transforms (staging a W-column tile costs more than it hides) and mixed for the rows.
 static bool pipe4_enabled() {
   static const bool on = [] {
     const char* ev = getenv("CRAVA_PIPE4");
-    return !(ev && ev[0] == '0');
+    return ev && ev[0] == '1';
   }();
   return on;
 }
