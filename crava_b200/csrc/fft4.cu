@@ -470,6 +470,7 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   constexpr int N = N1 * N2;
   int W = 8;
   if (const char* ev = getenv("CRAVA_LINE4_W")) W = std::max(1, atoi(ev));
+  if (const char* ev = getenv(sign < 0.f ? "CRAVA_LINE4_WF" : "CRAVA_LINE4_WI")) W = std::max(1, atoi(ev));
   while (W > 1 && W / 2 >= ni) W /= 2;
   int lw = 0;
   while ((1 << lw) < W) lw++;
@@ -511,7 +512,8 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
 template <int N1, int N2>
 static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, const float2* twn, cudaStream_t st) {
   using L = RowLayout<N1, N2>;
-  const int T = 256;
+  int T = 256;
+  if (const char* ev = getenv("CRAVA_X4_T")) T = std::max(64, std::min(256, atoi(ev) / 32 * 32));
   int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
   if (const char* ev = getenv("CRAVA_X4_RPC")) rpc = std::max(1, std::min(rpc, atoi(ev)));
   if (pipe4_enabled()) {
