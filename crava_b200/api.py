@@ -26,15 +26,16 @@ OK, EINVAL, ENOMEM, ECUDA, ETIMEDOUT, ENUMERIC, ENOTSUP, ESTATE = range(8)
 ROLE_DATA, ROLE_MEAN, ROLE_PRIOR_COV, ROLE_ERR_CORR, ROLE_POST_COV, ROLE_SIM, ROLE_NOISE, \
     ROLE_RESIDUAL, ROLE_POST_MEAN = range(9)
 PRIOR_SEPARABLE, PRIOR_GRIDS = 0, 1
-FLAG_HOST_NOISE, FLAG_KEEP_RESIDUAL, FLAG_SPECTRAL_COV = 1, 2, 4
+FLAG_HOST_NOISE, FLAG_KEEP_RESIDUAL, FLAG_SPECTRAL_COV, FLAG_NONCONST_THICK = 1, 2, 4, 8
 
 # exported symbols the header declares (checked by the CPU tests)
 EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_status_string",
            "crava_job_create", "crava_job_destroy", "crava_job_footprint", "crava_job_upload",
            "crava_job_download", "crava_job_device_ptr", "crava_job_run", "crava_job_counters",
            "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches", "crava_ctx_set_profiling",
-           "crava_ctx_kernel_times"]
-KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r", "xy_fwd", "xy_inv"]
+           "crava_ctx_kernel_times", "crava_job_divide_data"]
+KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r", "xy_fwd", "xy_inv", "thick_divide",
+                  "thick_fill"]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
 
 
@@ -56,7 +57,8 @@ class JobDesc(ctypes.Structure):
                 ("A", _dp), ("err_theta_cov", _dp), ("wavelet", _fp), ("wavelet_norm", _fp),
                 ("prior_var0", _dp), ("prior_mode", ctypes.c_int), ("corr_xy", _fp),
                 ("circ_corr_t", _fp), ("nsim", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("flags", ctypes.c_int), ("fp64_threshold", ctypes.c_float)]
+                ("flags", ctypes.c_int), ("fp64_threshold", ctypes.c_float),
+                ("rel_thick", _dp), ("energy_threshold", ctypes.c_float)]
 
 
 class Counters(ctypes.Structure):
@@ -99,6 +101,7 @@ def lib() -> ctypes.CDLL:
     L.crava_job_download.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
     L.crava_job_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.crava_job_run.argtypes = [vp, vp]
+    L.crava_job_divide_data.argtypes = [vp, vp]
     L.crava_job_counters.argtypes = [vp, ctypes.POINTER(Counters)]
     L.crava_fft_r2c.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
     L.crava_fft_c2r.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
@@ -196,6 +199,11 @@ def make_desc(blk, prior_mode: int = PRIOR_SEPARABLE, flags: int = 0, seed: Opti
     d.seed = int(blk.seed if seed is None else seed) & ((1 << 64) - 1)
     d.flags = flags
     d.fp64_threshold = float(fp64_threshold)
+    if getattr(blk, "rel_thick", None) is not None:
+        keep["relt"] = np.ascontiguousarray(blk.rel_thick, dtype=np.float64)
+        d.rel_thick = keep["relt"].ctypes.data_as(_dp)
+        d.energy_threshold = float(blk.energy_threshold)
+        d.flags |= FLAG_NONCONST_THICK
     return d, keep
 
 
@@ -213,6 +221,8 @@ class Job:
                  seed: Optional[int] = None, nsim: Optional[int] = None, fp64_threshold: float = 0.0):
         self.ctx = ctx
         self.blk = blk
+        if getattr(blk, "rel_thick", None) is not None:
+            flags |= FLAG_NONCONST_THICK
         self.flags = flags
         self.prior_mode = prior_mode
         self.nsim = blk.nsim if nsim is None else nsim
@@ -242,6 +252,11 @@ class Job:
 
     def run(self, stream=None):
         _check(lib().crava_job_run(self._h, stream))
+
+    def divide_data(self, stream=None):
+        """divideDataByScaleWavelet + interpolateSeismic on the uploaded data (non-constant
+        thickness jobs); returns after the work is done."""
+        _check(lib().crava_job_divide_data(self._h, stream))
 
     def counters(self) -> dict:
         c = Counters()
@@ -309,6 +324,8 @@ def invert_block(ctx: Context, blk, prior_mode=PRIOR_SEPARABLE, noise=None, keep
     job = Job(ctx, blk, prior_mode, flags, seed=seed, fp64_threshold=fp64_threshold)
     try:
         _keep = job.upload_block(cov_grids, err_corr, noise)
+        if job.flags & FLAG_NONCONST_THICK:
+            job.divide_data()
         job.run()
         out = job.download_outputs()
         out["counters"] = job.counters()

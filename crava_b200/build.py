@@ -7,13 +7,14 @@ from __future__ import annotations
 
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrava_gpu.so")
-SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "facies.cu"]
+SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "facies.cu", "thick.cu"]
 HEADERS = ["fft_core.cuh", "fft2.cuh", "kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -34,19 +35,23 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    for s in SOURCES:
+    def compile_one(s):
         src = os.path.join(CSRC, s)
         obj = os.path.join(objdir, s.replace(".cu", ".o"))
         cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed for {s}:\n{r.stdout}\n{r.stderr}")
-        if ptxas_info:
-            sys.stderr.write(r.stderr)
-        objs.append(obj)
+        return s, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    objs = []
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        for s, obj, r in ex.map(compile_one, SOURCES):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {s}:\n{r.stdout}\n{r.stderr}")
+            if ptxas_info:
+                sys.stderr.write(r.stderr)
+            objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -90,7 +90,7 @@ struct Plan {
 
 // Per-kernel-class CUDA-event timing (off unless crava_ctx_set_profiling enables it).
 enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_XY_FWD = 5, KT_XY_INV = 6,
-       KT_COUNT = 7 };
+       KT_THICK_DIVIDE = 7, KT_THICK_FILL = 8, KT_COUNT = 9 };
 
 struct ProfRec {
   int cat;
@@ -164,8 +164,15 @@ struct crava_job {
   float2* ct = nullptr;
   float* cxy_grid = nullptr; // staging for the corr_xy transform
   unsigned long long* counters = nullptr;
+  // CRAVA_FLAG_NONCONST_THICK: per-kz diagonal error terms, the data pre-processing
+  // parameters (device tables inside) and its work buffers
+  float* edk = nullptr;
+  double* eddk = nullptr;
+  ThickParams tp{};
+  float* energy = nullptr;
+  TraceOp* ops = nullptr;
   // host copies of the small inputs
-  std::vector<double> A, etc, pv;
+  std::vector<double> A, etc, pv, relt;
   std::vector<float> wav, wnorm, corr_xy, circ;
   bool ran = false;
   bool async = false;             // pool from cudaMallocAsync on alloc_stream
@@ -231,13 +238,38 @@ crava_status validate(const crava_job_desc* d) {
     return fail(CRAVA_EINVAL, "unknown prior mode");
   }
   if (!(d->lz > 0)) return fail(CRAVA_EINVAL, "lz must be positive");
-  if (d->flags & ~(CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL | CRAVA_FLAG_SPECTRAL_COV))
+  if (d->flags & ~(CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL | CRAVA_FLAG_SPECTRAL_COV |
+                   CRAVA_FLAG_NONCONST_THICK))
     return fail(CRAVA_EINVAL, "unknown flag");
+  if (d->flags & CRAVA_FLAG_NONCONST_THICK) {
+    if (!d->rel_thick || !d->circ_corr_t)
+      return fail(CRAVA_EINVAL, "non-constant thickness needs rel_thick and circ_corr_t");
+    for (size_t q = 0; q < (size_t)d->nxp * d->nyp; q++)
+      if (!(d->rel_thick[q] > 0) || !(d->rel_thick[q] < INFINITY))
+        return fail(CRAVA_EINVAL, "rel_thick must be finite and positive");
+    if (!(d->energy_threshold >= 0.f) || !(d->energy_threshold < INFINITY))
+      return fail(CRAVA_EINVAL, "energy_threshold must be finite and >= 0");
+    if (!(d->circ_corr_t[0] != 0.f)) return fail(CRAVA_EINVAL, "circ_corr_t[0] must be nonzero");
+    if (thick_tile_width(d->nzp) < 1) return fail(CRAVA_ENOTSUP, "nzp too long for the trace transform");
+  }
   if (!(d->fp64_threshold >= 0.f) || !(d->fp64_threshold < INFINITY))
     return fail(CRAVA_EINVAL, "fp64_threshold must be finite and >= 0");
   for (int l = 0; l < d->ntheta; l++)
     if (!(d->wavelet_norm[l] > 0)) return fail(CRAVA_EINVAL, "wavelet norm must be positive");
   return CRAVA_OK;
+}
+
+// Device bytes of the non-constant-thickness tables and work buffers (0 without the flag):
+// per-angle adjustment tables, the taper,
+// fill and distance tables, rel_thick, the trace energies and the interpolation plan.
+size_t thick_bytes(const crava_job_desc* d) {
+  if (!(d->flags & CRAVA_FLAG_NONCONST_THICK)) return 0;
+  const size_t nth = d->ntheta, cnzp = d->nzp / 2 + 1, nxy = (size_t)d->nx * d->ny;
+  return 2 * align256(sizeof(float2) * nth * cnzp) + align256(sizeof(float) * nth * cnzp) +
+         2 * align256(sizeof(float) * d->nzp) + align256(sizeof(int) * d->nxp) + align256(sizeof(int) * d->nyp) +
+         align256(sizeof(float) * d->nxp) + align256(sizeof(float) * d->nyp) +
+         align256(sizeof(double) * d->nxp * d->nyp) + align256(sizeof(float) * nth * nxy) +
+         align256(sizeof(TraceOp) * nth * nxy);
 }
 
 size_t footprint(const crava_job_desc* d) {
@@ -250,8 +282,9 @@ size_t footprint(const crava_job_desc* d) {
   size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) + align256(sizeof(float2) * d->nzp * sep_stride) +
                   3 * align256(sizeof(double2) * d->nzp * d->ntheta) + align256(d->nzp) +
                   align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float2) * d->nzp) +
-                  align256(sizeof(float) * 2 * cnxp * d->nyp) + 256;
-  return ngrids * gb + tables;
+                  align256(sizeof(float) * 2 * cnxp * d->nyp) + 256 + align256(sizeof(float) * d->nzp * d->ntheta) +
+                  align256(sizeof(double) * d->nzp * d->ntheta);
+  return ngrids * gb + tables + thick_bytes(d);
 }
 
 // DFT of a real vector in double precision, e^{-2 pi i k t / n}.
@@ -280,9 +313,47 @@ std::vector<cd> dft(const std::vector<double>& x) {
 
 // Per-kz operator tables, constant-thickness branch of computePostMeanResidAndFFTCov.
 // With kwd/e1d/e2d given, the same three tables are also written in double.
+double j_etc(const crava_job_desc& d, int l) { return d.err_theta_cov[l * d.ntheta + l]; }
+
+// Wavelet::getCAmp(k, scale) (src/wavelet.cpp:337-382) on a float spectrum c[0..cnzp),
+// in float as the reference evaluates it.
+std::complex<float> camp_scaled_host(const std::vector<std::complex<float>>& c, int nzp, int k, float scale) {
+  const int cn = nzp / 2 + 1;
+  const bool mirror = k >= cn;
+  const float om = float(mirror ? nzp - k : k) / scale;
+  if (om >= cn) return {0.f, 0.f};
+  const int lo = int(std::floor(om));
+  int hi = lo + 1;
+  if (hi >= cn) hi -= 1;
+  const float dO = om - float(lo);
+  float re = c[lo].real() * (1.0f - dO) + c[hi].real() * dO;
+  float im = c[lo].imag() * (1.0f - dO) + c[hi].imag() * dO;
+  if (mirror) im = -im;
+  return {re / scale, im / scale};
+}
+
+// fillInverseAbskWRobust (src/avoinversion.cpp:1296-1322): 1/|W(k)| from the larger of the
+// spectrum and the spectrum sampled at 0.999 stretch, per kz; a large number where both vanish.
+std::vector<double> inverse_abs_kw_robust(const std::vector<cd>& W, int n, float wnorm) {
+  const int cn = n / 2 + 1;
+  std::vector<std::complex<float>> c(cn);
+  for (int k = 0; k < cn; k++) c[k] = {(float)W[k].real(), (float)W[k].imag()};
+  std::vector<double> out(n);
+  for (int k = 0; k < n; k++) {
+    const std::complex<float> v = k < cn ? c[k] : std::conj(c[n - k]);
+    const std::complex<float> vf = camp_scaled_host(c, n, k, 0.999f);
+    const float m = v.real() * v.real() + v.imag() * v.imag();
+    const float mf = vf.real() * vf.real() + vf.imag() * vf.imag();
+    const float mx = std::max(m, mf);
+    out[k] = mx > 0.0f ? (double)float(1.0 / std::sqrt(mx)) : (double)(wnorm * n * n * 100.0f);
+  }
+  return out;
+}
+
 void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vector<float2>& e1,
-                     std::vector<float2>& e2, std::vector<uint8_t>& inv, std::vector<double2>* kwd = nullptr,
-                     std::vector<double2>* e1d = nullptr, std::vector<double2>* e2d = nullptr) {
+                     std::vector<float2>& e2, std::vector<uint8_t>& inv, std::vector<double2>* kwd,
+                     std::vector<double2>* e1d,std::vector<double2>* e2d, std::vector<float>& edk,
+                     std::vector<double>* eddk) {
   int n = d.nzp, nth = d.ntheta;
   kw.assign((size_t)n * nth, make_float2(0, 0));
   e1 = kw;
@@ -298,6 +369,22 @@ void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vect
   d1[0] = -1.0;
   d1[n - 1] = 1.0;
   std::vector<cd> kD = dft(d1);
+  // diff3Operator = central(backward(diff1Operator)) (src/avoinversion.cpp:842-848)
+  // diagonal error term wnc errThetaCov_ll |e3_l(k)|^2; e3 = 1 for constant thickness
+  edk.assign((size_t)n * nth, 0.f);
+  if (eddk) eddk->assign((size_t)n * nth, 0.0);
+  for (int k = 0; k < n; k++)
+    for (int l = 0; l < nth; l++) {
+      edk[(size_t)k * nth + l] = float(d.wnc * j_etc(d, l));
+      if (eddk) (*eddk)[(size_t)k * nth + l] = d.wnc * j_etc(d, l);
+    }
+  std::vector<cd> kD3;
+  if (d.flags & CRAVA_FLAG_NONCONST_THICK) {
+    std::vector<double> f2(n), f3(n);
+    for (int i = 0; i < n; i++) f2[i] = (i == 0) ? d1[0] - d1[n - 1] : d1[i] - d1[i - 1];
+    for (int i = 0; i < n; i++) f3[i] = 0.5 * (f2[(i + 1) % n] - f2[(i + n - 1) % n]);
+    kD3 = dft(f3);
+  }
   for (int l = 0; l < nth; l++) {
     std::vector<float> wf(d.wavelet + (size_t)l * n, d.wavelet + (size_t)(l + 1) * n);
     std::vector<double> w(wf.begin(), wf.end());
@@ -317,10 +404,23 @@ void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vect
     std::vector<double> e3(f3.begin(), f3.end());
     std::vector<cd> E3 = dft(e3);
     double wn = d.wavelet_norm[l];
+    const bool nonconst = (d.flags & CRAVA_FLAG_NONCONST_THICK) != 0;
+    std::vector<double> e3r;
+    if (nonconst) e3r = inverse_abs_kw_robust(W, n, d.wavelet_norm[l]);
     for (int k = 0; k < n; k++) {
       cd kwv = std::conj(W[k]) * kD[k];
       cd a = std::conj(W[k]) / wn;
       cd b = norm3 > 0 ? std::conj(E3[k]) / (double)norm3 : cd(0, 0);
+      if (nonconst) {
+        // K = kD A, errMult1 = 1/|w|, errMult2 = kD3/|errorSmooth3|, errMult3 = robust
+        // 1/|W| (src/avoinversion.cpp:976-1014, fillInverseAbskWRobust :1296-1322)
+        kwv = kD[k];
+        a = cd(1.0f / d.wavelet_norm[l], 0.0);
+        b = norm3 > 0 ? kD3[k] * (double)(1.0f / norm3) : cd(0, 0);
+        const double ev = (double)d.wnc * j_etc(d, l) * e3r[k] * e3r[k];
+        edk[(size_t)k * nth + l] = (float)ev;
+        if (eddk) (*eddk)[(size_t)k * nth + l] = ev;
+      }
       kw[(size_t)k * nth + l] = make_float2((float)kwv.real(), (float)kwv.imag());
       e1[(size_t)k * nth + l] = make_float2((float)a.real(), (float)a.imag());
       e2[(size_t)k * nth + l] = make_float2((float)b.real(), (float)b.imag());
@@ -336,6 +436,113 @@ void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vect
     int kk = std::min(k, n - k);
     float rf = static_cast<float>((d.nz * 1000.0f) / (d.lz * n) * kk);
     inv[k] = (rf > d.low_cut * d.min_rel_thick && rf < d.high_cut) ? 1 : 0;
+  }
+}
+
+// Host tables of the data pre-processing of one job (computeAdjustmentFactor,
+// src/avoinversion.cpp:630-719, and the taper/fill helpers of FFTGrid), in the float
+// arithmetic of the reference wherever it computes in float.
+struct ThickTables {
+  std::vector<float2> wamp, es3;
+  std::vector<float> tau2, ztaper, distx, disty, distz;
+  std::vector<int> fillx, filly;
+  float wn2[kMaxTheta], modW[kMaxTheta], err_var[kMaxTheta];
+};
+
+void build_thick_tables(const crava_job_desc& d, ThickTables& t) {
+  const int n = d.nzp, cn = n / 2 + 1, nth = d.ntheta;
+  t.wamp.assign((size_t)nth * cn, make_float2(0, 0));
+  t.es3 = t.wamp;
+  t.tau2.assign((size_t)nth * cn, 0.f);
+  // Wavelet::findNormWithinFrequencyBand (src/wavelet.cpp:903-925) with the wavelet's dz
+  const float dz = (float)(d.lz / d.nz);
+  const float dOmega = static_cast<float>(1.0 / (n * dz * 0.001));
+  const int loI = std::max(0, (int)std::floor(d.low_cut / dOmega));
+  const int hiI = std::min(cn, (int)std::ceil(d.high_cut / dOmega));
+  const float maxfreq = static_cast<float>((n / 2) * 1000.0 * d.nz) / static_cast<float>(d.lz * n);
+  // getPriorCorrTFiltered (src/seismicparametersholder.cpp:842-868) of the temporal
+  // correlation circCorrT / circCorrT[0] (extractParamCorrFromCovVp, :1008-1028)
+  std::vector<float> corrT(n);
+  for (int i = 0; i < n; i++) {
+    const int refk = i < n / 2 + 1 ? i : n - i;
+    corrT[i] = refk < d.nz ? d.circ_corr_t[refk] / d.circ_corr_t[0] : 0.f;
+  }
+  for (int l = 0; l < nth; l++) {
+    const float* wf = d.wavelet + (size_t)l * n;
+    std::vector<cd> W = dft(std::vector<double>(wf, wf + n));
+    // errorSmooth3 = central(backward(forward(w))) in float (src/wavelet1D.cpp:441-500)
+    std::vector<float> f1(n), f2(n), f3(n);
+    for (int i = 0; i < n; i++) f1[i] = (i == n - 1) ? wf[0] - wf[i] : wf[i + 1] - wf[i];
+    for (int i = 0; i < n; i++) f2[i] = (i == 0) ? f1[0] - f1[n - 1] : f1[i] - f1[i - 1];
+    for (int i = 0; i < n; i++) f3[i] = (float)(0.5 * (f2[(i + 1) % n] - f2[(i + n - 1) % n]));
+    std::vector<cd> E3 = dft(std::vector<double>(f3.begin(), f3.end()));
+    std::vector<std::complex<float>> e3f(cn);
+    for (int k = 0; k < cn; k++) e3f[k] = {(float)E3[k].real(), (float)E3[k].imag()};
+    const double fac = 1.0 / double(n);
+    double norm2 = 0.0;
+    for (int i = loI; i < hiI; i++)
+      norm2 += static_cast<double>(2.0 * fac * (e3f[i].real() * e3f[i].real() + e3f[i].imag() * e3f[i].imag()));
+    if (loI == 0) norm2 -= fac * (e3f[0].real() * e3f[0].real() + e3f[0].imag() * e3f[0].imag());
+    const float c3 = 1.0f / static_cast<float>(std::sqrt(norm2));
+    for (int k = 0; k < cn; k++) {
+      t.wamp[(size_t)l * cn + k] = make_float2((float)W[k].real(), (float)W[k].imag());
+      float2 v = make_float2(e3f[k].real() * c3, e3f[k].imag() * c3);
+      // multiplyRAmpByConstant (src/wavelet.cpp:507-515) writes RMISSING into the floats
+      // at index >= nzp of the complex array: the last entry's imaginary part, and its
+      // real part too when nzp is even
+      if (k == cn - 1) {
+        v.y = -99999.0f;
+        if (n % 2 == 0) v.x = -99999.0f;
+      }
+      t.es3[(size_t)l * cn + k] = v;
+    }
+    // reflection-coefficient time covariance (computeElasticImpedanceTimeCovariance +
+    // computeReflectionCoefficientTimeCovariance, src/avoinversion.cpp:369-401), then |Re|
+    // of its transform
+    const float Al[3] = {(float)d.A[l * 3 + 0], (float)d.A[l * 3 + 1], (float)d.A[l * 3 + 2]};
+    double eiVar = 0.0;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) eiVar += Al[a] * static_cast<float>(d.prior_var0[a * 3 + b]) * Al[b];
+    std::vector<float> rc(n);
+    for (int k = 0; k < n; k++) rc[k] = static_cast<float>(eiVar * corrT[k]);
+    {
+      const float first = rc[0];
+      float prev = rc[n - 1];
+      for (int i = 0; i < n - 1; i++) {
+        const float curr = rc[i], next = rc[i + 1];
+        rc[i] = 2 * curr - next - prev;
+        prev = curr;
+      }
+      rc[n - 1] = 2 * rc[n - 1] - first - prev;
+    }
+    std::vector<cd> RC = dft(std::vector<double>(rc.begin(), rc.end()));
+    for (int k = 0; k < cn; k++) t.tau2[(size_t)l * cn + k] = std::fabs((float)RC[k].real());
+    const float norm = d.wavelet_norm[l];
+    t.wn2[l] = norm * norm;
+    float modW = norm;
+    modW *= modW;
+    modW *= maxfreq / static_cast<float>(d.high_cut);
+    t.modW[l] = modW;
+    t.err_var[l] = static_cast<float>(j_etc(d, l));
+  }
+  t.ztaper.assign(n, 1.f);
+  t.distz.assign(n, 0.f);
+  for (int k = 0; k < n; k++) {
+    const float dk = dist_to_boundary(k, d.nz, n);
+    t.distz[k] = dk;
+    if (k > d.nz) t.ztaper[k] = std::max<float>(1 - dk * dk, 0);
+  }
+  t.distx.resize(d.nxp);
+  t.fillx.resize(d.nxp);
+  for (int i = 0; i < d.nxp; i++) {
+    t.distx[i] = dist_to_boundary(i, d.nx, d.nxp);
+    t.fillx[i] = fill_number(i, d.nx, d.nxp);
+  }
+  t.disty.resize(d.nyp);
+  t.filly.resize(d.nyp);
+  for (int i = 0; i < d.nyp; i++) {
+    t.disty[i] = dist_to_boundary(i, d.ny, d.nyp);
+    t.filly[i] = fill_number(i, d.ny, d.nyp);
   }
 }
 
@@ -583,8 +790,13 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->d.prior_var0 = j->pv.data();
   j->d.wavelet = j->wav.data();
   j->d.wavelet_norm = j->wnorm.data();
+  if (d.flags & CRAVA_FLAG_NONCONST_THICK) {
+    j->relt.assign(d.rel_thick, d.rel_thick + (size_t)d.nxp * d.nyp);
+    if (j->circ.empty()) j->circ.assign(d.circ_corr_t, d.circ_corr_t + d.nzp);
+  }
   j->d.corr_xy = j->corr_xy.empty() ? nullptr : j->corr_xy.data();
   j->d.circ_corr_t = j->circ.empty() ? nullptr : j->circ.data();
+  j->d.rel_thick = j->relt.empty() ? nullptr : j->relt.data();
 
   {
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -637,6 +849,46 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->ct = (float2*)take(sizeof(float2) * d.nzp);
   j->cxy_grid = (float*)take(sizeof(float) * j->rnxp * d.nyp);
   j->counters = (unsigned long long*)take(256);
+  ThickTables tt;
+  const bool nonconst = (d.flags & CRAVA_FLAG_NONCONST_THICK) != 0;
+  j->edk = (float*)take(sizeof(float) * d.nzp * d.ntheta);
+  j->eddk = (double*)take(sizeof(double) * d.nzp * d.ntheta);
+  if (nonconst) {
+    const size_t nth = d.ntheta, cn = d.nzp / 2 + 1, nxy = (size_t)d.nx * d.ny;
+    ThickParams& tp = j->tp;
+    tp.wamp = (const float2*)take(sizeof(float2) * nth * cn);
+    tp.es3 = (const float2*)take(sizeof(float2) * nth * cn);
+    tp.tau2 = (const float*)take(sizeof(float) * nth * cn);
+    tp.ztaper = (const float*)take(sizeof(float) * d.nzp);
+    tp.distz = (const float*)take(sizeof(float) * d.nzp);
+    tp.fillx = (const int*)take(sizeof(int) * d.nxp);
+    tp.filly = (const int*)take(sizeof(int) * d.nyp);
+    tp.distx = (const float*)take(sizeof(float) * d.nxp);
+    tp.disty = (const float*)take(sizeof(float) * d.nyp);
+    tp.rel_thick = (const double*)take(sizeof(double) * d.nxp * d.nyp);
+    j->energy = (float*)take(sizeof(float) * nth * nxy);
+    j->ops = (TraceOp*)take(sizeof(TraceOp) * nth * nxy);
+    build_thick_tables(d, tt);
+    tp.nx = d.nx; tp.ny = d.ny; tp.nz = d.nz;
+    tp.nxp = d.nxp; tp.nyp = d.nyp; tp.nzp = d.nzp;
+    tp.rnxp = j->rnxp;
+    tp.cnzp = (int)cn;
+    tp.W = thick_tile_width(d.nzp);
+    tp.logW = 0;
+    while ((1 << tp.logW) < tp.W) tp.logW++;
+    tp.nIT = ((d.nxp + 1) / 2 + tp.W - 1) / tp.W;
+    for (int l = 0; l < d.ntheta; l++) {
+      tp.grid[l] = j->in_data[l];
+      tp.wn2[l] = tt.wn2[l];
+      tp.modW[l] = tt.modW[l];
+      tp.err_var[l] = tt.err_var[l];
+    }
+    tp.wnc = d.wnc;
+    tp.low_cut = d.low_cut;
+    tp.high_cut = d.high_cut;
+    tp.rsq = static_cast<float>(std::sqrt(static_cast<float>(d.nzp)));
+    tp.lz = d.lz;
+  }
 #define JOB_TRY(call)                                          \
   do {                                                         \
     cudaError_t e_ = (call);                                   \
@@ -651,7 +903,27 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   std::vector<float2> kw, e1, e2;
   std::vector<double2> kwd, e1d, e2d;
   std::vector<uint8_t> inv;
-  build_kz_tables(j->d, kw, e1, e2, inv, &kwd, &e1d, &e2d);
+  std::vector<float> edk;
+  std::vector<double> eddk;
+  build_kz_tables(j->d, kw, e1, e2, inv, &kwd, &e1d, &e2d, edk, &eddk);
+  auto up = [&](const void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
+  };
+  JOB_TRY(up(j->edk, edk.data(), sizeof(float) * edk.size()));
+  JOB_TRY(up(j->eddk, eddk.data(), sizeof(double) * eddk.size()));
+  if (nonconst) {
+    ThickParams& tp = j->tp;
+    JOB_TRY(up(tp.wamp, tt.wamp.data(), sizeof(float2) * tt.wamp.size()));
+    JOB_TRY(up(tp.es3, tt.es3.data(), sizeof(float2) * tt.es3.size()));
+    JOB_TRY(up(tp.tau2, tt.tau2.data(), sizeof(float) * tt.tau2.size()));
+    JOB_TRY(up(tp.ztaper, tt.ztaper.data(), sizeof(float) * tt.ztaper.size()));
+    JOB_TRY(up(tp.distz, tt.distz.data(), sizeof(float) * tt.distz.size()));
+    JOB_TRY(up(tp.fillx, tt.fillx.data(), sizeof(int) * tt.fillx.size()));
+    JOB_TRY(up(tp.filly, tt.filly.data(), sizeof(int) * tt.filly.size()));
+    JOB_TRY(up(tp.distx, tt.distx.data(), sizeof(float) * tt.distx.size()));
+    JOB_TRY(up(tp.disty, tt.disty.data(), sizeof(float) * tt.disty.size()));
+    JOB_TRY(up(tp.rel_thick, j->relt.data(), sizeof(double) * j->relt.size()));
+  }
   JOB_TRY(cudaMemcpyAsync(j->kwd, kwd.data(), sizeof(double2) * kwd.size(), cudaMemcpyHostToDevice, st));
   JOB_TRY(cudaMemcpyAsync(j->e1d, e1d.data(), sizeof(double2) * e1d.size(), cudaMemcpyHostToDevice, st));
   JOB_TRY(cudaMemcpyAsync(j->e2d, e2d.data(), sizeof(double2) * e2d.size(), cudaMemcpyHostToDevice, st));
@@ -869,6 +1141,8 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   }
   zp.kz.kw = job->kw; zp.kz.e1 = job->e1; zp.kz.e2 = job->e2; zp.kz.inv = job->inv;
   zp.kz.kwd = job->kwd; zp.kz.e1d = job->e1d; zp.kz.e2d = job->e2d;
+  zp.kz.ed = job->edk;     // null unless CRAVA_FLAG_NONCONST_THICK
+  zp.kz.edd = job->eddk;
   zp.fp64_threshold = d.fp64_threshold;
   for (int l = 0; l < d.ntheta; l++) {
     for (int c = 0; c < 3; c++) zp.Ad[l][c] = job->A[l * 3 + c];
@@ -914,6 +1188,59 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out) {
   for (int q = 0; q < 6; q++) CUDA_TRY(cudaMemcpy(&v[q], job->cov[q], sizeof(float), cudaMemcpyDeviceToHost));
   float P[9] = {v[0], v[3], v[4], v[3], v[1], v[5], v[4], v[5], v[2]};
   std::memcpy(out->post_var0, P, sizeof(P));
+  return CRAVA_OK;
+}
+
+crava_status crava_job_divide_data(crava_job* job, void* stream) {
+  if (!job) return fail(CRAVA_EINVAL, "null job");
+  const crava_job_desc& d = job->d;
+  if (!(d.flags & CRAVA_FLAG_NONCONST_THICK))
+    return fail(CRAVA_ESTATE, "crava_job_divide_data needs a job with CRAVA_FLAG_NONCONST_THICK");
+  crava_ctx* ctx = job->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  Plan* pz;
+  crava_status s;
+  if ((s = get_plan(ctx, d.nzp, &pz, true))) return s;
+  ThickParams& tp = job->tp;
+  tp.zp = pz->lp;
+  tp.twz = pz->tw;
+  const int nth = d.ntheta;
+  const size_t nxy = (size_t)d.nx * d.ny;
+  int nl = 0;
+  // divideDataByScaleWavelet, then the trace energies of interpolateSeismic
+  {
+    ProfScope ps(ctx, KT_THICK_DIVIDE, st);
+    CUDA_TRY(launch_thick_divide(tp, nth, st, &nl));
+  }
+  {
+    ProfScope ps(ctx, KT_THICK_FILL, st);
+    CUDA_TRY(launch_trace_energy(tp, nth, job->energy, st, &nl));
+  }
+  std::vector<float> energy(nth * nxy);
+  CUDA_TRY(cudaMemcpyAsync(energy.data(), job->energy, sizeof(float) * energy.size(), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  // per angle: the interpolation plan (host), its levels in order, then the extrapolation
+  std::vector<std::vector<TraceOp>> ops(nth);
+  for (int l = 0; l < nth; l++) {
+    std::vector<int> level_start;
+    int box[4];
+    plan_trace_interpolation(energy.data() + l * nxy, d.nx, d.ny, d.energy_threshold, ops[l], level_start, box);
+    TraceOp* dops = job->ops + l * nxy;
+    if (!ops[l].empty())
+      CUDA_TRY(cudaMemcpyAsync(dops, ops[l].data(), sizeof(TraceOp) * ops[l].size(), cudaMemcpyHostToDevice, st));
+    ProfScope ps(ctx, KT_THICK_FILL, st);
+    for (size_t L = 1; L + 1 < level_start.size(); L++)
+      CUDA_TRY(launch_trace_interp(tp.grid[l], job->rnxp, d.nyp, d.nzp, d.nx, dops + level_start[L],
+                                   level_start[L + 1] - level_start[L], st, &nl));
+    // no good trace at all: the reference would clamp into an empty box; nothing is copied
+    if (box[0] <= box[1] && box[2] <= box[3]) CUDA_TRY(launch_extrapolate(tp, l, box, st, &nl));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->launches += nl;
+  }
   return CRAVA_OK;
 }
 
@@ -1034,8 +1361,11 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   if (d.prior_mode != CRAVA_PRIOR_SEPARABLE)
     return fail(CRAVA_ENOTSUP, "crava_invert_noalloc takes the separable prior only");
   if (d.fp64_threshold > 0.f) return fail(CRAVA_ENOTSUP, "crava_invert_noalloc runs FP32 only");
-  if (d.flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL | CRAVA_FLAG_SPECTRAL_COV))
-    return fail(CRAVA_ENOTSUP, "crava_invert_noalloc supports neither host noise nor residual output");
+  if (d.flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_KEEP_RESIDUAL | CRAVA_FLAG_SPECTRAL_COV |
+                 CRAVA_FLAG_NONCONST_THICK))
+    return fail(CRAVA_ENOTSUP,
+                "crava_invert_noalloc supports neither host noise, residual or spectral output nor non-constant "
+                "thickness");
   const int nin = d.ntheta + 3, nout = 9 + 3 * d.nsim;
   for (int q = 0; q < nin; q++)
     if (!d_in[q]) return fail(CRAVA_EINVAL, "null input grid");
@@ -1067,6 +1397,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   const size_t o_e1 = take(sizeof(float2) * d.nzp * d.ntheta);
   const size_t o_e2 = take(sizeof(float2) * d.nzp * d.ntheta);
   const size_t o_inv = take(d.nzp);
+  const size_t o_ed = take(sizeof(float) * d.nzp * d.ntheta);
   const size_t o_cxy = take(sizeof(float) * rnxp * d.nyp);
   const size_t o_ct = take(sizeof(float2) * d.nzp);
   const size_t o_cnt = take(4 * sizeof(unsigned long long));
@@ -1079,7 +1410,8 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   // host-built tables, copied into the scratch on the stream
   std::vector<float2> kw, e1, e2;
   std::vector<uint8_t> inv;
-  build_kz_tables(d, kw, e1, e2, inv);
+  std::vector<float> edk;
+  build_kz_tables(d, kw, e1, e2, inv, nullptr, nullptr, nullptr, edk, nullptr);
   std::vector<double> c(d.circ_corr_t, d.circ_corr_t + d.nzp);
   std::vector<cd> C = dft(c);
   std::vector<float2> ct(d.nzp);
@@ -1098,6 +1430,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   CUDA_TRY(put(o_e1, e1.data(), sizeof(float2) * e1.size()));
   CUDA_TRY(put(o_e2, e2.data(), sizeof(float2) * e2.size()));
   CUDA_TRY(put(o_inv, inv.data(), inv.size()));
+  CUDA_TRY(put(o_ed, edk.data(), sizeof(float) * edk.size()));
   CUDA_TRY(put(o_ct, ct.data(), sizeof(float2) * ct.size()));
   CUDA_TRY(put(o_cxy, gxy.data(), sizeof(float) * gxy.size()));
   CUDA_TRY(cudaMemsetAsync(base + o_cnt, 0, 4 * sizeof(unsigned long long), st));
@@ -1160,6 +1493,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   zp.kz.e1 = (const float2*)(base + o_e1);
   zp.kz.e2 = (const float2*)(base + o_e2);
   zp.kz.inv = (const uint8_t*)(base + o_inv);
+  zp.kz.ed = (const float*)(base + o_ed);
   zp.zp = pz.lp;
   zp.twz = twz;
   zp.seed = d.seed;
@@ -1477,8 +1811,8 @@ crava_status crava_serve_submit(crava_server* sv, const crava_job_desc* desc, co
   if (!sv || !desc || !host_in || !ticket) return fail(CRAVA_EINVAL, "null argument");
   crava_status s = validate(desc);
   if (s) return s;
-  if (desc->prior_mode != CRAVA_PRIOR_SEPARABLE || (desc->flags & CRAVA_FLAG_HOST_NOISE))
-    return fail(CRAVA_ENOTSUP, "served jobs take the separable prior and device noise");
+  if (desc->prior_mode != CRAVA_PRIOR_SEPARABLE || (desc->flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_NONCONST_THICK)))
+    return fail(CRAVA_ENOTSUP, "served jobs take the separable prior, device noise and constant thickness");
   ServeReq* r = new ServeReq();
   r->d = *desc;
   const int nth = desc->ntheta;

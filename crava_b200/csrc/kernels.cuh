@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fft_core.cuh"
 
 namespace crava {
@@ -29,6 +31,8 @@ struct KzTables {
   const double2* kwd;   // the same three tables in double, read by the FP64
   const double2* e1d;   //   re-factorisation of flagged bins
   const double2* e2d;
+  const float* ed;      // nzp x nth : wnc errThetaCov_ll |e3_l(k)|^2 (e3 = 1 for constant
+  const double* edd;    //   thickness); edd in double, null: the per-angle constants edd
 };
 
 struct ZParams {
@@ -79,6 +83,51 @@ struct FaciesBoxHost {
   int rs;
   size_t fstride;
 };
+
+// Non-constant-thickness data pre-processing (thick.cu).  Per-angle tables of
+// computeAdjustmentFactor over kz < cnzp: wamp the wavelet spectrum (cAmp), es3 the
+// band-normalised spectrum of the third difference of the wavelet, tau2 |Re| of the
+// reflection-coefficient covariance spectrum.
+struct ThickParams {
+  int nx, ny, nz, nxp, nyp, nzp, rnxp, cnzp;
+  int W, logW, nIT;            // W complex lines (2W traces) per CTA, log2 W, tiles per row
+  float* grid[kMaxTheta];      // the data grids, processed in place
+  const double* rel_thick;     // nxp x nyp, Simbox::getRelThick(i, j)
+  const float2* wamp;          // nth x cnzp
+  const float2* es3;           // nth x cnzp
+  const float* tau2;           // nth x cnzp
+  const float* ztaper;         // nzp: 1, or max(1 - dist^2, 0) for kz > nz
+  const int* fillx;            // nxp, nyp: getFillNumber of every padded index
+  const int* filly;
+  const float* distx;          // nxp, nyp, nzp: getDistToBoundary of every padded index
+  const float* disty;
+  const float* distz;
+  float wn2[kMaxTheta];        // (wavelet norm)^2
+  float modW[kMaxTheta];       // norm^2 * maxfrequency / highCut
+  float err_var[kMaxTheta];    // errThetaCov_ll
+  float wnc, low_cut, high_cut;
+  float rsq;                   // float(sqrt(float(nzp)))
+  double lz;
+  LinePlan zp;
+  const float2* twz;
+};
+// One interpolateTrace: trace t (i + nx j) <- mean of nb[] (left, right, up, down; -1 absent)
+struct TraceOp {
+  int t;
+  int nb[4];
+  int nt;
+};
+size_t thick_smem_bytes(int W, int nzp);
+int thick_tile_width(int nzp);
+cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, int* nlaunch);
+cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, cudaStream_t st, int* nlaunch);
+cudaError_t launch_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, const TraceOp* ops, int nops,
+                                cudaStream_t st, int* nlaunch);
+cudaError_t launch_extrapolate(const ThickParams& P, int l, const int box[4], cudaStream_t st, int* nlaunch);
+float dist_to_boundary(int i, int n, int np);
+int fill_number(int i, int n, int np);
+void plan_trace_interpolation(const float* energy, int nx, int ny, float threshold, std::vector<TraceOp>& ops,
+                              std::vector<int>& level_start, int box[4]);
 
 // four-step launchers (fft4.cu): lengths of its size table only
 bool four_step_supported(int n);

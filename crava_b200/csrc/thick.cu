@@ -1,0 +1,375 @@
+// Non-constant-thickness pre-processing of the seismic data (sm_100a):
+//
+//   AVOInversion::divideDataByScaleWavelet + computeAdjustmentFactor
+//     (src/avoinversion.cpp:484-719): every trace (i, j) of the padded grid is tapered in
+//     the z padding, transformed along z, multiplied inside the band by a per-trace factor
+//     that swaps the trace's stretched wavelet for a global one, and transformed back;
+//   FFTGrid::interpolateSeismic / interpolateTrace / extrapolateSeismic
+//     (src/fftgrid.cpp:2349-2516): traces whose energy is at or below the threshold are
+//     replaced by the mean of their good neighbours, and every trace outside the box of
+//     good traces (the lateral padding included) by a tapered copy of its mirror trace.
+//
+// The trace transform packs two real traces (x = 2m, 2m + 1, adjacent floats) into one
+// complex line, transforms W such lines of one (j, angle) together in shared memory with
+// the Stockham engine, separates the two half spectra, multiplies each by its own factor,
+// recombines them and transforms back: one read and one write of the grid.  The factor is
+// evaluated per (trace, kz) in the reference's float arithmetic with explicitly rounded
+// operations (no contraction into FMA), so it equals the reference's float value for the
+// same tables.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace crava {
+
+namespace {
+
+__device__ __forceinline__ float sq2(float2 v) { return __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)); }
+
+// Wavelet::getCAmp(k, scale) for k < cnzp (src/wavelet.cpp:337-382): the spectrum of the
+// wavelet stretched by `scale`, linear interpolation at k / scale, divided by scale.
+__device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, float scale) {
+  const float om = __fdiv_rn((float)k, scale);
+  if (!(om < (float)cnzp)) return make_float2(0.f, 0.f);
+  const int lo = (int)floorf(om);
+  int hi = lo + 1;
+  if (hi >= cnzp) hi -= 1;
+  const float d = __fsub_rn(om, (float)lo);
+  const float e = __fsub_rn(1.f, d);
+  const float2 a = __ldg(c + lo), b = __ldg(c + hi);
+  const float re = __fadd_rn(__fmul_rn(a.x, e), __fmul_rn(b.x, d));
+  const float im = __fadd_rn(__fmul_rn(a.y, e), __fmul_rn(b.y, d));
+  return make_float2(__fdiv_rn(re, scale), __fdiv_rn(im, scale));
+}
+
+// computeAdjustmentFactor (src/avoinversion.cpp:630-719) at one kz < cnzp for a trace
+// whose wavelet is stretched by sf; local wavelet = global wavelet (1D wavelet without
+// local shift or gain grids), so eSkGlob uses the unstretched spectrum of the same tables.
+__device__ __forceinline__ float2 adjustment(const ThickParams& P, int l, int k, float sf) {
+  const int cn = P.cnzp;
+  const float2* wa = P.wamp + (size_t)l * cn;
+  const float2* es = P.es3 + (size_t)l * cn;
+  const float wn2 = P.wn2[l], wnc = P.wnc, ev = P.err_var[l];
+  const float2 wLoc = camp_scaled(wa, cn, k, sf);
+  const float wLoc2 = sq2(wLoc);
+  const float2 wGlob = __ldg(wa + k);
+  const float wGlob2 = sq2(wGlob);
+  const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(camp_scaled(es, cn, k, sf)));
+  const float sG = __fadd_rn(__fdiv_rn(wGlob2, wn2), sq2(__ldg(es + k)));
+  const float c = __fmul_rn(__fsub_rn(1.f, wnc), 0.5f);
+  float s2L = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sL)));
+  const float s2G = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sG)));
+  const float tau2 = __ldg(P.tau2 + (size_t)l * cn + k);
+  const float tm = __fmul_rn(0.05f, P.modW[l]);
+  float wG2A = wGlob2, wL2A = wLoc2;
+  if (wGlob2 < tm) wG2A = __fmul_rn(0.5f, __fadd_rn(wGlob2, tm));
+  if (wLoc2 < tm) wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, tm));
+  const float tg = __fmul_rn(0.05f, wG2A);
+  if (wL2A < tg) {
+    wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, tg));
+    s2L = __fmul_rn(s2L, __fdiv_rn(wL2A, wLoc2));
+  }
+  const float dL = __fadd_rn(__fmul_rn(tau2, wL2A), s2L);
+  const float q = __fdiv_rn(wG2A, __fadd_rn(__fmul_rn(tau2, wGlob2), s2G));
+  return make_float2(__fdiv_rn(__fdiv_rn(wLoc.x, dL), q), __fdiv_rn(__fdiv_rn(wLoc.y, dL), q));
+}
+
+// One CTA: W complex lines (2W traces x = 2(m0 + w) + {0, 1}) of row j of angle blockIdx.z.
+__global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ ThickParams P) {
+  extern __shared__ float2 sm[];
+  const int nzp = P.nzp, W = P.W, lw = P.logW, half = nzp / 2;
+  float2* tw = sm;
+  float2* R = tw + nzp;
+  float2* SC = R + (size_t)W * nzp;
+  __shared__ float s_sf[2 * 32];
+  __shared__ double s_df[2 * 32];
+  __shared__ int s_live[2 * 32];   // the trace has a nonzero tapered sample
+  const int tid = threadIdx.x, T = blockDim.x;
+  const int j = blockIdx.y, l = blockIdx.z;
+  const int m0 = blockIdx.x * W;
+  float* g = P.grid[l];
+  const size_t kstride = (size_t)P.nyp * P.rnxp;
+  float* row = g + (size_t)j * P.rnxp;
+  for (int t = tid; t < nzp; t += T) tw[t] = P.twz[t];
+  // per trace: stretch sf = relThick (float, as getCAmp receives it) and
+  // deltaF = nz*1000 / (relThick * lz * nzp) (src/avoinversion.cpp:557-560)
+  if (tid < 2 * W) {
+    const int i = 2 * m0 + tid;
+    double rt = 1.0;
+    if (i < P.nxp) rt = P.rel_thick[(size_t)j * P.nxp + i];
+    s_sf[tid] = (float)rt;
+    s_df[tid] = __ddiv_rn(__dmul_rn((double)P.nz, 1000.0), __dmul_rn(__dmul_rn(rt, P.lz), (double)nzp));
+    s_live[tid] = 0;
+  }
+  __syncthreads();
+  // load, 1/sqrt(nzp) and the z taper (:539-551); traces at or beyond nxp load as zero.
+  // A trace whose tapered samples are all zero (a dead trace) is stored back as exact
+  // zeros, as the reference's own real transform returns it, although the trace sharing
+  // its complex line leaks rounding into it.
+  for (int e = tid; e < W * nzp; e += T) {
+    const int w = e & (W - 1), k = e >> lw;
+    const int m = m0 + w;
+    float2 v = make_float2(0.f, 0.f);
+    if (2 * m < P.nxp) {
+      const float* p = row + (size_t)k * kstride + 2 * m;
+      if (2 * m + 1 < P.nxp) v = *reinterpret_cast<const float2*>(p);
+      else v.x = *p;
+      const float tz = __ldg(P.ztaper + k);
+      v.x = __fmul_rn(__fdiv_rn(v.x, P.rsq), tz);
+      v.y = __fmul_rn(__fdiv_rn(v.y, P.rsq), tz);
+      if (v.x != 0.f) s_live[2 * w] = 1;
+      if (v.y != 0.f) s_live[2 * w + 1] = 1;
+    }
+    R[e] = v;
+  }
+  __syncthreads();
+  fft_lines<true, -1>(R, SC, W, 1, W, P.zp, tw);
+  __syncthreads();
+  // half spectra of the two traces, Z = A + iB: A(k) = (Z(k) + conj Z(-k)) / 2,
+  // B(k) = (Z(k) - conj Z(-k)) / 2i; factor and band per trace; the c2r of the reference
+  // ignores the imaginary parts at DC and Nyquist; Z'(k) = A' + iB', Z'(-k) = conj A' + i conj B'
+  for (int e = tid; e < W * (half + 1); e += T) {
+    const int w = e & (W - 1), k = e >> lw;
+    const int kk = (k == 0) ? 0 : nzp - k;
+    const float2 z = R[k * W + w], zc = R[kk * W + w];
+    float2 a = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    float2 b = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    const int m = m0 + w;
+    float2 fa = make_float2(0.f, 0.f), fb = fa;
+    if (2 * m < P.nxp) {
+      const double fk = __dmul_rn(s_df[2 * w], (double)k);
+      if (fk < (double)P.high_cut && fk > (double)P.low_cut) fa = adjustment(P, l, k, s_sf[2 * w]);
+    }
+    if (2 * m + 1 < P.nxp) {
+      const double fk = __dmul_rn(s_df[2 * w + 1], (double)k);
+      if (fk < (double)P.high_cut && fk > (double)P.low_cut) fb = adjustment(P, l, k, s_sf[2 * w + 1]);
+    }
+    a = cmul(a, fa);
+    b = cmul(b, fb);
+    if (k == 0 || 2 * k == nzp) {
+      a.y = 0.f;
+      b.y = 0.f;
+    }
+    R[k * W + w] = make_float2(a.x - b.y, a.y + b.x);
+    if (kk != k) R[kk * W + w] = make_float2(a.x + b.y, b.x - a.y);
+  }
+  __syncthreads();
+  fft_lines<true, 1>(R, SC, W, 1, W, P.zp, tw);
+  __syncthreads();
+  for (int e = tid; e < W * nzp; e += T) {
+    const int w = e & (W - 1), k = e >> lw;
+    const int m = m0 + w;
+    if (2 * m >= P.nxp) continue;
+    float* p = row + (size_t)k * kstride + 2 * m;
+    const float2 v = R[e];
+    const float2 o = make_float2(s_live[2 * w] ? __fdiv_rn(v.x, P.rsq) : 0.f,
+                                 s_live[2 * w + 1] ? __fdiv_rn(v.y, P.rsq) : 0.f);
+    if (2 * m + 1 < P.nxp) *reinterpret_cast<float2*>(p) = o;
+    else *p = o.x;
+  }
+}
+
+// Energy of every interior trace over its first nz samples, summed in order in float
+// (src/fftgrid.cpp:2360-2371).
+__global__ void k_trace_energy(const __grid_constant__ ThickParams P, float* energy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, l = blockIdx.z;
+  if (i >= P.nx) return;
+  const float* g = P.grid[l] + (size_t)j * P.rnxp + i;
+  const size_t kstride = (size_t)P.nyp * P.rnxp;
+  float e = 0.f;
+  for (int k = 0; k < P.nz; k++) {
+    const float v = g[(size_t)k * kstride];
+    e = __fadd_rn(e, __fmul_rn(v, v));
+  }
+  energy[((size_t)l * P.ny + j) * P.nx + i] = e;
+}
+
+// interpolateTrace (src/fftgrid.cpp:2440-2480) for a list of independent operations: the
+// target trace becomes the mean of its listed neighbours (left, right, up, down order).
+__global__ void k_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, const TraceOp* ops) {
+  const TraceOp op = ops[blockIdx.x];
+  const size_t kstride = (size_t)nyp * rnxp;
+  for (int k = blockIdx.y * blockDim.x + threadIdx.x; k < nzp; k += gridDim.y * blockDim.x) {
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int n = op.nb[q];
+      if (n >= 0) s = __fadd_rn(s, g[(size_t)k * kstride + (size_t)(n / nx) * rnxp + n % nx]);
+    }
+    g[(size_t)k * kstride + (size_t)(op.t / nx) * rnxp + op.t % nx] = __fdiv_rn(s, (float)op.nt);
+  }
+}
+
+// extrapolateSeismic (src/fftgrid.cpp:2484-2516): every voxel of a trace outside the box
+// of good traces takes the value of its mirror trace (getFillNumber, clamped into the box)
+// times (max(1 - dx^2 - dy^2 - dz^2, 0))^3 of the distances to the boundary.  The mirror
+// traces lie inside the box, which this kernel never writes.
+__global__ void k_extrapolate(const __grid_constant__ ThickParams P, int l, int imin, int imax, int jmin, int jmax) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= P.nxp) return;
+  if (!(i < imin || i > imax || j < jmin || j > jmax)) return;
+  int ri = __ldg(P.fillx + i), rj = __ldg(P.filly + j);
+  ri = ri < imin ? imin : (ri > imax ? imax : ri);
+  rj = rj < jmin ? jmin : (rj > jmax ? jmax : rj);
+  float* g = P.grid[l] + (size_t)k * P.nyp * P.rnxp;
+  const float v = g[(size_t)rj * P.rnxp + ri];
+  const float dx = __ldg(P.distx + i), dy = __ldg(P.disty + j), dz = __ldg(P.distz + k);
+  double t = 1.0 - (double)__fmul_rn(dx, dx);
+  t -= (double)__fmul_rn(dy, dy);
+  t -= (double)__fmul_rn(dz, dz);
+  t = t > 0.0 ? t : 0.0;
+  const float mult = (float)(t * t * t);
+  g[(size_t)j * P.rnxp + i] = __fmul_rn(mult, v);
+}
+
+}  // namespace
+
+size_t thick_smem_bytes(int W, int nzp) { return sizeof(float2) * ((size_t)nzp + 2 * (size_t)W * nzp); }
+
+int thick_tile_width(int nzp) {
+  for (int W = 16; W >= 1; W /= 2)
+    if (thick_smem_bytes(W, nzp) <= 100 * 1024) return W;
+  return 0;
+}
+
+cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, int* nlaunch) {
+  if (P.W < 1 || P.W > 32 || (P.W & (P.W - 1)) || (1 << P.logW) != P.W) return cudaErrorInvalidValue;
+  const size_t smem = thick_smem_bytes(P.W, P.nzp);
+  cudaError_t e = cudaFuncSetAttribute(k_thick_divide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)P.nIT, (unsigned)P.nyp, (unsigned)nth);
+  k_thick_divide<<<grid, 256, smem, st>>>(P);
+  if (nlaunch) (*nlaunch)++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, cudaStream_t st, int* nlaunch) {
+  dim3 grid((unsigned)((P.nx + 127) / 128), (unsigned)P.ny, (unsigned)nth);
+  k_trace_energy<<<grid, 128, 0, st>>>(P, energy);
+  if (nlaunch) (*nlaunch)++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, const TraceOp* ops, int nops,
+                                cudaStream_t st, int* nlaunch) {
+  if (nops <= 0) return cudaSuccess;
+  dim3 grid((unsigned)nops, (unsigned)((nzp + 255) / 256));
+  k_trace_interp<<<grid, 256, 0, st>>>(g, rnxp, nyp, nzp, nx, ops);
+  if (nlaunch) (*nlaunch)++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extrapolate(const ThickParams& P, int l, const int box[4], cudaStream_t st, int* nlaunch) {
+  dim3 grid((unsigned)((P.nxp + 127) / 128), (unsigned)P.nyp, (unsigned)P.nzp);
+  k_extrapolate<<<grid, 128, 0, st>>>(P, l, box[0], box[1], box[2], box[3]);
+  if (nlaunch) (*nlaunch)++;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ host side
+
+// FFTGrid::getDistToBoundary (src/fftgrid.cpp:1158-1197) for 0 <= i < np.
+float dist_to_boundary(int i, int n, int np) {
+  if (i < n) return 0.f;
+  const float taper = static_cast<float>(std::min(n, np - n) / 2.1);
+  const int below = np - i, above = i - (n - 1);
+  return above < below ? static_cast<float>(above) / taper : static_cast<float>(below) / taper;
+}
+
+// FFTGrid::getFillNumber (src/fftgrid.cpp:1103-1141) for 0 <= i < np.
+int fill_number(int i, int n, int np) {
+  if (i < n) return i;
+  const int below = np - i - 1, above = i - n + 1;
+  return above < below ? std::max(n - above, n / 2) : std::min(below, n / 2);
+}
+
+// The control flow of FFTGrid::interpolateSeismic (src/fftgrid.cpp:2349-2437) and
+// interpolateTrace (:2440-2480) on the energy map of one angle: which trace is replaced
+// by the mean of which neighbours, in the reference's order.  It depends on the flags
+// only, never on the trace values, so it is planned here and executed on the device.  Each
+// operation gets a level one above the highest level among the operations that produced
+// its neighbours; operations of one level are independent (every trace is written at most
+// once, and only traces with even flags -- good or already interpolated -- are read).
+// Returns the operations grouped by level (level_start[L] .. level_start[L+1]) and the
+// box of good traces {imin, imax, jmin, jmax}.
+void plan_trace_interpolation(const float* energy, int nx, int ny, float threshold, std::vector<TraceOp>& ops,
+                              std::vector<int>& level_start, int box[4]) {
+  const int n = nx * ny;
+  std::vector<short> flags(n);
+  float total = 0.f;
+  for (int q = 0; q < n; q++) total += energy[q];
+  const float limit = threshold * total / float(n);
+  int imin = nx, imax = 0, jmin = ny, jmax = 0, flag = 0;
+  for (int j = 0, q = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++, q++) {
+      const int cur = energy[q] <= limit ? 1 : 0;
+      flags[q] = (short)(flag + cur);
+      if (cur == 1) {
+        flag = 2;
+      } else {
+        imin = std::min(imin, i);
+        imax = std::max(imax, i);
+        jmin = std::min(jmin, j);
+        jmax = std::max(jmax, j);
+      }
+    }
+  std::vector<int> level(n, 0);
+  std::vector<TraceOp> raw;
+  auto interp = [&](int index, int i, int j) -> int {
+    const bool left = i > 0 && flags[index - 1] % 2 == 0;
+    const bool right = i < nx - 1 && flags[index + 1] % 2 == 0;
+    const bool up = j > 0 && flags[index - nx] % 2 == 0;
+    const bool down = j < ny - 1 && flags[index + nx] % 2 == 0;
+    const int nt = (int)left + (int)right + (int)up + (int)down;
+    if (nt > 1) {
+      TraceOp op;
+      op.t = index;
+      op.nb[0] = left ? index - 1 : -1;
+      op.nb[1] = right ? index + 1 : -1;
+      op.nb[2] = up ? index - nx : -1;
+      op.nb[3] = down ? index + nx : -1;
+      op.nt = nt;
+      int lv = 0;
+      for (int q = 0; q < 4; q++)
+        if (op.nb[q] >= 0) lv = std::max(lv, level[op.nb[q]]);
+      level[index] = lv + 1;
+      raw.push_back(op);
+      flags[index]--;
+    }
+    return flags[index];
+  };
+  for (int j = 0, cur = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++, cur++) {
+      if (flags[cur] % 2 != 1) continue;
+      if (interp(cur, i, j) % 2 != 0) continue;
+      int index = cur - 1;
+      while (index >= 0 && flags[index] > 1) {
+        if (flags[index] % 2 == 1) interp(index, index % nx, index / nx);
+        index--;
+      }
+      if (index < 0) index = 0;
+      index++;
+      while (index <= cur && flags[index - 1] == 0) {
+        if (flags[index] > 1) flags[index] -= 2;
+        index++;
+      }
+    }
+  int maxl = 0;
+  for (const TraceOp& op : raw) maxl = std::max(maxl, level[op.t]);
+  level_start.assign(maxl + 2, 0);
+  for (const TraceOp& op : raw) level_start[level[op.t] + 1]++;
+  for (int L = 1; L < (int)level_start.size(); L++) level_start[L] += level_start[L - 1];
+  ops.assign(raw.size(), TraceOp{});
+  std::vector<int> fillp(level_start.begin(), level_start.end());
+  for (const TraceOp& op : raw) ops[fillp[level[op.t]]++] = op;
+  box[0] = imin;
+  box[1] = imax;
+  box[2] = jmin;
+  box[3] = jmax;
+}
+
+}  // namespace crava

@@ -152,7 +152,7 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
         Sd[l][m] = make_float2(g * (kw[l].x * kw[m].x + kw[l].y * kw[m].y) + lam * b.x,
                                g * (kw[l].y * kw[m].x - kw[l].x * kw[m].y) + lam * b.y);
       }
-      Sd[l][l] = make_float2(Sd[l][l].x + P.ed[l], 0.f);
+      Sd[l][l] = make_float2(Sd[l][l].x + __ldg(P.kz.ed + k * NTH + l), 0.f);
 #pragma unroll
       for (int j = 0; j < 3; j++) {
         const float a = rho * P.AP[l][j];
@@ -185,7 +185,8 @@ __device__ __forceinline__ bool bin_posterior(const ZParams& P, int k, const flo
         float2 ee = make_float2(e1[l].x * e1[m].x + e1[l].y * e1[m].y + e2[l].x * e2[m].x + e2[l].y * e2[m].y,
                                 e1[l].y * e1[m].x - e1[l].x * e1[m].y + e2[l].y * e2[m].x - e2[l].x * e2[m].y);
         Sd[l][m] = make_float2(kk.x * g + c * ee.x, kk.y * g + c * ee.y);
-        if (l == m) Sd[l][m] = make_float2(Sd[l][m].x + P.ed[l], 0.f);
+        if (l == m)
+          Sd[l][m] = make_float2(Sd[l][m].x + __ldg(P.kz.ed + k * NTH + l), 0.f);
       }
 #pragma unroll
       for (int j = 0; j < 3; j++) Y[l][j] = make_float2(kw[l].x * AS[l][j], kw[l].y * AS[l][j]);
@@ -340,7 +341,7 @@ __device__ __noinline__ bool bin_posterior_fp64(const ZParams& P, int k, const f
       double2 ee = make_double2(e1[l].x * e1[m].x + e1[l].y * e1[m].y + e2[l].x * e2[m].x + e2[l].y * e2[m].y,
                                 e1[l].y * e1[m].x - e1[l].x * e1[m].y + e2[l].y * e2[m].x - e2[l].x * e2[m].y);
       Sd[l][m] = make_double2(kk.x * g + c * ee.x, kk.y * g + c * ee.y);
-      if (l == m) Sd[l][m] = make_double2(Sd[l][m].x + P.edd[l], 0.0);
+      if (l == m) Sd[l][m] = make_double2(Sd[l][m].x + (P.kz.edd ? P.kz.edd[k * NTH + l] : P.edd[l]), 0.0);
       Sfull[l][m] = Sd[l][m];
       Sfull[m][l] = make_double2(Sd[l][m].x, -Sd[l][m].y);
     }

@@ -218,6 +218,25 @@ void AVOInversion::run() {
   d.seed = set_.seed;
   d.flags = CRAVA_FLAG_KEEP_RESIDUAL | (noise_ ? CRAVA_FLAG_HOST_NOISE : 0);
   d.fp64_threshold = set_.fp64Threshold;
+  // non-constant thickness: the temporal correlation the adjustment factor needs is the
+  // covVp column at (0, 0) (SeismicParametersHolder::extractParamCorrFromCovVp,
+  // src/seismicparametersholder.cpp:1008-1028) unless the separable factor is given
+  std::vector<float> corrCol;
+  if (!set_.relThick.empty()) {
+    if (set_.relThick.size() != (size_t)d.nxp * d.nyp)
+      throw Error(CRAVA_EINVAL, "AVOInversion: relThick needs nxp*nyp values");
+    d.flags |= CRAVA_FLAG_NONCONST_THICK;
+    d.rel_thick = set_.relThick.data();
+    d.energy_threshold = set_.energyThreshold;
+    if (!separable_) {
+      if (!sp_.covVp) throw Error(CRAVA_EINVAL, "AVOInversion: covVp is missing");
+      const float* cv = sp_.covVp->getRealData();
+      const size_t rnxp = 2 * (size_t)(d.nxp / 2 + 1);
+      corrCol.resize(d.nzp);
+      for (int k = 0; k < d.nzp; k++) corrCol[k] = cv[(size_t)k * rnxp * d.nyp];
+      d.circ_corr_t = corrCol.data();
+    }
+  }
 
   crava_job* job = nullptr;
   check(crava_job_create(ctx_->get(), &d, &job));
@@ -242,6 +261,8 @@ void AVOInversion::run() {
     if ((int)noise_->size() != 3 * nsim) throw Error(CRAVA_EINVAL, "simulate: 3 noise grids per realisation");
     for (int q = 0; q < 3 * nsim; q++) up(CRAVA_ROLE_NOISE, q, (*noise_)[q]);
   }
+  // the constructor's divideDataByScaleWavelet (src/avoinversion.cpp:226-227)
+  if (d.flags & CRAVA_FLAG_NONCONST_THICK) check(crava_job_divide_data(job, nullptr));
   check(crava_job_run(job, nullptr));
   // outputs in place of the inputs, as the reference overwrites them
   FFTGrid* mean[3] = {sp_.meanVp, sp_.meanVs, sp_.meanRho};

@@ -137,6 +137,11 @@ struct AVOInversionSettings {
   int nSimulations = 0;
   uint64_t seed = 1;                       // device noise (product mode)
   float fp64Threshold = 0;                 // 0: FP32 only
+  // Simbox::getIsConstantThick() == false: Simbox::getRelThick(i, j) at every padded trace
+  // (nxp*nyp, index i+nxp*j); the data are then divided by the scale wavelet first
+  // (divideDataByScaleWavelet + interpolateSeismic).  Empty: constant thickness.
+  std::vector<double> relThick;
+  float energyThreshold = 0;               // ModelSettings::getEnergyThreshold
 };
 
 class AVOInversion {

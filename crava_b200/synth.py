@@ -131,6 +131,8 @@ class Block:
     corr_grad_j: float = 0.0
     nsim: int = 1
     seed: int = 1
+    rel_thick: Optional[np.ndarray] = None   # (nyp, nxp) float64: non-constant thickness
+    energy_threshold: float = 0.0
 
     @property
     def ntheta(self) -> int:

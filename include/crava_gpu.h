@@ -77,11 +77,17 @@ enum {
   CRAVA_FLAG_HOST_NOISE = 1,   /* realisation noise uploaded by the caller (parity with a
                                   sequential generator such as the reference RandomGen)   */
   CRAVA_FLAG_KEEP_RESIDUAL = 2, /* keep the residual spectra for CRAVA_ROLE_RESIDUAL         */
-  CRAVA_FLAG_SPECTRAL_COV = 4   /* leave the posterior covariance in the Fourier domain, as
+  CRAVA_FLAG_SPECTRAL_COV = 4,  /* leave the posterior covariance in the Fourier domain, as
                                    the reference holds it between computePostMeanResidAndFFTCov
                                    and invFFTCovGrids (src/avoinversion.cpp:1071-1077,
                                    src/seismicparametersholder.cpp:432-456): CRAVA_ROLE_POST_COV
                                    then reads complex cnxp*nyp*nzp per-bin S_post           */
+  CRAVA_FLAG_NONCONST_THICK = 8 /* Simbox with non-constant thickness: the data are divided
+                                   by the per-trace scale wavelet first (crava_job_divide_data)
+                                   and the per-bin posterior uses K = kD A with the
+                                   wavelet-normalised error multipliers of the reference's
+                                   non-constant branch (src/avoinversion.cpp:976-1014);
+                                   needs rel_thick and circ_corr_t                          */
 };
 
 /* One inversion block: the scalars and small arrays AVOInversion reads from ModelSettings,
@@ -109,6 +115,10 @@ typedef struct {
                                   (max/min pivot)^2 of Sd > t, or S_post/S < 1/t on a
                                   diagonal entry, is re-factorised in FP64 with one
                                   iterative-refinement step of the data solve         */
+  /* CRAVA_FLAG_NONCONST_THICK only (ignored otherwise): */
+  const double* rel_thick;     /* nxp*nyp, Simbox::getRelThick(i, j) at every padded trace
+                                  (index i+nxp*j), all > 0                              */
+  float energy_threshold;      /* ModelSettings::getEnergyThreshold (interpolateSeismic) */
 } crava_job_desc;
 
 typedef struct {
@@ -150,6 +160,17 @@ crava_status crava_job_device_ptr(crava_job* job, crava_role role, int index, fl
 crava_status crava_job_run(crava_job* job, void* stream);
 crava_status crava_job_counters(crava_job* job, crava_counters* out);
 
+/* CRAVA_FLAG_NONCONST_THICK jobs: AVOInversion::divideDataByScaleWavelet
+ * (src/avoinversion.cpp:484-612, with computeAdjustmentFactor :630-719) followed by
+ * FFTGrid::interpolateSeismic (src/fftgrid.cpp:2349-2516) on every DATA grid, in place,
+ * as the reference's constructor does before the data transform (:226-227).  Call it
+ * after the DATA uploads and before crava_job_run.  The trace-interpolation plan is made
+ * on the host from the trace energies, so the call returns after `stream` has finished
+ * the work.  Wavelets are 1D without local shift or gain grids (the local wavelet of
+ * every trace is the global one stretched by rel_thick).  Returns CRAVA_ESTATE for a job
+ * without the flag. */
+crava_status crava_job_divide_data(crava_job* job, void* stream);
+
 /* FFTGrid drop-ins on a device grid (src/fftgrid.cpp:1587-1612 / 1615-1643).
  * covariance != 0 selects the COVARIANCE scaling. */
 crava_status crava_fft_r2c(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream);
@@ -168,7 +189,8 @@ long long crava_ctx_kernel_launches(crava_ctx* ctx);
  * With profiling on, every launch is bracketed by CUDA events on its stream.
  * crava_ctx_kernel_times waits for the recorded launches and returns, per class
  *   0 forward x transform, 1 forward line transforms, 2 fused pencil pass,
- *   3 inverse line transforms, 4 inverse x transform,
+ *   3 inverse line transforms, 4 inverse x transform, 5/6 fused xy pass forward/inverse,
+ *   7 trace division (crava_job_divide_data), 8 trace energies, interpolation, extrapolation,
  * the summed milliseconds and launch counts (n entries), then clears them if reset. */
 crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable);
 crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset);

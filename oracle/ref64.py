@@ -167,17 +167,312 @@ def per_kz_operators(blk):
     K = np.zeros((nzp, nth, 3), dtype=np.complex128)
     e1 = np.zeros((nzp, nth), dtype=np.complex128)
     e2 = np.zeros((nzp, nth), dtype=np.complex128)
+    e3 = np.ones((nzp, nth))
+    nonconst = getattr(blk, "rel_thick", None) is not None
+    kD3 = np.fft.fft(diff_central(diff_backward(d1)))
     for l in range(nth):
         w = blk.wavelet[l].astype(np.float64)
         W = wavelet_spectrum_full(w)
+        es3 = diff_central(diff_backward(diff_forward(w)))
+        if nonconst:
+            # non-constant thickness (src/avoinversion.cpp:976-1014): K = kD A, errMult1 =
+            # 1/|w|, errMult2 = kD3/|errorSmooth3|, errMult3 = fillInverseAbskWRobust
+            K[:, l, :] = kD[:, None] * blk.A[l][None, :]
+            e1[:, l] = 1.0 / float(blk.wavelet_norm[l])
+            e2[:, l] = kD3 / real_norm(es3)
+            e3[:, l] = inverse_abs_kw_robust(W, float(blk.wavelet_norm[l]))
+            continue
         kW = np.conj(W) * kD
         K[:, l, :] = kW[:, None] * blk.A[l][None, :]
         e1[:, l] = np.conj(W) / float(blk.wavelet_norm[l])
-        es3 = diff_central(diff_backward(diff_forward(w)))
         e2[:, l] = np.conj(np.fft.fft(es3)) / real_norm(es3)
-    e3 = np.ones((nzp, nth))
     inv = invert_mask(blk)
     return K, e1, e2, e3, inv
+
+
+def camp_scaled32(c: np.ndarray, k, scale):
+    """Wavelet::getCAmp(k, scale) (src/wavelet.cpp:337-382) for 0 <= k < cnzp: linear
+    interpolation of the half spectrum c (complex64, cnzp entries) at k / scale, divided
+    by scale, in float32 with the reference's operation order.  k and scale broadcast."""
+    cn = c.shape[0]
+    f32 = np.float32
+    k = np.asarray(k)
+    scale = np.asarray(scale, dtype=f32)
+    om = k.astype(f32) / scale
+    valid = om < f32(cn)
+    lo = np.where(valid, np.floor(om), 0).astype(np.int64)
+    hi = lo + 1
+    hi = np.where(hi >= cn, hi - 1, hi)
+    d = (om - lo.astype(f32)).astype(f32)
+    e = (f32(1.0) - d).astype(f32)
+    cr, ci = c.real.astype(f32), c.imag.astype(f32)
+    re = (cr[lo] * e + cr[hi] * d) / scale
+    im = (ci[lo] * e + ci[hi] * d) / scale
+    re = np.where(valid, re, f32(0))
+    im = np.where(valid, im, f32(0))
+    return re.astype(f32), im.astype(f32)
+
+
+def inverse_abs_kw_robust(W: np.ndarray, wnorm: float) -> np.ndarray:
+    """AVOInversion::fillInverseAbskWRobust (src/avoinversion.cpp:1296-1322): per kz,
+    1/sqrt(max(|W(k)|^2, |W(k; 0.999)|^2)) in float32 (W the full spectrum; a large
+    number where both vanish)."""
+    n = W.shape[0]
+    cn = n // 2 + 1
+    f32 = np.float32
+    c = W[:cn].astype(np.complex64)
+    k = np.arange(n)
+    refk = np.where(k < cn, k, n - k)
+    v = W.astype(np.complex64)
+    m = (v.real * v.real + v.imag * v.imag).astype(f32)
+    fr, fi = camp_scaled32(c, refk, f32(0.999))
+    mf = (fr * fr + fi * fi).astype(f32)
+    mx = np.maximum(m, mf)
+    big = f32(wnorm) * f32(n) * f32(n) * f32(100.0)
+    with np.errstate(divide="ignore"):
+        r = np.where(mx > 0, (1.0 / np.sqrt(mx)).astype(f32), big)
+    return r.astype(np.float64)
+
+
+# ---------------------------------------------------------------- non-constant thickness
+
+def dist_to_boundary(i: int, n: int, np_: int) -> float:
+    """FFTGrid::getDistToBoundary (src/fftgrid.cpp:1158-1197), float32."""
+    if i < n:
+        return 0.0
+    taper = np.float32(min(n, np_ - n) / 2.1)
+    below, above = np_ - i, i - (n - 1)
+    return float(np.float32(above) / taper if above < below else np.float32(below) / taper)
+
+
+def fill_number(i: int, n: int, np_: int) -> int:
+    """FFTGrid::getFillNumber (src/fftgrid.cpp:1103-1141)."""
+    if i < n:
+        return i
+    below, above = np_ - i - 1, i - n + 1
+    return max(n - above, n // 2) if above < below else min(below, n // 2)
+
+
+def thick_tables(blk):
+    """Per-angle tables of AVOInversion::computeAdjustmentFactor (src/avoinversion.cpp:630-719)
+    over kz < cnzp, float32 where the reference computes in float: the wavelet half
+    spectrum, the band-normalised spectrum of errorSmooth3 (with the RMISSING that
+    multiplyRAmpByConstant writes into the floats at index >= nzp, src/wavelet.cpp:507-515),
+    |Re| of the reflection-coefficient covariance spectrum (:369-401) and the scalars."""
+    f32 = np.float32
+    n, nth = blk.nzp, blk.ntheta
+    cn = n // 2 + 1
+    dz = f32(blk.lz / blk.nz)
+    dOmega = f32(1.0 / float(f32(n * dz) * 0.001))
+    loI = max(0, int(np.floor(f32(blk.low_cut) / dOmega)))
+    hiI = min(cn, int(np.ceil(f32(blk.high_cut) / dOmega)))
+    maxfreq = f32((n // 2) * 1000.0 * blk.nz) / f32(blk.lz * n)
+    circ = blk.circ_corr_t.astype(f32)
+    corrT = np.zeros(n, dtype=f32)
+    for i in range(n):
+        refk = i if i < n // 2 + 1 else n - i
+        corrT[i] = circ[refk] / circ[0] if refk < blk.nz else f32(0)
+    out = {"wamp": [], "es3": [], "tau2": [], "wn2": [], "modW": [], "err_var": []}
+    for l in range(nth):
+        wf = blk.wavelet[l].astype(f32)
+        W = np.fft.fft(wf.astype(np.float64))
+        f1 = (np.roll(wf, -1) - wf).astype(f32)
+        f2 = (f1 - np.roll(f1, 1)).astype(f32)
+        f3 = (0.5 * (np.roll(f2, -1) - np.roll(f2, 1)).astype(np.float64)).astype(f32)
+        E3 = np.fft.fft(f3.astype(np.float64))[:cn].astype(np.complex64)
+        fac = 1.0 / n
+        sq = (E3.real * E3.real + E3.imag * E3.imag).astype(f32)
+        norm2 = 0.0
+        for i in range(loI, hiI):
+            norm2 += 2.0 * fac * float(sq[i])
+        if loI == 0:
+            norm2 -= fac * float(sq[0])
+        c3 = f32(1.0) / f32(np.sqrt(norm2))
+        es3 = (E3.real * c3).astype(f32) + 1j * (E3.imag * c3).astype(f32)
+        es3 = es3.astype(np.complex64)
+        es3.imag[cn - 1] = -99999.0
+        if n % 2 == 0:
+            es3.real[cn - 1] = -99999.0
+        Al = blk.A[l].astype(f32)
+        pv = blk.prior_var0
+        eiVar = 0.0
+        for a in range(3):
+            for b in range(3):
+                eiVar += float(Al[a] * f32(pv[a, b]) * Al[b])
+        rc = (eiVar * corrT.astype(np.float64)).astype(f32)
+        first, prev = rc[0], rc[n - 1]
+        for i in range(n - 1):
+            curr, nxt = rc[i], rc[i + 1]
+            rc[i] = f32(2) * curr - nxt - prev
+            prev = curr
+        rc[n - 1] = f32(2) * rc[n - 1] - first - prev
+        RC = np.fft.fft(rc.astype(np.float64))[:cn]
+        norm = f32(blk.wavelet_norm[l])
+        modW = norm * norm
+        modW = f32(modW * (maxfreq / f32(blk.high_cut)))
+        out["wamp"].append(W[:cn].astype(np.complex64))
+        out["es3"].append(es3)
+        out["tau2"].append(np.abs(RC.real.astype(f32)))
+        out["wn2"].append(f32(norm * norm))
+        out["modW"].append(modW)
+        out["err_var"].append(f32(blk.err_theta_cov[l, l]))
+    return out
+
+
+def adjustment_factor(tab, l: int, sf, k) -> np.ndarray:
+    """computeAdjustmentFactor (src/avoinversion.cpp:674-712) of angle l at kz k (< cnzp)
+    for traces stretched by sf (float32), local wavelet = global wavelet; float32 with the
+    reference's operation order.  sf and k broadcast; returns complex128."""
+    f32 = np.float32
+    wa, es = tab["wamp"][l], tab["es3"][l]
+    wn2, modW, ev = tab["wn2"][l], tab["modW"][l], tab["err_var"][l]
+    wnc = f32(tab["wnc"])
+    k = np.asarray(k)
+    lr, li = camp_scaled32(wa, k, sf)
+    wLoc2 = (lr * lr + li * li).astype(f32)
+    gr, gi = wa.real.astype(f32)[k], wa.imag.astype(f32)[k]
+    wGlob2 = (gr * gr + gi * gi).astype(f32)
+    er, ei = camp_scaled32(es, k, sf)
+    sL = (wLoc2 / wn2 + (er * er + ei * ei)).astype(f32)
+    sgr, sgi = es.real.astype(f32)[k], es.imag.astype(f32)[k]
+    sG = (wGlob2 / wn2 + (sgr * sgr + sgi * sgi)).astype(f32)
+    c = (f32(1.0) - wnc) * f32(0.5)
+    s2L = (ev * (wnc + c * sL)).astype(f32)
+    s2G = (ev * (wnc + c * sG)).astype(f32)
+    tau2 = tab["tau2"][l][k]
+    tm = f32(0.05) * modW
+    wG2A = np.where(wGlob2 < tm, f32(0.5) * (wGlob2 + tm), wGlob2).astype(f32)
+    wL2A = np.where(wLoc2 < tm, f32(0.5) * (wLoc2 + tm), wLoc2).astype(f32)
+    tg = (f32(0.05) * wG2A).astype(f32)
+    adj = wL2A < tg
+    wL2A = np.where(adj, f32(0.5) * (wLoc2 + tg), wL2A).astype(f32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        s2L = np.where(adj, s2L * (wL2A / wLoc2), s2L).astype(f32)
+        dL = (tau2 * wL2A + s2L).astype(f32)
+        q = (wG2A / (tau2 * wGlob2 + s2G)).astype(f32)
+        fr = ((lr / dL) / q).astype(f32)
+        fi = ((li / dL) / q).astype(f32)
+    return fr.astype(np.float64) + 1j * fi.astype(np.float64)
+
+
+def divide_data_by_scale_wavelet(blk) -> np.ndarray:
+    """AVOInversion::divideDataByScaleWavelet (src/avoinversion.cpp:484-612) on every data
+    grid: per trace (i < nxp, j < nyp) the 1/sqrt(nzp) scale and z taper, r2c along z,
+    the adjustment factor inside the band deltaF*k in (lowCut, highCut) with
+    deltaF = nz*1000/(relThick*lz*nzp) and zero outside, c2r, 1/sqrt(nzp).  The transforms
+    in float64.  Returns (ntheta, nzp, nyp, rnxp) float64 (padding columns zero)."""
+    f32 = np.float32
+    nxp, nyp, nzp, nz = blk.nxp, blk.nyp, blk.nzp, blk.nz
+    cn = nzp // 2 + 1
+    tab = thick_tables(blk)
+    tab["wnc"] = blk.wnc
+    rsq = f32(np.sqrt(f32(nzp)))
+    taper = np.ones(nzp, dtype=f32)
+    for k in range(nzp):
+        if k > nz:
+            dk = f32(dist_to_boundary(k, nz, nzp))
+            taper[k] = max(f32(1) - dk * dk, f32(0))
+    rt = np.asarray(blk.rel_thick, dtype=np.float64)            # (nyp, nxp)
+    sf = rt.astype(f32)
+    deltaF = float(nz) * 1000.0 / (rt * float(blk.lz) * float(nzp))
+    k = np.arange(cn)
+    fk = deltaF[None] * k[:, None, None]                         # (cn, nyp, nxp)
+    band = (fk < float(f32(blk.high_cut))) & (fk > float(f32(blk.low_cut)))
+    out = np.zeros((blk.ntheta, nzp, nyp, 2 * (nxp // 2 + 1)))
+    for l in range(blk.ntheta):
+        v = (blk.data[l][..., :nxp].astype(f32) / rsq).astype(f32) * taper[:, None, None]
+        spec = np.fft.rfft(v.astype(np.float64), axis=0)
+        fac = adjustment_factor(tab, l, sf[None], k[:, None, None])
+        spec = np.where(band, spec * fac, 0.0)
+        res = np.fft.irfft(spec, n=nzp, axis=0) * nzp / float(rsq)
+        out[l, ..., :nxp] = res
+    return out
+
+
+def plan_trace_interpolation(energy: np.ndarray, nx: int, ny: int, threshold: float):
+    """The control flow of FFTGrid::interpolateSeismic / interpolateTrace
+    (src/fftgrid.cpp:2349-2480) on one angle's energy map (ny, nx) float32: returns the
+    interpolations in the reference's order as (target, [neighbour indices]) with index
+    i + nx*j, and the box (imin, imax, jmin, jmax) of good traces."""
+    e = np.asarray(energy, dtype=np.float32).reshape(-1)
+    n = nx * ny
+    total = np.float32(0)
+    for q in range(n):
+        total = np.float32(total + e[q])
+    limit = np.float32(np.float32(threshold) * total / np.float32(n))
+    flags = [0] * n
+    imin, imax, jmin, jmax, flag = nx, 0, ny, 0, 0
+    for q in range(n):
+        i, j = q % nx, q // nx
+        cur = 1 if e[q] <= limit else 0
+        flags[q] = flag + cur
+        if cur:
+            flag = 2
+        else:
+            imin, imax, jmin, jmax = min(imin, i), max(imax, i), min(jmin, j), max(jmax, j)
+    ops = []
+
+    def interp(index, i, j):
+        nb = []
+        if i > 0 and flags[index - 1] % 2 == 0:
+            nb.append(index - 1)
+        if i < nx - 1 and flags[index + 1] % 2 == 0:
+            nb.append(index + 1)
+        if j > 0 and flags[index - nx] % 2 == 0:
+            nb.append(index - nx)
+        if j < ny - 1 and flags[index + nx] % 2 == 0:
+            nb.append(index + nx)
+        if len(nb) > 1:
+            ops.append((index, nb))
+            flags[index] -= 1
+        return flags[index]
+
+    for cur in range(n):
+        i, j = cur % nx, cur // nx
+        if flags[cur] % 2 == 1 and interp(cur, i, j) % 2 == 0:
+            index = cur - 1
+            while index >= 0 and flags[index] > 1:
+                if flags[index] % 2 == 1:
+                    interp(index, index % nx, index // nx)
+                index -= 1
+            index = max(index, 0) + 1
+            while index <= cur and flags[index - 1] == 0:
+                if flags[index] > 1:
+                    flags[index] -= 2
+                index += 1
+    return ops, (imin, imax, jmin, jmax)
+
+
+def interpolate_seismic(grid: np.ndarray, blk, threshold: float) -> np.ndarray:
+    """FFTGrid::interpolateSeismic (src/fftgrid.cpp:2349-2437) on one real grid (nzp, nyp,
+    rnxp): energies over k < nz in float32 order, the interpolation plan, then
+    extrapolateSeismic (:2484-2516) outside the box of good traces.  Returns a new grid."""
+    nx, ny, nz, nxp, nyp, nzp = blk.nx, blk.ny, blk.nz, blk.nxp, blk.nyp, blk.nzp
+    g = np.array(grid, dtype=np.float64)
+    v32 = g[:nz, :ny, :nx].astype(np.float32)
+    energy = np.zeros((ny, nx), dtype=np.float32)
+    for k in range(nz):
+        energy = (energy + v32[k] * v32[k]).astype(np.float32)
+    ops, (imin, imax, jmin, jmax) = plan_trace_interpolation(energy, nx, ny, threshold)
+    for t, nb in ops:
+        s = sum(g[:, q // nx, q % nx] for q in nb)
+        g[:, t // nx, t % nx] = s / len(nb)
+    if imin > imax or jmin > jmax:
+        return g
+    dx = np.array([dist_to_boundary(i, nx, nxp) for i in range(nxp)], dtype=np.float32)
+    dy = np.array([dist_to_boundary(j, ny, nyp) for j in range(nyp)], dtype=np.float32)
+    dzv = np.array([dist_to_boundary(k, nz, nzp) for k in range(nzp)], dtype=np.float32)
+    ri = np.clip([fill_number(i, nx, nxp) for i in range(nxp)], imin, imax)
+    rj = np.clip([fill_number(j, ny, nyp) for j in range(nyp)], jmin, jmax)
+    I = np.arange(nxp)[None, :]
+    J = np.arange(nyp)[:, None]
+    outside = (I < imin) | (I > imax) | (J < jmin) | (J > jmax)        # (nyp, nxp)
+    src = g[:, rj[:, None], ri[None, :]]                               # (nzp, nyp, nxp)
+    t = 1.0 - (dx * dx)[None, None, :].astype(np.float64) - (dy * dy)[None, :, None].astype(np.float64) \
+        - (dzv * dzv)[:, None, None].astype(np.float64)
+    mult = np.maximum(t, 0.0) ** 3
+    g[..., :nxp] = np.where(outside[None], mult * src, g[..., :nxp])
+    return g
 
 
 def real_frequency(blk) -> np.ndarray:
