@@ -35,9 +35,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
+    shared = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "crava_gpu.h")]
+
     def compile_one(s):
         src = os.path.join(CSRC, s)
         obj = os.path.join(objdir, s.replace(".cu", ".o"))
+        # an object is reused when it is newer than its source and every shared header
+        if not force and not ptxas_info and not _newer(obj, [src] + shared):
+            return s, obj, None
         cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
@@ -47,9 +52,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     # the translation units are independent: compile them side by side
     with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
         for s, obj, r in ex.map(compile_one, SOURCES):
-            if r.returncode != 0:
+            if r is not None and r.returncode != 0:
                 raise RuntimeError(f"nvcc failed for {s}:\n{r.stdout}\n{r.stderr}")
-            if ptxas_info:
+            if r is not None and ptxas_info:
                 sys.stderr.write(r.stderr)
             objs.append(obj)
     tmp = LIB + ".tmp"

@@ -265,7 +265,7 @@ crava_status validate(const crava_job_desc* d) {
 size_t thick_bytes(const crava_job_desc* d) {
   if (!(d->flags & CRAVA_FLAG_NONCONST_THICK)) return 0;
   const size_t nth = d->ntheta, cnzp = d->nzp / 2 + 1, nxy = (size_t)d->nx * d->ny;
-  return 2 * align256(sizeof(float2) * nth * cnzp) + align256(sizeof(float) * nth * cnzp) +
+  return 3 * align256(sizeof(float2) * nth * cnzp) + align256(sizeof(float) * nth * cnzp) +
          2 * align256(sizeof(float) * d->nzp) + align256(sizeof(int) * d->nxp) + align256(sizeof(int) * d->nyp) +
          align256(sizeof(float) * d->nxp) + align256(sizeof(float) * d->nyp) +
          align256(sizeof(double) * d->nxp * d->nyp) + align256(sizeof(float) * nth * nxy) +
@@ -443,7 +443,7 @@ void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vect
 // src/avoinversion.cpp:630-719, and the taper/fill helpers of FFTGrid), in the float
 // arithmetic of the reference wherever it computes in float.
 struct ThickTables {
-  std::vector<float2> wamp, es3;
+  std::vector<float2> wamp, es3, glob;
   std::vector<float> tau2, ztaper, distx, disty, distz;
   std::vector<int> fillx, filly;
   float wn2[kMaxTheta], modW[kMaxTheta], err_var[kMaxTheta];
@@ -453,6 +453,7 @@ void build_thick_tables(const crava_job_desc& d, ThickTables& t) {
   const int n = d.nzp, cn = n / 2 + 1, nth = d.ntheta;
   t.wamp.assign((size_t)nth * cn, make_float2(0, 0));
   t.es3 = t.wamp;
+  t.glob = t.wamp;
   t.tau2.assign((size_t)nth * cn, 0.f);
   // Wavelet::findNormWithinFrequencyBand (src/wavelet.cpp:903-925) with the wavelet's dz
   const float dz = (float)(d.lz / d.nz);
@@ -524,6 +525,20 @@ void build_thick_tables(const crava_job_desc& d, ThickTables& t) {
     modW *= maxfreq / static_cast<float>(d.high_cut);
     t.modW[l] = modW;
     t.err_var[l] = static_cast<float>(j_etc(d, l));
+    // the trace-independent part of computeAdjustmentFactor (src/avoinversion.cpp:679-712),
+    // float operations in the reference's order
+    const float wn2 = t.wn2[l], wnc = d.wnc, ev = t.err_var[l];
+    const float c = (1.0f - wnc) * 0.5f;
+    const float tm = 0.05f * modW;
+    for (int k = 0; k < cn; k++) {
+      const float2 wg = t.wamp[(size_t)l * cn + k], es = t.es3[(size_t)l * cn + k];
+      const float wGlob2 = wg.x * wg.x + wg.y * wg.y;
+      const float sG = wGlob2 / wn2 + (es.x * es.x + es.y * es.y);
+      const float s2G = ev * (wnc + c * sG);
+      const float wG2A = wGlob2 < tm ? 0.5f * (wGlob2 + tm) : wGlob2;
+      const float tau2 = t.tau2[(size_t)l * cn + k];
+      t.glob[(size_t)l * cn + k] = make_float2(0.05f * wG2A, wG2A / (tau2 * wGlob2 + s2G));
+    }
   }
   t.ztaper.assign(n, 1.f);
   t.distz.assign(n, 0.f);
@@ -859,6 +874,7 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     tp.wamp = (const float2*)take(sizeof(float2) * nth * cn);
     tp.es3 = (const float2*)take(sizeof(float2) * nth * cn);
     tp.tau2 = (const float*)take(sizeof(float) * nth * cn);
+    tp.glob = (const float2*)take(sizeof(float2) * nth * cn);
     tp.ztaper = (const float*)take(sizeof(float) * d.nzp);
     tp.distz = (const float*)take(sizeof(float) * d.nzp);
     tp.fillx = (const int*)take(sizeof(int) * d.nxp);
@@ -874,6 +890,11 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     tp.rnxp = j->rnxp;
     tp.cnzp = (int)cn;
     tp.W = thick_tile_width(d.nzp);
+    if (const char* ev = getenv("CRAVA_THICK_W")) {
+      int w = 1;
+      while (w * 2 <= std::min(16, atoi(ev))) w *= 2;
+      if (thick_smem_bytes(w, d.nzp) <= 227 * 1024) tp.W = w;
+    }
     tp.logW = 0;
     while ((1 << tp.logW) < tp.W) tp.logW++;
     tp.nIT = ((d.nxp + 1) / 2 + tp.W - 1) / tp.W;
@@ -916,6 +937,7 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     JOB_TRY(up(tp.wamp, tt.wamp.data(), sizeof(float2) * tt.wamp.size()));
     JOB_TRY(up(tp.es3, tt.es3.data(), sizeof(float2) * tt.es3.size()));
     JOB_TRY(up(tp.tau2, tt.tau2.data(), sizeof(float) * tt.tau2.size()));
+    JOB_TRY(up(tp.glob, tt.glob.data(), sizeof(float2) * tt.glob.size()));
     JOB_TRY(up(tp.ztaper, tt.ztaper.data(), sizeof(float) * tt.ztaper.size()));
     JOB_TRY(up(tp.distz, tt.distz.data(), sizeof(float) * tt.distz.size()));
     JOB_TRY(up(tp.fillx, tt.fillx.data(), sizeof(int) * tt.fillx.size()));

@@ -96,6 +96,7 @@ struct ThickParams {
   const float2* wamp;          // nth x cnzp
   const float2* es3;           // nth x cnzp
   const float* tau2;           // nth x cnzp
+  const float2* glob;          // nth x cnzp: {0.05 wGlob2Adj, wGlob2Adj / (tau2 wGlob2 + sigma2Glob)}
   const float* ztaper;         // nzp: 1, or max(1 - dist^2, 0) for kz > nz
   const int* fillx;            // nxp, nyp: getFillNumber of every padded index
   const int* filly;

@@ -49,6 +49,9 @@ __device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, 
 // computeAdjustmentFactor (src/avoinversion.cpp:630-719) at one kz < cnzp for a trace
 // whose wavelet is stretched by sf; local wavelet = global wavelet (1D wavelet without
 // local shift or gain grids), so eSkGlob uses the unstretched spectrum of the same tables.
+// The quantities of the global wavelet (wGlob2Adj, tolFac*wGlob2Adj and the quotient
+// wGlob2Adj / (tau2 wGlob2 + sigma2Glob)) do not depend on the trace: the host evaluates
+// them per (angle, kz) with the same float operations (glob[] = {tg, q}).
 __device__ __forceinline__ float2 adjustment(const ThickParams& P, int l, int k, float sf) {
   const int cn = P.cnzp;
   const float2* wa = P.wamp + (size_t)l * cn;
@@ -56,26 +59,20 @@ __device__ __forceinline__ float2 adjustment(const ThickParams& P, int l, int k,
   const float wn2 = P.wn2[l], wnc = P.wnc, ev = P.err_var[l];
   const float2 wLoc = camp_scaled(wa, cn, k, sf);
   const float wLoc2 = sq2(wLoc);
-  const float2 wGlob = __ldg(wa + k);
-  const float wGlob2 = sq2(wGlob);
   const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(camp_scaled(es, cn, k, sf)));
-  const float sG = __fadd_rn(__fdiv_rn(wGlob2, wn2), sq2(__ldg(es + k)));
   const float c = __fmul_rn(__fsub_rn(1.f, wnc), 0.5f);
   float s2L = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sL)));
-  const float s2G = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sG)));
   const float tau2 = __ldg(P.tau2 + (size_t)l * cn + k);
+  const float2 glob = __ldg(P.glob + (size_t)l * cn + k);
   const float tm = __fmul_rn(0.05f, P.modW[l]);
-  float wG2A = wGlob2, wL2A = wLoc2;
-  if (wGlob2 < tm) wG2A = __fmul_rn(0.5f, __fadd_rn(wGlob2, tm));
+  float wL2A = wLoc2;
   if (wLoc2 < tm) wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, tm));
-  const float tg = __fmul_rn(0.05f, wG2A);
-  if (wL2A < tg) {
-    wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, tg));
+  if (wL2A < glob.x) {
+    wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, glob.x));
     s2L = __fmul_rn(s2L, __fdiv_rn(wL2A, wLoc2));
   }
   const float dL = __fadd_rn(__fmul_rn(tau2, wL2A), s2L);
-  const float q = __fdiv_rn(wG2A, __fadd_rn(__fmul_rn(tau2, wGlob2), s2G));
-  return make_float2(__fdiv_rn(__fdiv_rn(wLoc.x, dL), q), __fdiv_rn(__fdiv_rn(wLoc.y, dL), q));
+  return make_float2(__fdiv_rn(__fdiv_rn(wLoc.x, dL), glob.y), __fdiv_rn(__fdiv_rn(wLoc.y, dL), glob.y));
 }
 
 // One CTA: W complex lines (2W traces x = 2(m0 + w) + {0, 1}) of row j of angle blockIdx.z.
@@ -110,20 +107,32 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   // A trace whose tapered samples are all zero (a dead trace) is stored back as exact
   // zeros, as the reference's own real transform returns it, although the trace sharing
   // its complex line leaks rounding into it.
+  // every copy is issued before the first is waited for (cp.async); a line whose second
+  // trace lies at nxp (odd nxp) is read by a plain load of its first float
+  {
+    const uint32_t rb = smem_addr(R);
+    for (int e = tid; e < W * nzp; e += T) {
+      const int w = e & (W - 1), k = e >> lw;
+      const int m = m0 + w;
+      const float* p = row + (size_t)k * kstride + 2 * m;
+      if (2 * m + 1 < P.nxp) {
+        cp_async8(rb + 8u * (uint32_t)e, p);
+      } else {
+        R[e] = make_float2(2 * m < P.nxp ? *p : 0.f, 0.f);
+      }
+    }
+    cp_async_commit();
+    cp_async_wait_0();
+  }
+  __syncthreads();
   for (int e = tid; e < W * nzp; e += T) {
     const int w = e & (W - 1), k = e >> lw;
-    const int m = m0 + w;
-    float2 v = make_float2(0.f, 0.f);
-    if (2 * m < P.nxp) {
-      const float* p = row + (size_t)k * kstride + 2 * m;
-      if (2 * m + 1 < P.nxp) v = *reinterpret_cast<const float2*>(p);
-      else v.x = *p;
-      const float tz = __ldg(P.ztaper + k);
-      v.x = __fmul_rn(__fdiv_rn(v.x, P.rsq), tz);
-      v.y = __fmul_rn(__fdiv_rn(v.y, P.rsq), tz);
-      if (v.x != 0.f) s_live[2 * w] = 1;
-      if (v.y != 0.f) s_live[2 * w + 1] = 1;
-    }
+    float2 v = R[e];
+    const float tz = __ldg(P.ztaper + k);
+    v.x = __fmul_rn(__fdiv_rn(v.x, P.rsq), tz);
+    v.y = __fmul_rn(__fdiv_rn(v.y, P.rsq), tz);
+    if (v.x != 0.f) s_live[2 * w] = 1;
+    if (v.y != 0.f) s_live[2 * w + 1] = 1;
     R[e] = v;
   }
   __syncthreads();
@@ -208,10 +217,20 @@ __global__ void k_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, con
 // of good traces takes the value of its mirror trace (getFillNumber, clamped into the box)
 // times (max(1 - dx^2 - dy^2 - dz^2, 0))^3 of the distances to the boundary.  The mirror
 // traces lie inside the box, which this kernel never writes.
-__global__ void k_extrapolate(const __grid_constant__ ThickParams P, int l, int imin, int imax, int jmin, int jmax) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= P.nxp) return;
-  if (!(i < imin || i > imax || j < jmin || j > jmax)) return;
+// The launch covers only traces outside the box: rows0 = 1 takes the rows j < jmin and
+// j > jmax (all i); rows0 = 0 the columns i < imin and i > imax of the rows inside.
+__global__ void k_extrapolate(const __grid_constant__ ThickParams P, int l, int imin, int imax, int jmin, int jmax,
+                              int rows0) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, k = blockIdx.z;
+  int i, j;
+  if (rows0) {
+    i = x;
+    j = y < jmin ? y : jmax + 1 + (y - jmin);
+  } else {
+    i = x < imin ? x : imax + 1 + (x - imin);
+    j = jmin + y;
+  }
+  if (i >= P.nxp || j >= P.nyp) return;
   int ri = __ldg(P.fillx + i), rj = __ldg(P.filly + j);
   ri = ri < imin ? imin : (ri > imax ? imax : ri);
   rj = rj < jmin ? jmin : (rj > jmax ? jmax : rj);
@@ -264,9 +283,20 @@ cudaError_t launch_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, co
 }
 
 cudaError_t launch_extrapolate(const ThickParams& P, int l, const int box[4], cudaStream_t st, int* nlaunch) {
-  dim3 grid((unsigned)((P.nxp + 127) / 128), (unsigned)P.nyp, (unsigned)P.nzp);
-  k_extrapolate<<<grid, 128, 0, st>>>(P, l, box[0], box[1], box[2], box[3]);
-  if (nlaunch) (*nlaunch)++;
+  const int imin = box[0], imax = box[1], jmin = box[2], jmax = box[3];
+  const int nrows = jmin + (P.nyp - 1 - jmax);         // rows outside the box
+  const int ncols = imin + (P.nxp - 1 - imax);         // columns outside, rows inside
+  if (nrows > 0) {
+    dim3 grid((unsigned)((P.nxp + 127) / 128), (unsigned)nrows, (unsigned)P.nzp);
+    k_extrapolate<<<grid, 128, 0, st>>>(P, l, imin, imax, jmin, jmax, 1);
+    if (nlaunch) (*nlaunch)++;
+  }
+  if (ncols > 0) {
+    const int T = std::min(128, (ncols + 31) / 32 * 32);
+    dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)(jmax - jmin + 1), (unsigned)P.nzp);
+    k_extrapolate<<<grid, T, 0, st>>>(P, l, imin, imax, jmin, jmax, 0);
+    if (nlaunch) (*nlaunch)++;
+  }
   return cudaGetLastError();
 }
 

@@ -403,6 +403,25 @@ def make_block_fast(spec: BlockSpec) -> Block:
                  wnc=spec.wnc, nsim=spec.nsim, seed=spec.seed)
 
 
+def rel_thick_surface(nxp: int, nyp: int, lo: float = 0.75, hi: float = 1.3, seed: int = 3) -> np.ndarray:
+    """A smooth Simbox::getRelThick surface over the padded lateral grid, (nyp, nxp) float64
+    in [lo, hi]: a non-constant-thickness block (top and base not parallel)."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(nxp)[None, :] / nxp
+    y = np.arange(nyp)[:, None] / nyp
+    a, b = rng.uniform(0, 2 * np.pi, 2)
+    s = 0.5 + 0.25 * np.sin(2 * np.pi * x + a) + 0.25 * np.cos(2 * np.pi * 1.5 * y + b)
+    return (lo + (hi - lo) * s).astype(np.float64)
+
+
+def with_rel_thick(blk: Block, seed: int = 3, threshold: float = 0.0) -> Block:
+    """The block with a non-constant thickness surface (rel_thick, min_rel_thick over the
+    simbox) and the interpolateSeismic energy threshold."""
+    rt = rel_thick_surface(blk.nxp, blk.nyp, seed=seed)
+    return dataclasses.replace(blk, rel_thick=rt, min_rel_thick=float(rt[:blk.ny, :blk.nx].min()),
+                               energy_threshold=threshold)
+
+
 # --- the configurations of the benchmark suite -------------------------------------
 
 def config0(seed: int = 11) -> BlockSpec:

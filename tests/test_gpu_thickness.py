@@ -30,22 +30,10 @@ def rel(x, ref):
     return float(np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300))
 
 
-def rel_thick_surface(nxp, nyp, lo=0.75, hi=1.3, seed=3):
-    """A smooth relative-thickness surface over the padded lateral grid (index i + nxp*j)."""
-    rng = np.random.default_rng(seed)
-    x = np.arange(nxp)[None, :] / nxp
-    y = np.arange(nyp)[:, None] / nyp
-    a, b = rng.uniform(0, 2 * np.pi, 2)
-    s = 0.5 + 0.25 * np.sin(2 * np.pi * x + a) + 0.25 * np.cos(2 * np.pi * 1.5 * y + b)
-    return (lo + (hi - lo) * s).astype(np.float64)
-
-
 def thick_block(nx=40, ny=30, nz=50, nxp=48, nyp=40, nzp=64, nsim=1, seed=5, threshold=0.0, theta=(8.0, 20.0, 32.0)):
     spec = synth.BlockSpec(nx=nx, ny=ny, nz=nz, nxp=nxp, nyp=nyp, nzp=nzp, nsim=nsim, seed=seed, theta_deg=theta,
                            peak_hz=(30.0,) * len(theta), sn=(6.0,) * len(theta))
-    blk = synth.make_block(spec)
-    rt = rel_thick_surface(blk.nxp, blk.nyp, seed=seed)
-    return dataclasses.replace(blk, rel_thick=rt, min_rel_thick=float(rt[:ny, :nx].min()), energy_threshold=threshold)
+    return synth.with_rel_thick(synth.make_block(spec), seed=seed, threshold=threshold)
 
 
 def oracle_divided(blk):
