@@ -150,6 +150,14 @@ int main(int argc, char** argv) {
         noise.push_back(own.back().get());
       }
     }
+    // optional trailing section: non-constant thickness (relThick nxp*nyp doubles, then the
+    // energy threshold)
+    int nonconst = 0;
+    if (fread(&nonconst, sizeof(int), 1, fi) == 1 && nonconst) {
+      set.relThick.resize((size_t)nxp * nyp);
+      rd.read(set.relThick.data(), set.relThick.size());
+      set.energyThreshold = rd.one<float>();
+    }
     fclose(fi);
 
     // FFTGrid round trip on a copy of the first DATA grid

@@ -62,6 +62,10 @@ def write_block(path, blk, grids, noise):
             np.asarray(blk.mean[a], dtype=np.float32).tofile(f)
         if noise is not None:
             np.ascontiguousarray(noise, dtype=np.complex64).tofile(f)
+        if getattr(blk, "rel_thick", None) is not None:
+            np.array([1], dtype=np.int32).tofile(f)
+            np.ascontiguousarray(blk.rel_thick, dtype=np.float64).tofile(f)
+            np.array([blk.energy_threshold], dtype=np.float32).tofile(f)
 
 
 def read_out(path, blk):
@@ -107,3 +111,29 @@ def test_host_layer_matches_oracle(tmp_path, grids):
     assert np.allclose(out["post_var0"].reshape(3, 3), ref64.post_var0(post), rtol=1e-3)
     scale = float(np.abs(blk.data[0]).max())
     assert out["fft_roundtrip"] < 1e-5 * scale
+
+
+@pytest.mark.parametrize("grids", [False, True])
+def test_host_layer_nonconst_thickness(tmp_path, grids):
+    """AVOInversionSettings::relThick: the layer divides the data by the scale wavelet
+    (crava_job_divide_data) before the inversion, and in GRIDS mode reads the temporal
+    correlation from the covVp grid's (0, 0) column."""
+    import dataclasses
+    assert os.path.exists(DEMO)
+    blk = synth.make_block(synth.BlockSpec(nx=30, ny=28, nz=40, nxp=36, nyp=32, nzp=48, theta_deg=(8.0, 20.0, 32.0),
+                                           peak_hz=(30.0,) * 3, sn=(5.0,) * 3, nsim=0, seed=19))
+    blk = synth.with_rel_thick(blk, seed=7)
+    fin, fout = tmp_path / "block.bin", tmp_path / "out.bin"
+    write_block(fin, blk, grids, None)
+    r = subprocess.run([DEMO, str(fin), str(fout)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = read_out(fout, blk)
+    div = ref64.divide_data_by_scale_wavelet(blk)
+    divided = np.stack([ref64.interpolate_seismic(div[l], blk, blk.energy_threshold) for l in range(blk.ntheta)])
+    post = ref64.posterior(dataclasses.replace(blk, data=divided))
+    nx = blk.nxp
+    assert out["counters"][0] == post.n_inverted
+    for a in range(3):
+        assert crel(out["mean"][a][..., :nx], post.mean[a][..., :nx]) < 1e-4, ("mean", a)
+    for q in range(6):
+        assert crel(out["cov"][q][..., :nx], post.cov[q][..., :nx]) < 1e-3, ("cov", q)
