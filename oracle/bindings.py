@@ -67,7 +67,43 @@ def ref32_lib():
         _ref32.ref32_ifft.argtypes = [_fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _ref32.ref32_sim_noise.argtypes = [ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, _fp]
+        _ref32.ref32_divide_traces.argtypes = [_fp, ctypes.c_int, ctypes.c_int, _fp, _fp,
+                                               ctypes.POINTER(ctypes.c_ubyte)]
     return _ref32
+
+
+def ref32_divide(blk) -> np.ndarray:
+    """AVOInversion::divideDataByScaleWavelet on every data grid with the reference's FFTW
+    2.1.2 float transforms (ref32_divide_traces), the adjustment factor and band from the
+    float32 restatement in ref64.  Returns (ntheta, nzp, nyp, rnxp) float32, the padding
+    columns untouched."""
+    from oracle import ref64
+    f32 = np.float32
+    nxp, nyp, nzp, nz = blk.nxp, blk.nyp, blk.nzp, blk.nz
+    cn = nzp // 2 + 1
+    tab = ref64.thick_tables(blk)
+    tab["wnc"] = blk.wnc
+    taper = np.ones(nzp, dtype=f32)
+    for k in range(nzp):
+        if k > nz:
+            dk = f32(ref64.dist_to_boundary(k, nz, nzp))
+            taper[k] = max(f32(1) - dk * dk, f32(0))
+    rt = np.asarray(blk.rel_thick, dtype=np.float64)
+    sf = rt.astype(f32).reshape(-1)
+    deltaF = (float(nz) * 1000.0 / (rt * float(blk.lz) * float(nzp))).reshape(-1)
+    k = np.arange(cn)
+    fk = deltaF[:, None] * k[None, :]
+    band = np.ascontiguousarray((fk < float(f32(blk.high_cut))) & (fk > float(f32(blk.low_cut))), dtype=np.uint8)
+    out = np.array(blk.data, dtype=np.float32)
+    for l in range(blk.ntheta):
+        fac = ref64.adjustment_factor(tab, l, sf[:, None], k[None, :])
+        fac = np.where(band.astype(bool), fac, 0.0)
+        f = np.ascontiguousarray(fac.astype(np.complex64)).view(np.float32)
+        traces = np.ascontiguousarray(np.moveaxis(out[l][..., :nxp], 0, -1).reshape(-1, nzp))
+        ref32_lib().ref32_divide_traces(_f(traces), traces.shape[0], nzp, _f(taper), _f(f),
+                                        band.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+        out[l][..., :nxp] = np.moveaxis(traces.reshape(nyp, nxp, nzp), -1, 0)
+    return out
 
 
 def sim_noise(seed: int, nsim: int, nxp: int, nyp: int, nzp: int, use_ref: bool = False) -> np.ndarray:

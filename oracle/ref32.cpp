@@ -17,6 +17,7 @@
 //   AVOInversion::getNextErrorVariance, fillkW, fillkWNorm  :1236-1300
 //   AVOInversion::simulate                         src/avoinversion.cpp:1354-1511
 //   SeismicParametersHolder::invFFTCovGrids        src/seismicparametersholder.cpp:432-456
+//   AVOInversion::divideDataByScaleWavelet, the trace transform   src/avoinversion.cpp:537-588
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -401,6 +402,44 @@ int ref32_invert(const ref32_block* b, float** mean, float** cov, float* errcorr
   for (int l = 0; l < nth; l++) delete[] Af[l];
   delete[] Af;
   return 0;
+}
+
+// The trace transform of AVOInversion::divideDataByScaleWavelet (src/avoinversion.cpp:
+// 537-588) with the reference's FFTW: ntr traces of nzp floats (traces[t*nzp + k]), each
+// divided by float(sqrt(float(nzp))), tapered (taper[k], 1 up to nz), transformed by a
+// 1D in-place rfftwnd plan, multiplied by factor[t*cnzp + k] (complex) where band[t*cnzp + k]
+// and zeroed elsewhere, transformed back and divided by float(sqrt(float(nzp))), in place.
+void ref32_divide_traces(float* traces, int ntr, int nzp, const float* taper, const float* factor,
+                         const unsigned char* band) {
+  const int cn = nzp / 2 + 1;
+  std::vector<float> r(2 * cn);
+  fftw_complex* c = reinterpret_cast<fftw_complex*>(r.data());
+  int n = nzp;
+  rfftwnd_plan p1 = rfftwnd_create_plan(1, &n, FFTW_REAL_TO_COMPLEX, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_plan p2 = rfftwnd_create_plan(1, &n, FFTW_COMPLEX_TO_REAL, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  const float rsq = static_cast<float>(std::sqrt(static_cast<float>(nzp)));
+  for (int t = 0; t < ntr; t++) {
+    float* tr = traces + (size_t)t * nzp;
+    for (int k = 0; k < nzp; k++) r[k] = tr[k] / rsq * taper[k];
+    rfftwnd_one_real_to_complex(p1, r.data(), c);
+    const float* f = factor + 2 * (size_t)t * cn;
+    const unsigned char* b = band + (size_t)t * cn;
+    for (int k = 0; k < cn; k++) {
+      if (b[k]) {
+        const float fr = f[2 * k], fi = f[2 * k + 1];
+        const float tmp = c[k].re * fr - c[k].im * fi;
+        c[k].im = c[k].im * fr + c[k].re * fi;
+        c[k].re = tmp;
+      } else {
+        c[k].re = 0.0f;
+        c[k].im = 0.0f;
+      }
+    }
+    rfftwnd_one_complex_to_real(p2, c, r.data());
+    for (int k = 0; k < nzp; k++) tr[k] = r[k] / rsq;
+  }
+  rfftwnd_destroy_plan(p1);
+  rfftwnd_destroy_plan(p2);
 }
 
 // Noise grids of nsim realisations exactly as simulate draws them from RandomGen(seed):

@@ -3,7 +3,8 @@
 Pins: FFTGrid::getFillNumber / getDistToBoundary against the sequences the reference
 documents beside them (src/fftgrid.cpp:1105-1108, 1160-1163); the interpolation plan of
 interpolateSeismic against hand-traced cases; the adjustment factor's limit (unit
-stretch, no stabilisation: 1/conj(W)); the ABI's validation of the new fields.
+stretch, no stabilisation: 1/conj(W)); the division against the reference's FFTW trace
+loop (oracle/_ref); the ABI's validation of the new fields.
 """
 import ctypes
 import dataclasses
@@ -140,3 +141,21 @@ def test_abi_validates_the_thickness_fields(blk):
     d.rel_thick = keep["relt"].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     d.energy_threshold = -1.0
     assert api.lib().crava_job_footprint(ctypes.byref(d), ctypes.byref(out)) == api.EINVAL
+
+
+def test_division_restatement_matches_the_reference_fftw():
+    """divideDataByScaleWavelet in float64 (ref64) against the same trace loop over the
+    reference's own FFTW 2.1.2 float transforms (oracle/_ref): the two agree to FP32
+    rounding, so the float64 restatement carries the reference's transform conventions
+    (scalings, half spectrum, band cut)."""
+    from oracle import bindings as ob
+    if not ob.ref32_available():
+        pytest.skip("oracle/_ref not built")
+    b = synth.make_block(synth.BlockSpec(nx=20, ny=16, nz=50, nxp=24, nyp=18, nzp=64, nsim=0, seed=9))
+    b = synth.with_rel_thick(b, seed=4)
+    ref = ob.ref32_divide(b)
+    mine = ref64.divide_data_by_scale_wavelet(b)
+    for l in range(b.ntheta):
+        x, r = mine[l][..., :b.nxp], ref[l][..., :b.nxp].astype(np.float64)
+        assert np.linalg.norm(x - r) / np.linalg.norm(r) < 2e-6
+        assert np.linalg.norm(r - b.data[l][..., :b.nxp]) > 1e-2 * np.linalg.norm(r)
