@@ -170,6 +170,7 @@ struct crava_job {
   double* eddk = nullptr;
   ThickParams tp{};
   float* energy = nullptr;
+  int* nzero = nullptr;            // zero-energy traces per angle
   TraceOp* ops = nullptr;
   // host copies of the small inputs
   std::vector<double> A, etc, pv, relt;
@@ -269,7 +270,7 @@ size_t thick_bytes(const crava_job_desc* d) {
          2 * align256(sizeof(float) * d->nzp) + align256(sizeof(int) * d->nxp) + align256(sizeof(int) * d->nyp) +
          align256(sizeof(float) * d->nxp) + align256(sizeof(float) * d->nyp) +
          align256(sizeof(double) * d->nxp * d->nyp) + align256(sizeof(float) * nth * nxy) +
-         align256(sizeof(TraceOp) * nth * nxy);
+         align256(sizeof(TraceOp) * nth * nxy) + align256(sizeof(int) * kMaxTheta);
 }
 
 size_t footprint(const crava_job_desc* d) {
@@ -884,6 +885,7 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     tp.rel_thick = (const double*)take(sizeof(double) * d.nxp * d.nyp);
     j->energy = (float*)take(sizeof(float) * nth * nxy);
     j->ops = (TraceOp*)take(sizeof(TraceOp) * nth * nxy);
+    j->nzero = (int*)take(sizeof(int) * kMaxTheta);
     build_thick_tables(d, tt);
     tp.nx = d.nx; tp.ny = d.ny; tp.nz = d.nz;
     tp.nxp = d.nxp; tp.nyp = d.nyp; tp.nzp = d.nzp;
@@ -908,6 +910,10 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     tp.low_cut = d.low_cut;
     tp.high_cut = d.high_cut;
     tp.rsq = static_cast<float>(std::sqrt(static_cast<float>(d.nzp)));
+    {
+      int e = 0;
+      tp.inv_rsq = std::frexp(tp.rsq, &e) == 0.5f ? 1.0f / tp.rsq : 0.f;   // rsq = 2^(e-1)
+    }
     tp.lz = d.lz;
   }
 #define JOB_TRY(call)                                          \
@@ -1237,17 +1243,29 @@ crava_status crava_job_divide_data(crava_job* job, void* stream) {
   }
   {
     ProfScope ps(ctx, KT_THICK_FILL, st);
-    CUDA_TRY(launch_trace_energy(tp, nth, job->energy, st, &nl));
+    CUDA_TRY(launch_trace_energy(tp, nth, job->energy, job->nzero, st, &nl));
   }
-  std::vector<float> energy(nth * nxy);
-  CUDA_TRY(cudaMemcpyAsync(energy.data(), job->energy, sizeof(float) * energy.size(), cudaMemcpyDeviceToHost, st));
+  // A zero threshold flags exactly the zero-energy traces: an angle without one needs no
+  // plan (no interpolation; the box of good traces is the whole interior), and only the
+  // other angles' energy maps come back to the host.
+  std::vector<int> nzero(nth);
+  CUDA_TRY(cudaMemcpyAsync(nzero.data(), job->nzero, sizeof(int) * nth, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
+  const bool zero_thr = d.energy_threshold == 0.f;
+  std::vector<float> energy(nth * nxy);
+  bool need = false;
+  for (int l = 0; l < nth; l++) need |= !zero_thr || nzero[l] > 0;
+  if (need) {
+    CUDA_TRY(cudaMemcpyAsync(energy.data(), job->energy, sizeof(float) * energy.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+  }
   // per angle: the interpolation plan (host), its levels in order, then the extrapolation
   std::vector<std::vector<TraceOp>> ops(nth);
   for (int l = 0; l < nth; l++) {
     std::vector<int> level_start;
-    int box[4];
-    plan_trace_interpolation(energy.data() + l * nxy, d.nx, d.ny, d.energy_threshold, ops[l], level_start, box);
+    int box[4] = {0, d.nx - 1, 0, d.ny - 1};
+    if (!zero_thr || nzero[l] > 0)
+      plan_trace_interpolation(energy.data() + l * nxy, d.nx, d.ny, d.energy_threshold, ops[l], level_start, box);
     TraceOp* dops = job->ops + l * nxy;
     if (!ops[l].empty())
       CUDA_TRY(cudaMemcpyAsync(dops, ops[l].data(), sizeof(TraceOp) * ops[l].size(), cudaMemcpyHostToDevice, st));

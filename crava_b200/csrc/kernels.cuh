@@ -108,6 +108,8 @@ struct ThickParams {
   float err_var[kMaxTheta];    // errThetaCov_ll
   float wnc, low_cut, high_cut;
   float rsq;                   // float(sqrt(float(nzp)))
+  float inv_rsq;               // 1/rsq when rsq is a power of two (x/rsq == x*inv_rsq exactly),
+                               // else 0: the kernel divides
   double lz;
   LinePlan zp;
   const float2* twz;
@@ -121,7 +123,8 @@ struct TraceOp {
 size_t thick_smem_bytes(int W, int nzp);
 int thick_tile_width(int nzp);
 cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, int* nlaunch);
-cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, cudaStream_t st, int* nlaunch);
+cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, int* nzero, cudaStream_t st,
+                                int* nlaunch);
 cudaError_t launch_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, const TraceOp* ops, int nops,
                                 cudaStream_t st, int* nlaunch);
 cudaError_t launch_extrapolate(const ThickParams& P, int l, const int box[4], cudaStream_t st, int* nlaunch);

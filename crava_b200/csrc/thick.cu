@@ -30,6 +30,12 @@ namespace {
 
 __device__ __forceinline__ float sq2(float2 v) { return __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)); }
 
+// x / float(sqrt(float(nzp))) correctly rounded; a multiplication when the divisor is a
+// power of two (nzp = 4^m), which rounds the same exact quotient once
+__device__ __forceinline__ float div_rsq(const ThickParams& P, float x) {
+  return P.inv_rsq != 0.f ? __fmul_rn(x, P.inv_rsq) : __fdiv_rn(x, P.rsq);
+}
+
 // Wavelet::getCAmp(k, scale) for k < cnzp (src/wavelet.cpp:337-382): the spectrum of the
 // wavelet stretched by `scale`, linear interpolation at k / scale, divided by scale.
 __device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, float scale) {
@@ -129,8 +135,8 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
     const int w = e & (W - 1), k = e >> lw;
     float2 v = R[e];
     const float tz = __ldg(P.ztaper + k);
-    v.x = __fmul_rn(__fdiv_rn(v.x, P.rsq), tz);
-    v.y = __fmul_rn(__fdiv_rn(v.y, P.rsq), tz);
+    v.x = __fmul_rn(div_rsq(P, v.x), tz);
+    v.y = __fmul_rn(div_rsq(P, v.y), tz);
     if (v.x != 0.f) s_live[2 * w] = 1;
     if (v.y != 0.f) s_live[2 * w + 1] = 1;
     R[e] = v;
@@ -175,16 +181,16 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
     if (2 * m >= P.nxp) continue;
     float* p = row + (size_t)k * kstride + 2 * m;
     const float2 v = R[e];
-    const float2 o = make_float2(s_live[2 * w] ? __fdiv_rn(v.x, P.rsq) : 0.f,
-                                 s_live[2 * w + 1] ? __fdiv_rn(v.y, P.rsq) : 0.f);
+    const float2 o = make_float2(s_live[2 * w] ? div_rsq(P, v.x) : 0.f, s_live[2 * w + 1] ? div_rsq(P, v.y) : 0.f);
     if (2 * m + 1 < P.nxp) *reinterpret_cast<float2*>(p) = o;
     else *p = o.x;
   }
 }
 
 // Energy of every interior trace over its first nz samples, summed in order in float
-// (src/fftgrid.cpp:2360-2371).
-__global__ void k_trace_energy(const __grid_constant__ ThickParams P, float* energy) {
+// (src/fftgrid.cpp:2360-2371); nzero[l] counts the traces of angle l with zero energy (the
+// only ones a zero threshold flags).
+__global__ void k_trace_energy(const __grid_constant__ ThickParams P, float* energy, int* nzero) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, l = blockIdx.z;
   if (i >= P.nx) return;
   const float* g = P.grid[l] + (size_t)j * P.rnxp + i;
@@ -195,6 +201,7 @@ __global__ void k_trace_energy(const __grid_constant__ ThickParams P, float* ene
     e = __fadd_rn(e, __fmul_rn(v, v));
   }
   energy[((size_t)l * P.ny + j) * P.nx + i] = e;
+  if (e == 0.f) atomicAdd(nzero + l, 1);
 }
 
 // interpolateTrace (src/fftgrid.cpp:2440-2480) for a list of independent operations: the
@@ -266,9 +273,12 @@ cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, cudaStream_t st, int* nlaunch) {
+cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, int* nzero, cudaStream_t st,
+                                int* nlaunch) {
+  cudaError_t e = cudaMemsetAsync(nzero, 0, sizeof(int) * nth, st);
+  if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((P.nx + 127) / 128), (unsigned)P.ny, (unsigned)nth);
-  k_trace_energy<<<grid, 128, 0, st>>>(P, energy);
+  k_trace_energy<<<grid, 128, 0, st>>>(P, energy, nzero);
   if (nlaunch) (*nlaunch)++;
   return cudaGetLastError();
 }
