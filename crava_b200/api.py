@@ -33,7 +33,7 @@ EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_s
            "crava_job_create", "crava_job_destroy", "crava_job_footprint", "crava_job_upload",
            "crava_job_download", "crava_job_device_ptr", "crava_job_run", "crava_job_counters",
            "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches", "crava_ctx_set_profiling",
-           "crava_ctx_kernel_times", "crava_job_divide_data"]
+           "crava_ctx_kernel_times", "crava_job_divide_data", "crava_job_fill_prior"]
 KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r", "xy_fwd", "xy_inv", "thick_divide",
                   "thick_fill"]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
@@ -102,6 +102,7 @@ def lib() -> ctypes.CDLL:
     L.crava_job_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.crava_job_run.argtypes = [vp, vp]
     L.crava_job_divide_data.argtypes = [vp, vp]
+    L.crava_job_fill_prior.argtypes = [vp, ctypes.c_float, ctypes.c_float, vp]
     L.crava_job_counters.argtypes = [vp, ctypes.POINTER(Counters)]
     L.crava_fft_r2c.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
     L.crava_fft_c2r.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
@@ -252,6 +253,11 @@ class Job:
 
     def run(self, stream=None):
         _check(lib().crava_job_run(self._h, stream))
+
+    def fill_prior(self, corr_grad_i: float = 0.0, corr_grad_j: float = 0.0, stream=None):
+        """GRIDS-mode job: generate the six prior covariance grids and the error-correlation
+        grid on the device from corr_xy and circ_corr_t (InitializeCorrelations)."""
+        _check(lib().crava_job_fill_prior(self._h, float(corr_grad_i), float(corr_grad_j), stream))
 
     def divide_data(self, stream=None):
         """divideDataByScaleWavelet + interpolateSeismic on the uploaded data (non-constant

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrava_gpu.so")
-SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "facies.cu", "thick.cu"]
+SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "facies.cu", "thick.cu", "prior.cu"]
 HEADERS = ["fft_core.cuh", "fft2.cuh", "kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

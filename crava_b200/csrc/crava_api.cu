@@ -797,7 +797,8 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->pv.assign(d.prior_var0, d.prior_var0 + 9);
   j->wav.assign(d.wavelet, d.wavelet + (size_t)d.ntheta * d.nzp);
   j->wnorm.assign(d.wavelet_norm, d.wavelet_norm + d.ntheta);
-  if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) {
+  // the factors are kept in GRIDS mode too when given: crava_job_fill_prior builds the grids
+  if (d.prior_mode == CRAVA_PRIOR_SEPARABLE || (d.corr_xy && d.circ_corr_t)) {
     j->corr_xy.assign(d.corr_xy, d.corr_xy + (size_t)d.nxp * d.nyp);
     j->circ.assign(d.circ_corr_t, d.circ_corr_t + d.nzp);
   }
@@ -1216,6 +1217,48 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out) {
   for (int q = 0; q < 6; q++) CUDA_TRY(cudaMemcpy(&v[q], job->cov[q], sizeof(float), cudaMemcpyDeviceToHost));
   float P[9] = {v[0], v[3], v[4], v[3], v[1], v[5], v[4], v[5], v[2]};
   std::memcpy(out->post_var0, P, sizeof(P));
+  return CRAVA_OK;
+}
+
+crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_grad_j, void* stream) {
+  if (!job) return fail(CRAVA_EINVAL, "null job");
+  const crava_job_desc& d = job->d;
+  if (d.prior_mode != CRAVA_PRIOR_GRIDS)
+    return fail(CRAVA_ESTATE, "crava_job_fill_prior needs a CRAVA_PRIOR_GRIDS job");
+  if (job->corr_xy.empty() || job->circ.empty())
+    return fail(CRAVA_EINVAL, "crava_job_fill_prior needs corr_xy and circ_corr_t in the job description");
+  if (!std::isfinite(corr_grad_i) || !std::isfinite(corr_grad_j))
+    return fail(CRAVA_EINVAL, "correlation gradients must be finite");
+  crava_ctx* ctx = job->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  // corrXY and circCorrT into buffers that only SEPARABLE jobs use otherwise
+  float* cxy = job->cxy_grid;
+  float* ct = reinterpret_cast<float*>(job->ct);
+  CUDA_TRY(cudaMemcpyAsync(cxy, job->corr_xy.data(), sizeof(float) * job->corr_xy.size(), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(ct, job->circ.data(), sizeof(float) * job->circ.size(), cudaMemcpyHostToDevice, st));
+  PriorFill P;
+  const int qa[6] = {0, 1, 2, 0, 0, 1}, qb[6] = {0, 1, 2, 1, 2, 2};
+  for (int q = 0; q < 6; q++) {
+    P.cov[q] = job->in_cov[q];
+    P.pv[q] = static_cast<float>(job->pv[qa[q] * 3 + qb[q]]);
+  }
+  P.err = job->in_err;
+  P.cxy = cxy;
+  P.ct = ct;
+  P.gi = corr_grad_i;
+  P.gj = corr_grad_j;
+  P.nxp = d.nxp;
+  P.nyp = d.nyp;
+  P.nzp = d.nzp;
+  P.rnxp = job->rnxp;
+  int nl = 0;
+  CUDA_TRY(launch_fill_prior(P, st, &nl));
+  // the host vectors stay with the job; wait so that the call has the reference's
+  // synchronous semantics like the uploads it replaces
+  CUDA_TRY(cudaStreamSynchronize(st));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->launches += nl;
   return CRAVA_OK;
 }
 

@@ -114,6 +114,19 @@ struct ThickParams {
   LinePlan zp;
   const float2* twz;
 };
+// Prior grids of a GRIDS-mode job generated on the device (prior.cu): the six covariance
+// grids fillInParamCorr x priorVar0 and the error-correlation grid fillInErrCorr.
+struct PriorFill {
+  float* cov[6];               // order Vp, Vs, Rho, VpVs, VpRho, VsRho
+  float* err;
+  const float* cxy;            // nxp x nyp corrXY
+  const float* ct;             // nzp circCorrT
+  float pv[6];                 // float(priorVar0(a, b)) in the grid order
+  float gi, gj;                // correlation gradients (samples per lateral index)
+  int nxp, nyp, nzp, rnxp;
+};
+cudaError_t launch_fill_prior(const PriorFill& P, cudaStream_t st, int* nlaunch);
+
 // One interpolateTrace: trace t (i + nx j) <- mean of nb[] (left, right, up, down; -1 absent)
 struct TraceOp {
   int t;

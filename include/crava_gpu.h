@@ -171,6 +171,16 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out);
  * without the flag. */
 crava_status crava_job_divide_data(crava_job* job, void* stream);
 
+/* CRAVA_PRIOR_GRIDS jobs whose description also carries corr_xy and circ_corr_t: the six
+ * prior covariance grids and the error-correlation grid are generated on the device, in
+ * place of their uploads, as SeismicParametersHolder::InitializeCorrelations
+ * (src/seismicparametersholder.cpp:333-348: FFTGrid::fillInParamCorr x priorVar0,
+ * src/fftgrid.cpp:878-928) and FFTGrid::fillInErrCorr (src/fftgrid.cpp:777-828) fill them,
+ * with the lateral correlation gradients corr_grad_i, corr_grad_j (samples per index) and
+ * the reference's float arithmetic (the grids are equal bit for bit).  Call before
+ * crava_job_run; returns after `stream` has finished the work. */
+crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_grad_j, void* stream);
+
 /* FFTGrid drop-ins on a device grid (src/fftgrid.cpp:1587-1612 / 1615-1643).
  * covariance != 0 selects the COVARIANCE scaling. */
 crava_status crava_fft_r2c(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int nzp, int covariance, void* stream);

@@ -84,25 +84,26 @@ def fill_param_corr(corr_xy, circ_corr_t, nxp, nyp, nzp, grad_i=0.0, grad_j=0.0)
 
 
 def fill_err_corr(corr_xy, nxp, nyp, nzp, grad_i=0.0, grad_j=0.0):
-    """FFTGrid::fillInErrCorr (src/fftgrid.cpp:777-828): corrXY at the (rotated) k=0 lag."""
-    out = np.zeros((nzp, nyp, nxp), dtype=np.float32)
-    cxy = corr_xy.astype(np.float32)
-    for j in range(nyp):
-        cj = j if j < -(j - nyp) else j - nyp
-        for i in range(nxp):
-            ci = i if i < -(i - nxp) else i - nxp
-            for k in range(nzp):
-                subk = np.float32(k + ci * grad_i + cj * grad_j)
-                if abs(subk) < 1.0 or abs(subk - nzp) < 1.0:
-                    basek = int(subk)
-                    subk = np.float32(subk - basek)
-                    while basek < -1:
-                        basek += nzp
-                    while basek >= 1:
-                        basek -= nzp
-                    if basek < 0:
-                        subk = np.float32(1 - subk)
-                    out[k, j, i] = np.float32((1 - subk) * cxy[j, i])
+    """FFTGrid::fillInErrCorr (src/fftgrid.cpp:777-828): corrXY at the (rotated) k=0 lag,
+    subK = k + cycleI*gradI + cycleJ*gradJ in float left to right as the reference."""
+    f32 = np.float32
+    cxy = corr_xy.astype(f32)
+    i = np.arange(nxp)
+    j = np.arange(nyp)
+    ci = np.where(i < -(i - nxp), i, i - nxp).astype(f32)
+    cj = np.where(j < -(j - nyp), j, j - nyp).astype(f32)
+    ti = (ci * f32(grad_i)).astype(f32)[None, :]
+    tj = (cj * f32(grad_j)).astype(f32)[:, None]
+    out = np.zeros((nzp, nyp, nxp), dtype=f32)
+    for k in range(nzp):
+        sub = ((f32(k) + ti).astype(f32) + tj).astype(f32)                 # (nyp, nxp)
+        hit = (np.abs(sub) < f32(1.0)) | (np.abs((sub - f32(nzp)).astype(f32)) < f32(1.0))
+        base = np.trunc(sub).astype(np.int64)
+        s = (sub - base.astype(f32)).astype(f32)
+        base = np.where(base < -1, base + nzp, base)
+        base = np.where(base >= 1, base - nzp, base)
+        s = np.where(base < 0, (f32(1) - s).astype(f32), s)
+        out[k] = np.where(hit, ((f32(1) - s).astype(f32) * cxy).astype(f32), f32(0))
     return out
 
 

@@ -1,0 +1,89 @@
+"""Prior grids generated on the device (crava_job_fill_prior) against the oracle.
+
+InitializeCorrelations' six covariance grids (fillInParamCorr x priorVar0) and fillInErrCorr
+with lateral correlation gradients: the device grids equal the oracle's float32 restatement of
+the reference's float arithmetic bit for bit; the inversion on them matches the FP64 oracle
+with the constant-thickness parity tolerances (mean 1e-4, covariance 1e-3).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+from oracle import ref64
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(x, ref):
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    return float(np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def grad_block(gi, gj, dims=(30, 24, 40, 32, 27, 48), nsim=0):
+    nx, ny, nz, nxp, nyp, nzp = dims
+    spec = synth.BlockSpec(nx=nx, ny=ny, nz=nz, nxp=nxp, nyp=nyp, nzp=nzp, theta_deg=(8.0, 20.0, 32.0),
+                           peak_hz=(30.0,) * 3, sn=(5.0,) * 3, nsim=nsim, seed=23, corr_grad_i=gi, corr_grad_j=gj)
+    return synth.make_block(spec)
+
+
+@pytest.mark.parametrize("gi,gj", [(0.0, 0.0), (0.37, -0.21), (-1.3, 0.8)])
+def test_filled_grids_equal_the_reference_float_grids(ctx, gi, gj):
+    blk = grad_block(gi, gj)
+    job = api.Job(ctx, blk, api.PRIOR_GRIDS)
+    try:
+        job.fill_prior(blk.corr_grad_i, blk.corr_grad_j)
+        covs, _pairs = ref64.prior_cov_grids(blk)
+        for q in range(6):
+            got = job.download(api.ROLE_PRIOR_COV, q)[..., :blk.nxp]
+            assert np.array_equal(got, covs[q]), q
+        err = ref64.fill_err_corr(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp, blk.corr_grad_i, blk.corr_grad_j)
+        assert np.array_equal(job.download(api.ROLE_ERR_CORR, 0)[..., :blk.nxp], err)
+    finally:
+        job.close()
+
+
+def test_inversion_on_filled_grids_matches_oracle(ctx):
+    blk = grad_block(0.37, -0.21)
+    job = api.Job(ctx, blk, api.PRIOR_GRIDS)
+    try:
+        for l in range(blk.ntheta):
+            job.upload(api.ROLE_DATA, l, blk.data[l])
+        for a in range(3):
+            job.upload(api.ROLE_MEAN, a, blk.mean[a])
+        job.fill_prior(blk.corr_grad_i, blk.corr_grad_j)
+        job.run()
+        out = job.download_outputs()
+        cnt = job.counters()
+    finally:
+        job.close()
+    post = ref64.posterior(blk)
+    nxp = blk.nxp
+    for a in range(3):
+        assert rel(out["mean"][a][..., :nxp], post.mean[a][..., :nxp]) < 1e-4, a
+    for q in range(6):
+        assert rel(out["cov"][q][..., :nxp], post.cov[q][..., :nxp]) < 1e-3, q
+    assert cnt["inverted_bins"] == post.n_inverted
+    # the gradients matter: the zero-gradient prior gives a different posterior
+    flat = ref64.posterior(dataclasses.replace(blk, corr_grad_i=0.0, corr_grad_j=0.0))
+    assert rel(flat.cov[0][..., :nxp], post.cov[0][..., :nxp]) > 1e-3
+
+
+def test_fill_prior_needs_a_grids_job(ctx):
+    blk = grad_block(0.0, 0.0)
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE)
+    try:
+        with pytest.raises(api.CravaError) as ei:
+            job.fill_prior(0.1, 0.1)
+        assert ei.value.status == api.ESTATE
+    finally:
+        job.close()

@@ -118,14 +118,18 @@ def test_dead_traces_interpolated(ctx, threshold):
             assert np.any(got[0][:, j, i] != 0.0)
 
 
-@pytest.mark.parametrize("prior_mode", [api.PRIOR_SEPARABLE, api.PRIOR_GRIDS])
-def test_nonconst_inversion_matches_oracle(ctx, prior_mode):
-    blk = thick_block(nsim=0)
-    kw = {}
+@pytest.mark.parametrize("prior_mode,fp64,dims", [
+    (api.PRIOR_SEPARABLE, 0.0, None), (api.PRIOR_GRIDS, 0.0, None),
+    (api.PRIOR_SEPARABLE, 1.0, None),                      # every bin refactorised in FP64
+    (api.PRIOR_SEPARABLE, 0.0, (33, 21, 90, 35, 27, 105)),  # odd nxp and nzp
+])
+def test_nonconst_inversion_matches_oracle(ctx, prior_mode, fp64, dims):
+    blk = thick_block(*dims, nsim=0) if dims else thick_block(nsim=0)
+    kw = {"fp64_threshold": fp64}
     if prior_mode == api.PRIOR_GRIDS:
         covs, _pairs = ref64.prior_cov_grids(blk)
-        kw = {"cov_grids": [c[..., :blk.nxp] for c in covs],
-              "err_corr": ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)[..., :blk.nxp]}
+        kw.update(cov_grids=[c[..., :blk.nxp] for c in covs],
+                  err_corr=ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)[..., :blk.nxp])
     out = api.invert_block(ctx, blk, prior_mode=prior_mode, **kw)
     ref_blk = dataclasses.replace(blk, data=oracle_divided(blk))
     post = ref64.posterior(ref_blk)
