@@ -158,6 +158,12 @@ int main(int argc, char** argv) {
       rd.read(set.relThick.data(), set.relThick.size());
       set.energyThreshold = rd.one<float>();
     }
+    // optional trailing section after it: correlation gradients (two floats)
+    int grads = 0;
+    if (fread(&grads, sizeof(int), 1, fi) == 1 && grads) {
+      set.corrGradI = rd.one<float>();
+      set.corrGradJ = rd.one<float>();
+    }
     fclose(fi);
 
     // FFTGrid round trip on a copy of the first DATA grid

@@ -207,8 +207,11 @@ void AVOInversion::run() {
   d.wavelet = wav.data();
   d.wavelet_norm = wn.data();
   d.prior_var0 = pv.data();
+  // factors with nonzero correlation gradients: InitializeCorrelations' grids are generated
+  // on the device (crava_job_fill_prior) and inverted in GRIDS mode
+  const bool gradients = separable_ && (set_.corrGradI != 0.f || set_.corrGradJ != 0.f);
   if (separable_) {
-    d.prior_mode = CRAVA_PRIOR_SEPARABLE;
+    d.prior_mode = gradients ? CRAVA_PRIOR_GRIDS : CRAVA_PRIOR_SEPARABLE;
     d.corr_xy = corrXY_.data();
     d.circ_corr_t = circCorrT_.data();
   } else {
@@ -256,6 +259,8 @@ void AVOInversion::run() {
   if (!separable_) {
     for (int q = 0; q < 6; q++) up(CRAVA_ROLE_PRIOR_COV, q, cov[q]);
     up(CRAVA_ROLE_ERR_CORR, 0, sp_.errCorr);
+  } else if (gradients) {
+    check(crava_job_fill_prior(job, set_.corrGradI, set_.corrGradJ, nullptr));
   }
   if (noise_) {
     if ((int)noise_->size() != 3 * nsim) throw Error(CRAVA_EINVAL, "simulate: 3 noise grids per realisation");

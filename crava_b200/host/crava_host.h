@@ -142,6 +142,9 @@ struct AVOInversionSettings {
   // (divideDataByScaleWavelet + interpolateSeismic).  Empty: constant thickness.
   std::vector<double> relThick;
   float energyThreshold = 0;               // ModelSettings::getEnergyThreshold
+  // lateral correlation gradients of InitializeCorrelations (samples per index); with the
+  // separable factors and a nonzero gradient the prior grids are generated on the device
+  float corrGradI = 0, corrGradJ = 0;
 };
 
 class AVOInversion {

@@ -62,10 +62,16 @@ def write_block(path, blk, grids, noise):
             np.asarray(blk.mean[a], dtype=np.float32).tofile(f)
         if noise is not None:
             np.ascontiguousarray(noise, dtype=np.complex64).tofile(f)
-        if getattr(blk, "rel_thick", None) is not None:
-            np.array([1], dtype=np.int32).tofile(f)
+        nonconst = getattr(blk, "rel_thick", None) is not None
+        grads = not grids and (blk.corr_grad_i != 0.0 or blk.corr_grad_j != 0.0)
+        if nonconst or grads:
+            np.array([1 if nonconst else 0], dtype=np.int32).tofile(f)
+        if nonconst:
             np.ascontiguousarray(blk.rel_thick, dtype=np.float64).tofile(f)
             np.array([blk.energy_threshold], dtype=np.float32).tofile(f)
+        if grads:
+            np.array([1], dtype=np.int32).tofile(f)
+            np.array([blk.corr_grad_i, blk.corr_grad_j], dtype=np.float32).tofile(f)
 
 
 def read_out(path, blk):
@@ -131,6 +137,27 @@ def test_host_layer_nonconst_thickness(tmp_path, grids):
     div = ref64.divide_data_by_scale_wavelet(blk)
     divided = np.stack([ref64.interpolate_seismic(div[l], blk, blk.energy_threshold) for l in range(blk.ntheta)])
     post = ref64.posterior(dataclasses.replace(blk, data=divided))
+    nx = blk.nxp
+    assert out["counters"][0] == post.n_inverted
+    for a in range(3):
+        assert crel(out["mean"][a][..., :nx], post.mean[a][..., :nx]) < 1e-4, ("mean", a)
+    for q in range(6):
+        assert crel(out["cov"][q][..., :nx], post.cov[q][..., :nx]) < 1e-3, ("cov", q)
+
+
+def test_host_layer_correlation_gradients(tmp_path):
+    """AVOInversionSettings::corrGradI/J with the separable factors: the layer generates
+    InitializeCorrelations' grids on the device (crava_job_fill_prior) and inverts in GRIDS
+    mode; the result matches the oracle's posterior on the gradient prior."""
+    assert os.path.exists(DEMO)
+    blk = synth.make_block(synth.BlockSpec(nx=30, ny=28, nz=40, theta_deg=(8.0, 20.0, 32.0), peak_hz=(30.0,) * 3,
+                                           sn=(5.0,) * 3, nsim=0, seed=29, corr_grad_i=0.37, corr_grad_j=-0.21))
+    fin, fout = tmp_path / "block.bin", tmp_path / "out.bin"
+    write_block(fin, blk, False, None)
+    r = subprocess.run([DEMO, str(fin), str(fout)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = read_out(fout, blk)
+    post = ref64.posterior(blk)
     nx = blk.nxp
     assert out["counters"][0] == post.n_inverted
     for a in range(3):
