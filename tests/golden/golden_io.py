@@ -26,4 +26,7 @@ def load(name):
                       wnc=float(sc("wnc")), min_rel_thick=float(sc("min_rel_thick")),
                       corr_grad_i=float(sc("corr_grad_i")), corr_grad_j=float(sc("corr_grad_j")),
                       nsim=int(sc("nsim")), seed=int(sc("seed")))
+    if "rel_thick" in z:
+        blk.rel_thick = z["rel_thick"]
+        blk.energy_threshold = float(z["energy_threshold"])
     return blk, z

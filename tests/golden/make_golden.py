@@ -59,9 +59,30 @@ def make(name, kw, noise_seed=1234):
     return out
 
 
+# Non-constant thickness: divideDataByScaleWavelet's trace loop over the reference's FFTW
+# 2.1.2 float plans (oracle/_ref ref32_divide_traces), padded block, rel_thick surface.
+THICK_CASES = {
+    "t1_nonconst": (dict(nx=14, ny=10, nz=24, nxp=16, nyp=12, nzp=32, theta_deg=(8.0, 20.0, 32.0),
+                         peak_hz=(30.0,) * 3, sn=(5.0,) * 3, nsim=0, seed=12), 11),
+}
+
+
+def make_thick(name, kw, surface_seed):
+    blk = synth.with_rel_thick(synth.make_block(synth.BlockSpec(**kw)), seed=surface_seed)
+    out = {k: np.asarray(getattr(blk, k)) for k in SCALARS}
+    out.update({k: getattr(blk, k) for k in ARRAYS})
+    out.update({"rel_thick": blk.rel_thick, "energy_threshold": np.float32(blk.energy_threshold),
+                "ref_divided": ob.ref32_divide(blk)})
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return out
+
+
 if __name__ == "__main__":
     if not ob.ref32_available():
         sys.exit("oracle/_ref/libref32.so missing: run `make -C oracle` with the reference tree present")
     for name, kw in CASES.items():
         make(name, kw)
+        print("wrote", name)
+    for name, (kw, sseed) in THICK_CASES.items():
+        make_thick(name, kw, sseed)
         print("wrote", name)

@@ -164,3 +164,16 @@ def test_noalloc_and_serving_reject_nonconst(ctx):
     arr_out = (vp * 9)(*([1] * 9))
     st = api.lib().crava_invert_noalloc(__import__("ctypes").byref(d), arr_in, arr_out, None)
     assert st == api.ENOTSUP
+
+
+def test_divide_data_matches_the_golden_fixture(ctx):
+    """The GPU division against the reference-FFTW division frozen in
+    tests/golden/t1_nonconst.npz (followed by the oracle's interpolateSeismic, which for
+    this block only rebuilds the padding)."""
+    from tests.golden import golden_io
+    blk, z = golden_io.load("t1_nonconst")
+    got = gpu_divided(ctx, blk)
+    ref = np.stack([ref64.interpolate_seismic(z["ref_divided"][l].astype(np.float64), blk, blk.energy_threshold)
+                    for l in range(blk.ntheta)])
+    for l in range(blk.ntheta):
+        assert rel(got[l][..., :blk.nxp], ref[l][..., :blk.nxp]) < TOL_DIV, l

@@ -159,3 +159,15 @@ def test_division_restatement_matches_the_reference_fftw():
         x, r = mine[l][..., :b.nxp], ref[l][..., :b.nxp].astype(np.float64)
         assert np.linalg.norm(x - r) / np.linalg.norm(r) < 2e-6
         assert np.linalg.norm(r - b.data[l][..., :b.nxp]) > 1e-2 * np.linalg.norm(r)
+
+
+def test_division_restatement_matches_the_golden_fixture():
+    """The committed fixture tests/golden/t1_nonconst.npz holds the division computed over
+    the reference's FFTW 2.1.2 float plans (make_golden.py); the float64 restatement agrees."""
+    from tests.golden import golden_io
+    b, z = golden_io.load("t1_nonconst")
+    mine = ref64.divide_data_by_scale_wavelet(b)
+    ref = z["ref_divided"]
+    for l in range(b.ntheta):
+        x, r = mine[l][..., :b.nxp], ref[l][..., :b.nxp].astype(np.float64)
+        assert np.linalg.norm(x - r) / np.linalg.norm(r) < 2e-6, l
