@@ -64,7 +64,7 @@ class JobDesc(ctypes.Structure):
 class Counters(ctypes.Structure):
     _fields_ = [("inverted_bins", ctypes.c_longlong), ("chol_fallbacks", ctypes.c_longlong),
                 ("sim_chol_zero", ctypes.c_longlong), ("fp64_bins", ctypes.c_longlong),
-                ("post_var0", ctypes.c_float * 9)]
+                ("post_var0", ctypes.c_float * 9), ("nonfinite_tiles", ctypes.c_longlong)]
 
 
 class FaciesDesc(ctypes.Structure):
@@ -265,10 +265,13 @@ class Job:
         _check(lib().crava_job_divide_data(self._h, stream))
 
     def counters(self) -> dict:
+        """Per-job counters after a run; raises CravaError (status ENUMERIC) when the data
+        or prior-mean grids held a NaN or Inf."""
         c = Counters()
         _check(lib().crava_job_counters(self._h, ctypes.byref(c)))
         return {"inverted_bins": c.inverted_bins, "chol_fallbacks": c.chol_fallbacks,
                 "sim_chol_zero": c.sim_chol_zero, "fp64_bins": c.fp64_bins,
+                "nonfinite_tiles": c.nonfinite_tiles,
                 "post_var0": np.array(list(c.post_var0), dtype=np.float32).reshape(3, 3)}
 
     def upload_block(self, cov_grids=None, err_corr=None, noise=None):

@@ -255,6 +255,26 @@ crava_status validate(const crava_job_desc* d) {
   }
   if (!(d->fp64_threshold >= 0.f) || !(d->fp64_threshold < INFINITY))
     return fail(CRAVA_EINVAL, "fp64_threshold must be finite and >= 0");
+  {
+    // the small inputs of the description are read on the host: a NaN or Inf there is
+    // rejected before anything reaches the device
+    auto finite = [](const auto* p, size_t n) {
+      for (size_t q = 0; q < n; q++)
+        if (!std::isfinite((double)p[q])) return false;
+      return true;
+    };
+    const size_t nth = (size_t)d->ntheta;
+    if (!finite(d->A, 3 * nth) || !finite(d->err_theta_cov, nth * nth) || !finite(d->prior_var0, 9) ||
+        !finite(d->wavelet, nth * d->nzp) || !finite(d->wavelet_norm, nth) || !std::isfinite(d->lz) ||
+        !std::isfinite(d->min_rel_thick) || !std::isfinite(d->low_cut) || !std::isfinite(d->high_cut) ||
+        !std::isfinite(d->wnc))
+      return fail(CRAVA_ENUMERIC, "non-finite value in the job description (A, err_theta_cov, prior_var0, "
+                                  "wavelets or scalars)");
+    if (d->corr_xy && !finite(d->corr_xy, (size_t)d->nxp * d->nyp))
+      return fail(CRAVA_ENUMERIC, "non-finite value in corr_xy");
+    if (d->circ_corr_t && !finite(d->circ_corr_t, (size_t)d->nzp))
+      return fail(CRAVA_ENUMERIC, "non-finite value in circ_corr_t");
+  }
   for (int l = 0; l < d->ntheta; l++)
     if (!(d->wavelet_norm[l] > 0)) return fail(CRAVA_EINVAL, "wavelet norm must be positive");
   return CRAVA_OK;
@@ -1067,7 +1087,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   const crava_job_desc& d = job->d;
   cudaStream_t st = (cudaStream_t)stream;
   CUDA_TRY(cudaSetDevice(ctx->device));
-  CUDA_TRY(cudaMemsetAsync(job->counters, 0, 4 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(job->counters, 0, kNumCounters * sizeof(unsigned long long), st));
   const bool grids = d.prior_mode == CRAVA_PRIOR_GRIDS;
   const float fs = fwd_scale(job->N);
   crava_status s;
@@ -1170,7 +1190,8 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   }
   zp.kz.kw = job->kw; zp.kz.e1 = job->e1; zp.kz.e2 = job->e2; zp.kz.inv = job->inv;
   zp.kz.kwd = job->kwd; zp.kz.e1d = job->e1d; zp.kz.e2d = job->e2d;
-  zp.kz.ed = job->edk;     // null unless CRAVA_FLAG_NONCONST_THICK
+  zp.kz.ed = job->edk;     // always uploaded: wnc errThetaCov_ll per kz, times |e3(k)|^2 with
+                           // CRAVA_FLAG_NONCONST_THICK
   zp.kz.edd = job->eddk;
   zp.fp64_threshold = d.fp64_threshold;
   for (int l = 0; l < d.ntheta; l++) {
@@ -1207,16 +1228,20 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out) {
   if (!job || !out) return fail(CRAVA_EINVAL, "null argument");
   if (!job->ran) return fail(CRAVA_ESTATE, "counters are defined only after crava_job_run");
   CUDA_TRY(cudaSetDevice(job->ctx->device));
-  unsigned long long c[4];
+  unsigned long long c[kNumCounters];
   CUDA_TRY(cudaMemcpy(c, job->counters, sizeof(c), cudaMemcpyDeviceToHost));
   out->inverted_bins = (long long)c[0];
   out->chol_fallbacks = (long long)c[1];
   out->sim_chol_zero = (long long)c[2];
   out->fp64_bins = (long long)c[3];
+  out->nonfinite_tiles = (long long)c[4];
   float v[6];
   for (int q = 0; q < 6; q++) CUDA_TRY(cudaMemcpy(&v[q], job->cov[q], sizeof(float), cudaMemcpyDeviceToHost));
   float P[9] = {v[0], v[3], v[4], v[3], v[1], v[5], v[4], v[5], v[2]};
   std::memcpy(out->post_var0, P, sizeof(P));
+  if (c[4] > 0)
+    return fail(CRAVA_ENUMERIC, "the data or prior-mean grids hold non-finite values (" + std::to_string(c[4]) +
+                                    " pencil tiles of non-finite spectra)");
   return CRAVA_OK;
 }
 
@@ -1386,10 +1411,9 @@ crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int n
 // ---------------------------------------------------------------------------------------
 // Inversion without device allocation (crava_invert_noalloc).
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA stream capture whose
-// allocations are forbidden, plugins hosted by an application that owns the device memory
-// pool and forbids other allocators, or hot loops where an allocation's implicit device
-// synchronisation is not acceptable.  For them this entry point runs one small block with
+// Some callers cannot call cudaMalloc: plugins hosted by an application that owns the
+// device memory pool and forbids other allocators, or hot loops where an allocation's
+// implicit device synchronisation is not acceptable.  For them this entry point runs one small block with
 // every intermediate in g_noalloc_scratch, a fixed array in the library's own device image:
 // each GPU that loads the library holds its CRAVA_NOALLOC_SCRATCH_BYTES until the process
 // exits, every call reuses it (so calls whose work overlaps on the GPU race), and blocks
@@ -1483,7 +1507,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   const size_t o_ed = take(sizeof(float) * d.nzp * d.ntheta);
   const size_t o_cxy = take(sizeof(float) * rnxp * d.nyp);
   const size_t o_ct = take(sizeof(float2) * d.nzp);
-  const size_t o_cnt = take(4 * sizeof(unsigned long long));
+  const size_t o_cnt = take(kNumCounters * sizeof(unsigned long long));
   if (off > (size_t)CRAVA_NOALLOC_SCRATCH_BYTES)
     return fail(CRAVA_ENOTSUP, "block needs " + std::to_string(off) + " bytes of scratch; crava_invert_noalloc has " +
                                    std::to_string((size_t)CRAVA_NOALLOC_SCRATCH_BYTES));
@@ -1516,7 +1540,7 @@ extern "C" crava_status crava_invert_noalloc(const crava_job_desc* desc, const f
   CUDA_TRY(put(o_ed, edk.data(), sizeof(float) * edk.size()));
   CUDA_TRY(put(o_ct, ct.data(), sizeof(float2) * ct.size()));
   CUDA_TRY(put(o_cxy, gxy.data(), sizeof(float) * gxy.size()));
-  CUDA_TRY(cudaMemsetAsync(base + o_cnt, 0, 4 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(base + o_cnt, 0, kNumCounters * sizeof(unsigned long long), st));
   const float2* twx = (const float2*)(base + o_twx);
   const float2* twn = (const float2*)(base + o_twn);
   const float2* twy = (const float2*)(base + o_twy);
@@ -1841,7 +1865,15 @@ void serve_loop(crava_server* sv) {
         if (!sv->busy[k]) { slot = k; break; }
       if (slot < 0) break;
       ServeReq* r = sv->pending.front();
-      if (!serve_admit(sv, r, slot)) break;  // waits for memory to be released
+      if (!serve_admit(sv, r, slot)) {
+        // out of memory with nothing in flight: no release will ever make room, so the
+        // request fails instead of holding the queue
+        if (!sv->inflight.empty()) break;   // waits for memory to be released
+        r->state = CRAVA_REQ_FAILED;
+        r->status = CRAVA_ENOMEM;
+        r->err = "job does not fit the device memory even with nothing else in flight";
+        r->t_start = now_ms();
+      }
       sv->pending.pop_front();
       if (r->state == CRAVA_REQ_FAILED) r->t_done = now_ms();
       progressed = true;
@@ -1896,6 +1928,9 @@ crava_status crava_serve_submit(crava_server* sv, const crava_job_desc* desc, co
   if (s) return s;
   if (desc->prior_mode != CRAVA_PRIOR_SEPARABLE || (desc->flags & (CRAVA_FLAG_HOST_NOISE | CRAVA_FLAG_NONCONST_THICK)))
     return fail(CRAVA_ENOTSUP, "served jobs take the separable prior, device noise and constant thickness");
+  if (sv->ctx->budget > 0 && footprint(desc) > sv->ctx->budget)
+    return fail(CRAVA_ENOMEM, "job footprint " + std::to_string(footprint(desc)) + " bytes exceeds the context budget " +
+                                  std::to_string(sv->ctx->budget));
   ServeReq* r = new ServeReq();
   r->d = *desc;
   const int nth = desc->ntheta;

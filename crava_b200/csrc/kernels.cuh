@@ -70,8 +70,10 @@ struct ZParams {
   double ecd[kMaxTheta][kMaxTheta];
   double edd[kMaxTheta];
   unsigned long long* counters;    // [0] inverted bins [1] chol fallbacks [2] zero sim bins
-                                   // [3] bins re-factorised in FP64
+                                   // [3] bins re-factorised in FP64 [4] pencil tiles whose
+                                   // input spectra are not finite
 };
+constexpr int kNumCounters = 5;
 
 constexpr int kMaxFacies = 16;
 struct FaciesPrior { float p[kMaxFacies]; };

@@ -543,6 +543,14 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     }
   }
 
+  // A NaN or Inf anywhere in a data or prior-mean grid reaches every bin through the three
+  // transforms, so one bin per tile tells whether the inputs were finite.
+  if (tid == 0 && P.counters) {
+    float s = 0.f;
+#pragma unroll
+    for (int g = 0; g < GIN; g++) s += fabsf(R[g * W].x) + fabsf(R[g * W].y);
+    if (!isfinite(s)) atomicAdd(P.counters + 4, 1ull);
+  }
   // ---- per-bin posterior (src/avoinversion.cpp:1016-1082)
   unsigned long long n_inv = 0, n_fail = 0, n_zero_bins = 0, n_fp64 = 0;
   for (int b = tid; b < TS; b += T) {

@@ -33,7 +33,9 @@ typedef enum {
   CRAVA_ENOMEM = 2,     /* device allocation failed or the HBM budget is exceeded */
   CRAVA_ECUDA = 3,      /* a CUDA runtime call failed (message in crava_last_error) */
   CRAVA_ETIMEDOUT = 4,  /* a bounded wait gave up                                  */
-  CRAVA_ENUMERIC = 5,   /* non-finite input detected                               */
+  CRAVA_ENUMERIC = 5,   /* non-finite input detected: a NaN or Inf in the job description
+                           (at crava_job_create) or in the data / prior-mean grids (reported
+                           by crava_job_counters after the run)                     */
   CRAVA_ENOTSUP = 6,    /* size or configuration outside what the kernels handle   */
   CRAVA_ESTATE = 7      /* call out of order (e.g. download before run)            */
 } crava_status;
@@ -127,6 +129,9 @@ typedef struct {
   long long sim_chol_zero;     /* realisation bins left at zero (simulate fallback) */
   long long fp64_bins;         /* bins re-factorised in FP64 (fp64_threshold > 0)   */
   float post_var0[9];          /* SeismicParametersHolder::updatePriorVar after the run */
+  long long nonfinite_tiles;   /* pencil tiles whose input spectra held a NaN or Inf: the
+                                  data or prior-mean grids were not finite; then
+                                  crava_job_counters returns CRAVA_ENUMERIC              */
 } crava_counters;
 
 /* Context on one device; hbm_budget = 0 means no limit beyond the device's memory. */
@@ -267,19 +272,21 @@ crava_status crava_serve_stop(crava_server* sv);
 
 /* One block, end to end, with no device allocation (no counterpart in the reference).
  *
- * For callers that cannot allocate device memory: code inside a CUDA stream capture that
- * forbids allocation, plugins in applications that own the device memory pool, loops that
- * cannot afford an allocation's implicit synchronisation.  All intermediates live in a
- * fixed array of CRAVA_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that
- * loads the library keeps until the process exits.  The caller passes device grids:
+ * For callers that cannot allocate device memory: plugins hosted by an application that
+ * owns the device memory pool and admits no other allocator, and loops that cannot afford
+ * the implicit device synchronisation of an allocation.  All intermediates live in a fixed
+ * array of CRAVA_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the
+ * library keeps until the process exits.  The caller passes device grids:
  *   d_in  : ntheta data grids, then the 3 prior mean grids (real, read only);
  *   d_out : 3 posterior mean, 6 posterior covariance, 3*nsim realisations (real).
  * Separable prior only, FP32 only (fp64_threshold 0); no host noise, no residual or
- * spectral covariance output.  Blocks whose intermediates
- * exceed the array return CRAVA_ENOTSUP.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress), so make that call before any stream
- * capture.  Every call shares the array: calls whose work overlaps on the GPU (other
- * streams, other threads) race; serialise them on one stream. */
+ * spectral covariance output; the per-job counters are not reported.  Blocks whose
+ * intermediates exceed the array return CRAVA_ENOTSUP.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress).  The small per-kz and twiddle
+ * tables are built on the host and copied into the array on `stream` from pageable host
+ * memory, so the call returns after those copies have left the host buffers.  Every call
+ * shares the array: calls whose work overlaps on the GPU (other streams, other threads)
+ * race; serialise them on one stream. */
 #define CRAVA_NOALLOC_SCRATCH_BYTES (64u << 20)
 crava_status crava_invert_noalloc(const crava_job_desc* desc, const float* const* d_in, float* const* d_out,
                                   void* stream);

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own FP32 numerics.
 
-    python tests/golden/make_golden.py          (needs oracle/_ref/libref32.so, built by
-                                                 `make -C oracle` from the reference tree)
+    python tests/golden/make_golden.py [name ...]   (needs oracle/_ref/libref32.so, built by
+                                                     `make -C oracle` from the reference tree)
 
 Each fixture holds one small block's inputs (the synth.Block arrays), the reference-path
 outputs computed by oracle/_ref (FFTW 2.1.2 float + lib_matr.c with the restated loops):
@@ -33,6 +33,12 @@ CASES = {
                          seed=9, corr_grad_i=0.3, corr_grad_j=-0.2),
     "g5_one_angle_wideband": dict(nx=10, ny=8, nz=24, theta_deg=(20.0,), peak_hz=(40.0,), sn=(8.0,), nsim=1, seed=10,
                                   low_cut=1.0, high_cut=200.0),
+    # the production block's z length, angle stacks and realisations (540x540x256 workload:
+    # 5 angles 5..45 deg, Ricker 25..35 Hz, nzp 256, 4 realisations) on a 6x4 lateral window,
+    # so the pencil pass runs the same instantiation as on the full block
+    "g6_production_pencil": dict(nx=6, ny=4, nz=256, theta_deg=(5.0, 15.0, 25.0, 35.0, 45.0),
+                                 peak_hz=(25.0, 27.5, 30.0, 32.5, 35.0), sn=(5.0,) * 5, lateral_range=2000.0,
+                                 angular=("spherical", 20.0), nsim=4, seed=21),
 }
 
 SCALARS = ["nx", "ny", "nz", "nxp", "nyp", "nzp", "lz", "low_int_cut", "low_cut", "high_cut", "wnc",
@@ -80,9 +86,12 @@ def make_thick(name, kw, surface_seed):
 if __name__ == "__main__":
     if not ob.ref32_available():
         sys.exit("oracle/_ref/libref32.so missing: run `make -C oracle` with the reference tree present")
+    only = set(sys.argv[1:])   # optional fixture names; all of them by default
     for name, kw in CASES.items():
-        make(name, kw)
-        print("wrote", name)
+        if not only or name in only:
+            make(name, kw)
+            print("wrote", name)
     for name, (kw, sseed) in THICK_CASES.items():
-        make_thick(name, kw, sseed)
-        print("wrote", name)
+        if not only or name in only:
+            make_thick(name, kw, sseed)
+            print("wrote", name)

@@ -110,3 +110,22 @@ def test_host_layer_built_and_exports_the_reference_entry_points():
                  "crava_b200::AVOInversion::simulate(", "crava_b200::FFTGrid::getNextComplex()",
                  "crava_b200::FFTGrid::setRealValue("):
         assert name in syms, name
+
+
+@pytest.mark.parametrize("array", ["A", "err_theta_cov", "prior_var0", "wavelet", "corr_xy", "circ_corr_t"])
+def test_non_finite_description_rejected_as_numeric(small, array):
+    """A NaN in any of the description's host arrays is reported as CRAVA_ENUMERIC before
+    anything reaches a device (a job whose prior or wavelets are not finite would spread NaN
+    through every bin of the block)."""
+    blk = small
+    src = {"A": blk.A, "err_theta_cov": blk.err_theta_cov, "prior_var0": blk.prior_var0,
+           "wavelet": blk.wavelet, "corr_xy": blk.corr_xy, "circ_corr_t": blk.circ_corr_t}[array]
+    bad = np.array(src, copy=True)
+    bad.flat[bad.size // 2] = np.nan
+    d, keep = api.make_desc(blk)
+    ptype = ctypes.POINTER(ctypes.c_double if bad.dtype == np.float64 else ctypes.c_float)
+    bad = np.ascontiguousarray(bad)
+    setattr(d, array, bad.ctypes.data_as(ptype))
+    out = ctypes.c_size_t()
+    assert api.lib().crava_job_footprint(ctypes.byref(d), ctypes.byref(out)) == api.ENUMERIC
+    assert b"non-finite" in api.lib().crava_last_error()

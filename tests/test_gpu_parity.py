@@ -225,3 +225,78 @@ def test_against_reference_fixtures(ctx, name):
             assert crel(sep["mean"][a][..., :nx], z["ref_mean"][a][..., :nx]) < TOL_MEAN
         for q in range(6):
             assert crel(sep["cov"][q][..., :nx], z["ref_cov"][q][..., :nx]) < TOL_COV
+
+
+# ------------------------------------------------------------------ the production workload's instantiation
+
+def _production_block(nx, ny):
+    """The 540x540x256 workload (5 angles 5..45 deg, Ricker 25..35 Hz, nzp 256, 4 realisations,
+    separable prior) on a lateral window whose long side keeps the 540-point transform."""
+    spec = synth.config1(seed=21)
+    spec.nx, spec.ny = nx, ny
+    return synth.make_block(spec)
+
+
+@pytest.mark.parametrize("lateral", [(540, 12), (12, 540)])
+def test_production_instantiation_against_fp64_oracle(ctx, lateral):
+    """Same pencil-pass instantiation as the full 540x540x256 block (5 angle stacks, nzp 256
+    through the 16x16 four-step z split, 4 realisations in two batches of two) and the 540-point
+    row (x) or column (y) transforms, with the reference RandomGen noise (parity mode):
+    posterior mean 1e-4, covariance 1e-3, realisations 1e-4, residual spectra 1e-3."""
+    blk = _production_block(*lateral)
+    post = ref64.posterior(blk)
+    noise = ob.sim_noise(17, blk.nsim, blk.nxp, blk.nyp, blk.nzp)
+    out = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=noise, keep_residual=True)
+    _check_posterior(blk, out, post, post.n_inverted)
+    for l in range(blk.ntheta):
+        assert crel(out["resid_spec"][l], post.resid_spec[l]) < 1e-3, ("resid", l)
+    for s in range(blk.nsim):
+        sim = ref64.simulate(blk, post, noise[s])
+        for a in range(3):
+            assert crel(out["sims"][s, a][..., :blk.nxp], sim[a][..., :blk.nxp]) < TOL_SIM, (s, a)
+
+
+def test_production_instantiation_device_noise_statistics(ctx):
+    """Product-mode noise on the production instantiation: per voxel, each realisation's
+    deviation from the posterior mean has the posterior variance (covariance at lag 0), and
+    the mean and covariance match the FP64 oracle as in parity mode."""
+    blk = _production_block(540, 12)
+    post = ref64.posterior(blk)
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=99)
+    _keep = job.upload_block()
+    job.run()
+    out = job.download_outputs()
+    c = job.counters()
+    job.close()
+    nx = blk.nxp
+    assert c["inverted_bins"] == post.n_inverted
+    for a in range(3):
+        assert crel(out["mean"][a][..., :nx], post.mean[a][..., :nx]) < TOL_MEAN
+    for q in range(6):
+        assert crel(out["cov"][q][..., :nx], post.cov[q][..., :nx]) < TOL_COV
+    dev = out["sims"][..., :nx] - out["mean"][None, ..., :nx]
+    for a in range(3):
+        emp = float(np.mean(dev[:, a].astype(np.float64) ** 2))
+        assert 0.85 < emp / post.cov[a, 0, 0, 0] < 1.15, (a, emp, post.cov[a, 0, 0, 0])
+
+
+@pytest.mark.parametrize("grid", ["data", "mean"])
+def test_non_finite_grid_reported_as_numeric(ctx, grid):
+    """A single NaN voxel in a data or prior-mean grid: the run completes, and the counters
+    call reports CRAVA_ENUMERIC (the NaN reaches every bin through the transforms)."""
+    blk = synth.make_block(synth.BlockSpec(nx=16, ny=12, nz=20, nsim=1, seed=3))
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=5)
+    _keep = job.upload_block()
+    g = np.array((blk.data[1] if grid == "data" else blk.mean[2]), copy=True)
+    g[7, 5, 3] = np.nan
+    _keep.append(job.upload(api.ROLE_DATA if grid == "data" else api.ROLE_MEAN, 1 if grid == "data" else 2, g))
+    job.run()
+    with pytest.raises(api.CravaError) as ei:
+        job.counters()
+    assert ei.value.status == api.ENUMERIC
+    # the same job with finite inputs runs clean again
+    _keep.append(job.upload(api.ROLE_DATA if grid == "data" else api.ROLE_MEAN, 1 if grid == "data" else 2,
+                            blk.data[1] if grid == "data" else blk.mean[2]))
+    job.run()
+    assert job.counters()["nonfinite_tiles"] == 0
+    job.close()

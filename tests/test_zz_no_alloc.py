@@ -1,10 +1,11 @@
 """crava_invert_noalloc: the inversion entry point that allocates no device memory.
 
-It exists for callers that cannot allocate device memory (inside a stream capture that
-forbids allocation, inside an application that owns the device memory pool).  Its
+It exists for callers that cannot allocate device memory (a plugin inside an application
+that owns the device memory pool and admits no other allocator).  Its
 intermediates live in a fixed array inside the library; this test calls it through the
 C ABI twice in a row on the same block and checks each call against the ordinary job
-entry point (crava_job_create / crava_job_run) with the tolerances of the parity tests:
+entry point (crava_job_create / crava_job_run), and the posterior mean and covariance
+against the FP64 oracle, with the tolerances of the parity tests:
 posterior mean 1e-4, covariance 1e-3, realisations 1e-4 (norm-wise relative).  The file
 sorts last so that a run stopping at the first failure has already run every other test.
 """
@@ -72,6 +73,14 @@ def test_noalloc_matches_job_entry_point_twice():
     # inputs are read only
     for l in range(blk.ntheta):
         assert np.array_equal(d_in[l].cpu().numpy(), blk.data[l])
+    # and the posterior itself against the FP64 oracle (realisations use device noise, so
+    # they are checked against the job entry point above only)
+    from oracle import ref64
+    post = ref64.posterior(blk)
+    for a in range(3):
+        assert rel(got[a][..., :nx], post.mean[a][..., :nx]) < TOL["mean"], ("oracle mean", a)
+    for q in range(6):
+        assert rel(got[3 + q][..., :nx], post.cov[q][..., :nx]) < TOL["cov"], ("oracle cov", q)
     ctx.close()
 
 
