@@ -177,7 +177,7 @@ def reference_main(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref32.so was not built (reference tree absent at build time)"}))
         return
     ncores = os.cpu_count() or 1
-    nproc = max(1, min(16, ncores // 2))
+    nproc = max(1, min(64, ncores))
     vals = run_cpu_sample(nproc=nproc, steps=args.steps, warmup=args.warmup)
     v = statistics.median(vals)
     smp = sample_spec()
@@ -260,6 +260,18 @@ def batched_leg(ctx, torch, n_blocks=64, nsim=16, reps=3, branches=16):
     e1.record(st)
     torch.cuda.synchronize()
     t_plain = e0.elapsed_time(e1) / 1000.0
+    # the ceiling of any batching: the plain path's wall time against the device time of its
+    # kernels (per-launch CUDA events); a plain path whose wall time is mostly kernel time
+    # leaves batching little to gain
+    ctx.set_profiling(True)
+    ctx.kernel_times(reset=True)
+    for j in jobs:
+        j.run(sh)
+        st.synchronize()
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times(reset=True)
+    ctx.set_profiling(False)
+    t_kernels = sum(v[0] for v in kt.values()) / 1000.0
     bt = api.Batch(ctx, jobs, branches=branches)
     bt.run(sh)
     torch.cuda.synchronize()
@@ -278,7 +290,52 @@ def batched_leg(ctx, torch, n_blocks=64, nsim=16, reps=3, branches=16):
                         f"{nsim} realisations, separable prior, white-noise seismic of seismic amplitude",
             "voxels": vox, "voxels_per_s": vox / t_b, "jobs_per_s": n_blocks / t_b, "ms_per_batch": 1000 * t_b,
             "plain_voxels_per_s": vox / t_plain, "plain_jobs_per_s": n_blocks / t_plain,
-            "speedup_vs_plain": t_plain / t_b, "branches": branches, "gpu_launches_per_batch": launches}
+            "speedup_vs_plain": t_plain / t_b, "branches": branches, "gpu_launches_per_batch": launches,
+            "plain_kernel_ms_sum": 1000 * t_kernels, "plain_wall_ms": 1000 * t_plain,
+            "plain_gpu_busy": t_kernels / t_plain,
+            "speedup_ceiling": t_plain / t_kernels,
+            "ceiling_note": "plain wall time / sum of its kernel times: batching can remove host gaps and "
+                            "overlap launch tails, not kernel work"}
+
+
+def cfg3_leg(torch, steps, warmup):
+    """The precision-study block 768x768x320 (6 angles 5..50 deg, band 2..120 Hz, S/N 2..10,
+    1 realisation): ms per job on resident inputs and its job roofline
+    B_alg = 12 N (G_in + G_out) = 12 * 188,743,680 * (9 + 12) bytes = 47.56 GB."""
+    from crava_b200 import api, synth
+    blk = synth.make_block_fast(synth.config3())
+    ctx = api.Context(torch.cuda.current_device())
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=3000)
+    keep = job.upload_block()
+    st = torch.cuda.current_stream()
+    sh = st.cuda_stream
+    for _ in range(warmup):
+        job.run(sh)
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.kernel_times(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        job.run(sh)
+    e1.record(st)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times(reset=True)
+    ctx.set_profiling(False)
+    ms = e0.elapsed_time(e1) / steps
+    peak, peak_kind = peaks()
+    nin, nout = blk.ntheta + 3, 9 + 3 * job.nsim
+    B_alg = 12 * blk.n_voxels * (nin + nout)
+    del keep
+    job.close()
+    ctx.close()
+    return {"workload": f"single block {blk.nx}x{blk.ny}x{blk.nz}, {blk.ntheta} angles 5..50 deg, band 2..120 Hz, "
+                        f"S/N 2..10, {job.nsim} realisation, separable prior; inputs white noise of seismic amplitude",
+            "steps": steps, "warmup": warmup, "ms_per_job": ms, "voxels_per_s": blk.n_voxels / (ms / 1000.0),
+            "job_roofline": {"alg_bytes": B_alg, "achieved_gbs": B_alg / (ms / 1000.0) / 1e9,
+                             "frac": B_alg / (ms / 1000.0) / 1e9 / peak, "peak_gbs": peak, "peak_kind": peak_kind,
+                             "target_frac": 0.6, "target_ms": B_alg / (0.6 * peak * 1e9) * 1000.0},
+            "kernel_ms_per_job": {c: kt[c][0] / steps for c in kt if kt[c][1]}}
 
 
 def served_leg(torch, n_jobs=48, distinct=8, rate=20.0, nsim=16, max_inflight=8, budget_gb=120):
@@ -549,8 +606,9 @@ def main():
 
     job.close()
     job2.close()
-    batched = served = None
+    batched = served = cfg3 = None
     if rank == 0 and not args.no_legs and not args.dims:
+        cfg3 = cfg3_leg(torch, steps=max(3, min(args.steps, 10)), warmup=max(3, args.warmup))
         batched = batched_leg(ctx, torch)
         served = served_leg(torch)
     clocks = summarize_clocks(clk_path, physical_gpu_index(local_rank))
@@ -582,6 +640,7 @@ def main():
             "kernel_share": share,
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "config3": cfg3,
             "batched": batched,
             "served": served,
         }

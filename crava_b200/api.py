@@ -124,6 +124,10 @@ def lib() -> ctypes.CDLL:
     L.crava_facies_smooth.argtypes = [vp, ctypes.POINTER(FaciesDesc), ctypes.POINTER(ctypes.c_double), vp, vp]
     L.crava_facies_prob.argtypes = [vp, ctypes.POINTER(FaciesDesc), vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
+    L.crava_tuning_set.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    L.crava_tuning_get.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.crava_tuning_load.argtypes = [ctypes.c_char_p]
+    L.crava_tuning_path.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -132,6 +136,31 @@ def _check(status: int):
     if status != OK:
         L = lib()
         raise CravaError(status, (L.crava_last_error() or b"").decode())
+
+
+def tuning_set(key: str, n: int, value: int):
+    """Override one schedule entry for this process (value < 0 removes it)."""
+    _check(lib().crava_tuning_set(key.encode(), int(n), int(value)))
+
+
+def tuning_get(key: str, n: int) -> int:
+    """The schedule value a launch would use (-1: the built-in default)."""
+    v = ctypes.c_int()
+    _check(lib().crava_tuning_get(key.encode(), int(n), ctypes.byref(v)))
+    return v.value
+
+
+def tuning_load(path: str):
+    _check(lib().crava_tuning_load(str(path).encode()))
+
+
+def tuning_path() -> str:
+    return (lib().crava_tuning_path() or b"").decode()
+
+
+def pencil_key(nzp: int, ntheta: int) -> int:
+    """Size key of the pencil-pass schedule entries."""
+    return nzp * 16 + ntheta
 
 
 class Context:

@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrava_gpu.so")
-SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "facies.cu", "thick.cu", "prior.cu"]
-HEADERS = ["fft_core.cuh", "fft2.cuh", "kernels.cuh"]
+SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "zpass.cu", "pencil.cu", "facies.cu", "thick.cu", "prior.cu"]
+HEADERS = ["fft_core.cuh", "fft2.cuh", "kernels.cuh", "pencil_common.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -58,7 +58,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                 sys.stderr.write(r.stderr)
             objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+    cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-ldl"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -88,6 +88,64 @@ struct Plan {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------------------
+// Schedule table (kernels.cuh `tuned`): "key n value" lines of the schedule file, loaded
+// once per process from CRAVA_SCHEDULES or else schedules.txt beside this library, and
+// entries set through crava_tuning_set.
+
+#include <dlfcn.h>
+#include <fstream>
+#include <sstream>
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::pair<std::string, int>, int> g_tune;
+bool g_tune_loaded = false;
+std::string g_tune_path;
+
+bool tune_parse(const std::string& path, std::map<std::pair<std::string, int>, int>& out) {
+  std::ifstream f(path);
+  if (!f) return false;
+  std::string line;
+  while (std::getline(f, line)) {
+    const size_t h = line.find('#');
+    if (h != std::string::npos) line.resize(h);
+    std::istringstream is(line);
+    std::string key;
+    long long n, v;
+    if (is >> key >> n >> v) out[{key, (int)n}] = (int)v;
+  }
+  return true;
+}
+
+void tune_load_default_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  std::string path;
+  if (const char* ev = getenv("CRAVA_SCHEDULES")) path = ev;
+  else {
+    Dl_info info;
+    if (dladdr((void*)&tune_parse, &info) && info.dli_fname) {
+      path = info.dli_fname;
+      const size_t sl = path.rfind('/');
+      path = (sl == std::string::npos ? std::string(".") : path.substr(0, sl)) + "/schedules.txt";
+    }
+  }
+  if (!path.empty() && tune_parse(path, g_tune)) g_tune_path = path;
+}
+}  // namespace
+
+namespace crava {
+int tuned(const char* key, int n, int fallback) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_default_locked();
+  auto it = g_tune.find({key, n});
+  if (it != g_tune.end()) return it->second;
+  it = g_tune.find({key, -1});
+  return it != g_tune.end() ? it->second : fallback;
+}
+}  // namespace crava
+
 // Per-kernel-class CUDA-event timing (off unless crava_ctx_set_profiling enables it).
 enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_XY_FWD = 5, KT_XY_INV = 6,
        KT_THICK_DIVIDE = 7, KT_THICK_FILL = 8, KT_COUNT = 9 };
@@ -162,6 +220,10 @@ struct crava_job {
   uint8_t* inv = nullptr;
   float2* cxy = nullptr;     // SEPARABLE
   float2* ct = nullptr;
+  float4* eig = nullptr;     // SEPARABLE: eigen tables of the in-place pencil kernel (pencil.cu)
+  bool eig_ok = false;       //   built and applicable: crava_job_run launches k_pencil
+  int n_inv_rows = 0;        //   inverted kz
+  std::string eig_why;       //   why the general kernel runs instead
   float* cxy_grid = nullptr; // staging for the corr_xy transform
   unsigned long long* counters = nullptr;
   // CRAVA_FLAG_NONCONST_THICK: per-kz diagonal error terms, the data pre-processing
@@ -293,6 +355,8 @@ size_t thick_bytes(const crava_job_desc* d) {
          align256(sizeof(TraceOp) * nth * nxy) + align256(sizeof(int) * kMaxTheta);
 }
 
+size_t eig_table_bytes(const crava_job_desc* d);
+
 size_t footprint(const crava_job_desc* d) {
   size_t cnxp = d->nxp / 2 + 1;
   size_t gb = align256(sizeof(float) * 2 * cnxp * d->nyp * d->nzp);
@@ -305,7 +369,7 @@ size_t footprint(const crava_job_desc* d) {
                   align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float2) * d->nzp) +
                   align256(sizeof(float) * 2 * cnxp * d->nyp) + 256 + align256(sizeof(float) * d->nzp * d->ntheta) +
                   align256(sizeof(double) * d->nzp * d->ntheta);
-  return ngrids * gb + tables + thick_bytes(d);
+  return ngrids * gb + tables + thick_bytes(d) + eig_table_bytes(d);
 }
 
 // DFT of a real vector in double precision, e^{-2 pi i k t / n}.
@@ -458,6 +522,172 @@ void build_kz_tables(const crava_job_desc& d, std::vector<float2>& kw, std::vect
     float rf = static_cast<float>((d.nz * 1000.0f) / (d.lz * n) * kk);
     inv[k] = (rf > d.low_cut * d.min_rel_thick && rf < d.high_cut) ? 1 : 0;
   }
+}
+
+// Four-step split of a z length that the in-place pencil kernels handle (kernels.cuh
+// ZParams.zsplit): 1 16x16, 2 20x16, 3 16x8; 0 for the other lengths.
+int zsplit_of(int nzp) { return nzp == 256 ? 1 : nzp == 320 ? 2 : nzp == 128 ? 3 : 0; }
+int zsplit_n1(int zs) { return zs == 1 ? 16 : zs == 2 ? 20 : zs == 3 ? 16 : 0; }
+int zsplit_n2(int zs) { return zs == 1 ? 16 : zs == 2 ? 16 : zs == 3 ? 8 : 0; }
+
+// Eigen tables of a separable-prior job: bytes on the device (0 when no split applies).
+size_t eig_table_bytes(const crava_job_desc* d) {
+  if (d->prior_mode != CRAVA_PRIOR_SEPARABLE || !zsplit_of(d->nzp)) return 0;
+  return align256(sizeof(float) * (size_t)EigLayout(d->ntheta).floats * d->nzp);
+}
+
+// Hermitian eigen-decomposition A = U diag(lam) U^H of a small matrix (n <= 8) by cyclic
+// Jacobi rotations in double (Jacobi's method with a phase per rotation that makes the
+// pivot real).  A is overwritten; the columns of U are the eigenvectors.
+void herm_eig(int n, cd (&A)[kMaxTheta][kMaxTheta], double (&lam)[kMaxTheta], cd (&U)[kMaxTheta][kMaxTheta]) {
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < n; k++) U[i][k] = i == k ? cd(1, 0) : cd(0, 0);
+  for (int sweep = 0; sweep < 64; sweep++) {
+    double off = 0, diag = 0;
+    for (int i = 0; i < n; i++) {
+      diag += std::norm(A[i][i]);
+      for (int k = i + 1; k < n; k++) off += std::norm(A[i][k]);
+    }
+    if (off <= 1e-32 * diag || off == 0.0) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = std::abs(A[p][q]);
+        if (apq == 0.0) continue;
+        const cd ph = A[p][q] / apq;                   // A_pq = |A_pq| ph
+        const double theta = (A[q][q].real() - A[p][p].real()) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        // G = D R: D = diag(.., conj(ph) at q) makes the pivot real, R the real rotation
+        const cd gpp = c, gpq = sn, gqp = -sn * std::conj(ph), gqq = c * std::conj(ph);
+        for (int k = 0; k < n; k++) {   // A G, U G
+          const cd akp = A[k][p], akq = A[k][q];
+          A[k][p] = akp * gpp + akq * gqp;
+          A[k][q] = akp * gpq + akq * gqq;
+          const cd ukp = U[k][p], ukq = U[k][q];
+          U[k][p] = ukp * gpp + ukq * gqp;
+          U[k][q] = ukp * gpq + ukq * gqq;
+        }
+        for (int k = 0; k < n; k++) {   // G^H (A G)
+          const cd apk = A[p][k], aqk = A[q][k];
+          A[p][k] = std::conj(gpp) * apk + std::conj(gqp) * aqk;
+          A[q][k] = std::conj(gpq) * apk + std::conj(gqq) * aqk;
+        }
+        A[p][q] = A[q][p] = cd(0, 0);
+        A[p][p] = cd(A[p][p].real(), 0);
+        A[q][q] = cd(A[q][q].real(), 0);
+      }
+  }
+  for (int i = 0; i < n; i++) lam[i] = A[i][i].real();
+}
+
+// Job constants of the separable posterior in the float values the pencil kernels use:
+// AP = A P0 (ntheta x 3) and G0 = A P0 A^T.
+void sep_constants(const std::vector<double>& A, const std::vector<double>& pv, int nth,
+                   float (&G0)[kMaxTheta][kMaxTheta], float (&AP)[kMaxTheta][3]) {
+  for (int l = 0; l < nth; l++) {
+    double ap[3] = {0, 0, 0};
+    for (int c = 0; c < 3; c++)
+      for (int b = 0; b < 3; b++) ap[c] += A[l * 3 + b] * pv[b * 3 + c];
+    for (int c = 0; c < 3; c++) AP[l][c] = (float)ap[c];
+    for (int m = 0; m < nth; m++) {
+      double g = 0;
+      for (int c = 0; c < 3; c++) g += ap[c] * A[m * 3 + c];
+      G0[l][m] = (float)g;
+    }
+  }
+}
+
+// Tables of the eigen form of the separable posterior (pencil.cu), one row per z position
+// in the order the in-place four-step transform leaves the spectrum in (position
+// k1 + N2 k2 holds kz = k2 + N1 k1), float4 group g of position p at rows[4 (g nzp + p)].
+// Per inverted kz, from the float values the general kernel uses (kw, M2 = the septab
+// lower triangle, ed, |ct|, G0 = A P0 A^T, AP = A P0):
+//   M = |ct| (kw kw^H) o G0 + M2,  E = diag(ed),  E^-1/2 M E^-1/2 = U diag(Lam) U^H,
+//   V = U^H E^-1/2,  Q = |ct| V diag(kw) AP,  H_l = conj(Q_la) Q_lb.
+// Rows of kz outside the inversion band are zero (prior kept, residual = data).  Returns
+// false with the reason when the form does not apply: some ed <= 0, an eigenvalue of M
+// clearly negative, or a reference Cholesky of Sd that could reach its 1e-20 pivot test
+// (pivots of Sd >= min ed; Sd_00 <= lam_max M_00 + ed_0, lam_max <= sum |corrXY|).
+bool build_eig_tables(const crava_job_desc& d, const std::vector<float2>& kw, const std::vector<float2>& sep,
+                      const std::vector<float>& edk, const std::vector<uint8_t>& inv, const std::vector<float2>& ct,
+                      const float (&G0)[kMaxTheta][kMaxTheta], const float (&AP)[kMaxTheta][3], double lam_max,
+                      std::vector<float>& rows, int& n_inv_rows, std::string& why) {
+  const int n = d.ntheta, nzp = d.nzp, zs = zsplit_of(nzp);
+  const int N1 = zsplit_n1(zs), N2 = zsplit_n2(zs);
+  const EigLayout L(n);
+  const int G4 = L.floats / 4;
+  rows.assign((size_t)L.floats * nzp, 0.f);
+  n_inv_rows = 0;
+  const int tri = n * (n + 1) / 2;
+  for (int p = 0; p < nzp; p++) {
+    const int kz = p / N2 + N1 * (p % N2);
+    if (!inv[kz]) continue;
+    n_inv_rows++;
+    double row[4 * 96] = {};
+    const double cta = std::fabs((double)ct[kz].x);
+    cd kwv[kMaxTheta];
+    double e[kMaxTheta];
+    for (int l = 0; l < n; l++) {
+      kwv[l] = cd(kw[(size_t)kz * n + l].x, kw[(size_t)kz * n + l].y);
+      e[l] = edk[(size_t)kz * n + l];
+      if (!(e[l] > 0)) { why = "white-noise error term not positive"; return false; }
+    }
+    cd M[kMaxTheta][kMaxTheta], U[kMaxTheta][kMaxTheta];
+    for (int l = 0; l < n; l++)
+      for (int m = 0; m <= l; m++) {
+        const float2 b = sep[(size_t)kz * tri + l * (l + 1) / 2 + m];
+        const cd v = cta * (double)G0[l][m] * kwv[l] * std::conj(kwv[m]) + cd(b.x, b.y);
+        M[l][m] = v;
+        M[m][l] = std::conj(v);
+      }
+    const double m00 = M[0][0].real();
+    double emin = e[0];
+    for (int l = 1; l < n; l++) emin = std::min(emin, e[l]);
+    if (!(emin > 1e-18 * (lam_max * m00 + e[0]))) { why = "data covariance too close to singular"; return false; }
+    for (int l = 0; l < n; l++)
+      for (int m = 0; m < n; m++) M[l][m] /= std::sqrt(e[l] * e[m]);
+    double lam[kMaxTheta];
+    herm_eig(n, M, lam, U);
+    double lmax = 0;
+    for (int l = 0; l < n; l++) lmax = std::max(lmax, std::fabs(lam[l]));
+    for (int l = 0; l < n; l++) {
+      // float rounding of the rank-deficient parts leaves eigenvalues of order -1e-7 lmax:
+      // those are zero; a clearly negative one means M is not a covariance
+      if (lam[l] < -1e-4 * lmax) { why = "prior part of the data covariance not positive semidefinite"; return false; }
+      lam[l] = std::max(lam[l], 0.0);
+    }
+    cd V[kMaxTheta][kMaxTheta], Q[kMaxTheta][3];
+    for (int l = 0; l < n; l++)
+      for (int m = 0; m < n; m++) V[l][m] = std::conj(U[m][l]) / std::sqrt(e[m]);
+    for (int l = 0; l < n; l++)
+      for (int a = 0; a < 3; a++) {
+        cd acc = 0;
+        for (int m = 0; m < n; m++) acc += V[l][m] * kwv[m] * (double)AP[m][a];
+        Q[l][a] = cta * acc;
+      }
+    for (int l = 0; l < n; l++) {
+      row[L.kw + 2 * l] = kwv[l].real();
+      row[L.kw + 2 * l + 1] = kwv[l].imag();
+      row[L.lam + l] = lam[l];
+      double* r = row + L.rows + l * L.rs;   // V row l, then Q_l (6) and H_l (9)
+      for (int m = 0; m < n; m++) {
+        r[2 * m] = V[l][m].real();
+        r[2 * m + 1] = V[l][m].imag();
+      }
+      for (int a = 0; a < 3; a++) {
+        r[L.vpad + 2 * a] = Q[l][a].real();
+        r[L.vpad + 2 * a + 1] = Q[l][a].imag();
+      }
+      const cd h01 = std::conj(Q[l][0]) * Q[l][1], h02 = std::conj(Q[l][0]) * Q[l][2],
+               h12 = std::conj(Q[l][1]) * Q[l][2];
+      const double h[9] = {std::norm(Q[l][0]), std::norm(Q[l][1]), std::norm(Q[l][2]), h01.real(), h01.imag(),
+                           h02.real(), h02.imag(), h12.real(), h12.imag()};
+      for (int c = 0; c < 9; c++) r[L.vpad + 6 + c] = h[c];
+    }
+    for (int g = 0; g < G4; g++)
+      for (int c = 0; c < 4; c++) rows[4 * ((size_t)g * nzp + p) + c] = (float)row[4 * g + c];
+  }
+  return true;
 }
 
 // Host tables of the data pre-processing of one job (computeAdjustmentFactor,
@@ -714,6 +944,38 @@ const char* crava_status_string(crava_status s) {
   return "unknown status";
 }
 
+crava_status crava_tuning_set(const char* key, int n, int value) {
+  if (!key || !*key) return fail(CRAVA_EINVAL, "null schedule key");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_default_locked();
+  if (value < 0) g_tune.erase({key, n});
+  else g_tune[{key, n}] = value;
+  return CRAVA_OK;
+}
+
+crava_status crava_tuning_get(const char* key, int n, int* value) {
+  if (!key || !value) return fail(CRAVA_EINVAL, "null argument");
+  *value = crava::tuned(key, n, -1);
+  return CRAVA_OK;
+}
+
+crava_status crava_tuning_load(const char* path) {
+  if (!path) return fail(CRAVA_EINVAL, "null path");
+  std::map<std::pair<std::string, int>, int> t;
+  if (!tune_parse(path, t)) return fail(CRAVA_EINVAL, std::string("cannot read schedule file ") + path);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_loaded = true;
+  g_tune.swap(t);
+  g_tune_path = path;
+  return CRAVA_OK;
+}
+
+const char* crava_tuning_path(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_default_locked();
+  return g_tune_path.c_str();
+}
+
 crava_status crava_ctx_create(crava_ctx** ctx, int device, size_t hbm_budget) {
   if (!ctx) return fail(CRAVA_EINVAL, "null ctx");
   int n = 0;
@@ -886,6 +1148,7 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->ct = (float2*)take(sizeof(float2) * d.nzp);
   j->cxy_grid = (float*)take(sizeof(float) * j->rnxp * d.nyp);
   j->counters = (unsigned long long*)take(256);
+  if (eig_table_bytes(&d)) j->eig = (float4*)take(eig_table_bytes(&d));
   ThickTables tt;
   const bool nonconst = (d.flags & CRAVA_FLAG_NONCONST_THICK) != 0;
   j->edk = (float*)take(sizeof(float) * d.nzp * d.ntheta);
@@ -913,9 +1176,9 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     tp.rnxp = j->rnxp;
     tp.cnzp = (int)cn;
     tp.W = thick_tile_width(d.nzp);
-    if (const char* ev = getenv("CRAVA_THICK_W")) {
+    if (const int tw = tuned("thick_w", d.nzp, 0)) {
       int w = 1;
-      while (w * 2 <= std::min(16, atoi(ev))) w *= 2;
+      while (w * 2 <= std::min(16, tw)) w *= 2;
       if (thick_smem_bytes(w, d.nzp) <= 227 * 1024) tp.W = w;
     }
     tp.logW = 0;
@@ -999,12 +1262,30 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
         }
     }
     JOB_TRY(cudaMemcpyAsync(j->septab, sep.data(), sizeof(float2) * sep.size(), cudaMemcpyHostToDevice, st));
-    // temporal factor: DFT of circCorrT (1D, double)
+    // temporal factor: DFT of circCorrT (1D, double); a symmetric circular correlation (the
+    // form computeCircCorrT builds, src/seismicparametersholder.cpp:624-660) has a real
+    // spectrum, whose imaginary part is then exactly zero
     std::vector<double> c(j->circ.begin(), j->circ.end());
     std::vector<cd> C = dft(c);
+    bool sym = true;
+    for (int t = 1; t < d.nzp && sym; t++) sym = j->circ[t] == j->circ[d.nzp - t];
     std::vector<float2> ct(d.nzp);
-    for (int k = 0; k < d.nzp; k++) ct[k] = make_float2((float)C[k].real(), (float)C[k].imag());
+    for (int k = 0; k < d.nzp; k++) ct[k] = make_float2((float)C[k].real(), sym ? 0.f : (float)C[k].imag());
     JOB_TRY(cudaMemcpyAsync(j->ct, ct.data(), sizeof(float2) * d.nzp, cudaMemcpyHostToDevice, st));
+    // the eigen form of the per-bin posterior (pencil.cu) where it applies
+    if (!j->eig) j->eig_why = "z length without an in-place four-step split";
+    else if (!sym) j->eig_why = "circular temporal correlation not symmetric";
+    else if (d.fp64_threshold > 0.f) j->eig_why = "FP64 re-factorisation requested";
+    else {
+      float G0[kMaxTheta][kMaxTheta], AP[kMaxTheta][3];
+      sep_constants(j->A, j->pv, nth, G0, AP);
+      double lam_max = 0;
+      for (float v : j->corr_xy) lam_max += std::fabs((double)v);
+      std::vector<float> rows;
+      j->eig_ok = build_eig_tables(d, kw, sep, edk, inv, ct, G0, AP, lam_max, rows, j->n_inv_rows, j->eig_why);
+      if (j->eig_ok)
+        JOB_TRY(cudaMemcpyAsync(j->eig, rows.data(), sizeof(float) * rows.size(), cudaMemcpyHostToDevice, st));
+    }
     // lateral factor: 2D transform of corrXY on the device (x then y)
     std::vector<float> g((size_t)j->rnxp * d.nyp, 0.f);
     for (int jj = 0; jj < d.nyp; jj++)
@@ -1112,8 +1393,8 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   }
   // the fused pencil pass
   Plan* pz;
-  const char* r16 = getenv("CRAVA_ZPASS_R16");
-  if ((s = get_plan(ctx, d.nzp, &pz, !(r16 && r16[0] == '0')))) return s;
+  const int skey = d.nzp * 16 + d.ntheta;   // schedule key of the pencil pass
+  if ((s = get_plan(ctx, d.nzp, &pz, tuned("zpass_r16", d.nzp, 1) != 0))) return s;
   ZParams zp;
   std::memset(&zp, 0, sizeof(zp));
   zp.nxp = d.nxp; zp.nyp = d.nyp; zp.nzp = d.nzp; zp.cnxp = job->cnxp;
@@ -1134,20 +1415,19 @@ crava_status crava_job_run(crava_job* job, void* stream) {
       }
     }
   }
-  if (const char* ev = getenv("CRAVA_ZPASS_W")) W = std::max(1, atoi(ev));
-  if (const char* ev = getenv("CRAVA_ZPASS_GT")) GT = std::max(3, atoi(ev));
-  if (const char* ev = getenv("CRAVA_ZPASS_SB")) SB = std::max(1, atoi(ev));
+  W = std::max(1, tuned("zpass_w", skey, W));
+  GT = std::max(3, tuned("zpass_gt", skey, GT));
+  SB = std::max(1, tuned("zpass_sb", skey, SB));
   SB = std::min(SB, GT / 3);
   T = zpass_smem_bytes(W, d.nzp, d.ntheta, GT, SB) > 113 * 1024 ? 512 : 256;
-  if (const char* ev = getenv("CRAVA_ZPASS_T")) T = std::max(64, atoi(ev));
+  T = std::max(64, std::min(512, tuned("zpass_threads", skey, T) / 32 * 32));
   if (zpass_smem_bytes(W, d.nzp, d.ntheta, GT, SB) > 227 * 1024)
     return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
   zp.GT = GT;
   zp.SB = SB;
   zp.W = W;
   {
-    const char* ev = getenv("CRAVA_ZPASS_FOUR");
-    const bool four = !(ev && ev[0] == '0') && GT >= Gs;
+    const bool four = tuned("zpass_four", d.nzp, 1) != 0 && GT >= Gs;
     zp.zsplit = !four ? 0 : d.nzp == 256 ? 1 : d.nzp == 320 ? 2 : d.nzp == 128 ? 3 : 0;
   }
   zp.logW = 0;
@@ -1170,17 +1450,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.cxy = job->cxy;
   zp.ct = job->ct;
   zp.septab = grids ? nullptr : job->septab;
-  for (int l = 0; l < d.ntheta; l++) {
-    double ap[3] = {0, 0, 0};
-    for (int c = 0; c < 3; c++)
-      for (int b = 0; b < 3; b++) ap[c] += job->A[l * 3 + b] * job->pv[b * 3 + c];
-    for (int c = 0; c < 3; c++) zp.AP[l][c] = (float)ap[c];
-    for (int m = 0; m < d.ntheta; m++) {
-      double g = 0;
-      for (int c = 0; c < 3; c++) g += ap[c] * job->A[m * 3 + c];
-      zp.G0[l][m] = (float)g;
-    }
-  }
+  sep_constants(job->A, job->pv, d.ntheta, zp.G0, zp.AP);
   const int qa[6] = {0, 1, 2, 0, 0, 1}, qb[6] = {0, 1, 2, 1, 2, 2};
   for (int q = 0; q < 6; q++) zp.pv[q] = static_cast<float>(job->pv[qa[q] * 3 + qb[q]]);
   for (int l = 0; l < d.ntheta; l++) {
@@ -1204,7 +1474,32 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.seed = d.seed;
   zp.counters = job->counters;
   int nl = 0;
-  {
+  if (job->eig_ok && tuned("pencil_kernel", skey, 2) == 2) {
+    // eigen form: in-place z transforms, W x-bins per tile (schedule keys pencil_w,
+    // pencil_threads); by default two CTAs per SM where the tile's shared memory allows
+    int Wp = 1;
+    while (Wp * 2 <= std::min(16, tuned("pencil_w", skey, 4))) Wp *= 2;
+    int SBp = std::max(1, std::min(std::max(d.nsim, 1), tuned("pencil_sb", skey, 1)));
+    while (SBp > 1 && pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) > 227 * 1024) SBp--;
+    while (Wp > 1 && pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) > 227 * 1024) Wp /= 2;
+    if (pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) > 227 * 1024)
+      return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
+    zp.SB = SBp;
+    zp.dense = tuned("pencil_dense", skey, 0);
+    zp.eig = job->eig;
+    zp.n_inv_rows = job->n_inv_rows;
+    zp.zsplit = zsplit_of(d.nzp);
+    zp.W = Wp;
+    zp.logW = 0;
+    while ((1 << zp.logW) < Wp) zp.logW++;
+    zp.nIT = (job->cnxp + zp.W - 1) / zp.W;
+    const int Tp = std::max(32, std::min(512, tuned("pencil_threads", skey,
+                                                    pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) <= 113 * 1024 ? 256
+                                                                                                         : 512) /
+                                                   32 * 32));
+    ProfScope ps(ctx, KT_ZPASS, st);
+    CUDA_TRY(launch_pencil(zp, Tp, st, &nl));
+  } else {
     ProfScope ps(ctx, KT_ZPASS, st);
     CUDA_TRY(launch_zpass(zp, T, st, &nl));
   }
@@ -1648,8 +1943,7 @@ crava_status prewarm_plans(crava_ctx* ctx, const crava_job_desc& d) {
   if ((s = get_xplans(ctx, d.nxp, &a, &b))) return s;
   if ((s = get_plan(ctx, d.nyp, &a))) return s;
   if ((s = get_plan(ctx, d.nzp, &a))) return s;
-  const char* r16 = getenv("CRAVA_ZPASS_R16");
-  return get_plan(ctx, d.nzp, &a, !(r16 && r16[0] == '0'));
+  return get_plan(ctx, d.nzp, &a, tuned("zpass_r16", d.nzp, 1) != 0);
 }
 
 }  // namespace

@@ -349,15 +349,9 @@ __global__ void __launch_bounds__(256) k_line4p(const __grid_constant__ GridSet 
   cp_async_wait_0();
 }
 
-// Opt-in (CRAVA_PIPE4=1): measured slower than the one-unit kernels for the column
+// Opt-in (schedule key pipe4): measured slower than the one-unit kernels for the column
 // transforms (staging a W-column tile costs more than it hides) and mixed for the rows.
-static bool pipe4_enabled() {
-  static const bool on = [] {
-    const char* ev = getenv("CRAVA_PIPE4");
-    return ev && ev[0] == '1';
-  }();
-  return on;
-}
+static bool pipe4_enabled(int n) { return tuned("pipe4", n, 0) != 0; }
 
 static cudaError_t resident_grid(const void* fn, int T, size_t smem, int units, int* grid) {
   int dev = 0, nsm = 0, per_sm = 0;
@@ -454,13 +448,7 @@ __global__ void __launch_bounds__(256, 2) k_xy4(const __grid_constant__ GridSet 
   X(768, 32, 24)                 \
   X(1024, 32, 32)
 
-static bool four_step_enabled() {
-  static const bool on = [] {
-    const char* ev = getenv("CRAVA_FOUR_STEP");
-    return !(ev && ev[0] == '0');
-  }();
-  return on;
-}
+static bool four_step_enabled(int n) { return tuned("four_step", n, 1) != 0; }
 
 static int round_up32(int t) { return std::max(64, (t + 31) / 32 * 32); }
 
@@ -470,9 +458,7 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   constexpr int N = N1 * N2;
   // 8-column tiles; 16 for inverse transforms up to 540 points (measured faster there,
   // slower at 768)
-  int W = (sign > 0.f && N <= 540) ? 16 : 8;
-  if (const char* ev = getenv("CRAVA_LINE4_W")) W = std::max(1, atoi(ev));
-  if (const char* ev = getenv(sign < 0.f ? "CRAVA_LINE4_WF" : "CRAVA_LINE4_WI")) W = std::max(1, atoi(ev));
+  int W = std::max(1, tuned(sign < 0.f ? "line4_w_fwd" : "line4_w_inv", N, (sign > 0.f && N <= 540) ? 16 : 8));
   while (W > 1 && W / 2 >= ni) W /= 2;
   int lw = 0;
   while ((1 << lw) < W) lw++;
@@ -480,7 +466,7 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   const int SK = W < 16 ? (((W - N2 * W) % 16) + 16) % 16 : 0;
   const int T = std::min(256, round_up32(W * std::max(N1, N2)));
   const int nIT = (ni + W - 1) / W;
-  if (pipe4_enabled()) {
+  if (pipe4_enabled(N)) {
     // two staged tiles and the work tile: narrower tiles for the longest lines
     int Wp = W;
     while (Wp > 1 && sizeof(float2) * (2 * (size_t)Wp * N) + line4_smem<N1, N2>(Wp, SK) > 104 * 1024) Wp /= 2;
@@ -516,11 +502,11 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   using L = RowLayout<N1, N2>;
   // 128-thread blocks: more CTAs per SM and cheaper barriers than 256 (measured 15 % faster);
   // the inverse rows up to h = 270 are faster still at 64 (3.53 vs 3.66 ms at 540x540x256)
-  int T = (!fwd && L::H <= 270) ? 64 : 128;
-  if (const char* ev = getenv("CRAVA_X4_T")) T = std::max(64, std::min(256, atoi(ev) / 32 * 32));
+  const int T = std::max(64, std::min(256, tuned(fwd ? "x4_threads_fwd" : "x4_threads_inv", L::H,
+                                                   (!fwd && L::H <= 270) ? 64 : 128) / 32 * 32));
   int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
-  if (const char* ev = getenv("CRAVA_X4_RPC")) rpc = std::max(1, std::min(rpc, atoi(ev)));
-  if (pipe4_enabled()) {
+  rpc = std::max(1, std::min(rpc, tuned(fwd ? "x4_rpc_fwd" : "x4_rpc_inv", L::H, rpc)));
+  if (pipe4_enabled(L::H)) {
     const int nchunk = (rows + rpc - 1) / rpc;
     const size_t smem = sizeof(float2) * (2 * (size_t)L::H + 2 * (size_t)rpc * (L::H + 1) + (size_t)rpc * L::PITCH);
     const void* fn = fwd ? (const void*)k_x4p<N1, N2, true> : (const void*)k_x4p<N1, N2, false>;
@@ -551,8 +537,7 @@ static cudaError_t xy4(bool fwd, const GridSet& gs, int nzp, const float2* twx, 
   const int rpc = std::max(1, T / HX1);
   int W = 8, lw = 3;
   const int SK = (((W - NY2 * W) % 16) + 16) % 16;
-  int C = 8;
-  if (const char* ev = getenv("CRAVA_XY_CLUSTER")) C = std::max(1, std::min(16, atoi(ev)));
+  const int C = std::max(1, std::min(16, tuned("xy_cluster", H, 8)));
   const size_t work = std::max(x4_smem<HX1, HX2>(false, rpc), line4_smem<NY1, NY2>(W, SK));
   const size_t smem = sizeof(float2) * (2 * (size_t)H + NY) + work;
   const void* fn = fwd ? (const void*)k_xy4<HX1, HX2, NY1, NY2, true> : (const void*)k_xy4<HX1, HX2, NY1, NY2, false>;
@@ -587,18 +572,12 @@ static cudaError_t xy4(bool fwd, const GridSet& gs, int nzp, const float2* twx, 
   X(540, 540, 18, 15, 27, 20) \
   X(768, 768, 24, 16, 32, 24)
 
-// Opt-in (CRAVA_XY_FUSED=1): at 540^2 and 768^2 the two separate passes are still faster,
-// both being bound by latency rather than by HBM traffic.
-static bool xy_enabled() {
-  static const bool on = [] {
-    const char* ev = getenv("CRAVA_XY_FUSED");
-    return ev && ev[0] == '1';
-  }();
-  return on;
-}
+// Opt-in (schedule key xy_fused, n = nxp): at 540^2 and 768^2 the two separate passes are
+// still faster, both being bound by latency rather than by HBM traffic.
+static bool xy_enabled(int nxp) { return tuned("xy_fused", nxp, 0) != 0; }
 
 bool xy_fused_supported(int nxp, int nyp) {
-  if (!xy_enabled() || !four_step_enabled()) return false;
+  if (!xy_enabled(nxp) || !four_step_enabled(nxp)) return false;
 #define CRAVA_CASE(NX, NY, A, B, C2, D) \
   if (nxp == NX && nyp == NY) return true;
   CRAVA_XY_PAIRS(CRAVA_CASE)
@@ -617,7 +596,7 @@ cudaError_t launch_xy4(bool fwd, const GridSet& gs, int nxp, int nyp, int nzp, c
 }
 
 bool four_step_supported(int n) {
-  if (!four_step_enabled()) return false;
+  if (!four_step_enabled(n)) return false;
   switch (n) {
 #define CRAVA_CASE(NN, A, B) case NN:
     CRAVA_FOUR_STEP_SIZES(CRAVA_CASE)

@@ -437,13 +437,7 @@ static int round_threads(int t) {
   return t < 64 ? 64 : t;
 }
 
-static bool pipe_enabled() {
-  static const bool on = [] {
-    const char* ev = getenv("CRAVA_PIPE");
-    return !(ev && ev[0] == '0');
-  }();
-  return on;
-}
+static bool pipe_enabled() { return tuned("pipe", -1, 1) != 0; }
 
 // Persistent grid: resident CTAs of `fn` at (T, smem) on every SM of the current device,
 // no more than the work units.
@@ -464,11 +458,9 @@ static cudaError_t launch_x(bool fwd, const GridSet& gs, int nxp, int rows, cons
   const int n = even ? nxp / 2 : nxp;
   if (even && four_step_supported(n)) return launch_x4(fwd, gs, nxp, rows, tw, twn, st, nlaunch);
   if (even && pipe_enabled()) {
-    // rows per unit and threads: about 8 points per thread (CRAVA_X_PPT overrides)
-    int ppt = 8;
-    if (const char* ev = getenv("CRAVA_X_PPT")) ppt = std::max(1, atoi(ev));
-    int rpc = std::max(1, std::min(64, 2048 / n));
-    if (const char* ev = getenv("CRAVA_X_RPC")) rpc = std::max(1, atoi(ev));
+    // rows per unit and threads: about 8 points per thread (schedule keys x_ppt, x_rpc)
+    const int ppt = std::max(1, tuned("x_ppt", n, 8));
+    const int rpc = std::max(1, tuned("x_rpc", n, std::max(1, std::min(64, 2048 / n))));
     const int T = std::min(512, round_threads((rpc * n + ppt - 1) / ppt));
     const int h = n, cnxp = h + 1;
     const size_t smem = fwd ? sizeof(float2) * (size_t)(2 * h + 3 * rpc * h)
@@ -484,9 +476,8 @@ static cudaError_t launch_x(bool fwd, const GridSet& gs, int nxp, int rows, cons
     if (nlaunch) (*nlaunch)++;
     return cudaGetLastError();
   }
-  // rows per CTA and threads: about 16 points per thread (CRAVA_X_PPT overrides)
-  int ppt = 16;
-  if (const char* ev = getenv("CRAVA_X_PPT")) ppt = std::max(1, atoi(ev));
+  // rows per CTA and threads: about 16 points per thread (schedule key x_ppt1)
+  const int ppt = std::max(1, tuned("x_ppt1", n, 16));
   int rpc = std::max(1, std::min(64, 2048 / n));
   int T = std::min(512, round_threads((rpc * n + ppt - 1) / ppt));
   size_t smem = sizeof(float2) * (size_t)(n + (even ? nxp / 2 : 0) + 2 * rpc * n);
@@ -515,19 +506,14 @@ cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& p
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch) {
   if (four_step_supported(n)) return launch_line4(gs, ni, n, pstride, no, ostride, tw, sign, st, nlaunch);
-  int W = 16;
-  if (const char* ev = getenv("CRAVA_LINE_W")) W = std::max(1, atoi(ev));
+  int W = std::max(1, tuned("line_w", n, 16));
   while (W > 1 && W * n > 8192) W /= 2;
   while (W > 1 && W / 2 >= ni) W /= 2;  // power of two, not wider than needed
-  int tdiv = 16;
-  if (const char* ev = getenv("CRAVA_LINE_TDIV")) tdiv = std::max(1, atoi(ev));
+  const int tdiv = std::max(1, tuned("line_tdiv", n, 16));
   int T = std::min(512, round_threads((W * n + tdiv - 1) / tdiv));
   int nIT = (ni + W - 1) / W;
   // the pipelined form measured slower for column tiles (fewer resident CTAs): opt-in
-  static const bool line_pipe = [] {
-    const char* ev = getenv("CRAVA_LINE_PIPE");
-    return ev && ev[0] == '1';
-  }();
+  const bool line_pipe = tuned("line_pipe", n, 0) != 0;
   if (line_pipe) {
     const size_t smem = sizeof(float2) * (size_t)(n + 3 * W * n);
     const void* fn = sign < 0.f ? (const void*)k_line_pipe<-1> : (const void*)k_line_pipe<1>;

@@ -9,6 +9,12 @@
 
 namespace crava {
 
+// Schedule table: tile shapes and kernel choices by name and size (n), from the schedule
+// file the library loads at first use (schedules.txt beside the library, written by
+// crava_b200/autotune.py; CRAVA_SCHEDULES names another file) or set through
+// crava_tuning_set.  An entry for n, else one for n = -1 (any size), else `fallback`.
+int tuned(const char* key, int n, int fallback);
+
 constexpr int kMaxGrids = 64;   // grids per batched transform launch
 constexpr int kMaxTheta = 8;    // angle stacks per block
 constexpr int kMaxSim = 16;     // realisations per job launch
@@ -69,6 +75,11 @@ struct ZParams {
   double Ad[kMaxTheta][3];         // A, ec, ed in double for that path
   double ecd[kMaxTheta][kMaxTheta];
   double edd[kMaxTheta];
+  // eigen form of the separable posterior (pencil.cu): per-position rows of the per-kz
+  // tables, float4 group g of position p at eig[g * nzp + p]; null for the general kernel
+  const float4* eig;
+  int n_inv_rows;                  // inverted kz (counted per tile, not per bin)
+  int dense;                       // 1: the 80-register instantiation (two CTAs per SM)
   unsigned long long* counters;    // [0] inverted bins [1] chol fallbacks [2] zero sim bins
                                    // [3] bins re-factorised in FP64 [4] pencil tiles whose
                                    // input spectra are not finite
@@ -173,6 +184,25 @@ cudaError_t launch_x_c2r(const GridSet& gs, int nxp, int rows, const LinePlan& p
 cudaError_t launch_line_fft(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
                             const LinePlan& pl, const float2* tw, float sign, cudaStream_t st, int* nlaunch);
 cudaError_t launch_zpass(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch);
+// pencil.cu: the separable-prior pencil pass in its eigen form, for the four-step z lengths
+// (zp.zsplit 1..3); zp.eig from build_eig_tables
+cudaError_t launch_pencil(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch);
+size_t pencil_smem_bytes(int W, int nzp, int nth, int SB);
+// Float layout of one position's row of the eigen tables: kw (2n floats), Lam (n), then per
+// angle l a row of V (2n floats) and Q_l (6) + H_l (9); sections padded to 4 floats so the
+// kernel reads them as float4 groups and streams one angle's row at a time.
+struct EigLayout {
+  int kw, lam, rows, vpad, rs, floats;
+  explicit EigLayout(int n) {
+    auto pad = [](int x) { return (x + 3) / 4 * 4; };
+    kw = 0;
+    lam = pad(2 * n);
+    rows = lam + pad(n);
+    vpad = pad(2 * n);
+    rs = vpad + 16;
+    floats = rows + n * rs;
+  }
+};
 size_t zpass_smem_bytes(int W, int nzp, int nth);                  // GT = 3, SB = 1
 size_t zpass_smem_bytes(int W, int nzp, int nth, int GT, int SB);
 // facies.cu: prior[] and out[] are host arrays (copied into the launch parameters)

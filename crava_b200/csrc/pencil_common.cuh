@@ -1,0 +1,111 @@
+// Device helpers shared by the two pencil-pass kernels (zpass.cu, pencil.cu): the
+// counter-based noise of product-mode realisations and the reference-semantics Cholesky
+// factorisation of small Hermitian matrices.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_core.cuh"
+
+namespace crava {
+
+// ------------------------------------------------------------------ noise (product mode)
+
+// Philox-4x32 (Salmon, Moraes, Dror, Shaw, SC'11) with 7 rounds, which the authors
+// report passes TestU01 BigCrush.
+__device__ __forceinline__ uint4 philox4x32_7(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 7; r++) {
+    uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Box-Muller with the hardware approximations of log, sine and cosine: their absolute
+// errors (about 2^-21 on these ranges) are far below what the normals' statistics can show.
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, float& n1) {
+  float u1 = ((float)a + 0.5f) * 2.3283064365386963e-10f;
+  float u2 = ((float)b + 0.5f) * 2.3283064365386963e-10f - 0.5f;   // (-1/2, 1/2)
+  float rad = sqrtf(-2.0f * __logf(u1));
+  float sn, cs;
+  __sincosf(6.283185307179586f * u2, &sn, &cs);   // angle in (-pi, pi)
+  n0 = rad * cs;
+  n1 = rad * sn;
+}
+
+// Three standard complex normals (one per parameter) for bin (i,j,k) of realisation s,
+// Hermitian-consistent on the planes whose x-bin is its own mirror (i = 0, and
+// i = nxp/2 for even nxp): the pair (j,k) / (-j,-k) share one draw (conjugated),
+// self-mirrored bins are real with unit variance, all others have variance 1/2 per
+// component (the properties FFTGrid::fillInComplexNoise gives its noise,
+// src/fftgrid.cpp:997-1055, with the mirror-plane test done on the x index).
+__device__ __forceinline__ void device_noise3(uint64_t seed, int s, int i, int j, int k, int nyp, int nzp,
+                                              int cnxp, bool nxp_even, float2 (&z)[3]) {
+  bool mirror_plane = (i == 0) || (nxp_even && i == cnxp - 1);
+  int jj = j, kk = k;
+  bool conj = false, self = false;
+  if (mirror_plane) {
+    int jc = j == 0 ? 0 : nyp - j;
+    int kc = k == 0 ? 0 : nzp - k;
+    long long a = (long long)j + (long long)nyp * k, b = (long long)jc + (long long)nyp * kc;
+    if (a == b) self = true;
+    else if (b < a) { jj = jc; kk = kc; conj = true; }
+  }
+  uint64_t bin = ((uint64_t)kk * nyp + jj) * cnxp + i;
+  uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  uint4 r0 = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 0u), key);
+  uint4 r1 = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 1u), key);
+  float n[6];
+  box_muller(r0.x, r0.y, n[0], n[1]);
+  box_muller(r0.z, r0.w, n[2], n[3]);
+  box_muller(r1.x, r1.y, n[4], n[5]);
+  const float h = self ? 1.0f : 0.70710678118654752f;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    z[c] = make_float2(h * n[2 * c], self ? 0.f : h * n[2 * c + 1]);
+    if (conj) z[c].y = -z[c].y;
+  }
+}
+
+// ------------------------------------------------------------------ per-bin algebra
+
+// lib_matrCholCpx (libs/lib/lib_matr.c:78-168) on the lower triangle of a Hermitian
+// n x n matrix a[][]: the reference scales by a00, rejects a00 <= 0, a scaled diagonal
+// <= 1e-20 before its update or an updated pivot <= 1e-20, factors and rescales by
+// sqrt(a00).  Here the factor is computed unscaled with the two pivot tests applied as
+// a_ii > 1e-20 a00 (the same comparisons up to rounding), and each pivot's reciprocal
+// comes from one reciprocal square root.  No division.  The diagonal entry holds
+// (L_ii, 1 / L_ii): its imaginary part, zero for a Hermitian factor, carries the reciprocal.
+template <int N>
+__device__ __forceinline__ bool chol_ref(float2 (&a)[N][N]) {
+  const float f = a[0][0].x;
+  if (!(f > 0.f)) return false;
+  const float tol = 1e-20f * f;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    if (!(a[i][i].x > tol)) return false;
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      float2 s = a[i][j];
+#pragma unroll
+      for (int k = 0; k < j; k++) {  // - L_ik conj(L_jk)
+        s.x -= a[i][k].x * a[j][k].x + a[i][k].y * a[j][k].y;
+        s.y -= -(a[i][k].x * a[j][k].y) + a[i][k].y * a[j][k].x;
+      }
+      a[i][j] = make_float2(s.x * a[j][j].y, s.y * a[j][j].y);
+    }
+    float r = a[i][i].x;
+#pragma unroll
+    for (int k = 0; k < i; k++) r -= a[i][k].x * a[i][k].x + a[i][k].y * a[i][k].y;
+    if (!(r > tol)) return false;
+    const float rs = rsqrtf(r);
+    a[i][i] = make_float2(r * rs, rs);
+  }
+  return true;
+}
+
+}  // namespace crava

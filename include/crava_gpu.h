@@ -196,6 +196,20 @@ crava_status crava_fft_c2r(crava_ctx* ctx, float* dgrid, int nxp, int nyp, int n
 crava_status crava_fft_r2c_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance);
 crava_status crava_fft_c2r_host(crava_ctx* ctx, float* hgrid, int nxp, int nyp, int nzp, int covariance);
 
+/* Schedules (no counterpart in the reference, whose FFTW plans pick their own codelets):
+ * tile shapes and kernel choices of the transform and pencil kernels, looked up by key and
+ * size n.  The library loads them once per process from the file CRAVA_SCHEDULES names, or
+ * else schedules.txt beside the library (written by crava_b200/autotune.py; lines
+ * "key n value", n = -1 for every size); built-in defaults apply where the table has no
+ * entry.  crava_tuning_set overrides one entry for this process (value < 0 removes it),
+ * crava_tuning_get returns the value a launch would use (-1: the built-in default),
+ * crava_tuning_load replaces the table from another file, and crava_tuning_path names the
+ * file in use ("" when none was found).  Keys: see crava_b200/autotune.py. */
+crava_status crava_tuning_set(const char* key, int n, int value);
+crava_status crava_tuning_get(const char* key, int n, int* value);
+crava_status crava_tuning_load(const char* path);
+const char* crava_tuning_path(void);
+
 /* Kernels launched by this library since the context was created (all entry points). */
 long long crava_ctx_kernel_launches(crava_ctx* ctx);
 

@@ -129,3 +129,29 @@ def test_non_finite_description_rejected_as_numeric(small, array):
     out = ctypes.c_size_t()
     assert api.lib().crava_job_footprint(ctypes.byref(d), ctypes.byref(out)) == api.ENUMERIC
     assert b"non-finite" in api.lib().crava_last_error()
+
+
+def test_schedule_table_set_get_load(tmp_path):
+    """The schedule table: per-size entries, the any-size entry (n = -1), removal, and a file
+    of "key n value" lines with comments replacing the table."""
+    key = "test_only_key"
+    assert api.tuning_get(key, 7) == -1
+    api.tuning_set(key, -1, 3)
+    assert api.tuning_get(key, 7) == 3
+    api.tuning_set(key, 7, 5)
+    assert api.tuning_get(key, 7) == 5 and api.tuning_get(key, 8) == 3
+    api.tuning_set(key, 7, -1)
+    api.tuning_set(key, -1, -1)
+    assert api.tuning_get(key, 7) == -1
+    f = tmp_path / "sched.txt"
+    f.write_text("# comment line\n" + key + " 256 4   # trailing comment\n" + key + " -1 2\n")
+    before = api.tuning_path()
+    api.tuning_load(str(f))
+    try:
+        assert api.tuning_path() == str(f)
+        assert api.tuning_get(key, 256) == 4 and api.tuning_get(key, 320) == 2
+    finally:
+        if before:
+            api.tuning_load(before)
+    with pytest.raises(api.CravaError):
+        api.tuning_load(str(tmp_path / "missing.txt"))

