@@ -338,30 +338,40 @@ def cfg3_leg(torch, steps, warmup):
             "kernel_ms_per_job": {c: kt[c][0] / steps for c in kt if kt[c][1]}}
 
 
-def served_leg(torch, n_jobs=48, distinct=8, rate=20.0, nsim=16, max_inflight=8, budget_gb=120):
-    """Served stream: Poisson arrivals at `rate` jobs/s of blocks log-uniform between
-    64x64x64 and 512x512x256, 3..6 angles, 16 realisations; host->device inputs, inversion,
-    device->host of the posterior mean, covariance and first realisation per request.
-    Against the plain one-job-at-a-time path (create, upload, run, download, release)."""
+def served_leg(torch, n_jobs=48, n_models=6, rate=20.0, nsim=16, max_inflight=8, budget_gb=120):
+    """Served stream: Poisson arrivals at `rate` jobs/s; every request drawn fresh: one of
+    n_models interval models (nz, 3..6 angles, priors within +-30% of the 64x64x128 block,
+    wavelets) and its own lateral shape, so that voxel counts are log-uniform between 64^3 and
+    512x512x256; 16 realisations; host->device inputs, inversion, device->host of the
+    posterior mean, covariance and first realisation per request.  Against the plain
+    one-job-at-a-time path (create, upload, run, download, release) on a context without the
+    resident table cache.  Input values come from a shared random pinned pool and outputs
+    land in a shared pinned scratch (the inversion's cost does not depend on the values; the
+    test suite checks every result alone and in a served mix)."""
     import numpy as np
     from crava_b200 import api, synth
-    specs = synth.served_specs(n_jobs, nsim=nsim)
-    uniq = [synth.make_block_fast(s) for s in specs[:distinct]]
-    reqs = [i % distinct for i in range(n_jobs)]
-    bufs = []
-    for b in uniq:
-        shape = (b.nzp, b.nyp, 2 * (b.nxp // 2 + 1))
-        ins = [torch.from_numpy(np.ascontiguousarray(b.data[l])).pin_memory() for l in range(b.ntheta)] +               [torch.from_numpy(np.ascontiguousarray(b.mean[a])).pin_memory() for a in range(3)]
-        outs = [torch.empty(shape, dtype=torch.float32).pin_memory() for _ in range(12)] +                [None] * (3 * nsim - 3)
-        bufs.append((ins, outs))
-    vox = sum(uniq[i].n_voxels for i in reqs)
-    ctx = api.Context(torch.cuda.current_device(), hbm_budget=int(budget_gb * 1e9))
+    specs = synth.served_stream_specs(n_jobs, n_models=n_models, nsim=nsim)
+    blocks = [synth.make_block_fast(sp, data=False) for sp in specs]
+    shapes = [(b.nzp, b.nyp, 2 * (b.nxp // 2 + 1)) for b in blocks]
+    gmax = max(int(np.prod(sh)) for sh in shapes)
+    rng = np.random.default_rng(5)
+    pool_in = torch.empty(9 * gmax, dtype=torch.float32).pin_memory()
+    pool_in.numpy()[:] = rng.standard_normal(9 * gmax, dtype=np.float32) * np.float32(0.02)
+    pool_out = torch.empty(12 * gmax, dtype=torch.float32).pin_memory()
+
+    def bufs(k):
+        b, n = blocks[k], int(np.prod(shapes[k]))
+        ins = [pool_in[q * gmax:q * gmax + n].view(shapes[k]) for q in range(b.ntheta + 3)]
+        outs = [pool_out[q * gmax:q * gmax + n].view(shapes[k]) for q in range(12)] + [None] * (3 * nsim - 3)
+        return ins, outs
+
+    vox = sum(b.n_voxels for b in blocks)
     # plain path
+    ctx = api.Context(torch.cuda.current_device(), hbm_budget=int(budget_gb * 1e9))
     t0 = time.perf_counter()
-    for i in reqs:
-        b = uniq[i]
-        j = api.Job(ctx, b, api.PRIOR_SEPARABLE, 0, seed=900 + i)
-        ins, outs = bufs[i]
+    for k, b in enumerate(blocks):
+        j = api.Job(ctx, b, api.PRIOR_SEPARABLE, 0, seed=900 + k)
+        ins, outs = bufs(k)
         for q, h in enumerate(ins):
             role, idx = (api.ROLE_DATA, q) if q < b.ntheta else (api.ROLE_MEAN, q - b.ntheta)
             api._check(api.lib().crava_job_upload(j._h, role, idx, h.data_ptr(), None))
@@ -372,30 +382,34 @@ def served_leg(torch, n_jobs=48, distinct=8, rate=20.0, nsim=16, max_inflight=8,
         torch.cuda.synchronize()
         j.close()
     t_plain = time.perf_counter() - t0
-    # served at `rate` (Poisson) and saturated (all at once)
-    rng = np.random.default_rng(77)
+    ctx.close()
+    # served at `rate` (Poisson) and saturated (all at once), each on a fresh context
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_jobs))
     res = {}
     for mode in ("poisson", "saturated"):
+        ctx = api.Context(torch.cuda.current_device(), hbm_budget=int(budget_gb * 1e9))
         sv = api.Server(ctx, max_inflight=max_inflight)
         tickets = []
         t0 = time.perf_counter()
-        for k, i in enumerate(reqs):
+        for k, b in enumerate(blocks):
             if mode == "poisson":
                 dt = arrivals[k] - (time.perf_counter() - t0)
                 if dt > 0:
                     time.sleep(dt)
-            ins, outs = bufs[i]
-            tickets.append(sv.submit(uniq[i], ins, outs, seed=900 + i))
+            ins, outs = bufs(k)
+            tickets.append(sv.submit(b, ins, outs, seed=900 + k))
         infos = [sv.wait(t, timeout_ms=600000) for t in tickets]
         t_all = time.perf_counter() - t0
         sv.stop()
+        cache = ctx.table_cache_stats()
+        ctx.close()
         lat = np.array([x["latency_ms"] for x in infos])
         res[mode] = {"jobs_per_s": n_jobs / t_all, "voxels_per_s": vox / t_all,
                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                     "speedup_vs_plain": t_plain / t_all}
-    ctx.close()
-    return {"workload": f"{n_jobs} requests over {distinct} blocks log-uniform 64^3..512x512x256 voxels, 3..6 angles, "
+                     "speedup_vs_plain": t_plain / t_all,
+                     "table_cache": {"hits": cache["hits"], "misses": cache["misses"], "entries": cache["entries"]}}
+    return {"workload": f"{n_jobs} requests, each drawn fresh: one of {n_models} interval models (nz, 3..6 angles, "
+                        f"+-30% priors, wavelets) and its own lateral shape, voxels log-uniform 64^3..512x512x256, "
                         f"{nsim} realisations; outputs mean+cov+1 realisation to host; {rate:g} jobs/s Poisson",
             "voxels": vox, "plain_jobs_per_s": n_jobs / t_plain, "plain_voxels_per_s": vox / t_plain,
             "max_inflight": max_inflight, "budget_gb": budget_gb, **res}

@@ -124,6 +124,16 @@ def lib() -> ctypes.CDLL:
     L.crava_facies_smooth.argtypes = [vp, ctypes.POINTER(FaciesDesc), ctypes.POINTER(ctypes.c_double), vp, vp]
     L.crava_facies_prob.argtypes = [vp, ctypes.POINTER(FaciesDesc), vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
+    L.crava_job_local_noise.argtypes = [vp, vp, vp]
+    L.crava_facies_prob_local_noise.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, vp,
+                                                ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
+    L.crava_job_fill_prior_auto_cov.argtypes = [vp, vp, ctypes.c_float, ctypes.c_float, vp]
+    L.crava_circ_corr_t.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    L.crava_circ_auto_cov.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp]
+    L.crava_ctx_set_table_cache.argtypes = [vp, ctypes.c_size_t]
+    L.crava_ctx_table_cache_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                             ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
     L.crava_tuning_set.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     L.crava_tuning_get.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.crava_tuning_load.argtypes = [ctypes.c_char_p]
@@ -158,6 +168,23 @@ def tuning_path() -> str:
     return (lib().crava_tuning_path() or b"").decode()
 
 
+def circ_corr_t(prior_corr_t, min_int_fq: int, nzp: int) -> np.ndarray:
+    """computeCircCorrT + makeCircCorrTPosDef on the host (crava_circ_corr_t)."""
+    a = np.ascontiguousarray(prior_corr_t, dtype=np.float64)
+    out = np.empty(nzp, dtype=np.float32)
+    _check(lib().crava_circ_corr_t(a.ctypes.data, len(a), int(min_int_fq), int(nzp), out.ctypes.data))
+    return out
+
+
+def circ_auto_cov(auto_cov, nzp: int, dz: float) -> np.ndarray:
+    """Estimated circular auto-covariances made positive definite and tapered
+    (crava_circ_auto_cov); auto_cov (nlag, 3, 3); returns (6, nzp)."""
+    a = np.ascontiguousarray(auto_cov, dtype=np.float64)
+    out = np.empty((6, nzp), dtype=np.float32)
+    _check(lib().crava_circ_auto_cov(a.ctypes.data, a.shape[0], int(nzp), float(dz), out.ctypes.data))
+    return out
+
+
 def pencil_key(nzp: int, ntheta: int) -> int:
     """Size key of the pencil-pass schedule entries."""
     return nzp * 16 + ntheta
@@ -185,6 +212,17 @@ class Context:
         cnt = (ctypes.c_longlong * n)()
         _check(lib().crava_ctx_kernel_times(self._h, ms, cnt, n, int(reset)))
         return {k: (ms[i], cnt[i]) for i, k in enumerate(KERNEL_CLASSES)}
+
+    def set_table_cache(self, max_bytes: int):
+        """Resident per-kz and lateral tables shared by jobs of the same model (0: off)."""
+        _check(lib().crava_ctx_set_table_cache(self._h, int(max_bytes)))
+
+    def table_cache_stats(self) -> dict:
+        h, m, n = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int()
+        b = ctypes.c_size_t()
+        _check(lib().crava_ctx_table_cache_stats(self._h, ctypes.byref(h), ctypes.byref(m), ctypes.byref(b),
+                                                 ctypes.byref(n)))
+        return {"hits": h.value, "misses": m.value, "bytes": b.value, "entries": n.value}
 
     def close(self):
         if self._h:
@@ -288,10 +326,25 @@ class Job:
         grid on the device from corr_xy and circ_corr_t (InitializeCorrelations)."""
         _check(lib().crava_job_fill_prior(self._h, float(corr_grad_i), float(corr_grad_j), stream))
 
+    def fill_prior_auto_cov(self, circ_auto_cov, corr_grad_i: float = 0.0, corr_grad_j: float = 0.0, stream=None):
+        """GRIDS-mode job with estimated covariance: the six covariance grids
+        FillInLateralCorr(corrXY, circAutoCov_q) and the error-correlation grid on the device."""
+        a = np.ascontiguousarray(circ_auto_cov, dtype=np.float32)
+        assert a.shape == (6, self.blk.nzp), a.shape
+        _check(lib().crava_job_fill_prior_auto_cov(self._h, a.ctypes.data, float(corr_grad_i), float(corr_grad_j),
+                                                   stream))
+
     def divide_data(self, stream=None):
         """divideDataByScaleWavelet + interpolateSeismic on the uploaded data (non-constant
         thickness jobs); returns after the work is done."""
         _check(lib().crava_job_divide_data(self._h, stream))
+
+    def local_noise(self, scales: np.ndarray, stream=None):
+        """correctVpVsRho and the local-noise mixing of the realisations, in place on the
+        posterior mean and realisation grids; scales (ntheta, ny, nx) local noise scales."""
+        a = np.ascontiguousarray(scales, dtype=np.float32)
+        assert a.shape == (self.blk.ntheta, self.blk.ny, self.blk.nx), a.shape
+        _check(lib().crava_job_local_noise(self._h, a.ctypes.data, stream))
 
     def counters(self) -> dict:
         """Per-job counters after a run; raises CravaError (status ENUMERIC) when the data
@@ -427,14 +480,20 @@ class Server:
         return t.value
 
     def poll(self, ticket: int) -> dict:
+        """A request's state; after its final state has been reported the ticket is released."""
         info = RequestInfo()
         _check(lib().crava_serve_poll(self._h, ticket, ctypes.byref(info)))
+        if info.state in (REQ_DONE, REQ_FAILED):
+            self._keep.pop(ticket, None)
         return {"state": info.state, "status": info.status, "queue_ms": info.queue_ms, "latency_ms": info.latency_ms}
 
     def wait(self, ticket: int, timeout_ms: float = 600000.0) -> dict:
+        """Waits for a request; raises CravaError with the request's status when it failed."""
         info = RequestInfo()
-        _check(lib().crava_serve_wait(self._h, ticket, timeout_ms, ctypes.byref(info)))
-        self._keep.pop(ticket, None)
+        st = lib().crava_serve_wait(self._h, ticket, timeout_ms, ctypes.byref(info))
+        if st != ETIMEDOUT:
+            self._keep.pop(ticket, None)
+        _check(st)
         return {"state": info.state, "status": info.status, "queue_ms": info.queue_ms, "latency_ms": info.latency_ms}
 
     def stop(self):
@@ -473,3 +532,19 @@ def facies_prob(ctx: Context, fd, d_density: int, density_row: int, d_post, nx, 
     prob = (ctypes.c_void_p * len(d_prob))(*d_prob)
     _check(lib().crava_facies_prob(ctx.handle, ctypes.byref(fd), d_density, density_row, post, nx, ny, nz, nxp, nyp,
                                    prob, d_seis_lh, stream))
+
+
+def facies_prob_local_noise(ctx: Context, corner_descs, d_densities, density_row: int, noise_scale, d_post, nx, ny,
+                            nz, nxp, nyp, d_prob, d_seis_lh=None, stream=None):
+    """Facies probabilities with local noise: 2^nang corner density volumes (corner_descs,
+    d_densities), noise_scale (nang, ny, nx) host maps."""
+    nang = int(np.asarray(noise_scale).shape[0]) if np.asarray(noise_scale).ndim == 3 else 0
+    assert len(corner_descs) == 1 << nang and len(d_densities) == 1 << nang
+    arr = (FaciesDesc * len(corner_descs))(*corner_descs)
+    dens = (ctypes.c_void_p * len(d_densities))(*d_densities)
+    sc = np.ascontiguousarray(noise_scale, dtype=np.float32)
+    post = (ctypes.c_void_p * 3)(*d_post)
+    prob = (ctypes.c_void_p * len(d_prob))(*d_prob)
+    _check(lib().crava_facies_prob_local_noise(ctx.handle, arr, nang, dens, int(density_row),
+                                               sc.ctypes.data if nang else None, post, nx, ny, nz, nxp, nyp, prob,
+                                               d_seis_lh, stream))

@@ -155,6 +155,41 @@ struct ProfRec {
   cudaEvent_t a, b;
 };
 
+namespace {
+// Per-block device tables: the per-kz operator tables of the prior and wavelet model (with
+// the separable factors and the eigen tables of pencil.cu) and the lateral correlation
+// spectrum.  They sit in the job's pool, or in an entry of the context's resident cache
+// shared by every job with the same model (crava_ctx_set_table_cache).
+struct KzSet {
+  float2 *kw = nullptr, *e1 = nullptr, *e2 = nullptr, *septab = nullptr, *ct = nullptr;
+  double2 *kwd = nullptr, *e1d = nullptr, *e2d = nullptr;
+  uint8_t* inv = nullptr;
+  float* edk = nullptr;
+  double* eddk = nullptr;
+  float4* eig = nullptr;
+  bool eig_base = false;     // eigen tables built; a job applies them when its largest
+  double lam_limit = 0;      //   lateral factor is below lam_limit
+  int n_inv_rows = 0;
+  std::string eig_why;
+};
+
+struct LatSet {
+  float2* cxy = nullptr;     // nyp x cnxp spectrum of corrXY
+  float* grid = nullptr;     // its real staging grid
+};
+
+struct CacheEntry {
+  std::string key;
+  char* mem = nullptr;
+  size_t bytes = 0;
+  int refs = 0;
+  uint64_t tick = 0;
+  cudaEvent_t ready = nullptr;   // recorded after the tables were built, on the building stream
+  KzSet k;
+  LatSet l;
+};
+}  // namespace
+
 struct crava_ctx {
   int device = 0;
   size_t budget = 0;
@@ -169,9 +204,17 @@ struct crava_ctx {
   std::mutex stage_mu;         // device staging grid of the host-grid transforms
   float* stage = nullptr;
   size_t stage_bytes = 0;
+  // resident table cache: key (model bytes) -> device tables, least recently used evicted
+  std::mutex cache_mu;
+  std::map<std::string, CacheEntry*> cache;
+  size_t cache_max = 0, cache_bytes = 0;
+  long long cache_hits = 0, cache_misses = 0;
+  uint64_t cache_tick = 0;
 };
 
 namespace {
+void cache_evict_locked(crava_ctx* ctx, size_t want, cudaStream_t st);
+
 // Brackets one launch with events on its stream when profiling is on.
 struct ProfScope {
   crava_ctx* ctx;
@@ -225,6 +268,10 @@ struct crava_job {
   int n_inv_rows = 0;        //   inverted kz
   std::string eig_why;       //   why the general kernel runs instead
   float* cxy_grid = nullptr; // staging for the corr_xy transform
+  float* fill_xy = nullptr;  // GRIDS: corrXY and circCorrT for crava_job_fill_prior
+  float* fill_t = nullptr;
+  CacheEntry* kz_entry = nullptr;   // tables held in the context's cache (referenced)
+  CacheEntry* lat_entry = nullptr;
   unsigned long long* counters = nullptr;
   // CRAVA_FLAG_NONCONST_THICK: per-kz diagonal error terms, the data pre-processing
   // parameters (device tables inside) and its work buffers
@@ -357,20 +404,37 @@ size_t thick_bytes(const crava_job_desc* d) {
 
 size_t eig_table_bytes(const crava_job_desc* d);
 
-size_t footprint(const crava_job_desc* d) {
+// Device bytes of one job, in three parts: the grids (caller inputs, work grids, counters,
+// non-constant-thickness buffers), the per-kz tables of its prior and wavelet model, and its
+// lateral correlation factor.  The last two live in the job's pool, or in the context's
+// resident table cache when that is on (crava_ctx_set_table_cache).
+size_t grid_part_bytes(const crava_job_desc* d) {
   size_t cnxp = d->nxp / 2 + 1;
   size_t gb = align256(sizeof(float) * 2 * cnxp * d->nyp * d->nzp);
   size_t ngrids = 2 * ((size_t)d->ntheta + 3) + 6 + 3 * (size_t)d->nsim;
   if (d->prior_mode == CRAVA_PRIOR_GRIDS) ngrids += 6 + 2;
   if (d->flags & CRAVA_FLAG_HOST_NOISE) ngrids += 3 * (size_t)d->nsim;
-  const size_t sep_stride = (size_t)d->ntheta * (d->ntheta + 1) / 2;
-  size_t tables = 3 * align256(sizeof(float2) * d->nzp * d->ntheta) + align256(sizeof(float2) * d->nzp * sep_stride) +
-                  3 * align256(sizeof(double2) * d->nzp * d->ntheta) + align256(d->nzp) +
-                  align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float2) * d->nzp) +
-                  align256(sizeof(float) * 2 * cnxp * d->nyp) + 256 + align256(sizeof(float) * d->nzp * d->ntheta) +
-                  align256(sizeof(double) * d->nzp * d->ntheta);
-  return ngrids * gb + tables + thick_bytes(d) + eig_table_bytes(d);
+  const size_t fill = d->prior_mode == CRAVA_PRIOR_GRIDS
+                          ? align256(sizeof(float) * 2 * cnxp * d->nyp) + align256(sizeof(float) * d->nzp)
+                          : 0;
+  return ngrids * gb + 256 + thick_bytes(d) + fill;
 }
+
+size_t kz_set_bytes(const crava_job_desc* d) {
+  const size_t sep_stride = (size_t)d->ntheta * (d->ntheta + 1) / 2;
+  return 3 * align256(sizeof(float2) * d->nzp * d->ntheta) + align256(sizeof(float2) * d->nzp * sep_stride) +
+         3 * align256(sizeof(double2) * d->nzp * d->ntheta) + align256(d->nzp) + align256(sizeof(float2) * d->nzp) +
+         align256(sizeof(float) * d->nzp * d->ntheta) + align256(sizeof(double) * d->nzp * d->ntheta) +
+         eig_table_bytes(d);
+}
+
+size_t lat_set_bytes(const crava_job_desc* d) {
+  if (d->prior_mode != CRAVA_PRIOR_SEPARABLE) return 0;
+  const size_t cnxp = d->nxp / 2 + 1;
+  return align256(sizeof(float2) * cnxp * d->nyp) + align256(sizeof(float) * 2 * cnxp * d->nyp);
+}
+
+size_t footprint(const crava_job_desc* d) { return grid_part_bytes(d) + kz_set_bytes(d) + lat_set_bytes(d); }
 
 // DFT of a real vector in double precision, e^{-2 pi i k t / n}.
 std::vector<cd> dft(const std::vector<double>& x) {
@@ -605,13 +669,15 @@ void sep_constants(const std::vector<double>& A, const std::vector<double>& pv, 
 //   M = |ct| (kw kw^H) o G0 + M2,  E = diag(ed),  E^-1/2 M E^-1/2 = U diag(Lam) U^H,
 //   V = U^H E^-1/2,  Q = |ct| V diag(kw) AP,  H_l = conj(Q_la) Q_lb.
 // Rows of kz outside the inversion band are zero (prior kept, residual = data).  Returns
-// false with the reason when the form does not apply: some ed <= 0, an eigenvalue of M
-// clearly negative, or a reference Cholesky of Sd that could reach its 1e-20 pivot test
-// (pivots of Sd >= min ed; Sd_00 <= lam_max M_00 + ed_0, lam_max <= sum |corrXY|).
+// false with the reason when the form does not apply: some ed <= 0 or an eigenvalue of M
+// clearly negative.  lam_limit: the largest lateral factor lam for which no reference
+// Cholesky of Sd could reach its 1e-20 pivot test (pivots of Sd >= min ed, Sd_00 <=
+// lam M_00 + ed_0); a job applies the form when max lam (<= sum |corrXY|) is below it.
 bool build_eig_tables(const crava_job_desc& d, const std::vector<float2>& kw, const std::vector<float2>& sep,
                       const std::vector<float>& edk, const std::vector<uint8_t>& inv, const std::vector<float2>& ct,
-                      const float (&G0)[kMaxTheta][kMaxTheta], const float (&AP)[kMaxTheta][3], double lam_max,
+                      const float (&G0)[kMaxTheta][kMaxTheta], const float (&AP)[kMaxTheta][3], double& lam_limit,
                       std::vector<float>& rows, int& n_inv_rows, std::string& why) {
+  lam_limit = INFINITY;
   const int n = d.ntheta, nzp = d.nzp, zs = zsplit_of(nzp);
   const int N1 = zsplit_n1(zs), N2 = zsplit_n2(zs);
   const EigLayout L(n);
@@ -643,7 +709,7 @@ bool build_eig_tables(const crava_job_desc& d, const std::vector<float2>& kw, co
     const double m00 = M[0][0].real();
     double emin = e[0];
     for (int l = 1; l < n; l++) emin = std::min(emin, e[l]);
-    if (!(emin > 1e-18 * (lam_max * m00 + e[0]))) { why = "data covariance too close to singular"; return false; }
+    if (m00 > 0) lam_limit = std::min(lam_limit, (emin * 1e18 - e[0]) / m00);
     for (int l = 0; l < n; l++)
       for (int m = 0; m < n; m++) M[l][m] /= std::sqrt(e[l] * e[m]);
     double lam[kMaxTheta];
@@ -944,6 +1010,104 @@ const char* crava_status_string(crava_status s) {
   return "unknown status";
 }
 
+crava_status crava_circ_corr_t(const double* prior_corr_t, int n, int min_int_fq, int nzp, float* out) {
+  if (!prior_corr_t || !out || n < 1 || nzp < 2) return fail(CRAVA_EINVAL, "bad arguments");
+  if (!(prior_corr_t[0] != 0.0)) return fail(CRAVA_EINVAL, "prior_corr_t[0] must be nonzero");
+  // circular extension (computeCircCorrT, src/seismicparametersholder.cpp:624-660)
+  std::vector<double> c(nzp, 0.0);
+  for (int k = 0; k < nzp; k++) {
+    const int refk = k < nzp / 2 + 1 ? k : nzp - k;
+    c[k] = refk < n ? (double)(float)prior_corr_t[refk] : 0.0;
+  }
+  // makeCircCorrTPosDef (:805-840): spectrum zero at k <= minIntFq, |.| elsewhere, back
+  // transform (unnormalised) and divide by the lag-0 value
+  std::vector<cd> C = dft(c);
+  std::vector<double> mag(nzp / 2 + 1);
+  for (int k = 0; k <= nzp / 2; k++) mag[k] = k <= min_int_fq ? 0.0 : std::abs(C[k]);
+  std::vector<double> back(nzp, 0.0);
+  for (int t = 0; t < nzp; t++) {
+    double acc = mag[0];
+    for (int k = 1; k <= nzp / 2; k++) {
+      const double w = (2 * k == nzp) ? 1.0 : 2.0;   // Hermitian pairs k, nzp - k
+      acc += w * mag[k] * std::cos(2.0 * M_PI * (double)((long long)k * t % nzp) / nzp);
+    }
+    back[t] = acc;
+  }
+  if (!(back[0] > 1e-5))
+    return fail(CRAVA_EINVAL, "circular temporal correlation undefined: too few layers for the correlation range");
+  for (int t = 0; t < nzp; t++) out[t] = (float)(back[t] / back[0]);
+  return CRAVA_OK;
+}
+
+crava_status crava_circ_auto_cov(const double* auto_cov, int nlag, int nzp, double dz, float* out) {
+  if (!auto_cov || !out || nlag < 1 || nzp < 2 || !(dz > 0)) return fail(CRAVA_EINVAL, "bad arguments");
+  const double eps = 1e-10;
+  // ComputeCircAutoCov per pair (src/seismicparametersholder.cpp:559-620) with the lag-0
+  // test of InitializeCorrelations (:247-274): lag k of pair (i, j) forward, (j, i) backward
+  std::vector<std::vector<double>> circ(9, std::vector<double>(nzp, 0.0));
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      std::vector<double>& c = circ[3 * i + j];
+      const bool zero = !(std::fabs(auto_cov[3 * i + j]) > eps);
+      for (int k = 0; k < nlag; k++) {
+        if (k < nzp) c[k] = zero ? 0.0 : (double)(float)auto_cov[9 * k + 3 * i + j];
+        if (k < nlag - 1 && nzp - k - 1 >= 0 && nzp - k - 1 < nzp)
+          c[nzp - k - 1] = zero ? 0.0 : (double)(float)auto_cov[9 * (k + 1) + 3 * j + i];
+      }
+    }
+  // MakeCircAutoCovPosDef (:622-720): per frequency, D^-1 C(f) D^-1 with D the lag-0 standard
+  // deviations, its eigenvalues replaced by their absolute values, scaled back, inverse
+  // transformed and divided by nzp
+  const int nh = nzp / 2 + 1;
+  std::vector<std::vector<cd>> F(9);
+  for (int q = 0; q < 9; q++) F[q] = dft(circ[q]);
+  double dstd[3];
+  for (int i = 0; i < 3; i++) {
+    if (!(circ[4 * i][0] > 0)) return fail(CRAVA_EINVAL, "auto-covariance with a non-positive lag-0 variance");
+    dstd[i] = std::sqrt(circ[4 * i][0]);
+  }
+  for (int f = 0; f < nh; f++) {
+    cd A[kMaxTheta][kMaxTheta], U[kMaxTheta][kMaxTheta];
+    double lam[kMaxTheta];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) A[i][j] = F[3 * i + j][f] / (dstd[i] * dstd[j]);
+    for (int i = 0; i < 3; i++)   // the Hermitian part (exact for a consistent estimate)
+      for (int j = 0; j <= i; j++) {
+        const cd h = 0.5 * (A[i][j] + std::conj(A[j][i]));
+        A[i][j] = h;
+        A[j][i] = std::conj(h);
+      }
+    herm_eig(3, A, lam, U);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        cd acc = 0;
+        for (int m = 0; m < 3; m++) acc += U[i][m] * std::fabs(lam[m]) * std::conj(U[j][m]);
+        F[3 * i + j][f] = acc * (dstd[i] * dstd[j]);
+      }
+  }
+  // TaperCircAutoCovFunction (:722-757): Gaussian taper of 50 ms standard deviation (at most
+  // nzp / 2 samples), cut below 1e-10
+  double sd = 50.0 / dz;
+  if (sd > nzp / 2.0) sd = nzp / 2.0;
+  const int pairs[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+  for (int g = 0; g < 6; g++) {
+    const std::vector<cd>& X = F[3 * pairs[g][0] + pairs[g][1]];
+    for (int t = 0; t < nzp; t++) {
+      double acc = X[0].real();
+      for (int k = 1; k < nh; k++) {
+        const double ang = 2.0 * M_PI * (double)((long long)k * t % nzp) / nzp;
+        const double w = (2 * k == nzp) ? 1.0 : 2.0;
+        acc += w * (X[k].real() * std::cos(ang) - X[k].imag() * std::sin(ang));
+      }
+      const int m = t < nzp / 2 + 1 ? t : nzp - t;
+      const double e = std::exp(-0.5 * std::pow((double)(float)m / sd, 2));
+      const double taper = e > 1e-10 ? (double)(float)e : 0.0;
+      out[(size_t)g * nzp + t] = (float)(acc / nzp * taper);
+    }
+  }
+  return CRAVA_OK;
+}
+
 crava_status crava_tuning_set(const char* key, int n, int value) {
   if (!key || !*key) return fail(CRAVA_EINVAL, "null schedule key");
   std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -992,9 +1156,35 @@ crava_status crava_ctx_create(crava_ctx** ctx, int device, size_t hbm_budget) {
 crava_status crava_ctx_destroy(crava_ctx* ctx) {
   if (!ctx) return CRAVA_OK;
   cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
   for (auto& kv : ctx->plans) cudaFree(kv.second.tw);
   if (ctx->stage) cudaFree(ctx->stage);
+  for (auto& kv : ctx->cache) {
+    if (kv.second->ready) cudaEventDestroy(kv.second->ready);
+    cudaFree(kv.second->mem);
+    delete kv.second;
+  }
   delete ctx;
+  return CRAVA_OK;
+}
+
+crava_status crava_ctx_set_table_cache(crava_ctx* ctx, size_t max_bytes) {
+  if (!ctx) return fail(CRAVA_EINVAL, "null context");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> lk(ctx->cache_mu);
+  ctx->cache_max = max_bytes;
+  cache_evict_locked(ctx, 0, 0);   // unreferenced entries above the new limit
+  return CRAVA_OK;
+}
+
+crava_status crava_ctx_table_cache_stats(crava_ctx* ctx, long long* hits, long long* misses, size_t* bytes,
+                                         int* entries) {
+  if (!ctx) return fail(CRAVA_EINVAL, "null context");
+  std::lock_guard<std::mutex> lk(ctx->cache_mu);
+  if (hits) *hits = ctx->cache_hits;
+  if (misses) *misses = ctx->cache_misses;
+  if (bytes) *bytes = ctx->cache_bytes;
+  if (entries) *entries = (int)ctx->cache.size();
   return CRAVA_OK;
 }
 
@@ -1045,8 +1235,16 @@ crava_status crava_job_footprint(const crava_job_desc* desc, size_t* bytes) {
 
 namespace {
 
+void cache_release(crava_ctx* ctx, CacheEntry* e) {
+  if (!e) return;
+  std::lock_guard<std::mutex> lk(ctx->cache_mu);
+  e->refs--;
+}
+
 void job_release(crava_job* j) {
   if (!j) return;
+  cache_release(j->ctx, j->kz_entry);
+  cache_release(j->ctx, j->lat_entry);
   if (j->pool) {
     if (j->async) cudaFreeAsync(j->pool, j->alloc_stream);
     else cudaFree(j->pool);
@@ -1056,16 +1254,236 @@ void job_release(crava_job* j) {
   delete j;
 }
 
+// Builds the per-kz tables of model d into mem (kz_set_bytes(d) bytes) on stream st: the
+// operator tables of computePostMeanResidAndFFTCov, the separable factors (error part of Sd,
+// temporal spectrum) and the eigen tables of the in-place pencil kernel.
+crava_status kz_set_build(const crava_job_desc& d, const std::vector<double>& A, const std::vector<double>& etc,
+                          const std::vector<double>& pv, const std::vector<float>& circ, char* mem, cudaStream_t st,
+                          KzSet& k) {
+  char* p = mem;
+  auto take = [&](size_t bytes) { char* q = p; p += align256(bytes); return q; };
+  const int nth = d.ntheta;
+  k.kw = (float2*)take(sizeof(float2) * d.nzp * nth);
+  k.e1 = (float2*)take(sizeof(float2) * d.nzp * nth);
+  k.e2 = (float2*)take(sizeof(float2) * d.nzp * nth);
+  k.kwd = (double2*)take(sizeof(double2) * d.nzp * nth);
+  k.e1d = (double2*)take(sizeof(double2) * d.nzp * nth);
+  k.e2d = (double2*)take(sizeof(double2) * d.nzp * nth);
+  k.septab = (float2*)take(sizeof(float2) * d.nzp * ((size_t)nth * (nth + 1) / 2));
+  k.inv = (uint8_t*)take(d.nzp);
+  k.ct = (float2*)take(sizeof(float2) * d.nzp);
+  k.edk = (float*)take(sizeof(float) * d.nzp * nth);
+  k.eddk = (double*)take(sizeof(double) * d.nzp * nth);
+  if (eig_table_bytes(&d)) k.eig = (float4*)take(eig_table_bytes(&d));
+  std::vector<float2> kw, e1, e2;
+  std::vector<double2> kwd, e1d, e2d;
+  std::vector<uint8_t> inv;
+  std::vector<float> edk;
+  std::vector<double> eddk;
+  build_kz_tables(d, kw, e1, e2, inv, &kwd, &e1d, &e2d, edk, &eddk);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  };
+  CUDA_TRY(up(k.edk, edk.data(), sizeof(float) * edk.size()));
+  CUDA_TRY(up(k.eddk, eddk.data(), sizeof(double) * eddk.size()));
+  CUDA_TRY(up(k.kwd, kwd.data(), sizeof(double2) * kwd.size()));
+  CUDA_TRY(up(k.e1d, e1d.data(), sizeof(double2) * e1d.size()));
+  CUDA_TRY(up(k.e2d, e2d.data(), sizeof(double2) * e2d.size()));
+  CUDA_TRY(up(k.kw, kw.data(), sizeof(float2) * kw.size()));
+  CUDA_TRY(up(k.e1, e1.data(), sizeof(float2) * e1.size()));
+  CUDA_TRY(up(k.e2, e2.data(), sizeof(float2) * e2.size()));
+  CUDA_TRY(up(k.inv, inv.data(), inv.size()));
+  if (d.prior_mode != CRAVA_PRIOR_SEPARABLE) {
+    k.eig_why = "prior given as grids";
+    return CRAVA_OK;
+  }
+  // Separable prior: the error part of Sd per kz, M2 = ec o (e1 e1^H + e2 e2^H) with
+  // ec = (1 - wnc) errThetaCov / 2 (getNextErrorVariance, src/avoinversion.cpp:1236-1272),
+  // lower triangle row by row.
+  const int tri = nth * (nth + 1) / 2;
+  std::vector<float2> sep((size_t)d.nzp * tri);
+  for (int kz = 0; kz < d.nzp; kz++) {
+    float2* row = sep.data() + (size_t)kz * tri;
+    const double2* a1 = e1d.data() + (size_t)kz * nth;
+    const double2* a2 = e2d.data() + (size_t)kz * nth;
+    for (int l = 0; l < nth; l++)
+      for (int m = 0; m <= l; m++) {
+        const cd ee = cd(a1[l].x, a1[l].y) * std::conj(cd(a1[m].x, a1[m].y)) +
+                      cd(a2[l].x, a2[l].y) * std::conj(cd(a2[m].x, a2[m].y));
+        const cd m2 = ee * (0.5 * (1.0 - d.wnc) * etc[l * nth + m]);
+        row[l * (l + 1) / 2 + m] = make_float2((float)m2.real(), (float)m2.imag());
+      }
+  }
+  CUDA_TRY(up(k.septab, sep.data(), sizeof(float2) * sep.size()));
+  // temporal factor: DFT of circCorrT (1D, double); a symmetric circular correlation (the
+  // form computeCircCorrT builds, src/seismicparametersholder.cpp:624-660) has a real
+  // spectrum, whose imaginary part is then exactly zero
+  std::vector<double> c(circ.begin(), circ.end());
+  std::vector<cd> C = dft(c);
+  bool sym = true;
+  for (int t = 1; t < d.nzp && sym; t++) sym = circ[t] == circ[d.nzp - t];
+  std::vector<float2> ct(d.nzp);
+  for (int kz = 0; kz < d.nzp; kz++) ct[kz] = make_float2((float)C[kz].real(), sym ? 0.f : (float)C[kz].imag());
+  CUDA_TRY(up(k.ct, ct.data(), sizeof(float2) * d.nzp));
+  // the eigen form of the per-bin posterior (pencil.cu) where it applies
+  if (!k.eig) k.eig_why = "z length without an in-place four-step split";
+  else if (!sym) k.eig_why = "circular temporal correlation not symmetric";
+  else if (d.fp64_threshold > 0.f) k.eig_why = "FP64 re-factorisation requested";
+  else {
+    float G0[kMaxTheta][kMaxTheta], AP[kMaxTheta][3];
+    sep_constants(A, pv, nth, G0, AP);
+    std::vector<float> rows;
+    k.eig_base = build_eig_tables(d, kw, sep, edk, inv, ct, G0, AP, k.lam_limit, rows, k.n_inv_rows, k.eig_why);
+    if (k.eig_base) CUDA_TRY(up(k.eig, rows.data(), sizeof(float) * rows.size()));
+  }
+  return CRAVA_OK;
+}
+
+// Builds the lateral factor of model d into mem (lat_set_bytes(d) bytes) on stream st: the
+// 2D transform of corrXY (x then y) on the device.
+crava_status lat_set_build(crava_ctx* ctx, const crava_job_desc& d, const std::vector<float>& corr_xy, char* mem,
+                           cudaStream_t st, LatSet& l) {
+  const int cnxp = d.nxp / 2 + 1, rnxp = 2 * cnxp;
+  l.cxy = (float2*)mem;
+  l.grid = (float*)(mem + align256(sizeof(float2) * cnxp * d.nyp));
+  std::vector<float> g((size_t)rnxp * d.nyp, 0.f);
+  for (int jj = 0; jj < d.nyp; jj++)
+    for (int ii = 0; ii < d.nxp; ii++) g[(size_t)jj * rnxp + ii] = corr_xy[(size_t)jj * d.nxp + ii];
+  CUDA_TRY(cudaMemcpyAsync(l.grid, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st));
+  Plan *px, *pn, *py;
+  crava_status ps;
+  if ((ps = get_xplans(ctx, d.nxp, &px, &pn)) || (ps = get_plan(ctx, d.nyp, &py))) return ps;
+  GridSet gs;
+  gs.n = 1;
+  gs.p[0] = l.grid;
+  gs.src[0] = l.grid;
+  gs.scale[0] = 1.0f;
+  int nl = 0;
+  CUDA_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, pn->tw, st, &nl));
+  CUDA_TRY(launch_line_fft(gs, cnxp, d.nyp, (size_t)cnxp, 1, 0, py->lp, py->tw, -1.f, st, &nl));
+  CUDA_TRY(cudaMemcpyAsync(l.cxy, l.grid, sizeof(float2) * cnxp * d.nyp, cudaMemcpyDeviceToDevice, st));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+// Cache keys: the bytes every table of the entry depends on.
+template <class T>
+void key_put(std::string& k, const T* p, size_t n) {
+  if (p && n) k.append(reinterpret_cast<const char*>(p), sizeof(T) * n);
+}
+std::string kz_key(const crava_job_desc& d) {
+  std::string k = "K";
+  const int iv[6] = {d.nz, d.nzp, d.ntheta, d.prior_mode, d.flags & CRAVA_FLAG_NONCONST_THICK,
+                     d.fp64_threshold > 0.f ? 1 : 0};
+  key_put(k, iv, 6);
+  const double dv[2] = {d.lz, d.min_rel_thick};
+  key_put(k, dv, 2);
+  const float fv[3] = {d.low_cut, d.high_cut, d.wnc};
+  key_put(k, fv, 3);
+  key_put(k, d.A, 3 * (size_t)d.ntheta);
+  key_put(k, d.err_theta_cov, (size_t)d.ntheta * d.ntheta);
+  key_put(k, d.prior_var0, 9);
+  key_put(k, d.wavelet, (size_t)d.ntheta * d.nzp);
+  key_put(k, d.wavelet_norm, (size_t)d.ntheta);
+  if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) key_put(k, d.circ_corr_t, (size_t)d.nzp);
+  return k;
+}
+std::string lat_key(const crava_job_desc& d) {
+  std::string k = "L";
+  const int iv[2] = {d.nxp, d.nyp};
+  key_put(k, iv, 2);
+  key_put(k, d.corr_xy, (size_t)d.nxp * d.nyp);
+  return k;
+}
+
+// Frees unreferenced entries, least recently used first, until `want` more bytes fit under
+// both the cache limit and the context budget (or nothing is left to free).  Caller holds
+// cache_mu.
+void cache_evict_locked(crava_ctx* ctx, size_t want, cudaStream_t st) {
+  for (;;) {
+    size_t allocated;
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      allocated = ctx->allocated;
+    }
+    const bool over_cache = ctx->cache_bytes + want > ctx->cache_max;
+    const bool over_budget = ctx->budget && allocated + want > ctx->budget;
+    if (!over_cache && !over_budget) return;
+    CacheEntry* victim = nullptr;
+    for (auto& kv : ctx->cache)
+      if (kv.second->refs == 0 && (!victim || kv.second->tick < victim->tick)) victim = kv.second;
+    if (!victim) return;
+    ctx->cache.erase(victim->key);
+    ctx->cache_bytes -= victim->bytes;
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      ctx->allocated -= victim->bytes;
+    }
+    if (victim->ready) cudaEventDestroy(victim->ready);
+    cudaFreeAsync(victim->mem, st);   // no job references it: its users have completed
+    delete victim;
+  }
+}
+
+// The cached tables of `key`, built on a miss by build(mem, entry) into new device memory
+// on stream st; a hit makes st wait for the stream that built them.  The entry stays
+// referenced until cache_release.
+template <class Build>
+crava_status cache_acquire(crava_ctx* ctx, const std::string& key, size_t bytes, cudaStream_t st, Build build,
+                           CacheEntry** out) {
+  std::lock_guard<std::mutex> lk(ctx->cache_mu);
+  auto it = ctx->cache.find(key);
+  if (it != ctx->cache.end()) {
+    CacheEntry* e = it->second;
+    e->refs++;
+    e->tick = ++ctx->cache_tick;
+    ctx->cache_hits++;
+    if (e->ready) CUDA_TRY(cudaStreamWaitEvent(st, e->ready, 0));
+    *out = e;
+    return CRAVA_OK;
+  }
+  ctx->cache_misses++;
+  cache_evict_locked(ctx, bytes, st);
+  {
+    std::lock_guard<std::mutex> lk2(ctx->mu);
+    if (ctx->budget && ctx->allocated + bytes > ctx->budget)
+      return fail(CRAVA_ENOMEM, "table cache entry of " + std::to_string(bytes) + " bytes exceeds the budget");
+    ctx->allocated += bytes;
+  }
+  CacheEntry* e = new CacheEntry();
+  e->key = key;
+  e->bytes = bytes;
+  cudaError_t ce = cudaMallocAsync((void**)&e->mem, bytes, st);
+  crava_status s = ce == cudaSuccess ? build(e->mem, *e) : fail(CRAVA_ENOMEM, "table cache allocation");
+  if (!s && cudaEventCreateWithFlags(&e->ready, cudaEventDisableTiming) != cudaSuccess) s = CRAVA_ECUDA;
+  if (!s && cudaEventRecord(e->ready, st) != cudaSuccess) s = CRAVA_ECUDA;
+  if (s) {
+    if (e->mem) cudaFreeAsync(e->mem, st);
+    if (e->ready) cudaEventDestroy(e->ready);
+    std::lock_guard<std::mutex> lk2(ctx->mu);
+    ctx->allocated -= bytes;
+    delete e;
+    return s;
+  }
+  e->refs = 1;
+  e->tick = ++ctx->cache_tick;
+  ctx->cache[key] = e;
+  ctx->cache_bytes += bytes;
+  *out = e;
+  return CRAVA_OK;
+}
+
 // Job set-up on stream st.  async: the pool comes from the stream-ordered allocator and
 // nothing waits for the GPU (the serving loop); otherwise the call returns with the job
-// ready (the public crava_job_create).
+// ready (the public crava_job_create).  With the context's table cache on, the per-kz and
+// lateral tables are shared entries of the cache instead of parts of the job's pool.
 crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStream_t st, bool async,
                              crava_job** job) {
   if (!ctx || !job) return fail(CRAVA_EINVAL, "null argument");
   crava_status s = validate(desc);
   if (s) return s;
   CUDA_TRY(cudaSetDevice(ctx->device));
-  size_t need = footprint(desc);
   crava_job* j = new crava_job();
   j->ctx = ctx;
   j->d = *desc;
@@ -1097,14 +1515,27 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->d.circ_corr_t = j->circ.empty() ? nullptr : j->circ.data();
   j->d.rel_thick = j->relt.empty() ? nullptr : j->relt.data();
 
+  bool cached;
   {
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    if (ctx->budget && ctx->allocated + need > ctx->budget) {
-      size_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
-      delete j;
-      return fail(CRAVA_ENOMEM, "job needs " + std::to_string(need) + " bytes; budget left " + std::to_string(left));
+    std::lock_guard<std::mutex> lk(ctx->cache_mu);
+    cached = ctx->cache_max > 0;
+  }
+  const size_t need = grid_part_bytes(&d) + (cached ? 0 : kz_set_bytes(&d) + lat_set_bytes(&d));
+  for (int attempt = 0;; attempt++) {
+    std::unique_lock<std::mutex> lk(ctx->mu);
+    if (!ctx->budget || ctx->allocated + need <= ctx->budget) {
+      ctx->allocated += need;
+      break;
     }
-    ctx->allocated += need;
+    const size_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
+    lk.unlock();
+    if (attempt == 0) {   // unreferenced cached tables give way to a job
+      std::lock_guard<std::mutex> ck(ctx->cache_mu);
+      cache_evict_locked(ctx, need, st);
+      continue;
+    }
+    delete j;
+    return fail(CRAVA_ENOMEM, "job needs " + std::to_string(need) + " bytes; budget left " + std::to_string(left));
   }
   j->async = async;
   j->alloc_stream = st;
@@ -1132,27 +1563,15 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     for (int q = 0; q < 6; q++) j->in_cov[q] = (float*)take(gb);
     j->in_err = (float*)take(gb);
     j->err = (float*)take(gb);
+    j->fill_xy = (float*)take(sizeof(float) * j->rnxp * d.nyp);
+    j->fill_t = (float*)take(sizeof(float) * d.nzp);
   }
   for (int q = 0; q < 3 * d.nsim; q++) j->sim[q] = (float*)take(gb);
   if (d.flags & CRAVA_FLAG_HOST_NOISE)
     for (int q = 0; q < 3 * d.nsim; q++) j->noise[q] = (float*)take(gb);
-  j->kw = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
-  j->e1 = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
-  j->e2 = (float2*)take(sizeof(float2) * d.nzp * d.ntheta);
-  j->kwd = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
-  j->e1d = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
-  j->e2d = (double2*)take(sizeof(double2) * d.nzp * d.ntheta);
-  j->septab = (float2*)take(sizeof(float2) * d.nzp * ((size_t)d.ntheta * (d.ntheta + 1) / 2));
-  j->inv = (uint8_t*)take(d.nzp);
-  j->cxy = (float2*)take(sizeof(float2) * j->cnxp * d.nyp);
-  j->ct = (float2*)take(sizeof(float2) * d.nzp);
-  j->cxy_grid = (float*)take(sizeof(float) * j->rnxp * d.nyp);
   j->counters = (unsigned long long*)take(256);
-  if (eig_table_bytes(&d)) j->eig = (float4*)take(eig_table_bytes(&d));
   ThickTables tt;
   const bool nonconst = (d.flags & CRAVA_FLAG_NONCONST_THICK) != 0;
-  j->edk = (float*)take(sizeof(float) * d.nzp * d.ntheta);
-  j->eddk = (double*)take(sizeof(double) * d.nzp * d.ntheta);
   if (nonconst) {
     const size_t nth = d.ntheta, cn = d.nzp / 2 + 1, nxy = (size_t)d.nx * d.ny;
     ThickParams& tp = j->tp;
@@ -1209,19 +1628,17 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
       return st_;                                              \
     }                                                          \
   } while (0)
-
-  // per-kz tables
-  std::vector<float2> kw, e1, e2;
-  std::vector<double2> kwd, e1d, e2d;
-  std::vector<uint8_t> inv;
-  std::vector<float> edk;
-  std::vector<double> eddk;
-  build_kz_tables(j->d, kw, e1, e2, inv, &kwd, &e1d, &e2d, edk, &eddk);
+#define JOB_STATUS(call)                                       \
+  do {                                                         \
+    crava_status s_ = (call);                                  \
+    if (s_) {                                                  \
+      job_release(j);                                          \
+      return s_;                                               \
+    }                                                          \
+  } while (0)
   auto up = [&](const void* dst, const void* src, size_t bytes) {
     return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
   };
-  JOB_TRY(up(j->edk, edk.data(), sizeof(float) * edk.size()));
-  JOB_TRY(up(j->eddk, eddk.data(), sizeof(double) * eddk.size()));
   if (nonconst) {
     ThickParams& tp = j->tp;
     JOB_TRY(up(tp.wamp, tt.wamp.data(), sizeof(float2) * tt.wamp.size()));
@@ -1236,83 +1653,48 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
     JOB_TRY(up(tp.disty, tt.disty.data(), sizeof(float) * tt.disty.size()));
     JOB_TRY(up(tp.rel_thick, j->relt.data(), sizeof(double) * j->relt.size()));
   }
-  JOB_TRY(cudaMemcpyAsync(j->kwd, kwd.data(), sizeof(double2) * kwd.size(), cudaMemcpyHostToDevice, st));
-  JOB_TRY(cudaMemcpyAsync(j->e1d, e1d.data(), sizeof(double2) * e1d.size(), cudaMemcpyHostToDevice, st));
-  JOB_TRY(cudaMemcpyAsync(j->e2d, e2d.data(), sizeof(double2) * e2d.size(), cudaMemcpyHostToDevice, st));
-  JOB_TRY(cudaMemcpyAsync(j->kw, kw.data(), sizeof(float2) * kw.size(), cudaMemcpyHostToDevice, st));
-  JOB_TRY(cudaMemcpyAsync(j->e1, e1.data(), sizeof(float2) * e1.size(), cudaMemcpyHostToDevice, st));
-  JOB_TRY(cudaMemcpyAsync(j->e2, e2.data(), sizeof(float2) * e2.size(), cudaMemcpyHostToDevice, st));
-  JOB_TRY(cudaMemcpyAsync(j->inv, inv.data(), inv.size(), cudaMemcpyHostToDevice, st));
-  if (d.prior_mode == CRAVA_PRIOR_SEPARABLE) {
-    // Separable prior: the error part of Sd per kz, M2 = ec o (e1 e1^H + e2 e2^H) with
-    // ec = (1 - wnc) errThetaCov / 2 (getNextErrorVariance, src/avoinversion.cpp:1236-1272),
-    // lower triangle row by row.
-    const int nth = d.ntheta, tri = nth * (nth + 1) / 2;
-    std::vector<float2> sep((size_t)d.nzp * tri);
-    for (int k = 0; k < d.nzp; k++) {
-      float2* row = sep.data() + (size_t)k * tri;
-      const double2* a1 = e1d.data() + (size_t)k * nth;
-      const double2* a2 = e2d.data() + (size_t)k * nth;
-      for (int l = 0; l < nth; l++)
-        for (int m = 0; m <= l; m++) {
-          const cd ee = cd(a1[l].x, a1[l].y) * std::conj(cd(a1[m].x, a1[m].y)) +
-                        cd(a2[l].x, a2[l].y) * std::conj(cd(a2[m].x, a2[m].y));
-          const cd m2 = ee * (0.5 * (1.0 - d.wnc) * j->etc[l * nth + m]);
-          row[l * (l + 1) / 2 + m] = make_float2((float)m2.real(), (float)m2.imag());
-        }
+  // per-kz and lateral tables: entries of the resident cache, or parts of the pool
+  KzSet ks;
+  LatSet ls;
+  const bool sepmode = d.prior_mode == CRAVA_PRIOR_SEPARABLE;
+  if (cached) {
+    JOB_STATUS(cache_acquire(ctx, kz_key(d), kz_set_bytes(&d), st,
+                             [&](char* mem, CacheEntry& ce) {
+                               return kz_set_build(d, j->A, j->etc, j->pv, j->circ, mem, st, ce.k);
+                             },
+                             &j->kz_entry));
+    ks = j->kz_entry->k;
+    if (sepmode) {
+      JOB_STATUS(cache_acquire(ctx, lat_key(d), lat_set_bytes(&d), st,
+                               [&](char* mem, CacheEntry& ce) { return lat_set_build(ctx, d, j->corr_xy, mem, st, ce.l); },
+                               &j->lat_entry));
+      ls = j->lat_entry->l;
     }
-    JOB_TRY(cudaMemcpyAsync(j->septab, sep.data(), sizeof(float2) * sep.size(), cudaMemcpyHostToDevice, st));
-    // temporal factor: DFT of circCorrT (1D, double); a symmetric circular correlation (the
-    // form computeCircCorrT builds, src/seismicparametersholder.cpp:624-660) has a real
-    // spectrum, whose imaginary part is then exactly zero
-    std::vector<double> c(j->circ.begin(), j->circ.end());
-    std::vector<cd> C = dft(c);
-    bool sym = true;
-    for (int t = 1; t < d.nzp && sym; t++) sym = j->circ[t] == j->circ[d.nzp - t];
-    std::vector<float2> ct(d.nzp);
-    for (int k = 0; k < d.nzp; k++) ct[k] = make_float2((float)C[k].real(), sym ? 0.f : (float)C[k].imag());
-    JOB_TRY(cudaMemcpyAsync(j->ct, ct.data(), sizeof(float2) * d.nzp, cudaMemcpyHostToDevice, st));
-    // the eigen form of the per-bin posterior (pencil.cu) where it applies
-    if (!j->eig) j->eig_why = "z length without an in-place four-step split";
-    else if (!sym) j->eig_why = "circular temporal correlation not symmetric";
-    else if (d.fp64_threshold > 0.f) j->eig_why = "FP64 re-factorisation requested";
-    else {
-      float G0[kMaxTheta][kMaxTheta], AP[kMaxTheta][3];
-      sep_constants(j->A, j->pv, nth, G0, AP);
-      double lam_max = 0;
-      for (float v : j->corr_xy) lam_max += std::fabs((double)v);
-      std::vector<float> rows;
-      j->eig_ok = build_eig_tables(d, kw, sep, edk, inv, ct, G0, AP, lam_max, rows, j->n_inv_rows, j->eig_why);
-      if (j->eig_ok)
-        JOB_TRY(cudaMemcpyAsync(j->eig, rows.data(), sizeof(float) * rows.size(), cudaMemcpyHostToDevice, st));
+  } else {
+    char* km = take(kz_set_bytes(&d));
+    JOB_STATUS(kz_set_build(d, j->A, j->etc, j->pv, j->circ, km, st, ks));
+    if (sepmode) {
+      char* lm = take(lat_set_bytes(&d));
+      JOB_STATUS(lat_set_build(ctx, d, j->corr_xy, lm, st, ls));
     }
-    // lateral factor: 2D transform of corrXY on the device (x then y)
-    std::vector<float> g((size_t)j->rnxp * d.nyp, 0.f);
-    for (int jj = 0; jj < d.nyp; jj++)
-      for (int ii = 0; ii < d.nxp; ii++) g[(size_t)jj * j->rnxp + ii] = j->corr_xy[(size_t)jj * d.nxp + ii];
-    JOB_TRY(cudaMemcpyAsync(j->cxy_grid, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st));
-    Plan *px, *pn, *py;
-    crava_status ps;
-    if ((ps = get_xplans(ctx, d.nxp, &px, &pn)) || (ps = get_plan(ctx, d.nyp, &py))) {
-      job_release(j);
-      return ps;
-    }
-    GridSet gs;
-    gs.n = 1;
-    gs.p[0] = j->cxy_grid;
-    gs.src[0] = j->cxy_grid;
-    gs.scale[0] = 1.0f;
-    int nl = 0;
-    JOB_TRY(launch_x_r2c(gs, d.nxp, d.nyp, px->lp, px->tw, pn->tw, st, &nl));
-    JOB_TRY(launch_line_fft(gs, j->cnxp, d.nyp, (size_t)j->cnxp, 1, 0, py->lp, py->tw, -1.f, st, &nl));
-    JOB_TRY(cudaMemcpyAsync(j->cxy, j->cxy_grid, sizeof(float2) * j->cnxp * d.nyp, cudaMemcpyDeviceToDevice, st));
-    {
-      std::lock_guard<std::mutex> lk(ctx->mu);
-      ctx->launches += nl;
-    }
+  }
+  j->kw = ks.kw; j->e1 = ks.e1; j->e2 = ks.e2;
+  j->kwd = ks.kwd; j->e1d = ks.e1d; j->e2d = ks.e2d;
+  j->septab = ks.septab; j->inv = ks.inv; j->ct = ks.ct;
+  j->edk = ks.edk; j->eddk = ks.eddk; j->eig = ks.eig;
+  j->cxy = ls.cxy; j->cxy_grid = ls.grid;
+  j->n_inv_rows = ks.n_inv_rows;
+  j->eig_why = ks.eig_why;
+  if (ks.eig_base) {
+    // the eigen form needs every reference Cholesky of the block clear of its pivot test
+    double lam_max = 0;
+    for (float v : j->corr_xy) lam_max += std::fabs((double)v);
+    j->eig_ok = lam_max < ks.lam_limit;
+    if (!j->eig_ok) j->eig_why = "data covariance too close to singular";
   }
   if (!async) JOB_TRY(cudaStreamSynchronize(st));
 #undef JOB_TRY
+#undef JOB_STATUS
   *job = j;
   return CRAVA_OK;
 }
@@ -1540,7 +1922,166 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out) {
   return CRAVA_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Real symmetric n x n eigen-decomposition in double (herm_eig on a real matrix keeps its
+// eigenvectors real), eigenvalues in descending order, each eigenvector's largest-magnitude
+// component positive.
+void sym_eig_sorted(int n, const double* a, double* w, double* v /* n x n, column i = vector i */) {
+  cd A[kMaxTheta][kMaxTheta], U[kMaxTheta][kMaxTheta];
+  double lam[kMaxTheta];
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < n; k++) A[i][k] = cd(0.5 * (a[i * n + k] + a[k * n + i]), 0);
+  herm_eig(n, A, lam, U);
+  std::vector<int> idx(n);
+  for (int i = 0; i < n; i++) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] > lam[y]; });
+  for (int c = 0; c < n; c++) {
+    const int src = idx[c];
+    w[c] = lam[src];
+    int big = 0;
+    for (int r = 1; r < n; r++)
+      if (std::fabs(U[r][src].real()) > std::fabs(U[big][src].real())) big = r;
+    const double sg = U[big][src].real() < 0 ? -1.0 : 1.0;
+    for (int r = 0; r < n; r++) v[r * n + c] = sg * U[r][src].real();
+  }
+}
+
+// f(A) = V diag(f(w)) V^T of a real symmetric n x n matrix.
+template <class F>
+std::vector<double> sym_fun(int n, const double* a, F f) {
+  std::vector<double> w(n), v((size_t)n * n), r((size_t)n * n, 0.0);
+  sym_eig_sorted(n, a, w.data(), v.data());
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < n; k++)
+      for (int c = 0; c < n; c++) r[i * n + k] += v[i * n + c] * f(w[c]) * v[k * n + c];
+  return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_job_local_noise(crava_job* job, const float* scales, void* stream) {
+  if (!job || !scales) return fail(CRAVA_EINVAL, "null argument");
+  if (!job->ran) return fail(CRAVA_ESTATE, "crava_job_local_noise follows crava_job_run");
+  const crava_job_desc& d = job->d;
+  const int n = d.ntheta;
+  const size_t nxy = (size_t)d.nx * d.ny;
+  std::vector<double> inv_min(n);
+  for (int l = 0; l < n; l++) {
+    double mn = INFINITY;
+    for (size_t q = 0; q < nxy; q++) {
+      const float v = scales[(size_t)l * nxy + q];
+      if (!(v > 0.f) || !std::isfinite(v)) return fail(CRAVA_EINVAL, "local noise scales must be finite and > 0");
+      mn = std::min(mn, (double)v);
+    }
+    inv_min[l] = 1.0 / mn;
+  }
+  crava_ctx* ctx = job->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  crava_counters c;
+  crava_status s = crava_job_counters(job, &c);
+  if (s) return s;
+  // job constants (AVOInversion::computeG, src/avoinversion.cpp:1943-2026, and the
+  // trace-independent parts of newPosteriorCovPointwise / correctVpVsRho)
+  double Sm[9], Smd[9], Sdel[9];
+  for (int q = 0; q < 9; q++) {
+    Sm[q] = job->pv[q];
+    Smd[q] = c.post_var0[q];
+    Sdel[q] = Sm[q] - Smd[q];
+  }
+  std::vector<double> SdelP = sym_fun(3, Sdel, [](double w) { return w > 0.0 ? w : 0.0; });
+  std::vector<double> Sinv = sym_fun(3, Sm, [](double w) { return w > 1e-7 ? 1.0 / std::sqrt(w) : 0.0; });
+  double Am[9] = {0};
+  for (int i = 0; i < 3; i++)
+    for (int k = 0; k < 3; k++)
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) Am[i * 3 + k] += Sinv[i * 3 + a] * SdelP[a * 3 + b] * Sinv[b * 3 + k];
+  double ew[3], ev[9];
+  sym_eig_sorted(3, Am, ew, ev);   // NRLib::Sort3x3: descending
+  double lg[3] = {0, 0, 0};
+  for (int i = 0; i < std::min(n, 3); i++)
+    if (ew[i] > 0) lg[i] = std::sqrt(ew[i] / (1.0 - ew[i]));
+  std::vector<double> Sth(job->etc.begin(), job->etc.end());
+  std::vector<double> S12 = sym_fun(n, Sth.data(), [](double w) { return w > 0.0 ? std::sqrt(w) : 0.0; });
+  // G = SigmaTheta^1/2 Lg Evec^T Sinv  (n x 3); Lg is n x 3 with Lg(i, i) = lg_i
+  std::vector<double> G((size_t)n * 3, 0.0);
+  for (int r = 0; r < n; r++)
+    for (int k = 0; k < 3; k++) {
+      double t = 0;
+      for (int i = 0; i < std::min(n, 3); i++) {
+        double et = 0;   // (Evec^T Sinv)_ik
+        for (int a = 0; a < 3; a++) et += ev[a * 3 + i] * Sinv[a * 3 + k];
+        t += S12[r * n + i] * lg[i] * et;
+      }
+      G[r * 3 + k] = t;
+    }
+  LocalNoiseParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.nx = d.nx; P.ny = d.ny; P.nz = d.nz; P.nyp = d.nyp; P.rnxp = job->rnxp;
+  P.nth = n; P.nsim = d.nsim;
+  for (int l = 0; l < n; l++) P.inv_min[l] = inv_min[l];
+  for (int r = 0; r < n; r++) {
+    for (int k = 0; k < 3; k++) {
+      double t = 0;
+      for (int a = 0; a < 3; a++) t += G[r * 3 + a] * Sm[a * 3 + k];
+      P.b[r][k] = t;
+    }
+    for (int m = 0; m < n; m++) P.sth[r][m] = Sth[r * n + m];
+  }
+  for (int r = 0; r < n; r++)
+    for (int m = 0; m < n; m++) {
+      double t = 0;
+      for (int k = 0; k < 3; k++) t += P.b[r][k] * G[m * 3 + k];
+      P.gsg[r][m] = t;
+    }
+  std::vector<double> sdel = sym_fun(3, Sdel, [](double w) { return w > 1e-7 ? 1.0 / std::sqrt(w) : 0.0; });
+  std::vector<double> smdi = sym_fun(3, Smd, [](double w) { return w > 0.0 ? 1.0 / std::sqrt(w) : 0.0; });
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      P.sm[a][b] = Sm[a * 3 + b];
+      P.sdel[a][b] = sdel[a * 3 + b];
+      P.smdi[a][b] = smdi[a * 3 + b];
+    }
+  for (int a = 0; a < 3; a++) {
+    P.prior_mean[a] = job->in_mean[a];
+    P.post[a] = job->mean[a];
+  }
+  for (int q = 0; q < 3 * d.nsim; q++) P.sim[q] = job->sim[q];
+  float* dscale = nullptr;
+  CUDA_TRY(cudaMallocAsync((void**)&dscale, sizeof(float) * n * nxy, st));
+  P.scale = dscale;
+  cudaError_t e = cudaMemcpyAsync(dscale, scales, sizeof(float) * n * nxy, cudaMemcpyHostToDevice, st);
+  int nl = 0;
+  if (e == cudaSuccess) e = launch_local_noise(P, st, &nl);
+  cudaFreeAsync(dscale, st);
+  if (e != cudaSuccess) return cuda_fail(e, "local noise correction");
+  CUDA_TRY(cudaStreamSynchronize(st));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+static crava_status fill_prior_impl(crava_job* job, const float* act_host, float corr_grad_i, float corr_grad_j,
+                                    void* stream);
+
 crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_grad_j, void* stream) {
+  return fill_prior_impl(job, nullptr, corr_grad_i, corr_grad_j, stream);
+}
+
+crava_status crava_job_fill_prior_auto_cov(crava_job* job, const float* circ_auto_cov, float corr_grad_i,
+                                           float corr_grad_j, void* stream) {
+  if (!circ_auto_cov) return fail(CRAVA_EINVAL, "null auto-covariance");
+  return fill_prior_impl(job, circ_auto_cov, corr_grad_i, corr_grad_j, stream);
+}
+
+static crava_status fill_prior_impl(crava_job* job, const float* act_host, float corr_grad_i, float corr_grad_j,
+                                    void* stream) {
   if (!job) return fail(CRAVA_EINVAL, "null job");
   const crava_job_desc& d = job->d;
   if (d.prior_mode != CRAVA_PRIOR_GRIDS)
@@ -1552,9 +2093,8 @@ crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_
   crava_ctx* ctx = job->ctx;
   cudaStream_t st = (cudaStream_t)stream;
   CUDA_TRY(cudaSetDevice(ctx->device));
-  // corrXY and circCorrT into buffers that only SEPARABLE jobs use otherwise
-  float* cxy = job->cxy_grid;
-  float* ct = reinterpret_cast<float*>(job->ct);
+  float* cxy = job->fill_xy;
+  float* ct = job->fill_t;
   CUDA_TRY(cudaMemcpyAsync(cxy, job->corr_xy.data(), sizeof(float) * job->corr_xy.size(), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(ct, job->circ.data(), sizeof(float) * job->circ.size(), cudaMemcpyHostToDevice, st));
   PriorFill P;
@@ -1566,6 +2106,15 @@ crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_
   P.err = job->in_err;
   P.cxy = cxy;
   P.ct = ct;
+  P.act = nullptr;
+  float* dact = nullptr;
+  if (act_host) {
+    for (size_t q = 0; q < 6 * (size_t)d.nzp; q++)
+      if (!std::isfinite(act_host[q])) return fail(CRAVA_ENUMERIC, "non-finite auto-covariance");
+    CUDA_TRY(cudaMallocAsync((void**)&dact, sizeof(float) * 6 * d.nzp, st));
+    CUDA_TRY(cudaMemcpyAsync(dact, act_host, sizeof(float) * 6 * d.nzp, cudaMemcpyHostToDevice, st));
+    P.act = dact;
+  }
   P.gi = corr_grad_i;
   P.gj = corr_grad_j;
   P.nxp = d.nxp;
@@ -1573,7 +2122,9 @@ crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_
   P.nzp = d.nzp;
   P.rnxp = job->rnxp;
   int nl = 0;
-  CUDA_TRY(launch_fill_prior(P, st, &nl));
+  cudaError_t fe = launch_fill_prior(P, st, &nl);
+  if (dact) cudaFreeAsync(dact, st);
+  if (fe != cudaSuccess) return cuda_fail(fe, "launch_fill_prior");
   // the host vectors stay with the job; wait so that the call has the reference's
   // synchronous semantics like the uploads it replaces
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -2061,6 +2612,7 @@ struct ServeReq {
   crava_job* job = nullptr;
   int slot = -1;
   cudaEvent_t done = nullptr;
+  unsigned long long* nonfinite = nullptr;  // pinned host word the job's counter is copied to
 };
 
 }  // namespace
@@ -2079,29 +2631,38 @@ struct crava_server {
   std::vector<ServeReq*> inflight;
   std::map<uint64_t, ServeReq*> reqs;
   long long completed = 0;
+  unsigned long long* nf = nullptr;   // pinned, one word per stream: the job's non-finite counter
 };
 
 namespace {
 
-// Starts one request on a free stream; returns false when it does not fit yet.
-bool serve_admit(crava_server* sv, ServeReq* r, int slot) {
+// Starts request r on stream slot `slot`: job creation (tables from the resident cache),
+// uploads, the inversion, downloads and the completion event.  Runs on the loop thread
+// without the server lock; touches only r's job fields, which no other thread reads.
+// CRAVA_ENOMEM: the job does not fit now, nothing was allocated.
+crava_status serve_admit(crava_server* sv, ServeReq* r, int slot) {
   cudaStream_t st = sv->streams[slot];
   crava_job* job = nullptr;
   crava_status s = job_create_impl(sv->ctx, &r->d, st, true, &job);
-  if (s == CRAVA_ENOMEM) return false;
-  r->t_start = now_ms();
   if (s) {
-    r->status = s;
-    r->err = crava_last_error();
-    r->state = CRAVA_REQ_FAILED;
-    return true;
+    if (s != CRAVA_ENOMEM) r->err = crava_last_error();
+    return s;
   }
+  // the job holds its own copies of the description's arrays now
+  r->A = {}; r->etc = {}; r->pv = {}; r->wav = {}; r->wn = {}; r->cxy = {}; r->circ = {};
   r->job = job;
   r->slot = slot;
   const int nth = r->d.ntheta;
   for (int l = 0; l < nth && !s; l++) s = crava_job_upload(job, CRAVA_ROLE_DATA, l, r->in[l], st);
   for (int a = 0; a < 3 && !s; a++) s = crava_job_upload(job, CRAVA_ROLE_MEAN, a, r->in[nth + a], st);
   if (!s) s = crava_job_run(job, st);
+  if (!s) {
+    sv->nf[slot] = 0;
+    r->nonfinite = sv->nf + slot;
+    if (cudaMemcpyAsync(r->nonfinite, job->counters + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) !=
+        cudaSuccess)
+      s = CRAVA_ECUDA;
+  }
   for (size_t q = 0; q < r->out.size() && !s; q++) {
     if (!r->out[q]) continue;
     if (q < 3) s = crava_job_download(job, CRAVA_ROLE_POST_MEAN, (int)q, r->out[q], st);
@@ -2111,18 +2672,15 @@ bool serve_admit(crava_server* sv, ServeReq* r, int slot) {
   if (!s && cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) s = CRAVA_ECUDA;
   if (!s && cudaEventRecord(r->done, st) != cudaSuccess) s = CRAVA_ECUDA;
   if (s) {
-    r->status = s;
     r->err = crava_last_error();
-    r->state = CRAVA_REQ_FAILED;
     cudaStreamSynchronize(st);
+    if (r->done) cudaEventDestroy(r->done);
+    r->done = nullptr;
     job_release(job);
     r->job = nullptr;
-    return true;
+    if (s == CRAVA_ENOMEM) s = CRAVA_ECUDA;   // a failure after admission is not a retry
   }
-  r->state = CRAVA_REQ_RUNNING;
-  sv->busy[slot] = 1;
-  sv->inflight.push_back(r);
-  return true;
+  return s;
 }
 
 void serve_loop(crava_server* sv) {
@@ -2136,41 +2694,60 @@ void serve_loop(crava_server* sv) {
       cudaError_t q = cudaEventQuery(r->done);
       if (q == cudaErrorNotReady) { i++; continue; }
       r->t_done = now_ms();
-      if (q != cudaSuccess) {
-        r->status = CRAVA_ECUDA;
-        r->err = cudaGetErrorString(q);
-        r->state = CRAVA_REQ_FAILED;
-      } else {
-        r->state = CRAVA_REQ_DONE;
-      }
       cudaEventDestroy(r->done);
       r->done = nullptr;
       job_release(r->job);
       r->job = nullptr;
+      // a job whose data or prior-mean grids were not finite fails with CRAVA_ENUMERIC
+      if (q == cudaSuccess) {
+        r->state = CRAVA_REQ_DONE;
+        if (r->nonfinite && *r->nonfinite) {
+          r->state = CRAVA_REQ_FAILED;
+          r->status = CRAVA_ENUMERIC;
+          r->err = "the data or prior-mean grids hold non-finite values";
+        }
+      } else {
+        r->status = CRAVA_ECUDA;
+        r->err = cudaGetErrorString(q);
+        r->state = CRAVA_REQ_FAILED;
+      }
       sv->busy[r->slot] = 0;
       sv->inflight.erase(sv->inflight.begin() + i);
       sv->completed++;
       progressed = true;
     }
-    // admissions, first come first served
+    // admissions, first come first served; the set-up runs without the lock
     while (!sv->pending.empty() && (int)sv->inflight.size() < sv->max_inflight && !sv->stopping) {
       int slot = -1;
       for (int k = 0; k < (int)sv->busy.size(); k++)
         if (!sv->busy[k]) { slot = k; break; }
       if (slot < 0) break;
       ServeReq* r = sv->pending.front();
-      if (!serve_admit(sv, r, slot)) {
-        // out of memory with nothing in flight: no release will ever make room, so the
-        // request fails instead of holding the queue
-        if (!sv->inflight.empty()) break;   // waits for memory to be released
-        r->state = CRAVA_REQ_FAILED;
-        r->status = CRAVA_ENOMEM;
-        r->err = "job does not fit the device memory even with nothing else in flight";
-        r->t_start = now_ms();
-      }
       sv->pending.pop_front();
-      if (r->state == CRAVA_REQ_FAILED) r->t_done = now_ms();
+      sv->busy[slot] = 1;
+      const bool idle = sv->inflight.empty();
+      lk.unlock();
+      crava_status s = serve_admit(sv, r, slot);
+      lk.lock();
       progressed = true;
+      if (s == CRAVA_ENOMEM && !idle) {
+        // waits at the head of the queue for memory that running jobs will release
+        sv->busy[slot] = 0;
+        sv->pending.push_front(r);
+        break;
+      }
+      if (s) {
+        // out of memory with nothing in flight can never succeed: fail it, keep serving
+        sv->busy[slot] = 0;
+        r->state = CRAVA_REQ_FAILED;
+        r->status = s;
+        if (s == CRAVA_ENOMEM) r->err = "job does not fit the device memory even with nothing else in flight";
+        r->t_start = r->t_done = now_ms();
+        continue;
+      }
+      r->t_start = now_ms();
+      r->state = CRAVA_REQ_RUNNING;
+      sv->inflight.push_back(r);
     }
     if (sv->stopping) {
       for (ServeReq* r : sv->pending) {
@@ -2187,6 +2764,20 @@ void serve_loop(crava_server* sv) {
   sv->cv.notify_all();
 }
 
+// Fills info from r (caller holds the lock); a request in a final state is released.
+void serve_report(crava_server* sv, ServeReq* r, crava_request_info* info) {
+  if (info) {
+    info->state = r->state;
+    info->status = r->status;
+    info->queue_ms = (r->t_start > 0 ? r->t_start : now_ms()) - r->t_submit;
+    info->latency_ms = r->t_done > 0 ? r->t_done - r->t_submit : -1.0;
+  }
+  if (r->state == CRAVA_REQ_DONE || r->state == CRAVA_REQ_FAILED) {
+    sv->reqs.erase(r->id);
+    delete r;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -2201,9 +2792,18 @@ crava_status crava_serve_start(crava_ctx* ctx, int max_inflight, crava_server** 
     uint64_t thr = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
+  {
+    // served jobs keep their tables resident: on by default for a serving context
+    std::lock_guard<std::mutex> lk(ctx->cache_mu);
+    if (ctx->cache_max == 0) ctx->cache_max = (size_t)256 << 20;
+  }
   crava_server* sv = new crava_server();
   sv->ctx = ctx;
   sv->max_inflight = max_inflight;
+  if (cudaHostAlloc((void**)&sv->nf, sizeof(unsigned long long) * max_inflight, cudaHostAllocDefault) != cudaSuccess) {
+    delete sv;
+    return fail(CRAVA_ENOMEM, "pinned host words of the server");
+  }
   sv->streams.resize(max_inflight);
   sv->busy.assign(max_inflight, 0);
   for (auto& s : sv->streams) {
@@ -2265,12 +2865,8 @@ crava_status crava_serve_poll(crava_server* sv, uint64_t ticket, crava_request_i
   if (!sv || !info) return fail(CRAVA_EINVAL, "null argument");
   std::lock_guard<std::mutex> lk(sv->mu);
   auto it = sv->reqs.find(ticket);
-  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket");
-  const ServeReq* r = it->second;
-  info->state = r->state;
-  info->status = r->status;
-  info->queue_ms = (r->t_start > 0 ? r->t_start : now_ms()) - r->t_submit;
-  info->latency_ms = r->t_done > 0 ? r->t_done - r->t_submit : -1.0;
+  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket (or its final state was already reported)");
+  serve_report(sv, it->second, info);
   return CRAVA_OK;
 }
 
@@ -2279,16 +2875,17 @@ crava_status crava_serve_wait(crava_server* sv, uint64_t ticket, double timeout_
   const double t_end = now_ms() + timeout_ms;
   std::unique_lock<std::mutex> lk(sv->mu);
   auto it = sv->reqs.find(ticket);
-  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket");
+  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket (or its final state was already reported)");
   ServeReq* r = it->second;
   while (r->state == CRAVA_REQ_QUEUED || r->state == CRAVA_REQ_RUNNING) {
     double left = t_end - now_ms();
     if (left <= 0) return fail(CRAVA_ETIMEDOUT, "request not finished within the timeout");
     sv->cv.wait_for(lk, std::chrono::microseconds((long long)std::min(left * 1000.0, 10000.0)));
   }
-  lk.unlock();
-  if (info) crava_serve_poll(sv, ticket, info);
-  if (r->state == CRAVA_REQ_FAILED) return fail(r->status ? r->status : CRAVA_ECUDA, r->err);
+  const crava_status st = r->state == CRAVA_REQ_FAILED ? (r->status ? r->status : CRAVA_ECUDA) : CRAVA_OK;
+  const std::string err = r->err;
+  serve_report(sv, r, info);
+  if (st) return fail(st, err);
   return CRAVA_OK;
 }
 
@@ -2306,6 +2903,7 @@ crava_status crava_serve_stop(crava_server* sv) {
     cudaStreamDestroy(s);
   }
   for (auto& kv : sv->reqs) delete kv.second;
+  if (sv->nf) cudaFreeHost(sv->nf);
   delete sv;
   return CRAVA_OK;
 }
@@ -2388,6 +2986,69 @@ crava_status crava_facies_smooth(crava_ctx* ctx, const crava_facies_desc* fd, co
   cudaStreamSynchronize(st);
   cudaFree(d_sm);
   return s;
+}
+
+crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_desc* corners, int nang,
+                                           const float* const* d_density, int density_row, const float* noise_scale,
+                                           const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
+                                           float* const* d_prob, float* d_seis_lh, void* stream) {
+  if (!ctx || !corners || !d_density || !d_post || !d_prob || (nang > 0 && !noise_scale))
+    return fail(CRAVA_EINVAL, "null argument");
+  if (nang < 0 || nang > kMaxFaciesAngles) return fail(CRAVA_ENOTSUP, "local-noise angles must be 0..4");
+  const crava_facies_desc* fd = corners;
+  if (fd->nfacies < 1 || fd->nfacies > kMaxFacies) return fail(CRAVA_EINVAL, "nfacies must be 1..16");
+  if (nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny) return fail(CRAVA_EINVAL, "bad grid dimensions");
+  for (int f = 0; f <= fd->nfacies; f++)
+    if (!d_prob[f]) return fail(CRAVA_EINVAL, "null probability grid");
+  const int nc = 1 << nang;
+  FaciesCornersHost hc;
+  hc.nang = nang;
+  for (int c = 0; c < nc; c++) {
+    for (int d = 0; d < 3; d++) {
+      if (corners[c].nbins[d] < 1 || !(corners[c].dv[d] > 0)) return fail(CRAVA_EINVAL, "bad density box");
+      hc.box[c].nb[d] = corners[c].nbins[d];
+      hc.box[c].vmin[d] = corners[c].vmin[d];
+      hc.box[c].dv[d] = corners[c].dv[d];
+    }
+    if (density_row < corners[c].nbins[0]) return fail(CRAVA_EINVAL, "density row stride below the vp bin count");
+    if (!d_density[c]) return fail(CRAVA_EINVAL, "null density volume");
+    hc.box[c].rs = density_row;
+    hc.box[c].fstride = (size_t)density_row * corners[c].nbins[1] * corners[c].nbins[2];
+    hc.dens[c] = d_density[c];
+  }
+  // relative noise scale of every trace per angle (calculateFaciesProb, src/faciesprob.cpp:1961-1977)
+  const size_t nxy = (size_t)nx * ny;
+  std::vector<float> t((size_t)nang * nxy);
+  for (int a = 0; a < nang; a++) {
+    double mn = INFINITY, mx = -INFINITY;
+    for (size_t q = 0; q < nxy; q++) {
+      const double v = noise_scale[(size_t)a * nxy + q];
+      if (!std::isfinite(v)) return fail(CRAVA_ENUMERIC, "non-finite noise scale");
+      mn = std::min(mn, v);
+      mx = std::max(mx, v);
+    }
+    for (size_t q = 0; q < nxy; q++)
+      t[(size_t)a * nxy + q] = mn == mx ? 0.f : (float)(((double)noise_scale[(size_t)a * nxy + q] - mn) / (mx - mn));
+  }
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  float* dt = nullptr;
+  if (nang > 0) {
+    CUDA_TRY(cudaMallocAsync((void**)&dt, sizeof(float) * t.size(), st));
+    CUDA_TRY(cudaMemcpyAsync(dt, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice, st));
+  }
+  hc.t = dt;
+  // undefSum = p_undefined / (bins of the first density volume), as the reference
+  const float undef_sum = fd->p_undefined / (float)(fd->nbins[0] * fd->nbins[1] * fd->nbins[2]);
+  const int rnxp_in = 2 * (nxp / 2 + 1), rnxp_out = 2 * (nx / 2 + 1);
+  cudaError_t e = launch_facies_prob_corners(d_post[0], d_post[1], d_post[2], nx, ny, nz, rnxp_in, nyp, rnxp_out, hc,
+                                             fd->nfacies, fd->prior, undef_sum, d_prob, d_seis_lh, st);
+  if (dt) cudaFreeAsync(dt, st);
+  if (e != cudaSuccess) return cuda_fail(e, "launch_facies_prob_corners");
+  if (nang > 0) CUDA_TRY(cudaStreamSynchronize(st));   // the host t table
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->launches += 1;
+  return CRAVA_OK;
 }
 
 crava_status crava_facies_prob(crava_ctx* ctx, const crava_facies_desc* fd, const float* d_density, int density_row,

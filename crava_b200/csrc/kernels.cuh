@@ -86,7 +86,26 @@ struct ZParams {
 };
 constexpr int kNumCounters = 5;
 
+// Local-noise shrinkage (localnoise.cu): per-trace maps of the posterior and realisations
+// from the local noise scales; the matrices are job constants computed on the host.
+struct LocalNoiseParams {
+  int nx, ny, nz, nyp, rnxp, nth, nsim;
+  const float* scale;                 // nth x ny x nx local noise scales, index i + nx (j + ny l)
+  double inv_min[kMaxTheta];          // 1 / (smallest scale of angle l)
+  double gsg[kMaxTheta][kMaxTheta];   // G Sm G^T
+  double sth[kMaxTheta][kMaxTheta];   // SigmaTheta (errThetaCov)
+  double b[kMaxTheta][3];             // G Sm
+  double sm[3][3];                    // priorVar0
+  double sdel[3][3];                  // (Sm - Smd)^-1/2, eigenvalues <= 1e-7 dropped
+  double smdi[3][3];                  // Smd^-1/2, eigenvalues <= 0 dropped
+  const float* prior_mean[3];         // real grids (FFTGrid layout)
+  float* post[3];                     // posterior mean, corrected in place
+  float* sim[3 * kMaxSim];            // realisations, corrected in place
+};
+cudaError_t launch_local_noise(const LocalNoiseParams& P, cudaStream_t st, int* nlaunch);
+
 constexpr int kMaxFacies = 16;
+constexpr int kMaxFaciesAngles = 4;   // local-noise angles of the facies densities (16 corners)
 struct FaciesPrior { float p[kMaxFacies]; };
 struct FaciesOut { float* p[kMaxFacies + 1]; };
 struct FaciesBoxHost {
@@ -135,6 +154,8 @@ struct PriorFill {
   const float* cxy;            // nxp x nyp corrXY
   const float* ct;             // nzp circCorrT
   float pv[6];                 // float(priorVar0(a, b)) in the grid order
+  const float* act;            // estimated covariance: 6 x nzp circular auto-covariances in the
+                               // grid order (FFTGrid::FillInLateralCorr; pv unused), or null
   float gi, gj;                // correlation gradients (samples per lateral index)
   int nxp, nyp, nzp, rnxp;
 };
@@ -211,5 +232,15 @@ cudaError_t launch_facies_prob(const float* vp, const float* vs, const float* rh
                                int nf, const float* prior, float undef_sum, float* const* out, float* seis_lh,
                                cudaStream_t st);
 cudaError_t launch_spec_mul(float2* a, const float2* b, size_t n, cudaStream_t st);
+struct FaciesCornersHost {
+  int nang;
+  const float* t;                                 // device, nang x ny x nx
+  FaciesBoxHost box[1 << kMaxFaciesAngles];
+  const float* dens[1 << kMaxFaciesAngles];       // device density volume of each corner
+};
+cudaError_t launch_facies_prob_corners(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz,
+                                       int rnxp_in, int nyp_in, int rnxp_out, const FaciesCornersHost& hc, int nf,
+                                       const float* prior, float undef_sum, float* const* out, float* seis_lh,
+                                       cudaStream_t st);
 
 }  // namespace crava

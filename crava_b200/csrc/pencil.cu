@@ -1,472 +1,23 @@
-// The separable-prior pencil pass in its eigen form (sm_100a).
-//
-// Per (x-tile, y) pencil, like k_zpass (zpass.cu): forward z transform of the data and
-// prior-mean spectra, the per-bin posterior of AVOInversion::computePostMeanResidAndFFTCov
-// (src/avoinversion.cpp:944-1091), the realisations of AVOInversion::simulate
-// (src/avoinversion.cpp:1401-1511) and the inverse z transform of every output spectrum,
-// with the spectra kept on chip between the two transforms.
-//
-// The per-bin algebra.  With a separable prior whose temporal factor has a real spectrum
-// (a symmetric circular correlation, as SeismicParametersHolder::computeCircCorrT builds it,
-// src/seismicparametersholder.cpp:624-660), every bin of one kz has the data covariance
-//     Sd = lam M_k + E_k,   M_k = |ct_k| (kw kw^H) o G0 + M2_k,   E_k = diag(ed_k) > 0,
-// with lam = |Re corrXY-spectrum(i, j)| the only lateral variable, and K S = lam |ct_k|
-// diag(kw) A P0.  From the Hermitian eigen-decomposition E^-1/2 M_k E^-1/2 = U diag(Lam) U^H
-// (per kz, on the host, in double) and V = U^H E^-1/2, Q = |ct_k| V diag(kw) A P0:
-//     mu_post = mu + lam Q^H diag(1 / (lam Lam + 1)) V (d - K mu)
-//     S_post  = rho P0 - lam^2 sum_l conj(Q_la) Q_lb / (lam Lam_l + 1)
-//     resid   = d - K mu_post
-// which equals the reference's Sd^-1 regrouping exactly in exact arithmetic: a few small
-// matrix-vector products per bin instead of a per-bin Cholesky factorisation and solves.
-// Sd is positive definite for every lam >= 0 (Sd >= E_k), so the reference's Cholesky
-// never falls back here; the host checks that before it chooses this kernel.
-//
-// The z transforms run in place: the forward four-step transform leaves kz = k2 + N1 k1 at
-// position k1 + N2 k2 (no scratch buffer), the per-bin step reads its tables in that
-// position order, and the inverse transform takes that order back to natural order.  With
-// no transform scratch the tile needs (G + 3) slots of W x nzp complex values, so two CTAs
-// share an SM at nzp = 256 with one realisation per batch.
-#include <cuda_runtime.h>
-#include <stdint.h>
-
-#include "fft2.cuh"
-#include "fft_core.cuh"
-#include "kernels.cuh"
-#include "pencil_common.cuh"
+// Launcher of the eigen-form pencil pass (kernel in pencil.cuh, instantiated per z split in
+// pencil_s1.cu, pencil_s2.cu and pencil_s3.cu).
+#include "pencil.cuh"
 
 namespace crava {
-
-// ------------------------------------------------------------------ in-place z transforms
-
-// Forward transform of nl lines (line l at x + l, point p at x + l + p ps) of length
-// N1 N2, natural order in, position k1 + N2 k2 <- X[k2 + N1 k1] out.
-template <int N1, int N2>
-__device__ __forceinline__ void zfwd_inplace(float2* x, int nl, int ps, const float2* tw) {
-  const int T = blockDim.x;
-  const float rl = __frcp_rn((float)nl);
-  const int mstep = N2 * ps;
-  // pass 1, item t < N2: N1-point DFT over positions t + N2 m, twiddle w^(t k2), back to
-  // positions t + N2 k2
-  for (int q = threadIdx.x; q < nl * N2; q += T) {
-    int l;
-    const int t = fdivmod(q, nl, rl, l);
-    float2* y = x + l + t * ps;
-    four_step_pass1<N1, N2, -1>(
-        t, tw, [&](int, int m) { return y[m * mstep]; }, [&](int, int k2, float2 v) { y[k2 * mstep] = v; });
-  }
-  __syncthreads();
-  // pass 2, item k2 < N1: N2-point DFT over the run t + N2 k2 (t < N2), X[k2 + N1 k1] back to
-  // position k1 + N2 k2
-  for (int q = threadIdx.x; q < nl * N1; q += T) {
-    int l;
-    const int k2 = fdivmod(q, nl, rl, l);
-    float2* y = x + l + k2 * mstep;
-    float2 v[N2];
-#pragma unroll
-    for (int t = 0; t < N2; t++) v[t] = y[t * ps];
-    Dft<N2>::run(v, -1.f);
-#pragma unroll
-    for (int k1 = 0; k1 < N2; k1++) y[k1 * ps] = v[k1];
-  }
-  __syncthreads();
-}
-
-// Inverse transform (unnormalised, e^{+2 pi i}) of nl lines holding X[k2 + N1 k1] at position
-// k1 + N2 k2; natural order out:
-//   x[t + N2 m] = sum_k2 w1^(-m k2) w^(-t k2) sum_k1 w2^(-t k1) X[k2 + N1 k1].
-template <int N1, int N2>
-__device__ __forceinline__ void zinv_inplace(float2* x, int nl, int ps, const float2* tw) {
-  const int T = blockDim.x;
-  const float rl = __frcp_rn((float)nl);
-  const int mstep = N2 * ps;
-  // pass A, item k2 < N1: N2-point inverse DFT over the run k1 + N2 k2, twiddle w^(-t k2),
-  // back to positions t + N2 k2
-  for (int q = threadIdx.x; q < nl * N1; q += T) {
-    int l;
-    const int k2 = fdivmod(q, nl, rl, l);
-    float2* y = x + l + k2 * mstep;
-    float2 v[N2];
-#pragma unroll
-    for (int k1 = 0; k1 < N2; k1++) v[k1] = y[k1 * ps];
-    Dft<N2>::run(v, 1.f);
-#pragma unroll
-    for (int t = 1; t < N2; t++) {
-      float2 w = tw[t * k2];   // t k2 < N1 N2
-      v[t] = cmul(v[t], make_float2(w.x, -w.y));
-    }
-#pragma unroll
-    for (int t = 0; t < N2; t++) y[t * ps] = v[t];
-  }
-  __syncthreads();
-  // pass B, item t < N2: N1-point inverse DFT over positions t + N2 k2, natural order back
-  for (int q = threadIdx.x; q < nl * N2; q += T) {
-    int l;
-    const int t = fdivmod(q, nl, rl, l);
-    float2* y = x + l + t * ps;
-    float2 v[N1];
-#pragma unroll
-    for (int k2 = 0; k2 < N1; k2++) v[k2] = y[k2 * mstep];
-    Dft<N1>::run(v, 1.f);
-#pragma unroll
-    for (int m = 0; m < N1; m++) y[m * mstep] = v[m];
-  }
-  __syncthreads();
-}
-
-// ------------------------------------------------------------------ per-bin algebra
-
-// Section of N floats (N % 4 == 0) of the row of position p: group g at e[g * stride].
-template <int N>
-__device__ __forceinline__ void ldrow(float (&out)[N], const float4* __restrict__ e, int stride) {
-#pragma unroll
-  for (int g = 0; g < N / 4; g++) {
-    const float4 v = __ldg(e + g * stride);
-    out[4 * g] = v.x;
-    out[4 * g + 1] = v.y;
-    out[4 * g + 2] = v.z;
-    out[4 * g + 3] = v.w;
-  }
-}
-
-constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
-
-// mu_post, S_post (order 00 11 22 01 02 12) and the residual (in d) of one bin from the row
-// e (float4 groups at stride nzp) of its position, laid out as EigLayout: the angles' rows
-// are streamed one at a time.
-template <int NTH>
-__device__ __forceinline__ void bin_posterior_eig(const ZParams& P, const float4* __restrict__ e, float lam,
-                                                  float rho, const float2 (&mu)[3], float2 (&d)[NTH],
-                                                  float2 (&mu_post)[3], float2 (&sp)[6]) {
-  constexpr int VP = pad4(2 * NTH), OKW = 0, OL = VP, OR = OL + pad4(NTH), RS = VP + 16;
-  const int st = P.nzp;
-  float kw[VP];
-  ldrow(kw, e + (OKW / 4) * st, st);
-  float Lm[pad4(NTH)];
-  ldrow(Lm, e + (OL / 4) * st, st);
-  // y = d - K mu, K = diag(kw) A
-  float2 y[NTH];
-#pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    float2 am = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int a = 0; a < 3; a++) am = make_float2(am.x + P.A[l][a] * mu[a].x, am.y + P.A[l][a] * mu[a].y);
-    y[l] = csub(d[l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
-  }
-  float2 mp[3] = {mu[0], mu[1], mu[2]};
-  float s00 = rho * P.pv[0], s11 = rho * P.pv[1], s22 = rho * P.pv[2];
-  float2 s01 = make_float2(rho * P.pv[3], 0.f), s02 = make_float2(rho * P.pv[4], 0.f),
-         s12 = make_float2(rho * P.pv[5], 0.f);
-#pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    // r_l = (V y)_l, s_l = r_l lam / (lam Lam_l + 1), w_l = lam^2 / (lam Lam_l + 1)
-    float V[VP];
-    ldrow(V, e + ((OR + l * RS) / 4) * st, st);
-    float2 r = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int m = 0; m < NTH; m++) r = cadd(r, cmul(make_float2(V[2 * m], V[2 * m + 1]), y[m]));
-    const float inv = __frcp_rn(fmaf(lam, Lm[l], 1.0f));
-    const float f = lam * inv;
-    const float2 sl = make_float2(r.x * f, r.y * f);
-    const float wl = lam * f;
-    // mu_post += conj(Q_l.) s_l;  S_post -= w_l H_l, H_l = (|Q_l0|^2, |Q_l1|^2, |Q_l2|^2,
-    // conj(Q_l0) Q_l1, conj(Q_l0) Q_l2, conj(Q_l1) Q_l2)
-    float QH[16];
-    ldrow(QH, e + ((OR + l * RS + VP) / 4) * st, st);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const float qr = QH[2 * a], qi = QH[2 * a + 1];
-      mp[a].x += qr * sl.x + qi * sl.y;
-      mp[a].y += qr * sl.y - qi * sl.x;
-    }
-    const float* h = QH + 6;
-    s00 -= wl * h[0];
-    s11 -= wl * h[1];
-    s22 -= wl * h[2];
-    s01 = make_float2(s01.x - wl * h[3], s01.y - wl * h[4]);
-    s02 = make_float2(s02.x - wl * h[5], s02.y - wl * h[6]);
-    s12 = make_float2(s12.x - wl * h[7], s12.y - wl * h[8]);
-  }
-#pragma unroll
-  for (int a = 0; a < 3; a++) mu_post[a] = mp[a];
-  sp[0] = make_float2(s00, 0.f);
-  sp[1] = make_float2(s11, 0.f);
-  sp[2] = make_float2(s22, 0.f);
-  sp[3] = s01;
-  sp[4] = s02;
-  sp[5] = s12;
-  // residual d - K mu_post = y - K (mu_post - mu) (the data spectrum itself where the row
-  // is zero: kz not inverted)
-#pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    float2 am = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-      am = make_float2(am.x + P.A[l][a] * (mp[a].x - mu[a].x), am.y + P.A[l][a] * (mp[a].y - mu[a].y));
-    d[l] = csub(y[l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
-  }
-}
-
-// ------------------------------------------------------------------ the kernel
-
-// Shared-memory layout of one tile (W consecutive x-bins at one y, all NZ = N1 N2 positions):
-//   tw  [NZ]             z twiddles e^{-2 pi i t / NZ}
-//   R   [NZ][G][W]       G = max(nth + 3, 9) slots per bin: data 0..nth-1, mean nth..nth+2;
-//                        after the per-bin step S_post (or its realisation factor) 0..5 and
-//                        mu_post 6..8
-//   S3  [NZ][3 SB][W]    the output spectra of SB realisations, transformed together
-// Element (slot g, position p, x-offset w) of R is R[(p G + g) W + w].
-// DENSE: bounded for two 384-thread CTAs per SM (at most 80 registers), the other form for
-// one CTA of up to 512 threads (up to 128 registers).
-template <int NTH, int N1, int N2, bool DENSE>
-__global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(const __grid_constant__ ZParams P) {
-  extern __shared__ float2 sm[];
-  constexpr int NZ = N1 * N2;
-  constexpr int G = NTH + 3 > 9 ? NTH + 3 : 9;
-  constexpr int GIN = NTH + 3;
-  const int W = P.W, lw = P.logW, SB = P.SB;
-  const int TS = W * NZ;
-  float2* tw = sm;
-  float2* R = tw + NZ;
-  float2* S3 = R + G * TS;
-  __shared__ unsigned long long cnt[2];
-  const int T = blockDim.x, tid = threadIdx.x;
-  const int it = blockIdx.x % P.nIT;
-  const int j = blockIdx.x / P.nIT;
-  const int i0 = it * W;
-  const int nw = min(W, P.cnxp - i0);
-  const size_t kstride = (size_t)P.nyp * P.cnxp;
-  const size_t base = (size_t)j * P.cnxp + i0;
-
-  if (tid < 2) cnt[tid] = 0;
-  for (int t = tid; t < NZ; t += T) tw[t] = P.twz[t];
-  // ---- inputs: slot g <- data[g] (g < NTH) or mean[g - NTH], natural kz order; x-bins
-  //      beyond the grid are zero-filled
-  {
-    const uint32_t rb = smem_addr(R);
-    for (int e = tid; e < TS; e += T) {
-      const int w = e & (W - 1), k = e >> lw;
-      const bool ok = w < nw;
-      const size_t go = base + (ok ? (size_t)k * kstride + w : 0);
-      const uint32_t sa = rb + 8u * (uint32_t)(k * G * W + w);
-#pragma unroll
-      for (int g = 0; g < GIN; g++)
-        cp_async8_zfill(sa + 8u * (uint32_t)(g * W), (g < NTH ? P.data[g] : P.mean[g - NTH]) + go, ok);
-    }
-    cp_async_commit();
-    cp_async_wait_0();
-  }
-  __syncthreads();
-  zfwd_inplace<N1, N2>(R, GIN * W, G * W, tw);
-  // a NaN or Inf in any input grid reaches every bin through the transforms
-  if (tid == 0 && P.counters) {
-    float s = 0.f;
-#pragma unroll
-    for (int g = 0; g < GIN; g++) s += fabsf(R[g * W].x) + fabsf(R[g * W].y);
-    if (!isfinite(s)) atomicAdd(P.counters + 4, 1ull);
-  }
-
-  // ---- per-bin posterior; bin at position p holds kz = p / N2 + N1 (p % N2)
-  unsigned long long n_zero_bins = 0;
-  for (int b = tid; b < TS; b += T) {
-    const int p = b >> lw, w = b & (W - 1);
-    if (w >= nw) continue;
-    const int kz = p / N2 + N1 * (p % N2);
-    const int i = i0 + w;
-    float2* slot = R + p * G * W + w;
-    const float2 cx = __ldg(P.cxy + (size_t)j * P.cnxp + i);
-    const float lam = fabsf(cx.x);
-    const float rho = fabsf(cx.x * __ldg(P.ct + kz).x);
-    float2 mu[3], d[NTH];
-#pragma unroll
-    for (int a = 0; a < 3; a++) mu[a] = slot[(NTH + a) * W];
-#pragma unroll
-    for (int l = 0; l < NTH; l++) d[l] = slot[l * W];
-    float2 mp[3], sp[6];
-    bin_posterior_eig<NTH>(P, P.eig + p, lam, rho, mu, d, mp, sp);
-    if (P.keep_resid) {
-      const size_t gidx = base + (size_t)kz * kstride + w;
-#pragma unroll
-      for (int l = 0; l < NTH; l++) P.data[l][gidx] = d[l];
-    }
-    // the realisation factor of S_post once for all realisations (lib_matrCholCpx(3),
-    // simulate :1425-1443): slots 0..5 then hold L (slot 0's imaginary part -1 marks it) or,
-    // where the factorisation fails, S_post itself; the covariance output is rebuilt as
-    // L L^H before its inverse transform
-    float2 C[3][3];
-    C[0][0] = sp[0]; C[1][1] = sp[1]; C[2][2] = sp[2];
-    C[0][1] = sp[3]; C[0][2] = sp[4]; C[1][2] = sp[5];
-    C[1][0] = make_float2(sp[3].x, -sp[3].y);
-    C[2][0] = make_float2(sp[4].x, -sp[4].y);
-    C[2][1] = make_float2(sp[5].x, -sp[5].y);
-    if (P.nsim > 0 && chol_ref<3>(C)) {
-      slot[0] = make_float2(C[0][0].x, -1.f);
-      slot[W] = make_float2(C[1][1].x, 0.f);
-      slot[2 * W] = make_float2(C[2][2].x, 0.f);
-      slot[3 * W] = C[1][0];
-      slot[4 * W] = C[2][0];
-      slot[5 * W] = C[2][1];
-    } else {
-      if (P.nsim > 0) n_zero_bins++;
-#pragma unroll
-      for (int q = 0; q < 6; q++) slot[q * W] = sp[q];
-    }
-#pragma unroll
-    for (int a = 0; a < 3; a++) slot[(6 + a) * W] = mp[a];
-  }
-  __syncthreads();
-
-  // ---- realisations (src/avoinversion.cpp:1401-1511), the mean added in the spectral
-  //      domain; SB realisations per batch share one transform call
-#pragma unroll 1
-  for (int s0 = 0; s0 < P.nsim; s0 += SB) {
-    const int nb = min(SB, P.nsim - s0);
-    const int SG = 3 * SB;   // slot stride of S3
-    for (int b = tid; b < TS; b += T) {
-      const int p = b >> lw, w = b & (W - 1);
-      float2* o3 = S3 + p * SG * W + w;
-      if (w >= nw) {
-        for (int q = 0; q < 3 * nb; q++) o3[q * W] = make_float2(0.f, 0.f);
-        continue;
-      }
-      const int kz = p / N2 + N1 * (p % N2);
-      const int i = i0 + w;
-      const float2* slot = R + p * G * W + w;
-      const float2 l0 = slot[0];
-      const float2 m0 = slot[6 * W], m1 = slot[7 * W], m2 = slot[8 * W];
-#pragma unroll 1
-      for (int sb = 0; sb < nb; sb++) {
-        const int s = s0 + sb;
-        float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        if (l0.y == -1.f) {
-          float2 z[3];
-          if (P.host_noise) {
-            const size_t gidx = base + (size_t)kz * kstride + w;
-#pragma unroll
-            for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
-          } else {
-            device_noise3(P.seed, s, i, j, kz, P.nyp, NZ, P.cnxp, P.nxp_even, z);
-          }
-          const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
-          sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
-          sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
-          sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
-        }
-        o3[(3 * sb) * W] = cadd(m0, sd[0]);
-        o3[(3 * sb + 1) * W] = cadd(m1, sd[1]);
-        o3[(3 * sb + 2) * W] = cadd(m2, sd[2]);
-      }
-    }
-    __syncthreads();
-    zinv_inplace<N1, N2>(S3, 3 * nb * W, SG * W, tw);
-    for (int e = tid; e < TS; e += T) {
-      const int w = e & (W - 1), k = e >> lw;
-      if (w >= nw) continue;
-      const size_t go = base + (size_t)k * kstride + w;
-      const float2* r = S3 + k * SG * W + w;
-      for (int c = 0; c < 3 * nb; c++) P.sim[3 * s0 + c][go] = r[c * W];
-    }
-    __syncthreads();
-  }
-  // ---- S_post = L L^H where slots 0..5 hold the factor
-  if (P.nsim > 0) {
-    for (int b = tid; b < TS; b += T) {
-      const int p = b >> lw, w = b & (W - 1);
-      float2* slot = R + p * G * W + w;
-      const float2 l0 = slot[0];
-      if (l0.y != -1.f) continue;
-      const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
-      slot[0] = make_float2(l0.x * l0.x, 0.f);
-      slot[W] = make_float2(l10.x * l10.x + l10.y * l10.y + l1.x * l1.x, 0.f);
-      slot[2 * W] = make_float2(l20.x * l20.x + l20.y * l20.y + l21.x * l21.x + l21.y * l21.y + l2.x * l2.x, 0.f);
-      slot[3 * W] = make_float2(l0.x * l10.x, -l0.x * l10.y);
-      slot[4 * W] = make_float2(l0.x * l20.x, -l0.x * l20.y);
-      slot[5 * W] = make_float2(l10.x * l20.x + l10.y * l20.y + l1.x * l21.x,
-                                l10.y * l20.x - l10.x * l20.y - l1.x * l21.y);
-    }
-    __syncthreads();
-  }
-  // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
-  //      and mean (6..8); spectral covariance slots stay in position order
-  const int gs0 = P.cov_spectral ? 6 : 0;
-  zinv_inplace<N1, N2>(R + gs0 * W, (9 - gs0) * W, G * W, tw);
-  for (int e = tid; e < TS; e += T) {
-    const int w = e & (W - 1), k = e >> lw;
-    if (w >= nw) continue;
-    const size_t go = base + (size_t)k * kstride + w;
-    const int so = k * G * W + w;
-#pragma unroll
-    for (int g = 0; g < 9; g++) {
-      if (g < gs0) {
-        const int kz = k / N2 + N1 * (k % N2);
-        P.cov[g][base + (size_t)kz * kstride + w] = R[so + g * W];
-      } else {
-        (g < 6 ? P.cov[g] : P.mean[g - 6])[go] = R[so + g * W];
-      }
-    }
-  }
-
-  // counters: inverted bins per tile column from the host's count of inverted kz
-  unsigned long long n_zero = n_zero_bins * (unsigned long long)P.nsim;
-  for (int off = 16; off > 0; off >>= 1) n_zero += __shfl_down_sync(0xffffffffu, n_zero, off);
-  if ((tid & 31) == 0 && n_zero) atomicAdd(&cnt[0], n_zero);
-  __syncthreads();
-  if (tid == 0 && P.counters) {
-    atomicAdd(P.counters + 0, (unsigned long long)P.n_inv_rows * (unsigned long long)nw);
-    if (cnt[0]) atomicAdd(P.counters + 2, cnt[0]);
-  }
-}
-
-// ------------------------------------------------------------------ launcher
 
 size_t pencil_smem_bytes(int W, int nzp, int nth, int SB) {
   const int G = nth + 3 > 9 ? nth + 3 : 9;
   return sizeof(float2) * ((size_t)nzp + (size_t)(G + 3 * SB) * W * nzp);
 }
 
-template <int NTH, int N1, int N2, bool DENSE>
-static cudaError_t launch_pencil_d(const ZParams& zp, int threads, cudaStream_t st) {
-  const size_t smem = pencil_smem_bytes(zp.W, zp.nzp, zp.nth, zp.SB);
-  auto fn = k_pencil<NTH, N1, N2, DENSE>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  fn<<<dim3((unsigned)(zp.nIT * zp.nyp)), threads, smem, st>>>(zp);
-  return cudaGetLastError();
-}
-
-// The dense form is instantiated for up to 6 angle stacks and 256 / 320 points (the
-// production and precision-study lengths).
-template <int NTH, int N1, int N2>
-static cudaError_t launch_pencil_t(const ZParams& zp, int threads, cudaStream_t st) {
-  if constexpr (NTH <= 6 && N2 == 16) {
-    if (zp.dense && threads <= 384) return launch_pencil_d<NTH, N1, N2, true>(zp, threads, st);
-  }
-  return launch_pencil_d<NTH, N1, N2, false>(zp, threads, st);
-}
-
-template <int NTH>
-static cudaError_t launch_pencil_n(const ZParams& zp, int threads, cudaStream_t st) {
-  switch (zp.zsplit) {
-    case 1: return zp.nzp == 256 ? launch_pencil_t<NTH, 16, 16>(zp, threads, st) : cudaErrorInvalidValue;
-    case 2: return zp.nzp == 320 ? launch_pencil_t<NTH, 20, 16>(zp, threads, st) : cudaErrorInvalidValue;
-    case 3: return zp.nzp == 128 ? launch_pencil_t<NTH, 16, 8>(zp, threads, st) : cudaErrorInvalidValue;
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 cudaError_t launch_pencil(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch) {
   if ((zp.W & (zp.W - 1)) || (1 << zp.logW) != zp.W || !zp.eig || threads < 32 || threads > 512 || zp.SB < 1 ||
-      zp.SB > kMaxSim)
+      zp.SB > kMaxSim || zp.nth < 1 || zp.nth > kMaxTheta)
     return cudaErrorInvalidValue;
   if (nlaunch) (*nlaunch)++;
-  switch (zp.nth) {
-    case 1: return launch_pencil_n<1>(zp, threads, st);
-    case 2: return launch_pencil_n<2>(zp, threads, st);
-    case 3: return launch_pencil_n<3>(zp, threads, st);
-    case 4: return launch_pencil_n<4>(zp, threads, st);
-    case 5: return launch_pencil_n<5>(zp, threads, st);
-    case 6: return launch_pencil_n<6>(zp, threads, st);
-    case 7: return launch_pencil_n<7>(zp, threads, st);
-    case 8: return launch_pencil_n<8>(zp, threads, st);
+  switch (zp.zsplit) {
+    case 1: return launch_pencil_split1(zp, threads, st);
+    case 2: return launch_pencil_split2(zp, threads, st);
+    case 3: return launch_pencil_split3(zp, threads, st);
     default: return cudaErrorInvalidValue;
   }
 }

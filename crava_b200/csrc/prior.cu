@@ -1,9 +1,10 @@
 // Prior covariance grids generated on the device (sm_100a), for GRIDS-mode jobs:
 //
-//   SeismicParametersHolder::InitializeCorrelations, the branch without estimated
-//   covariance (src/seismicparametersholder.cpp:333-348): six grids
-//   fillInParamCorr(corrXY, circCorrT, gradI, gradJ) x float(priorVar0(a, b))
-//   (FFTGrid::fillInParamCorr, src/fftgrid.cpp:878-928, multiplyByScalar);
+//   SeismicParametersHolder::InitializeCorrelations (src/seismicparametersholder.cpp:235-353):
+//   without estimated covariance six grids fillInParamCorr(corrXY, circCorrT, gradI, gradJ)
+//   x float(priorVar0(a, b)) (FFTGrid::fillInParamCorr, src/fftgrid.cpp:878-928,
+//   multiplyByScalar); with it FillInLateralCorr(corrXY, circAutoCov_ab, gradI, gradJ)
+//   (src/fftgrid.cpp:830-876), the same interpolation of each grid's own temporal function;
 //   FFTGrid::fillInErrCorr(corrXY, gradI, gradJ) (src/fftgrid.cpp:777-828).
 //
 // One thread per voxel writes all seven grids: 28 bytes per voxel of HBM writes instead of
@@ -29,18 +30,29 @@ __global__ void k_fill_prior(const __grid_constant__ PriorFill P) {
   const float sub = __fadd_rn(__fadd_rn((float)k, __fmul_rn((float)ci, P.gi)), __fmul_rn((float)cj, P.gj));
   const float cxy = __ldg(P.cxy + (size_t)j * P.nxp + i);
   const size_t o = ((size_t)k * P.nyp + j) * P.rnxp + i;
-  // fillInParamCorr: linear interpolation of circCorrT at subK (cyclic), times corrXY
+  // fillInParamCorr: linear interpolation of circCorrT at subK (cyclic), times corrXY; with
+  // estimated covariance FillInLateralCorr, the same with each grid's own auto-covariance
   {
     int base = (int)floorf(sub);
     const float s = __fsub_rn(sub, (float)base);
     base %= nzp;
     if (base < 0) base += nzp;
     const int nxt = base != nzp - 1 ? base + 1 : 0;
-    float v = __fmul_rn(__fsub_rn(1.f, s), __ldg(P.ct + base));
-    v = __fadd_rn(v, __fmul_rn(s, __ldg(P.ct + nxt)));
-    v = __fmul_rn(v, cxy);
+    if (P.act) {
 #pragma unroll
-    for (int q = 0; q < 6; q++) P.cov[q][o] = __fmul_rn(v, P.pv[q]);
+      for (int q = 0; q < 6; q++) {
+        const float* t = P.act + (size_t)q * nzp;
+        float v = __fmul_rn(__fsub_rn(1.f, s), __ldg(t + base));
+        v = __fadd_rn(v, __fmul_rn(s, __ldg(t + nxt)));
+        P.cov[q][o] = __fmul_rn(v, cxy);
+      }
+    } else {
+      float v = __fmul_rn(__fsub_rn(1.f, s), __ldg(P.ct + base));
+      v = __fadd_rn(v, __fmul_rn(s, __ldg(P.ct + nxt)));
+      v = __fmul_rn(v, cxy);
+#pragma unroll
+      for (int q = 0; q < 6; q++) P.cov[q][o] = __fmul_rn(v, P.pv[q]);
+    }
   }
   // fillInErrCorr: corrXY weighted by the distance of subK to the nearest multiple of nzp,
   // zero beyond one sample

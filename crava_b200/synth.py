@@ -363,10 +363,11 @@ def make_block(spec: BlockSpec) -> Block:
                  nsim=spec.nsim, seed=spec.seed)
 
 
-def make_block_fast(spec: BlockSpec) -> Block:
+def make_block_fast(spec: BlockSpec, data: bool = True) -> Block:
     """Same shapes, operators and priors as make_block, with the seismic replaced by seeded
-    white noise of seismic amplitude (no prior realisation, no forward model).  The
-    inversion's cost does not depend on the data values, so throughput runs over many
+    white noise of seismic amplitude (no prior realisation, no forward model); data=False
+    leaves the data and prior-mean grids out (None) for callers that supply their own
+    buffers.  The inversion's cost does not depend on the data values, so throughput runs over many
     blocks use this to keep input synthesis short."""
     nxp, nyp, nzp = spec.padded()
     nx, ny, nz = spec.nx, spec.ny, spec.nz
@@ -386,16 +387,19 @@ def make_block_fast(spec: BlockSpec) -> Block:
     wav = np.stack([wavelet_fft_order(nzp, spec.dt, f) for f in spec.peak_hz])
     wnorm = np.array([wavelet_norm(w) for w in wav], dtype=np.float32)
     rnxp = 2 * (nxp // 2 + 1)
-    data = np.zeros((nth, nzp, nyp, rnxp), dtype=np.float32)
     amp = np.float32(0.02)
-    for l in range(nth):
-        data[l, :, :, :nxp] = rng.standard_normal((nzp, nyp, nxp), dtype=np.float32) * amp
+    grids = data
+    data = mean = None
+    if grids:
+        data = np.zeros((nth, nzp, nyp, rnxp), dtype=np.float32)
+        for l in range(nth):
+            data[l, :, :, :nxp] = rng.standard_normal((nzp, nyp, nxp), dtype=np.float32) * amp
+        mean = np.zeros((3, nzp, nyp, rnxp), dtype=np.float32)
+        for a in range(3):
+            mean[a, :, :, :nxp] = np.float32(spec.mean[a])
     err_var = np.full(nth, float(amp) ** 2) / np.asarray(spec.sn, dtype=np.float64)
     ang = angular_corr(spec.theta_deg, spec.angular[0], spec.angular[1]).astype(np.float32)
     etc = (np.sqrt(err_var)[:, None] * np.sqrt(err_var)[None, :] * ang).astype(np.float32).astype(np.float64)
-    mean = np.zeros((3, nzp, nyp, rnxp), dtype=np.float32)
-    for a in range(3):
-        mean[a, :, :, :nxp] = np.float32(spec.mean[a])
     return Block(spec=spec, nx=nx, ny=ny, nz=nz, nxp=nxp, nyp=nyp, nzp=nzp, lz=nz * spec.dt,
                  A=A, err_theta_cov=etc, wavelet=wav, wavelet_norm=wnorm, prior_var0=P0,
                  corr_xy=cxy, prior_corr_t=pct, circ_corr_t=cct, low_int_cut=low_int_cut,
@@ -472,6 +476,36 @@ def served_specs(n_jobs: int = 48, seed: int = 51, nsim: int = 16) -> list[Block
         out.append(BlockSpec(nx=nx, ny=ny, nz=nz, theta_deg=tuple(np.linspace(5.0, 45.0, nth)),
                              peak_hz=(30.0,) * nth, sn=(5.0,) * nth, std=base.std, corr=base.corr,
                              nsim=nsim, seed=seed * 1000 + b))
+    return out
+
+
+def served_stream_specs(n_jobs: int = 48, n_models: int = 6, seed: int = 61, nsim: int = 16) -> list[BlockSpec]:
+    """A served stream of fresh requests: n_models interval models (nz smooth in [64, 256],
+    3..6 angles 5..45 deg, priors within +-30% of the 64x64x128 block, Ricker 30 Hz) and, per
+    request, one model and a lateral shape such that the voxel counts are log-uniform between
+    64x64x64 and 512x512x256 (x, y smooth in [64, 512])."""
+    rng = np.random.default_rng(seed)
+    xy = np.array(smooth_sizes(64, 512))
+    zz = np.array(smooth_sizes(64, 256))
+    base = config0()
+    models = []
+    for m in range(n_models):
+        nth = int(rng.integers(3, 7))
+        jit = lambda v: tuple(float(x) * float(rng.uniform(0.7, 1.3)) for x in v)
+        models.append(dict(nz=int(rng.choice(zz)), theta_deg=tuple(np.linspace(5.0, 45.0, nth)),
+                           peak_hz=(30.0,) * nth, sn=(5.0,) * nth, std=jit(base.std),
+                           corr=tuple(float(np.clip(c * rng.uniform(0.7, 1.3), -0.9, 0.9)) for c in base.corr),
+                           lateral_range=base.lateral_range * float(rng.uniform(0.7, 1.3)),
+                           temporal_range=base.temporal_range * float(rng.uniform(0.7, 1.3))))
+    lo, hi = math.log(64 * 64 * 64), math.log(512 * 512 * 256)
+    out = []
+    for b in range(n_jobs):
+        m = models[int(rng.integers(0, n_models))]
+        target = math.exp(rng.uniform(lo, hi))
+        nxy = math.sqrt(target / m["nz"])
+        nx = int(xy[np.argmin(np.abs(xy - nxy * rng.uniform(0.85, 1.15)))])
+        ny = int(xy[np.argmin(np.abs(xy - nxy * rng.uniform(0.85, 1.15)))])
+        out.append(BlockSpec(nx=nx, ny=ny, nsim=nsim, seed=seed * 1000 + b, **m))
     return out
 
 

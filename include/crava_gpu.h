@@ -140,6 +140,18 @@ crava_status crava_ctx_destroy(crava_ctx* ctx);
 const char* crava_last_error(void);
 const char* crava_status_string(crava_status s);
 
+/* Resident table cache (no counterpart in the reference, which builds every interval's
+ * operators anew, src/avoinversion.cpp:845-934): with max_bytes > 0, jobs of this context
+ * keep their per-kz tables (wavelet and prior-model operators, separable factors, eigen
+ * tables) and their lateral correlation spectrum in device entries shared by every job with
+ * the same model, built on first use and evicted least recently used beyond max_bytes or
+ * under the context's HBM budget; 0 turns it off (the tables then sit in each job's pool).
+ * crava_serve_start turns it on (256 MiB) when it is off.  Stats: hits and misses of entry
+ * lookups, bytes and number of resident entries. */
+crava_status crava_ctx_set_table_cache(crava_ctx* ctx, size_t max_bytes);
+crava_status crava_ctx_table_cache_stats(crava_ctx* ctx, long long* hits, long long* misses, size_t* bytes,
+                                         int* entries);
+
 /* Job = one AVOInversion on one block.  Allocates the device grids for the block.
  * Replaces the AVOInversion constructor's set-up (src/avoinversion.cpp:53-111). */
 crava_status crava_job_create(crava_ctx* ctx, const crava_job_desc* desc, crava_job** job);
@@ -176,6 +188,17 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out);
  * without the flag. */
 crava_status crava_job_divide_data(crava_job* job, void* stream);
 
+/* Local noise (ModelAVODynamic::GetUseLocalNoise): AVOInversion::correctVpVsRho with
+ * newPosteriorCovPointwise (src/avoinversion.cpp:2028-2302) and the local-noise mixing of
+ * the realisations in simulate (:1485-1504), applied after crava_job_run to the posterior
+ * mean and realisation grids in place.  scales: ntheta host maps of the local noise scale,
+ * nx*ny floats each (index i + nx*j), all finite and > 0.  Per trace the 3x3 maps come from
+ * G (AVOInversion::computeG, :1943-2026, computed on the host: its eigenvectors are taken
+ * with the largest-magnitude component positive), the posterior lag-0 covariance
+ * (updatePriorVar) and the trace's scales; the prior mean is the job's prior-mean input.
+ * Returns after `stream` has finished the work. */
+crava_status crava_job_local_noise(crava_job* job, const float* scales, void* stream);
+
 /* CRAVA_PRIOR_GRIDS jobs whose description also carries corr_xy and circ_corr_t: the six
  * prior covariance grids and the error-correlation grid are generated on the device, in
  * place of their uploads, as SeismicParametersHolder::InitializeCorrelations
@@ -185,6 +208,30 @@ crava_status crava_job_divide_data(crava_job* job, void* stream);
  * the reference's float arithmetic (the grids are equal bit for bit).  Call before
  * crava_job_run; returns after `stream` has finished the work. */
 crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_grad_j, void* stream);
+
+/* CRAVA_PRIOR_GRIDS jobs with estimated covariance (InitializeCorrelations with
+ * cov_estimated, src/seismicparametersholder.cpp:247-325): the six prior covariance grids
+ * FFTGrid::FillInLateralCorr(corrXY, circAutoCov_ab, gradI, gradJ) (src/fftgrid.cpp:830-876)
+ * and the error-correlation grid, generated on the device.  circ_auto_cov: 6 x nzp floats,
+ * the circular auto-covariances of the pairs Vp, Vs, Rho, VpVs, VpRho, VsRho (from
+ * crava_circ_auto_cov).  Returns after `stream` has finished the work. */
+crava_status crava_job_fill_prior_auto_cov(crava_job* job, const float* circ_auto_cov, float corr_grad_i,
+                                           float corr_grad_j, void* stream);
+
+/* Host-side temporal prior functions (no device needed).
+ * crava_circ_corr_t: SeismicParametersHolder::computeCircCorrT with makeCircCorrTPosDef
+ * (src/seismicparametersholder.cpp:624-660, 805-840): the circular temporal correlation of
+ * nzp samples from the lags 0..n-1 of prior_corr_t, its spectrum zeroed at k <= min_int_fq
+ * and made non-negative, normalised to 1 at lag 0 (CRAVA_EINVAL where the reference aborts:
+ * a lag-0 value below 1e-5).
+ * crava_circ_auto_cov: ComputeCircAutoCov, MakeCircAutoCovPosDef and
+ * TaperCircAutoCovFunction (:559-757) of estimated auto-covariances auto_cov (nlag 3x3
+ * matrices, lag-major, row-major each; lag k of pair (i, j) is the forward lag, (j, i) the
+ * backward one), sampling dz ms: out = 6 x nzp floats in the order Vp, Vs, Rho, VpVs, VpRho,
+ * VsRho.  Both evaluate their transforms in double; the reference's FFTW float path agrees
+ * to float rounding. */
+crava_status crava_circ_corr_t(const double* prior_corr_t, int n, int min_int_fq, int nzp, float* out);
+crava_status crava_circ_auto_cov(const double* auto_cov, int nlag, int nzp, double dz, float* out);
 
 /* FFTGrid drop-ins on a device grid (src/fftgrid.cpp:1587-1612 / 1615-1643).
  * covariance != 0 selects the COVARIANCE scaling. */
@@ -249,6 +296,20 @@ crava_status crava_facies_prob(crava_ctx* ctx, const crava_facies_desc* fd, cons
                                const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
                                float* const* d_prob, float* d_seis_lh, void* stream);
 
+/* The same with local noise (calculateFaciesProb with noiseScale, findDensity's corners,
+ * src/faciesprob.cpp:1307-1423, 1961-1977): 2^nang density volumes (nang <= 4 angles with a
+ * local noise scale), corner c built for the angles' extreme scales (bit a of c: the largest
+ * scale of angle a), each with its own box corners[c] (nfacies, prior and p_undefined are
+ * read from corners[0]) and device volume d_density[c]; noise_scale: nang host maps of nx*ny
+ * floats (index i + nx*j).  A voxel's density is the corner densities weighted by
+ * prod_a (t_a or 1 - t_a), t_a = (scale_a - min_a) / (max_a - min_a) of its trace (0 when the
+ * map is constant).  nang = 0 is the single-volume case.  Returns after `stream` has
+ * finished the work when nang > 0. */
+crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_desc* corners, int nang,
+                                           const float* const* d_density, int density_row, const float* noise_scale,
+                                           const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
+                                           float* const* d_prob, float* d_seis_lh, void* stream);
+
 /* Batches (no counterpart in the reference, which inverts one interval at a time,
  * main.cpp:217-353): the runs of n created jobs, of any sizes and angle counts, captured
  * once into a CUDA graph with `branches` concurrent branches; every crava_batch_run
@@ -262,7 +323,9 @@ crava_status crava_batch_destroy(crava_batch* b);
  * are admitted first come first served while the in-flight count is below max_inflight
  * and their footprint fits the context's HBM budget; each runs on its own stream (inputs
  * host->device, the inversion, outputs device->host) and overlaps with the others; its
- * device memory is released, stream-ordered, when it completes.  host_in: ntheta data
+ * device memory is released, stream-ordered, when it completes.  The per-kz and lateral
+ * tables of requests stay resident in the context's table cache, so requests that share
+ * a prior and wavelet model (or a lateral grid and correlation) skip their set-up.  host_in: ntheta data
  * grids then 3 prior mean grids; host_out: 3 posterior mean, 6 covariance, 3*nsim
  * realisation grids (NULL entries are not downloaded).  Host buffers stay owned by the
  * caller and must stay valid until the request is done (pinned buffers keep the copies
@@ -278,6 +341,11 @@ typedef struct {
 crava_status crava_serve_start(crava_ctx* ctx, int max_inflight, crava_server** out);
 crava_status crava_serve_submit(crava_server* sv, const crava_job_desc* desc, const float* const* host_in,
                                 float* const* host_out, uint64_t* ticket);
+/* Poll and wait report a request's state; once they have reported its final state (done or
+ * failed) the request's record is released and its ticket is no longer known.  A request
+ * whose data or prior-mean grids hold a NaN or Inf fails with CRAVA_ENUMERIC; one that
+ * cannot fit the device memory even with nothing else in flight fails with CRAVA_ENOMEM
+ * (a job larger than the context budget is refused at submit). */
 crava_status crava_serve_poll(crava_server* sv, uint64_t ticket, crava_request_info* info);
 /* Waits at most timeout_ms; CRAVA_ETIMEDOUT when the request is still queued or running. */
 crava_status crava_serve_wait(crava_server* sv, uint64_t ticket, double timeout_ms, crava_request_info* info);

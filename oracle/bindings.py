@@ -69,6 +69,8 @@ def ref32_lib():
                                            ctypes.c_int, _fp]
         _ref32.ref32_divide_traces.argtypes = [_fp, ctypes.c_int, ctypes.c_int, _fp, _fp,
                                                ctypes.POINTER(ctypes.c_ubyte)]
+        _ref32.ref32_facies_prob.argtypes = [P(_fp), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             P(_fp), P(ctypes.c_double), ctypes.c_int, _fp, ctypes.c_float, _fp, _fp]
     return _ref32
 
 
@@ -184,3 +186,22 @@ def ref32_invert(blk, cov_grids, err_corr, nsim=0, seed=0, noise=None) -> Ref32R
     r.sims = np.stack(sims).reshape(nsim, 3, nzp, nyp, rnxp) if nsim else None
     r.n_inverted, r.n_chol_fail = cnt[0], cnt[1]
     return r
+
+
+def ref32_facies_prob(post, corners, prior, p_undefined, t):
+    """calculateFaciesProb + findDensity in the reference's float arithmetic (ref32).
+    post: 3 arrays (nz, ny, nx); corners: list of (dens (nf, nr, nb, na), nbins, vmin, dv);
+    t: (nang, ny, nx) relative noise scales.  Returns (nf + 1, nz, ny, nx) float32."""
+    lib = ref32_lib()
+    nz, ny, nx = post[0].shape
+    P = [np.ascontiguousarray(p, dtype=np.float32) for p in post]
+    D = [np.ascontiguousarray(c[0], dtype=np.float32) for c in corners]
+    box = np.array([list(c[2]) + list(c[3]) + list(c[1]) for c in corners], dtype=np.float64)
+    nf = D[0].shape[0]
+    pr = np.ascontiguousarray(prior, dtype=np.float32)
+    tt = np.ascontiguousarray(t, dtype=np.float32)
+    out = np.empty((nf + 1, nz, ny, nx), dtype=np.float32)
+    lib.ref32_facies_prob((_fp * 3)(*[_f(p) for p in P]), nx, ny, nz, tt.shape[0], (_fp * len(D))(*[_f(d) for d in D]),
+                          box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nf, _f(pr), float(p_undefined),
+                          _f(tt) if tt.size else None, _f(out))
+    return out

@@ -18,6 +18,8 @@
 //   AVOInversion::simulate                         src/avoinversion.cpp:1354-1511
 //   SeismicParametersHolder::invFFTCovGrids        src/seismicparametersholder.cpp:432-456
 //   AVOInversion::divideDataByScaleWavelet, the trace transform   src/avoinversion.cpp:537-588
+//   FaciesProb::findDensity + calculateFaciesProb (local-noise corners)
+//                                                 src/faciesprob.cpp:1307-1423, 1909-2075
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -449,6 +451,74 @@ void ref32_sim_noise(unsigned int seed, int nsim, int nxp, int nyp, int nzp, flo
   size_t csize = size_t(nxp / 2 + 1) * nyp * nzp;
   for (int g = 0; g < nsim * 3; g++)
     fill_complex_noise(reinterpret_cast<fftw_complex*>(out + size_t(g) * 2 * csize), nxp, nyp, nzp);
+}
+
+
+// FaciesProb::calculateFaciesProb with findDensity (src/faciesprob.cpp:1909-2075, 1307-1423)
+// in the reference's float arithmetic: per voxel, for every corner volume c (2^nang of them,
+// the single-volume case nang = 0) Simbox::getInterpolationIndexes of a flat, unrotated box
+// (src/simbox.cpp:745-760: (x - xmin) / dx - 0.5 in double), the clamped trilinear sum in float
+// with the reference's term order, the corner weights prod (t or 1 - t) by the bits of c, the
+// prior weighting and the normalisation with undefSum.  post: 3 arrays of nx*ny*nz (index
+// i + nx (j + ny k)); dens[c]: nf cubes of nb0*nb1*nb2 (index j + nb0 (k + nb1 l)); box[c]:
+// 9 doubles (vmin[3], dv[3], nb[3]); t: nang x nx*ny; out: (nf + 1) x nx*ny*nz.
+void ref32_facies_prob(const float* const* post, int nx, int ny, int nz, int nang, const float* const* dens,
+                       const double* box, int nf, const float* prior, float p_undefined, const float* t,
+                       float* out) {
+  const int nc = 1 << nang;
+  const size_t nvox = (size_t)nx * ny * nz;
+  const float undefSum = p_undefined / (float)((int)box[6] * (int)box[7] * (int)box[8]);
+  std::vector<float> value(nc), val(nf);
+  for (size_t e = 0; e < nvox; e++) {
+    const size_t tr = e % ((size_t)nx * ny);
+    const float vp = post[0][e], vs = post[1][e], rho = post[2][e];
+    float sum = undefSum;
+    for (int l = 0; l < nf; l++) {
+      for (int c = 0; c < nc; c++) {
+        const double* b = box + 9 * c;
+        const int nb[3] = {(int)b[6], (int)b[7], (int)b[8]};
+        const double full[3] = {((double)vp - b[0]) / b[3] - 0.5, ((double)vs - b[1]) / b[4] - 0.5,
+                                ((double)rho - b[2]) / b[5] - 0.5};
+        int i1[3], i2[3];
+        float w[3];
+        for (int d = 0; d < 3; d++) {
+          i1[d] = static_cast<int>(floor(full[d]));
+          if (i1[d] < 0) { i1[d] = 0; i2[d] = 0; w[d] = 0; }
+          else if (i1[d] >= nb[d] - 1) { i1[d] = nb[d] - 1; i2[d] = i1[d]; w[d] = 0; }
+          else { i2[d] = i1[d] + 1; w[d] = static_cast<float>(full[d] - i1[d]); }
+        }
+        const float* D = dens[c] + (size_t)l * nb[0] * nb[1] * nb[2];
+        auto at = [&](int j, int k, int m) { return std::max<float>(0, D[j + (size_t)nb[0] * (k + (size_t)nb[1] * m)]); };
+        const float wj = w[0], wk = w[1], wl = w[2];
+        float v = 0;
+        v += (1.0f - wj) * (1.0f - wk) * (1.0f - wl) * at(i1[0], i1[1], i1[2]);
+        v += (1.0f - wj) * (1.0f - wk) * (wl) * at(i1[0], i1[1], i2[2]);
+        v += (1.0f - wj) * (wk) * (1.0f - wl) * at(i1[0], i2[1], i1[2]);
+        v += (1.0f - wj) * (wk) * (wl) * at(i1[0], i2[1], i2[2]);
+        v += (wj) * (1.0f - wk) * (1.0f - wl) * at(i2[0], i1[1], i1[2]);
+        v += (wj) * (1.0f - wk) * (wl) * at(i2[0], i1[1], i2[2]);
+        v += (wj) * (wk) * (1.0f - wl) * at(i2[0], i2[1], i1[2]);
+        v += (wj) * (wk) * (wl) * at(i2[0], i2[1], i2[2]);
+        value[c] = v;
+      }
+      float valuesum = 0;
+      for (int c = 0; c < nc; c++) {
+        int factor = 1;
+        for (int a = 0; a < nang; a++) {
+          if (a > 0) factor *= 2;
+          const float ta = t[(size_t)a * nx * ny + tr];
+          if ((c & factor) > 0) value[c] *= ta;
+          else value[c] *= (1 - ta);
+        }
+        valuesum += value[c];
+      }
+      const float dns = valuesum > 0.0 ? valuesum : 0.0f;
+      val[l] = prior[l] * dns;
+      sum = sum + val[l];
+    }
+    for (int l = 0; l < nf; l++) out[(size_t)l * nvox + e] = val[l] / sum;
+    out[(size_t)nf * nvox + e] = undefSum / sum;
+  }
 }
 
 }  // extern "C"

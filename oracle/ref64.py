@@ -611,10 +611,13 @@ class Posterior:
         self.n_chol_fail = 0
 
 
-def posterior(blk, slab: int = 16) -> Posterior:
-    """AVOInversion constructor FFTs + computePostMeanResidAndFFTCov + invFFTCovGrids."""
+def posterior(blk, slab: int = 16, cov_grids=None) -> Posterior:
+    """AVOInversion constructor FFTs + computePostMeanResidAndFFTCov + invFFTCovGrids;
+    cov_grids: the six prior covariance grids when not those of prior_cov_grids(blk)."""
     nxp, nyp, nzp, nth = blk.nxp, blk.nyp, blk.nzp, blk.ntheta
     covs, pairs = prior_cov_grids(blk)
+    if cov_grids is not None:
+        covs = [np.asarray(c, dtype=np.float32) for c in cov_grids]
     cov_spec = [fft_in_place(c, nxp, True) for c in covs]
     if abs(blk.corr_grad_i) > 0 or abs(blk.corr_grad_j) > 0:
         ec = fill_err_corr(blk.corr_xy, nxp, nyp, nzp, blk.corr_grad_i, blk.corr_grad_j)
@@ -770,3 +773,179 @@ def facies_prob(post, dens, nbins, vmin, dv, prior, p_undefined, nx, ny, nz):
         vals.append(prior[f] * np.maximum(d, 0.0))
     s = undef + sum(vals)
     return np.stack([x / s for x in vals] + [undef / s])
+
+
+# ---------------------------------------------------------------- local noise (row f3)
+
+def _sym_eig_sorted(a):
+    """Eigen-decomposition of a real symmetric matrix, eigenvalues descending (NRLib::Sort3x3
+    order), each eigenvector's largest-magnitude component positive (the reference takes
+    LAPACK's signs, which this environment cannot reproduce)."""
+    w, v = np.linalg.eigh(0.5 * (a + a.T))
+    idx = np.argsort(-w, kind="stable")
+    w, v = w[idx], v[:, idx]
+    big = np.argmax(np.abs(v), axis=0)
+    sg = np.sign(v[big, np.arange(v.shape[1])])
+    sg[sg == 0] = 1.0
+    return w, v * sg
+
+
+def _sym_fun(a, f):
+    """V diag(f(w)) V^T of symmetric a (batched over leading axes)."""
+    w, v = np.linalg.eigh(0.5 * (a + np.swapaxes(a, -1, -2)))
+    return (v * f(w)[..., None, :]) @ np.swapaxes(v, -1, -2)
+
+
+def compute_g(Sm, Smd, Sth):
+    """AVOInversion::computeG (src/avoinversion.cpp:1943-2026): G = Sth^1/2 Lg Evec^T Sm^-1/2
+    with (Eval, Evec) the sorted eigen-decomposition of Sm^-1/2 (Sm - Smd)_+ Sm^-1/2 and
+    Lg(i, i) = sqrt(Eval_i / (1 - Eval_i)) for i < min(ntheta, 3)."""
+    n = Sth.shape[0]
+    Sdel = _sym_fun(Sm - Smd, lambda w: np.where(w > 0, w, 0.0))
+    Sinv = _sym_fun(Sm, lambda w: np.where(w > 1e-7, 1.0 / np.sqrt(np.maximum(w, 1e-300)), 0.0))
+    A = Sinv @ Sdel @ Sinv
+    ew, ev = _sym_eig_sorted(A)
+    Lg = np.zeros((n, 3))
+    for i in range(min(n, 3)):
+        if ew[i] > 0:
+            Lg[i, i] = np.sqrt(ew[i] / (1.0 - ew[i]))
+    S12 = _sym_fun(Sth, lambda w: np.sqrt(np.maximum(w, 0.0)))
+    return S12 @ Lg @ ev.T @ Sinv
+
+
+def local_noise_maps(Sm, Smd, Sth, scales):
+    """newPosteriorCovPointwise (src/avoinversion.cpp:2028-2118) per trace: the map S of the
+    posterior deviation from the prior mean and the map Msim of a realisation's deviation
+    (sigmamdnew_ times postVar0^-1/2, :2226-2239).  scales: (ntheta, ny, nx) already divided
+    by each angle's minimum.  Returns S, Msim of shape (ny, nx, 3, 3)."""
+    G = compute_g(Sm, Smd, Sth)
+    d = np.sqrt(np.moveaxis(scales, 0, -1))                       # (ny, nx, n)
+    M = G @ Sm @ G.T + d[..., :, None] * Sth * d[..., None, :]
+    Minv = _sym_fun(M, lambda w: np.where(w > 1e-8, 1.0 / np.where(w > 1e-8, w, 1.0), 0.0))
+    delta = Sm @ G.T @ Minv @ G @ Sm
+    smd = Sm - delta
+    rs = _sym_fun(smd, lambda w: np.sqrt(np.maximum(w, 0.0)))
+    rd = _sym_fun(delta, lambda w: np.sqrt(np.maximum(w, 0.0)))
+    sdel = _sym_fun(Sm - Smd, lambda w: np.where(w > 1e-7, 1.0 / np.sqrt(np.maximum(w, 1e-300)), 0.0))
+    smdi = _sym_fun(Smd, lambda w: np.where(w > 0, 1.0 / np.sqrt(np.maximum(w, 1e-300)), 0.0))
+    return rd @ sdel, rs @ smdi
+
+
+def local_noise_correct(blk, post_mean, sims, scales, post_var0_mat):
+    """correctVpVsRho (src/avoinversion.cpp:2146-2270) on the posterior mean (3, nzp, nyp,
+    rnxp) and the local-noise mixing of simulate (:1485-1504) on realisations (nsim, 3, ...)
+    holding posterior + noise; scales (ntheta, ny, nx) raw local noise scales.  Returns the
+    corrected copies."""
+    nx, ny, nz = blk.nx, blk.ny, blk.nz
+    sc = scales / scales.reshape(scales.shape[0], -1).min(axis=1)[:, None, None]
+    S, Ms = local_noise_maps(np.asarray(blk.prior_var0, dtype=np.float64), np.asarray(post_var0_mat, np.float64),
+                             np.asarray(blk.err_theta_cov, dtype=np.float64), sc)
+    pm = np.asarray(blk.mean, dtype=np.float64)[:, :nz, :ny, :nx]
+    pr = np.asarray(post_mean, dtype=np.float64)[:, :nz, :ny, :nx]
+    dev = pr - pm
+    new = pm + np.einsum("yxab,bzyx->azyx", S, dev)
+    out_mean = np.array(post_mean, dtype=np.float64, copy=True)
+    out_mean[:, :nz, :ny, :nx] = new
+    out_sims = None
+    if sims is not None:
+        out_sims = np.array(sims, dtype=np.float64, copy=True)
+        for s in range(sims.shape[0]):
+            noise = np.asarray(sims[s], dtype=np.float64)[:, :nz, :ny, :nx] - pr
+            out_sims[s, :, :nz, :ny, :nx] = new + np.einsum("yxab,bzyx->azyx", Ms, noise)
+    return out_mean, out_sims
+
+
+# ---------------------------------------------------------------- temporal prior functions (row f2)
+
+def circ_corr_t(prior_t, min_int_fq: int, nzp: int) -> np.ndarray:
+    """SeismicParametersHolder::computeCircCorrT + makeCircCorrTPosDef
+    (src/seismicparametersholder.cpp:624-660, 805-840) in float64: circular extension of the
+    lags (as float), spectrum zeroed at k <= minIntFq and |.| elsewhere, unnormalised back
+    transform divided by its lag-0 value."""
+    n = len(prior_t)
+    c = np.zeros(nzp)
+    for k in range(nzp):
+        refk = k if k < nzp // 2 + 1 else nzp - k
+        c[k] = float(np.float32(prior_t[refk])) if refk < n else 0.0
+    mag = np.abs(np.fft.rfft(c))
+    mag[: min_int_fq + 1] = 0.0
+    back = np.fft.irfft(mag, n=nzp) * nzp
+    if not back[0] > 1e-5:
+        raise ValueError("circular temporal correlation undefined")
+    return (back / back[0]).astype(np.float32)
+
+
+def circ_auto_cov(auto_cov, nzp: int, dz: float) -> np.ndarray:
+    """ComputeCircAutoCov + MakeCircAutoCovPosDef + TaperCircAutoCovFunction
+    (src/seismicparametersholder.cpp:559-757) with the lag-0 test of InitializeCorrelations
+    (:247-274), in float64.  auto_cov: (nlag, 3, 3); returns (6, nzp) float32 in the order
+    Vp, Vs, Rho, VpVs, VpRho, VsRho."""
+    ac = np.asarray(auto_cov, dtype=np.float64)
+    nlag = ac.shape[0]
+    circ = np.zeros((3, 3, nzp))
+    for i in range(3):
+        for j in range(3):
+            zero = not abs(ac[0, i, j]) > 1e-10
+            for k in range(nlag):
+                if k < nzp:
+                    circ[i, j, k] = 0.0 if zero else float(np.float32(ac[k, i, j]))
+                if k < nlag - 1 and 0 <= nzp - k - 1 < nzp:
+                    circ[i, j, nzp - k - 1] = 0.0 if zero else float(np.float32(ac[k + 1, j, i]))
+    F = np.fft.rfft(circ, axis=-1)                      # (3, 3, nh)
+    d = np.sqrt(np.array([circ[i, i, 0] for i in range(3)]))
+    A = np.moveaxis(F, -1, 0) / (d[:, None] * d[None, :])   # (nh, 3, 3)
+    A = 0.5 * (A + np.conj(np.swapaxes(A, -1, -2)))
+    w, v = np.linalg.eigh(A)
+    Aa = (v * np.abs(w)[:, None, :]) @ np.conj(np.swapaxes(v, -1, -2))
+    F2 = np.moveaxis(Aa * (d[:, None] * d[None, :]), 0, -1)
+    back = np.fft.irfft(F2, n=nzp, axis=-1)             # irfft divides by nzp already
+    sd = min(50.0 / dz, nzp / 2.0)
+    t = np.arange(nzp)
+    m = np.where(t < nzp // 2 + 1, t, nzp - t).astype(np.float32).astype(np.float64)
+    e = np.exp(-0.5 * (m / sd) ** 2)
+    taper = np.where(e > 1e-10, e.astype(np.float32).astype(np.float64), 0.0)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    return np.stack([back[a, b] * taper for a, b in pairs]).astype(np.float32)
+
+
+def facies_density_corners(post, corners, scales, nx, ny, nz, t=None):
+    """findDensity with local noise (src/faciesprob.cpp:1307-1423) and the relative noise
+    scales of calculateFaciesProb (:1961-1977), float64.  corners: list of 2^nang tuples
+    (dens (nf, nr, nb, na), nbins, vmin, dv); scales: (nang, ny, nx), or t: the relative
+    scales themselves.  Returns (nf, nz, ny, nx) densities (before the prior weighting)."""
+    if t is None:
+        nang = scales.shape[0]
+        t = np.zeros_like(np.asarray(scales, dtype=np.float64))
+        for a in range(nang):
+            mn, mx = float(scales[a].min()), float(scales[a].max())
+            t[a] = 0.0 if mn == mx else ((scales[a].astype(np.float64) - mn) / (mx - mn)).astype(np.float32)
+    t = np.asarray(t, dtype=np.float64)
+    nang = t.shape[0]
+    v = [np.asarray(post[d][:nz, :ny, :nx], dtype=np.float64) for d in range(3)]
+    nf = corners[0][0].shape[0]
+    out = np.zeros((nf, nz, ny, nx))
+    for c, (dens, nbins, vmin, dv) in enumerate(corners):
+        idx, w = [], []
+        for d in range(3):
+            f = (v[d] - vmin[d]) / dv[d] - 0.5
+            i1 = np.floor(f).astype(np.int64)
+            lo = i1 < 0
+            hi = i1 >= nbins[d] - 1
+            idx.append((np.where(lo, 0, np.where(hi, nbins[d] - 1, i1)),
+                        np.where(lo | hi, np.where(lo, 0, nbins[d] - 1), i1 + 1)))
+            w.append(np.where(lo | hi, 0.0, f - i1))
+        wc = np.ones((ny, nx))
+        for a in range(nang):
+            wc = wc * (t[a] if (c >> a) & 1 else 1.0 - t[a])
+        for f in range(nf):
+            D = np.maximum(np.asarray(dens[f], dtype=np.float64), 0.0)
+            d = 0.0
+            for a in (0, 1):
+                wa = w[0] if a else 1 - w[0]
+                for b in (0, 1):
+                    wb = w[1] if b else 1 - w[1]
+                    for e in (0, 1):
+                        we = w[2] if e else 1 - w[2]
+                        d = d + wa * wb * we * D[idx[2][e], idx[1][b], idx[0][a]]
+            out[f] += d * wc[None]
+    return np.maximum(out, 0.0)

@@ -83,6 +83,38 @@ def make_thick(name, kw, surface_seed):
     return out
 
 
+# Facies probabilities with local-noise corners: calculateFaciesProb + findDensity in the
+# reference's float arithmetic (oracle/_ref ref32_facies_prob) on seeded posterior values,
+# 2^2 corner density volumes with their own boxes, and relative noise scales.
+FACIES_CASES = {"f1_facies_corners": dict(nx=9, ny=7, nz=11, nang=2, nf=3, nbins=(12, 10, 8), seed=13)}
+
+
+def make_facies(name, kw):
+    rng = np.random.default_rng(kw["seed"])
+    nx, ny, nz, nang, nf, nbins = kw["nx"], kw["ny"], kw["nz"], kw["nang"], kw["nf"], kw["nbins"]
+    centre = np.array([np.log(3000.0), np.log(1500.0), np.log(2300.0)])
+    post = [(centre[a] + 0.15 * rng.standard_normal((nz, ny, nx))).astype(np.float32) for a in range(3)]
+    dens, boxes = [], []
+    for c in range(1 << nang):
+        widen = 0.1 * (1 + c)
+        vmin = [float(p.min()) - widen for p in post]
+        dv = [(float(p.max()) + widen - vmin[d]) / nbins[d] for d, p in enumerate(post)]
+        d = rng.random((nf, nbins[2], nbins[1], nbins[0])).astype(np.float32)
+        d[:, :2] -= 0.3        # some negative entries: findDensity clamps them to zero
+        dens.append(d)
+        boxes.append(np.array(vmin + dv + list(nbins), dtype=np.float64))
+    prior = np.array([0.2, 0.5, 0.3], dtype=np.float32)[:nf]
+    scales = (1.0 + 2.0 * rng.random((nang, ny, nx))).astype(np.float32)
+    # calculateFaciesProb's relative scales (src/faciesprob.cpp:1961-1977): double, stored as float
+    t = np.stack([((scales[a].astype(np.float64) - scales[a].min()) / (float(scales[a].max()) - scales[a].min()))
+                  for a in range(nang)]).astype(np.float32)
+    corners = [(dens[c], nbins, list(boxes[c][:3]), list(boxes[c][3:6])) for c in range(1 << nang)]
+    out = ob.ref32_facies_prob(post, corners, prior, 0.05, t)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), post=np.stack(post), dens=np.stack(dens),
+                        boxes=np.stack(boxes), prior=prior, p_undefined=np.float32(0.05), scales=scales, t=t,
+                        ref_prob=out)
+
+
 if __name__ == "__main__":
     if not ob.ref32_available():
         sys.exit("oracle/_ref/libref32.so missing: run `make -C oracle` with the reference tree present")
@@ -94,4 +126,8 @@ if __name__ == "__main__":
     for name, (kw, sseed) in THICK_CASES.items():
         if not only or name in only:
             make_thick(name, kw, sseed)
+            print("wrote", name)
+    for name, kw in FACIES_CASES.items():
+        if not only or name in only:
+            make_facies(name, kw)
             print("wrote", name)

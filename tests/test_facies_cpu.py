@@ -62,3 +62,23 @@ def test_facies_smoother_is_normalised_and_symmetric():
     h[0, 2, 3, 4] = 1.0
     out = ref64.facies_smooth(h, (10, 8, 6), (0.05, 0.05, 0.05), S)
     assert np.isclose(out.sum(), 1.0)
+
+
+def test_corner_density_oracle_matches_reference_arithmetic_fixture():
+    """The float64 restatement of findDensity with local-noise corners against the
+    reference's float arithmetic (tests/golden/f1_facies_corners.npz, written by
+    tests/golden/make_golden.py from oracle/_ref): 1e-6."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "f1_facies_corners.npz"))
+    post = list(z["post"])
+    nz, ny, nx = post[0].shape
+    corners = [(z["dens"][c], tuple(int(v) for v in z["boxes"][c][6:9]), list(z["boxes"][c][:3]),
+                list(z["boxes"][c][3:6])) for c in range(z["dens"].shape[0])]
+    dens = ref64.facies_density_corners(post, corners, None, nx, ny, nz, t=z["t"])
+    nb = corners[0][1]
+    undef = float(z["p_undefined"]) / float(nb[0] * nb[1] * nb[2])
+    val = z["prior"].astype(np.float64)[:, None, None, None] * dens
+    tot = undef + val.sum(axis=0)
+    ref = np.concatenate([val / tot, (undef / tot)[None]])
+    got = z["ref_prob"].astype(np.float64)
+    assert np.linalg.norm(ref - got) / np.linalg.norm(got) < 1e-6

@@ -124,3 +124,60 @@ def test_wait_times_out_and_stop_fails_queued(ctx, blocks):
     assert e.value.status == api.ETIMEDOUT
     sv.wait(ts[0], timeout_ms=120000)
     sv.stop()
+
+
+def test_served_oversized_request_fails_and_the_next_one_runs(blocks):
+    """A request larger than the context budget is refused at submit; one that cannot be
+    allocated with nothing else in flight fails with ENOMEM instead of holding the queue, and
+    the request behind it completes."""
+    small = blocks[0]
+    fp = api.footprint(small)
+    c = api.Context(0, hbm_budget=int(fp * 1.5))
+    sv = api.Server(c, max_inflight=2)
+    big = synth.make_block_fast(synth.BlockSpec(nx=200, ny=200, nz=128, nsim=16, seed=3))
+    bi, bo = _host_buffers(big, big.nsim)
+    with pytest.raises(api.CravaError) as e:
+        sv.submit(big, bi, bo, seed=1)
+    assert e.value.status == api.ENOMEM
+    si, so = _host_buffers(small, small.nsim)
+    t = sv.submit(small, si, so, seed=2)
+    assert sv.wait(t, timeout_ms=120000)["state"] == api.REQ_DONE
+    sv.stop()
+    c.close()
+
+
+def test_served_non_finite_request_fails_with_numeric(ctx, blocks):
+    b = blocks[1]
+    sv = api.Server(ctx, max_inflight=2)
+    ins, outs = _host_buffers(b, b.nsim)
+    ins[0].numpy()[3, 2, 1] = np.nan
+    t_bad = sv.submit(b, ins, outs, seed=1)
+    ins2, outs2 = _host_buffers(b, b.nsim)
+    t_ok = sv.submit(b, ins2, outs2, seed=1)
+    with pytest.raises(api.CravaError) as e:
+        sv.wait(t_bad, timeout_ms=120000)
+    assert e.value.status == api.ENUMERIC
+    assert sv.wait(t_ok, timeout_ms=120000)["state"] == api.REQ_DONE
+    # the final state has been reported: the ticket is released
+    with pytest.raises(api.CravaError):
+        sv.poll(t_ok)
+    sv.stop()
+
+
+def test_table_cache_hits_and_results_unchanged(blocks, alone):
+    """Jobs with the same model share resident tables: the second job of a model is a cache
+    hit, and its results equal the uncached job's bit for bit."""
+    c = api.Context(0)
+    c.set_table_cache(64 << 20)
+    for rep in range(2):
+        for i, b in enumerate(blocks):
+            j = api.Job(c, b, api.PRIOR_SEPARABLE, 0, seed=100 + i)
+            _k = j.upload_block()
+            j.run()
+            got = j.download_outputs()
+            for k in ("mean", "cov", "sims"):
+                assert np.array_equal(got[k], alone[i][k]), (rep, i, k)
+            j.close()
+    st = c.table_cache_stats()
+    assert st["hits"] >= 2 * len(blocks) and st["entries"] >= len(blocks)
+    c.close()

@@ -78,3 +78,83 @@ def test_facies_prob_on_posterior_mean(ctx):
     pad = outs[0].cpu().numpy()[..., blk.nx:]
     assert pad.size == 0 or np.all(pad == -99999.0)
     job.close()
+
+
+@pytest.mark.parametrize("nang", [0, 2, 3])
+def test_facies_prob_with_local_noise_corners(ctx, nang):
+    """findDensity with local noise: 2^nang corner volumes (each its own box), weighted per
+    trace by the relative noise scales, against the oracle (1e-5); nang = 0 equals the
+    single-volume entry point."""
+    import torch
+    blk = synth.make_block(synth.config0())
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=3)
+    _k = job.upload_block()
+    job.run()
+    mean = [job.download(api.ROLE_POST_MEAN, a) for a in range(3)]
+    job.close()
+    m = [x[..., :blk.nx] for x in mean]
+    rng = np.random.default_rng(11 + nang)
+    nf, nbins = 3, (24, 20, 12)
+    prior = [0.3, 0.3, 0.4]
+    corners, descs, keep, d_dens = [], [], [], []
+    for c in range(1 << nang):
+        widen = 0.05 * (1 + c)          # the corner boxes differ
+        vmin = [float(x.min()) - widen for x in m]
+        dv = [(float(x.max()) + widen - vmin[i]) / nbins[i] for i, x in enumerate(m)]
+        dens = rng.random((nf, nbins[2], nbins[1], nbins[0])).astype(np.float32)
+        corners.append((dens, nbins, vmin, dv))
+        fd, k = api.facies_desc(prior, nbins, vmin, dv, 0.02)
+        descs.append(fd)
+        keep.append(k)
+        d_dens.append(torch.from_numpy(dens).cuda())
+    scales = (1.0 + 2.0 * rng.random((nang, blk.ny, blk.nx))).astype(np.float32)
+    rnx = 2 * (blk.nx // 2 + 1)
+    outs = [torch.zeros((blk.nz, blk.ny, rnx), dtype=torch.float32, device="cuda") for _ in range(nf + 1)]
+    d_mean = [torch.from_numpy(x).cuda() for x in mean]
+    api.facies_prob_local_noise(ctx, descs, [t.data_ptr() for t in d_dens], nbins[0], scales,
+                                [t.data_ptr() for t in d_mean], blk.nx, blk.ny, blk.nz, blk.nxp, blk.nyp,
+                                [t.data_ptr() for t in outs])
+    torch.cuda.synchronize()
+    got = np.stack([t.cpu().numpy()[..., :blk.nx] for t in outs])
+    dens_ref = ref64.facies_density_corners(mean, corners, scales, blk.nx, blk.ny, blk.nz)
+    undef = 0.02 / float(np.prod(nbins))
+    val = np.asarray(prior)[:, None, None, None] * dens_ref
+    tot = undef + val.sum(axis=0)
+    ref = np.concatenate([val / tot, (undef / tot)[None]])
+    assert rel(got, ref) < 1e-5
+    if nang == 0:
+        ref1 = ref64.facies_prob(mean, corners[0][0], nbins, corners[0][2], corners[0][3], prior, 0.02,
+                                 blk.nx, blk.ny, blk.nz)
+        assert rel(got, ref1) < 1e-5
+
+
+def test_facies_corners_against_reference_arithmetic_fixture(ctx):
+    """crava_facies_prob_local_noise against the reference's float arithmetic
+    (tests/golden/f1_facies_corners.npz from oracle/_ref): 2 local-noise angles, 4 corner
+    volumes with their own boxes, negative density entries clamped; 1e-6."""
+    import os
+    import torch
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "f1_facies_corners.npz"))
+    nz, ny, nx = z["post"][0].shape
+    rnx = 2 * (nx // 2 + 1)
+    d_post = []
+    for a in range(3):
+        g = np.zeros((nz, ny, rnx), dtype=np.float32)
+        g[..., :nx] = z["post"][a]
+        d_post.append(torch.from_numpy(g).cuda())
+    descs, keep, d_dens = [], [], []
+    prior = [float(p) for p in z["prior"]]
+    for c in range(z["dens"].shape[0]):
+        b = z["boxes"][c]
+        nb = tuple(int(v) for v in b[6:9])
+        fd, k = api.facies_desc(prior, nb, list(b[:3]), list(b[3:6]), float(z["p_undefined"]))
+        descs.append(fd)
+        keep.append(k)
+        d_dens.append(torch.from_numpy(np.ascontiguousarray(z["dens"][c])).cuda())
+    nf = len(prior)
+    outs = [torch.zeros((nz, ny, rnx), dtype=torch.float32, device="cuda") for _ in range(nf + 1)]
+    api.facies_prob_local_noise(ctx, descs, [t.data_ptr() for t in d_dens], int(z["boxes"][0][6]), z["scales"],
+                                [t.data_ptr() for t in d_post], nx, ny, nz, nx, ny, [t.data_ptr() for t in outs])
+    torch.cuda.synchronize()
+    got = np.stack([t.cpu().numpy()[..., :nx] for t in outs])
+    assert rel(got, z["ref_prob"].astype(np.float64)) < 1e-6
