@@ -479,6 +479,113 @@ def nonconst_main(args):
     ctx.close()
 
 
+def kernels_main(args):
+    """The auxiliary kernels on the production block (540x540x256, 5 angles, 4 realisations;
+    --dims for another size): the local-noise correction, facies probabilities (single volume
+    and 4 local-noise corner volumes), the prior-grid generation of a GRIDS job, and the
+    general-length transforms of a 250x250x200 block (lengths outside the four-step table).
+    Each is timed with the library's CUDA-event timers over `steps` calls after `warmup`;
+    achieved GB/s = algorithmic bytes / device time.  One JSON line of its own."""
+    import numpy as np
+    import torch
+    from crava_b200 import api, synth
+
+    dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else None
+    peak, peak_kind = peaks()
+    ctx = api.Context(0)
+    out = {}
+
+    def timed(cls, fn, alg_bytes, note):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ctx.set_profiling(True)
+        ctx.kernel_times(reset=True)
+        for _ in range(args.steps):
+            fn()
+        torch.cuda.synchronize()
+        ms, n = ctx.kernel_times(reset=True)[cls]
+        ctx.set_profiling(False)
+        per = ms / max(n, 1)
+        gbs = alg_bytes / (per / 1000.0) / 1e9
+        return {"ms_per_launch": per, "launches": n, "alg_bytes_per_launch": alg_bytes, "achieved_gbs": gbs,
+                "frac": gbs / peak, "bytes_model": note}
+
+    blk = synth.make_block_fast(workload_spec(0, dims))
+    nvox = blk.nx * blk.ny * blk.nz
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=5)
+    keep = job.upload_block()
+    job.run()
+    rng = np.random.default_rng(3)
+    scales = (1.0 + rng.random((blk.ntheta, blk.ny, blk.nx))).astype(np.float32)
+    nsim = job.nsim
+    out["local_noise"] = timed("local_noise", lambda: job.local_noise(scales), 4 * nvox * (9 + 6 * nsim),
+                               "per voxel: posterior, prior mean and realisations read, posterior and "
+                               "realisations written (4 B each)")
+    # facies probabilities on the posterior mean
+    d_post = [job.device_ptr(api.ROLE_POST_MEAN, a) for a in range(3)]
+    nf, nbins = 3, (100, 100, 50)
+    rnx = 2 * (blk.nx // 2 + 1)
+    probs = [torch.empty((blk.nz, blk.ny, rnx), dtype=torch.float32, device="cuda") for _ in range(nf + 1)]
+    mean_host = [job.download(api.ROLE_POST_MEAN, a)[..., :blk.nx] for a in range(3)]
+    descs, dkeep, dens = [], [], []
+    for c in range(4):
+        vmin = [float(m.min()) - 0.05 * (1 + c) for m in mean_host]
+        dv = [(float(m.max()) + 0.05 * (1 + c) - vmin[i]) / nbins[i] for i, m in enumerate(mean_host)]
+        fd, k = api.facies_desc([0.3, 0.3, 0.4], nbins, vmin, dv, 0.02)
+        descs.append(fd)
+        dkeep.append(k)
+        dens.append(torch.rand((nf, nbins[2], nbins[1], nbins[0]), device="cuda"))
+    fbytes = nvox * (12 + 4 * (nf + 1))
+    out["facies_single"] = timed("facies", lambda: api.facies_prob(
+        ctx, descs[0], dens[0].data_ptr(), nbins[0], d_post, blk.nx, blk.ny, blk.nz, blk.nxp, blk.nyp,
+        [t.data_ptr() for t in probs]), fbytes, "per voxel: 3 posterior values read, nf+1 probabilities written")
+    sc2 = scales[:2]
+    out["facies_corners"] = timed("facies", lambda: api.facies_prob_local_noise(
+        ctx, descs, [d.data_ptr() for d in dens], nbins[0], sc2, d_post, blk.nx, blk.ny, blk.nz, blk.nxp, blk.nyp,
+        [t.data_ptr() for t in probs]), fbytes, "as facies_single, 4 corner volumes (2 local-noise angles)")
+    del keep
+    job.close()
+    # prior grids of a GRIDS job
+    gjob = api.Job(ctx, blk, api.PRIOR_GRIDS, 0, seed=5)
+    out["fill_prior"] = timed("fill_prior", lambda: gjob.fill_prior(0.3, -0.2), 28 * blk.nxp * blk.nyp * blk.nzp,
+                              "7 grids written (4 B per padded voxel each)")
+    gjob.close()
+    # general-length transforms
+    spec = synth.config1(seed=9)
+    spec.nx, spec.ny, spec.nz = 250, 250, 200
+    gblk = synth.make_block_fast(spec)
+    g = api.Job(ctx, gblk, api.PRIOR_SEPARABLE, 0, seed=5)
+    gk = g.upload_block()
+    for _ in range(args.warmup):
+        g.run()
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.kernel_times(reset=True)
+    for _ in range(args.steps):
+        g.run()
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times(reset=True)
+    ctx.set_profiling(False)
+    nin, nout = gblk.ntheta + 3, 9 + 3 * g.nsim
+    ng = {"x_r2c": nin, "line_fwd": nin, "line_inv": nout, "x_c2r": nout, "zpass": 1}
+    gen = {}
+    for c in ng:
+        ms, n = kt[c]
+        per = ms / max(n, 1)
+        ab = alg_bytes(gblk, g.nsim, c, ng[c])
+        gen[c] = {"ms_per_launch": per, "launches": n, "alg_bytes_per_launch": ab,
+                  "achieved_gbs": ab / (per / 1000.0) / 1e9, "frac": ab / (per / 1000.0) / 1e9 / peak}
+    out["general_lengths_250x250x200"] = gen
+    del gk
+    g.close()
+    ctx.close()
+    print(json.dumps({"metric": "auxiliary kernels: achieved HBM GB/s against algorithmic bytes",
+                      "workload": f"{blk.nx}x{blk.ny}x{blk.nz}, {blk.ntheta} angles, {nsim} realisations",
+                      "peak_gbs": peak, "peak_kind": peak_kind, "steps": args.steps, "warmup": args.warmup,
+                      "kernels": out}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -490,9 +597,13 @@ def main():
     ap.add_argument("--no-legs", action="store_true", help="skip the batched and served legs")
     ap.add_argument("--nonconst", action="store_true",
                     help="measure the non-constant-thickness path instead (one GPU, its own JSON line)")
+    ap.add_argument("--kernels", action="store_true",
+                    help="measure the auxiliary kernels instead (one GPU, its own JSON line)")
     args = ap.parse_args()
     if args.nonconst and args.impl == "ours":
         return nonconst_main(args)
+    if args.kernels and args.impl == "ours":
+        return kernels_main(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

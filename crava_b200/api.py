@@ -35,7 +35,7 @@ EXPORTS = ["crava_ctx_create", "crava_ctx_destroy", "crava_last_error", "crava_s
            "crava_fft_r2c", "crava_fft_c2r", "crava_ctx_kernel_launches", "crava_ctx_set_profiling",
            "crava_ctx_kernel_times", "crava_job_divide_data", "crava_job_fill_prior"]
 KERNEL_CLASSES = ["x_r2c", "line_fwd", "zpass", "line_inv", "x_c2r", "xy_fwd", "xy_inv", "thick_divide",
-                  "thick_fill"]
+                  "thick_fill", "local_noise", "facies", "fill_prior"]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
 
 

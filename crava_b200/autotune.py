@@ -12,6 +12,7 @@ fastest value.  The keys swept, with their size key n:
   pencil_sb      n = nzp*16 + ntheta   eigen form: realisations per transform batch
   pencil_threads n = nzp*16 + ntheta   eigen form: threads per CTA
   pencil_dense   n = nzp*16 + ntheta   eigen form: 1 = the 80-register instantiation
+  pencil_nb      n = nzp*16 + ntheta   eigen form: bins of one z position per thread (1 or 2)
   zpass_w, zpass_sb, zpass_threads     general kernel: tile width, realisations per batch,
                  n = nzp*16 + ntheta   threads per CTA
   line4_w_fwd, line4_w_inv   n = N     four-step column transforms: columns per tile
@@ -119,6 +120,8 @@ def tune_workload(name, w, reps, entries, log):
         # the tile width again, now with the realisation batch and threads chosen
         sweep(ctx, job, stream, reps, "pencil_w", pk, [2, 4, 8], ["zpass"], log)
         eig_best = sweep(ctx, job, stream, reps, "pencil_threads", pk, [128, 256, 512], ["zpass"], log)
+        # one or two bins of a z position per thread in the per-bin step
+        eig_best = sweep(ctx, job, stream, reps, "pencil_nb", pk, [1, 2], ["zpass"], log)
         # the 80-register form: two CTAs of up to 384 threads per SM
         if nth <= 6 and nzp in (256, 320):
             keep_w, keep_t, keep_sb = (api.tuning_get(k, pk) for k in ("pencil_w", "pencil_threads", "pencil_sb"))
@@ -138,8 +141,8 @@ def tune_workload(name, w, reps, entries, log):
     gen_best = sweep(ctx, job, stream, reps, "zpass_threads", pk, [256, 512], ["zpass"], log)
     if eig_best and (not gen_best or eig_best[1] <= gen_best[1]):
         api.tuning_set("pencil_kernel", pk, 2)
-    for key in ("pencil_kernel", "pencil_w", "pencil_sb", "pencil_threads", "pencil_dense", "zpass_w", "zpass_sb",
-                "zpass_threads"):
+    for key in ("pencil_kernel", "pencil_w", "pencil_sb", "pencil_threads", "pencil_dense", "pencil_nb", "zpass_w",
+                "zpass_sb", "zpass_threads"):
         v = api.tuning_get(key, pk)
         if v >= 0:
             entries[(key, pk)] = v

@@ -148,7 +148,8 @@ int tuned(const char* key, int n, int fallback) {
 
 // Per-kernel-class CUDA-event timing (off unless crava_ctx_set_profiling enables it).
 enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_XY_FWD = 5, KT_XY_INV = 6,
-       KT_THICK_DIVIDE = 7, KT_THICK_FILL = 8, KT_COUNT = 9 };
+       KT_THICK_DIVIDE = 7, KT_THICK_FILL = 8, KT_LOCAL_NOISE = 9, KT_FACIES = 10, KT_FILL_PRIOR = 11,
+       KT_COUNT = 12 };
 
 struct ProfRec {
   int cat;
@@ -1868,6 +1869,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
       return fail(CRAVA_ENOTSUP, "pencil tile does not fit in shared memory");
     zp.SB = SBp;
     zp.dense = tuned("pencil_dense", skey, 0);
+    zp.nb2 = tuned("pencil_nb", skey, 1) == 2;
     zp.eig = job->eig;
     zp.n_inv_rows = job->n_inv_rows;
     zp.zsplit = zsplit_of(d.nzp);
@@ -2058,7 +2060,10 @@ crava_status crava_job_local_noise(crava_job* job, const float* scales, void* st
   P.scale = dscale;
   cudaError_t e = cudaMemcpyAsync(dscale, scales, sizeof(float) * n * nxy, cudaMemcpyHostToDevice, st);
   int nl = 0;
-  if (e == cudaSuccess) e = launch_local_noise(P, st, &nl);
+  if (e == cudaSuccess) {
+    ProfScope ps(ctx, KT_LOCAL_NOISE, st);
+    e = launch_local_noise(P, st, &nl);
+  }
   cudaFreeAsync(dscale, st);
   if (e != cudaSuccess) return cuda_fail(e, "local noise correction");
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -2122,7 +2127,11 @@ static crava_status fill_prior_impl(crava_job* job, const float* act_host, float
   P.nzp = d.nzp;
   P.rnxp = job->rnxp;
   int nl = 0;
-  cudaError_t fe = launch_fill_prior(P, st, &nl);
+  cudaError_t fe;
+  {
+    ProfScope ps(ctx, KT_FILL_PRIOR, st);
+    fe = launch_fill_prior(P, st, &nl);
+  }
   if (dact) cudaFreeAsync(dact, st);
   if (fe != cudaSuccess) return cuda_fail(fe, "launch_fill_prior");
   // the host vectors stay with the job; wait so that the call has the reference's
@@ -3038,49 +3047,39 @@ crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_de
     CUDA_TRY(cudaMemcpyAsync(dt, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice, st));
   }
   hc.t = dt;
+  // facies-interleaved copies of the volumes for the lookups
+  size_t pbytes = 0;
+  for (int c = 0; c < nc; c++) pbytes += align256(facies_packed_bytes(hc.box[c], fd->nfacies));
+  char* pk = nullptr;
+  CUDA_TRY(cudaMallocAsync((void**)&pk, pbytes, st));
+  for (int c = 0, off = 0; c < nc; c++) {
+    hc.packed[c] = (float4*)(pk + off);
+    off += (int)align256(facies_packed_bytes(hc.box[c], fd->nfacies));
+  }
   // undefSum = p_undefined / (bins of the first density volume), as the reference
   const float undef_sum = fd->p_undefined / (float)(fd->nbins[0] * fd->nbins[1] * fd->nbins[2]);
   const int rnxp_in = 2 * (nxp / 2 + 1), rnxp_out = 2 * (nx / 2 + 1);
-  cudaError_t e = launch_facies_prob_corners(d_post[0], d_post[1], d_post[2], nx, ny, nz, rnxp_in, nyp, rnxp_out, hc,
-                                             fd->nfacies, fd->prior, undef_sum, d_prob, d_seis_lh, st);
+  cudaError_t e;
+  {
+    ProfScope ps(ctx, KT_FACIES, st);
+    e = launch_facies_prob_corners(d_post[0], d_post[1], d_post[2], nx, ny, nz, rnxp_in, nyp, rnxp_out, hc,
+                                   fd->nfacies, fd->prior, undef_sum, d_prob, d_seis_lh, st);
+  }
+  cudaFreeAsync(pk, st);
   if (dt) cudaFreeAsync(dt, st);
   if (e != cudaSuccess) return cuda_fail(e, "launch_facies_prob_corners");
   if (nang > 0) CUDA_TRY(cudaStreamSynchronize(st));   // the host t table
   std::lock_guard<std::mutex> lk(ctx->mu);
-  ctx->launches += 1;
+  ctx->launches += 1 + nc;   // the packing of every volume and the lookups
   return CRAVA_OK;
 }
 
 crava_status crava_facies_prob(crava_ctx* ctx, const crava_facies_desc* fd, const float* d_density, int density_row,
                                const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
                                float* const* d_prob, float* d_seis_lh, void* stream) {
-  if (!ctx || !fd || !d_density || !d_post || !d_prob) return fail(CRAVA_EINVAL, "null argument");
-  if (fd->nfacies < 1 || fd->nfacies > kMaxFacies) return fail(CRAVA_EINVAL, "nfacies must be 1..16");
-  for (int d = 0; d < 3; d++)
-    if (fd->nbins[d] < 1 || !(fd->dv[d] > 0)) return fail(CRAVA_EINVAL, "bad density box");
-  if (nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny) return fail(CRAVA_EINVAL, "bad grid dimensions");
-  if (density_row < fd->nbins[0]) return fail(CRAVA_EINVAL, "density row stride below the vp bin count");
-  for (int f = 0; f <= fd->nfacies; f++)
-    if (!d_prob[f]) return fail(CRAVA_EINVAL, "null probability grid");
-  CUDA_TRY(cudaSetDevice(ctx->device));
-  FaciesBoxHost hb;
-  for (int d = 0; d < 3; d++) {
-    hb.nb[d] = fd->nbins[d];
-    hb.vmin[d] = fd->vmin[d];
-    hb.dv[d] = fd->dv[d];
-  }
-  hb.rs = density_row;
-  hb.fstride = (size_t)density_row * fd->nbins[1] * fd->nbins[2];
-  // FaciesProb::calculateFaciesProb: undefSum = p_undefined / (bins of the density volume)
-  const float undef_sum = fd->p_undefined / (float)(fd->nbins[0] * fd->nbins[1] * fd->nbins[2]);
-  const int rnxp_in = 2 * (nxp / 2 + 1), rnxp_out = 2 * (nx / 2 + 1);
-  CUDA_TRY(launch_facies_prob(d_post[0], d_post[1], d_post[2], nx, ny, nz, rnxp_in, nyp, rnxp_out, d_density, hb,
-                              fd->nfacies, fd->prior, undef_sum, d_prob, d_seis_lh, (cudaStream_t)stream));
-  {
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->launches += 1;
-  }
-  return CRAVA_OK;
+  // the single-volume case of the local-noise form (no noise angles, one corner)
+  return crava_facies_prob_local_noise(ctx, fd, 0, &d_density, density_row, nullptr, d_post, nx, ny, nz, nxp, nyp,
+                                       d_prob, d_seis_lh, stream);
 }
 
 }  // extern "C"

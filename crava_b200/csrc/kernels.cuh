@@ -80,6 +80,7 @@ struct ZParams {
   const float4* eig;
   int n_inv_rows;                  // inverted kz (counted per tile, not per bin)
   int dense;                       // 1: the 80-register instantiation (two CTAs per SM)
+  int nb2;                         // 1: two bins of one z position per thread in the per-bin step
   unsigned long long* counters;    // [0] inverted bins [1] chol fallbacks [2] zero sim bins
                                    // [3] bins re-factorised in FP64 [4] pencil tiles whose
                                    // input spectra are not finite
@@ -227,17 +228,15 @@ struct EigLayout {
 size_t zpass_smem_bytes(int W, int nzp, int nth);                  // GT = 3, SB = 1
 size_t zpass_smem_bytes(int W, int nzp, int nth, int GT, int SB);
 // facies.cu: prior[] and out[] are host arrays (copied into the launch parameters)
-cudaError_t launch_facies_prob(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz,
-                               int rnxp_in, int nyp_in, int rnxp_out, const float* dens, const FaciesBoxHost& hb,
-                               int nf, const float* prior, float undef_sum, float* const* out, float* seis_lh,
-                               cudaStream_t st);
 cudaError_t launch_spec_mul(float2* a, const float2* b, size_t n, cudaStream_t st);
 struct FaciesCornersHost {
   int nang;
   const float* t;                                 // device, nang x ny x nx
   FaciesBoxHost box[1 << kMaxFaciesAngles];
   const float* dens[1 << kMaxFaciesAngles];       // device density volume of each corner
+  float4* packed[1 << kMaxFaciesAngles];          // device scratch of facies_packed_bytes each
 };
+size_t facies_packed_bytes(const FaciesBoxHost& b, int nf);
 cudaError_t launch_facies_prob_corners(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz,
                                        int rnxp_in, int nyp_in, int rnxp_out, const FaciesCornersHost& hc, int nf,
                                        const float* prior, float undef_sum, float* const* out, float* seis_lh,

@@ -84,11 +84,73 @@ __device__ void sym3_sqrt(const double (&m)[3][3], double (&r)[3][3]) {
 
 }  // namespace
 
+// Block: 32 consecutive traces (threadIdx.x) x 8 slices of their z range (threadIdx.y).
+// The threads of slice 0 compute their trace's two maps and share them through shared
+// memory; every thread then streams its slice, so a warp reads 32 consecutive x of one
+// plane and each trace has eight independent streams in flight.
+constexpr int kLnTraces = 32, kLnSlices = 8;
+
 template <int NTH>
-__global__ void __launch_bounds__(128) k_local_noise(const __grid_constant__ LocalNoiseParams P) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void trace_maps(const LocalNoiseParams& P, int i, int j, float (&Sf)[3][3],
+                                           float (&Mf)[3][3]);
+
+template <int NTH>
+__global__ void __launch_bounds__(kLnTraces * kLnSlices) k_local_noise(const __grid_constant__ LocalNoiseParams P) {
+  __shared__ float maps[kLnTraces][2][3][3];
+  const int i = blockIdx.x * kLnTraces + threadIdx.x;
   const int j = blockIdx.y;
-  if (i >= P.nx || j >= P.ny) return;
+  const bool live = i < P.nx && j < P.ny;
+  if (threadIdx.y == 0 && live) {
+    float Sf[3][3], Mf[3][3];
+    trace_maps<NTH>(P, i, j, Sf, Mf);
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        maps[threadIdx.x][0][a][b] = Sf[a][b];
+        maps[threadIdx.x][1][a][b] = Mf[a][b];
+      }
+  }
+  __syncthreads();
+  if (!live) return;
+  float S[3][3], Ms[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      S[a][b] = maps[threadIdx.x][0][a][b];
+      Ms[a][b] = maps[threadIdx.x][1][a][b];
+    }
+  const size_t plane = (size_t)P.rnxp * P.nyp;
+  const size_t t0 = (size_t)j * P.rnxp + i;
+  for (int k = threadIdx.y; k < P.nz; k += kLnSlices) {
+    const size_t o = t0 + (size_t)k * plane;
+    float pm[3], pr[3], pn[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      pm[a] = P.prior_mean[a][o];
+      pr[a] = P.post[a][o];
+    }
+    const float dv = pr[0] - pm[0], ds = pr[1] - pm[1], dr = pr[2] - pm[2];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      pn[a] = pm[a] + S[a][0] * dv + S[a][1] * ds + S[a][2] * dr;
+      P.post[a][o] = pn[a];
+    }
+    for (int s = 0; s < P.nsim; s++) {
+      float n3[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) n3[a] = P.sim[3 * s + a][o] - pr[a];
+#pragma unroll
+      for (int a = 0; a < 3; a++) P.sim[3 * s + a][o] = pn[a] + (Ms[a][0] * n3[0] + Ms[a][1] * n3[1] + Ms[a][2] * n3[2]);
+    }
+  }
+}
+
+// The trace's maps S and Msim (double arithmetic, rounded to float for the voxel loop).
+template <int NTH>
+__device__ __forceinline__ void trace_maps(const LocalNoiseParams& P, int i, int j, float (&Sf)[3][3],
+                                           float (&Mf)[3][3]) {
   // M = G Sm G^T + D SigmaTheta D, then delta = B^T M^-1 B with B = G Sm
   double d[NTH];
 #pragma unroll
@@ -165,38 +227,21 @@ __global__ void __launch_bounds__(128) k_local_noise(const __grid_constant__ Loc
 #pragma unroll
       for (int b = 0; b < 3; b++) S[a][b] = Ms[a][b] = a == b ? 1.0 : 0.0;
   }
-  const size_t plane = (size_t)P.rnxp * P.nyp;
-  const size_t t0 = (size_t)j * P.rnxp + i;
-  for (int k = 0; k < P.nz; k++) {
-    const size_t o = t0 + (size_t)k * plane;
-    float pm[3], pr[3], pn[3];
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      pm[a] = P.prior_mean[a][o];
-      pr[a] = P.post[a][o];
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      Sf[a][b] = (float)S[a][b];
+      Mf[a][b] = (float)Ms[a][b];
     }
-    const float dv = pr[0] - pm[0], ds = pr[1] - pm[1], dr = pr[2] - pm[2];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      pn[a] = float(pm[a] + S[a][0] * dv + S[a][1] * ds + S[a][2] * dr);
-      P.post[a][o] = pn[a];
-    }
-    for (int s = 0; s < P.nsim; s++) {
-      float n3[3];
-#pragma unroll
-      for (int a = 0; a < 3; a++) n3[a] = P.sim[3 * s + a][o] - pr[a];
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-        P.sim[3 * s + a][o] = pn[a] + float(Ms[a][0] * n3[0] + Ms[a][1] * n3[1] + Ms[a][2] * n3[2]);
-    }
-  }
 }
 
 cudaError_t launch_local_noise(const LocalNoiseParams& P, cudaStream_t st, int* nlaunch) {
-  const dim3 grid((unsigned)((P.nx + 127) / 128), (unsigned)P.ny);
+  const dim3 grid((unsigned)((P.nx + kLnTraces - 1) / kLnTraces), (unsigned)P.ny);
+  const dim3 block(kLnTraces, kLnSlices);
   switch (P.nth) {
 #define LN_CASE(n) \
-  case n: k_local_noise<n><<<grid, 128, 0, st>>>(P); break;
+  case n: k_local_noise<n><<<grid, block, 0, st>>>(P); break;
     LN_CASE(1) LN_CASE(2) LN_CASE(3) LN_CASE(4) LN_CASE(5) LN_CASE(6) LN_CASE(7) LN_CASE(8)
 #undef LN_CASE
     default: return cudaErrorInvalidValue;

@@ -131,13 +131,14 @@ __device__ __forceinline__ void ldrow(float (&out)[N], const float4* __restrict_
 
 constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
 
-// mu_post, S_post (order 00 11 22 01 02 12) and the residual (in d) of one bin from the row
-// e (float4 groups at stride nzp) of its position, laid out as EigLayout: the angles' rows
-// are streamed one at a time.
-template <int NTH>
-__device__ __forceinline__ void bin_posterior_eig(const ZParams& P, const float4* __restrict__ e, float lam,
-                                                  float rho, const float2 (&mu)[3], float2 (&d)[NTH],
-                                                  float2 (&mu_post)[3], float2 (&sp)[6]) {
+// mu_post, S_post (order 00 11 22 01 02 12) and the residual (in d) of NB bins of one z
+// position from that position's row e (float4 groups at stride nzp), laid out as EigLayout:
+// the angles' rows are streamed one at a time and every row load serves all NB bins.
+template <int NTH, int NB>
+__device__ __forceinline__ void bin_posterior_eig(const ZParams& P, const float4* __restrict__ e,
+                                                  const float (&lam)[NB], const float (&rho)[NB],
+                                                  const float2 (&mu)[NB][3], float2 (&d)[NB][NTH],
+                                                  float2 (&mu_post)[NB][3], float2 (&sp)[NB][6]) {
   constexpr int VP = pad4(2 * NTH), OKW = 0, OL = VP, OR = OL + pad4(NTH), RS = VP + 16;
   const int st = P.nzp;
   float kw[VP];
@@ -145,66 +146,120 @@ __device__ __forceinline__ void bin_posterior_eig(const ZParams& P, const float4
   float Lm[pad4(NTH)];
   ldrow(Lm, e + (OL / 4) * st, st);
   // y = d - K mu, K = diag(kw) A
-  float2 y[NTH];
+  float2 y[NB][NTH];
 #pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    float2 am = make_float2(0.f, 0.f);
+  for (int b = 0; b < NB; b++)
 #pragma unroll
-    for (int a = 0; a < 3; a++) am = make_float2(am.x + P.A[l][a] * mu[a].x, am.y + P.A[l][a] * mu[a].y);
-    y[l] = csub(d[l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
+    for (int l = 0; l < NTH; l++) {
+      float2 am = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        am = make_float2(am.x + P.A[l][a] * mu[b][a].x, am.y + P.A[l][a] * mu[b][a].y);
+      y[b][l] = csub(d[b][l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
+    }
+  float2 mp[NB][3];
+  float s00[NB], s11[NB], s22[NB];
+  float2 s01[NB], s02[NB], s12[NB];
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) mp[b][a] = mu[b][a];
+    s00[b] = rho[b] * P.pv[0];
+    s11[b] = rho[b] * P.pv[1];
+    s22[b] = rho[b] * P.pv[2];
+    s01[b] = make_float2(rho[b] * P.pv[3], 0.f);
+    s02[b] = make_float2(rho[b] * P.pv[4], 0.f);
+    s12[b] = make_float2(rho[b] * P.pv[5], 0.f);
   }
-  float2 mp[3] = {mu[0], mu[1], mu[2]};
-  float s00 = rho * P.pv[0], s11 = rho * P.pv[1], s22 = rho * P.pv[2];
-  float2 s01 = make_float2(rho * P.pv[3], 0.f), s02 = make_float2(rho * P.pv[4], 0.f),
-         s12 = make_float2(rho * P.pv[5], 0.f);
 #pragma unroll
   for (int l = 0; l < NTH; l++) {
     // r_l = (V y)_l, s_l = r_l lam / (lam Lam_l + 1), w_l = lam^2 / (lam Lam_l + 1)
     float V[VP];
     ldrow(V, e + ((OR + l * RS) / 4) * st, st);
-    float2 r = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int m = 0; m < NTH; m++) r = cadd(r, cmul(make_float2(V[2 * m], V[2 * m + 1]), y[m]));
-    const float inv = __frcp_rn(fmaf(lam, Lm[l], 1.0f));
-    const float f = lam * inv;
-    const float2 sl = make_float2(r.x * f, r.y * f);
-    const float wl = lam * f;
-    // mu_post += conj(Q_l.) s_l;  S_post -= w_l H_l, H_l = (|Q_l0|^2, |Q_l1|^2, |Q_l2|^2,
-    // conj(Q_l0) Q_l1, conj(Q_l0) Q_l2, conj(Q_l1) Q_l2)
     float QH[16];
     ldrow(QH, e + ((OR + l * RS + VP) / 4) * st, st);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const float qr = QH[2 * a], qi = QH[2 * a + 1];
-      mp[a].x += qr * sl.x + qi * sl.y;
-      mp[a].y += qr * sl.y - qi * sl.x;
-    }
     const float* h = QH + 6;
-    s00 -= wl * h[0];
-    s11 -= wl * h[1];
-    s22 -= wl * h[2];
-    s01 = make_float2(s01.x - wl * h[3], s01.y - wl * h[4]);
-    s02 = make_float2(s02.x - wl * h[5], s02.y - wl * h[6]);
-    s12 = make_float2(s12.x - wl * h[7], s12.y - wl * h[8]);
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      float2 r = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int m = 0; m < NTH; m++) r = cadd(r, cmul(make_float2(V[2 * m], V[2 * m + 1]), y[b][m]));
+      const float inv = __frcp_rn(fmaf(lam[b], Lm[l], 1.0f));
+      const float f = lam[b] * inv;
+      const float2 sl = make_float2(r.x * f, r.y * f);
+      const float wl = lam[b] * f;
+      // mu_post += conj(Q_l.) s_l;  S_post -= w_l H_l, H_l = (|Q_l0|^2, |Q_l1|^2, |Q_l2|^2,
+      // conj(Q_l0) Q_l1, conj(Q_l0) Q_l2, conj(Q_l1) Q_l2)
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        const float qr = QH[2 * a], qi = QH[2 * a + 1];
+        mp[b][a].x += qr * sl.x + qi * sl.y;
+        mp[b][a].y += qr * sl.y - qi * sl.x;
+      }
+      s00[b] -= wl * h[0];
+      s11[b] -= wl * h[1];
+      s22[b] -= wl * h[2];
+      s01[b] = make_float2(s01[b].x - wl * h[3], s01[b].y - wl * h[4]);
+      s02[b] = make_float2(s02[b].x - wl * h[5], s02[b].y - wl * h[6]);
+      s12[b] = make_float2(s12[b].x - wl * h[7], s12[b].y - wl * h[8]);
+    }
   }
 #pragma unroll
-  for (int a = 0; a < 3; a++) mu_post[a] = mp[a];
-  sp[0] = make_float2(s00, 0.f);
-  sp[1] = make_float2(s11, 0.f);
-  sp[2] = make_float2(s22, 0.f);
-  sp[3] = s01;
-  sp[4] = s02;
-  sp[5] = s12;
-  // residual d - K mu_post = y - K (mu_post - mu) (the data spectrum itself where the row
-  // is zero: kz not inverted)
+  for (int b = 0; b < NB; b++) {
 #pragma unroll
-  for (int l = 0; l < NTH; l++) {
-    float2 am = make_float2(0.f, 0.f);
+    for (int a = 0; a < 3; a++) mu_post[b][a] = mp[b][a];
+    sp[b][0] = make_float2(s00[b], 0.f);
+    sp[b][1] = make_float2(s11[b], 0.f);
+    sp[b][2] = make_float2(s22[b], 0.f);
+    sp[b][3] = s01[b];
+    sp[b][4] = s02[b];
+    sp[b][5] = s12[b];
+    // residual d - K mu_post = y - K (mu_post - mu) (the data spectrum itself where the row
+    // is zero: kz not inverted)
 #pragma unroll
-    for (int a = 0; a < 3; a++)
-      am = make_float2(am.x + P.A[l][a] * (mp[a].x - mu[a].x), am.y + P.A[l][a] * (mp[a].y - mu[a].y));
-    d[l] = csub(y[l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
+    for (int l = 0; l < NTH; l++) {
+      float2 am = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        am = make_float2(am.x + P.A[l][a] * (mp[b][a].x - mu[b][a].x), am.y + P.A[l][a] * (mp[b][a].y - mu[b][a].y));
+      d[b][l] = csub(y[b][l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
+    }
   }
+}
+
+// Writes one bin's results into its slots: the residual (KEEP_RESIDUAL, at global index
+// gidx), S_post's realisation factor (lib_matrCholCpx(3), simulate :1425-1443) in slots 0..5
+// with slot 0's imaginary part -1 as the mark, or S_post itself where that factorisation
+// fails, and mu_post in slots 6..8.  Returns 1 for a bin whose realisations stay zero.
+template <int NTH>
+__device__ __forceinline__ int store_bin(const ZParams& P, float2* slot, int W, const float2 (&d)[NTH],
+                                         const float2 (&mp)[3], const float2 (&sp)[6], size_t gidx) {
+  if (P.keep_resid) {
+#pragma unroll
+    for (int l = 0; l < NTH; l++) P.data[l][gidx] = d[l];
+  }
+  float2 C[3][3];
+  C[0][0] = sp[0]; C[1][1] = sp[1]; C[2][2] = sp[2];
+  C[0][1] = sp[3]; C[0][2] = sp[4]; C[1][2] = sp[5];
+  C[1][0] = make_float2(sp[3].x, -sp[3].y);
+  C[2][0] = make_float2(sp[4].x, -sp[4].y);
+  C[2][1] = make_float2(sp[5].x, -sp[5].y);
+  int zero = 0;
+  if (P.nsim > 0 && chol_ref<3>(C)) {
+    slot[0] = make_float2(C[0][0].x, -1.f);
+    slot[W] = make_float2(C[1][1].x, 0.f);
+    slot[2 * W] = make_float2(C[2][2].x, 0.f);
+    slot[3 * W] = C[1][0];
+    slot[4 * W] = C[2][0];
+    slot[5 * W] = C[2][1];
+  } else {
+    if (P.nsim > 0) zero = 1;
+#pragma unroll
+    for (int q = 0; q < 6; q++) slot[q * W] = sp[q];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) slot[(6 + a) * W] = mp[a];
+  return zero;
 }
 
 // ------------------------------------------------------------------ the kernel
@@ -266,53 +321,53 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
     if (!isfinite(s)) atomicAdd(P.counters + 4, 1ull);
   }
 
-  // ---- per-bin posterior; bin at position p holds kz = p / N2 + N1 (p % N2)
+  // ---- per-bin posterior; bin at position p holds kz = p / N2 + N1 (p % N2).  A thread takes
+  //      NB bins of one position (x-offsets w, w + W/NB, ...), so each table row it loads
+  //      serves all of them
   unsigned long long n_zero_bins = 0;
-  for (int b = tid; b < TS; b += T) {
-    const int p = b >> lw, w = b & (W - 1);
-    if (w >= nw) continue;
+  const int NB = (W >= 2 && P.nb2) ? 2 : 1;
+  const int WB = W / NB, lwb = NB == 2 ? lw - 1 : lw;
+  for (int b = tid; b < TS / NB; b += T) {
+    const int p = b >> lwb, w0 = b & (WB - 1);
     const int kz = p / N2 + N1 * (p % N2);
-    const int i = i0 + w;
-    float2* slot = R + p * G * W + w;
-    const float2 cx = __ldg(P.cxy + (size_t)j * P.cnxp + i);
-    const float lam = fabsf(cx.x);
-    const float rho = fabsf(cx.x * __ldg(P.ct + kz).x);
-    float2 mu[3], d[NTH];
+    const float ctk = __ldg(P.ct + kz).x;
+    if (NB == 2) {
+      float lam[2], rho[2];
+      float2 mu[2][3], d[2][NTH], mp[2][3], sp[2][6];
 #pragma unroll
-    for (int a = 0; a < 3; a++) mu[a] = slot[(NTH + a) * W];
+      for (int u = 0; u < 2; u++) {
+        const int w = w0 + u * WB;
+        const bool ok = w < nw;
+        const float2 cx = ok ? __ldg(P.cxy + (size_t)j * P.cnxp + i0 + w) : make_float2(0.f, 0.f);
+        lam[u] = fabsf(cx.x);
+        rho[u] = fabsf(cx.x * ctk);
+        const float2* slot = R + p * G * W + w;
 #pragma unroll
-    for (int l = 0; l < NTH; l++) d[l] = slot[l * W];
-    float2 mp[3], sp[6];
-    bin_posterior_eig<NTH>(P, P.eig + p, lam, rho, mu, d, mp, sp);
-    if (P.keep_resid) {
-      const size_t gidx = base + (size_t)kz * kstride + w;
+        for (int a = 0; a < 3; a++) mu[u][a] = slot[(NTH + a) * W];
 #pragma unroll
-      for (int l = 0; l < NTH; l++) P.data[l][gidx] = d[l];
-    }
-    // the realisation factor of S_post once for all realisations (lib_matrCholCpx(3),
-    // simulate :1425-1443): slots 0..5 then hold L (slot 0's imaginary part -1 marks it) or,
-    // where the factorisation fails, S_post itself; the covariance output is rebuilt as
-    // L L^H before its inverse transform
-    float2 C[3][3];
-    C[0][0] = sp[0]; C[1][1] = sp[1]; C[2][2] = sp[2];
-    C[0][1] = sp[3]; C[0][2] = sp[4]; C[1][2] = sp[5];
-    C[1][0] = make_float2(sp[3].x, -sp[3].y);
-    C[2][0] = make_float2(sp[4].x, -sp[4].y);
-    C[2][1] = make_float2(sp[5].x, -sp[5].y);
-    if (P.nsim > 0 && chol_ref<3>(C)) {
-      slot[0] = make_float2(C[0][0].x, -1.f);
-      slot[W] = make_float2(C[1][1].x, 0.f);
-      slot[2 * W] = make_float2(C[2][2].x, 0.f);
-      slot[3 * W] = C[1][0];
-      slot[4 * W] = C[2][0];
-      slot[5 * W] = C[2][1];
+        for (int l = 0; l < NTH; l++) d[u][l] = slot[l * W];
+      }
+      bin_posterior_eig<NTH, 2>(P, P.eig + p, lam, rho, mu, d, mp, sp);
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int w = w0 + u * WB;
+        if (w < nw) n_zero_bins += store_bin<NTH>(P, R + p * G * W + w, W, d[u], mp[u], sp[u],
+                                                  base + (size_t)kz * kstride + w);
+      }
     } else {
-      if (P.nsim > 0) n_zero_bins++;
+      const int w = w0;
+      if (w >= nw) continue;
+      const float2 cx = __ldg(P.cxy + (size_t)j * P.cnxp + i0 + w);
+      float lam[1] = {fabsf(cx.x)}, rho[1] = {fabsf(cx.x * ctk)};
+      float2 mu[1][3], d[1][NTH], mp[1][3], sp[1][6];
+      const float2* slot = R + p * G * W + w;
 #pragma unroll
-      for (int q = 0; q < 6; q++) slot[q * W] = sp[q];
+      for (int a = 0; a < 3; a++) mu[0][a] = slot[(NTH + a) * W];
+#pragma unroll
+      for (int l = 0; l < NTH; l++) d[0][l] = slot[l * W];
+      bin_posterior_eig<NTH, 1>(P, P.eig + p, lam, rho, mu, d, mp, sp);
+      n_zero_bins += store_bin<NTH>(P, R + p * G * W + w, W, d[0], mp[0], sp[0], base + (size_t)kz * kstride + w);
     }
-#pragma unroll
-    for (int a = 0; a < 3; a++) slot[(6 + a) * W] = mp[a];
   }
   __syncthreads();
 

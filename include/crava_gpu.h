@@ -267,6 +267,7 @@ long long crava_ctx_kernel_launches(crava_ctx* ctx);
  *   0 forward x transform, 1 forward line transforms, 2 fused pencil pass,
  *   3 inverse line transforms, 4 inverse x transform, 5/6 fused xy pass forward/inverse,
  *   7 trace division (crava_job_divide_data), 8 trace energies, interpolation, extrapolation,
+ *   9 local-noise correction, 10 facies probabilities, 11 prior-grid generation,
  * the summed milliseconds and launch counts (n entries), then clears them if reset. */
 crava_status crava_ctx_set_profiling(crava_ctx* ctx, int enable);
 crava_status crava_ctx_kernel_times(crava_ctx* ctx, double* ms, long long* launches, int n, int reset);
