@@ -67,6 +67,13 @@ class Counters(ctypes.Structure):
                 ("post_var0", ctypes.c_float * 9), ("nonfinite_tiles", ctypes.c_longlong)]
 
 
+class SimboxGeom(ctypes.Structure):
+    _fields_ = [("x0", ctypes.c_double), ("y0", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("il0", ctypes.c_double), ("xl0", ctypes.c_double),
+                ("il_step_x", ctypes.c_double), ("il_step_y", ctypes.c_double), ("xl_step_x", ctypes.c_double),
+                ("xl_step_y", ctypes.c_double), ("angle", ctypes.c_double)]
+
+
 class FaciesDesc(ctypes.Structure):
     _fields_ = [("nfacies", ctypes.c_int), ("nbins", ctypes.c_int * 3), ("vmin", ctypes.c_double * 3),
                 ("dv", ctypes.c_double * 3), ("prior", _fp), ("p_undefined", ctypes.c_float)]
@@ -125,6 +132,10 @@ def lib() -> ctypes.CDLL:
     L.crava_facies_prob.argtypes = [vp, ctypes.POINTER(FaciesDesc), vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     L.crava_job_local_noise.argtypes = [vp, vp, vp]
+    L.crava_grid_write_crava.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(SimboxGeom), vp]
+    L.crava_grid_read_crava.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(SimboxGeom), vp]
     L.crava_facies_prob_local_noise.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, vp,
                                                 ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
@@ -548,3 +559,16 @@ def facies_prob_local_noise(ctx: Context, corner_descs, d_densities, density_row
     _check(lib().crava_facies_prob_local_noise(ctx.handle, arr, nang, dens, int(density_row),
                                                sc.ctypes.data if nang else None, post, nx, ny, nz, nxp, nyp, prob,
                                                d_seis_lh, stream))
+
+
+def grid_write_crava(ctx: Context, path: str, d_grid: int, rnxp: int, nyp: int, nzp: int, geom: dict, stream=None):
+    """FFTGrid::writeCravaFile of a device grid (rnxp x nyp x nzp floats)."""
+    g = SimboxGeom(**geom)
+    _check(lib().crava_grid_write_crava(ctx.handle, str(path).encode(), d_grid, rnxp, nyp, nzp, ctypes.byref(g), stream))
+
+
+def grid_read_crava(ctx: Context, path: str, d_grid: int, rnxp: int, nyp: int, nzp: int, stream=None) -> dict:
+    """FFTGrid::readCravaFile into a device grid; returns the file's simbox geometry."""
+    g = SimboxGeom()
+    _check(lib().crava_grid_read_crava(ctx.handle, str(path).encode(), d_grid, rnxp, nyp, nzp, ctypes.byref(g), stream))
+    return {k: getattr(g, k) for k, _t in SimboxGeom._fields_}

@@ -205,6 +205,11 @@ struct crava_ctx {
   std::mutex stage_mu;         // device staging grid of the host-grid transforms
   float* stage = nullptr;
   size_t stage_bytes = 0;
+  // CRAVA grid file staging: two pinned chunks, a device chunk and their events
+  std::mutex io_mu;
+  char* io_host[2] = {nullptr, nullptr};
+  char* io_dev = nullptr;
+  cudaEvent_t io_ev[2] = {nullptr, nullptr};
   // resident table cache: key (model bytes) -> device tables, least recently used evicted
   std::mutex cache_mu;
   std::map<std::string, CacheEntry*> cache;
@@ -1011,6 +1016,173 @@ const char* crava_status_string(crava_status s) {
   return "unknown status";
 }
 
+}  // extern "C"
+
+namespace {
+
+constexpr size_t kIoChunk = (size_t)32 << 20;   // bytes per staging chunk
+
+crava_status io_buffers(crava_ctx* ctx) {
+  for (int b = 0; b < 2; b++) {
+    if (!ctx->io_host[b]) CUDA_TRY(cudaHostAlloc((void**)&ctx->io_host[b], kIoChunk, cudaHostAllocDefault));
+    if (!ctx->io_ev[b]) CUDA_TRY(cudaEventCreateWithFlags(&ctx->io_ev[b], cudaEventDisableTiming));
+  }
+  if (!ctx->io_dev) CUDA_TRY(cudaMalloc(&ctx->io_dev, 2 * kIoChunk));
+  return CRAVA_OK;
+}
+
+void put_be(std::string& h, const void* p, size_t n) {
+  const unsigned char* c = (const unsigned char*)p;
+  for (size_t q = 0; q < n; q++) h.push_back((char)c[n - 1 - q]);   // little-endian host to big-endian
+}
+template <class T>
+T get_be(const unsigned char* c) {
+  unsigned char r[sizeof(T)];
+  for (size_t q = 0; q < sizeof(T); q++) r[q] = c[sizeof(T) - 1 - q];
+  T v;
+  std::memcpy(&v, r, sizeof(T));
+  return v;
+}
+
+const char kCravaTag[] = "crava_fftgrid_binary";
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_grid_write_crava(crava_ctx* ctx, const char* path, const float* d_grid, int rnxp, int nyp, int nzp,
+                                    const crava_simbox_geom* geom, void* stream) {
+  if (!ctx || !path || !d_grid || !geom || rnxp < 2 || nyp < 1 || nzp < 1) return fail(CRAVA_EINVAL, "bad arguments");
+  std::lock_guard<std::mutex> lk(ctx->io_mu);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  crava_status s = io_buffers(ctx);
+  if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(CRAVA_EINVAL, std::string("cannot open ") + path + " for writing");
+  std::string h = std::string(kCravaTag) + "\n";
+  const double d1[4] = {geom->x0, geom->y0, geom->dx, geom->dy};
+  for (double v : d1) put_be(h, &v, 8);
+  put_be(h, &geom->nx, 4);
+  put_be(h, &geom->ny, 4);
+  const double d2[7] = {geom->il0, geom->xl0, geom->il_step_x, geom->il_step_y, geom->xl_step_x, geom->xl_step_y,
+                        geom->angle};
+  for (double v : d2) put_be(h, &v, 8);
+  const int dims[3] = {rnxp, nyp, nzp};
+  for (int v : dims) put_be(h, &v, 4);
+  bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
+  const size_t total = sizeof(float) * (size_t)rnxp * nyp * nzp;
+  size_t pending_bytes[2] = {0, 0};
+  int nl = 0;
+  cudaError_t e = cudaSuccess;
+  // chunk c: swap into device staging half c%2, download into pinned half c%2; the file write
+  // of chunk c-1 runs while chunk c is in flight
+  for (size_t off = 0, c = 0; ok && e == cudaSuccess && off < total; off += kIoChunk, c++) {
+    const int b = (int)(c % 2);
+    const size_t n = std::min(kIoChunk, total - off);
+    if (pending_bytes[b]) {   // the chunk this half held is downloaded: write it out first
+      e = cudaEventSynchronize(ctx->io_ev[b]);
+      if (e == cudaSuccess) ok = std::fwrite(ctx->io_host[b], 1, pending_bytes[b], f) == pending_bytes[b];
+      pending_bytes[b] = 0;
+    }
+    uint32_t* dst = (uint32_t*)(ctx->io_dev + b * kIoChunk);
+    if (e == cudaSuccess) e = launch_bswap32(dst, (const uint32_t*)((const char*)d_grid + off), n / 4, st);
+    nl++;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->io_host[b], dst, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->io_ev[b], st);
+    pending_bytes[b] = n;
+    // the other half, if it holds the previous chunk, goes to the file now
+    const int o = 1 - b;
+    if (e == cudaSuccess && ok && pending_bytes[o]) {
+      e = cudaEventSynchronize(ctx->io_ev[o]);
+      if (e == cudaSuccess) ok = std::fwrite(ctx->io_host[o], 1, pending_bytes[o], f) == pending_bytes[o];
+      pending_bytes[o] = 0;
+    }
+  }
+  for (int b = 0; b < 2 && e == cudaSuccess && ok; b++)
+    if (pending_bytes[b]) {
+      e = cudaEventSynchronize(ctx->io_ev[b]);
+      if (e == cudaSuccess) ok = std::fwrite(ctx->io_host[b], 1, pending_bytes[b], f) == pending_bytes[b];
+    }
+  ok = (std::fclose(f) == 0) && ok;
+  if (e != cudaSuccess) return cuda_fail(e, "crava_grid_write_crava");
+  if (!ok) return fail(CRAVA_EINVAL, std::string("write error on ") + path);
+  std::lock_guard<std::mutex> lk2(ctx->mu);
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+crava_status crava_grid_read_crava(crava_ctx* ctx, const char* path, float* d_grid, int rnxp, int nyp, int nzp,
+                                   crava_simbox_geom* geom, void* stream) {
+  if (!ctx || !path || !d_grid || rnxp < 2 || nyp < 1 || nzp < 1) return fail(CRAVA_EINVAL, "bad arguments");
+  std::lock_guard<std::mutex> lk(ctx->io_mu);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  crava_status s = io_buffers(ctx);
+  if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(CRAVA_EINVAL, std::string("cannot open ") + path);
+  char tag[64] = {0};
+  size_t t = 0;
+  int ch;
+  while (t < sizeof(tag) - 1 && (ch = std::fgetc(f)) != EOF && ch != '\n') tag[t++] = (char)ch;
+  unsigned char hb[11 * 8 + 5 * 4];
+  if (std::strcmp(tag, kCravaTag) != 0 || std::fread(hb, 1, sizeof(hb), f) != sizeof(hb)) {
+    std::fclose(f);
+    return fail(CRAVA_EINVAL, std::string(path) + " is not a CRAVA binary grid");
+  }
+  const unsigned char* q = hb;
+  crava_simbox_geom g;
+  g.x0 = get_be<double>(q); q += 8;
+  g.y0 = get_be<double>(q); q += 8;
+  g.dx = get_be<double>(q); q += 8;
+  g.dy = get_be<double>(q); q += 8;
+  g.nx = get_be<int>(q); q += 4;
+  g.ny = get_be<int>(q); q += 4;
+  g.il0 = get_be<double>(q); q += 8;
+  g.xl0 = get_be<double>(q); q += 8;
+  g.il_step_x = get_be<double>(q); q += 8;
+  g.il_step_y = get_be<double>(q); q += 8;
+  g.xl_step_x = get_be<double>(q); q += 8;
+  g.xl_step_y = get_be<double>(q); q += 8;
+  g.angle = get_be<double>(q); q += 8;
+  const int frnxp = get_be<int>(q), fnyp = get_be<int>(q + 4), fnzp = get_be<int>(q + 8);
+  if (frnxp != rnxp || fnyp != nyp || fnzp != nzp) {
+    std::fclose(f);
+    return fail(CRAVA_EINVAL, std::string("grid on file ") + path + " is " + std::to_string(frnxp) + "x" +
+                                  std::to_string(fnyp) + "x" + std::to_string(fnzp) + ", the target " +
+                                  std::to_string(rnxp) + "x" + std::to_string(nyp) + "x" + std::to_string(nzp) +
+                                  " (readCravaFile: check the padding)");
+  }
+  if (geom) *geom = g;
+  const size_t total = sizeof(float) * (size_t)rnxp * nyp * nzp;
+  bool ok = true, used[2] = {false, false};
+  int nl = 0;
+  cudaError_t e = cudaSuccess;
+  // chunk c: read into pinned half c%2 once its previous upload finished, upload, swap in place
+  for (size_t off = 0, c = 0; ok && e == cudaSuccess && off < total; off += kIoChunk, c++) {
+    const int b = (int)(c % 2);
+    const size_t n = std::min(kIoChunk, total - off);
+    if (used[b]) e = cudaEventSynchronize(ctx->io_ev[b]);
+    if (e != cudaSuccess) break;
+    ok = std::fread(ctx->io_host[b], 1, n, f) == n;
+    if (!ok) break;
+    uint32_t* dst = (uint32_t*)((char*)d_grid + off);
+    e = cudaMemcpyAsync(dst, ctx->io_host[b], n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->io_ev[b], st);
+    if (e == cudaSuccess) e = launch_bswap32(dst, dst, n / 4, st);
+    nl++;
+    used[b] = true;
+  }
+  std::fclose(f);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "crava_grid_read_crava");
+  if (!ok) return fail(CRAVA_EINVAL, std::string(path) + " ends before its grid");
+  std::lock_guard<std::mutex> lk2(ctx->mu);
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
 crava_status crava_circ_corr_t(const double* prior_corr_t, int n, int min_int_fq, int nzp, float* out) {
   if (!prior_corr_t || !out || n < 1 || nzp < 2) return fail(CRAVA_EINVAL, "bad arguments");
   if (!(prior_corr_t[0] != 0.0)) return fail(CRAVA_EINVAL, "prior_corr_t[0] must be nonzero");
@@ -1165,6 +1337,11 @@ crava_status crava_ctx_destroy(crava_ctx* ctx) {
     cudaFree(kv.second->mem);
     delete kv.second;
   }
+  for (int b = 0; b < 2; b++) {
+    if (ctx->io_host[b]) cudaFreeHost(ctx->io_host[b]);
+    if (ctx->io_ev[b]) cudaEventDestroy(ctx->io_ev[b]);
+  }
+  if (ctx->io_dev) cudaFree(ctx->io_dev);
   delete ctx;
   return CRAVA_OK;
 }
@@ -2056,8 +2233,9 @@ crava_status crava_job_local_noise(crava_job* job, const float* scales, void* st
   }
   for (int q = 0; q < 3 * d.nsim; q++) P.sim[q] = job->sim[q];
   float* dscale = nullptr;
-  CUDA_TRY(cudaMallocAsync((void**)&dscale, sizeof(float) * n * nxy, st));
+  CUDA_TRY(cudaMallocAsync((void**)&dscale, sizeof(float) * (n + 18) * nxy, st));
   P.scale = dscale;
+  P.maps = dscale + n * nxy;
   cudaError_t e = cudaMemcpyAsync(dscale, scales, sizeof(float) * n * nxy, cudaMemcpyHostToDevice, st);
   int nl = 0;
   if (e == cudaSuccess) {

@@ -92,6 +92,7 @@ constexpr int kNumCounters = 5;
 struct LocalNoiseParams {
   int nx, ny, nz, nyp, rnxp, nth, nsim;
   const float* scale;                 // nth x ny x nx local noise scales, index i + nx (j + ny l)
+  float* maps;                        // ny x nx x 18 floats: every trace's S and Msim (scratch)
   double inv_min[kMaxTheta];          // 1 / (smallest scale of angle l)
   double gsg[kMaxTheta][kMaxTheta];   // G Sm G^T
   double sth[kMaxTheta][kMaxTheta];   // SigmaTheta (errThetaCov)
@@ -229,6 +230,9 @@ size_t zpass_smem_bytes(int W, int nzp, int nth);                  // GT = 3, SB
 size_t zpass_smem_bytes(int W, int nzp, int nth, int GT, int SB);
 // facies.cu: prior[] and out[] are host arrays (copied into the launch parameters)
 cudaError_t launch_spec_mul(float2* a, const float2* b, size_t n, cudaStream_t st);
+// gridio.cu: dst[e] = src[e] with the byte order of every 4-byte word reversed (dst == src
+// allowed)
+cudaError_t launch_bswap32(uint32_t* dst, const uint32_t* src, size_t n, cudaStream_t st);
 struct FaciesCornersHost {
   int nang;
   const float* t;                                 // device, nang x ny x nx

@@ -84,10 +84,11 @@ __device__ void sym3_sqrt(const double (&m)[3][3], double (&r)[3][3]) {
 
 }  // namespace
 
-// Block: 32 consecutive traces (threadIdx.x) x 8 slices of their z range (threadIdx.y).
-// The threads of slice 0 compute their trace's two maps and share them through shared
-// memory; every thread then streams its slice, so a warp reads 32 consecutive x of one
-// plane and each trace has eight independent streams in flight.
+// Two kernels: k_local_noise_maps computes every trace's two maps (one thread per trace, the
+// double-precision solves) into a table of 18 floats per trace; k_local_noise_apply streams
+// the voxels through them, a block of 32 consecutive traces (threadIdx.x) x 8 slices of their
+// z range (threadIdx.y), so a warp reads 32 consecutive x of one plane and each trace has
+// eight independent streams in flight.
 constexpr int kLnTraces = 32, kLnSlices = 8;
 
 template <int NTH>
@@ -95,31 +96,33 @@ __device__ __forceinline__ void trace_maps(const LocalNoiseParams& P, int i, int
                                            float (&Mf)[3][3]);
 
 template <int NTH>
-__global__ void __launch_bounds__(kLnTraces * kLnSlices) k_local_noise(const __grid_constant__ LocalNoiseParams P) {
-  __shared__ float maps[kLnTraces][2][3][3];
-  const int i = blockIdx.x * kLnTraces + threadIdx.x;
-  const int j = blockIdx.y;
-  const bool live = i < P.nx && j < P.ny;
-  if (threadIdx.y == 0 && live) {
-    float Sf[3][3], Mf[3][3];
-    trace_maps<NTH>(P, i, j, Sf, Mf);
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-      for (int b = 0; b < 3; b++) {
-        maps[threadIdx.x][0][a][b] = Sf[a][b];
-        maps[threadIdx.x][1][a][b] = Mf[a][b];
-      }
-  }
-  __syncthreads();
-  if (!live) return;
-  float S[3][3], Ms[3][3];
+__global__ void __launch_bounds__(128) k_local_noise_maps(const __grid_constant__ LocalNoiseParams P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= P.nx || j >= P.ny) return;
+  float Sf[3][3], Mf[3][3];
+  trace_maps<NTH>(P, i, j, Sf, Mf);
+  float* m = P.maps + 18 * ((size_t)j * P.nx + i);
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) {
-      S[a][b] = maps[threadIdx.x][0][a][b];
-      Ms[a][b] = maps[threadIdx.x][1][a][b];
+      m[3 * a + b] = Sf[a][b];
+      m[9 + 3 * a + b] = Mf[a][b];
+    }
+}
+
+__global__ void __launch_bounds__(kLnTraces * kLnSlices) k_local_noise_apply(const __grid_constant__ LocalNoiseParams P) {
+  const int i = blockIdx.x * kLnTraces + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= P.nx || j >= P.ny) return;
+  float S[3][3], Ms[3][3];
+  const float* m = P.maps + 18 * ((size_t)j * P.nx + i);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      S[a][b] = __ldg(m + 3 * a + b);
+      Ms[a][b] = __ldg(m + 9 + 3 * a + b);
     }
   const size_t plane = (size_t)P.rnxp * P.nyp;
   const size_t t0 = (size_t)j * P.rnxp + i;
@@ -237,16 +240,18 @@ __device__ __forceinline__ void trace_maps(const LocalNoiseParams& P, int i, int
 }
 
 cudaError_t launch_local_noise(const LocalNoiseParams& P, cudaStream_t st, int* nlaunch) {
-  const dim3 grid((unsigned)((P.nx + kLnTraces - 1) / kLnTraces), (unsigned)P.ny);
-  const dim3 block(kLnTraces, kLnSlices);
+  if (!P.maps) return cudaErrorInvalidValue;
+  const dim3 mgrid((unsigned)((P.nx + 127) / 128), (unsigned)P.ny);
   switch (P.nth) {
 #define LN_CASE(n) \
-  case n: k_local_noise<n><<<grid, block, 0, st>>>(P); break;
+  case n: k_local_noise_maps<n><<<mgrid, 128, 0, st>>>(P); break;
     LN_CASE(1) LN_CASE(2) LN_CASE(3) LN_CASE(4) LN_CASE(5) LN_CASE(6) LN_CASE(7) LN_CASE(8)
 #undef LN_CASE
     default: return cudaErrorInvalidValue;
   }
-  if (nlaunch) (*nlaunch)++;
+  const dim3 grid((unsigned)((P.nx + kLnTraces - 1) / kLnTraces), (unsigned)P.ny);
+  k_local_noise_apply<<<grid, dim3(kLnTraces, kLnSlices), 0, st>>>(P);
+  if (nlaunch) (*nlaunch) += 2;
   return cudaGetLastError();
 }
 

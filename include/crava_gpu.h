@@ -218,6 +218,27 @@ crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_
 crava_status crava_job_fill_prior_auto_cov(crava_job* job, const float* circ_auto_cov, float corr_grad_i,
                                            float corr_grad_j, void* stream);
 
+/* CRAVA binary grid files (FFTGrid::writeCravaFile / readCravaFile, src/fftgrid.cpp:2183-2270):
+ * the tag line "crava_fftgrid_binary", the simbox geometry below and rnxp, nyp, nzp as
+ * big-endian doubles and 4-byte integers, then the rnxp*nyp*nzp floats of the FFTGrid layout,
+ * big-endian.  The grid is staged straight between the file and the device grid d_grid in
+ * 32 MiB chunks through two pinned buffers of the context, the byte order reversed on the
+ * device; both calls return when the file and the device grid are complete.  The reader
+ * fails with CRAVA_EINVAL when the file's padded dimensions differ from the target's, as the
+ * reference does. */
+typedef struct {
+  double x0, y0, dx, dy;       /* Simbox::getx0, gety0, getdx, getdy            */
+  int nx, ny;                  /* Simbox::getnx, getny                          */
+  double il0, xl0;             /* Simbox::getIL0, getXL0                        */
+  double il_step_x, il_step_y; /* Simbox::getILStepX, getILStepY               */
+  double xl_step_x, xl_step_y; /* Simbox::getXLStepX, getXLStepY               */
+  double angle;                /* Simbox::getAngle                              */
+} crava_simbox_geom;
+crava_status crava_grid_write_crava(crava_ctx* ctx, const char* path, const float* d_grid, int rnxp, int nyp, int nzp,
+                                    const crava_simbox_geom* geom, void* stream);
+crava_status crava_grid_read_crava(crava_ctx* ctx, const char* path, float* d_grid, int rnxp, int nyp, int nzp,
+                                   crava_simbox_geom* geom, void* stream);
+
 /* Host-side temporal prior functions (no device needed).
  * crava_circ_corr_t: SeismicParametersHolder::computeCircCorrT with makeCircCorrTPosDef
  * (src/seismicparametersholder.cpp:624-660, 805-840): the circular temporal correlation of
