@@ -132,6 +132,8 @@ def lib() -> ctypes.CDLL:
     L.crava_facies_prob.argtypes = [vp, ctypes.POINTER(FaciesDesc), vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     L.crava_job_local_noise.argtypes = [vp, vp, vp]
+    L.crava_job_set_wavelet_grids.argtypes = [vp, ctypes.c_int, vp, vp]
+    L.crava_job_residual_synthetics.argtypes = [vp, vp]
     L.crava_grid_write_crava.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(SimboxGeom), vp]
     L.crava_grid_read_crava.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -349,6 +351,25 @@ class Job:
         """divideDataByScaleWavelet + interpolateSeismic on the uploaded data (non-constant
         thickness jobs); returns after the work is done."""
         _check(lib().crava_job_divide_data(self._h, stream))
+
+    def set_wavelet_grids(self, angle: int, shift_ms=None, gain=None):
+        """Local wavelet time shift (ms) and gain grids of one angle stack, (ny, nx) each or
+        None; -999 entries mean no shift / unit gain."""
+        arrs = []
+        for a in (shift_ms, gain):
+            if a is None:
+                arrs.append(None)
+                continue
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            assert a.shape == (self.blk.ny, self.blk.nx), a.shape
+            arrs.append(a)
+        _check(lib().crava_job_set_wavelet_grids(self._h, int(angle), *[None if a is None else a.ctypes.data
+                                                                         for a in arrs]))
+
+    def residual_synthetics(self, stream=None):
+        """multiplyDataByScaleWaveletAndWriteToFile: after a run with KEEP_RESIDUAL the residual
+        grids become the real residuals convolved with each trace's local wavelet."""
+        _check(lib().crava_job_residual_synthetics(self._h, stream))
 
     def local_noise(self, scales: np.ndarray, stream=None):
         """correctVpVsRho and the local-noise mixing of the realisations, in place on the

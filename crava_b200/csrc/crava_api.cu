@@ -291,6 +291,11 @@ struct crava_job {
   std::vector<double> A, etc, pv, relt;
   std::vector<float> wav, wnorm, corr_xy, circ;
   bool ran = false;
+  bool resid_real = false;        // the residual grids hold the wavelet-convolved residuals
+  // local wavelet grids (crava_job_set_wavelet_grids) and the wavelet half spectra of a job
+  // without the non-constant tables (crava_job_residual_synthetics): own allocations
+  float* wgrid = nullptr;         // ntheta x nx*ny shifts (samples), then ntheta x nx*ny gains
+  float2* wspec = nullptr;        // ntheta x cnzp
   bool async = false;             // pool from cudaMallocAsync on alloc_stream
   cudaStream_t alloc_stream = nullptr;
 };
@@ -770,7 +775,21 @@ struct ThickTables {
   std::vector<float> tau2, ztaper, distx, disty, distz;
   std::vector<int> fillx, filly;
   float wn2[kMaxTheta], modW[kMaxTheta], err_var[kMaxTheta];
+  float2 es3_last[kMaxTheta];   // es3 at cnzp - 1 before the RMISSING
 };
+
+// The half spectra of the wavelets (FFT order, Wavelet1D::fft1DInPlace) in float:
+// ntheta x cnzp.
+std::vector<float2> wavelet_spectra(const crava_job_desc& d) {
+  const int n = d.nzp, cn = n / 2 + 1;
+  std::vector<float2> w((size_t)d.ntheta * cn);
+  for (int l = 0; l < d.ntheta; l++) {
+    const float* wf = d.wavelet + (size_t)l * n;
+    std::vector<cd> W = dft(std::vector<double>(wf, wf + n));
+    for (int k = 0; k < cn; k++) w[(size_t)l * cn + k] = make_float2((float)W[k].real(), (float)W[k].imag());
+  }
+  return w;
+}
 
 void build_thick_tables(const crava_job_desc& d, ThickTables& t) {
   const int n = d.nzp, cn = n / 2 + 1, nth = d.ntheta;
@@ -815,6 +834,7 @@ void build_thick_tables(const crava_job_desc& d, ThickTables& t) {
       // at index >= nzp of the complex array: the last entry's imaginary part, and its
       // real part too when nzp is even
       if (k == cn - 1) {
+        t.es3_last[l] = v;
         v.y = -99999.0f;
         if (n % 2 == 0) v.x = -99999.0f;
       }
@@ -1429,6 +1449,8 @@ void job_release(crava_job* j) {
     std::lock_guard<std::mutex> lk(j->ctx->mu);
     j->ctx->allocated -= j->pool_bytes;
   }
+  if (j->wgrid) cudaFree(j->wgrid);
+  if (j->wspec) cudaFree(j->wspec);
   delete j;
 }
 
@@ -1786,6 +1808,7 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
       tp.wn2[l] = tt.wn2[l];
       tp.modW[l] = tt.modW[l];
       tp.err_var[l] = tt.err_var[l];
+      tp.es3_last[l] = tt.es3_last[l];
     }
     tp.wnc = d.wnc;
     tp.low_cut = d.low_cut;
@@ -2077,6 +2100,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     if ((s = inv_xy(ctx, g, sc, d.nxp, d.nyp, d.nzp, false, st))) return s;
   }
   job->ran = true;
+  job->resid_real = false;
   return CRAVA_OK;
 }
 
@@ -2334,6 +2358,9 @@ crava_status crava_job_divide_data(crava_job* job, void* stream) {
   ThickParams& tp = job->tp;
   tp.zp = pz->lp;
   tp.twz = pz->tw;
+  tp.mode = 0;
+  tp.wshift = job->wgrid;
+  tp.wgain = job->wgrid ? job->wgrid + (size_t)d.ntheta * d.nx * d.ny : nullptr;
   const int nth = d.ntheta;
   const size_t nxy = (size_t)d.nx * d.ny;
   int nl = 0;
@@ -2382,6 +2409,99 @@ crava_status crava_job_divide_data(crava_job* job, void* stream) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->launches += nl;
   }
+  return CRAVA_OK;
+}
+
+crava_status crava_job_set_wavelet_grids(crava_job* job, int angle, const float* shift_ms, const float* gain) {
+  if (!job) return fail(CRAVA_EINVAL, "null job");
+  const crava_job_desc& d = job->d;
+  if (angle < 0 || angle >= d.ntheta) return fail(CRAVA_EINVAL, "angle out of range");
+  const size_t nxy = (size_t)d.nx * d.ny;
+  // Wavelet1D::shiftAndScale takes iShift = shift / dz in float, dz the wavelet's sampling
+  // (lz / nz); WELLMISSING (-999) entries are no shift and unit gain
+  // (Wavelet::getLocalTimeshift / getLocalGainFactor, src/wavelet.cpp:1251-1278)
+  const float dz = (float)(d.lz / d.nz);
+  std::vector<float> sh(nxy, 0.f), gn(nxy, 1.f);
+  for (size_t t = 0; t < nxy; t++) {
+    if (shift_ms) {
+      if (!std::isfinite(shift_ms[t])) return fail(CRAVA_EINVAL, "shift grid holds a non-finite value");
+      if (shift_ms[t] != -999.0f) sh[t] = shift_ms[t] / dz;
+    }
+    if (gain) {
+      if (!std::isfinite(gain[t])) return fail(CRAVA_EINVAL, "gain grid holds a non-finite value");
+      if (gain[t] != -999.0f) gn[t] = gain[t];
+    }
+  }
+  CUDA_TRY(cudaSetDevice(job->ctx->device));
+  if (!job->wgrid) {
+    CUDA_TRY(cudaMalloc(&job->wgrid, sizeof(float) * 2 * d.ntheta * nxy));
+    std::vector<float> init(2 * d.ntheta * nxy, 0.f);
+    std::fill(init.begin() + d.ntheta * nxy, init.end(), 1.f);
+    CUDA_TRY(cudaMemcpy(job->wgrid, init.data(), sizeof(float) * init.size(), cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(cudaMemcpy(job->wgrid + angle * nxy, sh.data(), sizeof(float) * nxy, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(job->wgrid + (d.ntheta + angle) * nxy, gn.data(), sizeof(float) * nxy, cudaMemcpyHostToDevice));
+  return CRAVA_OK;
+}
+
+crava_status crava_job_residual_synthetics(crava_job* job, void* stream) {
+  if (!job) return fail(CRAVA_EINVAL, "null job");
+  const crava_job_desc& d = job->d;
+  if (!(d.flags & CRAVA_FLAG_KEEP_RESIDUAL))
+    return fail(CRAVA_ESTATE, "crava_job_residual_synthetics needs a job with CRAVA_FLAG_KEEP_RESIDUAL");
+  if (!job->ran) return fail(CRAVA_ESTATE, "the residuals are defined only after crava_job_run");
+  if (job->resid_real) return fail(CRAVA_ESTATE, "the residuals of this run are already convolved");
+  crava_ctx* ctx = job->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  Plan* pz;
+  crava_status s;
+  if ((s = get_plan(ctx, d.nzp, &pz, true))) return s;
+  if (thick_tile_width(d.nzp) < 1) return fail(CRAVA_ENOTSUP, "nzp too long for the trace transform");
+  const int nth = d.ntheta, cn = d.nzp / 2 + 1;
+  ThickParams tp{};
+  if (d.flags & CRAVA_FLAG_NONCONST_THICK) {
+    tp = job->tp;
+  } else {
+    if (!job->wspec) {
+      const std::vector<float2> w = wavelet_spectra(d);
+      CUDA_TRY(cudaMalloc(&job->wspec, sizeof(float2) * w.size()));
+      CUDA_TRY(cudaMemcpy(job->wspec, w.data(), sizeof(float2) * w.size(), cudaMemcpyHostToDevice));
+    }
+    tp.wamp = job->wspec;
+    tp.nx = d.nx; tp.ny = d.ny; tp.nz = d.nz;
+    tp.nxp = d.nxp; tp.nyp = d.nyp; tp.nzp = d.nzp;
+    tp.rnxp = job->rnxp;
+    tp.cnzp = cn;
+    tp.W = thick_tile_width(d.nzp);
+    tp.logW = 0;
+    while ((1 << tp.logW) < tp.W) tp.logW++;
+    tp.rsq = static_cast<float>(std::sqrt(static_cast<float>(d.nzp)));
+    int e = 0;
+    tp.inv_rsq = std::frexp(tp.rsq, &e) == 0.5f ? 1.0f / tp.rsq : 0.f;
+    tp.lz = d.lz;
+  }
+  tp.mode = 1;
+  tp.nIT = ((d.nx + 1) / 2 + tp.W - 1) / tp.W;
+  tp.rsq_out = static_cast<float>(std::sqrt(static_cast<double>(d.nzp)));
+  tp.zp = pz->lp;
+  tp.twz = pz->tw;
+  tp.wshift = job->wgrid;
+  tp.wgain = job->wgrid ? job->wgrid + (size_t)nth * d.nx * d.ny : nullptr;
+  for (int l = 0; l < nth; l++) tp.grid[l] = job->data[l];
+  // FFTGrid::invFFTInPlace of the residual spectra (src/avoinversion.cpp:744), then the
+  // per-trace convolution
+  std::vector<float*> g(job->data, job->data + nth);
+  std::vector<float> sc(nth, inv_scale(job->N, false));
+  if ((s = inv_xy(ctx, g, sc, d.nxp, d.nyp, d.nzp, true, st))) return s;
+  int nl = 0;
+  {
+    ProfScope ps(ctx, KT_THICK_DIVIDE, st);
+    CUDA_TRY(launch_thick_divide(tp, nth, st, &nl));
+  }
+  job->resid_real = true;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->launches += nl;
   return CRAVA_OK;
 }
 

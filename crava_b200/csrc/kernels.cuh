@@ -147,6 +147,15 @@ struct ThickParams {
   double lz;
   LinePlan zp;
   const float2* twz;
+  // local wavelets (Wavelet1D with shift and gain grids): per angle and trace i + nx j the
+  // shift in samples (shift / dz) and the gain; null: every local wavelet is the global one
+  const float* wshift;
+  const float* wgain;
+  float2 es3_last[kMaxTheta];  // es3 at cnzp - 1 before the RMISSING that the table carries
+  // 0: divideDataByScaleWavelet on every padded trace; 1: the wavelet convolution of
+  // multiplyDataByScaleWaveletAndWriteToFile on the traces i < nx, j < ny
+  int mode;
+  float rsq_out;               // mode 1: float(sqrt(double(nzp))), its final divisor
 };
 // Prior grids of a GRIDS-mode job generated on the device (prior.cu): the six covariance
 // grids fillInParamCorr x priorVar0 and the error-correlation grid fillInErrCorr.

@@ -37,8 +37,10 @@ __device__ __forceinline__ float div_rsq(const ThickParams& P, float x) {
 }
 
 // Wavelet::getCAmp(k, scale) for k < cnzp (src/wavelet.cpp:337-382): the spectrum of the
-// wavelet stretched by `scale`, linear interpolation at k / scale, divided by scale.
-__device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, float scale) {
+// wavelet stretched by `scale`, linear interpolation at k / scale, divided by scale; the
+// spectrum's value at bin m is at(m).
+template <class At>
+__device__ __forceinline__ float2 interp_scaled(int cnzp, int k, float scale, At at) {
   const float om = __fdiv_rn((float)k, scale);
   if (!(om < (float)cnzp)) return make_float2(0.f, 0.f);
   const int lo = (int)floorf(om);
@@ -46,10 +48,26 @@ __device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, 
   if (hi >= cnzp) hi -= 1;
   const float d = __fsub_rn(om, (float)lo);
   const float e = __fsub_rn(1.f, d);
-  const float2 a = __ldg(c + lo), b = __ldg(c + hi);
+  const float2 a = at(lo), b = at(hi);
   const float re = __fadd_rn(__fmul_rn(a.x, e), __fmul_rn(b.x, d));
   const float im = __fadd_rn(__fmul_rn(a.y, e), __fmul_rn(b.y, d));
   return make_float2(__fdiv_rn(re, scale), __fdiv_rn(im, scale));
+}
+
+__device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, float scale) {
+  return interp_scaled(cnzp, k, scale, [&](int m) { return __ldg(c + m); });
+}
+
+// Wavelet1D::shiftAndScale (src/wavelet1D.cpp:580-602) at bin m: the multiplier
+// float(gain cos(2 pi iShift m / nzp)) + i float(gain sin(-2 pi iShift m / nzp)), with the
+// angle and the products in double as the reference forms them, applied to c in float.
+__device__ __forceinline__ float2 shift_scale(float2 c, float ish, float gain, int m, int nzp) {
+  const double a = 2.0 * (3.14159265358979323846 * (double)ish * (double)m) / (double)(float)nzp;
+  double sn, cs;
+  sincos(a, &sn, &cs);
+  const float mr = (float)((double)gain * cs), mi = (float)((double)gain * -sn);
+  return make_float2(__fsub_rn(__fmul_rn(mr, c.x), __fmul_rn(mi, c.y)),
+                     __fadd_rn(__fmul_rn(mi, c.x), __fmul_rn(mr, c.y)));
 }
 
 // computeAdjustmentFactor (src/avoinversion.cpp:630-719) at one kz < cnzp for a trace
@@ -81,7 +99,70 @@ __device__ __forceinline__ float2 adjustment(const ThickParams& P, int l, int k,
   return make_float2(__fdiv_rn(__fdiv_rn(wLoc.x, dL), glob.y), __fdiv_rn(__fdiv_rn(wLoc.y, dL), glob.y));
 }
 
+// The local wavelet of a trace with shift ish (samples) and gain gn: its spectrum is the
+// global one through shiftAndScale (createLocalWavelet1D, src/wavelet1D.cpp:518-526) and
+// its errorSmooth3 the global errorSmooth3 turned by the same unit-modulus multiplier (the
+// band normalisation takes the gain out; the RMISSING entry at cnzp - 1 stays).  The
+// reference re-transforms the local wavelet between the two (the difference constructors
+// work on its samples); here the spectra are used directly.
+__device__ __forceinline__ float2 local_wavelet(const ThickParams& P, int l, int m, float ish, float gn) {
+  return shift_scale(__ldg(P.wamp + (size_t)l * P.cnzp + m), ish, gn, m, P.nzp);
+}
+
+__device__ __forceinline__ float2 local_es3(const ThickParams& P, int l, int m, float ish) {
+  const int cn = P.cnzp;
+  if (m < cn - 1) return shift_scale(__ldg(P.es3 + (size_t)l * cn + m), ish, 1.f, m, P.nzp);
+  float2 v = shift_scale(P.es3_last[l], ish, 1.f, m, P.nzp);
+  v.y = -99999.0f;
+  if (!(P.nzp & 1)) v.x = -99999.0f;
+  return v;
+}
+
+// computeAdjustmentFactor (src/avoinversion.cpp:630-719) with a local wavelet that carries
+// a shift and a gain: wLoc and eSkLoc from the local spectra stretched by sf, eSkGlob from
+// the local spectra unstretched (wLocal->getCAmp(k)), wGlob from the global wavelet; the
+// global wavelet's quotient then depends on the trace and is formed here with the host's
+// float operations.
+__device__ __forceinline__ float2 adjustment_local(const ThickParams& P, int l, int k, float sf, float ish, float gn) {
+  const int cn = P.cnzp;
+  const float wn2 = P.wn2[l], wnc = P.wnc, ev = P.err_var[l];
+  const float2 wLoc = interp_scaled(cn, k, sf, [&](int m) { return local_wavelet(P, l, m, ish, gn); });
+  const float wLoc2 = sq2(wLoc);
+  const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(interp_scaled(cn, k, sf, [&](int m) { return local_es3(P, l, m, ish); })));
+  const float c = __fmul_rn(__fsub_rn(1.f, wnc), 0.5f);
+  float s2L = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sL)));
+  const float sG = __fadd_rn(__fdiv_rn(sq2(local_wavelet(P, l, k, ish, gn)), wn2), sq2(local_es3(P, l, k, ish)));
+  const float s2G = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sG)));
+  const float wGlob2 = sq2(__ldg(P.wamp + (size_t)l * cn + k));
+  const float tau2 = __ldg(P.tau2 + (size_t)l * cn + k);
+  const float tm = __fmul_rn(0.05f, P.modW[l]);
+  const float wG2A = wGlob2 < tm ? __fmul_rn(0.5f, __fadd_rn(wGlob2, tm)) : wGlob2;
+  const float tg = __fmul_rn(0.05f, wG2A);
+  const float q = __fdiv_rn(wG2A, __fadd_rn(__fmul_rn(tau2, wGlob2), s2G));
+  float wL2A = wLoc2;
+  if (wLoc2 < tm) wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, tm));
+  if (wL2A < tg) {
+    wL2A = __fmul_rn(0.5f, __fadd_rn(wLoc2, tg));
+    s2L = __fmul_rn(s2L, __fdiv_rn(wL2A, wLoc2));
+  }
+  const float dL = __fadd_rn(__fmul_rn(tau2, wL2A), s2L);
+  return make_float2(__fdiv_rn(__fdiv_rn(wLoc.x, dL), q), __fdiv_rn(__fdiv_rn(wLoc.y, dL), q));
+}
+
+// The index of the unpadded trace whose local wavelet a padded trace uses
+// (src/avoinversion.cpp:525-543).
+__device__ __forceinline__ int wavelet_index(int i, int n, int np) {
+  if (i > 3 * n - 1) i = 0;
+  if (i > (np + n) / 2) i = np - i;
+  if (i >= n) i = 2 * n - i - 1;
+  return i;
+}
+
 // One CTA: W complex lines (2W traces x = 2(m0 + w) + {0, 1}) of row j of angle blockIdx.z.
+// Mode 0 divides every padded trace by its scale wavelet; mode 1 convolves the traces
+// i < nx, j < ny with their local wavelets (multiplyDataByScaleWaveletAndWriteToFile,
+// src/avoinversion.cpp:743-776: 1/sqrt(nzp), r2c, times the conjugate of
+// getCAmp(k, relThick) at every kz, c2r, 1/sqrt(nzp)) and leaves the other traces as they are.
 __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ ThickParams P) {
   extern __shared__ float2 sm[];
   const int nzp = P.nzp, W = P.W, lw = P.logW, half = nzp / 2;
@@ -90,10 +171,13 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   float2* SC = R + (size_t)W * nzp;
   __shared__ float s_sf[2 * 32];
   __shared__ double s_df[2 * 32];
+  __shared__ float s_ish[2 * 32], s_gn[2 * 32];   // local wavelet shift (samples) and gain
   __shared__ int s_live[2 * 32];   // the trace has a nonzero tapered sample
   const int tid = threadIdx.x, T = blockDim.x;
   const int j = blockIdx.y, l = blockIdx.z;
   const int m0 = blockIdx.x * W;
+  const bool conv = P.mode == 1;
+  const int nlive = conv ? P.nx : P.nxp;   // traces this mode reads and writes
   float* g = P.grid[l];
   const size_t kstride = (size_t)P.nyp * P.rnxp;
   float* row = g + (size_t)j * P.rnxp;
@@ -103,10 +187,19 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   if (tid < 2 * W) {
     const int i = 2 * m0 + tid;
     double rt = 1.0;
-    if (i < P.nxp) rt = P.rel_thick[(size_t)j * P.nxp + i];
+    if (P.rel_thick && i < P.nxp) rt = P.rel_thick[(size_t)j * P.nxp + i];
     s_sf[tid] = (float)rt;
     s_df[tid] = __ddiv_rn(__dmul_rn((double)P.nz, 1000.0), __dmul_rn(__dmul_rn(rt, P.lz), (double)nzp));
     s_live[tid] = 0;
+    float ish = 0.f, gn = 1.f;
+    if (P.wshift && i < P.nxp) {
+      const size_t t = (size_t)l * P.nx * P.ny + (size_t)wavelet_index(j, P.ny, P.nyp) * P.nx +
+                       wavelet_index(i, P.nx, P.nxp);
+      ish = P.wshift[t];
+      gn = P.wgain[t];
+    }
+    s_ish[tid] = ish;
+    s_gn[tid] = gn;
   }
   __syncthreads();
   // load, 1/sqrt(nzp) and the z taper (:539-551); traces at or beyond nxp load as zero.
@@ -121,10 +214,10 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
       const int w = e & (W - 1), k = e >> lw;
       const int m = m0 + w;
       const float* p = row + (size_t)k * kstride + 2 * m;
-      if (2 * m + 1 < P.nxp) {
+      if (2 * m + 1 < nlive) {
         cp_async8(rb + 8u * (uint32_t)e, p);
       } else {
-        R[e] = make_float2(2 * m < P.nxp ? *p : 0.f, 0.f);
+        R[e] = make_float2(2 * m < nlive ? *p : 0.f, 0.f);
       }
     }
     cp_async_commit();
@@ -134,7 +227,7 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   for (int e = tid; e < W * nzp; e += T) {
     const int w = e & (W - 1), k = e >> lw;
     float2 v = R[e];
-    const float tz = __ldg(P.ztaper + k);
+    const float tz = conv ? 1.f : __ldg(P.ztaper + k);
     v.x = __fmul_rn(div_rsq(P, v.x), tz);
     v.y = __fmul_rn(div_rsq(P, v.y), tz);
     if (v.x != 0.f) s_live[2 * w] = 1;
@@ -155,13 +248,32 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
     float2 b = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
     const int m = m0 + w;
     float2 fa = make_float2(0.f, 0.f), fb = fa;
-    if (2 * m < P.nxp) {
-      const double fk = __dmul_rn(s_df[2 * w], (double)k);
-      if (fk < (double)P.high_cut && fk > (double)P.low_cut) fa = adjustment(P, l, k, s_sf[2 * w]);
-    }
-    if (2 * m + 1 < P.nxp) {
-      const double fk = __dmul_rn(s_df[2 * w + 1], (double)k);
-      if (fk < (double)P.high_cut && fk > (double)P.low_cut) fb = adjustment(P, l, k, s_sf[2 * w + 1]);
+    if (conv) {
+      // the conjugate of the local wavelet's stretched spectrum (getCAmp returns the
+      // conjugate's value, src/avoinversion.cpp:761-768)
+      if (2 * m < nlive) {
+        const float ish = s_ish[2 * w], gn = s_gn[2 * w];
+        const float2 v = interp_scaled(P.cnzp, k, s_sf[2 * w], [&](int q) { return local_wavelet(P, l, q, ish, gn); });
+        fa = make_float2(v.x, -v.y);
+      }
+      if (2 * m + 1 < nlive) {
+        const float ish = s_ish[2 * w + 1], gn = s_gn[2 * w + 1];
+        const float2 v = interp_scaled(P.cnzp, k, s_sf[2 * w + 1], [&](int q) { return local_wavelet(P, l, q, ish, gn); });
+        fb = make_float2(v.x, -v.y);
+      }
+    } else {
+      if (2 * m < P.nxp) {
+        const double fk = __dmul_rn(s_df[2 * w], (double)k);
+        if (fk < (double)P.high_cut && fk > (double)P.low_cut)
+          fa = P.wshift ? adjustment_local(P, l, k, s_sf[2 * w], s_ish[2 * w], s_gn[2 * w])
+                        : adjustment(P, l, k, s_sf[2 * w]);
+      }
+      if (2 * m + 1 < P.nxp) {
+        const double fk = __dmul_rn(s_df[2 * w + 1], (double)k);
+        if (fk < (double)P.high_cut && fk > (double)P.low_cut)
+          fb = P.wshift ? adjustment_local(P, l, k, s_sf[2 * w + 1], s_ish[2 * w + 1], s_gn[2 * w + 1])
+                        : adjustment(P, l, k, s_sf[2 * w + 1]);
+      }
     }
     a = cmul(a, fa);
     b = cmul(b, fb);
@@ -178,11 +290,13 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   for (int e = tid; e < W * nzp; e += T) {
     const int w = e & (W - 1), k = e >> lw;
     const int m = m0 + w;
-    if (2 * m >= P.nxp) continue;
+    if (2 * m >= nlive) continue;
     float* p = row + (size_t)k * kstride + 2 * m;
     const float2 v = R[e];
-    const float2 o = make_float2(s_live[2 * w] ? div_rsq(P, v.x) : 0.f, s_live[2 * w + 1] ? div_rsq(P, v.y) : 0.f);
-    if (2 * m + 1 < P.nxp) *reinterpret_cast<float2*>(p) = o;
+    float2 o;
+    if (conv) o = make_float2(s_live[2 * w] ? __fdiv_rn(v.x, P.rsq_out) : 0.f, s_live[2 * w + 1] ? __fdiv_rn(v.y, P.rsq_out) : 0.f);
+    else o = make_float2(s_live[2 * w] ? div_rsq(P, v.x) : 0.f, s_live[2 * w + 1] ? div_rsq(P, v.y) : 0.f);
+    if (2 * m + 1 < nlive) *reinterpret_cast<float2*>(p) = o;
     else *p = o.x;
   }
 }
@@ -267,7 +381,7 @@ cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, 
   const size_t smem = thick_smem_bytes(P.W, P.nzp);
   cudaError_t e = cudaFuncSetAttribute(k_thick_divide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)P.nIT, (unsigned)P.nyp, (unsigned)nth);
+  dim3 grid((unsigned)P.nIT, (unsigned)(P.mode == 1 ? P.ny : P.nyp), (unsigned)nth);
   k_thick_divide<<<grid, 256, smem, st>>>(P);
   if (nlaunch) (*nlaunch)++;
   return cudaGetLastError();

@@ -183,10 +183,36 @@ crava_status crava_job_counters(crava_job* job, crava_counters* out);
  * as the reference's constructor does before the data transform (:226-227).  Call it
  * after the DATA uploads and before crava_job_run.  The trace-interpolation plan is made
  * on the host from the trace energies, so the call returns after `stream` has finished
- * the work.  Wavelets are 1D without local shift or gain grids (the local wavelet of
- * every trace is the global one stretched by rel_thick).  Returns CRAVA_ESTATE for a job
- * without the flag. */
+ * the work.  Wavelets are 1D: the local wavelet of every trace is the global one stretched
+ * by rel_thick, shifted and scaled by the trace's entries of the grids that
+ * crava_job_set_wavelet_grids gave (none: no shift, unit gain).  Returns CRAVA_ESTATE for a
+ * job without the flag. */
 crava_status crava_job_divide_data(crava_job* job, void* stream);
+
+/* Local wavelet grids of angle stack `angle` (Wavelet::getLocalTimeshift /
+ * getLocalGainFactor, src/wavelet.cpp:1251-1278, applied by Wavelet1D::shiftAndScale,
+ * src/wavelet1D.cpp:580-602, when createLocalWavelet1D builds a trace's wavelet): shift_ms
+ * (time shift in ms) and gain, nx*ny floats each (index i + nx*j), host memory; NULL for
+ * either means none; WELLMISSING (-999) entries mean no shift / unit gain.  Padded traces use
+ * the wavelet of the unpadded trace the reference maps them to (src/avoinversion.cpp:525-543).
+ * Used by crava_job_divide_data and crava_job_residual_synthetics from the next call on.  The
+ * first call allocates 2*ntheta*nx*ny floats of device memory outside the job's footprint
+ * (crava_job_footprint) and is synchronous.  The reference re-transforms each local wavelet
+ * before taking its errorSmooth3 spectrum (the difference constructors work on samples); this
+ * library turns the global spectra directly, which differs by the rounding of that round trip. */
+crava_status crava_job_set_wavelet_grids(crava_job* job, int angle, const float* shift_ms, const float* gain);
+
+/* AVOInversion::multiplyDataByScaleWaveletAndWriteToFile (src/avoinversion.cpp:721-790), the
+ * wavelet-convolved residuals the reference writes after the inversion (:1123): for a job
+ * with CRAVA_FLAG_KEEP_RESIDUAL after crava_job_run, every residual spectrum is transformed
+ * back (FFTGrid::invFFTInPlace) and every trace i < nx, j < ny is convolved along z with its
+ * local wavelet (1/sqrt(nzp), r2c, times the conjugate of the wavelet spectrum stretched by
+ * rel_thick (1 for constant thickness), shifted and scaled by the wavelet grids, c2r,
+ * 1/sqrt(nzp)); the padding traces keep the transformed-back residual.  CRAVA_ROLE_RESIDUAL
+ * then reads real rnxp*nyp*nzp grids.  Once per run (CRAVA_ESTATE otherwise).  A job without
+ * CRAVA_FLAG_NONCONST_THICK allocates its wavelet spectra (ntheta*(nzp/2+1) complex) on the
+ * first call, outside its footprint. */
+crava_status crava_job_residual_synthetics(crava_job* job, void* stream);
 
 /* Local noise (ModelAVODynamic::GetUseLocalNoise): AVOInversion::correctVpVsRho with
  * newPosteriorCovPointwise (src/avoinversion.cpp:2028-2302) and the local-noise mixing of

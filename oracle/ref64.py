@@ -214,6 +214,43 @@ def camp_scaled32(c: np.ndarray, k, scale):
     return re.astype(f32), im.astype(f32)
 
 
+def interp_scaled32(at, cn: int, k, scale):
+    """Wavelet::getCAmp(k, scale) as camp_scaled32 for a spectrum given by at(m) -> (re, im)
+    float32 arrays (m an index array broadcasting with k and scale)."""
+    f32 = np.float32
+    k = np.asarray(k)
+    scale = np.asarray(scale, dtype=f32)
+    om = k.astype(f32) / scale
+    valid = om < f32(cn)
+    lo = np.where(valid, np.floor(om), 0).astype(np.int64)
+    hi = lo + 1
+    hi = np.where(hi >= cn, hi - 1, hi)
+    d = (om - lo.astype(f32)).astype(f32)
+    e = (f32(1.0) - d).astype(f32)
+    ar, ai = at(lo)
+    br, bi = at(hi)
+    re = ((ar * e).astype(f32) + (br * d).astype(f32)).astype(f32) / scale
+    im = ((ai * e).astype(f32) + (bi * d).astype(f32)).astype(f32) / scale
+    re = np.where(valid, re, f32(0))
+    im = np.where(valid, im, f32(0))
+    return re.astype(f32), im.astype(f32)
+
+
+def shift_scale32(c: np.ndarray, ish, gain, m, nzp: int):
+    """Wavelet1D::shiftAndScale (src/wavelet1D.cpp:580-602) at bins m of the half spectrum c
+    (complex64): multiplier float(gain cos(a)) + i float(gain sin(-a)) with
+    a = 2 (pi iShift m) / float(nzp) in double, product in float32.  Returns (re, im)."""
+    f32 = np.float32
+    m = np.asarray(m)
+    a = 2.0 * (math.pi * np.asarray(ish, dtype=f32).astype(np.float64) * m.astype(np.float64)) / float(f32(nzp))
+    g = np.asarray(gain, dtype=f32).astype(np.float64)
+    mr = (g * np.cos(a)).astype(f32)
+    mi = (g * np.sin(-a)).astype(f32)
+    cr, ci = c.real.astype(f32)[m], c.imag.astype(f32)[m]
+    return ((mr * cr).astype(f32) - (mi * ci).astype(f32)).astype(f32), \
+        ((mi * cr).astype(f32) + (mr * ci).astype(f32)).astype(f32)
+
+
 def inverse_abs_kw_robust(W: np.ndarray, wnorm: float) -> np.ndarray:
     """AVOInversion::fillInverseAbskWRobust (src/avoinversion.cpp:1296-1322): per kz,
     1/sqrt(max(|W(k)|^2, |W(k; 0.999)|^2)) in float32 (W the full spectrum; a large
@@ -291,6 +328,7 @@ def thick_tables(blk):
         c3 = f32(1.0) / f32(np.sqrt(norm2))
         es3 = (E3.real * c3).astype(f32) + 1j * (E3.imag * c3).astype(f32)
         es3 = es3.astype(np.complex64)
+        out.setdefault("es3_last", []).append(es3[cn - 1])
         es3.imag[cn - 1] = -99999.0
         if n % 2 == 0:
             es3.real[cn - 1] = -99999.0
@@ -356,12 +394,104 @@ def adjustment_factor(tab, l: int, sf, k) -> np.ndarray:
     return fr.astype(np.float64) + 1j * fi.astype(np.float64)
 
 
-def divide_data_by_scale_wavelet(blk) -> np.ndarray:
+def adjustment_factor_local(tab, l: int, sf, k, ish, gn, nzp: int) -> np.ndarray:
+    """computeAdjustmentFactor (src/avoinversion.cpp:630-719) for traces whose local wavelet
+    carries a shift ish (samples) and a gain gn (createLocalWavelet1D + shiftAndScale,
+    src/wavelet1D.cpp:518-602): wLoc and eSkLoc from the shifted and scaled spectra stretched
+    by sf, eSkGlob from the same spectra unstretched, wGlob from the global wavelet.  The
+    local errorSmooth3 is the global one turned by the unit-modulus multiplier (its band
+    normalisation removes the gain) with the RMISSING entry at cnzp - 1 kept; the
+    reference's round trip of the local wavelet through the time domain is not restated.
+    float32 in the reference's operation order; sf, k, ish, gn broadcast."""
+    f32 = np.float32
+    wa, es = tab["wamp"][l], tab["es3"][l]
+    es_last = tab["es3_last"][l]
+    cn = wa.shape[0]
+    wn2, modW, ev = tab["wn2"][l], tab["modW"][l], tab["err_var"][l]
+    wnc = f32(tab["wnc"])
+    k = np.asarray(k)
+    es_true = es.copy()
+    es_true[cn - 1] = es_last
+
+    def wl(m):
+        return shift_scale32(wa, ish, gn, m, nzp)
+
+    def el(m):
+        r, i = shift_scale32(es_true, ish, f32(1.0), m, nzp)
+        last = np.asarray(m) == cn - 1
+        i = np.where(last, f32(-99999.0), i).astype(f32)
+        if nzp % 2 == 0:
+            r = np.where(last, f32(-99999.0), r).astype(f32)
+        return r, i
+
+    lr, li = interp_scaled32(wl, cn, k, sf)
+    wLoc2 = (lr * lr + li * li).astype(f32)
+    er, ei = interp_scaled32(el, cn, k, sf)
+    sL = (wLoc2 / wn2 + (er * er + ei * ei)).astype(f32)
+    gr, gi = wl(np.broadcast_to(k, np.broadcast(k, ish).shape))
+    sgr, sgi = el(np.broadcast_to(k, np.broadcast(k, ish).shape))
+    sG = ((gr * gr + gi * gi).astype(f32) / wn2 + (sgr * sgr + sgi * sgi)).astype(f32)
+    c = (f32(1.0) - wnc) * f32(0.5)
+    s2L = (ev * (wnc + c * sL)).astype(f32)
+    s2G = (ev * (wnc + c * sG)).astype(f32)
+    wgr, wgi = wa.real.astype(f32)[k], wa.imag.astype(f32)[k]
+    wGlob2 = (wgr * wgr + wgi * wgi).astype(f32)
+    tau2 = tab["tau2"][l][k]
+    tm = f32(0.05) * modW
+    wG2A = np.where(wGlob2 < tm, f32(0.5) * (wGlob2 + tm), wGlob2).astype(f32)
+    wL2A = np.where(wLoc2 < tm, f32(0.5) * (wLoc2 + tm), wLoc2).astype(f32)
+    tg = (f32(0.05) * wG2A).astype(f32)
+    adj = wL2A < tg
+    wL2A = np.where(adj, f32(0.5) * (wLoc2 + tg), wL2A).astype(f32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        s2L = np.where(adj, s2L * (wL2A / wLoc2), s2L).astype(f32)
+        dL = (tau2 * wL2A + s2L).astype(f32)
+        q = (wG2A / (tau2 * wGlob2 + s2G)).astype(f32)
+        fr = ((lr / dL) / q).astype(f32)
+        fi = ((li / dL) / q).astype(f32)
+    return fr.astype(np.float64) + 1j * fi.astype(np.float64)
+
+
+def wavelet_index(i: int, n: int, np_: int) -> int:
+    """The unpadded trace whose local wavelet padded trace i uses (src/avoinversion.cpp:525-543)."""
+    if i > 3 * n - 1:
+        i = 0
+    if i > (np_ + n) // 2:
+        i = np_ - i
+    if i >= n:
+        i = 2 * n - i - 1
+    return i
+
+
+def local_wavelet_maps(blk, shift_ms, gain):
+    """Per angle and padded trace (ntheta, nyp, nxp) the shift in samples (float(shift) /
+    float(dz), dz = lz / nz) and the gain of the local wavelet; -999 entries are no shift and
+    unit gain; None grids are none."""
+    f32 = np.float32
+    nth, nx, ny, nxp, nyp = blk.ntheta, blk.nx, blk.ny, blk.nxp, blk.nyp
+    dz = f32(blk.lz / blk.nz)
+    ish = np.zeros((nth, ny, nx), dtype=f32)
+    gn = np.ones((nth, ny, nx), dtype=f32)
+    for l in range(nth):
+        if shift_ms is not None and shift_ms[l] is not None:
+            sh = np.asarray(shift_ms[l], dtype=f32)
+            ish[l] = np.where(sh != f32(-999.0), (sh / dz).astype(f32), f32(0))
+        if gain is not None and gain[l] is not None:
+            g = np.asarray(gain[l], dtype=f32)
+            gn[l] = np.where(g != f32(-999.0), g, f32(1))
+    ii = np.array([wavelet_index(i, nx, nxp) for i in range(nxp)])
+    jj = np.array([wavelet_index(j, ny, nyp) for j in range(nyp)])
+    return ish[:, jj][:, :, ii], gn[:, jj][:, :, ii]
+
+
+def divide_data_by_scale_wavelet(blk, shift_ms=None, gain=None) -> np.ndarray:
     """AVOInversion::divideDataByScaleWavelet (src/avoinversion.cpp:484-612) on every data
     grid: per trace (i < nxp, j < nyp) the 1/sqrt(nzp) scale and z taper, r2c along z,
     the adjustment factor inside the band deltaF*k in (lowCut, highCut) with
     deltaF = nz*1000/(relThick*lz*nzp) and zero outside, c2r, 1/sqrt(nzp).  The transforms
-    in float64.  Returns (ntheta, nzp, nyp, rnxp) float64 (padding columns zero)."""
+    in float64.  shift_ms / gain: per angle (ny, nx) local wavelet grids or None
+    (adjustment_factor_local).  Returns (ntheta, nzp, nyp, rnxp) float64 (padding columns
+    zero)."""
     f32 = np.float32
     nxp, nyp, nzp, nz = blk.nxp, blk.nyp, blk.nzp, blk.nz
     cn = nzp // 2 + 1
@@ -380,13 +510,48 @@ def divide_data_by_scale_wavelet(blk) -> np.ndarray:
     fk = deltaF[None] * k[:, None, None]                         # (cn, nyp, nxp)
     band = (fk < float(f32(blk.high_cut))) & (fk > float(f32(blk.low_cut)))
     out = np.zeros((blk.ntheta, nzp, nyp, 2 * (nxp // 2 + 1)))
+    local = shift_ms is not None or gain is not None
+    if local:
+        ish, gn = local_wavelet_maps(blk, shift_ms, gain)
     for l in range(blk.ntheta):
         v = (blk.data[l][..., :nxp].astype(f32) / rsq).astype(f32) * taper[:, None, None]
         spec = np.fft.rfft(v.astype(np.float64), axis=0)
-        fac = adjustment_factor(tab, l, sf[None], k[:, None, None])
+        if local:
+            fac = adjustment_factor_local(tab, l, sf[None], k[:, None, None], ish[l][None], gn[l][None], nzp)
+        else:
+            fac = adjustment_factor(tab, l, sf[None], k[:, None, None])
         spec = np.where(band, spec * fac, 0.0)
         res = np.fft.irfft(spec, n=nzp, axis=0) * nzp / float(rsq)
         out[l, ..., :nxp] = res
+    return out
+
+
+def residual_synthetics(blk, resid: np.ndarray, shift_ms=None, gain=None) -> np.ndarray:
+    """AVOInversion::multiplyDataByScaleWaveletAndWriteToFile (src/avoinversion.cpp:721-790)
+    on real residual grids resid (ntheta, nzp, nyp, rnxp) (after invFFTInPlace): every trace
+    i < nx, j < ny divided by float(sqrt(float(nzp))), r2c along z, times the conjugate of
+    its local wavelet's spectrum stretched by relThick (getCAmp(k, sf)), c2r, divided by
+    float(sqrt(double(nzp))); the other traces as given.  Transforms in float64."""
+    f32 = np.float32
+    nx, ny, nzp = blk.nx, blk.ny, blk.nzp
+    cn = nzp // 2 + 1
+    rsq = f32(np.sqrt(f32(nzp)))
+    rsq_out = f32(np.sqrt(float(nzp)))
+    W = [np.fft.fft(blk.wavelet[l].astype(f32).astype(np.float64))[:cn].astype(np.complex64)
+         for l in range(blk.ntheta)]
+    rt = getattr(blk, "rel_thick", None)
+    sf = (np.asarray(rt, dtype=np.float64)[:ny, :nx].astype(f32) if rt is not None
+          else np.ones((ny, nx), dtype=f32))
+    ish, gn = local_wavelet_maps(blk, shift_ms, gain)
+    k = np.arange(cn)[:, None, None]
+    out = np.array(resid, dtype=np.float64, copy=True)
+    for l in range(blk.ntheta):
+        v = (np.asarray(resid[l][:, :ny, :nx], dtype=f32) / rsq).astype(f32)
+        spec = np.fft.rfft(v.astype(np.float64), axis=0)
+        wr, wi = interp_scaled32(lambda m: shift_scale32(W[l], ish[l][None, :ny, :nx], gn[l][None, :ny, :nx], m, nzp),
+                                 cn, k, sf[None])
+        spec = spec * (wr.astype(np.float64) - 1j * wi.astype(np.float64))
+        out[l][:, :ny, :nx] = np.fft.irfft(spec, n=nzp, axis=0) * nzp / float(rsq_out)
     return out
 
 

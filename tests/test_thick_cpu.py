@@ -171,3 +171,44 @@ def test_division_restatement_matches_the_golden_fixture():
     for l in range(b.ntheta):
         x, r = mine[l][..., :b.nxp], ref[l][..., :b.nxp].astype(np.float64)
         assert np.linalg.norm(x - r) / np.linalg.norm(r) < 2e-6, l
+
+
+def test_local_factor_with_neutral_grids_is_the_global_factor(blk):
+    """Zero shift and unit gain: the local-wavelet restatement of computeAdjustmentFactor
+    gives the global one bit for bit."""
+    tab = ref64.thick_tables(blk)
+    tab["wnc"] = blk.wnc
+    cn = blk.nzp // 2 + 1
+    k = np.arange(cn)[:, None]
+    sf = np.array([[0.8, 1.0, 1.3]], dtype=np.float32)
+    for l in range(blk.ntheta):
+        g = ref64.adjustment_factor(tab, l, sf, k)
+        loc = ref64.adjustment_factor_local(tab, l, sf, k, np.float32(0.0), np.float32(1.0), blk.nzp)
+        assert np.array_equal(g, loc)
+
+
+def test_wavelet_index_maps_padding_onto_the_interior():
+    n, np_ = 10, 16
+    idx = [ref64.wavelet_index(i, n, np_) for i in range(np_)]
+    assert idx[:n] == list(range(n))
+    assert all(0 <= i < n for i in idx)
+    assert idx[n] == n - 1 and idx[np_ - 1] == 1
+
+
+def test_residual_convolution_with_an_integer_shift_and_gain(blk):
+    """shiftAndScale by a whole number of samples s and a gain g: the convolved residual is
+    the unshifted one advanced by s samples and scaled by g (constant thickness, sf = 1)."""
+    b = dataclasses.replace(blk, rel_thick=None)
+    rng = np.random.default_rng(2)
+    resid = rng.standard_normal((b.ntheta, b.nzp, b.nyp, 2 * (b.nxp // 2 + 1)))
+    dz = b.lz / b.nz
+    s, g = 3, 1.5
+    shifts = [np.full((b.ny, b.nx), s * dz, np.float32)] * b.ntheta
+    gains = [np.full((b.ny, b.nx), g, np.float32)] * b.ntheta
+    base = ref64.residual_synthetics(b, resid)
+    got = ref64.residual_synthetics(b, resid, shifts, gains)
+    want = g * np.roll(base[:, :, :b.ny, :b.nx], -s, axis=1)
+    err = np.linalg.norm(got[:, :, :b.ny, :b.nx] - want) / np.linalg.norm(want)
+    assert err < 1e-5
+    # the traces outside the interior are untouched
+    assert np.array_equal(got[:, :, b.ny:], resid[:, :, b.ny:])
