@@ -74,6 +74,12 @@ class SimboxGeom(ctypes.Structure):
                 ("xl_step_y", ctypes.c_double), ("angle", ctypes.c_double)]
 
 
+class StormGeom(ctypes.Structure):
+    _fields_ = [("xmin", ctypes.c_double), ("lx", ctypes.c_double), ("ymin", ctypes.c_double), ("ly", ctypes.c_double),
+                ("lz", ctypes.c_double), ("angle", ctypes.c_double), ("cubetype", ctypes.c_int), ("flat", ctypes.c_int),
+                ("top_name", ctypes.c_char_p), ("bot_name", ctypes.c_char_p)]
+
+
 class FaciesDesc(ctypes.Structure):
     _fields_ = [("nfacies", ctypes.c_int), ("nbins", ctypes.c_int * 3), ("vmin", ctypes.c_double * 3),
                 ("dv", ctypes.c_double * 3), ("prior", _fp), ("p_undefined", ctypes.c_float)]
@@ -133,6 +139,8 @@ def lib() -> ctypes.CDLL:
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     L.crava_job_local_noise.argtypes = [vp, vp, vp]
     L.crava_job_set_wavelet_grids.argtypes = [vp, ctypes.c_int, vp, vp]
+    L.crava_grid_write_storm.argtypes = [vp, ctypes.c_char_p, vp] + [ctypes.c_int] * 7 + [ctypes.POINTER(StormGeom), vp]
+    L.crava_grid_read_storm.argtypes = [vp, ctypes.c_char_p, vp] + [ctypes.c_int] * 6 + [ctypes.POINTER(StormGeom), vp]
     L.crava_job_residual_synthetics.argtypes = [vp, vp]
     L.crava_grid_write_crava.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(SimboxGeom), vp]
@@ -593,3 +601,26 @@ def grid_read_crava(ctx: Context, path: str, d_grid: int, rnxp: int, nyp: int, n
     g = SimboxGeom()
     _check(lib().crava_grid_read_crava(ctx.handle, str(path).encode(), d_grid, rnxp, nyp, nzp, ctypes.byref(g), stream))
     return {k: getattr(g, k) for k, _t in SimboxGeom._fields_}
+
+
+def grid_write_storm(ctx: Context, path: str, d_grid: int, dims, padded_dims, geom: dict, padding: bool = False,
+                     stream=None):
+    """FFTGrid::writeStormFile (binary) of a padded real device grid; dims = (nx, ny, nz),
+    padded_dims = (nxp, nyp, nzp); geom: xmin, lx, ymin, ly, lz, angle (radians), cubetype and
+    either flat=1 or top_name/bot_name."""
+    g = dict(geom)
+    for k in ("top_name", "bot_name"):
+        if g.get(k) is not None:
+            g[k] = str(g[k]).encode()
+    gs = StormGeom(**g)
+    _check(lib().crava_grid_write_storm(ctx.handle, str(path).encode(), d_grid, *dims, *padded_dims, int(padding),
+                                        ctypes.byref(gs), stream))
+
+
+def grid_read_storm(ctx: Context, path: str, d_grid: int, dims, padded_dims, stream=None) -> dict:
+    """A STORM binary grid into a padded real device grid with FFTGrid's padding fill; returns
+    the header's geometry."""
+    gs = StormGeom()
+    _check(lib().crava_grid_read_storm(ctx.handle, str(path).encode(), d_grid, *dims, *padded_dims,
+                                       ctypes.byref(gs), stream))
+    return {k: getattr(gs, k) for k, _t in StormGeom._fields_ if k not in ("top_name", "bot_name")}

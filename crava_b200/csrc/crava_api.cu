@@ -1203,6 +1203,163 @@ crava_status crava_grid_read_crava(crava_ctx* ctx, const char* path, float* d_gr
   return CRAVA_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// NRLib::ToString(x, 6): fixed notation with six decimals.
+std::string fixed6(double x) {
+  char b[64];
+  std::snprintf(b, sizeof(b), "%.6f", x);
+  return b;
+}
+
+std::string storm_header(const crava_storm_geom& g, int nx, int ny, int nz) {
+  std::string h = "storm_petro_binary\n";
+  h += "0 " + std::to_string(g.cubetype) + " " + fixed6(-99999.0) + "\n";
+  h += "FFTGrid\n";
+  h += fixed6(g.xmin) + " " + fixed6(g.lx) + " " + fixed6(g.ymin) + " " + fixed6(g.ly) + " ";
+  if (g.flat) h += "0.0 " + fixed6(g.lz) + " 0.0 0.0\n";
+  else h += std::string(g.top_name ? g.top_name : "") + " " + (g.bot_name ? g.bot_name : "") + " 0.0 0.0\n";
+  h += fixed6(g.lz) + " " + fixed6(g.angle * 180.0 / 3.14159265358979323846) + "\n\n";
+  h += std::to_string(nx) + " " + std::to_string(ny) + " " + std::to_string(nz) + "\n";
+  return h;
+}
+
+bool read_line(FILE* f, std::string& line) {
+  line.clear();
+  int ch;
+  while ((ch = std::fgetc(f)) != EOF && ch != '\n') line.push_back((char)ch);
+  return ch != EOF || !line.empty();
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_grid_write_storm(crava_ctx* ctx, const char* path, const float* d_grid, int nx, int ny, int nz,
+                                    int nxp, int nyp, int nzp, int padding, const crava_storm_geom* geom,
+                                    void* stream) {
+  if (!ctx || !path || !d_grid || !geom || nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny || nzp < nz)
+    return fail(CRAVA_EINVAL, "bad arguments");
+  if (!geom->flat && (!geom->top_name || !geom->bot_name || !*geom->top_name || !*geom->bot_name))
+    return fail(CRAVA_EINVAL, "a STORM header that is not flat names its top and base surfaces");
+  std::lock_guard<std::mutex> lk(ctx->io_mu);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  crava_status s = io_buffers(ctx);
+  if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int rnxp = 2 * (nxp / 2 + 1);
+  const int wx = padding ? nxp : nx, wy = padding ? nyp : ny, wz = padding ? nzp : nz;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(CRAVA_EINVAL, std::string("cannot open ") + path + " for writing");
+  const std::string h = storm_header(*geom, wx, wy, wz);
+  bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
+  const size_t total = (size_t)wx * wy * wz, per = kIoChunk / 4;
+  size_t pending[2] = {0, 0};
+  int nl = 0;
+  cudaError_t e = cudaSuccess;
+  auto flush = [&](int b) {
+    if (!pending[b]) return;
+    e = cudaEventSynchronize(ctx->io_ev[b]);
+    if (e == cudaSuccess) ok = ok && std::fwrite(ctx->io_host[b], 4, pending[b], f) == pending[b];
+    pending[b] = 0;
+  };
+  // chunk c: gather and swap into device staging half c%2, download into pinned half c%2;
+  // the file write of the previous chunk runs while this one is in flight
+  for (size_t e0 = 0, c = 0; ok && e == cudaSuccess && e0 < total; e0 += per, c++) {
+    const int b = (int)(c % 2);
+    const size_t n = std::min(per, total - e0);
+    flush(b);
+    if (e != cudaSuccess || !ok) break;
+    uint32_t* dst = (uint32_t*)(ctx->io_dev + b * kIoChunk);
+    e = launch_storm_pack(dst, d_grid, wx, wy, e0, n, rnxp, nyp, st);
+    nl++;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->io_host[b], dst, 4 * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->io_ev[b], st);
+    pending[b] = n;
+    if (e == cudaSuccess) flush(1 - b);
+  }
+  for (int b = 0; b < 2 && e == cudaSuccess; b++) flush(b);
+  ok = ok && std::fwrite("0\n", 1, 2, f) == 2;
+  ok = (std::fclose(f) == 0) && ok;
+  if (e != cudaSuccess) return cuda_fail(e, "crava_grid_write_storm");
+  if (!ok) return fail(CRAVA_EINVAL, std::string("write error on ") + path);
+  std::lock_guard<std::mutex> lk2(ctx->mu);
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+crava_status crava_grid_read_storm(crava_ctx* ctx, const char* path, float* d_grid, int nx, int ny, int nz, int nxp,
+                                   int nyp, int nzp, crava_storm_geom* geom, void* stream) {
+  if (!ctx || !path || !d_grid || nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny || nzp < nz)
+    return fail(CRAVA_EINVAL, "bad arguments");
+  std::lock_guard<std::mutex> lk(ctx->io_mu);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  crava_status s = io_buffers(ctx);
+  if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(CRAVA_EINVAL, std::string("cannot open ") + path);
+  std::string l[7];
+  bool hok = true;
+  for (int q = 0; q < 7 && hok; q++) hok = read_line(f, l[q]);
+  crava_storm_geom g{};
+  int fnx = 0, fny = 0, fnz = 0, zero = -1;
+  double missing = 0.0;
+  char top[256] = {0}, bot[256] = {0};
+  double lzf = 0.0, deg = 0.0;
+  hok = hok && l[0] == "storm_petro_binary" &&
+        std::sscanf(l[1].c_str(), "%d %d %lf", &zero, &g.cubetype, &missing) == 3 &&
+        std::sscanf(l[4].c_str(), "%lf %lf", &lzf, &deg) == 2 && l[5].empty() &&
+        std::sscanf(l[6].c_str(), "%d %d %d", &fnx, &fny, &fnz) == 3 &&
+        std::sscanf(l[3].c_str(), "%lf %lf %lf %lf %255s %255s", &g.xmin, &g.lx, &g.ymin, &g.ly, top, bot) == 6;
+  if (!hok) {
+    std::fclose(f);
+    return fail(CRAVA_EINVAL, std::string(path) + " is not a STORM binary grid");
+  }
+  if (fnx != nx || fny != ny || fnz != nz) {
+    std::fclose(f);
+    return fail(CRAVA_EINVAL, std::string("grid on file ") + path + " is " + std::to_string(fnx) + "x" +
+                                  std::to_string(fny) + "x" + std::to_string(fnz) + ", expected " +
+                                  std::to_string(nx) + "x" + std::to_string(ny) + "x" + std::to_string(nz));
+  }
+  g.flat = std::strcmp(top, "0.0") == 0 ? 1 : 0;
+  g.lz = lzf;
+  g.angle = deg * 3.14159265358979323846 / 180.0;
+  g.top_name = g.bot_name = nullptr;
+  if (geom) *geom = g;
+  const int rnxp = 2 * (nxp / 2 + 1);
+  const size_t total = (size_t)nx * ny * nz, per = kIoChunk / 4;
+  bool ok = true, used[2] = {false, false};
+  int nl = 0;
+  cudaError_t e = cudaSuccess;
+  // chunk c: read into pinned half c%2 once its previous upload has finished, upload into
+  // device staging half c%2, scatter and swap into the grid
+  for (size_t e0 = 0, c = 0; ok && e == cudaSuccess && e0 < total; e0 += per, c++) {
+    const int b = (int)(c % 2);
+    const size_t n = std::min(per, total - e0);
+    if (used[b]) e = cudaEventSynchronize(ctx->io_ev[b]);
+    if (e != cudaSuccess) break;
+    ok = std::fread(ctx->io_host[b], 4, n, f) == n;
+    if (!ok) break;
+    uint32_t* src = (uint32_t*)(ctx->io_dev + b * kIoChunk);
+    e = cudaMemcpyAsync(src, ctx->io_host[b], 4 * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_storm_unpack(d_grid, src, nx, ny, e0, n, rnxp, nyp, st);
+    nl++;
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->io_ev[b], st);
+    used[b] = true;
+  }
+  std::fclose(f);
+  if (e == cudaSuccess && ok) e = launch_pad_fill(d_grid, nx, ny, nz, nxp, nyp, nzp, rnxp, st, &nl);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "crava_grid_read_storm");
+  if (!ok) return fail(CRAVA_EINVAL, std::string(path) + " ends before its grid");
+  std::lock_guard<std::mutex> lk2(ctx->mu);
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
 crava_status crava_circ_corr_t(const double* prior_corr_t, int n, int min_int_fq, int nzp, float* out) {
   if (!prior_corr_t || !out || n < 1 || nzp < 2) return fail(CRAVA_EINVAL, "bad arguments");
   if (!(prior_corr_t[0] != 0.0)) return fail(CRAVA_EINVAL, "prior_corr_t[0] must be nonzero");

@@ -242,6 +242,16 @@ cudaError_t launch_spec_mul(float2* a, const float2* b, size_t n, cudaStream_t s
 // gridio.cu: dst[e] = src[e] with the byte order of every 4-byte word reversed (dst == src
 // allowed)
 cudaError_t launch_bswap32(uint32_t* dst, const uint32_t* src, size_t n, cudaStream_t st);
+// STORM grid files (gridio.cu): elements e0 .. e0+n-1 of the dense ordering (i fastest) of
+// the nx x ny x nz region of a padded real grid (row pitch rnxp, nyp rows per slice) to
+// big-endian words and back, and the linear padding fill of FFTGrid's StormContGrid
+// constructor.
+cudaError_t launch_storm_pack(uint32_t* dst, const float* grid, int nx, int ny, size_t e0, size_t n, int rnxp,
+                              int nyp, cudaStream_t st);
+cudaError_t launch_storm_unpack(float* grid, const uint32_t* src, int nx, int ny, size_t e0, size_t n, int rnxp,
+                                int nyp, cudaStream_t st);
+cudaError_t launch_pad_fill(float* grid, int nx, int ny, int nz, int nxp, int nyp, int nzp, int rnxp, cudaStream_t st,
+                            int* nlaunch);
 struct FaciesCornersHost {
   int nang;
   const float* t;                                 // device, nang x ny x nx

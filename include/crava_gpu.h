@@ -265,6 +265,34 @@ crava_status crava_grid_write_crava(crava_ctx* ctx, const char* path, const floa
 crava_status crava_grid_read_crava(crava_ctx* ctx, const char* path, float* d_grid, int rnxp, int nyp, int nzp,
                                    crava_simbox_geom* geom, void* stream);
 
+/* STORM grid files.
+ * crava_grid_write_storm: FFTGrid::writeStormFile (src/fftgrid.cpp:1889-1930), binary form:
+ * the header of Simbox::getStormHeader (src/simbox.cpp:1012-1034; numbers in fixed notation
+ * with six decimals, the angle in degrees), then the nx*ny*nz values (padding = 0) or the
+ * nxp*nyp*nzp values (padding = 1) of the padded real device grid, i fastest then j then k, as
+ * big-endian floats, then "0\n".  Staged through the context's pinned chunks as the CRAVA
+ * format.
+ * crava_grid_read_storm: a STORM binary grid of that layout (storm_petro_binary, nx ny nz on
+ * the header's last line, which must equal the given ones) into the interior of a padded real
+ * device grid, whose padding is then filled as FFTGrid's StormContGrid constructor does
+ * (src/fftgrid.cpp:215-302: linear blends of the two edge values, z padding first, then y,
+ * then x, zero beyond nxp).  geom receives the header's numbers (top_name and bot_name NULL;
+ * flat when the surface fields read 0.0).  Both return after the work is done. */
+typedef struct {
+  double xmin, lx, ymin, ly;   /* Simbox::GetXMin, GetLX, GetYMin, GetLY        */
+  double lz;                   /* Simbox::GetLZ                                 */
+  double angle;                /* Simbox::GetAngle (radians)                    */
+  int cubetype;                /* FFTGrid cube type written into the header     */
+  int flat;                    /* 1: flat header (0.0 and lz in place of the surface names) */
+  const char* top_name;        /* flat == 0: the top and base surface names     */
+  const char* bot_name;
+} crava_storm_geom;
+crava_status crava_grid_write_storm(crava_ctx* ctx, const char* path, const float* d_grid, int nx, int ny, int nz,
+                                    int nxp, int nyp, int nzp, int padding, const crava_storm_geom* geom,
+                                    void* stream);
+crava_status crava_grid_read_storm(crava_ctx* ctx, const char* path, float* d_grid, int nx, int ny, int nz, int nxp,
+                                   int nyp, int nzp, crava_storm_geom* geom, void* stream);
+
 /* Host-side temporal prior functions (no device needed).
  * crava_circ_corr_t: SeismicParametersHolder::computeCircCorrT with makeCircCorrTPosDef
  * (src/seismicparametersholder.cpp:624-660, 805-840): the circular temporal correlation of

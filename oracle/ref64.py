@@ -1114,3 +1114,37 @@ def facies_density_corners(post, corners, scales, nx, ny, nz, t=None):
                         d = d + wa * wb * we * D[idx[2][e], idx[1][b], idx[0][a]]
             out[f] += d * wc[None]
     return np.maximum(out, 0.0)
+
+
+# ---------------------------------------------------------------- STORM grids
+
+def storm_padding(vals: np.ndarray, nxp: int, nyp: int, nzp: int) -> np.ndarray:
+    """FFTGrid(const StormContGrid*, nxp, nyp, nzp) (src/fftgrid.cpp:215-302): the interior
+    values vals (nz, ny, nx) float32 in a padded real grid (nzp, nyp, rnxp) whose padding is
+    the float32 blend c1 w1 + c2 w2 of two edge values, in the reference's loop and branch
+    order (k, then j, then i; z padding, else y padding, else x padding; zero beyond nxp)."""
+    f32 = np.float32
+    nz, ny, nx = vals.shape
+    rnxp = 2 * (nxp // 2 + 1)
+    g = np.zeros((nzp, nyp, rnxp), dtype=f32)
+    sc = f32(1.0) / f32(nzp - nz + 1)
+    sb = f32(1.0) / f32(nyp - ny + 1)
+    sa = f32(1.0) / f32(nxp - nx + 1)
+    ii = np.arange(nx, nxp)
+    wa1 = (sa * (ii - nx + 1).astype(f32)).astype(f32)
+    wa2 = (sa * (nxp - ii).astype(f32)).astype(f32)
+    for k in range(nzp):
+        for j in range(nyp):
+            row = g[k, j]
+            if k >= nz:
+                w1 = f32(sc * f32(k - nz + 1))
+                w2 = f32(sc * f32(nzp - k))
+                row[:nxp] = (g[0, j, :nxp] * w1).astype(f32) + (g[nz - 1, j, :nxp] * w2).astype(f32)
+            elif j >= ny:
+                w1 = f32(sb * f32(j - ny + 1))
+                w2 = f32(sb * f32(nyp - j))
+                row[:nxp] = (g[k, 0, :nxp] * w1).astype(f32) + (g[k, ny - 1, :nxp] * w2).astype(f32)
+            else:
+                row[:nx] = vals[k, j]
+                row[nx:nxp] = (row[0] * wa1).astype(f32) + (row[nx - 1] * wa2).astype(f32)
+    return g

@@ -61,3 +61,60 @@ def test_posterior_mean_written_as_crava_file(tmp_path):
     assert np.array_equal(vals.reshape(job.shape), job.download(api.ROLE_POST_MEAN, 0))
     job.close()
     ctx.close()
+
+
+STORM = dict(xmin=456000.0, lx=1525.0, ymin=6780000.5, ly=462.5, lz=120.0, angle=0.3, cubetype=3)
+
+
+def storm_header(g, nx, ny, nz, flat, top="", bot=""):
+    """Simbox::getStormHeader (src/simbox.cpp:1012-1034) restated with Python formatting."""
+    f = lambda x: "%.6f" % x
+    h = "storm_petro_binary\n0 %d %s\nFFTGrid\n" % (g["cubetype"], f(-99999.0))
+    h += " ".join(f(g[k]) for k in ("xmin", "lx", "ymin", "ly")) + " "
+    h += ("0.0 %s 0.0 0.0\n" % f(g["lz"])) if flat else ("%s %s 0.0 0.0\n" % (top, bot))
+    h += "%s %s\n\n%d %d %d\n" % (f(g["lz"]), f(g["angle"] * 180.0 / np.pi), nx, ny, nz)
+    return h.encode()
+
+
+@pytest.mark.parametrize("dims,flat,padding", [((61, 37, 45, 64, 40, 50), True, False),
+                                               ((61, 37, 45, 64, 40, 50), False, True),
+                                               ((300, 200, 250, 320, 210, 256), True, False)])
+def test_storm_file_format_round_trip_and_padding(tmp_path, dims, flat, padding):
+    import torch
+    from oracle import ref64
+    nx, ny, nz, nxp, nyp, nzp = dims
+    rnxp = 2 * (nxp // 2 + 1)
+    rng = np.random.default_rng(nx + nz)
+    grid = rng.standard_normal((nzp, nyp, rnxp)).astype(np.float32)
+    ctx = api.Context(0)
+    d = torch.from_numpy(grid).cuda()
+    path = tmp_path / "g.storm"
+    geom = dict(STORM, flat=1) if flat else dict(STORM, flat=0, top_name="top.irap", bot_name="base.irap")
+    api.grid_write_storm(ctx, str(path), d.data_ptr(), (nx, ny, nz), (nxp, nyp, nzp), geom, padding=padding)
+    raw = path.read_bytes()
+    wx, wy, wz = (nxp, nyp, nzp) if padding else (nx, ny, nz)
+    head = storm_header(STORM, wx, wy, wz, flat, "top.irap", "base.irap")
+    assert raw[:len(head)] == head
+    assert raw.endswith(b"0\n")
+    vals = np.frombuffer(raw[len(head):-2], dtype=">f4").reshape(wz, wy, wx)
+    assert np.array_equal(vals, grid[:wz, :wy, :wx])
+    if padding:
+        return
+    # read back: the interior as written, the padding as the StormContGrid constructor fills it
+    back = torch.full_like(d, 7.0)
+    g2 = api.grid_read_storm(ctx, str(path), back.data_ptr(), (nx, ny, nz), (nxp, nyp, nzp))
+    got = back.cpu().numpy()
+    ref = ref64.storm_padding(grid[:nz, :ny, :nx], nxp, nyp, nzp)
+    assert np.array_equal(got, ref)
+    assert g2["cubetype"] == STORM["cubetype"] and g2["flat"] == 1
+    assert g2["lz"] == pytest.approx(STORM["lz"]) and g2["angle"] == pytest.approx(STORM["angle"], abs=1e-7)
+    assert g2["xmin"] == pytest.approx(STORM["xmin"]) and g2["ly"] == pytest.approx(STORM["ly"])
+    with pytest.raises(api.CravaError) as e:
+        api.grid_read_storm(ctx, str(path), back.data_ptr(), (nx, ny, nz + 1), (nxp, nyp, nzp))
+    assert e.value.status == api.EINVAL
+    bad = tmp_path / "bad.storm"
+    bad.write_bytes(b"crava_fftgrid_binary\n" + raw[:200])
+    with pytest.raises(api.CravaError) as e:
+        api.grid_read_storm(ctx, str(bad), back.data_ptr(), (nx, ny, nz), (nxp, nyp, nzp))
+    assert e.value.status == api.EINVAL
+    ctx.close()

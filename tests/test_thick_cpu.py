@@ -212,3 +212,22 @@ def test_residual_convolution_with_an_integer_shift_and_gain(blk):
     assert err < 1e-5
     # the traces outside the interior are untouched
     assert np.array_equal(got[:, :, b.ny:], resid[:, :, b.ny:])
+
+
+def test_storm_padding_restatement_blends_the_edges():
+    """The StormContGrid padding: z padding blends slices 0 and nz-1 with weights that step
+    from the last slice's value towards the first slice's across the padding."""
+    rng = np.random.default_rng(1)
+    vals = rng.standard_normal((5, 4, 3)).astype(np.float32)
+    g = ref64.storm_padding(vals, 6, 7, 9)
+    assert np.array_equal(g[:5, :4, :3], vals)
+    assert np.all(g[..., 6:] == 0)
+    sc = np.float32(1.0) / np.float32(9 - 5 + 1)
+    k = 5
+    want = (g[0, 2, 1] * np.float32(sc * np.float32(k - 5 + 1))).astype(np.float32) + \
+        (g[4, 2, 1] * np.float32(sc * np.float32(9 - k))).astype(np.float32)
+    assert g[k, 2, 1] == want
+    # x padding of an interior row is the blend of its first and last values
+    sa = np.float32(1.0) / np.float32(6 - 3 + 1)
+    assert g[1, 1, 3] == (g[1, 1, 0] * np.float32(sa * 1)).astype(np.float32) + \
+        (g[1, 1, 2] * np.float32(sa * 3)).astype(np.float32)
