@@ -776,19 +776,33 @@ class Posterior:
         self.n_chol_fail = 0
 
 
-def posterior(blk, slab: int = 16, cov_grids=None) -> Posterior:
+def posterior(blk, slab: int = 16, cov_grids=None, separable: bool = False) -> Posterior:
     """AVOInversion constructor FFTs + computePostMeanResidAndFFTCov + invFFTCovGrids;
-    cov_grids: the six prior covariance grids when not those of prior_cov_grids(blk)."""
+    cov_grids: the six prior covariance grids when not those of prior_cov_grids(blk).
+    separable (zero correlation gradients only): the prior and error-correlation spectra
+    formed slab by slab as FFT2(corrXY) x FFT1(circCorrT) (and FFT2(corrXY) for the error
+    correlation, a delta in time) instead of transforming the seven full grids; equal to the
+    grid path up to the float32 rounding of the grids' products corrXY * circCorrT, and without
+    their memory, for full-size blocks."""
     nxp, nyp, nzp, nth = blk.nxp, blk.nyp, blk.nzp, blk.ntheta
-    covs, pairs = prior_cov_grids(blk)
-    if cov_grids is not None:
-        covs = [np.asarray(c, dtype=np.float32) for c in cov_grids]
-    cov_spec = [fft_in_place(c, nxp, True) for c in covs]
-    if abs(blk.corr_grad_i) > 0 or abs(blk.corr_grad_j) > 0:
-        ec = fill_err_corr(blk.corr_xy, nxp, nyp, nzp, blk.corr_grad_i, blk.corr_grad_j)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    if separable:
+        assert cov_grids is None and blk.corr_grad_i == 0 and blk.corr_grad_j == 0
+        c2 = np.fft.rfft2(np.asarray(blk.corr_xy, dtype=np.float64))        # (nyp, cnxp)
+        c1 = np.fft.fft(np.asarray(blk.circ_corr_t, dtype=np.float64))      # (nzp,)
+        pvs = [float(np.float32(blk.prior_var0[a, b])) for a, b in pairs]
+        cov_spec = None
+        err_spec = None
     else:
-        ec = fill_err_corr_zero_grad(blk.corr_xy, nxp, nyp, nzp)
-    err_spec = fft_in_place(ec, nxp, True)
+        covs, pairs = prior_cov_grids(blk)
+        if cov_grids is not None:
+            covs = [np.asarray(c, dtype=np.float32) for c in cov_grids]
+        cov_spec = [fft_in_place(c, nxp, True) for c in covs]
+        if abs(blk.corr_grad_i) > 0 or abs(blk.corr_grad_j) > 0:
+            ec = fill_err_corr(blk.corr_xy, nxp, nyp, nzp, blk.corr_grad_i, blk.corr_grad_j)
+        else:
+            ec = fill_err_corr_zero_grad(blk.corr_xy, nxp, nyp, nzp)
+        err_spec = fft_in_place(ec, nxp, True)
     data_spec = np.stack([fft_in_place(blk.data[l], nxp, False) for l in range(nth)])
     mean_spec = np.stack([fft_in_place(blk.mean[a], nxp, False) for a in range(3)])
     K, e1, e2, e3, inv = per_kz_operators(blk)
@@ -800,8 +814,14 @@ def posterior(blk, slab: int = 16, cov_grids=None) -> Posterior:
     cs = np.zeros((6,) + mean_spec.shape[1:], dtype=np.complex128)
     for k0 in range(0, nzp, slab):
         k1 = min(nzp, k0 + slab)
-        S = param_cov_from_spectra([c[k0:k1] for c in cov_spec], blk.prior_var0)  # (z,y,x,3,3)
-        lam = np.abs(err_spec[k0:k1].real)
+        if separable:
+            base = c1[k0:k1, None, None] * c2[None]
+            S = param_cov_from_spectra([pv * base for pv in pvs], blk.prior_var0)
+            lam = np.broadcast_to(np.abs(c2.real)[None], base.shape)
+            del base
+        else:
+            S = param_cov_from_spectra([c[k0:k1] for c in cov_spec], blk.prior_var0)  # (z,y,x,3,3)
+            lam = np.abs(err_spec[k0:k1].real)
         Kk, KS, Sd = _data_system(K, e1, e2, e3, Sth, wnc, S, lam, k0, k1)
         L, ok = chol_cpx(Sd)
         invk = np.broadcast_to(inv[k0:k1][:, None, None], ok.shape)

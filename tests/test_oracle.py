@@ -143,3 +143,15 @@ def test_cholesky_rejections_follow_reference():
     L, ok = ref64.chol_cpx(M)
     assert ok[0]
     assert np.allclose(np.tril(L[0]) @ np.tril(L[0]).conj().T, M[0])
+
+
+def test_separable_posterior_equals_the_grid_path():
+    """The slab-wise separable spectra give the grid path's posterior up to the float32
+    rounding of the prior grids' products."""
+    from crava_b200 import synth
+    blk = synth.make_block(synth.BlockSpec(nx=24, ny=20, nz=40, nsim=0, seed=4))
+    a = ref64.posterior(blk)
+    b = ref64.posterior(blk, slab=7, separable=True)
+    for x, y in ((b.mean, a.mean), (b.cov, a.cov)):
+        assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-6
+    assert a.n_inverted == b.n_inverted and a.n_chol_fail == b.n_chol_fail
