@@ -16,6 +16,7 @@ fastest value.  The keys swept, with their size key n:
   zpass_w, zpass_sb, zpass_threads     general kernel: tile width, realisations per batch,
                  n = nzp*16 + ntheta   threads per CTA
   line4_w_fwd, line4_w_inv   n = N     four-step column transforms: columns per tile
+  line4_threads_fwd, line4_threads_inv  four-step column transforms: threads per CTA (n = N)
   x4_threads_fwd, x4_threads_inv       four-step row transforms: threads per CTA
                  n = nxp/2
 
@@ -147,10 +148,14 @@ def tune_workload(name, w, reps, entries, log):
         if v >= 0:
             entries[(key, pk)] = v
     # four-step column (y) and row (x) transforms
-    for key, cls in (("line4_w_fwd", ["line_fwd"]), ("line4_w_inv", ["line_inv"])):
+    for key, tkey, cls in (("line4_w_fwd", "line4_threads_fwd", ["line_fwd"]),
+                           ("line4_w_inv", "line4_threads_inv", ["line_inv"])):
         b = sweep(ctx, job, stream, reps, key, nyp, [4, 8, 16, 32], cls, log)
         if b:
             entries[(key, nyp)] = b[0]
+        b = sweep(ctx, job, stream, reps, tkey, nyp, [128, 192, 256, 320, 384, 448, 512], cls, log)
+        if b:
+            entries[(tkey, nyp)] = b[0]
     if nxp % 2 == 0:
         h = nxp // 2
         for key, cls in (("x4_threads_fwd", ["x_r2c"]), ("x4_threads_inv", ["x_c2r"])):

@@ -63,7 +63,7 @@ constexpr size_t line4_smem(int W, int SK) {
 }
 
 template <int N1, int N2, int DIR>
-__global__ void __launch_bounds__(256) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
+__global__ void __launch_bounds__(512) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
                                                size_t ostride, int W, int lw, int nIT, int SK,
                                                const float2* __restrict__ twg) {
   constexpr int N = N1 * N2;
@@ -220,40 +220,64 @@ constexpr size_t x4_smem(bool fwd, int rpc) {
   return sizeof(float2) * ((size_t)rpc * L::PITCH + (fwd ? 0 : (size_t)rpc * (L::H + 1)));
 }
 
+// stage != 0: the twiddle tables are copied into shared memory first; 0: the passes read
+// them from global memory (L1-resident: every CTA of the launch reads the same 2 h values),
+// and the CTA's first barrier and the table copy go away.
 template <int N1, int N2>
 __global__ void __launch_bounds__(256) k_xr2c4(const __grid_constant__ GridSet gs, int rows, int rpc,
-                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+                                               const float2* __restrict__ twg, const float2* __restrict__ twn,
+                                               int stage) {
   constexpr int H = N1 * N2;
   extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* twh = tw + H;
-  for (int t = threadIdx.x; t < H; t += blockDim.x) {
-    tw[t] = twg[t];
-    twh[t] = twn[t];
+  const float2 *tw = twg, *twh = twn;
+  float2* Z = sm;
+  if (stage) {
+    float2* t1 = sm;
+    float2* t2 = t1 + H;
+    for (int t = threadIdx.x; t < H; t += blockDim.x) {
+      t1[t] = twg[t];
+      t2[t] = twn[t];
+    }
+    tw = t1;
+    twh = t2;
+    Z = t2 + H;
+    __syncthreads();
   }
   const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
   const float2* src = reinterpret_cast<const float2*>(gs.src[blockIdx.y]) + (size_t)row0 * (H + 1);
   float2* dst = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * (H + 1);
-  __syncthreads();
-  xr2c4_rows<N1, N2>(src, dst, nr, gs.scale[blockIdx.y], tw, twh, twh + H);
+  xr2c4_rows<N1, N2>(src, dst, nr, gs.scale[blockIdx.y], tw, twh, Z);
 }
 
 template <int N1, int N2>
 __global__ void __launch_bounds__(256) k_xc2r4(const __grid_constant__ GridSet gs, int rows, int rpc,
-                                               const float2* __restrict__ twg, const float2* __restrict__ twn) {
+                                               const float2* __restrict__ twg, const float2* __restrict__ twn,
+                                               int stage) {
   using L = RowLayout<N1, N2>;
-  constexpr int H = N1 * N2;
+  constexpr int H = N1 * N2, CN = H + 1;
   extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* twh = tw + H;
-  float2* Z = twh + H;
+  const float2 *tw = twg, *twh = twn;
+  float2* Z = sm;
   const int row0 = blockIdx.x * rpc, nr = min(rpc, rows - row0);
-  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * (H + 1);
-  for (int t = threadIdx.x; t < H; t += blockDim.x) {
-    tw[t] = twg[t];
-    twh[t] = twn[t];
+  float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)row0 * CN;
+  if (stage) {
+    float2* t1 = sm;
+    float2* t2 = t1 + H;
+    Z = t2 + H;
+    // the rows' copies go out before the tables are staged
+    float2* Xs = Z + rpc * L::PITCH;
+    const uint32_t xb = smem_addr(Xs);
+    for (int e = threadIdx.x; e < nr * CN; e += blockDim.x) cp_async8(xb + 8u * (uint32_t)e, g + e);
+    cp_async_commit();
+    for (int t = threadIdx.x; t < H; t += blockDim.x) {
+      t1[t] = twg[t];
+      t2[t] = twn[t];
+    }
+    cp_async_wait_0();
+    __syncthreads();
+    xc2r4_staged<N1, N2>(Xs, g, nr, gs.scale[blockIdx.y], t1, t2, Z);
+    return;
   }
-  __syncthreads();
   xc2r4_rows<N1, N2>(g, nr, gs.scale[blockIdx.y], tw, twh, Z, Z + rpc * L::PITCH);
 }
 
@@ -464,7 +488,11 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   while ((1 << lw) < W) lw++;
   W = 1 << lw;
   const int SK = W < 16 ? (((W - N2 * W) % 16) + 16) % 16 : 0;
-  const int T = std::min(256, round_up32(W * std::max(N1, N2)));
+  // threads per CTA: by default one item per thread of the longer pass up to 256; the
+  // schedule may set up to 512 (a whole number of warps), e.g. so that one pass runs in a
+  // single round
+  int T = std::min(256, round_up32(W * std::max(N1, N2)));
+  T = std::max(64, std::min(512, tuned(sign < 0.f ? "line4_threads_fwd" : "line4_threads_inv", N, T) / 32 * 32));
   const int nIT = (ni + W - 1) / W;
   if (pipe4_enabled(N)) {
     // two staged tiles and the work tile: narrower tiles for the longest lines
@@ -473,7 +501,7 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
     int lwp = 0;
     while ((1 << lwp) < Wp) lwp++;
     const int SKp = Wp < 16 ? (((Wp - N2 * Wp) % 16) + 16) % 16 : 0;
-    const int Tp = std::min(256, round_up32(Wp * std::max(N1, N2)));
+    const int Tp = std::min(256, round_up32(Wp * std::max(N1, N2)));   // k_line4p is bounded at 256
     const int nITp = (ni + Wp - 1) / Wp;
     const size_t smem = sizeof(float2) * ((size_t)N + 2 * (size_t)Wp * N) + line4_smem<N1, N2>(Wp, SKp);
     const void* fn = sign < 0.f ? (const void*)k_line4p<N1, N2, -1> : (const void*)k_line4p<N1, N2, 1>;
@@ -518,13 +546,16 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
     else k_x4p<N1, N2, false><<<grid, T, smem, st>>>(gs, rows, rpc, nchunk, tw, twn);
     return cudaGetLastError();
   }
-  const size_t smem = sizeof(float2) * 2 * (size_t)L::H + x4_smem<N1, N2>(fwd, rpc);
+  // twiddle tables staged in shared memory (schedule key x4_stage, default 1) or read from
+  // global memory
+  const int stage = tuned(fwd ? "x4_stage_fwd" : "x4_stage_inv", L::H, 1) != 0 ? 1 : 0;
+  const size_t smem = sizeof(float2) * 2 * (size_t)L::H * stage + x4_smem<N1, N2>(fwd, rpc);
   const void* fn = fwd ? (const void*)k_xr2c4<N1, N2> : (const void*)k_xc2r4<N1, N2>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((rows + rpc - 1) / rpc), gs.n);
-  if (fwd) k_xr2c4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn);
-  else k_xc2r4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn);
+  if (fwd) k_xr2c4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn, stage);
+  else k_xc2r4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn, stage);
   return cudaGetLastError();
 }
 
