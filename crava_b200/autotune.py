@@ -16,7 +16,10 @@ fastest value.  The keys swept, with their size key n:
   zpass_w, zpass_sb, zpass_threads     general kernel: tile width, realisations per batch,
                  n = nzp*16 + ntheta   threads per CTA
   line4_w_fwd, line4_w_inv   n = N     four-step column transforms: columns per tile
-  line4_threads_fwd, line4_threads_inv  four-step column transforms: threads per CTA (n = N)
+  line4_threads_fwd, line4_threads_inv  four-step column transforms: threads per CTA (n = N;
+                                        at most 256 forward, 512 inverse)
+  x4_stage_fwd, x4_stage_inv           four-step row transforms: 1 = twiddle tables staged in
+                                        shared memory, 0 = read from global memory (n = nxp/2)
   x4_threads_fwd, x4_threads_inv       four-step row transforms: threads per CTA
                  n = nxp/2
 
@@ -153,15 +156,25 @@ def tune_workload(name, w, reps, entries, log):
         b = sweep(ctx, job, stream, reps, key, nyp, [4, 8, 16, 32], cls, log)
         if b:
             entries[(key, nyp)] = b[0]
-        b = sweep(ctx, job, stream, reps, tkey, nyp, [128, 192, 256, 320, 384, 448, 512], cls, log)
+        tv = [128, 160, 192, 224, 256] + ([320, 384, 448, 512] if tkey.endswith("inv") else [])
+        b = sweep(ctx, job, stream, reps, tkey, nyp, tv, cls, log)
         if b:
             entries[(tkey, nyp)] = b[0]
     if nxp % 2 == 0:
         h = nxp // 2
-        for key, cls in (("x4_threads_fwd", ["x_r2c"]), ("x4_threads_inv", ["x_c2r"])):
-            b = sweep(ctx, job, stream, reps, key, h, [64, 128, 192, 256], cls, log)
-            if b:
-                entries[(key, h)] = b[0]
+        for key, skey, cls in (("x4_threads_fwd", "x4_stage_fwd", ["x_r2c"]),
+                               ("x4_threads_inv", "x4_stage_inv", ["x_c2r"])):
+            best = None
+            for stage in (1, 0):
+                api.tuning_set(skey, h, stage)
+                b = sweep(ctx, job, stream, reps, key, h, [64, 128, 192, 256], cls, log)
+                if b and (best is None or b[1] < best[2]):
+                    best = (stage, b[0], b[1])
+            if best:
+                api.tuning_set(skey, h, best[0])
+                api.tuning_set(key, h, best[1])
+                entries[(skey, h)] = best[0]
+                entries[(key, h)] = best[1]
     total = time_classes(ctx, job, stream, reps)
     log.append(f"# {name} tuned: " + ", ".join(f"{k} {v:.3f}" for k, v in sorted(total.items())) +
                f"; sum {sum(total.values()):.3f} ms")

@@ -291,6 +291,9 @@ struct crava_job {
   std::vector<double> A, etc, pv, relt;
   std::vector<float> wav, wnorm, corr_xy, circ;
   bool ran = false;
+  // GRIDS: the prior grids are the last crava_job_fill_prior's (priorVar0 x one correlation
+  // grid, pv00 > 0), so the run transforms one of them; any upload of a prior grid clears it
+  bool base_prior = false;
   bool resid_real = false;        // the residual grids hold the wavelet-convolved residuals
   // local wavelet grids (crava_job_set_wavelet_grids) and the wavelet half spectra of a job
   // without the non-constant tables (crava_job_residual_synthetics): own allocations
@@ -2077,6 +2080,7 @@ crava_status crava_job_device_ptr(crava_job* job, crava_role role, int index, fl
   crava_status s;
   float* p = grid_ptr(job, role, index, &s);
   if (s) return s;
+  if (role == CRAVA_ROLE_PRIOR_COV) job->base_prior = false;   // the caller may write the grid
   *dptr = p;
   return CRAVA_OK;
 }
@@ -2086,6 +2090,7 @@ crava_status crava_job_upload(crava_job* job, crava_role role, int index, const 
   crava_status s;
   float* p = grid_ptr(job, role, index, &s);
   if (s) return s;
+  if (role == CRAVA_ROLE_PRIOR_COV) job->base_prior = false;
   CUDA_TRY(cudaMemcpyAsync(p, host, sizeof(float) * job->rsize, cudaMemcpyHostToDevice, (cudaStream_t)stream));
   return CRAVA_OK;
 }
@@ -2125,7 +2130,10 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     std::vector<const float*> src;
     std::vector<float*> g;
     std::vector<float> sc;
-    for (int q = 0; q < 6; q++) { src.push_back(job->in_cov[q]); g.push_back(job->cov[q]); sc.push_back(1.0f); }
+    // SeismicParametersHolder::FFTCovGrids (src/seismicparametersholder.cpp:458-482): with a
+    // base prior the six spectra are priorVar0 multiples of one, and only the first is formed
+    const int ncov = job->base_prior ? 1 : 6;
+    for (int q = 0; q < ncov; q++) { src.push_back(job->in_cov[q]); g.push_back(job->cov[q]); sc.push_back(1.0f); }
     src.push_back(job->in_err);
     g.push_back(job->err);
     sc.push_back(1.0f);
@@ -2176,6 +2184,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.nth = d.ntheta;
   zp.nsim = d.nsim;
   zp.separable = grids ? 0 : 1;
+  zp.base_prior = (grids && job->base_prior) ? 1 : 0;
   zp.host_noise = (d.flags & CRAVA_FLAG_HOST_NOISE) ? 1 : 0;
   zp.keep_resid = (d.flags & CRAVA_FLAG_KEEP_RESIDUAL) ? 1 : 0;
   zp.cov_spectral = (d.flags & CRAVA_FLAG_SPECTRAL_COV) ? 1 : 0;
@@ -2493,6 +2502,8 @@ static crava_status fill_prior_impl(crava_job* job, const float* act_host, float
   }
   if (dact) cudaFreeAsync(dact, st);
   if (fe != cudaSuccess) return cuda_fail(fe, "launch_fill_prior");
+  // fillInParamCorr x priorVar0 (no estimated covariance): one correlation grid behind all six
+  job->base_prior = !act_host && job->pv[0] > 0.0;
   // the host vectors stay with the job; wait so that the call has the reference's
   // synchronous semantics like the uploads it replaces
   CUDA_TRY(cudaStreamSynchronize(st));

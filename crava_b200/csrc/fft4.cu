@@ -62,8 +62,10 @@ constexpr size_t line4_smem(int W, int SK) {
   return sizeof(float2) * ((size_t)W * N1 * N2 + (size_t)N1 * SK);
 }
 
+// Forward instances bounded at 256 threads (the register allocation the forward passes were
+// tuned with), inverse ones at 512 (a CTA may take one pass in a single round).
 template <int N1, int N2, int DIR>
-__global__ void __launch_bounds__(512) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
+__global__ void __launch_bounds__(DIR > 0 ? 512 : 256) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
                                                size_t ostride, int W, int lw, int nIT, int SK,
                                                const float2* __restrict__ twg) {
   constexpr int N = N1 * N2;
@@ -492,7 +494,8 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   // schedule may set up to 512 (a whole number of warps), e.g. so that one pass runs in a
   // single round
   int T = std::min(256, round_up32(W * std::max(N1, N2)));
-  T = std::max(64, std::min(512, tuned(sign < 0.f ? "line4_threads_fwd" : "line4_threads_inv", N, T) / 32 * 32));
+  T = std::max(64, std::min(sign < 0.f ? 256 : 512,
+                            tuned(sign < 0.f ? "line4_threads_fwd" : "line4_threads_inv", N, T) / 32 * 32));
   const int nIT = (ni + W - 1) / W;
   if (pipe4_enabled(N)) {
     // two staged tiles and the work tile: narrower tiles for the longest lines

@@ -48,6 +48,8 @@ struct ZParams {
   int zsplit;                  // four-step z transform: 0 none, 1 16x16, 2 20x16, 3 16x8
   int nth, nsim;
   int separable;               // 1: prior from cxy/ct factors, 0: from spectral grids
+  int base_prior;              // grids: the six prior spectra are pv x one base spectrum, only
+                               // cov[0] (= pv[0] x base) transformed
   int host_noise;              // 1: noise from `noise` grids
   int keep_resid;              // 1: write residual spectra into data grids
   int cov_spectral;            // 1: posterior covariance left as per-bin spectra

@@ -471,13 +471,20 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
       for (int q = 0; q < 6; q++) S[q] = P.pv[q] * rho;
       lam = fabsf(cx.x);
     } else {
-      // getNextParameterCovariance: |Re/pv| pv (no division when pv == 0)
+      // getNextParameterCovariance: |Re/pv| pv (no division when pv == 0); a base prior's
+      // pairs share |Re/pv| of the one spectrum transformed (pv[0] != 0)
+      if (P.base_prior) {
+        const float r0 = fabsf(P.cov[0][gidx].x / P.pv[0]);
 #pragma unroll
-      for (int q = 0; q < 6; q++) {
-        float re = P.cov[q][gidx].x;
-        float pv = P.pv[q];
-        if (pv != 0.f) re = re / pv;
-        S[q] = fabsf(re) * pv;
+        for (int q = 0; q < 6; q++) S[q] = r0 * P.pv[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+          float re = P.cov[q][gidx].x;
+          float pv = P.pv[q];
+          if (pv != 0.f) re = re / pv;
+          S[q] = fabsf(re) * pv;
+        }
       }
       lam = fabsf(P.errspec[gidx].x);
     }

@@ -232,7 +232,11 @@ crava_status crava_job_local_noise(crava_job* job, const float* scales, void* st
  * src/fftgrid.cpp:878-928) and FFTGrid::fillInErrCorr (src/fftgrid.cpp:777-828) fill them,
  * with the lateral correlation gradients corr_grad_i, corr_grad_j (samples per index) and
  * the reference's float arithmetic (the grids are equal bit for bit).  Call before
- * crava_job_run; returns after `stream` has finished the work. */
+ * crava_job_run; returns after `stream` has finished the work.  The six grids are then
+ * priorVar0 multiples of one correlation grid, so the next runs transform only the first
+ * (FFTCovGrids forms one spectrum, not six; getNextParameterCovariance scales its |Re/pv|
+ * by each pair's priorVar0, equal to the six-spectrum form up to the float rounding of the
+ * six grids' products), until a prior grid is uploaded or its device pointer taken. */
 crava_status crava_job_fill_prior(crava_job* job, float corr_grad_i, float corr_grad_j, void* stream);
 
 /* CRAVA_PRIOR_GRIDS jobs with estimated covariance (InitializeCorrelations with

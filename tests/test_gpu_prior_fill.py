@@ -121,3 +121,36 @@ def test_estimated_auto_cov_grids_and_inversion(ctx):
             assert rel(out["cov"][q][..., :blk.nxp], post.cov[q][..., :blk.nxp]) < 1e-3, q
     finally:
         job.close()
+
+
+def test_base_prior_path_equals_the_six_spectra_path(ctx):
+    """After crava_job_fill_prior the run transforms one prior grid and scales it per pair;
+    re-uploading the same six grids takes the six-spectra path.  Both agree to the float
+    rounding of the grids' products."""
+    blk = grad_block(0.37, -0.21, nsim=1)
+    outs = []
+    for reupload in (False, True):
+        job = api.Job(ctx, blk, api.PRIOR_GRIDS, seed=4)
+        try:
+            for l in range(blk.ntheta):
+                job.upload(api.ROLE_DATA, l, blk.data[l])
+            for a in range(3):
+                job.upload(api.ROLE_MEAN, a, blk.mean[a])
+            job.fill_prior(blk.corr_grad_i, blk.corr_grad_j)
+            if reupload:
+                for q in range(6):
+                    job.upload(api.ROLE_PRIOR_COV, q, job.download(api.ROLE_PRIOR_COV, q))
+            job.run()
+            o = job.download_outputs()
+            o["counters"] = job.counters()
+            outs.append(o)
+        finally:
+            job.close()
+    a, b = outs
+    nxp = blk.nxp
+    for q in range(3):
+        assert rel(a["mean"][q][..., :nxp], b["mean"][q][..., :nxp]) < 1e-5, q
+    for q in range(6):
+        assert rel(a["cov"][q][..., :nxp], b["cov"][q][..., :nxp]) < 1e-5, q
+    assert rel(a["sims"][..., :nxp], b["sims"][..., :nxp]) < 1e-4
+    assert a["counters"]["inverted_bins"] == b["counters"]["inverted_bins"]
