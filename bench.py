@@ -342,6 +342,44 @@ def cfg3_leg(torch, steps, warmup):
             "kernel_ms_per_job": {c: kt[c][0] / steps for c in kt if kt[c][1]}}
 
 
+def cufft_leg(torch, dims=(540, 540, 256), reps=10):
+    """Comparator only (not on the product path): one 3D real transform of a 540x540x256 grid
+    each way, the library's drop-in for FFTGrid::fftInPlace / invFFTInPlace (crava_fft_r2c /
+    crava_fft_c2r, in place on the padded layout) against cuFFT through torch.fft.rfftn /
+    irfftn (out of place), device time per transform with CUDA events."""
+    from crava_b200 import api
+    nx, ny, nz = dims
+    rnx = 2 * (nx // 2 + 1)
+    ctx = api.Context(torch.cuda.current_device())
+    g = torch.randn((nz, ny, rnx), device="cuda", dtype=torch.float32)
+    x = torch.randn((nz, ny, nx), device="cuda", dtype=torch.float32)
+    st = torch.cuda.current_stream()
+    sh = st.cuda_stream
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    out["crava_r2c_ms"] = timed(lambda: api.fft_r2c(ctx, g.data_ptr(), nx, ny, nz, False, sh))
+    out["crava_c2r_ms"] = timed(lambda: api.fft_c2r(ctx, g.data_ptr(), nx, ny, nz, False, sh))
+    y = torch.fft.rfftn(x, dim=(0, 1, 2))
+    out["cufft_r2c_ms"] = timed(lambda: torch.fft.rfftn(x, dim=(0, 1, 2)))
+    out["cufft_c2r_ms"] = timed(lambda: torch.fft.irfftn(y, s=(nz, ny, nx), dim=(0, 1, 2)))
+    del g, x, y
+    ctx.close()
+    return {"workload": f"one {nx}x{ny}x{nz} real grid, 3D r2c and c2r", "reps": reps, **out,
+            "note": "cuFFT is a comparator only; the library's transforms are the product path"}
+
+
 def served_leg(torch, n_jobs=48, n_models=6, rate=20.0, nsim=16, max_inflight=8, budget_gb=120):
     """Served stream: Poisson arrivals at `rate` jobs/s; every request drawn fresh: one of
     n_models interval models (nz, 3..6 angles, priors within +-30% of the 64x64x128 block,
@@ -735,9 +773,10 @@ def main():
 
     job.close()
     job2.close()
-    batched = served = cfg3 = None
+    batched = served = cfg3 = cufft = None
     if rank == 0 and not args.no_legs and not args.dims:
         cfg3 = cfg3_leg(torch, steps=max(3, min(args.steps, 10)), warmup=max(3, args.warmup))
+        cufft = cufft_leg(torch)
         batched = batched_leg(ctx, torch)
         served = served_leg(torch)
     clocks = summarize_clocks(clk_path, physical_gpu_index(local_rank))
@@ -770,6 +809,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "config3": cfg3,
+            "cufft_comparator": cufft,
             "batched": batched,
             "served": served,
         }

@@ -1,0 +1,54 @@
+// Four-step launchers (fft4.cuh) for part 5 of the size table in fft4.cu; the parts are
+// separate translation units so that they compile side by side.
+#include "fft4.cuh"
+
+namespace crava {
+
+#define CRAVA_FOUR_STEP_PART(X) \
+  X(24, 6, 4) \
+  X(35, 7, 5) \
+  X(49, 7, 7) \
+  X(64, 8, 8) \
+  X(84, 12, 7) \
+  X(108, 12, 9) \
+  X(135, 15, 9) \
+  X(162, 18, 9) \
+  X(196, 14, 14) \
+  X(240, 16, 15) \
+  X(280, 20, 14) \
+  X(324, 18, 18) \
+  X(384, 24, 16) \
+  X(441, 21, 21) \
+  X(504, 24, 21) \
+  X(576, 24, 24) \
+  X(648, 27, 24) \
+  X(750, 30, 25) \
+  X(840, 30, 28)
+
+cudaError_t four_step_line4_p5(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride,
+                                const float2* tw, float sign, cudaStream_t st) {
+  switch (n) {
+#define CRAVA_CASE(NN, A, B) \
+  case NN:                   \
+    return line4<A, B>(gs, ni, pstride, no, ostride, tw, sign, st);
+    CRAVA_FOUR_STEP_PART(CRAVA_CASE)
+#undef CRAVA_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t four_step_x4_p5(bool fwd, const GridSet& gs, int h, int rows, const float2* tw, const float2* twn,
+                             cudaStream_t st) {
+  switch (h) {
+#define CRAVA_CASE(NN, A, B) \
+  case NN:                   \
+    return x4<A, B>(fwd, gs, rows, tw, twn, st);
+    CRAVA_FOUR_STEP_PART(CRAVA_CASE)
+#undef CRAVA_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace crava
