@@ -278,6 +278,20 @@ __device__ __forceinline__ void cp_async8_zfill(uint32_t dst, const void* src, b
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// L2 prefetch of the global bytes [p, p + n) of a buffer [b0, b1) that holds them: the range
+// is widened to 16-byte boundaries (the bulk prefetch's alignment rule) inside the buffer and
+// the bytes that cannot be so widened are left out; a hint with no effect on the values.
+__device__ __forceinline__ void l2_prefetch(const void* p, size_t n, const void* b0, const void* b1) {
+  uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)15;
+  uintptr_t e = (reinterpret_cast<uintptr_t>(p) + n + 15) & ~(uintptr_t)15;
+  if (a < reinterpret_cast<uintptr_t>(b0)) a += 16;
+  if (e > reinterpret_cast<uintptr_t>(b1)) e -= 16;
+  if (e > a) {
+    const size_t ga = __cvta_generic_to_global(reinterpret_cast<const void*>(a));
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(ga), "r"((uint32_t)(e - a)) : "memory");
+  }
+}
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 

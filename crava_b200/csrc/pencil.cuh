@@ -114,6 +114,45 @@ __device__ __forceinline__ void zinv_inplace(float2* x, int nl, int ps, const fl
   __syncthreads();
 }
 
+// The same inverse transform with its last pass writing each line's natural-order outputs
+// straight out through store(l, k, value) (line l, z index k) instead of back to x; x is
+// free for reuse after the closing barrier.
+template <int N1, int N2, class Store>
+__device__ __forceinline__ void zinv_store(float2* x, int nl, int ps, const float2* tw, Store store) {
+  const int T = blockDim.x;
+  const float rl = __frcp_rn((float)nl);
+  const int mstep = N2 * ps;
+  for (int q = threadIdx.x; q < nl * N1; q += T) {
+    int l;
+    const int k2 = fdivmod(q, nl, rl, l);
+    float2* y = x + l + k2 * mstep;
+    float2 v[N2];
+#pragma unroll
+    for (int k1 = 0; k1 < N2; k1++) v[k1] = y[k1 * ps];
+    Dft<N2>::run(v, 1.f);
+#pragma unroll
+    for (int t = 1; t < N2; t++) {
+      float2 w = tw[t * k2];
+      v[t] = cmul(v[t], make_float2(w.x, -w.y));
+    }
+#pragma unroll
+    for (int t = 0; t < N2; t++) y[t * ps] = v[t];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nl * N2; q += T) {
+    int l;
+    const int t = fdivmod(q, nl, rl, l);
+    const float2* y = x + l + t * ps;
+    float2 v[N1];
+#pragma unroll
+    for (int k2 = 0; k2 < N1; k2++) v[k2] = y[k2 * mstep];
+    Dft<N1>::run(v, 1.f);
+#pragma unroll
+    for (int m = 0; m < N1; m++) store(l, t + N2 * m, v[m]);
+  }
+  __syncthreads();
+}
+
 // ------------------------------------------------------------------ per-bin algebra
 
 // Section of N floats (N % 4 == 0) of the row of position p: group g at e[g * stride].
@@ -413,15 +452,12 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
       }
     }
     __syncthreads();
-    zinv_inplace<N1, N2>(S3, 3 * nb * W, SG * W, tw);
-    for (int e = tid; e < TS; e += T) {
-      const int w = e & (W - 1), k = e >> lw;
-      if (w >= nw) continue;
-      const size_t go = base + (size_t)k * kstride + w;
-      const float2* r = S3 + k * SG * W + w;
-      for (int c = 0; c < 3 * nb; c++) P.sim[3 * s0 + c][go] = r[c * W];
-    }
-    __syncthreads();
+    // inverse z transform, the last pass storing the realisations' spectra (line l: grid
+    // 3 s0 + l / W, x-offset l % W)
+    zinv_store<N1, N2>(S3, 3 * nb * W, SG * W, tw, [&](int l, int k, float2 v) {
+      const int w = l & (W - 1);
+      if (w < nw) P.sim[3 * s0 + (l >> lw)][base + (size_t)k * kstride + w] = v;
+    });
   }
   // ---- S_post = L L^H where slots 0..5 hold the factor
   if (P.nsim > 0) {
@@ -443,21 +479,25 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
   }
   // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
   //      and mean (6..8); spectral covariance slots stay in position order
-  const int gs0 = P.cov_spectral ? 6 : 0;
-  zinv_inplace<N1, N2>(R + gs0 * W, (9 - gs0) * W, G * W, tw);
-  for (int e = tid; e < TS; e += T) {
-    const int w = e & (W - 1), k = e >> lw;
-    if (w >= nw) continue;
-    const size_t go = base + (size_t)k * kstride + w;
-    const int so = k * G * W + w;
+  if (!P.cov_spectral) {
+    // slots 0..5 to cov[0..5], 6..8 to mean[0..2], stored by the last pass
+    zinv_store<N1, N2>(R, 9 * W, G * W, tw, [&](int l, int k, float2 v) {
+      const int g = l >> lw, w = l & (W - 1);
+      if (w < nw) (g < 6 ? P.cov[g] : P.mean[g - 6])[base + (size_t)k * kstride + w] = v;
+    });
+  } else {
+    // spectral covariance: slots 0..5 stay in position order, stored at their kz
+    zinv_inplace<N1, N2>(R + 6 * W, 3 * W, G * W, tw);
+    for (int e = tid; e < TS; e += T) {
+      const int w = e & (W - 1), k = e >> lw;
+      if (w >= nw) continue;
+      const size_t go = base + (size_t)k * kstride + w;
+      const int so = k * G * W + w;
+      const int kz = k / N2 + N1 * (k % N2);
 #pragma unroll
-    for (int g = 0; g < 9; g++) {
-      if (g < gs0) {
-        const int kz = k / N2 + N1 * (k % N2);
-        P.cov[g][base + (size_t)kz * kstride + w] = R[so + g * W];
-      } else {
-        (g < 6 ? P.cov[g] : P.mean[g - 6])[go] = R[so + g * W];
-      }
+      for (int g = 0; g < 6; g++) P.cov[g][base + (size_t)kz * kstride + w] = R[so + g * W];
+#pragma unroll
+      for (int a = 0; a < 3; a++) P.mean[a][go] = R[so + (6 + a) * W];
     }
   }
 
