@@ -27,9 +27,11 @@ __device__ __forceinline__ uint4 philox4x32_7(uint4 c, uint2 k) {
 
 // Box-Muller with the hardware approximations of log, sine and cosine: their absolute
 // errors (about 2^-21 on these ranges) are far below what the normals' statistics can show.
+// u1 from a 26-bit integer a (radius: the largest |normal| is sqrt(2 ln 2^27) = 6.1), the angle
+// from a 16-bit integer b (resolution 2 pi / 65536).
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, float& n1) {
-  float u1 = ((float)a + 0.5f) * 2.3283064365386963e-10f;
-  float u2 = ((float)b + 0.5f) * 2.3283064365386963e-10f - 0.5f;   // (-1/2, 1/2)
+  float u1 = ((float)a + 0.5f) * 1.4901161193847656e-08f;        // (a + 1/2) / 2^26, in (0, 1)
+  float u2 = ((float)b + 0.5f) * 1.52587890625e-05f - 0.5f;      // (b + 1/2) / 2^16 - 1/2
   float rad = sqrtf(-2.0f * __logf(u1));
   float sn, cs;
   __sincosf(6.283185307179586f * u2, &sn, &cs);   // angle in (-pi, pi)
@@ -42,7 +44,10 @@ __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, fl
 // i = nxp/2 for even nxp): the pair (j,k) / (-j,-k) share one draw (conjugated),
 // self-mirrored bins are real with unit variance, all others have variance 1/2 per
 // component (the properties FFTGrid::fillInComplexNoise gives its noise,
-// src/fftgrid.cpp:997-1055, with the mirror-plane test done on the x index).
+// src/fftgrid.cpp:997-1055, with the mirror-plane test done on the x index).  One
+// Philox block (128 bits) per bin and realisation feeds the three Box-Muller pairs: three
+// 26-bit radius words (the top bits of words 0-2) and three 16-bit angle words (word 3's two
+// halves, and the low 6 + 6 + 4 bits of words 0-2).
 __device__ __forceinline__ void device_noise3(uint64_t seed, int s, int i, int j, int k, int nyp, int nzp,
                                               int cnxp, bool nxp_even, float2 (&z)[3]) {
   bool mirror_plane = (i == 0) || (nxp_even && i == cnxp - 1);
@@ -57,12 +62,12 @@ __device__ __forceinline__ void device_noise3(uint64_t seed, int s, int i, int j
   }
   uint64_t bin = ((uint64_t)kk * nyp + jj) * cnxp + i;
   uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-  uint4 r0 = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 0u), key);
-  uint4 r1 = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 1u), key);
+  const uint4 r = philox4x32_7(make_uint4((uint32_t)bin, (uint32_t)(bin >> 32), (uint32_t)s, 0u), key);
+  const uint32_t b2 = (r.x & 63u) | ((r.y & 63u) << 6) | ((r.z & 15u) << 12);
   float n[6];
-  box_muller(r0.x, r0.y, n[0], n[1]);
-  box_muller(r0.z, r0.w, n[2], n[3]);
-  box_muller(r1.x, r1.y, n[4], n[5]);
+  box_muller(r.x >> 6, r.w & 0xFFFFu, n[0], n[1]);
+  box_muller(r.y >> 6, r.w >> 16, n[2], n[3]);
+  box_muller(r.z >> 6, b2, n[4], n[5]);
   const float h = self ? 1.0f : 0.70710678118654752f;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
