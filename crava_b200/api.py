@@ -150,6 +150,8 @@ def lib() -> ctypes.CDLL:
                                                 ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     L.crava_job_fill_prior_auto_cov.argtypes = [vp, vp, ctypes.c_float, ctypes.c_float, vp]
+    L.crava_job_set_facies.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, vp,
+                                       ctypes.POINTER(vp), vp]
     L.crava_circ_corr_t.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
     L.crava_circ_auto_cov.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp]
     L.crava_ctx_set_table_cache.argtypes = [vp, ctypes.c_size_t]
@@ -319,6 +321,22 @@ class Job:
         self._h = ctypes.c_void_p()
         _check(lib().crava_job_create(ctx.handle, ctypes.byref(desc), ctypes.byref(self._h)))
         self.shape = (blk.nzp, blk.nyp, 2 * (blk.nxp // 2 + 1))
+
+    def set_facies(self, corner_descs, d_densities, density_row: int, noise_scale, d_prob, d_seis_lh=None):
+        """Facies probabilities written by every later run (crava_job_set_facies): 2^nang corner
+        descriptions and device volumes, noise_scale (nang, ny, nx) host maps or None, nfacies+1
+        device probability grids; corner_descs=None clears."""
+        if corner_descs is None:
+            _check(lib().crava_job_set_facies(self._h, None, 0, None, 0, None, None, None))
+            return
+        nang = int(np.asarray(noise_scale).shape[0]) if noise_scale is not None else 0
+        assert len(corner_descs) == 1 << nang and len(d_densities) == 1 << nang
+        arr = (FaciesDesc * len(corner_descs))(*corner_descs)
+        dens = (ctypes.c_void_p * len(d_densities))(*d_densities)
+        sc = np.ascontiguousarray(noise_scale, dtype=np.float32) if nang else None
+        prob = (ctypes.c_void_p * len(d_prob))(*d_prob)
+        _check(lib().crava_job_set_facies(self._h, arr, nang, dens, int(density_row),
+                                          sc.ctypes.data if nang else None, prob, d_seis_lh))
 
     def upload(self, role: int, index: int, host: np.ndarray, stream=None):
         a = np.ascontiguousarray(host)

@@ -301,6 +301,17 @@ struct crava_job {
   float2* wspec = nullptr;        // ntheta x cnzp
   bool async = false;             // pool from cudaMallocAsync on alloc_stream
   cudaStream_t alloc_stream = nullptr;
+  // facies probabilities evaluated by crava_job_run (crava_job_set_facies): the corner boxes
+  // with their packed volumes and trace noise scales in fac_mem (own allocation), the
+  // caller's probability grids
+  bool fac_on = false;
+  FaciesCornersHost fac_hc{};
+  int fac_nf = 0;
+  float fac_prior[kMaxFacies] = {};
+  float fac_undef = 0.f;
+  float* fac_prob[kMaxFacies + 1] = {};
+  float* fac_lh = nullptr;
+  char* fac_mem = nullptr;
 };
 
 namespace {
@@ -1611,6 +1622,7 @@ void job_release(crava_job* j) {
   }
   if (j->wgrid) cudaFree(j->wgrid);
   if (j->wspec) cudaFree(j->wspec);
+  if (j->fac_mem) cudaFree(j->fac_mem);
   delete j;
 }
 
@@ -2107,6 +2119,62 @@ crava_status crava_job_download(crava_job* job, crava_role role, int index, floa
   return CRAVA_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The inverse y and x transforms of the three posterior-mean grids with the facies
+// probabilities of crava_job_set_facies: the x transform and the evaluation in one pass
+// (launch_x4_facies) where the x length has a four-step split (schedule key facies_fused,
+// default 1), else the x transform and then the facies pass.
+crava_status inv_mean_facies(crava_ctx* ctx, crava_job* job, float ps, cudaStream_t st) {
+  const crava_job_desc& d = job->d;
+  Plan *px, *pn, *py;
+  crava_status s;
+  if ((s = get_xplans(ctx, d.nxp, &px, &pn)) || (s = get_plan(ctx, d.nyp, &py))) return s;
+  GridSet gs;
+  gs.n = 3;
+  for (int a = 0; a < 3; a++) { gs.p[a] = job->mean[a]; gs.src[a] = job->mean[a]; gs.scale[a] = ps; }
+  int nl = 0;
+  {
+    ProfScope pf(ctx, KT_LINE_INV, st);
+    CUDA_TRY(launch_line_fft(gs, job->cnxp, d.nyp, (size_t)job->cnxp, d.nzp, (size_t)job->cnxp * d.nyp, py->lp, py->tw,
+                             1.f, st, &nl));
+  }
+  const bool fused = d.nxp % 2 == 0 && four_step_supported(d.nxp / 2) && tuned("facies_fused", d.nxp / 2, 1) != 0;
+  const int rnxp_out = 2 * (d.nx / 2 + 1);
+  if (fused) {
+    FaciesFuse F;
+    for (int a = 0; a < 3; a++) F.mean[a] = job->mean[a];
+    F.scale = ps;
+    F.nx = d.nx; F.ny = d.ny; F.nz = d.nz; F.nyp = d.nyp;
+    F.rnxp_out = rnxp_out;
+    F.nf = job->fac_nf;
+    F.undef_sum = job->fac_undef;
+    for (int f = 0; f < job->fac_nf; f++) F.pr.p[f] = job->fac_prior[f];
+    for (int f = 0; f <= job->fac_nf; f++) F.out.p[f] = job->fac_prob[f];
+    F.seis_lh = job->fac_lh;
+    ProfScope pf(ctx, KT_FACIES, st);
+    CUDA_TRY(launch_x4_facies(F, job->fac_hc, d.nxp, d.nyp * d.nzp, px->tw, pn->tw, st, &nl));
+  } else {
+    {
+      ProfScope pf(ctx, KT_X_C2R, st);
+      CUDA_TRY(launch_x_c2r(gs, d.nxp, d.nyp * d.nzp, px->lp, px->tw, pn->tw, st, &nl));
+    }
+    ProfScope pf(ctx, KT_FACIES, st);
+    CUDA_TRY(launch_facies_eval(job->mean[0], job->mean[1], job->mean[2], d.nx, d.ny, d.nz, job->rnxp, d.nyp,
+                                rnxp_out, job->fac_hc, job->fac_nf, job->fac_prior, job->fac_undef, job->fac_prob,
+                                job->fac_lh, st));
+    nl++;
+  }
+  ctx->launches += nl;
+  return CRAVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 crava_status crava_job_run(crava_job* job, void* stream) {
   if (!job) return fail(CRAVA_EINVAL, "null job");
   crava_ctx* ctx = job->ctx;
@@ -2259,11 +2327,13 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     std::vector<float*> g;
     std::vector<float> sc;
     float ps = inv_scale(job->N, false), cs = inv_scale(job->N, true);
-    for (int a = 0; a < 3; a++) { g.push_back(job->mean[a]); sc.push_back(ps); }
+    if (!job->fac_on)
+      for (int a = 0; a < 3; a++) { g.push_back(job->mean[a]); sc.push_back(ps); }
     if (!(d.flags & CRAVA_FLAG_SPECTRAL_COV))
       for (int q = 0; q < 6; q++) { g.push_back(job->cov[q]); sc.push_back(cs); }
     for (int q = 0; q < 3 * d.nsim; q++) { g.push_back(job->sim[q]); sc.push_back(ps); }
     if ((s = inv_xy(ctx, g, sc, d.nxp, d.nyp, d.nzp, false, st))) return s;
+    if (job->fac_on && (s = inv_mean_facies(ctx, job, ps, st))) return s;
   }
   job->ran = true;
   job->resid_real = false;
@@ -3463,20 +3533,24 @@ crava_status crava_facies_smooth(crava_ctx* ctx, const crava_facies_desc* fd, co
   return s;
 }
 
-crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_desc* corners, int nang,
-                                           const float* const* d_density, int density_row, const float* noise_scale,
-                                           const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
-                                           float* const* d_prob, float* d_seis_lh, void* stream) {
-  if (!ctx || !corners || !d_density || !d_post || !d_prob || (nang > 0 && !noise_scale))
-    return fail(CRAVA_EINVAL, "null argument");
+}  // extern "C"
+
+namespace {
+
+// Checks of a facies description (corner boxes, volumes, probability grids) and the relative
+// noise scale of every trace per angle (calculateFaciesProb, src/faciesprob.cpp:1961-1977):
+// fills hc (without t and the packed volumes) and t (nang x ny x nx).
+crava_status facies_setup(const crava_facies_desc* corners, int nang, const float* const* d_density, int density_row,
+                          const float* noise_scale, int nx, int ny, float* const* d_prob, FaciesCornersHost& hc,
+                          std::vector<float>& t) {
   if (nang < 0 || nang > kMaxFaciesAngles) return fail(CRAVA_ENOTSUP, "local-noise angles must be 0..4");
   const crava_facies_desc* fd = corners;
   if (fd->nfacies < 1 || fd->nfacies > kMaxFacies) return fail(CRAVA_EINVAL, "nfacies must be 1..16");
-  if (nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny) return fail(CRAVA_EINVAL, "bad grid dimensions");
+  if (!fd->prior) return fail(CRAVA_EINVAL, "null facies prior");
   for (int f = 0; f <= fd->nfacies; f++)
     if (!d_prob[f]) return fail(CRAVA_EINVAL, "null probability grid");
   const int nc = 1 << nang;
-  FaciesCornersHost hc;
+  hc = FaciesCornersHost{};
   hc.nang = nang;
   for (int c = 0; c < nc; c++) {
     for (int d = 0; d < 3; d++) {
@@ -3491,9 +3565,8 @@ crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_de
     hc.box[c].fstride = (size_t)density_row * corners[c].nbins[1] * corners[c].nbins[2];
     hc.dens[c] = d_density[c];
   }
-  // relative noise scale of every trace per angle (calculateFaciesProb, src/faciesprob.cpp:1961-1977)
   const size_t nxy = (size_t)nx * ny;
-  std::vector<float> t((size_t)nang * nxy);
+  t.assign((size_t)nang * nxy, 0.f);
   for (int a = 0; a < nang; a++) {
     double mn = INFINITY, mx = -INFINITY;
     for (size_t q = 0; q < nxy; q++) {
@@ -3505,6 +3578,25 @@ crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_de
     for (size_t q = 0; q < nxy; q++)
       t[(size_t)a * nxy + q] = mn == mx ? 0.f : (float)(((double)noise_scale[(size_t)a * nxy + q] - mn) / (mx - mn));
   }
+  return CRAVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_desc* corners, int nang,
+                                           const float* const* d_density, int density_row, const float* noise_scale,
+                                           const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
+                                           float* const* d_prob, float* d_seis_lh, void* stream) {
+  if (!ctx || !corners || !d_density || !d_post || !d_prob || (nang > 0 && !noise_scale))
+    return fail(CRAVA_EINVAL, "null argument");
+  if (nx < 1 || ny < 1 || nz < 1 || nxp < nx || nyp < ny) return fail(CRAVA_EINVAL, "bad grid dimensions");
+  const crava_facies_desc* fd = corners;
+  FaciesCornersHost hc;
+  std::vector<float> t;
+  if (crava_status s = facies_setup(corners, nang, d_density, density_row, noise_scale, nx, ny, d_prob, hc, t)) return s;
+  const int nc = 1 << nang;
   CUDA_TRY(cudaSetDevice(ctx->device));
   cudaStream_t st = (cudaStream_t)stream;
   float* dt = nullptr;
@@ -3546,6 +3638,54 @@ crava_status crava_facies_prob(crava_ctx* ctx, const crava_facies_desc* fd, cons
   // the single-volume case of the local-noise form (no noise angles, one corner)
   return crava_facies_prob_local_noise(ctx, fd, 0, &d_density, density_row, nullptr, d_post, nx, ny, nz, nxp, nyp,
                                        d_prob, d_seis_lh, stream);
+}
+
+crava_status crava_job_set_facies(crava_job* job, const crava_facies_desc* corners, int nang,
+                                  const float* const* d_density, int density_row, const float* noise_scale,
+                                  float* const* d_prob, float* d_seis_lh) {
+  if (!job) return fail(CRAVA_EINVAL, "null job");
+  CUDA_TRY(cudaSetDevice(job->ctx->device));
+  if (job->fac_mem) {
+    CUDA_TRY(cudaDeviceSynchronize());   // a run still reading the packed volumes
+    cudaFree(job->fac_mem);
+    job->fac_mem = nullptr;
+  }
+  job->fac_on = false;
+  if (!corners) return CRAVA_OK;   // cleared
+  if (!d_density || !d_prob || (nang > 0 && !noise_scale)) return fail(CRAVA_EINVAL, "null argument");
+  const crava_job_desc& d = job->d;
+  FaciesCornersHost hc;
+  std::vector<float> t;
+  if (crava_status s = facies_setup(corners, nang, d_density, density_row, noise_scale, d.nx, d.ny, d_prob, hc, t))
+    return s;
+  const int nc = 1 << nang, nf = corners->nfacies;
+  size_t bytes = align256(sizeof(float) * t.size());
+  for (int c = 0; c < nc; c++) bytes += align256(facies_packed_bytes(hc.box[c], nf));
+  CUDA_TRY(cudaMalloc((void**)&job->fac_mem, bytes));
+  char* p = job->fac_mem;
+  float* dt = (float*)p;
+  p += align256(sizeof(float) * t.size());
+  for (int c = 0; c < nc; c++) {
+    hc.packed[c] = (float4*)p;
+    p += align256(facies_packed_bytes(hc.box[c], nf));
+  }
+  if (!t.empty()) CUDA_TRY(cudaMemcpy(dt, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
+  hc.t = nang > 0 ? dt : nullptr;
+  CUDA_TRY(launch_facies_pack(hc, nf, nullptr));
+  CUDA_TRY(cudaStreamSynchronize(nullptr));
+  job->fac_hc = hc;
+  job->fac_nf = nf;
+  for (int f = 0; f < nf; f++) job->fac_prior[f] = corners->prior[f];
+  // undefSum = p_undefined / (bins of the first density volume), as the reference
+  job->fac_undef = corners->p_undefined / (float)(corners->nbins[0] * corners->nbins[1] * corners->nbins[2]);
+  for (int f = 0; f <= nf; f++) job->fac_prob[f] = d_prob[f];
+  job->fac_lh = d_seis_lh;
+  job->fac_on = true;
+  {
+    std::lock_guard<std::mutex> lk(job->ctx->mu);
+    job->ctx->launches += nc;
+  }
+  return CRAVA_OK;
 }
 
 }  // extern "C"

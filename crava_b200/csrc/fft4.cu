@@ -1,6 +1,6 @@
 // Dispatch of the four-step transforms (kernels and launch templates in fft4.cuh) over the
 // size table below, and the fused xy pass (opt-in) for a few (nxp, nyp) pairs.
-#include "fft4.cuh"
+#include "fft4_facies.cuh"
 
 namespace crava {
 
@@ -132,7 +132,9 @@ namespace crava {
   cudaError_t four_step_line4_p##K(const GridSet& gs, int ni, int n, size_t pstride, int no, size_t ostride, \
                                    const float2* tw, float sign, cudaStream_t st);                         \
   cudaError_t four_step_x4_p##K(bool fwd, const GridSet& gs, int h, int rows, const float2* tw,              \
-                                const float2* twn, cudaStream_t st);
+                                const float2* twn, cudaStream_t st);                                          \
+  cudaError_t four_step_x4_facies_p##K(const FaciesFuse& F, const FaciesCorners& C, int h, int rows,           \
+                                       const float2* tw, const float2* twn, cudaStream_t st);
 CRAVA_PART_DECL(1)
 CRAVA_PART_DECL(2)
 CRAVA_PART_DECL(3)
@@ -181,6 +183,23 @@ cudaError_t launch_x4(bool fwd, const GridSet& gs, int nxp, int rows, const floa
     case 4: return four_step_x4_p4(fwd, gs, h, rows, tw, twn, st);
     case 5: return four_step_x4_p5(fwd, gs, h, rows, tw, twn, st);
     case 6: return four_step_x4_p6(fwd, gs, h, rows, tw, twn, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_x4_facies(const FaciesFuse& F, const FaciesCornersHost& hc, int nxp, int rows, const float2* tw,
+                             const float2* twn, cudaStream_t st, int* nlaunch) {
+  if (nxp & 1) return cudaErrorInvalidValue;
+  const int h = nxp / 2;
+  const FaciesCorners C = facies_corners(hc);
+  if (nlaunch) (*nlaunch)++;
+  switch (four_step_part(h)) {
+    case 1: return four_step_x4_facies_p1(F, C, h, rows, tw, twn, st);
+    case 2: return four_step_x4_facies_p2(F, C, h, rows, tw, twn, st);
+    case 3: return four_step_x4_facies_p3(F, C, h, rows, tw, twn, st);
+    case 4: return four_step_x4_facies_p4(F, C, h, rows, tw, twn, st);
+    case 5: return four_step_x4_facies_p5(F, C, h, rows, tw, twn, st);
+    case 6: return four_step_x4_facies_p6(F, C, h, rows, tw, twn, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -155,10 +155,11 @@ __device__ __forceinline__ void xr2c4_rows(const float2* src, float2* dst, int n
 
 // nr rows of half spectra in g (pitch h + 1) to scaled real rows in place; the merge step
 // as k_x_c2r (kernels.cu).  Z: rpc * PITCH, Xs: rpc * (h + 1).  Ends with a barrier.
-// The same from rows already staged in Xs (shared), writing g.
-template <int N1, int N2>
+// The same from rows already staged in Xs (shared), writing g; COPY: the real rows also go
+// to Vc (shared, row r at r * h pairs of samples).
+template <int N1, int N2, bool COPY = false>
 __device__ __forceinline__ void xc2r4_staged(const float2* Xs, float2* g, int nr, float scale, const float2* tw,
-                                             const float2* twh, float2* Z) {
+                                             const float2* twh, float2* Z, float2* Vc = nullptr) {
   using L = RowLayout<N1, N2>;
   constexpr int H = L::H, PITCH = L::PITCH;
   constexpr int CN = H + 1, NP = H / 2 + 1;
@@ -198,7 +199,11 @@ __device__ __forceinline__ void xc2r4_staged(const float2* Xs, float2* g, int nr
     four_step_pass2<N1, N2, 1>(k2, [&](int k, int t) { return z[L::pad(t, k)]; }, v);
     float2* X = g + (size_t)r * CN;
 #pragma unroll
-    for (int k1 = 0; k1 < N2; k1++) X[k2 + N1 * k1] = make_float2(v[k1].x * scale, v[k1].y * scale);
+    for (int k1 = 0; k1 < N2; k1++) {
+      const float2 o = make_float2(v[k1].x * scale, v[k1].y * scale);
+      X[k2 + N1 * k1] = o;
+      if (COPY) Vc[r * H + k2 + N1 * k1] = o;
+    }
     if (k2 == 0) X[H] = make_float2(0.f, 0.f);
   }
   __syncthreads();

@@ -1,6 +1,6 @@
-// Four-step launchers (fft4.cuh) for part 1 of the size table in fft4.cu; the parts are
+// Four-step launchers (fft4.cuh, fft4_facies.cuh) for part 1 of the size table in fft4.cu; the parts are
 // separate translation units so that they compile side by side.
-#include "fft4.cuh"
+#include "fft4_facies.cuh"
 
 namespace crava {
 
@@ -45,6 +45,19 @@ cudaError_t four_step_x4_p1(bool fwd, const GridSet& gs, int h, int rows, const 
 #define CRAVA_CASE(NN, A, B) \
   case NN:                   \
     return x4<A, B>(fwd, gs, rows, tw, twn, st);
+    CRAVA_FOUR_STEP_PART(CRAVA_CASE)
+#undef CRAVA_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t four_step_x4_facies_p1(const FaciesFuse& F, const FaciesCorners& C, int h, int rows, const float2* tw,
+                                    const float2* twn, cudaStream_t st) {
+  switch (h) {
+#define CRAVA_CASE(NN, A, B) \
+  case NN:                   \
+    return x4_facies<A, B>(F, C, rows, tw, twn, st);
     CRAVA_FOUR_STEP_PART(CRAVA_CASE)
 #undef CRAVA_CASE
     default:

@@ -262,6 +262,29 @@ struct FaciesCornersHost {
   float4* packed[1 << kMaxFaciesAngles];          // device scratch of facies_packed_bytes each
 };
 size_t facies_packed_bytes(const FaciesBoxHost& b, int nf);
+// the probabilities from volumes already packed (launch_facies_prob_corners = pack + eval)
+cudaError_t launch_facies_eval(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz, int rnxp_in,
+                               int nyp_in, int rnxp_out, const FaciesCornersHost& hc, int nf, const float* prior,
+                               float undef_sum, float* const* out, float* seis_lh, cudaStream_t st);
+// the facies-interleaved copies of every corner volume (hc.dens -> hc.packed)
+cudaError_t launch_facies_pack(const FaciesCornersHost& hc, int nf, cudaStream_t st);
+// What the inverse x transform of the posterior mean needs to evaluate the facies
+// probabilities in the same pass (fft4_facies.cuh).
+struct FaciesFuse {
+  float* mean[3];        // the posterior-mean grids: half spectra in, real rows out, in place
+  float scale;           // their FFTGrid inverse scale
+  int nx, ny, nz, nyp;   // voxels evaluated; the grids' padded y size (rows j + nyp k)
+  int rnxp_out;          // floats per row of the probability grids, 2 (nx / 2 + 1)
+  int nf;
+  float undef_sum;
+  FaciesPrior pr;
+  FaciesOut out;         // nf + 1 probability grids (the last the undefined class)
+  float* seis_lh;        // the seismic likelihood, or null
+};
+// The fused pass for even nxp whose half length has a four-step split (four_step_supported);
+// rows = nyp nzp.  The corner volumes must be packed already.
+cudaError_t launch_x4_facies(const FaciesFuse& F, const FaciesCornersHost& hc, int nxp, int rows, const float2* tw,
+                             const float2* twn, cudaStream_t st, int* nlaunch);
 cudaError_t launch_facies_prob_corners(const float* vp, const float* vs, const float* rho, int nx, int ny, int nz,
                                        int rnxp_in, int nyp_in, int rnxp_out, const FaciesCornersHost& hc, int nf,
                                        const float* prior, float undef_sum, float* const* out, float* seis_lh,

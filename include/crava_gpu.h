@@ -390,6 +390,21 @@ crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_de
                                            const float* const* d_post, int nx, int ny, int nz, int nxp, int nyp,
                                            float* const* d_prob, float* d_seis_lh, void* stream);
 
+/* Facies probabilities computed by crava_job_run itself (AVOInversion's constructor calls
+ * FaciesProb on the posterior right after the inversion, src/avoinversion.cpp:299-302 with
+ * src/faciesprob.cpp:1909-2075): the arguments of crava_facies_prob_local_noise for this job's
+ * lateral size and nz; every later crava_job_run writes d_prob[nfacies+1] (and d_seis_lh if
+ * not null, FFTGrid(nx,ny,nz) layout) from its posterior mean.  Where the x length nxp/2 has a
+ * four-step split, the inverse x transform of the posterior mean evaluates the densities in
+ * the same pass (the mean is not read back); otherwise a separate pass follows it.  The
+ * volumes are packed (and the noise scales tabulated) here into the job's own device memory;
+ * d_density may be freed afterwards, d_prob and d_seis_lh must stay valid while set.
+ * corners = NULL clears the evaluation.  Results are identical to crava_facies_prob_local_noise
+ * on the job's downloaded posterior mean. */
+crava_status crava_job_set_facies(crava_job* job, const crava_facies_desc* corners, int nang,
+                                  const float* const* d_density, int density_row, const float* noise_scale,
+                                  float* const* d_prob, float* d_seis_lh);
+
 /* Batches (no counterpart in the reference, which inverts one interval at a time,
  * main.cpp:217-353): the runs of n created jobs, of any sizes and angle counts, captured
  * once into a CUDA graph with `branches` concurrent branches; every crava_batch_run

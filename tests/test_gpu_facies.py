@@ -158,3 +158,65 @@ def test_facies_corners_against_reference_arithmetic_fixture(ctx):
     torch.cuda.synchronize()
     got = np.stack([t.cpu().numpy()[..., :nx] for t in outs])
     assert rel(got, z["ref_prob"].astype(np.float64)) < 1e-6
+
+
+@pytest.mark.parametrize("dims,nang", [((64, 64, 128), 0), ((64, 64, 128), 2), ((540, 12, 32), 1), ((28, 20, 24), 2)])
+def test_job_facies_in_the_mean_transform(ctx, dims, nang):
+    """crava_job_set_facies: the probabilities written by crava_job_run (in the inverse x
+    transform of the posterior mean where nxp/2 has a four-step split: 32 and 270 here; a
+    separate pass after it for nxp 28) equal crava_facies_prob_local_noise on the job's
+    posterior mean bit for bit, and the posterior mean itself is unchanged."""
+    import torch
+    spec = synth.config0()
+    spec.nx, spec.ny, spec.nz = dims
+    blk = synth.make_block(spec)
+    job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=3)
+    _k = job.upload_block()
+    job.run()
+    torch.cuda.synchronize()
+    mean = [job.download(api.ROLE_POST_MEAN, a) for a in range(3)]
+    m = [x[..., :blk.nx] for x in mean]
+    rng = np.random.default_rng(7 + nang)
+    nf, nbins = 3, (24, 20, 12)
+    prior = [0.25, 0.35, 0.4]
+    descs, keep, d_dens = [], [], []
+    for c in range(1 << nang):
+        widen = 0.04 * (1 + c)
+        vmin = [float(x.min()) - widen for x in m]
+        dv = [(float(x.max()) + widen - vmin[i]) / nbins[i] for i, x in enumerate(m)]
+        fd, k = api.facies_desc(prior, nbins, vmin, dv, 0.02)
+        descs.append(fd)
+        keep.append(k)
+        d_dens.append(torch.from_numpy(rng.random((nf, nbins[2], nbins[1], nbins[0])).astype(np.float32)).cuda())
+    scales = (1.0 + rng.random((nang, blk.ny, blk.nx))).astype(np.float32) if nang else None
+    rnx = 2 * (blk.nx // 2 + 1)
+
+    def grids():
+        return [torch.full((blk.nz, blk.ny, rnx), 7.0, dtype=torch.float32, device="cuda") for _ in range(nf + 2)]
+
+    ref = grids()
+    d_mean = [torch.from_numpy(x).cuda() for x in mean]
+    api.facies_prob_local_noise(ctx, descs, [t.data_ptr() for t in d_dens], nbins[0],
+                                scales if nang else np.zeros((0,)), [t.data_ptr() for t in d_mean], blk.nx, blk.ny,
+                                blk.nz, blk.nxp, blk.nyp, [t.data_ptr() for t in ref[:-1]], ref[-1].data_ptr())
+    got = grids()
+    job.set_facies(descs, [t.data_ptr() for t in d_dens], nbins[0], scales, [t.data_ptr() for t in got[:-1]],
+                   got[-1].data_ptr())
+    del d_dens   # the job holds packed copies
+    for rep in range(2):
+        for t in got:
+            t.fill_(7.0)
+        job.run()
+        torch.cuda.synchronize()
+        for a in range(3):
+            assert np.array_equal(job.download(api.ROLE_POST_MEAN, a), mean[a])
+        for g, r in zip(got, ref):
+            assert torch.equal(g, r)
+    assert np.all(got[0].cpu().numpy()[..., blk.nx:] == -99999.0)
+    job.set_facies(None, None, 0, None, None)
+    for t in got:
+        t.fill_(7.0)
+    job.run()
+    torch.cuda.synchronize()
+    assert bool((got[0] == 7.0).all())
+    job.close()
