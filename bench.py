@@ -586,6 +586,43 @@ def kernels_main(args):
     out["facies_corners"] = timed("facies", lambda: api.facies_prob_local_noise(
         ctx, descs, [d.data_ptr() for d in dens], nbins[0], sc2, d_post, blk.nx, blk.ny, blk.nz, blk.nxp, blk.nyp,
         [t.data_ptr() for t in probs]), fbytes, "as facies_single, 4 corner volumes (2 local-noise angles)")
+    # the whole run with the facies probabilities: the standalone pass after crava_job_run
+    # against crava_job_set_facies (evaluated inside the inverse x transform of the mean)
+    def run_classes(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ctx.set_profiling(True)
+        ctx.kernel_times(reset=True)
+        for _ in range(args.steps):
+            fn()
+        torch.cuda.synchronize()
+        kt = ctx.kernel_times(reset=True)
+        ctx.set_profiling(False)
+        cl = {c: kt[c][0] / args.steps for c in ("line_inv", "x_c2r", "facies")}
+        cl["sum"] = sum(cl.values())
+        cl["run_total"] = sum(v[0] for v in kt.values()) / args.steps
+        return cl
+
+    def separate():
+        job.run()
+        api.facies_prob(ctx, descs[0], dens[0].data_ptr(), nbins[0], d_post, blk.nx, blk.ny, blk.nz, blk.nxp,
+                        blk.nyp, [t.data_ptr() for t in probs])
+
+    sep = run_classes(separate)
+    job.set_facies([descs[0]], [dens[0].data_ptr()], nbins[0], None, [t.data_ptr() for t in probs])
+    forms = {}
+    for name, v in (("job_two_passes_ms", 0), ("job_one_pass_ms", 1)):
+        api.tuning_set("facies_fused", blk.nxp // 2, v)
+        forms[name] = run_classes(job.run)
+    api.tuning_set("facies_fused", blk.nxp // 2, -1)
+    job.set_facies(None, None, 0, None, None)
+    out["facies_in_mean_pass"] = dict(
+        separate_call_ms=sep, **forms,
+        note="ms per run by timer class: crava_job_run then crava_facies_prob (separate call), or "
+             "crava_job_set_facies with the evaluation as a pass after the inverse x transform of the mean "
+             "(two passes, the default) or inside it (one pass: the 3 mean grids transformed and evaluated by "
+             "one kernel, timer class facies); single density volume 100x100x50, 3 facies")
     del keep
     job.close()
     # prior grids of a GRIDS job

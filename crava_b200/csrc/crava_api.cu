@@ -2125,8 +2125,11 @@ namespace {
 
 // The inverse y and x transforms of the three posterior-mean grids with the facies
 // probabilities of crava_job_set_facies: the x transform and the evaluation in one pass
-// (launch_x4_facies) where the x length has a four-step split (schedule key facies_fused,
-// default 1), else the x transform and then the facies pass.
+// (launch_x4_facies) where the x length has a four-step split and the schedule key
+// facies_fused (n = nxp/2) is 1, else the x transform and then the facies pass.  The default
+// is the two passes: at 540x540x256 the one-pass form took 5.4 ms against 0.5 + 2.3 ms, its
+// density gathers (L2-latency bound) running at the transform kernel's occupancy (8 warps
+// per SM against about 40 in the facies pass).
 crava_status inv_mean_facies(crava_ctx* ctx, crava_job* job, float ps, cudaStream_t st) {
   const crava_job_desc& d = job->d;
   Plan *px, *pn, *py;
@@ -2141,7 +2144,7 @@ crava_status inv_mean_facies(crava_ctx* ctx, crava_job* job, float ps, cudaStrea
     CUDA_TRY(launch_line_fft(gs, job->cnxp, d.nyp, (size_t)job->cnxp, d.nzp, (size_t)job->cnxp * d.nyp, py->lp, py->tw,
                              1.f, st, &nl));
   }
-  const bool fused = d.nxp % 2 == 0 && four_step_supported(d.nxp / 2) && tuned("facies_fused", d.nxp / 2, 1) != 0;
+  const bool fused = d.nxp % 2 == 0 && four_step_supported(d.nxp / 2) && tuned("facies_fused", d.nxp / 2, 0) != 0;
   const int rnxp_out = 2 * (d.nx / 2 + 1);
   if (fused) {
     FaciesFuse F;

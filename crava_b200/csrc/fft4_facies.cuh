@@ -65,7 +65,7 @@ static cudaError_t x4_facies(const FaciesFuse& F, const FaciesCorners& C, int ro
                              const float2* twn, cudaStream_t st) {
   using L = RowLayout<N1, N2>;
   constexpr int H = N1 * N2;
-  const int T = std::max(64, std::min(256, tuned("x4_facies_threads", H, 128) / 32 * 32));
+  const int T = std::max(32, std::min(256, tuned("x4_facies_threads", H, 128) / 32 * 32));
   const int rpc = std::max(1, T / N1);
   const size_t smem = sizeof(float2) * (2 * (size_t)H + (size_t)rpc * (L::PITCH + H + 1) + 3 * (size_t)rpc * H);
   cudaError_t e = cudaFuncSetAttribute(k_xc2r4_facies<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

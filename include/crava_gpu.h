@@ -394,9 +394,10 @@ crava_status crava_facies_prob_local_noise(crava_ctx* ctx, const crava_facies_de
  * FaciesProb on the posterior right after the inversion, src/avoinversion.cpp:299-302 with
  * src/faciesprob.cpp:1909-2075): the arguments of crava_facies_prob_local_noise for this job's
  * lateral size and nz; every later crava_job_run writes d_prob[nfacies+1] (and d_seis_lh if
- * not null, FFTGrid(nx,ny,nz) layout) from its posterior mean.  Where the x length nxp/2 has a
- * four-step split, the inverse x transform of the posterior mean evaluates the densities in
- * the same pass (the mean is not read back); otherwise a separate pass follows it.  The
+ * not null, FFTGrid(nx,ny,nz) layout) from its posterior mean: a pass after the inverse x
+ * transform of the mean, or, where nxp/2 has a four-step split and the schedule entry
+ * facies_fused is 1, inside that transform (the mean is not read back; measured slower on
+ * B200, the density gathers then run at the transform kernel's occupancy).  The
  * volumes are packed (and the noise scales tabulated) here into the job's own device memory;
  * d_density may be freed afterwards, d_prob and d_seis_lh must stay valid while set.
  * corners = NULL clears the evaluation.  Results are identical to crava_facies_prob_local_noise

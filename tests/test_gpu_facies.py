@@ -162,10 +162,11 @@ def test_facies_corners_against_reference_arithmetic_fixture(ctx):
 
 @pytest.mark.parametrize("dims,nang", [((64, 64, 128), 0), ((64, 64, 128), 2), ((540, 12, 32), 1), ((28, 20, 24), 2)])
 def test_job_facies_in_the_mean_transform(ctx, dims, nang):
-    """crava_job_set_facies: the probabilities written by crava_job_run (in the inverse x
-    transform of the posterior mean where nxp/2 has a four-step split: 32 and 270 here; a
-    separate pass after it for nxp 28) equal crava_facies_prob_local_noise on the job's
-    posterior mean bit for bit, and the posterior mean itself is unchanged."""
+    """crava_job_set_facies: the probabilities written by crava_job_run equal
+    crava_facies_prob_local_noise on the job's posterior mean bit for bit, and the posterior
+    mean itself is unchanged, with the evaluation inside the inverse x transform of the mean
+    (schedule entry facies_fused = 1, where nxp/2 has a four-step split: 32 and 270 here) and
+    as a separate pass (the default; the only form for nxp 28)."""
     import torch
     spec = synth.config0()
     spec.nx, spec.ny, spec.nz = dims
@@ -203,15 +204,18 @@ def test_job_facies_in_the_mean_transform(ctx, dims, nang):
     job.set_facies(descs, [t.data_ptr() for t in d_dens], nbins[0], scales, [t.data_ptr() for t in got[:-1]],
                    got[-1].data_ptr())
     del d_dens   # the job holds packed copies
-    for rep in range(2):
-        for t in got:
-            t.fill_(7.0)
-        job.run()
-        torch.cuda.synchronize()
-        for a in range(3):
-            assert np.array_equal(job.download(api.ROLE_POST_MEAN, a), mean[a])
-        for g, r in zip(got, ref):
-            assert torch.equal(g, r)
+    for fused in (1, 0):
+        api.tuning_set("facies_fused", blk.nxp // 2, fused)
+        for rep in range(2):
+            for t in got:
+                t.fill_(7.0)
+            job.run()
+            torch.cuda.synchronize()
+            for a in range(3):
+                assert np.array_equal(job.download(api.ROLE_POST_MEAN, a), mean[a])
+            for g, r in zip(got, ref):
+                assert torch.equal(g, r)
+    api.tuning_set("facies_fused", blk.nxp // 2, -1)
     assert np.all(got[0].cpu().numpy()[..., blk.nx:] == -99999.0)
     job.set_facies(None, None, 0, None, None)
     for t in got:
