@@ -80,6 +80,37 @@ class StormGeom(ctypes.Structure):
                 ("top_name", ctypes.c_char_p), ("bot_name", ctypes.c_char_p)]
 
 
+class SegyDesc(ctypes.Structure):
+    _fields_ = [("x0", ctypes.c_double), ("y0", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("angle", ctypes.c_double), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dz", ctypes.c_double), ("top", _dp), ("top_z", ctypes.c_double), ("rel_thick", _dp),
+                ("zmin", ctypes.c_double), ("zmax", ctypes.c_double), ("il0", ctypes.c_double),
+                ("xl0", ctypes.c_double), ("il_step_x", ctypes.c_double), ("il_step_y", ctypes.c_double),
+                ("xl_step_x", ctypes.c_double), ("xl_step_y", ctypes.c_double), ("z0", ctypes.c_float),
+                ("header_format", ctypes.c_int), ("text", ctypes.POINTER(ctypes.c_char_p)), ("ntext", ctypes.c_int)]
+
+
+def segy_desc(geom: dict, top=None, rel_thick=None, text=None):
+    """A crava_segy_desc from geom (the scalar fields) and optional per-trace top / relative
+    thickness arrays (ny, nx) and textual-header lines; returns (desc, keep-alive objects)."""
+    d = SegyDesc(**{k: v for k, v in geom.items()})
+    keep = []
+    if top is not None:
+        t = np.ascontiguousarray(top, dtype=np.float64)
+        keep.append(t)
+        d.top = t.ctypes.data_as(_dp)
+    if rel_thick is not None:
+        r = np.ascontiguousarray(rel_thick, dtype=np.float64)
+        keep.append(r)
+        d.rel_thick = r.ctypes.data_as(_dp)
+    if text is not None:
+        arr = (ctypes.c_char_p * len(text))(*[str(x).encode() for x in text])
+        keep.append(arr)
+        d.text = ctypes.cast(arr, ctypes.POINTER(ctypes.c_char_p))
+        d.ntext = len(text)
+    return d, keep
+
+
 class FaciesDesc(ctypes.Structure):
     _fields_ = [("nfacies", ctypes.c_int), ("nbins", ctypes.c_int * 3), ("vmin", ctypes.c_double * 3),
                 ("dv", ctypes.c_double * 3), ("prior", _fp), ("p_undefined", ctypes.c_float)]
@@ -150,6 +181,8 @@ def lib() -> ctypes.CDLL:
                                                 ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     L.crava_job_fill_prior_auto_cov.argtypes = [vp, vp, ctypes.c_float, ctypes.c_float, vp]
+    L.crava_grid_write_segy.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(SegyDesc), vp]
     L.crava_job_set_facies.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, vp,
                                        ctypes.POINTER(vp), vp]
     L.crava_circ_corr_t.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
@@ -619,6 +652,12 @@ def grid_read_crava(ctx: Context, path: str, d_grid: int, rnxp: int, nyp: int, n
     g = SimboxGeom()
     _check(lib().crava_grid_read_crava(ctx.handle, str(path).encode(), d_grid, rnxp, nyp, nzp, ctypes.byref(g), stream))
     return {k: getattr(g, k) for k, _t in SimboxGeom._fields_}
+
+
+def grid_write_segy(ctx: Context, path: str, d_grid: int, rnxp: int, nyp: int, nzp: int, desc, stream=None):
+    """FFTGrid::writeSegyFile of a real device grid (rnxp x nyp x nzp floats); desc from segy_desc."""
+    _check(lib().crava_grid_write_segy(ctx.handle, str(path).encode(), d_grid, rnxp, nyp, nzp, ctypes.byref(desc),
+                                       stream))
 
 
 def grid_write_storm(ctx: Context, path: str, d_grid: int, dims, padded_dims, geom: dict, padding: bool = False,

@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrava_gpu.so")
-SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "fft4_p1.cu", "fft4_p2.cu", "fft4_p3.cu", "fft4_p4.cu", "fft4_p5.cu", "fft4_p6.cu", "zpass.cu", "zpass_n12.cu", "zpass_n34.cu", "zpass_n56.cu", "zpass_n78.cu", "pencil.cu", "pencil_s1.cu", "pencil_s2.cu", "pencil_s3.cu", "localnoise.cu", "gridio.cu", "facies.cu", "thick.cu", "prior.cu"]
-HEADERS = ["fft_core.cuh", "fft2.cuh", "fft4.cuh", "kernels.cuh", "pencil_common.cuh", "pencil.cuh", "zpass.cuh"]
+SOURCES = ["crava_api.cu", "kernels.cu", "fft4.cu", "fft4_p1.cu", "fft4_p2.cu", "fft4_p3.cu", "fft4_p4.cu", "fft4_p5.cu", "fft4_p6.cu", "zpass.cu", "zpass_n12.cu", "zpass_n34.cu", "zpass_n56.cu", "zpass_n78.cu", "pencil.cu", "pencil_s1.cu", "pencil_s2.cu", "pencil_s3.cu", "localnoise.cu", "gridio.cu", "facies.cu", "thick.cu", "prior.cu", "segy.cu"]
+HEADERS = ["fft_core.cuh", "fft2.cuh", "fft4.cuh", "kernels.cuh", "pencil_common.cuh", "pencil.cuh", "zpass.cuh", "facies.cuh", "fft4_facies.cuh", "ibm_float.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

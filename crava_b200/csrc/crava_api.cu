@@ -1374,6 +1374,225 @@ crava_status crava_grid_read_storm(crava_ctx* ctx, const char* path, float* d_gr
   return CRAVA_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// ASCII to EBCDIC as the SEG-Y rev 1 textual header uses it (code page 037 for the printable
+// characters; '[', ']', '^' and the controls 14, 15, 25, which the standard's table leaves out,
+// map to 0), the same table as NRLib's transtab (libs/nrlib/segy/commonheaders.cpp:29-48).
+const unsigned char kEbcdic[128] = {
+    0x00, 0x01, 0x02, 0x03, 0x37, 0x2d, 0x2e, 0x2f, 0x16, 0x05, 0x25, 0x0b, 0x0c, 0x0d, 0x00, 0x00,
+    0x10, 0x11, 0x12, 0x13, 0x3c, 0x3d, 0x32, 0x26, 0x18, 0x00, 0x3f, 0x27, 0x1c, 0x1d, 0x1e, 0x1f,
+    0x40, 0x5a, 0x7f, 0x7b, 0x5b, 0x6c, 0x50, 0x7d, 0x4d, 0x5d, 0x5c, 0x4e, 0x6b, 0x60, 0x4b, 0x61,
+    0xf0, 0xf1, 0xf2, 0xf3, 0xf4, 0xf5, 0xf6, 0xf7, 0xf8, 0xf9, 0x7a, 0x5e, 0x4c, 0x7e, 0x6e, 0x6f,
+    0x7c, 0xc1, 0xc2, 0xc3, 0xc4, 0xc5, 0xc6, 0xc7, 0xc8, 0xc9, 0xd1, 0xd2, 0xd3, 0xd4, 0xd5, 0xd6,
+    0xd7, 0xd8, 0xd9, 0xe2, 0xe3, 0xe4, 0xe5, 0xe6, 0xe7, 0xe8, 0xe9, 0x00, 0xe0, 0x00, 0x00, 0x6d,
+    0x79, 0x81, 0x82, 0x83, 0x84, 0x85, 0x86, 0x87, 0x88, 0x89, 0x91, 0x92, 0x93, 0x94, 0x95, 0x96,
+    0x97, 0x98, 0x99, 0xa2, 0xa3, 0xa4, 0xa5, 0xa6, 0xa7, 0xa8, 0xa9, 0xc0, 0x4f, 0xd0, 0xa1, 0x07};
+
+// The 3200-byte textual header: 40 card images "C nn" (the last "C40 END EBCDIC"), with CRAVA's
+// banner (TextualHeader::standardHeader) or the caller's lines from column 6 of line t + 2
+// (TextualHeader::SetLine(t + 1), 75 characters at most).
+std::string segy_text_header(const crava_segy_desc* d) {
+  std::string a(3200, ' ');
+  for (int l = 0; l < 40; l++) {
+    char card[8];
+    std::snprintf(card, sizeof(card), "C%2d", l + 1);
+    a.replace((size_t)l * 80, 3, card);
+  }
+  a.replace(39 * 80, 14, "C40 END EBCDIC");
+  if (!d->text) {
+    static const struct { int line; const char* s; } banner[] = {
+        {11, "THIS SEGY FILE WAS WRITTEN BY"}, {13, "THE CRAVA PROGRAM"}, {15, "DEVELOPED BY"},
+        {17, "RAGNAR HAUGE"}, {19, "ANNE RANDI SYVERSVEEN           AND"}, {21, "ODD KOLBJORNSEN"},
+        {23, "AT"}, {25, "THE NORWEGIAN COMPUTING CENTER"}, {27, "2003"}};
+    for (const auto& b : banner) a.replace((size_t)b.line * 80 + 12, std::strlen(b.s), b.s);
+  } else {
+    for (int t = 0; t < d->ntext && t < 39; t++) {
+      std::string s = d->text[t] ? d->text[t] : "";
+      s.resize(75, ' ');
+      a.replace((size_t)(t + 1) * 80 + 5, 75, s);
+    }
+  }
+  for (auto& c : a) c = (char)((unsigned char)c < 128 ? kEbcdic[(unsigned char)c] : 0);
+  return a;
+}
+
+void put_be16(unsigned char* p, int v) {
+  p[0] = (unsigned char)((v >> 8) & 0xff);
+  p[1] = (unsigned char)(v & 0xff);
+}
+void put_be32(unsigned char* p, int v) {
+  for (int q = 0; q < 4; q++) p[q] = (unsigned char)(((unsigned)v >> (24 - 8 * q)) & 0xffu);
+}
+
+}  // namespace
+
+extern "C" {
+
+crava_status crava_grid_write_segy(crava_ctx* ctx, const char* path, const float* d_grid, int rnxp, int nyp, int nzp,
+                                   const crava_segy_desc* d, void* stream) {
+  if (!ctx || !path || !d_grid || !d) return fail(CRAVA_EINVAL, "null argument");
+  if (d->nx < 1 || d->ny < 1 || d->nz < 2 || rnxp < d->nx || nyp < d->ny || nzp < d->nz || !(d->dx > 0) ||
+      !(d->dy > 0) || d->header_format < 0 || d->header_format > 5 || (d->text && d->ntext < 0))
+    return fail(CRAVA_EINVAL, "bad SegY description");
+  // the regular axis (FFTGrid::writeSegyFile, src/fftgrid.cpp:1980-1986)
+  float dz = static_cast<float>(std::floor(d->dz + 0.5));
+  if (dz == 0) dz = 1.0f;
+  const double nsd = std::ceil((d->zmax - static_cast<double>(d->z0)) / static_cast<double>(dz));
+  if (!(nsd >= 1.0) || nsd > 32767.0) return fail(CRAVA_EINVAL, "SegY sample count outside 1..32767");
+  const int ns = static_cast<int>(nsd);
+  // trace-header locations (1-based) of the format: x, y, inline, crossline
+  // (TraceHeaderFormat::Init, libs/nrlib/segy/traceheader.cpp:150-225)
+  static const int loc[6][4] = {{73, 77, 9, 21},    {73, 77, 221, 21},  {181, 185, 189, 193},
+                                {73, 77, 5, 21},    {73, 77, 181, 185}, {73, 77, 185, 189}};
+  const int* L = loc[d->header_format];
+  struct Rec {
+    int il, xl, ux, uy;
+    size_t idx;
+    SegyTrace tr;
+  };
+  std::vector<Rec> rec;
+  rec.reserve((size_t)d->nx * d->ny);
+  const double cr = std::cos(d->angle), sr = std::sin(d->angle);
+  for (int j = 0; j < d->ny; j++)
+    for (int i = 0; i < d->nx; i++) {
+      const size_t q = (size_t)i + (size_t)d->nx * j;
+      const double top = d->top ? d->top[q] : d->top_z;
+      if (top == -99999.0 || top == -999.0) continue;   // RMISSING / WELLMISSING: no record
+      // Simbox::getXYCoord (src/simbox.cpp:821-827), the coordinates as float, then double
+      const double rx = (static_cast<double>(i) + 0.5) * d->dx, ry = (static_cast<double>(j) + 0.5) * d->dy;
+      const double x = static_cast<double>(static_cast<float>(rx * cr - ry * sr + d->x0));
+      const double y = static_cast<double>(static_cast<float>(rx * sr + ry * cr + d->y0));
+      const double gdz = d->dz * (d->rel_thick ? d->rel_thick[q] : 1.0);
+      int first = static_cast<int>(std::floor(0.5 + (top - d->z0) / dz));
+      int end = static_cast<int>(std::floor(0.5 + ((top - d->z0) + d->nz * gdz) / dz));
+      end = std::min(end, ns);
+      first = std::min(first, ns);
+      Rec r;
+      // SegyGeometry::FindILXL (libs/nrlib/segy/segygeometry.cpp:1044-1049)
+      r.il = static_cast<int>(0.5 + d->il0 + (x - d->x0) * d->il_step_x + (y - d->y0) * d->il_step_y);
+      r.xl = static_cast<int>(0.5 + d->xl0 + (x - d->x0) * d->xl_step_x + (y - d->y0) * d->xl_step_y);
+      r.ux = static_cast<int>(x);
+      r.uy = static_cast<int>(y);
+      r.idx = q;
+      r.tr = SegyTrace{i, j, first, end, top, gdz};
+      rec.push_back(r);
+    }
+  // inline, crossline, then table index (SortILXL, libs/nrlib/segy/segy.cpp:1364-1381)
+  std::sort(rec.begin(), rec.end(), [](const Rec& a, const Rec& b) {
+    if (a.il != b.il) return a.il < b.il;
+    if (a.xl != b.xl) return a.xl < b.xl;
+    return a.idx < b.idx;
+  });
+  const size_t nrec = rec.size();
+  // 240-byte trace headers (TraceHeader::Write, traceheader.cpp:527-587), big-endian
+  std::vector<unsigned char> hdr(nrec * 240, 0);
+  std::vector<SegyTrace> trs(nrec);
+  const int dt = static_cast<short>(static_cast<unsigned short>(dz * 1000));
+  const int t0 = static_cast<short>(static_cast<float>(static_cast<short>(d->z0)));
+  for (size_t r = 0; r < nrec; r++) {
+    unsigned char* h = hdr.data() + r * 240;
+    put_be32(h + 36, 0);                 // offset
+    put_be16(h + 70, 1);                 // scalco
+    put_be32(h + L[0] - 1, rec[r].ux);
+    put_be32(h + L[1] - 1, rec[r].uy);
+    put_be16(h + 108, t0);               // start time
+    put_be16(h + 114, ns);
+    put_be16(h + 116, dt);
+    put_be32(h + L[2] - 1, rec[r].il);
+    put_be32(h + L[3] - 1, rec[r].xl);
+    trs[r] = rec[r].tr;
+  }
+  // binary header (BinaryHeader::Write, libs/nrlib/segy/commonheaders.cpp:233-265; written before
+  // the geometry is set, so its trace count per line is 0)
+  unsigned char bin[400] = {};
+  put_be32(bin + 0, 9999);
+  put_be32(bin + 4, 1);
+  put_be32(bin + 8, 1);
+  put_be16(bin + 16, static_cast<short>(1000 * static_cast<double>(dz)));
+  put_be16(bin + 20, static_cast<short>(ns));
+  put_be16(bin + 24, 1);   // IBM float samples
+  put_be16(bin + 26, 1);
+  put_be16(bin + 28, 4);
+  put_be16(bin + 54, 1);
+  put_be16(bin + 302, 1);  // constant trace length
+  const std::string text = segy_text_header(d);
+
+  std::lock_guard<std::mutex> lk(ctx->io_mu);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  crava_status s = io_buffers(ctx);
+  if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(CRAVA_EINVAL, std::string("cannot open ") + path + " for writing");
+  bool ok = std::fwrite(text.data(), 1, 3200, f) == 3200 && std::fwrite(bin, 1, 400, f) == 400;
+  // headers and per-trace parameters on the device, then chunks of whole records packed into
+  // the device staging half c%2 and downloaded into the pinned half c%2; the file write of chunk
+  // c-1 runs while chunk c is in flight
+  char* dmem = nullptr;
+  const size_t hb = align256(nrec * 240), tb = align256(nrec * sizeof(SegyTrace));
+  cudaError_t e = cudaSuccess;
+  if (nrec) {
+    e = cudaMallocAsync((void**)&dmem, hb + tb, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dmem, hdr.data(), nrec * 240, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dmem + hb, trs.data(), nrec * sizeof(SegyTrace), cudaMemcpyHostToDevice, st);
+  }
+  SegyPack P;
+  P.grid = d_grid;
+  P.rnxp = rnxp;
+  P.nyp = nyp;
+  P.nz = d->nz;
+  P.ns = ns;
+  P.z0 = d->z0;
+  P.dz = dz;
+  P.hdr = (const uint32_t*)dmem;
+  P.tr = (const SegyTrace*)(dmem + hb);
+  const size_t recb = 240 + 4 * (size_t)ns;
+  const size_t per = std::max<size_t>(1, kIoChunk / recb);
+  size_t pending[2] = {0, 0};
+  int nl = 0;
+  for (size_t r0 = 0, c = 0; ok && e == cudaSuccess && r0 < nrec; r0 += per, c++) {
+    const int b = (int)(c % 2);
+    const size_t nr = std::min(per, nrec - r0);
+    if (pending[b]) {
+      e = cudaEventSynchronize(ctx->io_ev[b]);
+      if (e == cudaSuccess) ok = std::fwrite(ctx->io_host[b], 1, pending[b], f) == pending[b];
+      pending[b] = 0;
+    }
+    uint32_t* dst = (uint32_t*)(ctx->io_dev + b * kIoChunk);
+    if (e == cudaSuccess) e = launch_segy_pack(P, r0, (int)nr, dst, st);
+    nl++;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->io_host[b], dst, nr * recb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->io_ev[b], st);
+    pending[b] = nr * recb;
+    const int o = 1 - b;
+    if (e == cudaSuccess && ok && pending[o]) {
+      e = cudaEventSynchronize(ctx->io_ev[o]);
+      if (e == cudaSuccess) ok = std::fwrite(ctx->io_host[o], 1, pending[o], f) == pending[o];
+      pending[o] = 0;
+    }
+  }
+  for (int b = 0; b < 2 && e == cudaSuccess && ok; b++)
+    if (pending[b]) {
+      e = cudaEventSynchronize(ctx->io_ev[b]);
+      if (e == cudaSuccess) ok = std::fwrite(ctx->io_host[b], 1, pending[b], f) == pending[b];
+    }
+  if (dmem) {
+    cudaFreeAsync(dmem, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (e != cudaSuccess) return cuda_fail(e, "crava_grid_write_segy");
+  if (!ok) return fail(CRAVA_EINVAL, std::string("writing ") + path + " failed");
+  {
+    std::lock_guard<std::mutex> lk2(ctx->mu);
+    ctx->launches += nl;
+  }
+  return CRAVA_OK;
+}
+
 crava_status crava_circ_corr_t(const double* prior_corr_t, int n, int min_int_fq, int nzp, float* out) {
   if (!prior_corr_t || !out || n < 1 || nzp < 2) return fail(CRAVA_EINVAL, "bad arguments");
   if (!(prior_corr_t[0] != 0.0)) return fail(CRAVA_EINVAL, "prior_corr_t[0] must be nonzero");

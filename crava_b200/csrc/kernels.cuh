@@ -254,6 +254,22 @@ cudaError_t launch_storm_unpack(float* grid, const uint32_t* src, int nx, int ny
                                 int nyp, cudaStream_t st);
 cudaError_t launch_pad_fill(float* grid, int nx, int ny, int nz, int nxp, int nyp, int nzp, int rnxp, cudaStream_t st,
                             int* nlaunch);
+// SegY records (segy.cu): per record (inline/crossline order) the trace's grid column, its
+// first and end regular samples with data, its top and grid sample spacing; hdr holds the 240-byte
+// trace headers (60 words per record, already big-endian).
+struct SegyTrace {
+  int i, j, first, end;
+  double ztop, gdz;
+};
+struct SegyPack {
+  const float* grid;
+  int rnxp, nyp, nz;
+  int ns;
+  float z0, dz;
+  const SegyTrace* tr;
+  const uint32_t* hdr;
+};
+cudaError_t launch_segy_pack(const SegyPack& P, size_t r0, int nr, uint32_t* out, cudaStream_t st);
 struct FaciesCornersHost {
   int nang;
   const float* t;                                 // device, nang x ny x nx

@@ -297,6 +297,36 @@ crava_status crava_grid_write_storm(crava_ctx* ctx, const char* path, const floa
 crava_status crava_grid_read_storm(crava_ctx* ctx, const char* path, float* d_grid, int nx, int ny, int nz, int nxp,
                                    int nyp, int nzp, crava_storm_geom* geom, void* stream);
 
+/* SegY file of a device grid: FFTGrid::writeSegyFile (src/fftgrid.cpp:1960-2050) with NRLib's
+ * SegY writer (libs/nrlib/segy/segy.cpp:294-320, 1218-1272, 1397-1430): the 3200-byte EBCDIC
+ * textual header (the standard CRAVA banner; or, with text, the empty header with text[t] in
+ * line t + 2 from column 6, at most 75 characters, t < 39, as TextualHeader::SetLine(t + 1)), the
+ * 400-byte binary header (sample interval 1000 dz, ns, format 1), then one record per trace
+ * whose top is not missing, in inline/crossline order: a 240-byte trace header (scalco 1, x, y,
+ * ns, dt, inline, crossline, start time z0, offset 0 at the locations of header_format) and ns
+ * IBM floats, big-endian.  Samples lie on the regular axis z0 + k dz, dz = round(simbox dz)
+ * (1 if that is 0), ns = ceil((zmax - z0) / dz); each trace's grid values (top + (k' + 1/2) of
+ * its simbox dz times rel_thick) are interpolated linearly onto it between the trace's first and
+ * last regular sample (FFTGrid::getRegularZInterpolatedRealValue, :2275-2306), zero outside.
+ * The trace resampling, the IBM conversion and the record packing run on the device; files are
+ * staged through two pinned chunks as crava_grid_write_crava. */
+typedef struct {
+  double x0, y0, dx, dy, angle;   /* simbox: GetXMin, GetYMin, cell size, rotation (radians)   */
+  int nx, ny, nz;                 /* simbox cells (the grid's nx_, ny_, nz_)                     */
+  double dz;                      /* simbox getdz()                                              */
+  const double* top;              /* nx*ny top z per trace (i + nx*j), -99999 = missing; or NULL */
+  double top_z;                   /*   constant top when top is NULL                             */
+  const double* rel_thick;        /* nx*ny relative thickness (i + nx*j), or NULL for 1          */
+  double zmin, zmax;              /* simbox getMinMaxZ                                           */
+  double il0, xl0, il_step_x, il_step_y, xl_step_x, xl_step_y;   /* simbox IL/XL geometry      */
+  float z0;                       /* time of the first regular sample                            */
+  int header_format;              /* 0 SeisWorks, 1 IESX, 2 SIP, 3 Charisma, 4 SIPX, 5 HESS      */
+  const char* const* text;        /* ntext textual header lines (line 1 first), or NULL          */
+  int ntext;
+} crava_segy_desc;
+crava_status crava_grid_write_segy(crava_ctx* ctx, const char* path, const float* d_grid, int rnxp, int nyp, int nzp,
+                                   const crava_segy_desc* desc, void* stream);
+
 /* Host-side temporal prior functions (no device needed).
  * crava_circ_corr_t: SeismicParametersHolder::computeCircCorrT with makeCircCorrTPosDef
  * (src/seismicparametersholder.cpp:624-660, 805-840): the circular temporal correlation of

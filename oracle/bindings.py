@@ -3,6 +3,8 @@
 * ``_build/liboracle.so``  -- plain-C restatement of the reference's noise source.
 * ``_ref/libref32.so``     -- the reference's FP32 numerics with the restated loops
                               (absent where the reference tree was not available at build).
+* ``_ref/libsegyref.so``   -- FFTGrid::writeSegyFile over NRLib's own SegY header, geometry
+                              and IBM-float code.
 """
 from __future__ import annotations
 
@@ -14,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF32_LIB = os.path.join(HERE, "_ref", "libref32.so")
+SEGYREF_LIB = os.path.join(HERE, "_ref", "libsegyref.so")
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -205,3 +208,14 @@ def ref32_facies_prob(post, corners, prior, p_undefined, t):
                           box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nf, _f(pr), float(p_undefined),
                           _f(tt) if tt.size else None, _f(out))
     return out
+
+
+def segy_ref_write(path: str, grid: np.ndarray, desc) -> None:
+    """The reference's SegY file of a host grid (nzp, nyp, rnxp float32) for a crava_segy_desc
+    (crava_b200.api.SegyDesc)."""
+    L = ctypes.CDLL(SEGYREF_LIB)
+    L.segy_ref_write.argtypes = [ctypes.c_char_p, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    g = np.ascontiguousarray(grid, dtype=np.float32)
+    rc = L.segy_ref_write(str(path).encode(), _f(g), g.shape[2], g.shape[1], ctypes.addressof(desc))
+    if rc != 0:
+        raise RuntimeError(f"segy_ref_write failed ({rc})")
