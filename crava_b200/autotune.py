@@ -22,6 +22,8 @@ fastest value.  The keys swept, with their size key n:
                                         shared memory, 0 = read from global memory (n = nxp/2)
   x4_threads_fwd, x4_threads_inv       four-step row transforms: threads per CTA
                  n = nxp/2
+  line4_pf_fwd, line4_pf_inv (n = N),  L2 prefetch of the tiles (rows) that many quarters of
+  x4_pf_fwd, x4_pf_inv (n = nxp/2)     the resident CTAs ahead; 0 = off
 
 The file holds one "key n value" line per entry; the library reads it at first use (it
 sits beside libcrava_gpu.so) and falls back to built-in defaults for sizes it does not list.
@@ -160,6 +162,10 @@ def tune_workload(name, w, reps, entries, log):
         b = sweep(ctx, job, stream, reps, tkey, nyp, tv, cls, log)
         if b:
             entries[(tkey, nyp)] = b[0]
+        pkey = "line4_pf_fwd" if tkey.endswith("fwd") else "line4_pf_inv"
+        b = sweep(ctx, job, stream, reps, pkey, nyp, [0, 2, 4], cls, log)
+        if b:
+            entries[(pkey, nyp)] = b[0]
     if nxp % 2 == 0:
         h = nxp // 2
         for key, skey, cls in (("x4_threads_fwd", "x4_stage_fwd", ["x_r2c"]),
@@ -175,6 +181,10 @@ def tune_workload(name, w, reps, entries, log):
                 api.tuning_set(key, h, best[1])
                 entries[(skey, h)] = best[0]
                 entries[(key, h)] = best[1]
+            pkey = key.replace("threads", "pf")
+            b = sweep(ctx, job, stream, reps, pkey, h, [0, 2, 4], cls, log)
+            if b:
+                entries[(pkey, h)] = b[0]
     total = time_classes(ctx, job, stream, reps)
     log.append(f"# {name} tuned: " + ", ".join(f"{k} {v:.3f}" for k, v in sorted(total.items())) +
                f"; sum {sum(total.values()):.3f} ms")

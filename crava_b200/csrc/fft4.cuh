@@ -69,7 +69,7 @@ constexpr size_t line4_smem(int W, int SK) {
 template <int N1, int N2, int DIR>
 __global__ void __launch_bounds__(DIR > 0 ? 512 : 256) k_line4(const __grid_constant__ GridSet gs, int ni, size_t pstride,
                                                size_t ostride, int W, int lw, int nIT, int SK,
-                                               const float2* __restrict__ twg) {
+                                               const float2* __restrict__ twg, int pf) {
   constexpr int N = N1 * N2;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -77,6 +77,20 @@ __global__ void __launch_bounds__(DIR > 0 ? 512 : 256) k_line4(const __grid_cons
   const int it = blockIdx.x % nIT, o = blockIdx.x / nIT;
   const int i0 = it * W, nw = min(W, ni - i0);
   float2* g = reinterpret_cast<float2*>(gs.p[blockIdx.y]) + (size_t)o * ostride + i0;
+  // pf > 0: the cache lines of the tile pf block indices on (x fastest) go to L2
+  if (pf > 0) {
+    const int tn = blockIdx.y * gridDim.x + blockIdx.x + pf;
+    if (tn < (int)(gridDim.x * gridDim.y)) {
+      const int gy = tn / gridDim.x, gx = tn - gy * gridDim.x;
+      const int itn = gx % nIT, on = gx / nIT;
+      const int nwn = min(W, ni - itn * W);
+      const float2* gn = reinterpret_cast<const float2*>(gs.p[gy]) + (size_t)on * ostride + itn * W;
+      for (int q = threadIdx.x; q < 2 * N; q += blockDim.x) {
+        const float2* row = gn + (size_t)(q >> 1) * pstride;
+        l2_prefetch_line((q & 1) ? (const void*)(row + nwn - 1) : (const void*)row);
+      }
+    }
+  }
   __syncthreads();
   line4_tile<N1, N2, DIR>(g, pstride, g, nw, pstride, W, lw, SK, tw, sm + N);
 }
@@ -530,8 +544,16 @@ static cudaError_t line4(const GridSet& gs, int ni, size_t pstride, int no, size
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(nIT * no), gs.n);
-  if (sign < 0.f) k_line4<N1, N2, -1><<<grid, T, smem, st>>>(gs, ni, pstride, ostride, W, lw, nIT, SK, tw);
-  else k_line4<N1, N2, 1><<<grid, T, smem, st>>>(gs, ni, pstride, ostride, W, lw, nIT, SK, tw);
+  // L2 line prefetch ahead of the tiles: schedule keys line4_pf_fwd / line4_pf_inv, the distance in
+  // quarters of the resident tiles (0 = off)
+  int pf = 0;
+  if (const int q = tuned(sign < 0.f ? "line4_pf_fwd" : "line4_pf_inv", N, 0)) {
+    int res = 0;
+    if ((e = resident_grid(fn, T, smem, 1 << 30, &res)) != cudaSuccess) return e;
+    pf = std::max(1, res * q / 4);
+  }
+  if (sign < 0.f) k_line4<N1, N2, -1><<<grid, T, smem, st>>>(gs, ni, pstride, ostride, W, lw, nIT, SK, tw, pf);
+  else k_line4<N1, N2, 1><<<grid, T, smem, st>>>(gs, ni, pstride, ostride, W, lw, nIT, SK, tw, pf);
   return cudaGetLastError();
 }
 
@@ -564,12 +586,15 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((rows + rpc - 1) / rpc), gs.n);
-  // L2 prefetch of the row chunk one wave ahead (schedule keys x4_pf_fwd / x4_pf_inv, 1 = on;
-  // measured faster for the forward rows at h = 270, slower for the inverse ones)
+  // L2 prefetch of the row chunk ahead of the CTAs (schedule keys x4_pf_fwd / x4_pf_inv: the
+  // distance in quarters of the resident CTAs, 0 = off; one wave, 4, measured faster for the
+  // forward rows at h = 270, slower for the inverse ones)
   int pf = 0;
-  if (tuned(fwd ? "x4_pf_fwd" : "x4_pf_inv", L::H, fwd ? 1 : 0) != 0 &&
-      (e = resident_grid(fn, T, smem, 1 << 30, &pf)) != cudaSuccess)
-    return e;
+  if (const int q = tuned(fwd ? "x4_pf_fwd" : "x4_pf_inv", L::H, fwd ? 4 : 0)) {
+    int res = 0;
+    if ((e = resident_grid(fn, T, smem, 1 << 30, &res)) != cudaSuccess) return e;
+    pf = std::max(1, res * q / 4);
+  }
   if (fwd) k_xr2c4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn, stage, pf);
   else k_xc2r4<N1, N2><<<grid, T, smem, st>>>(gs, rows, rpc, tw, twn, stage, pf);
   return cudaGetLastError();

@@ -292,6 +292,11 @@ __device__ __forceinline__ void l2_prefetch(const void* p, size_t n, const void*
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(ga), "r"((uint32_t)(e - a)) : "memory");
   }
 }
+// L2 prefetch of the cache line holding global address p (an ordinary load-unit request, no
+// bulk-copy unit); p must lie inside an allocation.
+__device__ __forceinline__ void l2_prefetch_line(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(__cvta_generic_to_global(p)));
+}
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
