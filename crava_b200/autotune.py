@@ -173,7 +173,7 @@ def tune_workload(name, w, reps, entries, log):
             best = None
             for stage in (1, 0):
                 api.tuning_set(skey, h, stage)
-                b = sweep(ctx, job, stream, reps, key, h, [64, 128, 192, 256], cls, log)
+                b = sweep(ctx, job, stream, reps, key, h, [64, 96, 128, 160, 192, 256], cls, log)
                 if b and (best is None or b[1] < best[2]):
                     best = (stage, b[0], b[1])
             if best:
