@@ -22,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcrava_gpu.so")
 
-OK, EINVAL, ENOMEM, ECUDA, ETIMEDOUT, ENUMERIC, ENOTSUP, ESTATE = range(8)
+OK, EINVAL, ENOMEM, ECUDA, ETIMEDOUT, ENUMERIC, ENOTSUP, ESTATE, EBUSY, ECANCELED = range(10)
 ROLE_DATA, ROLE_MEAN, ROLE_PRIOR_COV, ROLE_ERR_CORR, ROLE_POST_COV, ROLE_SIM, ROLE_NOISE, \
     ROLE_RESIDUAL, ROLE_POST_MEAN = range(9)
 PRIOR_SEPARABLE, PRIOR_GRIDS = 0, 1
@@ -164,6 +164,9 @@ def lib() -> ctypes.CDLL:
     L.crava_serve_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(RequestInfo)]
     L.crava_serve_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
     L.crava_serve_stop.argtypes = [vp]
+    L.crava_serve_set_queue_limit.argtypes = [vp, ctypes.c_int]
+    L.crava_serve_cancel.argtypes = [vp, ctypes.c_uint64]
+    L.crava_ctx_fail_next_allocs.argtypes = [vp, ctypes.c_int]
     L.crava_invert_noalloc.argtypes = [ctypes.POINTER(JobDesc), ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
     L.crava_facies_smooth.argtypes = [vp, ctypes.POINTER(FaciesDesc), ctypes.POINTER(ctypes.c_double), vp, vp]
     L.crava_facies_prob.argtypes = [vp, ctypes.POINTER(FaciesDesc), vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
@@ -257,6 +260,10 @@ class Context:
 
     def kernel_launches(self) -> int:
         return int(lib().crava_ctx_kernel_launches(self._h))
+
+    def fail_next_allocs(self, n: int):
+        """Fault injection: the next n job allocations fail with ENOMEM (crava_ctx_fail_next_allocs)."""
+        _check(lib().crava_ctx_fail_next_allocs(self._h, int(n)))
 
     def set_profiling(self, on: bool):
         _check(lib().crava_ctx_set_profiling(self._h, int(on)))
@@ -586,6 +593,14 @@ class Server:
             self._keep.pop(ticket, None)
         _check(st)
         return {"state": info.state, "status": info.status, "queue_ms": info.queue_ms, "latency_ms": info.latency_ms}
+
+    def set_queue_limit(self, max_queued: int):
+        """At most max_queued waiting requests; further submits raise CravaError(EBUSY)."""
+        _check(lib().crava_serve_set_queue_limit(self._h, int(max_queued)))
+
+    def cancel(self, ticket: int):
+        """Cancels a request that is still queued (CravaError(ESTATE) once admitted)."""
+        _check(lib().crava_serve_cancel(self._h, ticket))
 
     def stop(self):
         if self._h:

@@ -212,7 +212,7 @@ def main():
     props = torch.cuda.get_device_properties(torch.cuda.current_device())
     with open(args.out, "w") as f:
         f.write(f"# crava_b200 schedules: written by crava_b200/autotune.py on {props.name} "
-                f"({props.multi_processor_count} SMs), {datetime.datetime.utcnow():%Y-%m-%d %H:%M} UTC\n")
+                f"({props.multi_processor_count} SMs), {datetime.datetime.now(datetime.timezone.utc):%Y-%m-%d %H:%M} UTC\n")
         f.write("# key n value   (n: see crava_b200/autotune.py; -1 = every size)\n")
         for (k, n), v in sorted(entries.items()):
             f.write(f"{k} {n} {v}\n")

@@ -7,6 +7,7 @@
 //   AVOInversion::AVOInversion -> computePostMeanResidAndFFTCov -> simulate ->
 //   invFFTCovGrids (src/avoinversion.cpp:229-282).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <complex>
@@ -150,6 +151,10 @@ int tuned(const char* key, int n, int fallback) {
 enum { KT_X_R2C = 0, KT_LINE_FWD = 1, KT_ZPASS = 2, KT_LINE_INV = 3, KT_X_C2R = 4, KT_XY_FWD = 5, KT_XY_INV = 6,
        KT_THICK_DIVIDE = 7, KT_THICK_FILL = 8, KT_LOCAL_NOISE = 9, KT_FACIES = 10, KT_FILL_PRIOR = 11,
        KT_COUNT = 12 };
+// NVTX range names of the kernel classes (one range per pass, visible in Nsight Systems)
+const char* const kKtName[KT_COUNT] = {"x_r2c",        "line_fwd",   "pencil",      "line_inv",
+                                       "x_c2r",        "xy_fwd",     "xy_inv",      "thick_divide",
+                                       "thick_fill",   "local_noise", "facies",     "fill_prior"};
 
 struct ProfRec {
   int cat;
@@ -200,6 +205,7 @@ struct crava_ctx {
   std::map<int, Plan> plans;
   bool profiling = false;
   std::vector<ProfRec> prof;
+  int fail_allocs = 0;   // crava_ctx_fail_next_allocs: job allocations still to fail
   double kt_ms[KT_COUNT] = {};
   long long kt_n[KT_COUNT] = {};
   std::mutex stage_mu;         // device staging grid of the host-grid transforms
@@ -228,9 +234,11 @@ struct ProfScope {
   cudaStream_t st;
   cudaEvent_t a = nullptr;
   ProfScope(crava_ctx* c, int k, cudaStream_t s) : ctx(c), cat(k), st(s) {
+    nvtxRangePushA(kKtName[k]);
     if (ctx->profiling && cudaEventCreate(&a) == cudaSuccess) cudaEventRecord(a, st);
   }
   ~ProfScope() {
+    nvtxRangePop();
     if (!a) return;
     cudaEvent_t b;
     if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
@@ -1046,6 +1054,8 @@ const char* crava_status_string(crava_status s) {
     case CRAVA_ENUMERIC: return "numeric error";
     case CRAVA_ENOTSUP: return "not supported";
     case CRAVA_ESTATE: return "call out of order";
+    case CRAVA_EBUSY: return "queue full";
+    case CRAVA_ECANCELED: return "cancelled";
   }
   return "unknown status";
 }
@@ -2131,7 +2141,16 @@ crava_status job_create_impl(crava_ctx* ctx, const crava_job_desc* desc, cudaStr
   j->async = async;
   j->alloc_stream = st;
   j->pool_bytes = need;
-  cudaError_t e = async ? cudaMallocAsync((void**)&j->pool, need, st) : cudaMalloc(&j->pool, need);
+  bool injected = false;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->fail_allocs > 0) {
+      ctx->fail_allocs--;
+      injected = true;
+    }
+  }
+  cudaError_t e = injected ? cudaErrorMemoryAllocation
+                           : async ? cudaMallocAsync((void**)&j->pool, need, st) : cudaMalloc(&j->pool, need);
   if (e != cudaSuccess) {
     cudaGetLastError();
     j->pool = nullptr;
@@ -3395,6 +3414,7 @@ struct crava_server {
   bool stopping = false;
   uint64_t next_id = 1;
   std::deque<ServeReq*> pending;
+  int max_queued = 0;                 // 0: no limit
   std::vector<ServeReq*> inflight;
   std::map<uint64_t, ServeReq*> reqs;
   long long completed = 0;
@@ -3619,11 +3639,47 @@ crava_status crava_serve_submit(crava_server* sv, const crava_job_desc* desc, co
     delete r;
     return fail(CRAVA_ESTATE, "server is stopping");
   }
+  if (sv->max_queued > 0 && (int)sv->pending.size() >= sv->max_queued) {
+    delete r;
+    return fail(CRAVA_EBUSY, "server queue holds " + std::to_string(sv->max_queued) + " requests");
+  }
   r->id = sv->next_id++;
   r->t_submit = now_ms();
   sv->reqs[r->id] = r;
   sv->pending.push_back(r);
   *ticket = r->id;
+  sv->cv.notify_all();
+  return CRAVA_OK;
+}
+
+crava_status crava_ctx_fail_next_allocs(crava_ctx* ctx, int n) {
+  if (!ctx || n < 0) return fail(CRAVA_EINVAL, "bad argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->fail_allocs = n;
+  return CRAVA_OK;
+}
+
+crava_status crava_serve_set_queue_limit(crava_server* sv, int max_queued) {
+  if (!sv || max_queued < 0) return fail(CRAVA_EINVAL, "bad argument");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->max_queued = max_queued;
+  return CRAVA_OK;
+}
+
+crava_status crava_serve_cancel(crava_server* sv, uint64_t ticket) {
+  if (!sv) return fail(CRAVA_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return fail(CRAVA_EINVAL, "unknown ticket (or its final state was already reported)");
+  ServeReq* r = it->second;
+  auto q = std::find(sv->pending.begin(), sv->pending.end(), r);
+  if (r->state != CRAVA_REQ_QUEUED || q == sv->pending.end())
+    return fail(CRAVA_ESTATE, "the request is no longer queued");
+  sv->pending.erase(q);
+  r->state = CRAVA_REQ_FAILED;
+  r->status = CRAVA_ECANCELED;
+  r->err = "request cancelled";
+  r->t_done = now_ms();
   sv->cv.notify_all();
   return CRAVA_OK;
 }

@@ -37,7 +37,9 @@ typedef enum {
                            (at crava_job_create) or in the data / prior-mean grids (reported
                            by crava_job_counters after the run)                     */
   CRAVA_ENOTSUP = 6,    /* size or configuration outside what the kernels handle   */
-  CRAVA_ESTATE = 7      /* call out of order (e.g. download before run)            */
+  CRAVA_ESTATE = 7,     /* call out of order (e.g. download before run)            */
+  CRAVA_EBUSY = 8,      /* the server's queue is at its limit: submit again later  */
+  CRAVA_ECANCELED = 9   /* the request was cancelled before it started             */
 } crava_status;
 
 typedef struct crava_ctx crava_ctx;
@@ -477,6 +479,17 @@ crava_status crava_serve_poll(crava_server* sv, uint64_t ticket, crava_request_i
 crava_status crava_serve_wait(crava_server* sv, uint64_t ticket, double timeout_ms, crava_request_info* info);
 /* Finishes the running requests, fails the queued ones, joins the loop thread. */
 crava_status crava_serve_stop(crava_server* sv);
+/* At most max_queued requests wait for admission (0 = no limit, the default); a submit beyond
+ * it returns CRAVA_EBUSY and queues nothing. */
+crava_status crava_serve_set_queue_limit(crava_server* sv, int max_queued);
+/* Removes a request that is still queued: it fails with CRAVA_ECANCELED (poll and wait report
+ * that once).  A request already admitted runs to completion: CRAVA_ESTATE. */
+crava_status crava_serve_cancel(crava_server* sv, uint64_t ticket);
+
+/* Fault injection for callers' recovery paths (no counterpart in the reference): the next n
+ * device allocations of jobs created in ctx (crava_job_create, the served jobs) fail as if
+ * the device were out of memory (CRAVA_ENOMEM); nothing reaches the GPU. */
+crava_status crava_ctx_fail_next_allocs(crava_ctx* ctx, int n);
 
 /* One block, end to end, with no device allocation (no counterpart in the reference).
  *

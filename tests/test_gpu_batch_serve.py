@@ -181,3 +181,63 @@ def test_table_cache_hits_and_results_unchanged(blocks, alone):
     st = c.table_cache_stats()
     assert st["hits"] >= 2 * len(blocks) and st["entries"] >= len(blocks)
     c.close()
+
+
+def test_served_queue_limit_and_cancel(ctx, blocks):
+    """With one request running, a queue limit of 2 refuses the third waiting request with
+    EBUSY (nothing queued); a queued request can be cancelled (it fails with ECANCELED, reported
+    once), a running one cannot (ESTATE); the others complete."""
+    import time
+    sv = api.Server(ctx, max_inflight=1)
+    sv.set_queue_limit(2)
+    big = synth.make_block_fast(synth.BlockSpec(nx=256, ny=256, nz=128, nsim=16, seed=5))
+    bi, bo = _host_buffers(big, big.nsim)
+    t0 = sv.submit(big, bi, bo, seed=1)
+    deadline = time.time() + 60
+    while sv.poll(t0)["state"] == api.REQ_QUEUED and time.time() < deadline:
+        time.sleep(0.0005)
+    b = blocks[0]
+    bufs = [_host_buffers(b, b.nsim) for _ in range(3)]
+    t1 = sv.submit(b, *bufs[0], seed=2)
+    t2 = sv.submit(b, *bufs[1], seed=3)
+    with pytest.raises(api.CravaError) as e:
+        sv.submit(b, *bufs[2], seed=4)
+    assert e.value.status == api.EBUSY
+    sv.cancel(t2)
+    info = sv.poll(t2)
+    assert info["state"] == api.REQ_FAILED and info["status"] == api.ECANCELED
+    with pytest.raises(api.CravaError) as e:
+        sv.poll(t2)                      # the final state was reported once
+    assert e.value.status == api.EINVAL
+    with pytest.raises(api.CravaError) as e:
+        sv.cancel(t0)
+    assert e.value.status == api.ESTATE
+    assert sv.wait(t0, timeout_ms=120000)["state"] == api.REQ_DONE
+    assert sv.wait(t1, timeout_ms=120000)["state"] == api.REQ_DONE
+    sv.stop()
+
+
+def test_injected_allocation_failures(blocks):
+    """crava_ctx_fail_next_allocs: the next job creation fails with ENOMEM and the one after it
+    succeeds; a served request whose allocation fails with nothing in flight fails with ENOMEM
+    and the request behind it completes with the same result as alone."""
+    c = api.Context(0)
+    b = blocks[0]
+    c.fail_next_allocs(1)
+    with pytest.raises(api.CravaError) as e:
+        api.Job(c, b, api.PRIOR_SEPARABLE, 0, seed=1)
+    assert e.value.status == api.ENOMEM
+    j = api.Job(c, b, api.PRIOR_SEPARABLE, 0, seed=1)
+    j.close()
+    sv = api.Server(c, max_inflight=1)
+    c.fail_next_allocs(1)
+    bi, bo = _host_buffers(b, b.nsim)
+    t_bad = sv.submit(b, bi, bo, seed=1)
+    with pytest.raises(api.CravaError) as e:
+        sv.wait(t_bad, timeout_ms=120000)
+    assert e.value.status == api.ENOMEM
+    gi, go = _host_buffers(b, b.nsim)
+    t_ok = sv.submit(b, gi, go, seed=1)
+    assert sv.wait(t_ok, timeout_ms=120000)["state"] == api.REQ_DONE
+    sv.stop()
+    c.close()
