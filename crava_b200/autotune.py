@@ -9,7 +9,8 @@ fastest value.  The keys swept, with their size key n:
 
   pencil_kernel  n = nzp*16 + ntheta   1 general kernel (zpass.cu), 2 eigen form (pencil.cu)
   pencil_w       n = nzp*16 + ntheta   eigen form: x-bins per tile (power of two)
-  pencil_sb      n = nzp*16 + ntheta   eigen form: realisations per transform batch
+  pencil_sb      n = nzp*16 + ntheta   eigen form: realisations per transform batch (0: no
+                                       realisation slots, the mean stored first)
   pencil_threads n = nzp*16 + ntheta   eigen form: threads per CTA
   pencil_dense   n = nzp*16 + ntheta   eigen form: 1 = the 80-register instantiation
   pencil_nb      n = nzp*16 + ntheta   eigen form: bins of one z position per thread (1 or 2)
@@ -121,7 +122,7 @@ def tune_workload(name, w, reps, entries, log):
     if nzp in (128, 256, 320):
         api.tuning_set("pencil_kernel", pk, 2)
         sweep(ctx, job, stream, reps, "pencil_w", pk, [1, 2, 4, 8], ["zpass"], log)
-        sweep(ctx, job, stream, reps, "pencil_sb", pk, [1, 2, 4], ["zpass"], log)
+        sweep(ctx, job, stream, reps, "pencil_sb", pk, [0, 1, 2, 4], ["zpass"], log)
         eig_best = sweep(ctx, job, stream, reps, "pencil_threads", pk, [64, 128, 256, 384, 512], ["zpass"], log)
         # the tile width again, now with the realisation batch and threads chosen
         sweep(ctx, job, stream, reps, "pencil_w", pk, [2, 4, 8], ["zpass"], log)

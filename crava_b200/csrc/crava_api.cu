@@ -2537,7 +2537,10 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     // pencil_threads); by default two CTAs per SM where the tile's shared memory allows
     int Wp = 1;
     while (Wp * 2 <= std::min(16, tuned("pencil_w", skey, 4))) Wp *= 2;
-    int SBp = std::max(1, std::min(std::max(d.nsim, 1), tuned("pencil_sb", skey, 1)));
+    // realisations per transform batch; 0: no realisation slots (the mean is stored first and
+    // added back to each realisation), which lets wider tiles fit
+    int SBp = tuned("pencil_sb", skey, 1);
+    if (SBp != 0) SBp = std::max(1, std::min(std::max(d.nsim, 1), SBp));
     while (SBp > 1 && pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) > 227 * 1024) SBp--;
     while (Wp > 1 && pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) > 227 * 1024) Wp /= 2;
     if (pencil_smem_bytes(Wp, d.nzp, d.ntheta, SBp) > 227 * 1024)

@@ -10,7 +10,7 @@ size_t pencil_smem_bytes(int W, int nzp, int nth, int SB) {
 }
 
 cudaError_t launch_pencil(const ZParams& zp, int threads, cudaStream_t st, int* nlaunch) {
-  if ((zp.W & (zp.W - 1)) || (1 << zp.logW) != zp.W || !zp.eig || threads < 32 || threads > 512 || zp.SB < 1 ||
+  if ((zp.W & (zp.W - 1)) || (1 << zp.logW) != zp.W || !zp.eig || threads < 32 || threads > 512 || zp.SB < 0 ||
       zp.SB > kMaxSim || zp.nth < 1 || zp.nth > kMaxTheta)
     return cudaErrorInvalidValue;
   if (nlaunch) (*nlaunch)++;

@@ -410,10 +410,57 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
   }
   __syncthreads();
 
+  // ---- SB = 0: no realisation slots.  The posterior mean (slots 6..8) is transformed and
+  //      stored first; each realisation's L z then goes through those slots and the stored mean
+  //      is added in the last pass (IFFT(mu + L z) = IFFT(mu) + IFFT(L z)); the covariance last.
+  //      The tile needs G slots instead of G + 3, so wider tiles fit at the longer z lengths.
+  if (SB == 0) {
+    zinv_store<N1, N2>(R + 6 * W, 3 * W, G * W, tw, [&](int l, int k, float2 v) {
+      const int w = l & (W - 1);
+      if (w < nw) P.mean[l >> lw][base + (size_t)k * kstride + w] = v;
+    });
+#pragma unroll 1
+    for (int s = 0; s < P.nsim; s++) {
+      for (int b = tid; b < TS; b += T) {
+        const int p = b >> lw, w = b & (W - 1);
+        const float2* slot = R + p * G * W + w;
+        float2* o3 = R + (p * G + 6) * W + w;
+        float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        const float2 l0 = slot[0];
+        if (w < nw && l0.y == -1.f) {
+          const int kz = p / N2 + N1 * (p % N2);
+          float2 z[3];
+          if (P.host_noise) {
+            const size_t gidx = base + (size_t)kz * kstride + w;
+#pragma unroll
+            for (int c = 0; c < 3; c++) z[c] = P.noise[3 * s + c][gidx];
+          } else {
+            device_noise3(P.seed, s, i0 + w, j, kz, P.nyp, NZ, P.cnxp, P.nxp_even, z);
+          }
+          const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
+          sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
+          sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
+          sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
+        }
+        o3[0] = sd[0];
+        o3[W] = sd[1];
+        o3[2 * W] = sd[2];
+      }
+      __syncthreads();
+      // the mean this CTA stored above (visible after the barriers), read at L2
+      zinv_store<N1, N2>(R + 6 * W, 3 * W, G * W, tw, [&](int l, int k, float2 v) {
+        const int w = l & (W - 1);
+        if (w < nw) {
+          const size_t idx = base + (size_t)k * kstride + w;
+          P.sim[3 * s + (l >> lw)][idx] = cadd(__ldcg(P.mean[l >> lw] + idx), v);
+        }
+      });
+    }
+  }
   // ---- realisations (src/avoinversion.cpp:1401-1511), the mean added in the spectral
   //      domain; SB realisations per batch share one transform call
 #pragma unroll 1
-  for (int s0 = 0; s0 < P.nsim; s0 += SB) {
+  for (int s0 = 0; SB > 0 && s0 < P.nsim; s0 += SB) {
     const int nb = min(SB, P.nsim - s0);
     const int SG = 3 * SB;   // slot stride of S3
     for (int b = tid; b < TS; b += T) {
@@ -480,14 +527,16 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
   // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
   //      and mean (6..8); spectral covariance slots stay in position order
   if (!P.cov_spectral) {
-    // slots 0..5 to cov[0..5], 6..8 to mean[0..2], stored by the last pass
-    zinv_store<N1, N2>(R, 9 * W, G * W, tw, [&](int l, int k, float2 v) {
+    // slots 0..5 to cov[0..5], 6..8 to mean[0..2] (already stored when SB = 0), stored by the
+    // last pass
+    zinv_store<N1, N2>(R, (SB == 0 ? 6 : 9) * W, G * W, tw, [&](int l, int k, float2 v) {
       const int g = l >> lw, w = l & (W - 1);
       if (w < nw) (g < 6 ? P.cov[g] : P.mean[g - 6])[base + (size_t)k * kstride + w] = v;
     });
   } else {
-    // spectral covariance: slots 0..5 stay in position order, stored at their kz
-    zinv_inplace<N1, N2>(R + 6 * W, 3 * W, G * W, tw);
+    // spectral covariance: slots 0..5 stay in position order, stored at their kz (the mean,
+    // slots 6..8, is already stored when SB = 0)
+    if (SB > 0) zinv_inplace<N1, N2>(R + 6 * W, 3 * W, G * W, tw);
     for (int e = tid; e < TS; e += T) {
       const int w = e & (W - 1), k = e >> lw;
       if (w >= nw) continue;
@@ -496,8 +545,10 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
       const int kz = k / N2 + N1 * (k % N2);
 #pragma unroll
       for (int g = 0; g < 6; g++) P.cov[g][base + (size_t)kz * kstride + w] = R[so + g * W];
+      if (SB > 0) {
 #pragma unroll
-      for (int a = 0; a < 3; a++) P.mean[a][go] = R[so + (6 + a) * W];
+        for (int a = 0; a < 3; a++) P.mean[a][go] = R[so + (6 + a) * W];
+      }
     }
   }
 

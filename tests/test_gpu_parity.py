@@ -237,8 +237,8 @@ def _production_block(nx, ny):
     return synth.make_block(spec)
 
 
-@pytest.mark.parametrize("lateral", [(540, 12), (12, 540)])
-def test_production_instantiation_against_fp64_oracle(ctx, lateral):
+@pytest.mark.parametrize("lateral,sb", [((540, 12), None), ((12, 540), None), ((540, 12), 0)])
+def test_production_instantiation_against_fp64_oracle(ctx, lateral, sb):
     """Same pencil-pass instantiation as the full 540x540x256 block (5 angle stacks, nzp 256
     through the 16x16 four-step z split, 4 realisations) and the 540-point row (x) or column
     (y) transforms, with the reference RandomGen noise (parity mode): posterior mean 1e-4,
@@ -253,7 +253,16 @@ def test_production_instantiation_against_fp64_oracle(ctx, lateral):
     blk = _production_block(*lateral)
     post = ref64.posterior(blk)
     noise = ob.sim_noise(17, blk.nsim, blk.nxp, blk.nyp, blk.nzp)
-    out = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=noise, keep_residual=True)
+    # sb = 0: the pencil pass without realisation slots (the mean stored first and added back
+    # to every realisation)
+    pk = api.pencil_key(blk.nzp, blk.ntheta)
+    saved = api.tuning_get("pencil_sb", pk)
+    if sb is not None:
+        api.tuning_set("pencil_sb", pk, sb)
+    try:
+        out = api.invert_block(ctx, blk, api.PRIOR_SEPARABLE, noise=noise, keep_residual=True)
+    finally:
+        api.tuning_set("pencil_sb", pk, saved)
     _check_posterior(blk, out, post, post.n_inverted)
     if ob.ref32_available():
         covs, _ = ref64.prior_cov_grids(blk)

@@ -43,3 +43,24 @@ def test_schedule_forms_give_identical_results(ctx, sched):
     other = outputs(ctx, blk, sched)
     for key in ("mean", "cov", "sims"):
         assert np.array_equal(base[key], other[key]), key
+
+
+@pytest.mark.parametrize("dims", [(96, 40, 256), (64, 30, 320)])
+def test_pencil_without_realisation_slots(ctx, dims):
+    """pencil_sb = 0 (the eigen-form pencil pass storing the mean first and adding it back to each
+    realisation) against the default: the same mean and covariance bits, realisations equal to
+    FP32 rounding (IFFT(mu) + IFFT(L z) against IFFT(mu + L z)); at nzp 320 with 6 angles it is the
+    form that fits 8-bin tiles."""
+    nx, ny, nz = dims
+    nth = 5 if nz == 256 else 6
+    spec = synth.BlockSpec(nx=nx, ny=ny, nz=nz, nsim=3, seed=11, theta_deg=tuple(np.linspace(5.0, 45.0, nth)),
+                           peak_hz=(30.0,) * nth, sn=(5.0,) * nth)
+    blk = synth.make_block_fast(spec)
+    pk = api.pencil_key(blk.nzp, blk.ntheta)
+    base = outputs(ctx, blk, {("pencil_kernel", pk): 2, ("pencil_sb", pk): 1, ("pencil_w", pk): 4})
+    other = outputs(ctx, blk, {("pencil_kernel", pk): 2, ("pencil_sb", pk): 0, ("pencil_w", pk): 4})
+    wide = outputs(ctx, blk, {("pencil_kernel", pk): 2, ("pencil_sb", pk): 0, ("pencil_w", pk): 8})
+    for o in (other, wide):
+        assert np.array_equal(base["mean"], o["mean"]) and np.array_equal(base["cov"], o["cov"])
+        d = np.linalg.norm((o["sims"] - base["sims"]).astype(np.float64)) / np.linalg.norm(base["sims"])
+        assert d < 1e-6, d
