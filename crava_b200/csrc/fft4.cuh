@@ -564,8 +564,11 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   // the inverse rows up to h = 270 are faster still at 64 (3.53 vs 3.66 ms at 540x540x256)
   const int T = std::max(64, std::min(256, tuned(fwd ? "x4_threads_fwd" : "x4_threads_inv", L::H,
                                                    (!fwd && L::H <= 270) ? 64 : 128) / 32 * 32));
-  int rpc = std::max(1, T / N1);   // pass 2 of k_xr2c4 keeps one item per thread
-  rpc = std::max(1, std::min(rpc, tuned(fwd ? "x4_rpc_fwd" : "x4_rpc_inv", L::H, rpc)));
+  // rows per CTA: pass 2 of k_xr2c4 keeps one item per thread (at most T / N1 rows); the
+  // inverse rows loop over their items, so their schedule entry may also raise it (up to 64)
+  int rpc = std::max(1, T / N1);
+  const int rq = tuned(fwd ? "x4_rpc_fwd" : "x4_rpc_inv", L::H, rpc);
+  rpc = fwd ? std::max(1, std::min(rpc, rq)) : std::max(1, std::min(64, rq));
   if (pipe4_enabled(L::H)) {
     const int nchunk = (rows + rpc - 1) / rpc;
     const size_t smem = sizeof(float2) * (2 * (size_t)L::H + 2 * (size_t)rpc * (L::H + 1) + (size_t)rpc * L::PITCH);
