@@ -184,8 +184,7 @@ def tune_workload(name, w, reps, entries, log):
                 entries[(skey, h)] = best[0]
                 entries[(key, h)] = best[1]
             if key.endswith("inv"):   # rows per CTA of the inverse rows, beyond threads / N1
-                t = api.tuning_get(key, h)
-                b = sweep(ctx, job, stream, reps, "x4_rpc_inv", h, sorted({max(1, t // 18), 4, 8, 12}), cls, log)
+                b = sweep(ctx, job, stream, reps, "x4_rpc_inv", h, [2, 4, 6, 8, 12], cls, log)
                 if b:
                     entries[("x4_rpc_inv", h)] = b[0]
             pkey = key.replace("threads", "pf")
