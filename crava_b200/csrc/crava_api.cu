@@ -627,9 +627,9 @@ int zsplit_of(int nzp) { return nzp == 256 ? 1 : nzp == 320 ? 2 : nzp == 128 ? 3
 int zsplit_n1(int zs) { return zs == 1 ? 16 : zs == 2 ? 20 : zs == 3 ? 16 : 0; }
 int zsplit_n2(int zs) { return zs == 1 ? 16 : zs == 2 ? 16 : zs == 3 ? 8 : 0; }
 
-// Eigen tables of a separable-prior job: bytes on the device (0 when no split applies).
+// Eigen tables of a separable-prior job: bytes on the device (0 for other priors).
 size_t eig_table_bytes(const crava_job_desc* d) {
-  if (d->prior_mode != CRAVA_PRIOR_SEPARABLE || !zsplit_of(d->nzp)) return 0;
+  if (d->prior_mode != CRAVA_PRIOR_SEPARABLE) return 0;
   return align256(sizeof(float) * (size_t)EigLayout(d->ntheta).floats * d->nzp);
 }
 
@@ -719,7 +719,9 @@ bool build_eig_tables(const crava_job_desc& d, const std::vector<float2>& kw, co
   n_inv_rows = 0;
   const int tri = n * (n + 1) / 2;
   for (int p = 0; p < nzp; p++) {
-    const int kz = p / N2 + N1 * (p % N2);
+    // the in-place four-step order of k_pencil at its lengths, natural kz order otherwise
+    // (k_zpass)
+    const int kz = zs ? p / N2 + N1 * (p % N2) : p;
     if (!inv[kz]) continue;
     n_inv_rows++;
     double row[4 * 96] = {};
@@ -1927,7 +1929,7 @@ crava_status kz_set_build(const crava_job_desc& d, const std::vector<double>& A,
   for (int kz = 0; kz < d.nzp; kz++) ct[kz] = make_float2((float)C[kz].real(), sym ? 0.f : (float)C[kz].imag());
   CUDA_TRY(up(k.ct, ct.data(), sizeof(float2) * d.nzp));
   // the eigen form of the per-bin posterior (pencil.cu) where it applies
-  if (!k.eig) k.eig_why = "z length without an in-place four-step split";
+  if (!k.eig) k.eig_why = "no separable prior";
   else if (!sym) k.eig_why = "circular temporal correlation not symmetric";
   else if (d.fp64_threshold > 0.f) k.eig_why = "FP64 re-factorisation requested";
   else {
@@ -2532,7 +2534,7 @@ crava_status crava_job_run(crava_job* job, void* stream) {
   zp.seed = d.seed;
   zp.counters = job->counters;
   int nl = 0;
-  if (job->eig_ok && tuned("pencil_kernel", skey, 2) == 2) {
+  if (job->eig_ok && zsplit_of(d.nzp) && tuned("pencil_kernel", skey, 2) == 2) {
     // eigen form: in-place z transforms, W x-bins per tile (schedule keys pencil_w,
     // pencil_threads); by default two CTAs per SM where the tile's shared memory allows
     int Wp = 1;
@@ -2562,6 +2564,12 @@ crava_status crava_job_run(crava_job* job, void* stream) {
     ProfScope ps(ctx, KT_ZPASS, st);
     CUDA_TRY(launch_pencil(zp, Tp, st, &nl));
   } else {
+    // the general kernel takes the eigen form of the per-bin step where its tables apply
+    // (natural kz order at the lengths without the in-place split; schedule key zpass_eig)
+    if (job->eig_ok && !zsplit_of(d.nzp) && tuned("zpass_eig", d.nzp, 1) != 0) {
+      zp.eig = job->eig;
+      zp.n_inv_rows = job->n_inv_rows;
+    }
     ProfScope ps(ctx, KT_ZPASS, st);
     CUDA_TRY(launch_zpass(zp, T, st, &nl));
   }

@@ -1,6 +1,7 @@
 // Device helpers shared by the two pencil-pass kernels (zpass.cu, pencil.cu): the
-// counter-based noise of product-mode realisations and the reference-semantics Cholesky
-// factorisation of small Hermitian matrices.
+// counter-based noise of product-mode realisations, the reference-semantics Cholesky
+// factorisation of small Hermitian matrices and the eigen-form per-bin posterior of a
+// separable prior (its derivation is in pencil.cuh).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -111,6 +112,119 @@ __device__ __forceinline__ bool chol_ref(float2 (&a)[N][N]) {
     a[i][i] = make_float2(r * rs, rs);
   }
   return true;
+}
+
+// ------------------------------------------------------------------ eigen-form per-bin step
+
+// Section of N floats (N % 4 == 0) of the row of position p: group g at e[g * stride].
+template <int N>
+__device__ __forceinline__ void ldrow(float (&out)[N], const float4* __restrict__ e, int stride) {
+#pragma unroll
+  for (int g = 0; g < N / 4; g++) {
+    const float4 v = __ldg(e + g * stride);
+    out[4 * g] = v.x;
+    out[4 * g + 1] = v.y;
+    out[4 * g + 2] = v.z;
+    out[4 * g + 3] = v.w;
+  }
+}
+
+constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
+
+// mu_post, S_post (order 00 11 22 01 02 12) and the residual (in d) of NB bins of one z
+// position from that position's row e (float4 groups at stride nzp), laid out as EigLayout:
+// the angles' rows are streamed one at a time and every row load serves all NB bins.
+template <int NTH, int NB>
+__device__ __forceinline__ void bin_posterior_eig(const ZParams& P, const float4* __restrict__ e,
+                                                  const float (&lam)[NB], const float (&rho)[NB],
+                                                  const float2 (&mu)[NB][3], float2 (&d)[NB][NTH],
+                                                  float2 (&mu_post)[NB][3], float2 (&sp)[NB][6]) {
+  constexpr int VP = pad4(2 * NTH), OKW = 0, OL = VP, OR = OL + pad4(NTH), RS = VP + 16;
+  const int st = P.nzp;
+  float kw[VP];
+  ldrow(kw, e + (OKW / 4) * st, st);
+  float Lm[pad4(NTH)];
+  ldrow(Lm, e + (OL / 4) * st, st);
+  // y = d - K mu, K = diag(kw) A
+  float2 y[NB][NTH];
+#pragma unroll
+  for (int b = 0; b < NB; b++)
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+      float2 am = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        am = make_float2(am.x + P.A[l][a] * mu[b][a].x, am.y + P.A[l][a] * mu[b][a].y);
+      y[b][l] = csub(d[b][l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
+    }
+  float2 mp[NB][3];
+  float s00[NB], s11[NB], s22[NB];
+  float2 s01[NB], s02[NB], s12[NB];
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) mp[b][a] = mu[b][a];
+    s00[b] = rho[b] * P.pv[0];
+    s11[b] = rho[b] * P.pv[1];
+    s22[b] = rho[b] * P.pv[2];
+    s01[b] = make_float2(rho[b] * P.pv[3], 0.f);
+    s02[b] = make_float2(rho[b] * P.pv[4], 0.f);
+    s12[b] = make_float2(rho[b] * P.pv[5], 0.f);
+  }
+#pragma unroll
+  for (int l = 0; l < NTH; l++) {
+    // r_l = (V y)_l, s_l = r_l lam / (lam Lam_l + 1), w_l = lam^2 / (lam Lam_l + 1)
+    float V[VP];
+    ldrow(V, e + ((OR + l * RS) / 4) * st, st);
+    float QH[16];
+    ldrow(QH, e + ((OR + l * RS + VP) / 4) * st, st);
+    const float* h = QH + 6;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      float2 r = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int m = 0; m < NTH; m++) r = cadd(r, cmul(make_float2(V[2 * m], V[2 * m + 1]), y[b][m]));
+      const float inv = __frcp_rn(fmaf(lam[b], Lm[l], 1.0f));
+      const float f = lam[b] * inv;
+      const float2 sl = make_float2(r.x * f, r.y * f);
+      const float wl = lam[b] * f;
+      // mu_post += conj(Q_l.) s_l;  S_post -= w_l H_l, H_l = (|Q_l0|^2, |Q_l1|^2, |Q_l2|^2,
+      // conj(Q_l0) Q_l1, conj(Q_l0) Q_l2, conj(Q_l1) Q_l2)
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        const float qr = QH[2 * a], qi = QH[2 * a + 1];
+        mp[b][a].x += qr * sl.x + qi * sl.y;
+        mp[b][a].y += qr * sl.y - qi * sl.x;
+      }
+      s00[b] -= wl * h[0];
+      s11[b] -= wl * h[1];
+      s22[b] -= wl * h[2];
+      s01[b] = make_float2(s01[b].x - wl * h[3], s01[b].y - wl * h[4]);
+      s02[b] = make_float2(s02[b].x - wl * h[5], s02[b].y - wl * h[6]);
+      s12[b] = make_float2(s12[b].x - wl * h[7], s12[b].y - wl * h[8]);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) mu_post[b][a] = mp[b][a];
+    sp[b][0] = make_float2(s00[b], 0.f);
+    sp[b][1] = make_float2(s11[b], 0.f);
+    sp[b][2] = make_float2(s22[b], 0.f);
+    sp[b][3] = s01[b];
+    sp[b][4] = s02[b];
+    sp[b][5] = s12[b];
+    // residual d - K mu_post = y - K (mu_post - mu) (the data spectrum itself where the row
+    // is zero: kz not inverted)
+#pragma unroll
+    for (int l = 0; l < NTH; l++) {
+      float2 am = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        am = make_float2(am.x + P.A[l][a] * (mp[b][a].x - mu[b][a].x), am.y + P.A[l][a] * (mp[b][a].y - mu[b][a].y));
+      d[b][l] = csub(y[b][l], cmul(make_float2(kw[2 * l], kw[2 * l + 1]), am));
+    }
+  }
 }
 
 }  // namespace crava

@@ -496,7 +496,26 @@ __global__ void __launch_bounds__(512) k_zpass(const __grid_constant__ ZParams P
     BinOut o;
     bool inv = P.kz.inv[k] != 0;
     bool ok = false;
-    if (inv) {
+    if (!REFINE && P.eig) {
+      // separable prior with a real temporal spectrum: the eigen form of the per-bin step
+      // (bin_posterior_eig, tables in natural kz order), which never needs a fallback (the
+      // host bounds the lateral factor against the reference's pivot test before choosing it)
+      const float lam1[1] = {lam}, rho1[1] = {rho};
+      float2 mu1[1][3], d1[1][NTH], mp1[1][3], sp1[1][6];
+#pragma unroll
+      for (int a = 0; a < 3; a++) mu1[0][a] = mu[a];
+#pragma unroll
+      for (int l = 0; l < NTH; l++) d1[0][l] = d[l];
+      bin_posterior_eig<NTH, 1>(P, P.eig + k, lam1, rho1, mu1, d1, mp1, sp1);
+#pragma unroll
+      for (int a = 0; a < 3; a++) o.mu[a] = mp1[0][a];
+#pragma unroll
+      for (int q = 0; q < 6; q++) o.sp[q] = sp1[0][q];
+#pragma unroll
+      for (int l = 0; l < NTH; l++) d[l] = d1[0][l];
+      if (inv) n_inv++;
+      ok = true;
+    } else if (inv) {
       n_inv++;
       ok = P.septab ? bin_posterior<NTH, true>(P, k, S, lam, rho, mu, d, o)
                     : bin_posterior<NTH, false>(P, k, S, lam, rho, mu, d, o);
