@@ -176,34 +176,34 @@ __device__ __forceinline__ void xc2r4_staged(const float2* Xs, float2* g, int nr
                                              const float2* twh, float2* Z, float2* Vc = nullptr) {
   using L = RowLayout<N1, N2>;
   constexpr int H = L::H, PITCH = L::PITCH;
-  constexpr int CN = H + 1, NP = H / 2 + 1;
+  constexpr int CN = H + 1;
   const int T = blockDim.x, tid = threadIdx.x;
-  for (int e = tid; e < nr * NP; e += T) {
-    const int r = e / NP, k = e - r * NP;
-    const float2* X = Xs + r * CN;
-    float2* z = Z + r * PITCH;
-    if (k == 0) {
-      const float a = X[0].x, b = X[H].x;
-      z[0] = make_float2(a + b, a - b);
-      continue;
-    }
-    const float2 xk = X[k], xm = X[H - k];
-    const float2 P = make_float2(xk.x + xm.x, xk.y - xm.y);
-    const float2 M = make_float2(xk.x - xm.x, xk.y + xm.y);
-    const float2 w = twh[k];
-    const float2 Q = make_float2(M.x * w.x + M.y * w.y, M.y * w.x - M.x * w.y);
-    z[L::pad(k % N2, k / N2)] = make_float2(P.x - Q.y, P.y + Q.x);
-    if (2 * k != H) {
-      const int kk = H - k;
-      z[L::pad(kk % N2, kk / N2)] = make_float2(P.x + Q.y, -P.y + Q.x);
-    }
-  }
-  __syncthreads();
+  // pass 1 reads the half-length sequence z straight from the staged half spectrum: the merge
+  // z[k] = (X[k] + conj X[h-k]) + i w^k (X[k] - conj X[h-k]) (w = e^{2 pi i / nxp}) computed
+  // where pass 1 loads it, each z[k] with the operations of its pair's lower index k0 <= h/2
+  // (z[h - k0] is the mirrored combination of the same terms)
   for (int q = tid; q < nr * N2; q += T) {
     const int r = q / N2, t = q - r * N2;
+    const float2* X = Xs + r * CN;
     float2* z = Z + r * PITCH;
     four_step_pass1<N1, N2, 1>(
-        t, tw, [&](int, int m) { return z[L::pad(t, m)]; }, [&](int, int k2, float2 v) { z[L::pad(t, k2)] = v; });
+        t, tw,
+        [&](int, int m) {
+          const int k = t + N2 * m;
+          if (k == 0) {
+            const float a = X[0].x, b = X[H].x;
+            return make_float2(a + b, a - b);
+          }
+          const bool lo = 2 * k <= H;
+          const int k0 = lo ? k : H - k;
+          const float2 xk = X[k0], xm = X[H - k0];
+          const float2 P = make_float2(xk.x + xm.x, xk.y - xm.y);
+          const float2 M = make_float2(xk.x - xm.x, xk.y + xm.y);
+          const float2 w = twh[k0];
+          const float2 Q = make_float2(M.x * w.x + M.y * w.y, M.y * w.x - M.x * w.y);
+          return lo ? make_float2(P.x - Q.y, P.y + Q.x) : make_float2(P.x + Q.y, -P.y + Q.x);
+        },
+        [&](int, int k2, float2 v) { z[L::pad(t, k2)] = v; });
   }
   __syncthreads();
   for (int q = tid; q < nr * N1; q += T) {
