@@ -190,6 +190,23 @@ __device__ __forceinline__ int store_bin(const ZParams& P, float2* slot, int W, 
   return zero;
 }
 
+// S_post = L L^H of a bin whose slots 0..5 hold its realisation factor (written back there).
+// The products and sums are spelled out as explicit fused multiply-adds so that every call site
+// rounds them alike (the two realisation forms call it from different code).
+__device__ __forceinline__ void store_llh(float2* slot, int W, float2 l0, float2 l1, float2 l2, float2 l10,
+                                          float2 l20, float2 l21) {
+  slot[0] = make_float2(__fmul_rn(l0.x, l0.x), 0.f);
+  slot[W] = make_float2(__fmaf_rn(l10.x, l10.x, __fmaf_rn(l10.y, l10.y, __fmul_rn(l1.x, l1.x))), 0.f);
+  slot[2 * W] = make_float2(
+      __fmaf_rn(l20.x, l20.x,
+                __fmaf_rn(l20.y, l20.y, __fmaf_rn(l21.x, l21.x, __fmaf_rn(l21.y, l21.y, __fmul_rn(l2.x, l2.x))))),
+      0.f);
+  slot[3 * W] = make_float2(__fmul_rn(l0.x, l10.x), -__fmul_rn(l0.x, l10.y));
+  slot[4 * W] = make_float2(__fmul_rn(l0.x, l20.x), -__fmul_rn(l0.x, l20.y));
+  slot[5 * W] = make_float2(__fmaf_rn(l10.x, l20.x, __fmaf_rn(l10.y, l20.y, __fmul_rn(l1.x, l21.x))),
+                            __fmaf_rn(l10.y, l20.x, __fmaf_rn(-l10.x, l20.y, -__fmul_rn(l1.x, l21.y))));
+}
+
 // ------------------------------------------------------------------ the kernel
 
 // Shared-memory layout of one tile (W consecutive x-bins at one y, all NZ = N1 N2 positions):
@@ -330,6 +347,8 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
           sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
           sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
           sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
+          // the last realisation leaves S_post in slots 0..5 for the covariance output
+          if (s == P.nsim - 1) store_llh(R + p * G * W + w, W, l0, l1, l2, l10, l20, l21);
         }
         o3[0] = sd[0];
         o3[W] = sd[1];
@@ -364,11 +383,16 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
       const float2* slot = R + p * G * W + w;
       const float2 l0 = slot[0];
       const float2 m0 = slot[6 * W], m1 = slot[7 * W], m2 = slot[8 * W];
+      const bool fac = l0.y == -1.f;
+      float2 l1 = make_float2(0.f, 0.f), l2 = l1, l10 = l1, l20 = l1, l21 = l1;
+      if (fac) {
+        l1 = slot[W]; l2 = slot[2 * W]; l10 = slot[3 * W]; l20 = slot[4 * W]; l21 = slot[5 * W];
+      }
 #pragma unroll 1
       for (int sb = 0; sb < nb; sb++) {
         const int s = s0 + sb;
         float2 sd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        if (l0.y == -1.f) {
+        if (fac) {
           float2 z[3];
           if (P.host_noise) {
             const size_t gidx = base + (size_t)kz * kstride + w;
@@ -377,7 +401,6 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
           } else {
             device_noise3(P.seed, s, i, j, kz, P.nyp, NZ, P.cnxp, P.nxp_even, z);
           }
-          const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
           sd[0] = make_float2(l0.x * z[0].x, l0.x * z[0].y);
           sd[1] = cadd(cmul(l10, z[0]), make_float2(l1.x * z[1].x, l1.x * z[1].y));
           sd[2] = cadd(cadd(cmul(l20, z[0]), cmul(l21, z[1])), make_float2(l2.x * z[2].x, l2.x * z[2].y));
@@ -386,6 +409,8 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
         o3[(3 * sb + 1) * W] = cadd(m1, sd[1]);
         o3[(3 * sb + 2) * W] = cadd(m2, sd[2]);
       }
+      // the last batch leaves S_post in slots 0..5 for the covariance output
+      if (fac && s0 + nb == P.nsim) store_llh(R + p * G * W + w, W, l0, l1, l2, l10, l20, l21);
     }
     __syncthreads();
     // inverse z transform, the last pass storing the realisations' spectra (line l: grid
@@ -395,24 +420,7 @@ __global__ void __launch_bounds__(DENSE ? 384 : 512, DENSE ? 2 : 1) k_pencil(con
       if (w < nw) P.sim[3 * s0 + (l >> lw)][base + (size_t)k * kstride + w] = v;
     });
   }
-  // ---- S_post = L L^H where slots 0..5 hold the factor
-  if (P.nsim > 0) {
-    for (int b = tid; b < TS; b += T) {
-      const int p = b >> lw, w = b & (W - 1);
-      float2* slot = R + p * G * W + w;
-      const float2 l0 = slot[0];
-      if (l0.y != -1.f) continue;
-      const float2 l1 = slot[W], l2 = slot[2 * W], l10 = slot[3 * W], l20 = slot[4 * W], l21 = slot[5 * W];
-      slot[0] = make_float2(l0.x * l0.x, 0.f);
-      slot[W] = make_float2(l10.x * l10.x + l10.y * l10.y + l1.x * l1.x, 0.f);
-      slot[2 * W] = make_float2(l20.x * l20.x + l20.y * l20.y + l21.x * l21.x + l21.y * l21.y + l2.x * l2.x, 0.f);
-      slot[3 * W] = make_float2(l0.x * l10.x, -l0.x * l10.y);
-      slot[4 * W] = make_float2(l0.x * l20.x, -l0.x * l20.y);
-      slot[5 * W] = make_float2(l10.x * l20.x + l10.y * l20.y + l1.x * l21.x,
-                                l10.y * l20.x - l10.x * l20.y - l1.x * l21.y);
-    }
-    __syncthreads();
-  }
+  // (S_post = L L^H is back in slots 0..5: the last realisation wrote it)
   // ---- inverse z transform of posterior covariance (slots 0..5, unless it stays spectral)
   //      and mean (6..8); spectral covariance slots stay in position order
   if (!P.cov_spectral) {
