@@ -23,7 +23,7 @@ fastest value.  The keys swept, with their size key n:
                                         shared memory, 0 = read from global memory (n = nxp/2)
   x4_threads_fwd, x4_threads_inv       four-step row transforms: threads per CTA
                  n = nxp/2
-  x4_rpc_inv     n = nxp/2             inverse rows per CTA (default threads / N1)
+  x4_rpc_fwd, x4_rpc_inv  n = nxp/2    rows per CTA (defaults threads / (N1/2 + 1), threads / N1)
   line4_pf_fwd, line4_pf_inv (n = N),  L2 prefetch of the tiles (rows) that many quarters of
   x4_pf_fwd, x4_pf_inv (n = nxp/2)     the resident CTAs ahead; 0 = off
 
@@ -183,10 +183,10 @@ def tune_workload(name, w, reps, entries, log):
                 api.tuning_set(key, h, best[1])
                 entries[(skey, h)] = best[0]
                 entries[(key, h)] = best[1]
-            if key.endswith("inv"):   # rows per CTA of the inverse rows, beyond threads / N1
-                b = sweep(ctx, job, stream, reps, "x4_rpc_inv", h, [2, 4, 6, 8, 12], cls, log)
-                if b:
-                    entries[("x4_rpc_inv", h)] = b[0]
+            rkey = key.replace("threads", "rpc")   # rows per CTA
+            b = sweep(ctx, job, stream, reps, rkey, h, [2, 4, 6, 8, 12], cls, log)
+            if b:
+                entries[(rkey, h)] = b[0]
             pkey = key.replace("threads", "pf")
             b = sweep(ctx, job, stream, reps, pkey, h, [0, 2, 4], cls, log)
             if b:

@@ -107,16 +107,18 @@ struct RowLayout {
   static __device__ __forceinline__ int pad(int t, int m) { return t + m * (N2 + SK); }
 };
 
-// nr (<= blockDim / N1) rows, even nxp: src rows (h complex values x[2m] + i x[2m+1] each,
-// row pitch h + 1) to the scaled half spectra in dst (may equal src).  The split step as
-// k_x_r2c (kernels.cu).  Needs tw (length h) and twh (e^{-2 pi i k / nxp}, k < h) in
-// shared memory; Z: rpc * PITCH.  Ends with a barrier.
+// nr rows, even nxp: src rows (h complex values x[2m] + i x[2m+1] each, row pitch h + 1) to
+// the scaled half spectra in dst (may equal src).  The split step as k_x_r2c (kernels.cu),
+// done in registers: output k = k2 + N1 k1 of pass-2 item k2 has its mirror h - k in item
+// (N1 - k2) mod N1, so one thread takes both items of a pair (k2 <= N1 / 2) and forms every
+// X[k], X[h-k] from the two DFTs it holds.  Needs tw (length h) and twh (e^{-2 pi i k / nxp},
+// k < h) in shared memory; Z: rpc * PITCH.  Ends with a barrier.
 template <int N1, int N2>
 __device__ __forceinline__ void xr2c4_rows(const float2* src, float2* dst, int nr, float scale, const float2* tw,
                                            const float2* twh, float2* Z) {
   using L = RowLayout<N1, N2>;
   constexpr int H = L::H, PITCH = L::PITCH;
-  constexpr int CN = H + 1, NP = H / 2 + 1;
+  constexpr int CN = H + 1, NPI = N1 / 2 + 1;
   const int T = blockDim.x, tid = threadIdx.x;
   for (int q = tid; q < nr * N2; q += T) {
     const int r = q / N2, t = q - r * N2;
@@ -126,42 +128,40 @@ __device__ __forceinline__ void xr2c4_rows(const float2* src, float2* dst, int n
         t, tw, [&](int, int m) { return x[m * N2]; }, [&](int, int k2, float2 v) { z[L::pad(t, k2)] = v; });
   }
   __syncthreads();
-  // pass 2: one item per thread (nr N1 <= T), outputs held across the barrier
-  float2 v[N2];
-  const int q = tid;
-  const bool have = q < nr * N1;
-  const int r2 = have ? q / N1 : 0, k2 = have ? q - r2 * N1 : 0;
-  if (have) {
-    const float2* z = Z + r2 * PITCH;
-    four_step_pass2<N1, N2, -1>(k2, [&](int k, int t) { return z[L::pad(t, k)]; }, v);
-  }
-  __syncthreads();
-  if (have) {
-    float2* z = Z + r2 * PITCH;
-#pragma unroll
-    for (int k1 = 0; k1 < N2; k1++) z[k2 + N1 * k1] = v[k1];
-  }
-  __syncthreads();
-  for (int e = tid; e < nr * NP; e += T) {
-    const int r = e / NP, k = e - r * NP;
-    const float2* Zr = Z + r * PITCH;
+  for (int q = tid; q < nr * NPI; q += T) {
+    const int r = q / NPI, a = q - r * NPI;        // item a and its mirror item b
+    const int b = a == 0 ? 0 : N1 - a;
+    const float2* z = Z + r * PITCH;
+    float2 va[N2], vb[N2];
+    four_step_pass2<N1, N2, -1>(a, [&](int k, int t) { return z[L::pad(t, k)]; }, va);
+    if (b != a) four_step_pass2<N1, N2, -1>(b, [&](int k, int t) { return z[L::pad(t, k)]; }, vb);
     float2* X = dst + (size_t)r * CN;
-    if (k == 0) {
-      const float2 z0 = Zr[0];
-      X[0] = make_float2(scale * (z0.x + z0.y), 0.f);
-      X[H] = make_float2(scale * (z0.x - z0.y), 0.f);
-      continue;
-    }
-    const float2 A = Zr[k], Bc = Zr[H - k];
-    const float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y - Bc.y));
-    const float2 D = make_float2(A.x - Bc.x, A.y + Bc.y);
-    const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-    const float2 tt = cmul(twh[k], O);
-    const float2 xk = cadd(E, tt);
-    X[k] = make_float2(scale * xk.x, scale * xk.y);
-    if (2 * k != H) {
-      const float2 m = csub(E, tt);
-      X[H - k] = make_float2(scale * m.x, -scale * m.y);
+#pragma unroll
+    for (int k1 = 0; k1 < N2; k1++) {
+      const int k = a + N1 * k1;
+      if (k == 0) {
+        const float2 z0 = va[0];
+        X[0] = make_float2(scale * (z0.x + z0.y), 0.f);
+        X[H] = make_float2(scale * (z0.x - z0.y), 0.f);
+        continue;
+      }
+      // z[h - k]: item b's output N2 - 1 - k1 (N2 - k1 for item 0, its own mirror)
+      const float2 zm = a == 0 ? va[N2 - k1] : (b != a ? vb[N2 - 1 - k1] : va[N2 - 1 - k1]);
+      if (b == a && 2 * k > H) continue;           // a self-mirrored item's upper half: done below
+      // the pair (k0, h - k0), k0 <= h/2, as the separate split loop forms it
+      const bool lo = 2 * k <= H;
+      const int k0 = lo ? k : H - k;
+      const float2 A = lo ? va[k1] : zm, Bc = lo ? zm : va[k1];
+      const float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y - Bc.y));
+      const float2 D = make_float2(A.x - Bc.x, A.y + Bc.y);
+      const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+      const float2 tt = cmul(twh[k0], O);
+      const float2 xk = cadd(E, tt);
+      X[k0] = make_float2(scale * xk.x, scale * xk.y);
+      if (2 * k0 != H) {
+        const float2 m = csub(E, tt);
+        X[H - k0] = make_float2(scale * m.x, -scale * m.y);
+      }
     }
   }
   __syncthreads();
@@ -564,11 +564,10 @@ static cudaError_t x4(bool fwd, const GridSet& gs, int rows, const float2* tw, c
   // the inverse rows up to h = 270 are faster still at 64 (3.53 vs 3.66 ms at 540x540x256)
   const int T = std::max(64, std::min(256, tuned(fwd ? "x4_threads_fwd" : "x4_threads_inv", L::H,
                                                    (!fwd && L::H <= 270) ? 64 : 128) / 32 * 32));
-  // rows per CTA: pass 2 of k_xr2c4 keeps one item per thread (at most T / N1 rows); the
-  // inverse rows loop over their items, so their schedule entry may also raise it (up to 64)
-  int rpc = std::max(1, T / N1);
-  const int rq = tuned(fwd ? "x4_rpc_fwd" : "x4_rpc_inv", L::H, rpc);
-  rpc = fwd ? std::max(1, std::min(rpc, rq)) : std::max(1, std::min(64, rq));
+  // rows per CTA: by default a whole number of pass-2 items per thread (N1 items per row
+  // inverse, N1 / 2 + 1 item pairs forward); the schedule entry may set up to 64
+  int rpc = std::max(1, fwd ? T / (N1 / 2 + 1) : T / N1);
+  rpc = std::max(1, std::min(64, tuned(fwd ? "x4_rpc_fwd" : "x4_rpc_inv", L::H, rpc)));
   if (pipe4_enabled(L::H)) {
     const int nchunk = (rows + rpc - 1) / rpc;
     const size_t smem = sizeof(float2) * (2 * (size_t)L::H + 2 * (size_t)rpc * (L::H + 1) + (size_t)rpc * L::PITCH);
