@@ -56,7 +56,7 @@ class Ref32Block(ctypes.Structure):
                 ("lz", ctypes.c_double), ("min_rel_thick", ctypes.c_double),
                 ("low_cut", ctypes.c_float), ("high_cut", ctypes.c_float), ("wnc", ctypes.c_float),
                 ("A", _dp), ("err_theta_cov", _dp), ("wavelet", _fp), ("wavelet_norm", _fp),
-                ("prior_var0", _dp)]
+                ("prior_var0", _dp), ("nonconst", ctypes.c_int)]
 
 
 def ref32_lib():
@@ -149,10 +149,11 @@ class Ref32Result:
         self.n_chol_fail = 0
 
 
-def ref32_invert(blk, cov_grids, err_corr, nsim=0, seed=0, noise=None) -> Ref32Result:
+def ref32_invert(blk, cov_grids, err_corr, nsim=0, seed=0, noise=None, nonconst=False) -> Ref32Result:
     """Run the reference's FP32 path on one block.  cov_grids: six (nzp,nyp,nxp) float32
     prior covariance grids; err_corr: (nzp,nyp,nxp) float32; noise: optional
-    (nsim,3,nzp,nyp,cnxp) complex64 replacing the RandomGen draws."""
+    (nsim,3,nzp,nyp,cnxp) complex64 replacing the RandomGen draws; nonconst: the
+    non-constant-thickness branch of the per-bin step on blk.data taken as already divided."""
     lib = ref32_lib()
     nxp, nyp, nzp, nth = blk.nxp, blk.nyp, blk.nzp, blk.ntheta
     rnxp = 2 * (nxp // 2 + 1)
@@ -173,7 +174,8 @@ def ref32_invert(blk, cov_grids, err_corr, nsim=0, seed=0, noise=None) -> Ref32R
     wn = np.ascontiguousarray(blk.wavelet_norm, dtype=np.float32)
     pv = np.ascontiguousarray(blk.prior_var0, dtype=np.float64)
     b = Ref32Block(blk.nx, blk.ny, blk.nz, nxp, nyp, nzp, nth, float(blk.lz), float(blk.min_rel_thick),
-                   float(blk.low_cut), float(blk.high_cut), float(blk.wnc), _d(A), _d(etc), _f(wav), _f(wn), _d(pv))
+                   float(blk.low_cut), float(blk.high_cut), float(blk.wnc), _d(A), _d(etc), _f(wav), _f(wn), _d(pv),
+                   int(bool(nonconst)))
     arr = lambda L: (_fp * len(L))(*[_f(x) for x in L]) if L else None
     cnt = (ctypes.c_longlong * 2)()
     nz_in = None

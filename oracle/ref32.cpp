@@ -106,6 +106,31 @@ struct Vec1D {
     else { v.re = c[nzp - k].re; v.im = -c[nzp - k].im; }
     return v;
   }
+  // Wavelet::getCAmp(k, scale) (src/wavelet.cpp:336-393): the stretched wavelet's spectrum by
+  // linear interpolation at k / scale, divided by scale
+  fftw_complex camp_scaled(int k, float scale) const {
+    const fftw_complex* c = reinterpret_cast<const fftw_complex*>(a.data());
+    fftw_complex value;
+    float omega, dOmega;
+    int omU, omL;
+    const bool lo = k < cnzp;
+    omega = float(lo ? k : nzp - k) / scale;
+    if (omega >= cnzp) {
+      value.re = 0.0f;
+      value.im = 0.0f;
+    } else {
+      omL = int(std::floor(omega));
+      omU = int(std::floor(omega)) + 1;
+      if (omU >= cnzp) omU -= 1;
+      dOmega = omega - float(omL);
+      value.re = c[omL].re * (1.0f - dOmega) + c[omU].re * dOmega;
+      value.im = lo ? (c[omL].im * (1.0f - dOmega) + c[omU].im * dOmega)
+                    : (-c[omL].im * (1.0f - dOmega) - c[omU].im * dOmega);
+    }
+    value.re /= scale;
+    value.im /= scale;
+    return value;
+  }
   // Wavelet::findNorm, real branch (src/wavelet.cpp:882-889)
   float find_norm() const {
     double n2 = 0.0;
@@ -189,6 +214,8 @@ typedef struct {
   const float* wavelet;         // ntheta x nzp, FFT order
   const float* wavelet_norm;    // ntheta
   const double* prior_var0;     // 3 x 3
+  int nonconst;                 // 1: the non-constant-thickness branch (K = kD A,
+                                // src/avoinversion.cpp:976-1014) on data already divided
 } ref32_block;
 
 // In-place 3D transforms with FFTGrid's scaling.
@@ -227,6 +254,9 @@ int ref32_invert(const ref32_block* b, float** mean, float** cov, float* errcorr
   Vec1D diff1(nzp);
   diff1.a[0] = -1.0f;
   diff1.a[nzp - 1] = 1.0f;
+  // diff3Operator: the backward then central difference of diff1's samples (:846-851)
+  Vec1D diff3 = diff_of(diff_of(diff1, BWD), CEN);
+  diff3.fft();
   diff1.fft();
   std::vector<Vec1D> w_seis, w_norm, es3;
   std::vector<float> norm_seis(nth), norm_es3(nth);
@@ -276,22 +306,52 @@ int ref32_invert(const ref32_block* b, float** mean, float** cov, float* errcorr
   for (int k = 0; k < nzp; k++) {
     float realFrequency = static_cast<float>((b->nz * 1000.0f) / (b->lz * nzp) * std::min(k, nzp - k));
     fftw_complex kD = diff1.camp(k);
-    for (int l = 0; l < nth; l++) {           // fillkW
-      fftw_complex c = w_seis[l].camp(k);
-      kW[l].re = c.re;
-      kW[l].im = -c.im;
+    if (!b->nonconst) {
+      for (int l = 0; l < nth; l++) {           // fillkW
+        fftw_complex c = w_seis[l].camp(k);
+        kW[l].re = c.re;
+        kW[l].im = -c.im;
+      }
+      lib_matrProdScalVecCpx(kD, kW, nth);
+      lib_matrProdDiagCpxR(kW, Af, nth, 3, K);
+      for (int l = 0; l < nth; l++) {           // fillkWNorm x2, ones
+        fftw_complex c = w_norm[l].camp(k);
+        m1[l].re = c.re / norm_seis[l];
+        m1[l].im = -(c.im / norm_seis[l]);
+        fftw_complex e = es3[l].camp(k);
+        m2[l].re = e.re / norm_es3[l];
+        m2[l].im = -(e.im / norm_es3[l]);
+      }
+      lib_matrFillOnesVecCpx(m3, nth);
+    } else {
+      // K = D A, errMult1 = 1 / norm, errMult2 = kD3 / norm(errorSmooth3),
+      // errMult3 = fillInverseAbskWRobust (:976-1014, :1296-1322)
+      fftw_complex kD3 = diff3.camp(k);
+      lib_matrFillValueVecCpx(kD, m1, nth);
+      lib_matrProdDiagCpxR(m1, Af, nth, 3, K);
+      lib_matrFillOnesVecCpx(m1, nth);
+      for (int l = 0; l < nth; l++) m1[l].re /= norm_seis[l];
+      lib_matrFillValueVecCpx(kD3, m2, nth);
+      for (int l = 0; l < nth; l++) {
+        float errorSmoothMult = 1.0f / norm_es3[l];
+        m2[l].re *= errorSmoothMult;
+        m2[l].im *= errorSmoothMult;
+      }
+      for (int l = 0; l < nth; l++) {
+        fftw_complex value = w_norm[l].camp(k);
+        fftw_complex valueFine = w_norm[l].camp_scaled(k, 0.999f);
+        float modulus = value.re * value.re + value.im * value.im;
+        float modulusFine = valueFine.re * valueFine.re + valueFine.im * valueFine.im;
+        float maxMod = std::max(modulus, modulusFine);
+        if (maxMod > 0.0) {
+          m3[l].re = float(1.0 / std::sqrt(maxMod));
+          m3[l].im = 0.0f;
+        } else {
+          m3[l].re = w_norm[l].norm * nzp * nzp * 100.0f;
+          m3[l].im = 0.0;
+        }
+      }
     }
-    lib_matrProdScalVecCpx(kD, kW, nth);
-    lib_matrProdDiagCpxR(kW, Af, nth, 3, K);
-    for (int l = 0; l < nth; l++) {           // fillkWNorm x2, ones
-      fftw_complex c = w_norm[l].camp(k);
-      m1[l].re = c.re / norm_seis[l];
-      m1[l].im = -(c.im / norm_seis[l]);
-      fftw_complex e = es3[l].camp(k);
-      m2[l].re = e.re / norm_es3[l];
-      m2[l].im = -(e.im / norm_es3[l]);
-    }
-    lib_matrFillOnesVecCpx(m3, nth);
     bool inv = realFrequency > b->low_cut * b->min_rel_thick && realFrequency < b->high_cut;
     for (int j = 0; j < nyp; j++) {
       for (int i = 0; i < cnxp; i++, idx++) {

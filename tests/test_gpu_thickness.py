@@ -177,3 +177,35 @@ def test_divide_data_matches_the_golden_fixture(ctx):
                     for l in range(blk.ntheta)])
     for l in range(blk.ntheta):
         assert rel(got[l][..., :blk.nxp], ref[l][..., :blk.nxp]) < TOL_DIV, l
+
+
+def test_nonconst_posterior_against_reference_arithmetic(ctx):
+    """The non-constant branch of the per-bin step (K = kD A with the wavelet-normalised error
+    multipliers and fillInverseAbskWRobust, src/avoinversion.cpp:976-1014, 1296-1322) against the
+    reference's FP32 numerics (oracle/_ref: FFTW 2.1.2, lib_matr.c and that branch restated
+    around them), both on the same divided data: mean 1e-4, covariance 1e-3, inverted bins and
+    Cholesky fallbacks equal."""
+    from oracle import bindings as ob
+    if not ob.ref32_available():
+        pytest.skip("oracle/_ref not built")
+    blk = thick_block(nsim=0)
+    job = api.Job(ctx, blk)
+    try:
+        _keep = job.upload_block()
+        job.divide_data()
+        div = np.stack([job.download(api.ROLE_DATA, l) for l in range(blk.ntheta)])
+        job.run()
+        out = job.download_outputs()
+        cnt = job.counters()
+    finally:
+        job.close()
+    nxp = blk.nxp
+    ref_blk = dataclasses.replace(blk, data=div[..., :nxp])
+    covs, _ = ref64.prior_cov_grids(ref_blk)
+    ec = ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)
+    r32 = ob.ref32_invert(ref_blk, covs, ec, nsim=0, seed=1, nonconst=True)
+    assert cnt["inverted_bins"] == r32.n_inverted and cnt["chol_fallbacks"] == r32.n_chol_fail
+    for a in range(3):
+        assert rel(out["mean"][a][..., :nxp], r32.mean[a][..., :nxp]) < TOL_MEAN, a
+    for q in range(6):
+        assert rel(out["cov"][q][..., :nxp], r32.cov[q][..., :nxp]) < TOL_COV, q

@@ -155,3 +155,32 @@ def test_separable_posterior_equals_the_grid_path():
     for x, y in ((b.mean, a.mean), (b.cov, a.cov)):
         assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-6
     assert a.n_inverted == b.n_inverted and a.n_chol_fail == b.n_chol_fail
+
+
+def test_nonconst_branch_restatement_matches_reference_arithmetic():
+    """The FP64 restatement of the non-constant-thickness per-bin step (K = kD A, error
+    multipliers 1/norm, kD3/norm(errorSmooth3), fillInverseAbskWRobust) against the same branch
+    restated around the reference's FFTW 2.1.2 and lib_matr.c (oracle/_ref), on the same
+    divided data: mean and covariance within 1e-5; the constant-thickness branch differs."""
+    import dataclasses
+    from oracle import bindings as ob
+    if not ob.ref32_available():
+        pytest.skip("oracle/_ref not built")
+    from crava_b200 import synth
+    spec = synth.BlockSpec(nx=40, ny=30, nz=50, nxp=48, nyp=40, nzp=64, nsim=0, seed=5, theta_deg=(8.0, 20.0, 32.0),
+                           peak_hz=(30.0,) * 3, sn=(6.0,) * 3)
+    blk = synth.with_rel_thick(synth.make_block(spec), seed=5, threshold=0.0)
+    div = ref64.divide_data_by_scale_wavelet(blk)
+    div = np.stack([ref64.interpolate_seismic(div[l], blk, blk.energy_threshold) for l in range(blk.ntheta)])
+    rb = dataclasses.replace(blk, data=div)
+    post = ref64.posterior(rb)
+    covs, _ = ref64.prior_cov_grids(rb)
+    ec = ref64.fill_err_corr_zero_grad(blk.corr_xy, blk.nxp, blk.nyp, blk.nzp)
+    r32 = ob.ref32_invert(rb, covs, ec, nsim=0, seed=1, nonconst=True)
+    nx = blk.nxp
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+    assert r32.n_inverted == post.n_inverted and r32.n_chol_fail == 0
+    assert max(rel(r32.mean[a][..., :nx], post.mean[a][..., :nx]) for a in range(3)) < 1e-5
+    assert max(rel(r32.cov[q][..., :nx], post.cov[q][..., :nx]) for q in range(6)) < 1e-5
+    r32c = ob.ref32_invert(rb, covs, ec, nsim=0, seed=1, nonconst=False)
+    assert rel(r32c.mean[0][..., :nx], post.mean[0][..., :nx]) > 1e-3
