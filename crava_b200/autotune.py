@@ -123,7 +123,12 @@ def tune_workload(name, w, reps, entries, log):
     if nzp in (128, 256, 320):
         api.tuning_set("pencil_kernel", pk, 2)
         sweep(ctx, job, stream, reps, "pencil_w", pk, [1, 2, 4, 8], ["zpass"], log)
+        # the realisation batch at the widest tile (without realisation slots a wider tile
+        # may fit than with them); the width is swept again below
+        w_keep = api.tuning_get("pencil_w", pk)
+        api.tuning_set("pencil_w", pk, 8)
         sweep(ctx, job, stream, reps, "pencil_sb", pk, [0, 1, 2, 4], ["zpass"], log)
+        api.tuning_set("pencil_w", pk, w_keep)
         eig_best = sweep(ctx, job, stream, reps, "pencil_threads", pk, [64, 128, 256, 384, 512], ["zpass"], log)
         # the tile width again, now with the realisation batch and threads chosen
         sweep(ctx, job, stream, reps, "pencil_w", pk, [2, 4, 8], ["zpass"], log)
