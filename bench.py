@@ -90,6 +90,75 @@ def stop_clock_sampler(p, f):
     f.close()
 
 
+class NvmlClockSampler:
+    """SM clock and clock-event reasons of one GPU read through NVML every `interval` seconds
+    by a thread (reads only), so that a timed region of a fraction of a second still gets a
+    dozen samples beside nvidia-smi's 200 ms ones."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, gpu_index, interval=0.01):
+        import threading
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+            self._reason = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        except Exception:
+            self._nv = None
+            return
+        self._interval = interval
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)))
+                r = self._reason(self._h)
+                for name, const in self.REASONS:
+                    if r & getattr(nv, const, 0):
+                        self.reasons.add(name)
+            except Exception:
+                return
+            self._stop.wait(self._interval)
+
+    def stop(self):
+        if self._t is not None:
+            self._stop.set()
+            self._t.join(timeout=2)
+        if self._nv is not None:
+            try:
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
+        return self
+
+
+def merge_clocks(smi, nv):
+    """One clocks record: the median SM clock of the NVML samples, taken inside the timed region
+    alone, and the throttle reasons seen by either sampler (nvidia-smi's run also covers a
+    short idle lead-in, so its clocks only stand in when NVML gave nothing)."""
+    if smi is not None:
+        smi = {k: v for k, v in smi.items() if k != "_sm"}
+    if nv is None or not nv.sm:
+        return smi
+    reasons = set(nv.reasons) | set((smi or {}).get("reasons", []))
+    mx = nv.max_mhz if nv.max_mhz is not None else (smi or {}).get("sm_max_mhz")
+    return {"sm_mhz": statistics.median(nv.sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(nv.sm),
+            "sampler": "NVML every 10 ms over the timed steps", "nvidia_smi_samples": (smi or {}).get("samples", 0)}
+
+
 def summarize_clocks(path, gpu_index):
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     sm, mx, reasons = [], None, set()
@@ -112,7 +181,8 @@ def summarize_clocks(path, gpu_index):
                 reasons.add(nm)
     if not sm:
         return None
-    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+            "_sm": sm}
 
 
 def physical_gpu_index(local_rank):
@@ -743,11 +813,13 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nv_clocks = NvmlClockSampler(physical_gpu_index(local_rank))
     e0.record(stream)
     for _ in range(args.steps):
         job.run(sh)
     e1.record(stream)
     torch.cuda.synchronize()
+    nv_clocks.stop()
     if dist:
         dist.barrier()
     stop_clock_sampler(*sampler)
@@ -824,7 +896,7 @@ def main():
         cufft = cufft_leg(torch)
         batched = batched_leg(ctx, torch)
         served = served_leg(torch)
-    clocks = summarize_clocks(clk_path, physical_gpu_index(local_rank))
+    clocks = merge_clocks(summarize_clocks(clk_path, physical_gpu_index(local_rank)), nv_clocks)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -90,6 +90,38 @@ class SegyDesc(ctypes.Structure):
                 ("header_format", ctypes.c_int), ("text", ctypes.POINTER(ctypes.c_char_p)), ("ntext", ctypes.c_int)]
 
 
+class Wavelet3DDesc(ctypes.Structure):
+    _fields_ = [("grad_x", _fp), ("grad_y", _fp), ("theta", _fp), ("filter_ni", ctypes.c_int),
+                ("filter_nj", ctypes.c_int), ("filter_x0", ctypes.c_double), ("filter_y0", ctypes.c_double),
+                ("filter_dx", ctypes.c_double), ("filter_dy", ctypes.c_double), ("alpha1", _fp),
+                ("halpha", _fp), ("global_wavelet", _fp), ("global_wavelet_norm", _fp)]
+
+
+def wavelet3d_desc(theta, alpha1, global_wavelet, global_wavelet_norm, filter_geom, grad_x=None, grad_y=None,
+                   halpha=None):
+    """A crava_wavelet3d_desc: theta (ntheta radians), alpha1 / halpha (ntheta, nj, ni) filter
+    surfaces with filter_geom = (x0, y0, dx, dy) in degrees, the global wavelets (ntheta, nzp)
+    and their norms, optional (ny, nx) depth gradient maps; returns (desc, keep-alive arrays)."""
+    keep = []
+
+    def arr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        keep.append(a)
+        return a.ctypes.data_as(_fp)
+
+    al = np.asarray(alpha1)
+    d = Wavelet3DDesc()
+    d.grad_x, d.grad_y = arr(grad_x), arr(grad_y)
+    d.theta = arr(np.asarray(theta, dtype=np.float32).reshape(-1))
+    d.filter_nj, d.filter_ni = int(al.shape[-2]), int(al.shape[-1])
+    d.filter_x0, d.filter_y0, d.filter_dx, d.filter_dy = (float(v) for v in filter_geom)
+    d.alpha1, d.halpha = arr(alpha1), arr(halpha)
+    d.global_wavelet, d.global_wavelet_norm = arr(global_wavelet), arr(np.asarray(global_wavelet_norm).reshape(-1))
+    return d, keep
+
+
 def segy_desc(geom: dict, top=None, rel_thick=None, text=None):
     """A crava_segy_desc from geom (the scalar fields) and optional per-trace top / relative
     thickness arrays (ny, nx) and textual-header lines; returns (desc, keep-alive objects)."""
@@ -173,6 +205,7 @@ def lib() -> ctypes.CDLL:
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), vp, vp]
     L.crava_job_local_noise.argtypes = [vp, vp, vp]
     L.crava_job_set_wavelet_grids.argtypes = [vp, ctypes.c_int, vp, vp]
+    L.crava_job_set_wavelet_3d.argtypes = [vp, ctypes.POINTER(Wavelet3DDesc)]
     L.crava_grid_write_storm.argtypes = [vp, ctypes.c_char_p, vp] + [ctypes.c_int] * 7 + [ctypes.POINTER(StormGeom), vp]
     L.crava_grid_read_storm.argtypes = [vp, ctypes.c_char_p, vp] + [ctypes.c_int] * 6 + [ctypes.POINTER(StormGeom), vp]
     L.crava_job_residual_synthetics.argtypes = [vp, vp]
@@ -431,6 +464,17 @@ class Job:
             arrs.append(a)
         _check(lib().crava_job_set_wavelet_grids(self._h, int(angle), *[None if a is None else a.ctypes.data
                                                                          for a in arrs]))
+
+    def set_wavelet_3d(self, theta, alpha1, global_wavelet, global_wavelet_norm, filter_geom, grad_x=None,
+                       grad_y=None, halpha=None):
+        """3D wavelets for every angle (crava_job_set_wavelet_3d); arguments as wavelet3d_desc."""
+        nth, ny, nx = self.blk.ntheta, self.blk.ny, self.blk.nx
+        for g in (grad_x, grad_y):
+            assert g is None or np.shape(g) == (ny, nx), np.shape(g)
+        assert np.shape(alpha1)[0] == nth and np.shape(global_wavelet) == (nth, self.blk.nzp)
+        d, _keep = wavelet3d_desc(theta, alpha1, global_wavelet, global_wavelet_norm, filter_geom, grad_x, grad_y,
+                                  halpha)
+        _check(lib().crava_job_set_wavelet_3d(self._h, ctypes.byref(d)))
 
     def residual_synthetics(self, stream=None):
         """multiplyDataByScaleWaveletAndWriteToFile: after a run with KEEP_RESIDUAL the residual

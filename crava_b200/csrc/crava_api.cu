@@ -307,6 +307,15 @@ struct crava_job {
   // without the non-constant tables (crava_job_residual_synthetics): own allocations
   float* wgrid = nullptr;         // ntheta x nx*ny shifts (samples), then ntheta x nx*ny gains
   float2* wspec = nullptr;        // ntheta x cnzp
+  // 3D wavelets (crava_job_set_wavelet_3d), one own allocation: per angle and trace the dip
+  // adjustment (w3mult, w3par) and the global wavelets' half spectra (w3glob); the global
+  // wavelets' modW
+  void* w3mem = nullptr;
+  double* w3mult = nullptr;
+  float4* w3par = nullptr;
+  float2* w3glob = nullptr;
+  double w3den = 0.0;
+  float w3modW[kMaxTheta] = {};
   bool async = false;             // pool from cudaMallocAsync on alloc_stream
   cudaStream_t alloc_stream = nullptr;
   // facies probabilities evaluated by crava_job_run (crava_job_set_facies): the corner boxes
@@ -1853,6 +1862,7 @@ void job_release(crava_job* j) {
   }
   if (j->wgrid) cudaFree(j->wgrid);
   if (j->wspec) cudaFree(j->wspec);
+  if (j->w3mem) cudaFree(j->w3mem);
   if (j->fac_mem) cudaFree(j->fac_mem);
   delete j;
 }
@@ -2934,6 +2944,126 @@ crava_status crava_job_set_wavelet_grids(crava_job* job, int angle, const float*
   return CRAVA_OK;
 }
 
+namespace {
+
+// The 3D wavelets' tables of a job into the parameters of the trace kernel.
+void w3_into(const crava_job* job, ThickParams& tp) {
+  if (!job->w3mem) return;
+  tp.w3_mult = job->w3mult;
+  tp.w3_par = job->w3par;
+  tp.wglob = job->w3glob;
+  tp.w3_den = job->w3den;
+  for (int l = 0; l < job->d.ntheta; l++) tp.modW[l] = job->w3modW[l];
+}
+
+}  // namespace
+
+crava_status crava_job_set_wavelet_3d(crava_job* job, const crava_wavelet3d_desc* w) {
+  if (!job || !w) return fail(CRAVA_EINVAL, "null job or descriptor");
+  const crava_job_desc& d = job->d;
+  if (!w->theta || !w->alpha1 || !w->global_wavelet || !w->global_wavelet_norm)
+    return fail(CRAVA_EINVAL, "theta, alpha1 and the global wavelets are required");
+  if (w->filter_ni < 1 || w->filter_nj < 1) return fail(CRAVA_EINVAL, "filter surface needs ni, nj >= 1");
+  if (!(w->filter_dx > 0.0) || !(w->filter_dy > 0.0) || !std::isfinite(w->filter_dx) || !std::isfinite(w->filter_dy) ||
+      !std::isfinite(w->filter_x0) || !std::isfinite(w->filter_y0))
+    return fail(CRAVA_EINVAL, "filter surface origin and spacing must be finite, spacing > 0");
+  const int n = d.nzp, cn = n / 2 + 1, nth = d.ntheta;
+  const size_t nxy = (size_t)d.nx * d.ny, nij = (size_t)w->filter_ni * w->filter_nj;
+  for (int l = 0; l < nth; l++) {
+    if (!std::isfinite(w->theta[l])) return fail(CRAVA_EINVAL, "theta holds a non-finite value");
+    if (!(w->global_wavelet_norm[l] > 0.f) || !std::isfinite(w->global_wavelet_norm[l]))
+      return fail(CRAVA_EINVAL, "global wavelet norms must be finite and > 0");
+  }
+  for (size_t t = 0; t < (size_t)nth * n; t++)
+    if (!std::isfinite(w->global_wavelet[t])) return fail(CRAVA_EINVAL, "global wavelet holds a non-finite value");
+  for (const float* g : {w->grad_x, w->grad_y})
+    if (g)
+      for (size_t t = 0; t < nxy; t++)
+        if (!std::isfinite(g[t])) return fail(CRAVA_EINVAL, "gradient map holds a non-finite value");
+  for (const float* g : {w->alpha1, w->halpha})
+    if (g)
+      for (size_t t = 0; t < (size_t)nth * nij; t++)
+        if (!std::isfinite(g[t])) return fail(CRAVA_EINVAL, "filter surface holds a non-finite value");
+  // the global wavelets: half spectra (wGlob) and modW (src/avoinversion.cpp:666-672 with
+  // wGlobal = Wavelet3D::getGlobalWavelet)
+  const float maxfreq = static_cast<float>((n / 2) * 1000.0 * d.nz) / static_cast<float>(d.lz * n);
+  std::vector<float2> wg((size_t)nth * cn);
+  for (int l = 0; l < nth; l++) {
+    const float* wf = w->global_wavelet + (size_t)l * n;
+    std::vector<cd> W = dft(std::vector<double>(wf, wf + n));
+    for (int k = 0; k < cn; k++) wg[(size_t)l * cn + k] = make_float2((float)W[k].real(), (float)W[k].imag());
+    float modW = w->global_wavelet_norm[l];
+    modW *= modW;
+    modW *= maxfreq / static_cast<float>(d.high_cut);
+    job->w3modW[l] = modW;
+  }
+  CUDA_TRY(cudaSetDevice(job->ctx->device));
+  const size_t o_par = align256(sizeof(double) * nth * nxy);
+  const size_t o_glob = o_par + align256(sizeof(float4) * nth * nxy);
+  if (!job->w3mem) {
+    CUDA_TRY(cudaMalloc(&job->w3mem, o_glob + sizeof(float2) * nth * cn));
+    job->w3mult = (double*)job->w3mem;
+    job->w3par = (float4*)((char*)job->w3mem + o_par);
+    job->w3glob = (float2*)((char*)job->w3mem + o_glob);
+  }
+  CUDA_TRY(cudaMemcpy(job->w3glob, wg.data(), sizeof(float2) * wg.size(), cudaMemcpyHostToDevice));
+  // the 3D wavelets' own spectra and normalised errorSmooth3: the job's tables, or (constant
+  // thickness: only the convolution of crava_job_residual_synthetics reads the adjustment)
+  // the wavelet spectra alone
+  Wavelet3DFill F{};
+  if (d.flags & CRAVA_FLAG_NONCONST_THICK) {
+    F.wamp = job->tp.wamp;
+    F.es3 = job->tp.es3;
+    for (int l = 0; l < nth; l++) F.es3_last[l] = job->tp.es3_last[l];
+  } else {
+    if (!job->wspec) {
+      const std::vector<float2> ws = wavelet_spectra(d);
+      CUDA_TRY(cudaMalloc(&job->wspec, sizeof(float2) * ws.size()));
+      CUDA_TRY(cudaMemcpy(job->wspec, ws.data(), sizeof(float2) * ws.size(), cudaMemcpyHostToDevice));
+    }
+    F.wamp = job->wspec;
+  }
+  // Wavelet::findNormWithinFrequencyBand's band and adjustForAmplitudeEffect's
+  // double(nzp * dz * 1e-3), dz the wavelet's sampling lz / nz in float
+  const float dz = (float)(d.lz / d.nz);
+  const float dOmega = static_cast<float>(1.0 / (n * dz * 0.001));
+  F.loI = std::max(0, (int)std::floor(d.low_cut / dOmega));
+  F.hiI = std::min(cn, (int)std::ceil(d.high_cut / dOmega));
+  job->w3den = static_cast<double>(static_cast<float>(n) * dz) * 1e-3;
+  F.den = job->w3den;
+  F.nx = d.nx; F.ny = d.ny; F.nzp = n; F.cnzp = cn;
+  F.ni = w->filter_ni; F.nj = w->filter_nj;
+  F.x0 = w->filter_x0; F.y0 = w->filter_y0; F.dx = w->filter_dx; F.dy = w->filter_dy;
+  for (int l = 0; l < nth; l++) F.theta[l] = w->theta[l];
+  F.mult = job->w3mult;
+  F.par = job->w3par;
+  // the maps and surfaces, staged in one temporary allocation
+  const size_t o_gy = align256(sizeof(float) * nxy), o_a = 2 * o_gy, o_h = o_a + align256(sizeof(float) * nth * nij);
+  void* tmp = nullptr;
+  CUDA_TRY(cudaMalloc(&tmp, o_h + sizeof(float) * nth * nij));
+  char* tb = (char*)tmp;
+  cudaError_t e = cudaSuccess;
+  if (w->grad_x && e == cudaSuccess) e = cudaMemcpy(tb, w->grad_x, sizeof(float) * nxy, cudaMemcpyHostToDevice);
+  if (w->grad_y && e == cudaSuccess) e = cudaMemcpy(tb + o_gy, w->grad_y, sizeof(float) * nxy, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(tb + o_a, w->alpha1, sizeof(float) * nth * nij, cudaMemcpyHostToDevice);
+  if (w->halpha && e == cudaSuccess) e = cudaMemcpy(tb + o_h, w->halpha, sizeof(float) * nth * nij, cudaMemcpyHostToDevice);
+  F.gx = w->grad_x ? (const float*)tb : nullptr;
+  F.gy = w->grad_y ? (const float*)(tb + o_gy) : nullptr;
+  F.alpha1 = (const float*)(tb + o_a);
+  F.halpha = w->halpha ? (const float*)(tb + o_h) : nullptr;
+  int nl = 0;
+  if (e == cudaSuccess) e = launch_wavelet3d_fill(F, nth, 0, &nl);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  cudaFree(tmp);
+  CUDA_TRY(e);
+  if (d.flags & CRAVA_FLAG_NONCONST_THICK) w3_into(job, job->tp);
+  {
+    std::lock_guard<std::mutex> lk(job->ctx->mu);
+    job->ctx->launches += nl;
+  }
+  return CRAVA_OK;
+}
+
 crava_status crava_job_residual_synthetics(crava_job* job, void* stream) {
   if (!job) return fail(CRAVA_EINVAL, "null job");
   const crava_job_desc& d = job->d;
@@ -2970,6 +3100,7 @@ crava_status crava_job_residual_synthetics(crava_job* job, void* stream) {
     int e = 0;
     tp.inv_rsq = std::frexp(tp.rsq, &e) == 0.5f ? 1.0f / tp.rsq : 0.f;
     tp.lz = d.lz;
+    w3_into(job, tp);
   }
   tp.mode = 1;
   tp.nIT = ((d.nx + 1) / 2 + tp.W - 1) / tp.W;

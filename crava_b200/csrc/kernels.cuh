@@ -158,6 +158,36 @@ struct ThickParams {
   // multiplyDataByScaleWaveletAndWriteToFile on the traces i < nx, j < ny
   int mode;
   float rsq_out;               // mode 1: float(sqrt(double(nzp))), its final divisor
+  // 3D wavelets (Wavelet3D, src/wavelet3D.cpp:328-459): per angle and unpadded trace
+  // i + nx j the dip adjustment of the trace's local wavelet (Wavelet3DFill), or null for
+  // 1D wavelets
+  const double* w3_mult;       // multiplyer = alpha1(phi, psi) cos(psi) cos(theta)
+  const float4* w3_par;        // {Halpha, local stretch, norm^2 of the adjusted wavelet, gamma}
+  const float2* wglob;         // nth x cnzp: the global (average) wavelets' half spectra
+  double w3_den;               // double(nzp * dz * 1e-3): the bin spacing's reciprocal, 1/Hz
+};
+// Per-trace dip adjustment of 3D wavelets (Wavelet3D::getLocalStretch and
+// createLocalWavelet1D -> extractLocalWaveletByDip1D -> dipAdjustWavelet, src/wavelet3D.cpp:
+// 328-459; the filter surfaces are NRLib::RegularSurface<float> read by WaveletFilter,
+// src/waveletfilter.cpp:60-75): for every angle and unpadded trace, from the structure depth
+// gradients, phi, psi, the filter values alpha1 and Halpha, multiplyer and the stretch, then
+// the norm^2 of the adjusted wavelet (Parseval over its half spectrum) and gamma, the factor
+// that band-normalises the adjusted errorSmooth3 given the job's normalised table.
+struct Wavelet3DFill {
+  const float* gx;             // nx*ny depth gradients (i + nx j), or null: flat
+  const float* gy;
+  const float* alpha1;         // nth x ni*nj (i + ni j): phi (degrees) along i, psi along j
+  const float* halpha;         // nth x ni*nj, or null: no damping
+  int ni, nj;
+  double x0, y0, dx, dy;       // surface origin and spacing (degrees)
+  float theta[kMaxTheta];      // Wavelet::getTheta (radians)
+  const float2* wamp;          // nth x cnzp: the 3D wavelets' own half spectra
+  const float2* es3;           // nth x cnzp: band-normalised errorSmooth3 (RMISSING last), or null
+  float2 es3_last[kMaxTheta];  // es3 at cnzp - 1 before the RMISSING
+  int nx, ny, nzp, cnzp, loI, hiI;
+  double den;                  // double(nzp * dz * 1e-3)
+  double* mult;                // out: nth x nx*ny
+  float4* par;                 // out: nth x nx*ny
 };
 // Prior grids of a GRIDS-mode job generated on the device (prior.cu): the six covariance
 // grids fillInParamCorr x priorVar0 and the error-correlation grid fillInErrCorr.
@@ -183,6 +213,7 @@ struct TraceOp {
 size_t thick_smem_bytes(int W, int nzp);
 int thick_tile_width(int nzp);
 cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, int* nlaunch);
+cudaError_t launch_wavelet3d_fill(const Wavelet3DFill& F, int nth, cudaStream_t st, int* nlaunch);
 cudaError_t launch_trace_energy(const ThickParams& P, int nth, float* energy, int* nzero, cudaStream_t st,
                                 int* nlaunch);
 cudaError_t launch_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, const TraceOp* ops, int nops,

@@ -99,41 +99,76 @@ __device__ __forceinline__ float2 adjustment(const ThickParams& P, int l, int k,
   return make_float2(__fdiv_rn(__fdiv_rn(wLoc.x, dL), glob.y), __fdiv_rn(__fdiv_rn(wLoc.y, dL), glob.y));
 }
 
-// The local wavelet of a trace with shift ish (samples) and gain gn: its spectrum is the
-// global one through shiftAndScale (createLocalWavelet1D, src/wavelet1D.cpp:518-526) and
-// its errorSmooth3 the global errorSmooth3 turned by the same unit-modulus multiplier (the
-// band normalisation takes the gain out; the RMISSING entry at cnzp - 1 stays).  The
-// reference re-transforms the local wavelet between the two (the difference constructors
-// work on its samples); here the spectra are used directly.
-__device__ __forceinline__ float2 local_wavelet(const ThickParams& P, int l, int m, float ish, float gn) {
-  return shift_scale(__ldg(P.wamp + (size_t)l * P.cnzp + m), ish, gn, m, P.nzp);
+// The local wavelet of one trace: shift ish (samples) and gain gn of shiftAndScale, and for
+// 3D wavelets the dip adjustment (multiplyer, Halpha), the norm^2 of the adjusted wavelet and
+// gamma, which band-normalises its errorSmooth3 given the normalised table.  1D wavelets:
+// mult 1, Halpha 0, the global norm^2 and gamma 1, under which every factor below is an
+// exact 1.
+struct LocalWavelet {
+  float ish, gn;
+  double mult;
+  float H, wn2, gam;
+};
+
+// Wavelet1D::adjustForAmplitudeEffect (src/wavelet1D.cpp:605-636) at bin m: the factor
+// float(multiplyer * float(exp(-pi omega Halpha))) with omega = m / double(nzp dz 1e-3), or
+// float(multiplyer) when Halpha <= 0.
+__device__ __forceinline__ float dip_factor(double den, int m, double mult, float H) {
+  if (!(H > 0.f)) return (float)mult;
+  const double om = __ddiv_rn((double)m, den);
+  const float am = (float)exp(__dmul_rn(__dmul_rn(-3.14159265358979323846, om), (double)H));
+  return (float)__dmul_rn(mult, (double)am);
 }
 
-__device__ __forceinline__ float2 local_es3(const ThickParams& P, int l, int m, float ish) {
+// The local wavelet's spectrum at bin m: the global one through the dip adjustment
+// (extractLocalWaveletByDip1D, src/wavelet3D.cpp:436-459) and shiftAndScale
+// (createLocalWavelet1D, src/wavelet1D.cpp:518-526, src/wavelet3D.cpp:347-373).  Its
+// errorSmooth3 is the normalised table's entry times the same dip factor and gamma, turned by
+// the shift's unit-modulus multiplier (the band normalisation takes the gain out; the
+// RMISSING entry at cnzp - 1 stays).  The reference re-transforms the local wavelet between
+// these steps (the amplitude adjustment and the difference constructors work on its
+// samples); here the spectra are used directly.
+__device__ __forceinline__ float2 local_wavelet(const ThickParams& P, int l, int m, const LocalWavelet& w) {
+  float2 c = __ldg(P.wamp + (size_t)l * P.cnzp + m);
+  if (P.w3_mult) {
+    const float f = dip_factor(P.w3_den, m, w.mult, w.H);
+    c = make_float2(__fmul_rn(c.x, f), __fmul_rn(c.y, f));
+  }
+  return shift_scale(c, w.ish, w.gn, m, P.nzp);
+}
+
+__device__ __forceinline__ float2 local_es3(const ThickParams& P, int l, int m, const LocalWavelet& w) {
   const int cn = P.cnzp;
-  if (m < cn - 1) return shift_scale(__ldg(P.es3 + (size_t)l * cn + m), ish, 1.f, m, P.nzp);
-  float2 v = shift_scale(P.es3_last[l], ish, 1.f, m, P.nzp);
-  v.y = -99999.0f;
-  if (!(P.nzp & 1)) v.x = -99999.0f;
+  float2 c = m < cn - 1 ? __ldg(P.es3 + (size_t)l * cn + m) : P.es3_last[l];
+  if (P.w3_mult) {
+    const float f = dip_factor(P.w3_den, m, w.mult, w.H);
+    c = make_float2(__fmul_rn(__fmul_rn(c.x, f), w.gam), __fmul_rn(__fmul_rn(c.y, f), w.gam));
+  }
+  float2 v = shift_scale(c, w.ish, 1.f, m, P.nzp);
+  if (m == cn - 1) {
+    v.y = -99999.0f;
+    if (!(P.nzp & 1)) v.x = -99999.0f;
+  }
   return v;
 }
 
-// computeAdjustmentFactor (src/avoinversion.cpp:630-719) with a local wavelet that carries
-// a shift and a gain: wLoc and eSkLoc from the local spectra stretched by sf, eSkGlob from
-// the local spectra unstretched (wLocal->getCAmp(k)), wGlob from the global wavelet; the
+// computeAdjustmentFactor (src/avoinversion.cpp:630-719) with a trace's local wavelet: wLoc
+// and eSkLoc from the local spectra stretched by sf, eSkGlob from the local spectra
+// unstretched (wLocal->getCAmp(k)), wGlob from the global wavelet (the 1D wavelet itself, or
+// for 3D wavelets Wavelet3D::getGlobalWavelet, whose norm the host puts into modW); the
 // global wavelet's quotient then depends on the trace and is formed here with the host's
 // float operations.
-__device__ __forceinline__ float2 adjustment_local(const ThickParams& P, int l, int k, float sf, float ish, float gn) {
+__device__ __forceinline__ float2 adjustment_local(const ThickParams& P, int l, int k, float sf, const LocalWavelet& w) {
   const int cn = P.cnzp;
-  const float wn2 = P.wn2[l], wnc = P.wnc, ev = P.err_var[l];
-  const float2 wLoc = interp_scaled(cn, k, sf, [&](int m) { return local_wavelet(P, l, m, ish, gn); });
+  const float wn2 = w.wn2, wnc = P.wnc, ev = P.err_var[l];
+  const float2 wLoc = interp_scaled(cn, k, sf, [&](int m) { return local_wavelet(P, l, m, w); });
   const float wLoc2 = sq2(wLoc);
-  const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(interp_scaled(cn, k, sf, [&](int m) { return local_es3(P, l, m, ish); })));
+  const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(interp_scaled(cn, k, sf, [&](int m) { return local_es3(P, l, m, w); })));
   const float c = __fmul_rn(__fsub_rn(1.f, wnc), 0.5f);
   float s2L = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sL)));
-  const float sG = __fadd_rn(__fdiv_rn(sq2(local_wavelet(P, l, k, ish, gn)), wn2), sq2(local_es3(P, l, k, ish)));
+  const float sG = __fadd_rn(__fdiv_rn(sq2(local_wavelet(P, l, k, w)), wn2), sq2(local_es3(P, l, k, w)));
   const float s2G = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sG)));
-  const float wGlob2 = sq2(__ldg(P.wamp + (size_t)l * cn + k));
+  const float wGlob2 = sq2(__ldg((P.wglob ? P.wglob : P.wamp) + (size_t)l * cn + k));
   const float tau2 = __ldg(P.tau2 + (size_t)l * cn + k);
   const float tm = __fmul_rn(0.05f, P.modW[l]);
   const float wG2A = wGlob2 < tm ? __fmul_rn(0.5f, __fadd_rn(wGlob2, tm)) : wGlob2;
@@ -171,7 +206,7 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   float2* SC = R + (size_t)W * nzp;
   __shared__ float s_sf[2 * 32];
   __shared__ double s_df[2 * 32];
-  __shared__ float s_ish[2 * 32], s_gn[2 * 32];   // local wavelet shift (samples) and gain
+  __shared__ LocalWavelet s_lw[2 * 32];            // the traces' local wavelets
   __shared__ int s_live[2 * 32];   // the trace has a nonzero tapered sample
   const int tid = threadIdx.x, T = blockDim.x;
   const int j = blockIdx.y, l = blockIdx.z;
@@ -182,24 +217,36 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
   const size_t kstride = (size_t)P.nyp * P.rnxp;
   float* row = g + (size_t)j * P.rnxp;
   for (int t = tid; t < nzp; t += T) tw[t] = P.twz[t];
-  // per trace: stretch sf = relThick (float, as getCAmp receives it) and
-  // deltaF = nz*1000 / (relThick * lz * nzp) (src/avoinversion.cpp:557-560)
+  // per trace: the local wavelet, the stretch sf as getCAmp receives it (divide mode
+  // float(relThick * double(localStretch)), src/avoinversion.cpp:557; convolution mode
+  // float(relThick) * localStretch, :748; the local stretch is 1 for 1D wavelets) and
+  // deltaF = nz*1000 / (relThick * lz * nzp) (:559-560)
   if (tid < 2 * W) {
     const int i = 2 * m0 + tid;
     double rt = 1.0;
     if (P.rel_thick && i < P.nxp) rt = P.rel_thick[(size_t)j * P.nxp + i];
-    s_sf[tid] = (float)rt;
-    s_df[tid] = __ddiv_rn(__dmul_rn((double)P.nz, 1000.0), __dmul_rn(__dmul_rn(rt, P.lz), (double)nzp));
-    s_live[tid] = 0;
-    float ish = 0.f, gn = 1.f;
-    if (P.wshift && i < P.nxp) {
+    LocalWavelet lw{0.f, 1.f, 1.0, 0.f, P.wn2[l], 1.f};
+    float stretch = 1.f;
+    if ((P.wshift || P.w3_mult) && i < P.nxp) {
       const size_t t = (size_t)l * P.nx * P.ny + (size_t)wavelet_index(j, P.ny, P.nyp) * P.nx +
                        wavelet_index(i, P.nx, P.nxp);
-      ish = P.wshift[t];
-      gn = P.wgain[t];
+      if (P.wshift) {
+        lw.ish = P.wshift[t];
+        lw.gn = P.wgain[t];
+      }
+      if (P.w3_mult) {
+        const float4 q = P.w3_par[t];
+        lw.mult = P.w3_mult[t];
+        lw.H = q.x;
+        stretch = q.y;
+        lw.wn2 = q.z;
+        lw.gam = q.w;
+      }
     }
-    s_ish[tid] = ish;
-    s_gn[tid] = gn;
+    s_lw[tid] = lw;
+    s_sf[tid] = conv ? __fmul_rn((float)rt, stretch) : (float)__dmul_rn(rt, (double)stretch);
+    s_df[tid] = __ddiv_rn(__dmul_rn((double)P.nz, 1000.0), __dmul_rn(__dmul_rn(rt, P.lz), (double)nzp));
+    s_live[tid] = 0;
   }
   __syncthreads();
   // load, 1/sqrt(nzp) and the z taper (:539-551); traces at or beyond nxp load as zero.
@@ -252,26 +299,26 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
       // the conjugate of the local wavelet's stretched spectrum (getCAmp returns the
       // conjugate's value, src/avoinversion.cpp:761-768)
       if (2 * m < nlive) {
-        const float ish = s_ish[2 * w], gn = s_gn[2 * w];
-        const float2 v = interp_scaled(P.cnzp, k, s_sf[2 * w], [&](int q) { return local_wavelet(P, l, q, ish, gn); });
+        const LocalWavelet& lw = s_lw[2 * w];
+        const float2 v = interp_scaled(P.cnzp, k, s_sf[2 * w], [&](int q) { return local_wavelet(P, l, q, lw); });
         fa = make_float2(v.x, -v.y);
       }
       if (2 * m + 1 < nlive) {
-        const float ish = s_ish[2 * w + 1], gn = s_gn[2 * w + 1];
-        const float2 v = interp_scaled(P.cnzp, k, s_sf[2 * w + 1], [&](int q) { return local_wavelet(P, l, q, ish, gn); });
+        const LocalWavelet& lw = s_lw[2 * w + 1];
+        const float2 v = interp_scaled(P.cnzp, k, s_sf[2 * w + 1], [&](int q) { return local_wavelet(P, l, q, lw); });
         fb = make_float2(v.x, -v.y);
       }
     } else {
       if (2 * m < P.nxp) {
         const double fk = __dmul_rn(s_df[2 * w], (double)k);
         if (fk < (double)P.high_cut && fk > (double)P.low_cut)
-          fa = P.wshift ? adjustment_local(P, l, k, s_sf[2 * w], s_ish[2 * w], s_gn[2 * w])
+          fa = (P.wshift || P.w3_mult) ? adjustment_local(P, l, k, s_sf[2 * w], s_lw[2 * w])
                         : adjustment(P, l, k, s_sf[2 * w]);
       }
       if (2 * m + 1 < P.nxp) {
         const double fk = __dmul_rn(s_df[2 * w + 1], (double)k);
         if (fk < (double)P.high_cut && fk > (double)P.low_cut)
-          fb = P.wshift ? adjustment_local(P, l, k, s_sf[2 * w + 1], s_ish[2 * w + 1], s_gn[2 * w + 1])
+          fb = (P.wshift || P.w3_mult) ? adjustment_local(P, l, k, s_sf[2 * w + 1], s_lw[2 * w + 1])
                         : adjustment(P, l, k, s_sf[2 * w + 1]);
       }
     }
@@ -366,6 +413,105 @@ __global__ void k_extrapolate(const __grid_constant__ ThickParams P, int l, int 
   g[(size_t)j * P.rnxp + i] = __fmul_rn(mult, v);
 }
 
+// NRLib::RegularSurface<float>::GetZ (libs/nrlib/surface/regularsurface.hpp:367-394 with
+// GetCorners :670-703, FindGeneralIndex :640-644, CellRelX/Y :851-863, GetBilinearZ :328-337
+// and GetBilinearZMissingCorners :340-363; missing value -999) of a surface of ni x nj nodes
+// (i + ni j) with origin (x0, y0) and spacing (dx, dy), in double as NRLib forms it.
+__device__ float surface_z(const float* z, int ni, int nj, double x0, double y0, double dx, double dy,
+                           double x, double y) {
+  const float miss = -999.0f;
+  const double fx = __ddiv_rn(x - x0, dx), fy = __ddiv_rn(y - y0, dy);
+  const int i = (int)floor(fx), j = (int)floor(fy);
+  float c[4] = {miss, miss, miss, miss};
+  if (i + 1 >= 0 && i < ni && j + 1 >= 0 && j < nj) {
+    if (i >= 0 && j >= 0) c[0] = z[i + (size_t)ni * j];
+    if (i + 1 < ni && j >= 0) c[1] = z[i + 1 + (size_t)ni * j];
+    if (i >= 0 && j + 1 < nj) c[2] = z[i + (size_t)ni * (j + 1)];
+    if (i + 1 < ni && j + 1 < nj) c[3] = z[i + 1 + (size_t)ni * (j + 1)];
+  }
+  int nmiss = 0;
+  for (int q = 0; q < 4; q++) nmiss += c[q] == miss;
+  if (nmiss == 4) return miss;
+  const double u = fx - trunc(fx), v = fy - trunc(fy);
+  if (nmiss == 0) {
+    const float a = c[0], b = __fsub_rn(c[1], a), cc = __fsub_rn(c[2], a);
+    const float d = __fsub_rn(__fsub_rn(__fsub_rn(c[3], a), b), cc);
+    const double r = __dadd_rn(__dadd_rn(__dadd_rn((double)a, __dmul_rn((double)b, u)), __dmul_rn((double)cc, v)),
+                               __dmul_rn(__dmul_rn((double)d, u), v));
+    return (float)r;
+  }
+  const double w[4] = {__dmul_rn(1.0 - u, 1.0 - v), __dmul_rn(u, 1.0 - v), __dmul_rn(1.0 - u, v), __dmul_rn(u, v)};
+  double sum = 0.0, sw = 0.0;
+  for (int q = 0; q < 4; q++)
+    if (c[q] != miss) {
+      sum = __dadd_rn(sum, __dmul_rn(w[q], (double)c[q]));
+      sw = __dadd_rn(sw, w[q]);
+    }
+  if (sw == 0.0) return miss;
+  return (float)__ddiv_rn(sum, sw);
+}
+
+// One thread per (unpadded trace, angle): Wavelet3D::getLocalStretch and
+// createLocalWavelet1D (src/wavelet3D.cpp:328-373) with findPhi / findPsi (:819-851) and
+// dipAdjustWavelet (:452-459).  The reference's float calls (atan and cos of float
+// arguments) are taken as the double function rounded to float.  Then the norm^2 of the
+// adjusted wavelet (Wavelet::findNorm, src/wavelet.cpp:882-900, by Parseval over the half
+// spectrum in double) and gamma = 1 / findNormWithinFrequencyBand (:903-925) of the normalised
+// errorSmooth3 table times the same dip factors.
+__global__ void k_wavelet3d_fill(const __grid_constant__ Wavelet3DFill F) {
+  const int l = blockIdx.y;
+  const size_t nxy = (size_t)F.nx * F.ny;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxy) return;
+  const float gx = F.gx ? F.gx[t] : 0.f, gy = F.gy ? F.gy[t] : 0.f;
+  const double pi = 3.14159265358979323846;
+  double phi;
+  const double eps = 0.001;
+  if (gx > eps && gy >= 0.f) phi = (double)(float)atan((double)__fdiv_rn(gy, gx));
+  else if (gx > eps && gy < 0.f) phi = __dadd_rn(2.0 * pi, (double)(float)atan((double)__fdiv_rn(gy, gx)));
+  else if (gx < -eps) phi = __dadd_rn(pi, (double)(float)atan((double)__fdiv_rn(gy, gx)));
+  else if (gy >= 0.f) phi = 0.5 * pi;
+  else phi = 1.5 * pi;
+  const float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), 1.f));
+  const double psi = r > 1.f ? acos(__ddiv_rn(1.0, (double)r)) : 0.0;
+  const double cth = (double)(float)cos((double)F.theta[l]);
+  const double cpsi = __dmul_rn(cos(psi), cth);
+  const double xd = __ddiv_rn(__dmul_rn(phi, 180.0), pi), yd = __ddiv_rn(__dmul_rn(psi, 180.0), pi);
+  const size_t nij = (size_t)F.ni * F.nj;
+  const float a1 = surface_z(F.alpha1 + l * nij, F.ni, F.nj, F.x0, F.y0, F.dx, F.dy, xd, yd);
+  const float H = F.halpha ? surface_z(F.halpha + l * nij, F.ni, F.nj, F.x0, F.y0, F.dx, F.dy, xd, yd) : 0.f;
+  const double mult = __dmul_rn((double)a1, cpsi);
+  const int cn = F.cnzp;
+  const float2* wa = F.wamp + (size_t)l * cn;
+  double n2 = 0.0;
+  for (int k = 0; k < cn; k++) {
+    const float f = dip_factor(F.den, k, mult, H);
+    const float2 c = __ldg(wa + k);
+    const double cr = (double)__fmul_rn(c.x, f), ci = (double)__fmul_rn(c.y, f);
+    const double wk = (k == 0 || (k == cn - 1 && !(F.nzp & 1))) ? 1.0 : 2.0;
+    n2 = __dadd_rn(n2, __dmul_rn(wk, __dadd_rn(__dmul_rn(cr, cr), __dmul_rn(ci, ci))));
+  }
+  const float norm = (float)sqrt(__ddiv_rn(n2, (double)F.nzp));
+  float gam = 1.f;
+  if (F.es3) {
+    const double fac = __ddiv_rn(1.0, (double)F.nzp);
+    double e2 = 0.0;
+    float e0 = 0.f;
+    for (int k = F.loI; k < F.hiI; k++) {
+      const float f = dip_factor(F.den, k, mult, H);
+      const float2 c = k < cn - 1 ? __ldg(F.es3 + (size_t)l * cn + k) : F.es3_last[l];
+      const float er = __fmul_rn(c.x, f), ei = __fmul_rn(c.y, f);
+      const float p = __fadd_rn(__fmul_rn(er, er), __fmul_rn(ei, ei));
+      if (k == 0) e0 = p;
+      e2 = __dadd_rn(e2, __dmul_rn(2.0 * fac, (double)p));
+    }
+    if (F.loI == 0) e2 = __dsub_rn(e2, __dmul_rn(fac, (double)e0));
+    gam = __fdiv_rn(1.f, (float)sqrt(e2));
+  }
+  F.mult[l * nxy + t] = mult;
+  F.par[l * nxy + t] = make_float4(H, (float)cpsi, __fmul_rn(norm, norm), gam);
+}
+
 }  // namespace
 
 size_t thick_smem_bytes(int W, int nzp) { return sizeof(float2) * ((size_t)nzp + 2 * (size_t)W * nzp); }
@@ -402,6 +548,15 @@ cudaError_t launch_trace_interp(float* g, int rnxp, int nyp, int nzp, int nx, co
   if (nops <= 0) return cudaSuccess;
   dim3 grid((unsigned)nops, (unsigned)((nzp + 255) / 256));
   k_trace_interp<<<grid, 256, 0, st>>>(g, rnxp, nyp, nzp, nx, ops);
+  if (nlaunch) (*nlaunch)++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wavelet3d_fill(const Wavelet3DFill& F, int nth, cudaStream_t st, int* nlaunch) {
+  const size_t nxy = (size_t)F.nx * F.ny;
+  if (nxy == 0 || nth < 1 || nth > kMaxTheta) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((nxy + 127) / 128), (unsigned)nth);
+  k_wavelet3d_fill<<<grid, 128, 0, st>>>(F);
   if (nlaunch) (*nlaunch)++;
   return cudaGetLastError();
 }

@@ -426,6 +426,47 @@ def with_rel_thick(blk: Block, seed: int = 3, threshold: float = 0.0) -> Block:
                                energy_threshold=threshold)
 
 
+def wavelet3d_model(blk: Block, theta_deg, seed: int = 5, halpha: bool = True, missing: bool = True,
+                    flat: bool = False) -> dict:
+    """Synthetic 3D-wavelet inputs for a block (the crava_wavelet3d_desc fields, keyed as
+    api.Job.set_wavelet_3d takes them): smooth structure depth gradients of either sign up
+    to about 0.4 with a strip of near-zero x gradients (findPhi's small-|a| branches), filter
+    surfaces alpha1 = 1 + 0.2 sin(phi) cos(psi) and Halpha in 0.5..3 ms over phi 0..360 and
+    psi 0..90 degrees on 30 x 10 degree nodes (with a few missing nodes), and global wavelets
+    0.93 times the block's own, each with its norm.  flat: no gradients, theta 0, alpha1 1,
+    no Halpha and the block's own wavelets (the neutral model)."""
+    rng = np.random.default_rng(seed)
+    nth, nx, ny = blk.ntheta, blk.nx, blk.ny
+    ni, nj = 13, 10
+    phi = np.arange(ni) * 30.0
+    psi = np.arange(nj) * 10.0
+    if flat:
+        return dict(theta=np.zeros(nth, np.float32), alpha1=np.ones((nth, nj, ni), np.float32), halpha=None,
+                    filter_geom=(0.0, 0.0, 30.0, 10.0), grad_x=None, grad_y=None,
+                    global_wavelet=np.asarray(blk.wavelet, np.float32),
+                    global_wavelet_norm=np.asarray(blk.wavelet_norm, np.float32))
+    x = np.arange(nx)[None, :] / max(nx - 1, 1)
+    y = np.arange(ny)[:, None] / max(ny - 1, 1)
+    ph = rng.uniform(0, 2 * np.pi, 4)
+    gx = 0.4 * np.sin(2 * np.pi * x + ph[0]) * np.cos(np.pi * y + ph[1])
+    gy = 0.4 * np.cos(3 * np.pi * x + ph[2]) * np.sin(2 * np.pi * y + ph[3])
+    gx[:, : max(1, nx // 8)] *= 1e-3
+    a1 = np.empty((nth, nj, ni), np.float32)
+    ha = np.empty((nth, nj, ni), np.float32)
+    for l in range(nth):
+        a1[l] = 1.0 + 0.2 * np.sin(np.deg2rad(phi)[None, :] + 0.3 * l) * np.cos(np.deg2rad(psi)[:, None])
+        ha[l] = rng.uniform(0.0005, 0.003, (nj, ni))
+        if missing:
+            a1[l, 0, 3] = -999.0
+            ha[l, 1, 5] = -999.0
+    gw = (0.93 * np.asarray(blk.wavelet, np.float64)).astype(np.float32)
+    gnorm = np.sqrt((gw.astype(np.float64) ** 2).sum(axis=1)).astype(np.float32)
+    return dict(theta=np.deg2rad(np.asarray(theta_deg, np.float64)).astype(np.float32), alpha1=a1,
+                halpha=ha if halpha else None, filter_geom=(0.0, 0.0, 30.0, 10.0),
+                grad_x=gx.astype(np.float32), grad_y=gy.astype(np.float32), global_wavelet=gw,
+                global_wavelet_norm=gnorm)
+
+
 # --- the configurations of the benchmark suite -------------------------------------
 
 def config0(seed: int = 11) -> BlockSpec:

@@ -204,6 +204,41 @@ crava_status crava_job_divide_data(crava_job* job, void* stream);
  * library turns the global spectra directly, which differs by the rounding of that round trip. */
 crava_status crava_job_set_wavelet_grids(crava_job* job, int angle, const float* shift_ms, const float* gain);
 
+/* 3D wavelets (Wavelet3D, src/wavelet3D.cpp): the job's wavelets (crava_job_desc.wavelet) are
+ * the 3D wavelets' own pulses, and every trace's local wavelet is its angle's pulse adjusted
+ * for the local dip (createLocalWavelet1D -> extractLocalWaveletByDip1D -> dipAdjustWavelet,
+ * :347-373, :436-459: multiplyer = alpha1(phi, psi) cos(psi) cos(theta) and the damping
+ * exp(-pi f Halpha(phi, psi)) of Wavelet1D::adjustForAmplitudeEffect,
+ * src/wavelet1D.cpp:605-636), then shifted and scaled by the wavelet grids; its stretch is
+ * rel_thick * cos(psi) cos(theta) (getLocalStretch, :328-344), and the adjustment factor's
+ * global wavelet is the average wavelet (getGlobalWavelet), src/avoinversion.cpp:508-566.
+ * phi and psi come from the structure depth gradients of the trace (findPhi / findPsi,
+ * :819-851); alpha1 and Halpha are the wavelet filter surfaces (WaveletFilter,
+ * src/waveletfilter.cpp:27-75), read by bilinear interpolation as
+ * NRLib::RegularSurface<float>::GetZ at (phi, psi) in degrees. */
+typedef struct crava_wavelet3d_desc {
+  const float* grad_x;         /* nx*ny structure depth gradients (i + nx*j), or NULL: flat */
+  const float* grad_y;
+  const float* theta;          /* ntheta angles (radians, Wavelet::getTheta)   */
+  int filter_ni, filter_nj;    /* filter surface nodes: phi along i, psi along j */
+  double filter_x0, filter_y0; /* surface origin (degrees)                     */
+  double filter_dx, filter_dy; /* node spacing (degrees), > 0                  */
+  const float* alpha1;         /* ntheta x ni*nj (i + ni*j); -999 marks missing */
+  const float* halpha;         /* ntheta x ni*nj, or NULL: no Halpha surface   */
+  const float* global_wavelet; /* ntheta x nzp samples of the average wavelets, FFT order */
+  const float* global_wavelet_norm; /* ntheta, their Wavelet::getNorm          */
+} crava_wavelet3d_desc;
+
+/* Sets the job's wavelets to 3D wavelets (all angles) for crava_job_divide_data and
+ * crava_job_residual_synthetics from the next call on.  The dip adjustment of every angle and
+ * trace is evaluated on the device once, here: phi, psi, the filter values, the norm of the
+ * adjusted wavelet and the band normalisation of its errorSmooth3.  The first call allocates
+ * 12*ntheta*nx*ny bytes (plus the global wavelets' spectra) of device memory outside the job's
+ * footprint; the call is synchronous.  As with the wavelet grids, the reference re-transforms
+ * each local wavelet to samples between the adjustment steps; this library works on the
+ * spectra, which differs by the rounding of those round trips. */
+crava_status crava_job_set_wavelet_3d(crava_job* job, const crava_wavelet3d_desc* w);
+
 /* AVOInversion::multiplyDataByScaleWaveletAndWriteToFile (src/avoinversion.cpp:721-790), the
  * wavelet-convolved residuals the reference writes after the inversion (:1123): for a job
  * with CRAVA_FLAG_KEEP_RESIDUAL after crava_job_run, every residual spectrum is transformed

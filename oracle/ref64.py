@@ -240,13 +240,18 @@ def shift_scale32(c: np.ndarray, ish, gain, m, nzp: int):
     """Wavelet1D::shiftAndScale (src/wavelet1D.cpp:580-602) at bins m of the half spectrum c
     (complex64): multiplier float(gain cos(a)) + i float(gain sin(-a)) with
     a = 2 (pi iShift m) / float(nzp) in double, product in float32.  Returns (re, im)."""
+    m = np.asarray(m)
+    return shift_scale_vals32(c.real.astype(np.float32)[m], c.imag.astype(np.float32)[m], ish, gain, m, nzp)
+
+
+def shift_scale_vals32(cr, ci, ish, gain, m, nzp: int):
+    """shift_scale32 on the values (cr, ci) of bins m (float32 arrays)."""
     f32 = np.float32
     m = np.asarray(m)
     a = 2.0 * (math.pi * np.asarray(ish, dtype=f32).astype(np.float64) * m.astype(np.float64)) / float(f32(nzp))
     g = np.asarray(gain, dtype=f32).astype(np.float64)
     mr = (g * np.cos(a)).astype(f32)
     mi = (g * np.sin(-a)).astype(f32)
-    cr, ci = c.real.astype(f32)[m], c.imag.astype(f32)[m]
     return ((mr * cr).astype(f32) - (mi * ci).astype(f32)).astype(f32), \
         ((mi * cr).astype(f32) + (mr * ci).astype(f32)).astype(f32)
 
@@ -394,7 +399,7 @@ def adjustment_factor(tab, l: int, sf, k) -> np.ndarray:
     return fr.astype(np.float64) + 1j * fi.astype(np.float64)
 
 
-def adjustment_factor_local(tab, l: int, sf, k, ish, gn, nzp: int) -> np.ndarray:
+def adjustment_factor_local(tab, l: int, sf, k, ish, gn, nzp: int, w3=None) -> np.ndarray:
     """computeAdjustmentFactor (src/avoinversion.cpp:630-719) for traces whose local wavelet
     carries a shift ish (samples) and a gain gn (createLocalWavelet1D + shiftAndScale,
     src/wavelet1D.cpp:518-602): wLoc and eSkLoc from the shifted and scaled spectra stretched
@@ -402,22 +407,39 @@ def adjustment_factor_local(tab, l: int, sf, k, ish, gn, nzp: int) -> np.ndarray
     local errorSmooth3 is the global one turned by the unit-modulus multiplier (its band
     normalisation removes the gain) with the RMISSING entry at cnzp - 1 kept; the
     reference's round trip of the local wavelet through the time domain is not restated.
-    float32 in the reference's operation order; sf, k, ish, gn broadcast."""
+    float32 in the reference's operation order; sf, k, ish, gn broadcast.  w3: 3D wavelets
+    (wavelet3d_params of the angle: per-trace mult, H, wn2, gam broadcasting with ish, and the
+    global wavelet's half spectrum wglob, its modW and the bin spacing den); the local spectra
+    then carry the dip factor (dip_factor32), errorSmooth3 also gamma, the norm is the adjusted
+    wavelet's and wGlob the global wavelet's."""
     f32 = np.float32
     wa, es = tab["wamp"][l], tab["es3"][l]
     es_last = tab["es3_last"][l]
     cn = wa.shape[0]
     wn2, modW, ev = tab["wn2"][l], tab["modW"][l], tab["err_var"][l]
+    if w3 is not None:
+        wn2, modW = w3["wn2"], f32(w3["modW"])
     wnc = f32(tab["wnc"])
     k = np.asarray(k)
     es_true = es.copy()
     es_true[cn - 1] = es_last
 
     def wl(m):
-        return shift_scale32(wa, ish, gn, m, nzp)
+        m = np.asarray(m)
+        cr, ci = wa.real.astype(f32)[m], wa.imag.astype(f32)[m]
+        if w3 is not None:
+            f = dip_factor32(w3["den"], m, w3["mult"], w3["H"])
+            cr, ci = (cr * f).astype(f32), (ci * f).astype(f32)
+        return shift_scale_vals32(cr, ci, ish, gn, m, nzp)
 
     def el(m):
-        r, i = shift_scale32(es_true, ish, f32(1.0), m, nzp)
+        m = np.asarray(m)
+        cr, ci = es_true.real.astype(f32)[m], es_true.imag.astype(f32)[m]
+        if w3 is not None:
+            f = dip_factor32(w3["den"], m, w3["mult"], w3["H"])
+            cr = ((cr * f).astype(f32) * w3["gam"]).astype(f32)
+            ci = ((ci * f).astype(f32) * w3["gam"]).astype(f32)
+        r, i = shift_scale_vals32(cr, ci, ish, f32(1.0), m, nzp)
         last = np.asarray(m) == cn - 1
         i = np.where(last, f32(-99999.0), i).astype(f32)
         if nzp % 2 == 0:
@@ -434,7 +456,8 @@ def adjustment_factor_local(tab, l: int, sf, k, ish, gn, nzp: int) -> np.ndarray
     c = (f32(1.0) - wnc) * f32(0.5)
     s2L = (ev * (wnc + c * sL)).astype(f32)
     s2G = (ev * (wnc + c * sG)).astype(f32)
-    wgr, wgi = wa.real.astype(f32)[k], wa.imag.astype(f32)[k]
+    wgs = w3["wglob"] if w3 is not None else wa
+    wgr, wgi = wgs.real.astype(f32)[k], wgs.imag.astype(f32)[k]
     wGlob2 = (wgr * wgr + wgi * wgi).astype(f32)
     tau2 = tab["tau2"][l][k]
     tm = f32(0.05) * modW
@@ -450,6 +473,149 @@ def adjustment_factor_local(tab, l: int, sf, k, ish, gn, nzp: int) -> np.ndarray
         fr = ((lr / dL) / q).astype(f32)
         fi = ((li / dL) / q).astype(f32)
     return fr.astype(np.float64) + 1j * fi.astype(np.float64)
+
+
+def dip_factor32(den: float, m, mult, H):
+    """Wavelet1D::adjustForAmplitudeEffect (src/wavelet1D.cpp:605-636) at bins m: the factor
+    float(multiplyer * float(exp(-pi omega Halpha))) with omega = m / den (den =
+    double(nzp dz 1e-3)), or float(multiplyer) where Halpha <= 0.  float32 array."""
+    f32 = np.float32
+    m = np.asarray(m).astype(np.float64)
+    mult = np.asarray(mult, dtype=np.float64)
+    H = np.asarray(H, dtype=f32)
+    om = m / float(den)
+    am = np.exp((-math.pi * om) * H.astype(np.float64)).astype(f32)
+    return np.where(H > f32(0), (mult * am.astype(np.float64)).astype(f32), mult.astype(f32)).astype(f32)
+
+
+def surface_z(z: np.ndarray, geom, x: float, y: float) -> float:
+    """NRLib::RegularSurface<float>::GetZ (libs/nrlib/surface/regularsurface.hpp:367-394 with
+    GetCorners :670-703, FindGeneralIndex :640-644, CellRelX/Y :851-863, GetBilinearZ :328-337,
+    GetBilinearZMissingCorners :340-363) on z (nj, ni) with geom = (x0, y0, dx, dy); -999 is
+    missing.  Returns a float32 value."""
+    f32 = np.float32
+    miss = f32(-999.0)
+    nj, ni = z.shape
+    x0, y0, dx, dy = (float(v) for v in geom)
+    fx, fy = (x - x0) / dx, (y - y0) / dy
+    i, j = int(math.floor(fx)), int(math.floor(fy))
+    c = [miss] * 4
+    if i + 1 >= 0 and i < ni and j + 1 >= 0 and j < nj:
+        if i >= 0 and j >= 0:
+            c[0] = f32(z[j, i])
+        if i + 1 < ni and j >= 0:
+            c[1] = f32(z[j, i + 1])
+        if i >= 0 and j + 1 < nj:
+            c[2] = f32(z[j + 1, i])
+        if i + 1 < ni and j + 1 < nj:
+            c[3] = f32(z[j + 1, i + 1])
+    nmiss = sum(1 for v in c if v == miss)
+    if nmiss == 4:
+        return miss
+    u, v = math.modf(fx)[0], math.modf(fy)[0]
+    if nmiss == 0:
+        a = c[0]
+        b, cc = f32(c[1] - a), f32(c[2] - a)
+        d = f32(f32(f32(c[3] - a) - b) - cc)
+        return f32(float(a) + float(b) * u + float(cc) * v + float(d) * u * v)
+    w = [(1.0 - u) * (1.0 - v), u * (1.0 - v), (1.0 - u) * v, u * v]
+    sm = sw = 0.0
+    for q in range(4):
+        if c[q] != miss:
+            sm += w[q] * float(c[q])
+            sw += w[q]
+    return miss if sw == 0.0 else f32(sm / sw)
+
+
+def find_phi(a, b) -> float:
+    """Wavelet3D::findPhi (src/wavelet3D.cpp:819-838) of float32 gradients a, b; its float atan
+    taken as the double atan rounded to float32."""
+    f32 = np.float32
+    a, b = f32(a), f32(b)
+    eps = 0.001
+
+    def at():
+        return float(f32(math.atan(float(f32(b / a)))))
+    if a > eps and b >= 0:
+        return at()
+    if a > eps and b < 0:
+        return 2 * math.pi + at()
+    if a < -eps:
+        return math.pi + at()
+    return 0.5 * math.pi if b >= 0 else 1.5 * math.pi
+
+
+def find_psi(r) -> float:
+    """Wavelet3D::findPsi (src/wavelet3D.cpp:841-851)."""
+    return math.acos(1.0 / float(r)) if r > 1 else 0.0
+
+
+def wavelet3d_params(blk, w3):
+    """Per angle and unpadded trace the dip adjustment of 3D wavelets (Wavelet3D::
+    getLocalStretch / createLocalWavelet1D / dipAdjustWavelet, src/wavelet3D.cpp:328-459):
+    phi and psi from the depth gradients, alpha1 and Halpha from the filter surfaces at
+    (phi, psi) in degrees, multiplyer = alpha1 cos(psi) cos(theta) (cos of the float angle
+    rounded to float32), the stretch float32(cos(psi) cos(theta)), the norm^2 of the adjusted
+    wavelet (Wavelet::findNorm by Parseval over its half spectrum in float64, then
+    float32(norm)^2) and gamma = 1 / findNormWithinFrequencyBand of the job's normalised
+    errorSmooth3 times the dip factor.  w3: dict with theta, alpha1 / halpha (ntheta, nj, ni),
+    filter_geom (x0, y0, dx, dy), grad_x / grad_y (ny, nx) or None, global_wavelet (ntheta, nzp),
+    global_wavelet_norm.  Returns per angle a dict of (ny, nx) arrays mult, H, stretch, wn2,
+    gam and the scalars of adjustment_factor_local (wglob, modW, den)."""
+    f32 = np.float32
+    nx, ny, n = blk.nx, blk.ny, blk.nzp
+    cn = n // 2 + 1
+    tab = thick_tables(blk)
+    dz = f32(blk.lz / blk.nz)
+    den = float(f32(f32(n) * dz)) * 1e-3
+    dOmega = f32(1.0 / float(f32(n * dz) * 0.001))
+    loI = max(0, int(np.floor(f32(blk.low_cut) / dOmega)))
+    hiI = min(cn, int(np.ceil(f32(blk.high_cut) / dOmega)))
+    maxfreq = f32((n // 2) * 1000.0 * blk.nz) / f32(blk.lz * n)
+    gx = np.zeros((ny, nx), f32) if w3.get("grad_x") is None else np.asarray(w3["grad_x"], f32)
+    gy = np.zeros((ny, nx), f32) if w3.get("grad_y") is None else np.asarray(w3["grad_y"], f32)
+    k = np.arange(cn)
+    wk = np.where((k == 0) | ((k == cn - 1) & (n % 2 == 0)), 1.0, 2.0)
+    out = []
+    for l in range(blk.ntheta):
+        cth = float(f32(math.cos(float(f32(w3["theta"][l])))))
+        wa = tab["wamp"][l]
+        es = tab["es3"][l].copy()
+        es[cn - 1] = tab["es3_last"][l]
+        P = {k2: np.zeros((ny, nx), dt) for k2, dt in
+             (("mult", np.float64), ("H", f32), ("stretch", f32), ("wn2", f32), ("gam", f32))}
+        for j in range(ny):
+            for i in range(nx):
+                a, b = gx[j, i], gy[j, i]
+                phi = find_phi(a, b)
+                r = f32(np.sqrt(f32(f32(a * a) + f32(b * b)) + f32(1)))
+                psi = find_psi(r)
+                cpsi = math.cos(psi) * cth
+                xd, yd = phi * 180.0 / math.pi, psi * 180.0 / math.pi
+                a1 = surface_z(np.asarray(w3["alpha1"][l]), w3["filter_geom"], xd, yd)
+                H = f32(0) if w3.get("halpha") is None else surface_z(np.asarray(w3["halpha"][l]), w3["filter_geom"], xd, yd)
+                mult = float(a1) * cpsi
+                f = dip_factor32(den, k, mult, H)
+                cr, ci = (wa.real.astype(f32) * f).astype(f32), (wa.imag.astype(f32) * f).astype(f32)
+                n2 = float(np.sum(wk * (cr.astype(np.float64) ** 2 + ci.astype(np.float64) ** 2)))
+                norm = f32(math.sqrt(n2 / n))
+                er, ei = (es.real.astype(f32) * f).astype(f32), (es.imag.astype(f32) * f).astype(f32)
+                p = (er * er + ei * ei).astype(f32)
+                e2 = sum(2.0 * (1.0 / n) * float(p[q]) for q in range(loI, hiI))
+                if loI == 0:
+                    e2 -= (1.0 / n) * float(p[0])
+                P["mult"][j, i] = mult
+                P["H"][j, i] = H
+                P["stretch"][j, i] = f32(cpsi)
+                P["wn2"][j, i] = f32(norm * norm)
+                P["gam"][j, i] = f32(1) / f32(math.sqrt(e2))
+        gw = np.asarray(w3["global_wavelet"][l], f32)
+        P["wglob"] = np.fft.fft(gw.astype(np.float64))[:cn].astype(np.complex64)
+        gn_ = f32(w3["global_wavelet_norm"][l])
+        P["modW"] = f32(f32(gn_ * gn_) * (maxfreq / f32(blk.high_cut)))
+        P["den"] = den
+        out.append(P)
+    return out
 
 
 def wavelet_index(i: int, n: int, np_: int) -> int:
@@ -484,14 +650,25 @@ def local_wavelet_maps(blk, shift_ms, gain):
     return ish[:, jj][:, :, ii], gn[:, jj][:, :, ii]
 
 
-def divide_data_by_scale_wavelet(blk, shift_ms=None, gain=None) -> np.ndarray:
+def _w3_padded(blk, P):
+    """wavelet3d_params of one angle mapped onto the padded traces (nyp, nxp) by
+    wavelet_index; the scalars as they are."""
+    ii = np.array([wavelet_index(i, blk.nx, blk.nxp) for i in range(blk.nxp)])
+    jj = np.array([wavelet_index(j, blk.ny, blk.nyp) for j in range(blk.nyp)])
+    return {k: (v[jj][:, ii] if isinstance(v, np.ndarray) and v.shape == (blk.ny, blk.nx) else v)
+            for k, v in P.items()}
+
+
+def divide_data_by_scale_wavelet(blk, shift_ms=None, gain=None, w3=None) -> np.ndarray:
     """AVOInversion::divideDataByScaleWavelet (src/avoinversion.cpp:484-612) on every data
     grid: per trace (i < nxp, j < nyp) the 1/sqrt(nzp) scale and z taper, r2c along z,
     the adjustment factor inside the band deltaF*k in (lowCut, highCut) with
     deltaF = nz*1000/(relThick*lz*nzp) and zero outside, c2r, 1/sqrt(nzp).  The transforms
     in float64.  shift_ms / gain: per angle (ny, nx) local wavelet grids or None
-    (adjustment_factor_local).  Returns (ntheta, nzp, nyp, rnxp) float64 (padding columns
-    zero)."""
+    (adjustment_factor_local).  w3: 3D wavelets (the wavelet3d_params input dict): the stretch
+    becomes float32(relThick * double(local stretch)) (src/avoinversion.cpp:557) and the
+    factor adjustment_factor_local's 3D form.  Returns (ntheta, nzp, nyp, rnxp) float64
+    (padding columns zero)."""
     f32 = np.float32
     nxp, nyp, nzp, nz = blk.nxp, blk.nyp, blk.nzp, blk.nz
     cn = nzp // 2 + 1
@@ -510,13 +687,19 @@ def divide_data_by_scale_wavelet(blk, shift_ms=None, gain=None) -> np.ndarray:
     fk = deltaF[None] * k[:, None, None]                         # (cn, nyp, nxp)
     band = (fk < float(f32(blk.high_cut))) & (fk > float(f32(blk.low_cut)))
     out = np.zeros((blk.ntheta, nzp, nyp, 2 * (nxp // 2 + 1)))
-    local = shift_ms is not None or gain is not None
+    local = shift_ms is not None or gain is not None or w3 is not None
     if local:
         ish, gn = local_wavelet_maps(blk, shift_ms, gain)
+    w3p = wavelet3d_params(blk, w3) if w3 is not None else None
     for l in range(blk.ntheta):
         v = (blk.data[l][..., :nxp].astype(f32) / rsq).astype(f32) * taper[:, None, None]
         spec = np.fft.rfft(v.astype(np.float64), axis=0)
-        if local:
+        if w3p is not None:
+            P = _w3_padded(blk, w3p[l])
+            sfl = (rt * P["stretch"].astype(np.float64)).astype(f32)
+            W3 = {kk: (vv[None] if isinstance(vv, np.ndarray) and vv.ndim == 2 else vv) for kk, vv in P.items()}
+            fac = adjustment_factor_local(tab, l, sfl[None], k[:, None, None], ish[l][None], gn[l][None], nzp, w3=W3)
+        elif local:
             fac = adjustment_factor_local(tab, l, sf[None], k[:, None, None], ish[l][None], gn[l][None], nzp)
         else:
             fac = adjustment_factor(tab, l, sf[None], k[:, None, None])
@@ -526,12 +709,14 @@ def divide_data_by_scale_wavelet(blk, shift_ms=None, gain=None) -> np.ndarray:
     return out
 
 
-def residual_synthetics(blk, resid: np.ndarray, shift_ms=None, gain=None) -> np.ndarray:
+def residual_synthetics(blk, resid: np.ndarray, shift_ms=None, gain=None, w3=None) -> np.ndarray:
     """AVOInversion::multiplyDataByScaleWaveletAndWriteToFile (src/avoinversion.cpp:721-790)
     on real residual grids resid (ntheta, nzp, nyp, rnxp) (after invFFTInPlace): every trace
     i < nx, j < ny divided by float(sqrt(float(nzp))), r2c along z, times the conjugate of
     its local wavelet's spectrum stretched by relThick (getCAmp(k, sf)), c2r, divided by
-    float(sqrt(double(nzp))); the other traces as given.  Transforms in float64."""
+    float(sqrt(double(nzp))); the other traces as given.  w3: 3D wavelets (wavelet3d_params'
+    input): the local wavelet carries the dip factor and the stretch is float32(relThick) *
+    local stretch (:748).  Transforms in float64."""
     f32 = np.float32
     nx, ny, nzp = blk.nx, blk.ny, blk.nzp
     cn = nzp // 2 + 1
@@ -545,11 +730,23 @@ def residual_synthetics(blk, resid: np.ndarray, shift_ms=None, gain=None) -> np.
     ish, gn = local_wavelet_maps(blk, shift_ms, gain)
     k = np.arange(cn)[:, None, None]
     out = np.array(resid, dtype=np.float64, copy=True)
+    w3p = wavelet3d_params(blk, w3) if w3 is not None else None
     for l in range(blk.ntheta):
         v = (np.asarray(resid[l][:, :ny, :nx], dtype=f32) / rsq).astype(f32)
         spec = np.fft.rfft(v.astype(np.float64), axis=0)
-        wr, wi = interp_scaled32(lambda m: shift_scale32(W[l], ish[l][None, :ny, :nx], gn[l][None, :ny, :nx], m, nzp),
-                                 cn, k, sf[None])
+        sfl = sf
+        if w3p is not None:
+            P = w3p[l]
+            sfl = (sf * P["stretch"]).astype(f32)
+
+        def at(m, l=l):
+            m = np.asarray(m)
+            cr, ci = W[l].real.astype(f32)[m], W[l].imag.astype(f32)[m]
+            if w3p is not None:
+                fct = dip_factor32(w3p[l]["den"], m, w3p[l]["mult"][None], w3p[l]["H"][None])
+                cr, ci = (cr * fct).astype(f32), (ci * fct).astype(f32)
+            return shift_scale_vals32(cr, ci, ish[l][None, :ny, :nx], gn[l][None, :ny, :nx], m, nzp)
+        wr, wi = interp_scaled32(at, cn, k, sfl[None])
         spec = spec * (wr.astype(np.float64) - 1j * wi.astype(np.float64))
         out[l][:, :ny, :nx] = np.fft.irfft(spec, n=nzp, axis=0) * nzp / float(rsq_out)
     return out
