@@ -550,6 +550,8 @@ def nonconst_main(args):
     ctx = api.Context(0)
     job = api.Job(ctx, blk, api.PRIOR_SEPARABLE, 0, seed=1000)
     keep = job.upload_block()
+    if args.wavelet3d:
+        job.set_wavelet_3d(**synth.wavelet3d_model(blk, blk.spec.theta_deg, seed=7))
 
     def restore():
         for l in range(blk.ntheta):
@@ -587,7 +589,9 @@ def nonconst_main(args):
         "value": blk.n_voxels / (ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"single block {blk.nx}x{blk.ny}x{blk.nz}, {blk.ntheta} angles, {job.nsim} "
-                               f"realisations, rel_thick in [0.75, 1.3]", "l2": "inputs > 126 MB L2"},
+                               f"realisations, rel_thick in [0.75, 1.3]"
+                               + (", 3D wavelets (dip-adjusted per trace, Halpha damping)" if args.wavelet3d else ""),
+                   "l2": "inputs > 126 MB L2"},
         "gpu_launches": launches,
         "kernel_ms_per_step": {c: kt[c][0] / args.steps for c in kt if kt[c][1]},
         "roofline": {"bound": "hbm", "kernel": "thick_divide", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -752,6 +756,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--dims", default=None, help="nx,ny,nz of a smaller block (profiling runs only)")
     ap.add_argument("--no-legs", action="store_true", help="skip the batched and served legs")
+    ap.add_argument("--wavelet3d", action="store_true",
+                    help="with --nonconst: 3D wavelets (synthetic depth gradients and filter surfaces)")
     ap.add_argument("--nonconst", action="store_true",
                     help="measure the non-constant-thickness path instead (one GPU, its own JSON line)")
     ap.add_argument("--kernels", action="store_true",

@@ -31,6 +31,25 @@ def test_clock_summary(tmp_path):
     assert c["samples"] == 2
 
 
+def test_clock_merge_prefers_the_timed_region_samples(tmp_path):
+    p = tmp_path / "c.csv"
+    p.write_text(
+        "index, clocks.sm [MHz], clocks.max.sm [MHz], power.draw [W], active, hw, hwt, swt, swpc\n"
+        "0, 345 MHz, 1965 MHz, 120 W, 0x1, Not Active, Not Active, Not Active, Not Active\n"
+        "0, 1800 MHz, 1965 MHz, 990 W, 0x4, Not Active, Not Active, Not Active, Active\n")
+    smi = bench.summarize_clocks(str(p), 0)
+
+    class Nvml:
+        sm = [1965.0, 1950.0, 1965.0]
+        reasons = {"hw_slowdown"}
+        max_mhz = 1965.0
+    c = bench.merge_clocks(smi, Nvml())
+    assert c["sm_mhz"] == 1965.0 and c["samples"] == 3 and c["nvidia_smi_samples"] == 2
+    assert c["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    assert "_sm" not in c and "_sm" not in bench.merge_clocks(smi, None)
+    assert bench.merge_clocks(None, None) is None
+
+
 def test_physical_gpu_index(monkeypatch):
     monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "3,5")
     assert bench.physical_gpu_index(1) == 5
