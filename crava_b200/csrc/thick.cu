@@ -54,6 +54,13 @@ __device__ __forceinline__ float2 interp_scaled(int cnzp, int k, float scale, At
   return make_float2(__fdiv_rn(re, scale), __fdiv_rn(im, scale));
 }
 
+// interp_scaled's last step for two spectra at the same position: (a e + b d) / scale.
+__device__ __forceinline__ float2 lerp_scaled(float2 a, float2 b, float e, float d, float scale) {
+  const float re = __fadd_rn(__fmul_rn(a.x, e), __fmul_rn(b.x, d));
+  const float im = __fadd_rn(__fmul_rn(a.y, e), __fmul_rn(b.y, d));
+  return make_float2(__fdiv_rn(re, scale), __fdiv_rn(im, scale));
+}
+
 __device__ __forceinline__ float2 camp_scaled(const float2* c, int cnzp, int k, float scale) {
   return interp_scaled(cnzp, k, scale, [&](int m) { return __ldg(c + m); });
 }
@@ -137,19 +144,35 @@ __device__ __forceinline__ float2 local_wavelet(const ThickParams& P, int l, int
   return shift_scale(c, w.ish, w.gn, m, P.nzp);
 }
 
-__device__ __forceinline__ float2 local_es3(const ThickParams& P, int l, int m, const LocalWavelet& w) {
+// The local wavelet's spectrum (w) and errorSmooth3 (e) at bin m, as local_wavelet and its
+// errorSmooth3 above, sharing the dip factor and the shift's angle (one double exp and one
+// double sincos per bin; the same float operations as evaluating them apart).
+struct LocalBin {
+  float2 w, e;
+};
+
+__device__ __forceinline__ LocalBin local_pair(const ThickParams& P, int l, int m, const LocalWavelet& w) {
   const int cn = P.cnzp;
-  float2 c = m < cn - 1 ? __ldg(P.es3 + (size_t)l * cn + m) : P.es3_last[l];
+  float2 c = __ldg(P.wamp + (size_t)l * cn + m);
+  float2 s = m < cn - 1 ? __ldg(P.es3 + (size_t)l * cn + m) : P.es3_last[l];
   if (P.w3_mult) {
     const float f = dip_factor(P.w3_den, m, w.mult, w.H);
-    c = make_float2(__fmul_rn(__fmul_rn(c.x, f), w.gam), __fmul_rn(__fmul_rn(c.y, f), w.gam));
+    c = make_float2(__fmul_rn(c.x, f), __fmul_rn(c.y, f));
+    s = make_float2(__fmul_rn(__fmul_rn(s.x, f), w.gam), __fmul_rn(__fmul_rn(s.y, f), w.gam));
   }
-  float2 v = shift_scale(c, w.ish, 1.f, m, P.nzp);
+  const double a = 2.0 * (3.14159265358979323846 * (double)w.ish * (double)m) / (double)(float)P.nzp;
+  double sn, cs;
+  sincos(a, &sn, &cs);
+  const float mr = (float)((double)w.gn * cs), mi = (float)((double)w.gn * -sn);   // gain gn
+  const float nr = (float)cs, ni = (float)-sn;                                      // gain 1
+  LocalBin r;
+  r.w = make_float2(__fsub_rn(__fmul_rn(mr, c.x), __fmul_rn(mi, c.y)), __fadd_rn(__fmul_rn(mi, c.x), __fmul_rn(mr, c.y)));
+  r.e = make_float2(__fsub_rn(__fmul_rn(nr, s.x), __fmul_rn(ni, s.y)), __fadd_rn(__fmul_rn(ni, s.x), __fmul_rn(nr, s.y)));
   if (m == cn - 1) {
-    v.y = -99999.0f;
-    if (!(P.nzp & 1)) v.x = -99999.0f;
+    r.e.y = -99999.0f;
+    if (!(P.nzp & 1)) r.e.x = -99999.0f;
   }
-  return v;
+  return r;
 }
 
 // computeAdjustmentFactor (src/avoinversion.cpp:630-719) with a trace's local wavelet: wLoc
@@ -161,12 +184,25 @@ __device__ __forceinline__ float2 local_es3(const ThickParams& P, int l, int m, 
 __device__ __forceinline__ float2 adjustment_local(const ThickParams& P, int l, int k, float sf, const LocalWavelet& w) {
   const int cn = P.cnzp;
   const float wn2 = w.wn2, wnc = P.wnc, ev = P.err_var[l];
-  const float2 wLoc = interp_scaled(cn, k, sf, [&](int m) { return local_wavelet(P, l, m, w); });
+  // getCAmp(k, sf) of both local spectra (interp_scaled's steps, one position)
+  float2 wLoc = make_float2(0.f, 0.f), eLoc = wLoc;
+  const float om = __fdiv_rn((float)k, sf);
+  if (om < (float)cn) {
+    const int lo = (int)floorf(om);
+    int hi = lo + 1;
+    if (hi >= cn) hi -= 1;
+    const float d = __fsub_rn(om, (float)lo);
+    const float e = __fsub_rn(1.f, d);
+    const LocalBin A = local_pair(P, l, lo, w), B = local_pair(P, l, hi, w);
+    wLoc = lerp_scaled(A.w, B.w, e, d, sf);
+    eLoc = lerp_scaled(A.e, B.e, e, d, sf);
+  }
+  const LocalBin K = local_pair(P, l, k, w);
   const float wLoc2 = sq2(wLoc);
-  const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(interp_scaled(cn, k, sf, [&](int m) { return local_es3(P, l, m, w); })));
+  const float sL = __fadd_rn(__fdiv_rn(wLoc2, wn2), sq2(eLoc));
   const float c = __fmul_rn(__fsub_rn(1.f, wnc), 0.5f);
   float s2L = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sL)));
-  const float sG = __fadd_rn(__fdiv_rn(sq2(local_wavelet(P, l, k, w)), wn2), sq2(local_es3(P, l, k, w)));
+  const float sG = __fadd_rn(__fdiv_rn(sq2(K.w), wn2), sq2(K.e));
   const float s2G = __fmul_rn(ev, __fadd_rn(wnc, __fmul_rn(c, sG)));
   const float wGlob2 = sq2(__ldg((P.wglob ? P.wglob : P.wamp) + (size_t)l * cn + k));
   const float tau2 = __ldg(P.tau2 + (size_t)l * cn + k);
@@ -198,6 +234,10 @@ __device__ __forceinline__ int wavelet_index(int i, int n, int np) {
 // i < nx, j < ny with their local wavelets (multiplyDataByScaleWaveletAndWriteToFile,
 // src/avoinversion.cpp:743-776: 1/sqrt(nzp), r2c, times the conjugate of
 // getCAmp(k, relThick) at every kz, c2r, 1/sqrt(nzp)) and leaves the other traces as they are.
+// LOCAL: mode 0 with local wavelets (shift/gain grids or 3D wavelets), whose per-trace factor
+// needs more registers than the tabulated one; a separate instantiation keeps the plain
+// division at its own register count.
+template <bool LOCAL>
 __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ ThickParams P) {
   extern __shared__ float2 sm[];
   const int nzp = P.nzp, W = P.W, lw = P.logW, half = nzp / 2;
@@ -312,14 +352,13 @@ __global__ void __launch_bounds__(256) k_thick_divide(const __grid_constant__ Th
       if (2 * m < P.nxp) {
         const double fk = __dmul_rn(s_df[2 * w], (double)k);
         if (fk < (double)P.high_cut && fk > (double)P.low_cut)
-          fa = (P.wshift || P.w3_mult) ? adjustment_local(P, l, k, s_sf[2 * w], s_lw[2 * w])
-                        : adjustment(P, l, k, s_sf[2 * w]);
+          fa = LOCAL ? adjustment_local(P, l, k, s_sf[2 * w], s_lw[2 * w]) : adjustment(P, l, k, s_sf[2 * w]);
       }
       if (2 * m + 1 < P.nxp) {
         const double fk = __dmul_rn(s_df[2 * w + 1], (double)k);
         if (fk < (double)P.high_cut && fk > (double)P.low_cut)
-          fb = (P.wshift || P.w3_mult) ? adjustment_local(P, l, k, s_sf[2 * w + 1], s_lw[2 * w + 1])
-                        : adjustment(P, l, k, s_sf[2 * w + 1]);
+          fb = LOCAL ? adjustment_local(P, l, k, s_sf[2 * w + 1], s_lw[2 * w + 1])
+                     : adjustment(P, l, k, s_sf[2 * w + 1]);
       }
     }
     a = cmul(a, fa);
@@ -525,10 +564,12 @@ int thick_tile_width(int nzp) {
 cudaError_t launch_thick_divide(const ThickParams& P, int nth, cudaStream_t st, int* nlaunch) {
   if (P.W < 1 || P.W > 32 || (P.W & (P.W - 1)) || (1 << P.logW) != P.W) return cudaErrorInvalidValue;
   const size_t smem = thick_smem_bytes(P.W, P.nzp);
-  cudaError_t e = cudaFuncSetAttribute(k_thick_divide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const bool local = P.mode == 0 && (P.wshift || P.w3_mult);
+  auto* k = local ? k_thick_divide<true> : k_thick_divide<false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)P.nIT, (unsigned)(P.mode == 1 ? P.ny : P.nyp), (unsigned)nth);
-  k_thick_divide<<<grid, 256, smem, st>>>(P);
+  k<<<grid, 256, smem, st>>>(P);
   if (nlaunch) (*nlaunch)++;
   return cudaGetLastError();
 }
