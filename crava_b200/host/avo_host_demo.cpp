@@ -14,6 +14,8 @@
 //   f32    cov[6][rsize] errCorr[rsize]                        (grids)
 //   f32    data[ntheta][rsize] mean[3][rsize]
 //   f32    noise[3*nsim][rsize]                                (host_noise)
+//   then optional sections, each after an int32 flag: non-constant thickness, correlation
+//   gradients, 3D wavelets (see the reads below)
 // out.bin: f32 mean[3][rsize] cov[6][rsize] sims[3*nsim][rsize] resid[ntheta][rsize],
 //          int64 inverted_bins chol_fallbacks sim_chol_zero fp64_bins, f32 postVar0[9],
 //          f32 fft round-trip max abs error of one DATA grid (FFTGrid::fftInPlace +
@@ -163,6 +165,39 @@ int main(int argc, char** argv) {
     if (fread(&grads, sizeof(int), 1, fi) == 1 && grads) {
       set.corrGradI = rd.one<float>();
       set.corrGradJ = rd.one<float>();
+    }
+    // optional trailing section after it: 3D wavelets (int32 ni nj has_grad has_halpha, f64 x0 y0
+    // dx dy, f32 theta[ntheta], gradX/gradY[nx*ny] if has_grad, alpha1[ntheta*ni*nj],
+    // halpha[ntheta*ni*nj] if has_halpha, global wavelets[ntheta*nzp], their norms[ntheta])
+    int w3 = 0;
+    if (fread(&w3, sizeof(int), 1, fi) == 1 && w3) {
+      set.waveletDim = 3;
+      set.filterNI = rd.one<int>();
+      set.filterNJ = rd.one<int>();
+      const int has_grad = rd.one<int>(), has_halpha = rd.one<int>();
+      set.filterX0 = rd.one<double>();
+      set.filterY0 = rd.one<double>();
+      set.filterDX = rd.one<double>();
+      set.filterDY = rd.one<double>();
+      set.theta.resize(nth);
+      rd.read(set.theta.data(), nth);
+      if (has_grad) {
+        set.depthGradX.resize((size_t)nx * ny);
+        set.depthGradY.resize((size_t)nx * ny);
+        rd.read(set.depthGradX.data(), set.depthGradX.size());
+        rd.read(set.depthGradY.data(), set.depthGradY.size());
+      }
+      const size_t nij = (size_t)set.filterNI * set.filterNJ;
+      set.filterAlpha1.resize(nth * nij);
+      rd.read(set.filterAlpha1.data(), set.filterAlpha1.size());
+      if (has_halpha) {
+        set.filterHalpha.resize(nth * nij);
+        rd.read(set.filterHalpha.data(), set.filterHalpha.size());
+      }
+      set.globalWavelet.assign(nth, std::vector<float>(nzp));
+      for (int l = 0; l < nth; l++) rd.read(set.globalWavelet[l].data(), nzp);
+      set.globalWaveletNorm.resize(nth);
+      rd.read(set.globalWaveletNorm.data(), nth);
     }
     fclose(fi);
 

@@ -266,6 +266,46 @@ void AVOInversion::run() {
     if ((int)noise_->size() != 3 * nsim) throw Error(CRAVA_EINVAL, "simulate: 3 noise grids per realisation");
     for (int q = 0; q < 3 * nsim; q++) up(CRAVA_ROLE_NOISE, q, (*noise_)[q]);
   }
+  // the wavelets' local shift and gain grids, and 3D wavelets (used by the division)
+  const size_t nxy = (size_t)d.nx * d.ny;
+  for (int l = 0; l < nth; l++) {
+    const float* sh = (size_t)l < set_.waveletShift.size() && !set_.waveletShift[l].empty()
+                          ? set_.waveletShift[l].data() : nullptr;
+    const float* gn = (size_t)l < set_.waveletGain.size() && !set_.waveletGain[l].empty()
+                          ? set_.waveletGain[l].data() : nullptr;
+    if ((sh && set_.waveletShift[l].size() != nxy) || (gn && set_.waveletGain[l].size() != nxy))
+      throw Error(CRAVA_EINVAL, "AVOInversion: wavelet shift and gain grids need nx*ny values");
+    if (sh || gn) check(crava_job_set_wavelet_grids(job, l, sh, gn));
+  }
+  std::vector<float> gw;
+  if (set_.waveletDim == 3) {
+    const size_t nij = (size_t)set_.filterNI * set_.filterNJ;
+    if ((int)set_.theta.size() != nth || set_.filterAlpha1.size() != nth * nij ||
+        (!set_.filterHalpha.empty() && set_.filterHalpha.size() != nth * nij) ||
+        (int)set_.globalWavelet.size() != nth || (int)set_.globalWaveletNorm.size() != nth ||
+        (!set_.depthGradX.empty() && set_.depthGradX.size() != nxy) ||
+        (!set_.depthGradY.empty() && set_.depthGradY.size() != nxy))
+      throw Error(CRAVA_EINVAL, "AVOInversion: 3D wavelet settings have the wrong sizes");
+    for (int l = 0; l < nth; l++) {
+      if ((int)set_.globalWavelet[l].size() != d.nzp) throw Error(CRAVA_EINVAL, "AVOInversion: global wavelet needs nzp samples");
+      gw.insert(gw.end(), set_.globalWavelet[l].begin(), set_.globalWavelet[l].end());
+    }
+    crava_wavelet3d_desc w{};
+    w.grad_x = set_.depthGradX.empty() ? nullptr : set_.depthGradX.data();
+    w.grad_y = set_.depthGradY.empty() ? nullptr : set_.depthGradY.data();
+    w.theta = set_.theta.data();
+    w.filter_ni = set_.filterNI;
+    w.filter_nj = set_.filterNJ;
+    w.filter_x0 = set_.filterX0;
+    w.filter_y0 = set_.filterY0;
+    w.filter_dx = set_.filterDX;
+    w.filter_dy = set_.filterDY;
+    w.alpha1 = set_.filterAlpha1.data();
+    w.halpha = set_.filterHalpha.empty() ? nullptr : set_.filterHalpha.data();
+    w.global_wavelet = gw.data();
+    w.global_wavelet_norm = set_.globalWaveletNorm.data();
+    check(crava_job_set_wavelet_3d(job, &w));
+  }
   // the constructor's divideDataByScaleWavelet (src/avoinversion.cpp:226-227)
   if (d.flags & CRAVA_FLAG_NONCONST_THICK) check(crava_job_divide_data(job, nullptr));
   check(crava_job_run(job, nullptr));

@@ -142,6 +142,20 @@ struct AVOInversionSettings {
   // (divideDataByScaleWavelet + interpolateSeismic).  Empty: constant thickness.
   std::vector<double> relThick;
   float energyThreshold = 0;               // ModelSettings::getEnergyThreshold
+  // Local wavelets of the division (Wavelet::shiftGrid_ / gainGrid_ in ms and as factors,
+  // nx*ny per angle, index i+nx*j; an empty angle or an empty vector: none)
+  std::vector<std::vector<float>> waveletShift, waveletGain;
+  // 3D wavelets (Wavelet3D, getDim() == 3): the wavelets above are their own pulses; the
+  // filter surfaces, depth gradients, angles and global (average) wavelets as in
+  // crava_wavelet3d_desc.  waveletDim 1: none of these is used.
+  int waveletDim = 1;
+  std::vector<float> depthGradX, depthGradY;                 // nx*ny each, or empty
+  std::vector<float> theta;                                  // ntheta radians
+  int filterNI = 0, filterNJ = 0;
+  double filterX0 = 0, filterY0 = 0, filterDX = 1, filterDY = 1;
+  std::vector<float> filterAlpha1, filterHalpha;             // ntheta x ni*nj; Halpha may be empty
+  std::vector<std::vector<float>> globalWavelet;             // ntheta x nzp
+  std::vector<float> globalWaveletNorm;                      // ntheta
   // lateral correlation gradients of InitializeCorrelations (samples per index); with the
   // separable factors and a nonzero gradient the prior grids are generated on the device
   float corrGradI = 0, corrGradJ = 0;

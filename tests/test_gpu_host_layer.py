@@ -29,7 +29,7 @@ def crel(x, ref):
     return float(np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300))
 
 
-def write_block(path, blk, grids, noise):
+def write_block(path, blk, grids, noise, w3=None):
     rnxp = 2 * (blk.nxp // 2 + 1)
     shape = (blk.nzp, blk.nyp, rnxp)
 
@@ -64,14 +64,29 @@ def write_block(path, blk, grids, noise):
             np.ascontiguousarray(noise, dtype=np.complex64).tofile(f)
         nonconst = getattr(blk, "rel_thick", None) is not None
         grads = not grids and (blk.corr_grad_i != 0.0 or blk.corr_grad_j != 0.0)
-        if nonconst or grads:
+        if nonconst or grads or w3 is not None:
             np.array([1 if nonconst else 0], dtype=np.int32).tofile(f)
         if nonconst:
             np.ascontiguousarray(blk.rel_thick, dtype=np.float64).tofile(f)
             np.array([blk.energy_threshold], dtype=np.float32).tofile(f)
+        if grads or w3 is not None:
+            np.array([1 if grads else 0], dtype=np.int32).tofile(f)
         if grads:
-            np.array([1], dtype=np.int32).tofile(f)
             np.array([blk.corr_grad_i, blk.corr_grad_j], dtype=np.float32).tofile(f)
+        if w3 is not None:
+            a1 = np.asarray(w3["alpha1"], dtype=np.float32)
+            has_grad, has_h = w3["grad_x"] is not None, w3["halpha"] is not None
+            np.array([1, a1.shape[2], a1.shape[1], int(has_grad), int(has_h)], dtype=np.int32).tofile(f)
+            np.array(w3["filter_geom"], dtype=np.float64).tofile(f)
+            np.asarray(w3["theta"], dtype=np.float32).tofile(f)
+            if has_grad:
+                np.asarray(w3["grad_x"], dtype=np.float32).tofile(f)
+                np.asarray(w3["grad_y"], dtype=np.float32).tofile(f)
+            a1.tofile(f)
+            if has_h:
+                np.asarray(w3["halpha"], dtype=np.float32).tofile(f)
+            np.asarray(w3["global_wavelet"], dtype=np.float32).tofile(f)
+            np.asarray(w3["global_wavelet_norm"], dtype=np.float32).tofile(f)
 
 
 def read_out(path, blk):
@@ -119,22 +134,24 @@ def test_host_layer_matches_oracle(tmp_path, grids):
     assert out["fft_roundtrip"] < 1e-5 * scale
 
 
-@pytest.mark.parametrize("grids", [False, True])
-def test_host_layer_nonconst_thickness(tmp_path, grids):
+@pytest.mark.parametrize("grids,wavelet3d", [(False, False), (True, False), (False, True)])
+def test_host_layer_nonconst_thickness(tmp_path, grids, wavelet3d):
     """AVOInversionSettings::relThick: the layer divides the data by the scale wavelet
     (crava_job_divide_data) before the inversion, and in GRIDS mode reads the temporal
-    correlation from the covVp grid's (0, 0) column."""
+    correlation from the covVp grid's (0, 0) column; with waveletDim 3 the division uses the
+    dip-adjusted local wavelets of 3D wavelets (crava_job_set_wavelet_3d)."""
     import dataclasses
     assert os.path.exists(DEMO)
     blk = synth.make_block(synth.BlockSpec(nx=30, ny=28, nz=40, nxp=36, nyp=32, nzp=48, theta_deg=(8.0, 20.0, 32.0),
                                            peak_hz=(30.0,) * 3, sn=(5.0,) * 3, nsim=0, seed=19))
     blk = synth.with_rel_thick(blk, seed=7)
+    w3 = synth.wavelet3d_model(blk, blk.spec.theta_deg, seed=11) if wavelet3d else None
     fin, fout = tmp_path / "block.bin", tmp_path / "out.bin"
-    write_block(fin, blk, grids, None)
+    write_block(fin, blk, grids, None, w3=w3)
     r = subprocess.run([DEMO, str(fin), str(fout)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     out = read_out(fout, blk)
-    div = ref64.divide_data_by_scale_wavelet(blk)
+    div = ref64.divide_data_by_scale_wavelet(blk, w3=w3)
     divided = np.stack([ref64.interpolate_seismic(div[l], blk, blk.energy_threshold) for l in range(blk.ntheta)])
     post = ref64.posterior(dataclasses.replace(blk, data=divided))
     nx = blk.nxp
