@@ -50,6 +50,12 @@ def test_clock_merge_prefers_the_timed_region_samples(tmp_path):
     assert bench.merge_clocks(None, None) is None
 
 
+def test_fifo_replay():
+    span, lat = bench.fifo_replay([0.0, 0.1, 0.15, 1.0], [0.2, 0.05, 0.1, 0.05])
+    assert abs(span - 1.05) < 1e-12
+    assert [round(v, 6) for v in lat] == [200.0, 150.0, 200.0, 50.0]
+
+
 def test_physical_gpu_index(monkeypatch):
     monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "3,5")
     assert bench.physical_gpu_index(1) == 5
